@@ -1,0 +1,257 @@
+"""ctypes access to the CPU parity checker (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py.  The product (pepc_b200) never imports this.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REF = None
+
+D = C.POINTER(C.c_double)
+I64 = C.POINTER(C.c_int64)
+I32 = C.POINTER(C.c_int32)
+
+
+class OrcParams(C.Structure):
+    _fields_ = [
+        ("theta2", C.c_double),
+        ("eps2", C.c_double),
+        ("curve", C.c_int32),
+        ("walk", C.c_int32),
+        ("tile_size", C.c_int32),
+        ("force_cubic_domain", C.c_int32),
+        ("periodicity", C.c_int32 * 3),
+        ("mirror_box_layers", C.c_int32),
+        ("include_far_field_if_periodic", C.c_int32),
+        ("fmm_extrinsic_correction", C.c_int32),
+        ("t_lattice_1", C.c_double * 3),
+        ("t_lattice_2", C.c_double * 3),
+        ("t_lattice_3", C.c_double * 3),
+        ("lattice_origin", C.c_double * 3),
+        ("num_threads", C.c_int32),
+    ]
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError("oracle/liboracle.so is not built (run make -C oracle)")
+        L = C.CDLL(path)
+        L.orc_params_default.argtypes = [C.POINTER(OrcParams)]
+        L.orc_box_create.argtypes = [C.c_int64, D, D, D, C.c_int32, D]
+        L.orc_compute_keys.argtypes = [C.c_int64, D, D, D, D, D, C.c_int32, I64]
+        L.orc_key_to_coord.argtypes = [C.c_int64, D, D, C.c_int32, D]
+        L.orc_sort_radix.argtypes = [C.c_int64, I64, I64]
+        L.orc_multipole_from_particle.argtypes = [D, C.c_double, D]
+        L.orc_shift_multipoles_up.argtypes = [D, D, C.c_int32]
+        L.orc_force_leaf.argtypes = [D, D, C.c_double, D, D]
+        L.orc_force_twig.argtypes = [D, D, C.c_double, D, D]
+        L.orc_par_rand.argtypes = [C.c_int32, C.c_int64, D]
+        L.orc_create.argtypes = [C.POINTER(OrcParams)]
+        L.orc_create.restype = C.c_void_p
+        L.orc_destroy.argtypes = [C.c_void_p]
+        L.orc_grow_tree.argtypes = [C.c_void_p, C.c_int64, D, D, D, D, I64, I64, D, D, D, D]
+        L.orc_grow_tree.restype = C.c_int
+        L.orc_traverse_tree.argtypes = [C.c_void_p, C.c_int64, D, D, D, I64, D, D, D, D, D]
+        L.orc_traverse_tree.restype = C.c_int
+        L.orc_num_nodes.argtypes = [C.c_void_p]
+        L.orc_num_nodes.restype = C.c_int64
+        L.orc_tree_export.argtypes = [C.c_void_p, I64, I32, I64, I64, I64, I64, I64, D]
+        L.orc_box.argtypes = [C.c_void_p, D]
+        L.orc_counters.argtypes = [C.c_void_p, I64]
+        L.orc_direct.argtypes = [C.c_void_p, C.c_int64, I64, D, D, D, D]
+        L.orc_direct.restype = C.c_int
+        L.orc_lattice.argtypes = [C.c_void_p, C.c_int64, D, D, D, D, D, D, D]
+        L.orc_lattice.restype = C.c_int
+        L.orc_fmm_lattice_coefficients.argtypes = [C.POINTER(OrcParams), D]
+        _LIB = L
+    return _LIB
+
+
+def ref_lib():
+    """The reference's own sort, compiled from its sources into oracle/_ref."""
+    global _REF
+    if _REF is None:
+        path = os.path.join(HERE, "_ref", "libslref.so")
+        if not os.path.exists(path):
+            return None
+        R = C.CDLL(path)
+        R.ref_sort_keys.argtypes = [C.c_int64, I64, I64]
+        R.ref_sort_keys.restype = C.c_int
+        _REF = R
+    return _REF
+
+
+def dp(a):
+    return a.ctypes.data_as(D)
+
+
+def ip(a):
+    return a.ctypes.data_as(I64)
+
+
+def i32p(a):
+    return a.ctypes.data_as(I32)
+
+
+def f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def params(**kw):
+    p = OrcParams()
+    lib().orc_params_default(C.byref(p))
+    for k, v in kw.items():
+        if k in ("periodicity", "t_lattice_1", "t_lattice_2", "t_lattice_3", "lattice_origin"):
+            arr = getattr(p, k)
+            for i in range(3):
+                arr[i] = v[i]
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def box_create(x, y, z, force_cubic=False):
+    x, y, z = f64(x), f64(y), f64(z)
+    out = np.zeros(9)
+    lib().orc_box_create(len(x), dp(x), dp(y), dp(z), int(force_cubic), dp(out))
+    return out
+
+
+def compute_keys(x, y, z, boxmin, boxsize, curve=0):
+    x, y, z = f64(x), f64(y), f64(z)
+    bm, bs = f64(boxmin), f64(boxsize)
+    k = np.zeros(len(x), dtype=np.int64)
+    lib().orc_compute_keys(len(x), dp(x), dp(y), dp(z), dp(bm), dp(bs), curve, ip(k))
+    return k
+
+
+def key_to_coord(key, boxmin, boxsize, curve=0):
+    bm, bs = f64(boxmin), f64(boxsize)
+    out = np.zeros(3)
+    lib().orc_key_to_coord(int(key), dp(bm), dp(bs), curve, dp(out))
+    return out
+
+
+def sort_radix(keys):
+    k = np.array(keys, dtype=np.int64)
+    idx = np.arange(len(k), dtype=np.int64)
+    lib().orc_sort_radix(len(k), ip(k), ip(idx))
+    return k, idx
+
+
+def ref_sort(keys):
+    R = ref_lib()
+    if R is None:
+        return None
+    k = np.array(keys, dtype=np.int64)
+    idx = np.zeros(len(k), dtype=np.int64)
+    R.ref_sort_keys(len(k), ip(k), ip(idx))
+    return k, idx
+
+
+def par_rand(iseed, n):
+    out = np.zeros(n)
+    lib().orc_par_rand(int(iseed), int(n), dp(out))
+    return out
+
+
+def lattice_coefficients(p):
+    out = np.zeros(2 * 861)
+    lib().orc_fmm_lattice_coefficients(C.byref(p), dp(out))
+    return out[0::2] + 1j * out[1::2]
+
+
+class Oracle:
+    """Whole-path CPU restatement with the same call shape as pepc_b200.TreeCode."""
+
+    def __init__(self, **kw):
+        self.p = params(**kw)
+        self.h = lib().orc_create(C.byref(self.p))
+
+    def close(self):
+        if self.h:
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def grow_tree(self, x, y, z, q):
+        n = len(x)
+        x, y, z, q = f64(x), f64(y), f64(z), f64(q)
+        key = np.zeros(n, dtype=np.int64)
+        perm = np.zeros(n, dtype=np.int64)
+        xo, yo, zo, qo = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(n)
+        rc = lib().orc_grow_tree(self.h, n, dp(x), dp(y), dp(z), dp(q), ip(key), ip(perm),
+                                 dp(xo), dp(yo), dp(zo), dp(qo))
+        if rc != 0:
+            raise RuntimeError(f"orc_grow_tree failed: {rc}")
+        return dict(key=key, perm=perm, x=xo, y=yo, z=zo, q=qo)
+
+    def traverse_tree(self, x, y, z, keys=None, e=None, pot=None, work=None):
+        n = len(x)
+        x, y, z = f64(x), f64(y), f64(z)
+        ex = np.zeros(n) if e is None else f64(e[0]).copy()
+        ey = np.zeros(n) if e is None else f64(e[1]).copy()
+        ez = np.zeros(n) if e is None else f64(e[2]).copy()
+        pt = np.zeros(n) if pot is None else f64(pot).copy()
+        wk = np.zeros(n) if work is None else f64(work).copy()
+        kp = None
+        if keys is not None:
+            keys = np.ascontiguousarray(keys, dtype=np.int64)
+            kp = ip(keys)
+        rc = lib().orc_traverse_tree(self.h, n, dp(x), dp(y), dp(z), kp, dp(ex), dp(ey), dp(ez),
+                                     dp(pt), dp(wk))
+        if rc != 0:
+            raise RuntimeError(f"orc_traverse_tree failed: {rc}")
+        return dict(ex=ex, ey=ey, ez=ez, pot=pt, work=wk)
+
+    def tree(self):
+        n = lib().orc_num_nodes(self.h)
+        out = dict(key=np.zeros(n, np.int64), level=np.zeros(n, np.int32),
+                   leaves=np.zeros(n, np.int64), descendants=np.zeros(n, np.int64),
+                   parent=np.zeros(n, np.int64), first_child=np.zeros(n, np.int64),
+                   next_sibling=np.zeros(n, np.int64), moments=np.zeros((n, 15)))
+        lib().orc_tree_export(self.h, ip(out["key"]), i32p(out["level"]), ip(out["leaves"]),
+                              ip(out["descendants"]), ip(out["parent"]), ip(out["first_child"]),
+                              ip(out["next_sibling"]), dp(out["moments"]))
+        return out
+
+    def box(self):
+        out = np.zeros(9)
+        lib().orc_box(self.h, dp(out))
+        return out
+
+    def counters(self):
+        out = np.zeros(2, np.int64)
+        lib().orc_counters(self.h, ip(out))
+        return dict(interactions=int(out[0]), mac_evaluations=int(out[1]))
+
+    def direct(self, tidx):
+        tidx = np.ascontiguousarray(tidx, dtype=np.int64)
+        n = len(tidx)
+        ex, ey, ez, pt = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(n)
+        rc = lib().orc_direct(self.h, n, ip(tidx), dp(ex), dp(ey), dp(ez), dp(pt))
+        if rc != 0:
+            raise RuntimeError(f"orc_direct failed: {rc}")
+        return dict(ex=ex, ey=ey, ez=ez, pot=pt)
+
+    def lattice(self, x, y, z):
+        n = len(x)
+        x, y, z = f64(x), f64(y), f64(z)
+        ex, ey, ez, pt = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(n)
+        rc = lib().orc_lattice(self.h, n, dp(x), dp(y), dp(z), dp(ex), dp(ey), dp(ez), dp(pt))
+        if rc != 0:
+            raise RuntimeError("lattice term needs a periodic context")
+        return dict(ex=ex, ey=ey, ez=ez, pot=pt)

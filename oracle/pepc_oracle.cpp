@@ -1,0 +1,965 @@
+// pepc_oracle.cpp -- CPU FP64 restatement of PEPC's tree-code force evaluation.
+//
+// TEST INFRASTRUCTURE ONLY: this is the parity checker for libpepcg (the CUDA
+// library).  It is loaded by the tests, the smoke check and the CPU-baseline
+// leg of the benchmark, never by the product path.
+//
+// Every routine restates the reference (ALaDyn/pepc, Fortran 2003) and cites
+// the file:line it follows.  Paths are relative to the reference's src/ tree.
+// Build with -ffp-contract=off: the operation order below is the contract.
+
+#include "pepc_oracle.h"
+
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+namespace {
+
+constexpr int kMaxLevel = 20;  // treevars.f90:55 -> (64-2)/3 = 20 for idim = 3
+constexpr int64_t kNodeInvalid = -1;
+
+// ---------------------------------------------------------------------------
+// Box (treecode/lpepcsrc/module_box.f90:48-93)
+// ---------------------------------------------------------------------------
+struct Box {
+  double min[3], max[3], size[3];
+};
+
+Box box_create(int64_t n, const double* x, const double* y, const double* z, bool cubic) {
+  Box b;
+  const double* c[3] = {x, y, z};
+  for (int d = 0; d < 3; ++d) {
+    double lo = c[d][0], hi = c[d][0];
+    for (int64_t i = 1; i < n; ++i) {
+      lo = std::min(lo, c[d][i]);
+      hi = std::max(hi, c[d][i]);
+    }
+    b.min[d] = lo;
+    b.max[d] = hi;
+  }
+  if (cubic) {  // module_box.f90:71-74
+    double lo = std::min(b.min[0], std::min(b.min[1], b.min[2]));
+    double hi = std::max(b.max[0], std::max(b.max[1], b.max[2]));
+    for (int d = 0; d < 3; ++d) { b.min[d] = lo; b.max[d] = hi; }
+  }
+  // module_box.f90:81-84: safety margin of boxsize/10000 on both sides
+  for (int d = 0; d < 3; ++d) {
+    double s = b.max[d] - b.min[d];
+    b.min[d] = b.min[d] - s / 10000.0;
+    b.max[d] = b.max[d] + s / 10000.0;
+    b.size[d] = b.max[d] - b.min[d];
+  }
+  return b;
+}
+
+// ---------------------------------------------------------------------------
+// Keys (treecode/lpepcsrc/module_spacefilling.f90)
+// ---------------------------------------------------------------------------
+// coord_to_intcoord_with_refinement_length, module_spacefilling.f90:207-219:
+// s = boxsize / 2**maxlevel (:238), ic = int((x - boxmin) / s)  (truncation)
+inline void coord_to_intcoord(const Box& b, const double s[3], double x, double y, double z,
+                              int64_t ic[3]) {
+  ic[0] = (int64_t)((x - b.min[0]) / s[0]);
+  ic[1] = (int64_t)((y - b.min[1]) / s[1]);
+  ic[2] = (int64_t)((z - b.min[2]) / s[2]);
+}
+
+// intcoord_to_key_hilbert3D, module_spacefilling.f90:380-440 (Kamata et al.)
+const int kCI3[8] = {0, 1, 3, 2, 7, 6, 4, 5};          // :389
+const int kG3x[8] = {5, 6, 0, 5, 5, 0, 6, 5};          // :390, G3(:,0) exchange
+const int kG3r[8] = {0, 0, 0, 5, 0, 0, 6, 5};          // :390, G3(:,1) reverse
+
+int64_t intcoord_to_key_hilbert3d(const int64_t ic_in[3]) {
+  int64_t it[3] = {ic_in[0], ic_in[1], ic_in[2]};
+  int64_t key = 1;  // placeholder bit, :402
+  for (int i = kMaxLevel - 1; i >= 0; --i) {
+    int64_t cval = 0;
+    for (int j = 3; j >= 1; --j) {  // :409-412, cval = z<<2 | y<<1 | x
+      cval = (cval << 1) | ((it[j - 1] >> i) & 1);
+      it[j - 1] &= ~(int64_t(1) << i);
+    }
+    int h = kCI3[cval];
+    int exch = kG3x[h], rev = kG3r[h];
+    key = (key << 3) | h;  // :420
+    if (exch == 5) std::swap(it[0], it[2]);       // :425-428
+    else if (exch == 6) std::swap(it[1], it[2]);  // :429-432
+    for (int j = 1; j <= 3; ++j)                  // :436-438
+      if ((rev >> (j - 1)) & 1) it[j - 1] = (~it[j - 1]) & ((int64_t(1) << i) - 1);
+  }
+  return key;
+}
+
+// 3D Morton (Z) curve: bit interleave with the same digit convention as the
+// Hilbert cell value (z<<2 | y<<1 | x), generalising intcoord_to_key_morton1D
+// (module_spacefilling.f90:291-308).  Not in the reference for idim = 3.
+int64_t intcoord_to_key_morton3d(const int64_t ic[3]) {
+  int64_t key = 1;
+  for (int i = kMaxLevel - 1; i >= 0; --i) {
+    int64_t cval = (((ic[2] >> i) & 1) << 2) | (((ic[1] >> i) & 1) << 1) | ((ic[0] >> i) & 1);
+    key = (key << 3) | cval;
+  }
+  return key;
+}
+
+// level_from_key, module_spacefilling.f90:47-57
+inline int level_from_key(int64_t key) {
+  return (63 - __builtin_clzll((unsigned long long)key)) / 3;
+}
+
+// key_to_intcoord_hilbert, module_spacefilling.f90:501-565
+void key_to_intcoord_hilbert(int64_t key, int64_t ic[3]) {
+  static const int C3[8] = {0, 1, 3, 2, 6, 7, 5, 4};  // :515
+  int lev = level_from_key(key);
+  ic[0] = ic[1] = ic[2] = 0;
+  for (int i = 0; i < lev; ++i) {
+    int h = (int)((key >> (3 * i)) & 7);
+    int cval = C3[h], rev = kG3r[h], exch = kG3x[h];
+    if (i > 0) {
+      for (int j = 1; j <= 3; ++j)
+        if ((rev >> (j - 1)) & 1) ic[j - 1] = (~ic[j - 1]) & ((int64_t(1) << i) - 1);
+      for (int j = 1; j <= 2; ++j) {
+        if (!((exch >> (j - 1)) & 1)) continue;
+        for (int k = j + 1; k <= 3; ++k)
+          if ((exch >> (k - 1)) & 1) std::swap(ic[j - 1], ic[k - 1]);
+      }
+    }
+    for (int j = 1; j <= 3; ++j) ic[j - 1] |= (int64_t)((cval >> (j - 1)) & 1) << i;
+  }
+  for (int j = 0; j < 3; ++j) ic[j] <<= (kMaxLevel - lev);
+}
+
+void key_to_intcoord_morton3d(int64_t key, int64_t ic[3]) {
+  int lev = level_from_key(key);
+  ic[0] = ic[1] = ic[2] = 0;
+  for (int i = 0; i < lev; ++i)
+    for (int j = 0; j < 3; ++j) ic[j] |= ((key >> (3 * i + j)) & 1) << i;
+  for (int j = 0; j < 3; ++j) ic[j] <<= (kMaxLevel - lev);
+}
+
+// key_to_coord, module_spacefilling.f90:445-471
+void key_to_coord(const Box& b, int64_t key, int curve, double x[3]) {
+  int64_t ic[3];
+  if (curve == 1) key_to_intcoord_morton3d(key, ic);
+  else key_to_intcoord_hilbert(key, ic);
+  for (int d = 0; d < 3; ++d) {
+    double s = b.size[d] / (double)(int64_t(1) << kMaxLevel);
+    x[d] = ((double)ic[d] + 0.5) * s + b.min[d];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Local key sort: restatement of the SL library's in-place MSD radix sort
+// (treecode/sl_pepc/src/core/sort_radix.c:33-119 rs_rec_ip, :122-151
+// sort_radix_ip; width 10 and insertion threshold 256 from
+// src/include/sl_tune_intern.h:22,30; insertion kernel sort_insert.c:14-37).
+// The element is (key, index); the reference also carries the work weight,
+// which does not influence the order.
+// ---------------------------------------------------------------------------
+void insert_sort_bmask(int64_t* k, int64_t* ix, int64_t n, uint64_t bmask) {
+  for (int64_t i = 1; i < n; ++i) {
+    if ((uint64_t(k[i]) & bmask) < (uint64_t(k[i - 1]) & bmask)) {
+      int64_t j = i - 1;
+      int64_t tk = k[i], ti = ix[i];
+      do {
+        k[j + 1] = k[j];
+        ix[j + 1] = ix[j];
+        if (--j < 0) break;
+      } while ((uint64_t(tk) & bmask) < (uint64_t(k[j]) & bmask));
+      k[j + 1] = tk;
+      ix[j + 1] = ti;
+    }
+  }
+}
+
+void rs_rec_ip(int64_t* k, int64_t* ix, int64_t n, int rhigh, int rlow, int rwidth) {
+  const int width = std::min(rwidth, rhigh - rlow + 1);
+  rhigh -= width - 1;
+  const int64_t ncls = int64_t(1) << width;
+  const int64_t mask = ncls - 1;
+  std::vector<int64_t> c(ncls, 0), parts(ncls);
+  auto cls = [&](int64_t key) { return (key >> rhigh) & mask; };
+  for (int64_t i = 0; i < n; ++i) ++c[cls(k[i])];
+  parts[0] = 0;
+  for (int64_t i = 1; i < ncls; ++i) parts[i] = parts[i - 1] + c[i - 1];
+  int64_t end = 0;
+  for (int64_t i = 0; i < ncls; ++i) {
+    end += c[i];
+    int64_t xi = parts[i];
+    while (xi < end) {
+      int64_t j = cls(k[xi]);
+      while (j != i) {
+        int64_t kk = cls(k[parts[j]]);
+        if (kk != j) {
+          std::swap(k[xi], k[parts[j]]);
+          std::swap(ix[xi], ix[parts[j]]);
+        }
+        ++parts[j];
+        j = kk;
+      }
+      ++xi;
+    }
+  }
+  --rhigh;
+  if (rhigh >= rlow) {
+    uint64_t bmask = 0;
+    if (rhigh - rlow + 1 <= 63) bmask = uint64_t(1) << (rhigh - rlow + 1);
+    bmask = (bmask - 1) << rlow;
+    int64_t off = 0;
+    for (int64_t i = 0; i < ncls; ++i) {
+      if (c[i] > 256) rs_rec_ip(k + off, ix + off, c[i], rhigh, rlow, rwidth);
+      else if (c[i] > 1) insert_sort_bmask(k + off, ix + off, c[i], bmask);
+      off += c[i];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Coulomb backend (interaction_specific/coulomb/)
+// Moment record layout = t_tree_node_interaction_data
+// (module_interaction_specific_types_XYZQVM.f90:47-57):
+//   0..2 coc, 3 charge, 4 abs_charge, 5..7 dip, 8..10 quad, 11 xyquad,
+//   12 yzquad, 13 zxquad, 14 bmax
+// ---------------------------------------------------------------------------
+enum { M_COCX = 0, M_COCY, M_COCZ, M_Q, M_ABSQ, M_DX, M_DY, M_DZ, M_QXX, M_QYY, M_QZZ,
+       M_XY, M_YZ, M_ZX, M_BMAX, M_N };
+
+// multipole_from_particle, coulomb/module_interaction_specific.f90:67-79
+void multipole_from_particle(const double pos[3], double q, double* m) {
+  m[M_COCX] = pos[0]; m[M_COCY] = pos[1]; m[M_COCZ] = pos[2];
+  m[M_Q] = q;
+  m[M_ABSQ] = std::fabs(q);
+  for (int i = M_DX; i < M_N; ++i) m[i] = 0.0;
+}
+
+// shift_multipoles_up, coulomb/module_interaction_specific.f90:84-140
+void shift_multipoles_up(double* p, const double* const* ch, int nc) {
+  double charge = 0.0, absq = 0.0;
+  for (int j = 0; j < nc; ++j) charge = charge + ch[j][M_Q];   // :96
+  for (int j = 0; j < nc; ++j) absq = absq + ch[j][M_ABSQ];    // :97
+  double coc[3] = {0.0, 0.0, 0.0};
+  if (absq != 0.0) {  // :102-108
+    for (int j = 0; j < nc; ++j)
+      for (int d = 0; d < 3; ++d) coc[d] = coc[d] + ch[j][M_COCX + d] * ch[j][M_ABSQ];
+    for (int d = 0; d < 3; ++d) coc[d] = coc[d] / absq;
+  } else {  // :110-116, geometric mean of the children
+    for (int j = 0; j < nc; ++j)
+      for (int d = 0; d < 3; ++d) coc[d] = coc[d] + ch[j][M_COCX + d];
+    for (int d = 0; d < 3; ++d) coc[d] = coc[d] / (double)nc;
+  }
+  double dip[3] = {0, 0, 0}, quad[3] = {0, 0, 0}, xy = 0, yz = 0, zx = 0;
+  for (int j = 0; j < nc; ++j) {  // :125-137
+    const double* c = ch[j];
+    double s[3];
+    for (int d = 0; d < 3; ++d) s[d] = coc[d] - c[M_COCX + d];
+    for (int d = 0; d < 3; ++d) dip[d] = (dip[d] + c[M_DX + d]) + c[M_Q] * s[d];
+    for (int d = 0; d < 3; ++d)
+      quad[d] = ((quad[d] + c[M_QXX + d]) + c[M_DX + d] * s[d]) + (0.5 * c[M_Q]) * (s[d] * s[d]);
+    xy = (((xy + c[M_XY]) + c[M_DX] * s[1]) + c[M_DY] * s[0]) + (c[M_Q] * s[0]) * s[1];
+    yz = (((yz + c[M_YZ]) + c[M_DY] * s[2]) + c[M_DZ] * s[1]) + (c[M_Q] * s[1]) * s[2];
+    zx = (((zx + c[M_ZX]) + c[M_DZ] * s[0]) + c[M_DX] * s[2]) + (c[M_Q] * s[2]) * s[0];
+  }
+  double bmax = 0.0;  // :139
+  for (int j = 0; j < nc; ++j) {
+    const double* c = ch[j];
+    double a = coc[0] - c[M_COCX], b = coc[1] - c[M_COCY], d = coc[2] - c[M_COCZ];
+    double v = std::sqrt((a * a + b * b) + d * d) + c[M_BMAX];
+    if (j == 0 || v > bmax) bmax = v;
+  }
+  p[M_COCX] = coc[0]; p[M_COCY] = coc[1]; p[M_COCZ] = coc[2];
+  p[M_Q] = charge; p[M_ABSQ] = absq;
+  p[M_DX] = dip[0]; p[M_DY] = dip[1]; p[M_DZ] = dip[2];
+  p[M_QXX] = quad[0]; p[M_QYY] = quad[1]; p[M_QZZ] = quad[2];
+  p[M_XY] = xy; p[M_YZ] = yz; p[M_ZX] = zx; p[M_BMAX] = bmax;
+}
+
+// calc_force_coulomb_3D_direct, coulomb/module_coulomb_kernels.f90:242-257
+inline void force_leaf(const double* t, const double d[3], double dist2, double e[3],
+                       double& phi) {
+  double r = std::sqrt(dist2);
+  double rd = 1.0 / r;
+  double rd3charge = ((t[M_Q] * rd) * rd) * rd;
+  phi = t[M_Q] * rd;
+  e[0] = rd3charge * d[0];
+  e[1] = rd3charge * d[1];
+  e[2] = rd3charge * d[2];
+}
+
+// calc_force_coulomb_3D, coulomb/module_coulomb_kernels.f90:60-145
+inline void force_twig(const double* t, const double d[3], double dist2, double e[3],
+                       double& phi) {
+  const double dx = d[0], dy = d[1], dz = d[2];
+  const double r = std::sqrt(dist2);
+  const double rd = 1.0 / r;
+  const double rd2 = rd * rd;
+  const double rd3 = rd * rd2;
+  const double rd5 = rd3 * rd2;
+  const double rd7 = rd5 * rd2;
+  const double dx2 = dx * dx, dy2 = dy * dy, dz2 = dz * dz;
+  const double fdx = ((3.0 * dx2) * rd5) - rd3;
+  const double fdy = ((3.0 * dy2) * rd5) - rd3;
+  const double fdz = ((3.0 * dz2) * rd5) - rd3;
+  const double fdxy = ((3.0 * dx) * dy) * rd5;
+  const double fdyz = ((3.0 * dy) * dz) * rd5;
+  const double fdxz = ((3.0 * dx) * dz) * rd5;
+  const double m2rd5 = 2.0 * rd5;
+  const double m5rd7 = 5.0 * rd7;
+  const double pre1 = ((m5rd7 * dx) * dy) * dz;
+  const double pre2x = (m5rd7 * dx2) - rd5;
+  const double pre2y = (m5rd7 * dy2) - rd5;
+  const double pre2z = (m5rd7 * dz2) - rd5;
+  const double preQx = pre2x * t[M_QXX];
+  const double preQy = pre2y * t[M_QYY];
+  const double preQz = pre2z * t[M_QZZ];
+  phi = (((((((t[M_Q] * rd) - (((dx * t[M_DX]) + (dy * t[M_DY])) + (dz * t[M_DZ])) * rd3)
+            + fdx * t[M_QXX]) + fdy * t[M_QYY]) + fdz * t[M_QZZ]) + fdxy * t[M_XY])
+         + fdyz * t[M_YZ]) + fdxz * t[M_ZX];
+  e[0] = (((t[M_Q] * dx) * rd3) - (((fdx * t[M_DX]) + (fdxy * t[M_DY])) + (fdxz * t[M_DZ])))
+         + 3.0 * ((((dx * ((((pre2x - m2rd5) * t[M_QXX]) + preQy) + preQz))
+                    + ((dy * pre2x) * t[M_XY])) + ((dz * pre2x) * t[M_ZX])) + (pre1 * t[M_YZ]));
+  e[1] = (((t[M_Q] * dy) * rd3) - (((fdy * t[M_DY]) + (fdxy * t[M_DX])) + (fdyz * t[M_DZ])))
+         + 3.0 * ((((dy * ((((pre2y - m2rd5) * t[M_QYY]) + preQx) + preQz))
+                    + ((dx * pre2y) * t[M_XY])) + ((dz * pre2y) * t[M_YZ])) + (pre1 * t[M_ZX]));
+  e[2] = (((t[M_Q] * dz) * rd3) - (((fdz * t[M_DZ]) + (fdyz * t[M_DY])) + (fdxz * t[M_DX])))
+         + 3.0 * ((((dz * ((((pre2z - m2rd5) * t[M_QZZ]) + preQy) + preQx))
+                    + ((dx * pre2z) * t[M_ZX])) + ((dy * pre2z) * t[M_YZ])) + (pre1 * t[M_XY]));
+}
+
+// ---------------------------------------------------------------------------
+// Mirror boxes (treecode/lpepcsrc/module_mirror_boxes.f90:73-156)
+// ---------------------------------------------------------------------------
+std::vector<std::array<int, 3>> neighbour_boxes(const orc_params& p) {
+  int sw[3];
+  for (int d = 0; d < 3; ++d) sw[d] = p.periodicity[d] ? p.mirror_box_layers : 0;
+  std::vector<std::array<int, 3>> nb;
+  for (int i = -sw[0]; i <= -1; ++i)
+    for (int j = -sw[1]; j <= sw[1]; ++j)
+      for (int k = -sw[2]; k <= sw[2]; ++k) {
+        nb.push_back({i, j, k});
+        nb.push_back({-i, -j, -k});
+      }
+  for (int j = -sw[1]; j <= -1; ++j)
+    for (int k = -sw[2]; k <= sw[2]; ++k) {
+      nb.push_back({0, j, k});
+      nb.push_back({0, -j, -k});
+    }
+  for (int k = -sw[2]; k <= -1; ++k) {
+    nb.push_back({0, 0, k});
+    nb.push_back({0, 0, -k});
+  }
+  nb.push_back({0, 0, 0});  // central box last, :151
+  return nb;
+}
+
+// lattice_vect, module_mirror_boxes.f90:73-79 (integer * real promotes to FP64)
+void lattice_vect(const orc_params& p, const std::array<int, 3>& ijk, double v[3]) {
+  for (int d = 0; d < 3; ++d)
+    v[d] = ((double)ijk[0] * p.t_lattice_1[d] + (double)ijk[1] * p.t_lattice_2[d])
+           + (double)ijk[2] * p.t_lattice_3[d];
+}
+
+}  // namespace
+
+// forward declarations of the periodic lattice term (pepc_oracle_fmm.cpp)
+struct OrcFmm;
+OrcFmm* orc_fmm_create(const orc_params& p);
+void orc_fmm_destroy(OrcFmm* f);
+void orc_fmm_timestep(OrcFmm* f, int64_t n, const double* x, const double* y, const double* z,
+                      const double* q);
+void orc_fmm_sum_lattice_force(const OrcFmm* f, const double pos[3], double e[3], double* phi);
+
+// ---------------------------------------------------------------------------
+// Whole-path context
+// ---------------------------------------------------------------------------
+struct Node {
+  int64_t key;
+  int32_t level;
+  int64_t leaves, descendants;
+  int64_t parent, first_child, next_sibling;
+  int64_t particle;  // leaf: key-ordered particle index; twig: -1
+  double m[M_N];
+};
+
+struct orc_ctx {
+  orc_params p;
+  Box box;
+  int64_t n = 0;
+  std::vector<int64_t> keys, perm;
+  std::vector<double> x, y, z, q;
+  std::vector<Node> nodes;
+  int64_t root = kNodeInvalid;
+  double boxlength2[kMaxLevel + 1];
+  int64_t n_interactions = 0, n_mac = 0;
+  OrcFmm* fmm = nullptr;
+  bool periodic_far() const {
+    return (p.periodicity[0] || p.periodicity[1] || p.periodicity[2]) &&
+           p.include_far_field_if_periodic;
+  }
+};
+
+namespace {
+
+// tree_node_create_from_particle, module_tree_grow.f90:702-734
+int64_t make_leaf(orc_ctx* c, int64_t k, int64_t ip) {
+  Node nd{};
+  nd.key = k;
+  nd.level = level_from_key(k);
+  nd.leaves = 1;
+  nd.descendants = 0;
+  nd.parent = nd.first_child = nd.next_sibling = kNodeInvalid;
+  nd.particle = ip;
+  double pos[3] = {c->x[ip], c->y[ip], c->z[ip]};
+  multipole_from_particle(pos, c->q[ip], nd.m);
+  c->nodes.push_back(nd);
+  return (int64_t)c->nodes.size() - 1;
+}
+
+// tree_node_update_from_children, module_tree_grow.f90:762-821 (+ connect, module_tree.f90:409-433)
+void update_from_children(orc_ctx* c, int64_t pi, const std::vector<int64_t>& ch) {
+  Node& p = c->nodes[pi];
+  p.leaves = 0;
+  p.descendants = (int64_t)ch.size();
+  const double* cm[8];
+  for (size_t i = 0; i < ch.size(); ++i) {
+    p.leaves += c->nodes[ch[i]].leaves;
+    p.descendants += c->nodes[ch[i]].descendants;
+    cm[i] = c->nodes[ch[i]].m;
+  }
+  shift_multipoles_up(p.m, cm, (int)ch.size());
+  p.first_child = ch[0];
+  for (size_t i = 0; i < ch.size(); ++i) {
+    c->nodes[ch[i]].parent = pi;
+    c->nodes[ch[i]].next_sibling = (i + 1 < ch.size()) ? ch[i + 1] : kNodeInvalid;
+  }
+}
+
+// insert_helper, module_tree_grow.f90:623-696 (node indices in insertion order)
+int64_t insert_helper(orc_ctx* c, int64_t k, int l, int64_t& cur, int& err) {
+  const int64_t n = c->n;
+  auto is_anc = [&](int64_t kp) { return k == (kp >> (3 * (kMaxLevel - l))); };
+  bool first = cur < n && is_anc(c->keys[cur]);
+  bool second = cur + 1 < n && is_anc(c->keys[cur + 1]);
+  if (!first && !second) return kNodeInvalid;
+  if (first && !second) {
+    int64_t nd = make_leaf(c, k, cur);
+    ++cur;
+    return nd;
+  }
+  if (l >= kMaxLevel) {  // :671-675, "no more levels"
+    err = -2;
+    return kNodeInvalid;
+  }
+  Node tw{};
+  tw.key = k;
+  tw.level = l;
+  tw.particle = -1;
+  tw.parent = tw.first_child = tw.next_sibling = kNodeInvalid;
+  c->nodes.push_back(tw);
+  int64_t me = (int64_t)c->nodes.size() - 1;
+  std::vector<int64_t> ch;
+  for (int ic = 0; ic < 8; ++ic) {
+    int64_t cn = insert_helper(c, (k << 3) + ic, l + 1, cur, err);
+    if (err) return kNodeInvalid;
+    if (cn != kNodeInvalid) ch.push_back(cn);
+  }
+  update_from_children(c, me, ch);
+  return me;
+}
+
+struct Counters {
+  int64_t inter = 0, mac = 0;
+};
+
+// walk_single_particle, treecode/lpepcsrc/module_tree_walk_pthreads.f90:558-765.
+// At one rank every child is local, so the defer list only ever holds the
+// root (:601 parses it once and pushes the root's children); the todo list is
+// a LIFO stack.  Returns the number of partner leaves (completeness check :452).
+int64_t walk_pthreads(const orc_ctx* c, const double xt[3], const double vbox[3], double e[3],
+                      double& pot, double& work, Counters& cnt, std::vector<int64_t>& todo) {
+  const double shifted[3] = {xt[0] - vbox[0], xt[1] - vbox[1], xt[2] - vbox[2]};  // :595
+  int64_t partner = 0;
+  todo.clear();
+  for (int64_t ch = c->nodes[c->root].first_child; ch != kNodeInvalid;
+       ch = c->nodes[ch].next_sibling)
+    todo.push_back(ch);
+  const double eps2 = c->p.eps2, theta2 = c->p.theta2;
+  while (!todo.empty()) {
+    int64_t ni = todo.back();
+    todo.pop_back();
+    const Node& nd = c->nodes[ni];
+    double d[3] = {shifted[0] - nd.m[M_COCX], shifted[1] - nd.m[M_COCY],
+                   shifted[2] - nd.m[M_COCZ]};  // :614
+    double dist2 = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2];  // :615
+    if (nd.descendants == 0) {  // leaf, :617-631
+      partner += 1;
+      work += 1.0;
+      if (dist2 > 0.0) {
+        double ee[3], ph;
+        force_leaf(nd.m, d, dist2 + eps2, ee, ph);  // coulomb/...specific.f90:333
+        e[0] += ee[0]; e[1] += ee[1]; e[2] += ee[2];
+        pot += ph;
+      }
+      cnt.inter += 1;
+    } else {
+      cnt.mac += 1;
+      if (theta2 * dist2 > c->boxlength2[nd.level]) {  // mac, :635 / specific.f90:267
+        partner += nd.leaves;
+        double ee[3], ph;
+        force_twig(nd.m, d, dist2 + eps2, ee, ph);  // specific.f90:373
+        e[0] += ee[0]; e[1] += ee[1]; e[2] += ee[2];
+        pot += ph;
+        cnt.inter += 1;
+        work += 1.0;
+      } else {  // resolve: push all children, first .. last (:660-725)
+        for (int64_t ch = nd.first_child; ch != kNodeInvalid; ch = c->nodes[ch].next_sibling)
+          todo.push_back(ch);
+      }
+    }
+  }
+  return partner;
+}
+
+// tree_walk_single_aux, treecode/lpepcsrc/module_tree_walk_simple.f90:301-384
+void walk_simple_aux(const orc_ctx* c, int64_t ni, int np, const double (*xs)[3],
+                     const double vbox[3], double (*e)[3], double* pot, double* work,
+                     int64_t& partner, Counters& cnt) {
+  const Node& nd = c->nodes[ni];
+  const double eps2 = c->p.eps2, theta2 = c->p.theta2;
+  double d[32][3], d2[32];
+  if (nd.descendants == 0) {
+    partner += 1;
+    for (int ip = 0; ip < np; ++ip) {
+      for (int k = 0; k < 3; ++k) d[ip][k] = (xs[ip][k] - vbox[k]) - nd.m[M_COCX + k];
+      d2[ip] = (d[ip][0] * d[ip][0] + d[ip][1] * d[ip][1]) + d[ip][2] * d[ip][2];
+      cnt.inter += 1;
+      work[ip] += 1.0;
+      if (d2[ip] > 0.0) {
+        double ee[3], ph;
+        force_leaf(nd.m, d[ip], d2[ip] + eps2, ee, ph);
+        e[ip][0] += ee[0]; e[ip][1] += ee[1]; e[ip][2] += ee[2];
+        pot[ip] += ph;
+      }
+    }
+    return;
+  }
+  for (int ip = 0; ip < np; ++ip) {
+    cnt.mac += 1;
+    for (int k = 0; k < 3; ++k) d[ip][k] = (xs[ip][k] - vbox[k]) - nd.m[M_COCX + k];
+    d2[ip] = (d[ip][0] * d[ip][0] + d[ip][1] * d[ip][1]) + d[ip][2] * d[ip][2];
+    if (!(theta2 * d2[ip] > c->boxlength2[nd.level])) {  // MAC fails for this target: resolve
+      for (int64_t ch = nd.first_child; ch != kNodeInvalid; ch = c->nodes[ch].next_sibling)
+        walk_simple_aux(c, ch, np, xs, vbox, e, pot, work, partner, cnt);
+      return;
+    }
+  }
+  partner += nd.leaves;  // MAC OK for the whole tile: interact
+  for (int ip = 0; ip < np; ++ip) {
+    cnt.inter += 1;
+    work[ip] += 1.0;
+    double ee[3], ph;
+    force_twig(nd.m, d[ip], d2[ip] + eps2, ee, ph);
+    e[ip][0] += ee[0]; e[ip][1] += ee[1]; e[ip][2] += ee[2];
+    pot[ip] += ph;
+  }
+}
+
+// tree_walk_init_aux, module_tree_walk_simple.f90:168-211: recursive split of
+// the key-ordered targets into tiles of at most tile_size.
+void make_tiles(const int64_t* keys, int64_t lo, int64_t hi, int64_t k, int l, int ts,
+                std::vector<std::pair<int64_t, int64_t>>& tiles, int& err) {
+  int64_t np = hi - lo;
+  if (np == 0) return;
+  if (np <= ts) {
+    tiles.push_back({lo, hi});
+    return;
+  }
+  if (l >= kMaxLevel) {
+    err = -2;
+    return;
+  }
+  int64_t ps = lo;
+  for (int ic = 0; ic < 8; ++ic) {
+    int64_t ck = (k << 3) + ic;
+    int64_t pe = ps;
+    while (pe < hi && (keys[pe] >> (3 * (kMaxLevel - (l + 1)))) == ck) ++pe;
+    make_tiles(keys, ps, pe, ck, l + 1, ts, tiles, err);
+    if (err) return;
+    ps = pe;
+  }
+}
+
+template <class F>
+void parallel_for(int64_t n, int nthreads, F&& f) {
+  if (nthreads <= 1 || n < 64) {
+    for (int64_t i = 0; i < n; ++i) f(i, 0);
+    return;
+  }
+  std::atomic<int64_t> next{0};
+  std::vector<std::thread> th;
+  for (int t = 0; t < nthreads; ++t)
+    th.emplace_back([&, t] {
+      for (;;) {
+        int64_t i0 = next.fetch_add(64);
+        if (i0 >= n) break;
+        int64_t i1 = std::min(n, i0 + 64);
+        for (int64_t i = i0; i < i1; ++i) f(i, t);
+      }
+    });
+  for (auto& t : th) t.join();
+}
+
+}  // namespace
+
+extern "C" {
+
+void orc_params_default(orc_params* p) {
+  std::memset(p, 0, sizeof(*p));
+  p->theta2 = 0.36;   // coulomb/module_interaction_specific.f90:38
+  p->eps2 = 0.0;      // :39
+  p->curve = 0;
+  p->walk = 0;
+  p->tile_size = 16;  // module_tree_walk_simple.f90:40
+  p->mirror_box_layers = 1;             // module_mirror_boxes.f90:38
+  p->include_far_field_if_periodic = 1; // coulomb/...specific.f90:37
+  p->fmm_extrinsic_correction = 2;      // module_fmm_framework.f90:49
+  p->t_lattice_1[0] = 1.0;
+  p->t_lattice_2[1] = 1.0;
+  p->t_lattice_3[2] = 1.0;
+  p->num_threads = 1;
+}
+
+void orc_box_create(int64_t n, const double* x, const double* y, const double* z,
+                    int32_t force_cubic, double box9[9]) {
+  Box b = box_create(n, x, y, z, force_cubic != 0);
+  for (int d = 0; d < 3; ++d) {
+    box9[d] = b.min[d];
+    box9[3 + d] = b.max[d];
+    box9[6 + d] = b.size[d];
+  }
+}
+
+void orc_compute_keys(int64_t n, const double* x, const double* y, const double* z,
+                      const double boxmin[3], const double boxsize[3], int32_t curve,
+                      int64_t* keys) {
+  Box b{};
+  for (int d = 0; d < 3; ++d) { b.min[d] = boxmin[d]; b.size[d] = boxsize[d]; }
+  double s[3];
+  for (int d = 0; d < 3; ++d) s[d] = b.size[d] / (double)(int64_t(1) << kMaxLevel);
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t ic[3];
+    coord_to_intcoord(b, s, x[i], y[i], z[i], ic);
+    keys[i] = curve == 1 ? intcoord_to_key_morton3d(ic) : intcoord_to_key_hilbert3d(ic);
+  }
+}
+
+void orc_key_to_coord(int64_t key, const double boxmin[3], const double boxsize[3],
+                      int32_t curve, double xout[3]) {
+  Box b{};
+  for (int d = 0; d < 3; ++d) { b.min[d] = boxmin[d]; b.size[d] = boxsize[d]; }
+  key_to_coord(b, key, curve, xout);
+}
+
+void orc_sort_radix(int64_t n, int64_t* keys, int64_t* idx) {
+  if (n < 2) return;
+  rs_rec_ip(keys, idx, n, 63, 0, 10);
+}
+
+void orc_multipole_from_particle(const double pos[3], double q, double mp[15]) {
+  multipole_from_particle(pos, q, mp);
+}
+
+void orc_shift_multipoles_up(double parent[15], const double* children, int32_t nchild) {
+  const double* cm[8];
+  for (int i = 0; i < nchild && i < 8; ++i) cm[i] = children + 15 * i;
+  shift_multipoles_up(parent, cm, std::min(nchild, 8));
+}
+
+void orc_force_leaf(const double node[15], const double delta[3], double dist2, double e[3],
+                    double* phi) {
+  force_leaf(node, delta, dist2, e, *phi);
+}
+
+void orc_force_twig(const double node[15], const double delta[3], double dist2, double e[3],
+                    double* phi) {
+  force_twig(node, delta, dist2, e, *phi);
+}
+
+// par_rand, frontends/pepc-mini/module_helper.f90:592-658 (L'Ecuyer with
+// Bays-Durham shuffle, single precision result).  State persists across calls
+// exactly like the Fortran SAVE variables.
+void orc_par_rand(int32_t iseed, int64_t n, double* out) {
+  const int32_t IM1 = 2147483563, IM2 = 2147483399, IMM1 = IM1 - 1;
+  const int32_t IA1 = 40014, IA2 = 40692, IQ1 = 53668, IQ2 = 52774, IR1 = 12211, IR2 = 3791;
+  const int NTAB = 32;
+  const int32_t NDIV = 1 + IMM1 / NTAB;
+  const float AM = 1.0f / (float)IM1;
+  const float RNMX = 1.0f - 1.2e-7f;
+  static int32_t idum = -1, idum2 = 123456789, iy = 0, iv[32];
+  bool seeded = iseed >= 0;
+  for (int64_t c = 0; c < n; ++c) {
+    if (idum <= 0 || (seeded && c == 0)) {
+      if (seeded && c == 0) idum = iseed;
+      else idum = (-idum < 1) ? 1 : -idum;
+      idum2 = idum;
+      for (int j = NTAB + 7; j >= 0; --j) {
+        int32_t k = idum / IQ1;
+        idum = IA1 * (idum - k * IQ1) - k * IR1;
+        if (idum < 0) idum += IM1;
+        if (j < NTAB) iv[j] = idum;
+      }
+      iy = iv[0];
+    }
+    int32_t k = idum / IQ1;
+    idum = IA1 * (idum - k * IQ1) - k * IR1;
+    if (idum < 0) idum += IM1;
+    k = idum2 / IQ2;
+    idum2 = IA2 * (idum2 - k * IQ2) - k * IR2;
+    if (idum2 < 0) idum2 += IM2;
+    int j = iy / NDIV;
+    iy = iv[j] - idum2;
+    iv[j] = idum;
+    if (iy < 1) iy += IMM1;
+    float r = AM * (float)iy;
+    if (r > RNMX) r = RNMX;
+    out[c] = (double)r;
+  }
+}
+
+orc_ctx* orc_create(const orc_params* p) {
+  orc_ctx* c = new orc_ctx;
+  c->p = *p;
+  if (c->periodic_far()) c->fmm = orc_fmm_create(c->p);
+  return c;
+}
+
+void orc_destroy(orc_ctx* c) {
+  if (!c) return;
+  if (c->fmm) orc_fmm_destroy(c->fmm);
+  delete c;
+}
+
+int orc_grow_tree(orc_ctx* c, int64_t n, const double* x, const double* y, const double* z,
+                  const double* q, int64_t* key_out, int64_t* perm_out, double* x_out,
+                  double* y_out, double* z_out, double* q_out) {
+  if (n < 2) return -1;  // module_domains.f90:187-189: a rank needs >= 2 particles
+  c->n = n;
+  // tree_grow, module_tree_grow.f90:69-72
+  c->box = box_create(n, x, y, z, c->p.force_cubic_domain != 0);
+  std::vector<int64_t> keys(n), idx(n);
+  orc_compute_keys(n, x, y, z, c->box.min, c->box.size, c->p.curve, keys.data());
+  for (int64_t i = 0; i < n; ++i) idx[i] = i;
+  // domain_decompose at one rank, module_domains.f90:158-319: sort, permute
+  rs_rec_ip(keys.data(), idx.data(), n, 63, 0, 10);
+  c->keys = keys;
+  c->perm = idx;
+  c->x.resize(n); c->y.resize(n); c->z.resize(n); c->q.resize(n);
+  for (int64_t i = 0; i < n; ++i) {
+    c->x[i] = x[idx[i]]; c->y[i] = y[idx[i]]; c->z[i] = z[idx[i]]; c->q[i] = q[idx[i]];
+  }
+  // duplicate-key fix, module_domains.f90:268-307
+  std::vector<int64_t> lk = c->keys;
+  std::vector<int64_t> kd(n);
+  for (int64_t i = 0; i + 1 < n; ++i) kd[i] = lk[i + 1] - lk[i];
+  kd[n - 1] = 1;
+  for (int64_t i = 0; i < n; ++i) {
+    if (kd[i] < 1) {
+      for (int64_t j = 1; j <= std::max(n - 1 - i, i + 1); ++j) {
+        // Fortran 1-based: key_diffs(max(1, i-j)) with i 1-based -> 0-based max(0, i-j)
+        if (kd[std::max<int64_t>(0, i - j)] > 1) {
+          for (int64_t t = i - j + 1; t <= i; ++t) lk[t] -= 1;
+          kd[i] += 1;
+          kd[i - j] -= 1;
+          break;
+        } else if (kd[std::min<int64_t>(n - 2, i + j)] > 1) {
+          for (int64_t t = i + 1; t <= i + j; ++t) lk[t] += 1;
+          kd[i] += 1;
+          kd[i + j] -= 1;
+          break;
+        }
+      }
+    }
+  }
+  for (int64_t i = 0; i < n; ++i) {
+    if (lk[i] != c->keys[i]) {
+      c->keys[i] = lk[i];
+      double xx[3];
+      key_to_coord(c->box, lk[i], c->p.curve, xx);
+      c->x[i] = xx[0]; c->y[i] = xx[1]; c->z[i] = xx[2];
+    }
+  }
+  // tree_create, module_tree.f90:196-201
+  c->boxlength2[0] = std::max(c->box.size[0], std::max(c->box.size[1], c->box.size[2]));
+  c->boxlength2[0] = c->boxlength2[0] * c->boxlength2[0];
+  for (int i = 1; i <= kMaxLevel; ++i) c->boxlength2[i] = c->boxlength2[i - 1] / 4.0;
+  // tree_build_from_particles, module_tree_grow.f90:552-697
+  c->nodes.clear();
+  c->nodes.reserve(2 * n + 8);
+  int64_t cur = 0;
+  int err = 0;
+  c->root = insert_helper(c, 1, 0, cur, err);
+  if (err) return err;
+  // tree_build_upwards at one rank recomputes the root from its children
+  // (module_tree_grow.f90:410-536 with the level-1 branch nodes); identical
+  // inputs in identical order, so the root is unchanged.
+  if (c->nodes[c->root].leaves != n) return -4;
+  if (key_out) std::memcpy(key_out, c->keys.data(), n * sizeof(int64_t));
+  if (perm_out) std::memcpy(perm_out, c->perm.data(), n * sizeof(int64_t));
+  if (x_out) std::memcpy(x_out, c->x.data(), n * sizeof(double));
+  if (y_out) std::memcpy(y_out, c->y.data(), n * sizeof(double));
+  if (z_out) std::memcpy(z_out, c->z.data(), n * sizeof(double));
+  if (q_out) std::memcpy(q_out, c->q.data(), n * sizeof(double));
+  if (c->fmm) orc_fmm_timestep(c->fmm, n, c->x.data(), c->y.data(), c->z.data(), c->q.data());
+  return 0;
+}
+
+int orc_traverse_tree(orc_ctx* c, int64_t nt, const double* tx, const double* ty,
+                      const double* tz, const int64_t* tkeys, double* ex, double* ey,
+                      double* ez, double* pot, double* work) {
+  auto boxes = neighbour_boxes(c->p);
+  int nth = std::max(1, c->p.num_threads);
+  std::vector<Counters> cnt(nth);
+  std::atomic<int> bad{0};
+  // libpepc_traverse_tree, module_libpepc_main.f90:161-200: one walk per box,
+  // central box last, then the per-particle lattice term.
+  if (c->p.walk == 0) {
+    parallel_for(nt, nth, [&](int64_t i, int t) {
+      std::vector<int64_t> todo;
+      todo.reserve(1024);
+      double xt[3] = {tx[i], ty[i], tz[i]};
+      double e[3] = {ex[i], ey[i], ez[i]}, ph = pot[i], w = work[i];
+      for (auto& bx : boxes) {
+        double vb[3];
+        lattice_vect(c->p, bx, vb);
+        int64_t partner = walk_pthreads(c, xt, vb, e, ph, w, cnt[t], todo);
+        if (partner != c->n) bad.store(1);
+      }
+      ex[i] = e[0]; ey[i] = e[1]; ez[i] = e[2]; pot[i] = ph; work[i] = w;
+    });
+  } else {
+    std::vector<std::pair<int64_t, int64_t>> tiles;
+    int err = 0;
+    if (tkeys == nullptr) {
+      for (int64_t i = 0; i < nt; ++i) tiles.push_back({i, i + 1});
+    } else {
+      make_tiles(tkeys, 0, nt, 1, 0, std::min(32, std::max(1, c->p.tile_size)), tiles, err);
+      if (err) return err;
+    }
+    parallel_for((int64_t)tiles.size(), nth, [&](int64_t it, int t) {
+      int64_t lo = tiles[it].first, np = tiles[it].second - tiles[it].first;
+      double xs[32][3], e[32][3], ph[32], w[32];
+      for (int k = 0; k < np; ++k) {
+        xs[k][0] = tx[lo + k]; xs[k][1] = ty[lo + k]; xs[k][2] = tz[lo + k];
+        e[k][0] = ex[lo + k]; e[k][1] = ey[lo + k]; e[k][2] = ez[lo + k];
+        ph[k] = pot[lo + k]; w[k] = work[lo + k];
+      }
+      for (auto& bx : boxes) {
+        double vb[3];
+        lattice_vect(c->p, bx, vb);
+        int64_t partner = 0;
+        walk_simple_aux(c, c->root, (int)np, xs, vb, e, ph, w, partner, cnt[t]);
+        if (partner != c->n) bad.store(1);
+      }
+      for (int k = 0; k < np; ++k) {
+        ex[lo + k] = e[k][0]; ey[lo + k] = e[k][1]; ez[lo + k] = e[k][2];
+        pot[lo + k] = ph[k]; work[lo + k] = w[k];
+      }
+    });
+  }
+  c->n_interactions = 0;
+  c->n_mac = 0;
+  for (auto& k : cnt) { c->n_interactions += k.inter; c->n_mac += k.mac; }
+  if (c->fmm) {  // calc_force_per_particle, coulomb/...specific.f90:393-427
+    parallel_for(nt, nth, [&](int64_t i, int) {
+      double pos[3] = {tx[i], ty[i], tz[i]}, e[3], ph;
+      orc_fmm_sum_lattice_force(c->fmm, pos, e, &ph);
+      ex[i] += e[0]; ey[i] += e[1]; ez[i] += e[2]; pot[i] += ph;
+    });
+  }
+  return bad.load() ? -3 : 0;
+}
+
+int64_t orc_num_nodes(const orc_ctx* c) { return (int64_t)c->nodes.size(); }
+
+void orc_tree_export(const orc_ctx* c, int64_t* key, int32_t* level, int64_t* leaves,
+                     int64_t* descendants, int64_t* parent, int64_t* first_child,
+                     int64_t* next_sibling, double* moments15) {
+  for (size_t i = 0; i < c->nodes.size(); ++i) {
+    const Node& nd = c->nodes[i];
+    if (key) key[i] = nd.key;
+    if (level) level[i] = nd.level;
+    if (leaves) leaves[i] = nd.leaves;
+    if (descendants) descendants[i] = nd.descendants;
+    if (parent) parent[i] = nd.parent;
+    if (first_child) first_child[i] = nd.first_child;
+    if (next_sibling) next_sibling[i] = nd.next_sibling;
+    if (moments15) std::memcpy(moments15 + 15 * i, nd.m, 15 * sizeof(double));
+  }
+}
+
+void orc_box(const orc_ctx* c, double box9[9]) {
+  for (int d = 0; d < 3; ++d) {
+    box9[d] = c->box.min[d];
+    box9[3 + d] = c->box.max[d];
+    box9[6 + d] = c->box.size[d];
+  }
+}
+
+void orc_counters(const orc_ctx* c, int64_t out[2]) {
+  out[0] = c->n_interactions;
+  out[1] = c->n_mac;
+}
+
+int orc_direct(orc_ctx* c, int64_t ntest, const int64_t* tidx, double* ex, double* ey,
+               double* ez, double* pot) {
+  auto boxes = neighbour_boxes(c->p);
+  const int64_t n = c->n;
+  int nth = std::max(1, c->p.num_threads);
+  // directforce, utils/module_directsum.f90:86-159 (one rank: currank = 0)
+  parallel_for(ntest, nth, [&](int64_t j, int) {
+    int64_t tj = tidx[j];
+    double xt[3] = {c->x[tj], c->y[tj], c->z[tj]};
+    double e[3] = {0, 0, 0}, ph = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      double m[M_N];
+      double pos[3] = {c->x[i], c->y[i], c->z[i]};
+      multipole_from_particle(pos, c->q[i], m);
+      for (size_t ib = 0; ib < boxes.size(); ++ib) {
+        double vb[3];
+        lattice_vect(c->p, boxes[ib], vb);
+        double d[3] = {(xt[0] - vb[0]) - m[M_COCX], (xt[1] - vb[1]) - m[M_COCY],
+                       (xt[2] - vb[2]) - m[M_COCZ]};
+        if (ib + 1 == boxes.size() && tj == i) continue;  // self, :119-124
+        double dist2 = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2];
+        double ee[3], pp;
+        force_leaf(m, d, dist2 + c->p.eps2, ee, pp);
+        e[0] += ee[0]; e[1] += ee[1]; e[2] += ee[2];
+        ph += pp;
+      }
+    }
+    if (c->fmm) {  // :163-171
+      double le[3], lp;
+      orc_fmm_sum_lattice_force(c->fmm, xt, le, &lp);
+      e[0] += le[0]; e[1] += le[1]; e[2] += le[2]; ph += lp;
+    }
+    ex[j] = e[0]; ey[j] = e[1]; ez[j] = e[2]; pot[j] = ph;
+  });
+  return 0;
+}
+
+int orc_lattice(orc_ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
+                double* ex, double* ey, double* ez, double* pot) {
+  if (!c->fmm) return -1;
+  for (int64_t i = 0; i < nt; ++i) {
+    double pos[3] = {tx[i], ty[i], tz[i]}, e[3], ph;
+    orc_fmm_sum_lattice_force(c->fmm, pos, e, &ph);
+    ex[i] = e[0]; ey[i] = e[1]; ez[i] = e[2]; pot[i] = ph;
+  }
+  return 0;
+}
+
+}  // extern "C"
