@@ -1,0 +1,615 @@
+// api.cu -- the C ABI of libpepcg (include/pepcg.h): context lifetime,
+// device buffers, host <-> device staging and status reporting.
+//
+// Host-side orchestration only: every computation on particles and nodes is a
+// device kernel (grow.cu, walk_*.cu, lattice.cu, direct.cu).  There is no CPU
+// fallback: without a usable CUDA device every entry point fails with
+// PEPCG_ERR_CUDA.
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace pepcg {
+
+static thread_local std::string g_static_err;
+
+bool cuda_ok(Ctx* c, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return true;
+  std::string msg = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  if (c) c->err = msg;
+  else g_static_err = msg;
+  return false;
+}
+
+template <class T>
+bool ensure(Ctx* c, DBuf<T>& b, size_t n, const char* what) {
+  if (n <= b.cap) return true;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+  size_t want = n + n / 8 + 64;
+  cudaError_t e = cudaMalloc((void**)&b.p, want * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    c->err = std::string("device allocation failed for ") + what + " (" +
+             std::to_string(want * sizeof(T)) + " bytes): " + cudaGetErrorString(e);
+    b.p = nullptr;
+    return false;
+  }
+  b.cap = want;
+  return true;
+}
+
+template bool ensure<double>(Ctx*, DBuf<double>&, size_t, const char*);
+template bool ensure<float>(Ctx*, DBuf<float>&, size_t, const char*);
+template bool ensure<int64_t>(Ctx*, DBuf<int64_t>&, size_t, const char*);
+template bool ensure<int32_t>(Ctx*, DBuf<int32_t>&, size_t, const char*);
+template bool ensure<int8_t>(Ctx*, DBuf<int8_t>&, size_t, const char*);
+template bool ensure<uint64_t>(Ctx*, DBuf<uint64_t>&, size_t, const char*);
+template bool ensure<uint32_t>(Ctx*, DBuf<uint32_t>&, size_t, const char*);
+template bool ensure<unsigned long long>(Ctx*, DBuf<unsigned long long>&, size_t, const char*);
+template bool ensure<double4>(Ctx*, DBuf<double4>&, size_t, const char*);
+template bool ensure<double2>(Ctx*, DBuf<double2>&, size_t, const char*);
+template bool ensure<int2>(Ctx*, DBuf<int2>&, size_t, const char*);
+
+template <class T>
+static void release(DBuf<T>& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+}
+
+int status_to_code(Ctx* c, uint32_t st) {
+  if (st & ST_NONFINITE) {
+    c->err = "non-finite particle coordinate";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  if (st & ST_MAXLEVEL) {
+    c->err = "no more levels: keys could not be separated (module_tree_grow.f90:671-675)";
+    return PEPCG_ERR_MAXLEVEL;
+  }
+  if (st & ST_DUP_OVERFLOW) {
+    c->err = "too many duplicate keys for the duplicate-key fix";
+    return PEPCG_ERR_MAXLEVEL;
+  }
+  if (st & ST_TIMEOUT) {
+    c->err = "a bounded device wait gave up";
+    return PEPCG_ERR_TIMEOUT;
+  }
+  if (st & ST_INCOMPLETE) {
+    c->err = "walk incomplete: a target did not interact with all leaves "
+             "(module_tree_walk_pthreads.f90:452-457)";
+    return PEPCG_ERR_INCOMPLETE_WALK;
+  }
+  if (st & ST_NOT_NEUTRAL) {
+    c->err = "central box not charge-neutral: monopole removed (module_fmm_framework.f90:570-573)";
+    return PEPCG_WARN_NOT_NEUTRAL;
+  }
+  return PEPCG_OK;
+}
+
+// neighbour_boxes_prepare (module_mirror_boxes.f90:99-156) and lattice_vect (:73-79)
+static void prepare_boxes(Ctx* c) {
+  const pepcg_params& p = c->prm;
+  int sw[3];
+  for (int d = 0; d < 3; ++d) sw[d] = p.periodicity[d] ? p.mirror_box_layers : 0;
+  std::vector<int> nb;
+  auto push = [&](int i, int j, int k) {
+    nb.push_back(i);
+    nb.push_back(j);
+    nb.push_back(k);
+  };
+  for (int i = -sw[0]; i <= -1; ++i)
+    for (int j = -sw[1]; j <= sw[1]; ++j)
+      for (int k = -sw[2]; k <= sw[2]; ++k) {
+        push(i, j, k);
+        push(-i, -j, -k);
+      }
+  for (int j = -sw[1]; j <= -1; ++j)
+    for (int k = -sw[2]; k <= sw[2]; ++k) {
+      push(0, j, k);
+      push(0, -j, -k);
+    }
+  for (int k = -sw[2]; k <= -1; ++k) {
+    push(0, 0, k);
+    push(0, 0, -k);
+  }
+  push(0, 0, 0);
+  c->nboxes = (int)nb.size() / 3;
+  for (int b = 0; b < c->nboxes; ++b)
+    for (int d = 0; d < 3; ++d)
+      c->vbox[3 * b + d] = ((double)nb[3 * b] * p.t_lattice_1[d] + (double)nb[3 * b + 1] * p.t_lattice_2[d]) +
+                           (double)nb[3 * b + 2] * p.t_lattice_3[d];
+  c->periodic = p.periodicity[0] || p.periodicity[1] || p.periodicity[2];
+  c->far_field = c->periodic && p.include_far_field_if_periodic;
+}
+
+static int check_params(Ctx* c, const pepcg_params* p) {
+  if (p->force_law != 3) {
+    c->err = "only force_law = 3 (3D Coulomb) is supported";
+    return PEPCG_ERR_UNSUPPORTED;
+  }
+  if (p->mac_select != 0) {
+    c->err = "only mac_select = 0 (Barnes-Hut) is supported";
+    return PEPCG_ERR_UNSUPPORTED;
+  }
+  if (p->curve != PEPCG_CURVE_HILBERT && p->curve != PEPCG_CURVE_MORTON) {
+    c->err = "curve must be PEPCG_CURVE_HILBERT or PEPCG_CURVE_MORTON";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  if (p->precision != PEPCG_PRECISION_PLAIN && p->precision != PEPCG_PRECISION_MIXED) {
+    c->err = "precision must be PLAIN or MIXED";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  if (p->walk < 0 || p->walk > 2) {
+    c->err = "walk must be PER_TARGET, PER_TILE or GROUP";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  if (p->tile_size < 1 || p->tile_size > 32) {
+    c->err = "tile_size must be in 1..32";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  if (!(p->theta2 >= 0.0) || !(p->eps2 >= 0.0)) {
+    c->err = "theta2 and eps2 must be >= 0";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  if (p->mirror_box_layers < 0 || p->mirror_box_layers > 2) {
+    c->err = "mirror_box_layers must be in 0..2";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  return PEPCG_OK;
+}
+
+// tree_walk_init_aux (module_tree_walk_simple.f90:168-211) for keyed targets
+// that are not the grown particles: recursive split of the key-ordered
+// target keys into groups of at most T.
+static void tiles_rec(const int64_t* keys, int64_t lo, int64_t hi, int64_t k, int l, int T,
+                      std::vector<int32_t>& out, bool& err) {
+  int64_t np = hi - lo;
+  if (np == 0) return;
+  if (np <= T) {
+    out.push_back((int32_t)lo);
+    out.push_back((int32_t)np);
+    return;
+  }
+  if (l >= kMaxLevel) {
+    err = true;
+    return;
+  }
+  int64_t ps = lo;
+  for (int ic = 0; ic < 8; ++ic) {
+    int64_t ck = (k << 3) + ic;
+    int64_t pe = ps;
+    while (pe < hi && (keys[pe] >> (3 * (kMaxLevel - (l + 1)))) == ck) ++pe;
+    tiles_rec(keys, ps, pe, ck, l + 1, T, out, err);
+    if (err) return;
+    ps = pe;
+  }
+}
+
+int host_tiles(Ctx* c, int64_t nt, const int64_t* d_tkeys, int T, int2* d_tiles,
+               int64_t* ntiles) {
+  std::vector<int32_t> out;
+  if (d_tkeys == nullptr) {  // unkeyed targets: one tile each (:156-160)
+    out.resize(2 * nt);
+    for (int64_t i = 0; i < nt; ++i) {
+      out[2 * i] = (int32_t)i;
+      out[2 * i + 1] = 1;
+    }
+  } else {
+    std::vector<int64_t> keys(nt);
+    if (!cuda_ok(c, cudaMemcpyAsync(keys.data(), d_tkeys, nt * 8, cudaMemcpyDeviceToHost, c->stream),
+                 "tile keys") ||
+        !cuda_ok(c, cudaStreamSynchronize(c->stream), "tile keys"))
+      return PEPCG_ERR_CUDA;
+    if (keys[0] == 0) {  // KEY_INVALID: unkeyed (module_tree_walk_simple.f90:156)
+      out.resize(2 * nt);
+      for (int64_t i = 0; i < nt; ++i) {
+        out[2 * i] = (int32_t)i;
+        out[2 * i + 1] = 1;
+      }
+    } else {
+      bool err = false;
+      tiles_rec(keys.data(), 0, nt, 1, 0, T, out, err);
+      if (err) {
+        c->err = "walk_simple: insufficient key resolution in tile formation";
+        return PEPCG_ERR_MAXLEVEL;
+      }
+    }
+  }
+  *ntiles = (int64_t)out.size() / 2;
+  if (!cuda_ok(c, cudaMemcpyAsync(d_tiles, out.data(), out.size() * 4, cudaMemcpyHostToDevice,
+                                  c->stream), "tiles upload") ||
+      !cuda_ok(c, cudaStreamSynchronize(c->stream), "tiles upload"))
+    return PEPCG_ERR_CUDA;
+  return PEPCG_OK;
+}
+
+}  // namespace pepcg
+
+using namespace pepcg;
+
+static Ctx* as_ctx(void* p) { return static_cast<Ctx*>(p); }
+
+extern "C" {
+
+void pepcg_params_default(pepcg_params* p) {
+  std::memset(p, 0, sizeof(*p));
+  p->theta2 = 0.36;  // coulomb/module_interaction_specific.f90:38
+  p->eps2 = 0.0;     // :39
+  p->force_law = 3;  // :35
+  p->mac_select = 0; // :36
+  p->curve = PEPCG_CURVE_HILBERT;
+  p->precision = PEPCG_PRECISION_PLAIN;
+  p->walk = PEPCG_WALK_PER_TARGET;
+  p->tile_size = 16;  // module_tree_walk_simple.f90:40
+  p->mirror_box_layers = 1;
+  p->include_far_field_if_periodic = 1;
+  p->fmm_extrinsic_correction = 2;
+  p->t_lattice_1[0] = 1.0;
+  p->t_lattice_2[1] = 1.0;
+  p->t_lattice_3[2] = 1.0;
+  p->device = 0;
+}
+
+const char* pepcg_last_error(const void* ctx) {
+  if (!ctx) return g_static_err.c_str();
+  return static_cast<const Ctx*>(ctx)->err.c_str();
+}
+
+int pepcg_create(void** out, const pepcg_params* p) {
+  if (!out || !p) {
+    g_static_err = "pepcg_create: null argument";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  *out = nullptr;
+  Ctx* c = new (std::nothrow) Ctx;
+  if (!c) return PEPCG_ERR_OOM;
+  int rc = check_params(c, p);
+  if (rc) {
+    g_static_err = c->err;
+    delete c;
+    return rc;
+  }
+  c->prm = *p;
+  c->device = p->device;
+  int ndev = 0;
+  if (!cuda_ok(nullptr, cudaGetDeviceCount(&ndev), "cudaGetDeviceCount") || ndev == 0 ||
+      p->device < 0 || p->device >= ndev) {
+    if (ndev == 0 && g_static_err.empty()) g_static_err = "no CUDA device";
+    delete c;
+    return PEPCG_ERR_CUDA;
+  }
+  if (!cuda_ok(nullptr, cudaSetDevice(c->device), "cudaSetDevice") ||
+      !cuda_ok(nullptr, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream")) {
+    delete c;
+    return PEPCG_ERR_CUDA;
+  }
+  for (int i = 0; i < 8; ++i) cudaEventCreate(&c->ev[i]);
+  bool ok = cuda_ok(nullptr, cudaMalloc((void**)&c->d_box, 64 * sizeof(double)), "box") &&
+            cuda_ok(nullptr, cudaMalloc((void**)&c->d_status, 16), "status") &&
+            cuda_ok(nullptr, cudaMalloc((void**)&c->d_small, 16 * sizeof(unsigned long long)), "small") &&
+            cuda_ok(nullptr, cudaMalloc((void**)&c->d_vbox, 3 * 125 * sizeof(double)), "vbox") &&
+            cuda_ok(nullptr, cudaMalloc((void**)&c->d_part, 6 * 512 * sizeof(double)), "part");
+  if (!ok) {
+    pepcg_destroy(c);
+    return PEPCG_ERR_CUDA;
+  }
+  prepare_boxes(c);
+  cudaMemcpy(c->d_vbox, c->vbox, 3 * c->nboxes * sizeof(double), cudaMemcpyHostToDevice);
+  if (!ensure(c, c->counters, 8, "counters")) {
+    g_static_err = c->err;
+    pepcg_destroy(c);
+    return PEPCG_ERR_OOM;
+  }
+  if (c->far_field) {
+    rc = lattice_prepare(c);
+    if (rc) {
+      g_static_err = c->err;
+      pepcg_destroy(c);
+      return rc;
+    }
+  }
+  *out = c;
+  return PEPCG_OK;
+}
+
+int pepcg_destroy(void* ctx) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return PEPCG_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  release(c->x); release(c->y); release(c->z); release(c->q);
+  release(c->key); release(c->perm);
+  release(c->in_x); release(c->in_y); release(c->in_z); release(c->in_q);
+  release(c->skey); release(c->skey_alt); release(c->sval); release(c->sval_alt);
+  release(c->hist); release(c->orig_key); release(c->dup_list);
+  release(c->lev); release(c->lcpn);
+  release(c->cstart); release(c->cend); release(c->sstart); release(c->send);
+  release(c->scan_tmp);
+  release(c->nc4); release(c->meta); release(c->fwd); release(c->mom); release(c->aux);
+  release(c->mom32);
+  release(c->parent); release(c->nchild); release(c->upcnt); release(c->first_part);
+  release(c->nleaves); release(c->fpo2rpo); release(c->rpo2fpo); release(c->nkey);
+  release(c->tiles); release(c->counters); release(c->tgt); release(c->tkeys);
+  for (void* p : {(void*)c->d_box, (void*)c->d_status, (void*)c->d_small, (void*)c->d_vbox,
+                  (void*)c->d_part, (void*)c->d_mlattice, (void*)c->d_omega, (void*)c->d_mu,
+                  (void*)c->d_fmm_aux, (void*)c->d_factorial})
+    if (p) cudaFree(p);
+  for (int i = 0; i < 8; ++i)
+    if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return PEPCG_OK;
+}
+
+int pepcg_set_params(void* ctx, const pepcg_params* p) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || !p) return PEPCG_ERR_BAD_ARG;
+  int rc = check_params(c, p);
+  if (rc) return rc;
+  bool geom_changed = std::memcmp(p->periodicity, c->prm.periodicity, sizeof(p->periodicity)) ||
+                      p->mirror_box_layers != c->prm.mirror_box_layers ||
+                      std::memcmp(p->t_lattice_1, c->prm.t_lattice_1, 12 * sizeof(double)) ||
+                      p->include_far_field_if_periodic != c->prm.include_far_field_if_periodic ||
+                      p->fmm_extrinsic_correction != c->prm.fmm_extrinsic_correction ||
+                      p->curve != c->prm.curve || p->force_cubic_domain != c->prm.force_cubic_domain ||
+                      p->device != c->prm.device;
+  if (geom_changed) {
+    c->err = "pepcg_set_params: geometry, curve and device are fixed at creation";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  c->prm = *p;
+  return PEPCG_OK;
+}
+
+int pepcg_grow_tree_device(void* ctx, int64_t n, const double* d_x, const double* d_y,
+                           const double* d_z, const double* d_q) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || !d_x || !d_y || !d_z || !d_q) return PEPCG_ERR_BAD_ARG;
+  cudaSetDevice(c->device);
+  int rc = grow_device(c, n, d_x, d_y, d_z, d_q);
+  if (rc) return rc;
+  if (c->far_field) {
+    rc = lattice_timestep(c);
+    if (rc && rc != PEPCG_WARN_NOT_NEUTRAL) return rc;
+  }
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+  c->st.t_keys_ms = ms;
+  cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]);
+  c->st.t_sort_ms = ms;
+  cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
+  c->st.t_tree_ms = ms;
+  cudaEventElapsedTime(&ms, c->ev[3], c->ev[4]);
+  c->st.t_upward_ms = ms;
+  return rc;
+}
+
+int pepcg_grow_tree(void* ctx, int64_t n, const double* x, const double* y, const double* z,
+                    const double* q, int64_t* key_out, int64_t* perm_out, double* x_out,
+                    double* y_out, double* z_out) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || !x || !y || !z || !q || n < 0) return PEPCG_ERR_BAD_ARG;
+  cudaSetDevice(c->device);
+  if (n < 2) {
+    c->err = "pepcg_grow_tree: need at least 2 particles (module_domains.f90:187)";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  if (!ensure(c, c->in_x, n, "in_x") || !ensure(c, c->in_y, n, "in_y") ||
+      !ensure(c, c->in_z, n, "in_z") || !ensure(c, c->in_q, n, "in_q"))
+    return PEPCG_ERR_OOM;
+  cudaStream_t s = c->stream;
+  if (!cuda_ok(c, cudaMemcpyAsync(c->in_x.p, x, n * 8, cudaMemcpyHostToDevice, s), "H2D x") ||
+      !cuda_ok(c, cudaMemcpyAsync(c->in_y.p, y, n * 8, cudaMemcpyHostToDevice, s), "H2D y") ||
+      !cuda_ok(c, cudaMemcpyAsync(c->in_z.p, z, n * 8, cudaMemcpyHostToDevice, s), "H2D z") ||
+      !cuda_ok(c, cudaMemcpyAsync(c->in_q.p, q, n * 8, cudaMemcpyHostToDevice, s), "H2D q"))
+    return PEPCG_ERR_CUDA;
+  int rc = pepcg_grow_tree_device(c, n, c->in_x.p, c->in_y.p, c->in_z.p, c->in_q.p);
+  if (rc && rc != PEPCG_WARN_NOT_NEUTRAL) return rc;
+  bool ok = true;
+  if (key_out)
+    ok = ok && cuda_ok(c, cudaMemcpyAsync(key_out, c->key.p, n * 8, cudaMemcpyDeviceToHost, s), "D2H key");
+  if (perm_out) {
+    std::vector<int32_t> p32(n);
+    ok = ok && cuda_ok(c, cudaMemcpyAsync(p32.data(), c->perm.p, n * 4, cudaMemcpyDeviceToHost, s),
+                       "D2H perm") &&
+         cuda_ok(c, cudaStreamSynchronize(s), "D2H perm");
+    if (ok)
+      for (int64_t i = 0; i < n; ++i) perm_out[i] = p32[i];
+  }
+  if (x_out) ok = ok && cuda_ok(c, cudaMemcpyAsync(x_out, c->x.p, n * 8, cudaMemcpyDeviceToHost, s), "D2H x");
+  if (y_out) ok = ok && cuda_ok(c, cudaMemcpyAsync(y_out, c->y.p, n * 8, cudaMemcpyDeviceToHost, s), "D2H y");
+  if (z_out) ok = ok && cuda_ok(c, cudaMemcpyAsync(z_out, c->z.p, n * 8, cudaMemcpyDeviceToHost, s), "D2H z");
+  ok = ok && cuda_ok(c, cudaStreamSynchronize(s), "grow");
+  if (!ok) return PEPCG_ERR_CUDA;
+  return rc;
+}
+
+int pepcg_get_particles_device(void* ctx, int64_t* d_key, int64_t* d_perm, double* d_x,
+                               double* d_y, double* d_z, double* d_q) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return PEPCG_ERR_BAD_ARG;
+  if (!c->has_tree) {
+    c->err = "no grown tree";
+    return PEPCG_ERR_NO_TREE;
+  }
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  const int64_t n = c->n;
+  bool ok = true;
+  if (d_key) ok = ok && cuda_ok(c, cudaMemcpyAsync(d_key, c->key.p, n * 8, cudaMemcpyDeviceToDevice, s), "key");
+  if (d_x) ok = ok && cuda_ok(c, cudaMemcpyAsync(d_x, c->x.p, n * 8, cudaMemcpyDeviceToDevice, s), "x");
+  if (d_y) ok = ok && cuda_ok(c, cudaMemcpyAsync(d_y, c->y.p, n * 8, cudaMemcpyDeviceToDevice, s), "y");
+  if (d_z) ok = ok && cuda_ok(c, cudaMemcpyAsync(d_z, c->z.p, n * 8, cudaMemcpyDeviceToDevice, s), "z");
+  if (d_q) ok = ok && cuda_ok(c, cudaMemcpyAsync(d_q, c->q.p, n * 8, cudaMemcpyDeviceToDevice, s), "q");
+  if (d_perm) {
+    std::vector<int32_t> p32(n);
+    std::vector<int64_t> p64(n);
+    ok = ok && cuda_ok(c, cudaMemcpyAsync(p32.data(), c->perm.p, n * 4, cudaMemcpyDeviceToHost, s), "perm") &&
+         cuda_ok(c, cudaStreamSynchronize(s), "perm");
+    for (int64_t i = 0; ok && i < n; ++i) p64[i] = p32[i];
+    ok = ok && cuda_ok(c, cudaMemcpyAsync(d_perm, p64.data(), n * 8, cudaMemcpyHostToDevice, s), "perm");
+  }
+  ok = ok && cuda_ok(c, cudaStreamSynchronize(s), "get particles");
+  return ok ? PEPCG_OK : PEPCG_ERR_CUDA;
+}
+
+int pepcg_traverse_tree_device(void* ctx, int64_t nt, const double* d_tx, const double* d_ty,
+                               const double* d_tz, const int64_t* d_tkeys, double* d_ex,
+                               double* d_ey, double* d_ez, double* d_pot, double* d_work) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || nt < 0 || !d_tx || !d_ty || !d_tz || !d_ex || !d_ey || !d_ez || !d_pot || !d_work)
+    return PEPCG_ERR_BAD_ARG;
+  cudaSetDevice(c->device);
+  return traverse_device(c, nt, d_tx, d_ty, d_tz, d_tkeys, false, d_ex, d_ey, d_ez, d_pot, d_work);
+}
+
+int pepcg_traverse_self_device(void* ctx, double* d_ex, double* d_ey, double* d_ez,
+                               double* d_pot, double* d_work) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || !d_ex || !d_ey || !d_ez || !d_pot || !d_work) return PEPCG_ERR_BAD_ARG;
+  if (!c->has_tree) {
+    c->err = "no grown tree";
+    return PEPCG_ERR_NO_TREE;
+  }
+  cudaSetDevice(c->device);
+  return traverse_device(c, c->n, c->x.p, c->y.p, c->z.p, c->key.p, true, d_ex, d_ey, d_ez, d_pot,
+                         d_work);
+}
+
+int pepcg_traverse_tree(void* ctx, int64_t nt, const double* tx, const double* ty,
+                        const double* tz, const int64_t* tkeys, double* ex, double* ey,
+                        double* ez, double* pot, double* work) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || nt < 0 || !tx || !ty || !tz || !ex || !ey || !ez || !pot || !work)
+    return PEPCG_ERR_BAD_ARG;
+  if (nt == 0) return PEPCG_OK;
+  cudaSetDevice(c->device);
+  if (!ensure(c, c->tgt, 8 * nt, "targets") || (tkeys && !ensure(c, c->tkeys, nt, "tkeys")))
+    return PEPCG_ERR_OOM;
+  cudaStream_t s = c->stream;
+  double* b = c->tgt.p;
+  const double* hin[8] = {tx, ty, tz, ex, ey, ez, pot, work};
+  bool ok = true;
+  for (int k = 0; k < 8; ++k)
+    ok = ok && cuda_ok(c, cudaMemcpyAsync(b + k * nt, hin[k], nt * 8, cudaMemcpyHostToDevice, s), "H2D");
+  if (tkeys) ok = ok && cuda_ok(c, cudaMemcpyAsync(c->tkeys.p, tkeys, nt * 8, cudaMemcpyHostToDevice, s), "H2D");
+  if (!ok) return PEPCG_ERR_CUDA;
+  int rc = traverse_device(c, nt, b, b + nt, b + 2 * nt, tkeys ? c->tkeys.p : nullptr, false,
+                           b + 3 * nt, b + 4 * nt, b + 5 * nt, b + 6 * nt, b + 7 * nt);
+  if (rc && rc != PEPCG_WARN_NOT_NEUTRAL) return rc;
+  double* hout[5] = {ex, ey, ez, pot, work};
+  for (int k = 0; k < 5; ++k)
+    ok = ok && cuda_ok(c, cudaMemcpyAsync(hout[k], b + (3 + k) * nt, nt * 8, cudaMemcpyDeviceToHost, s), "D2H");
+  ok = ok && cuda_ok(c, cudaStreamSynchronize(s), "traverse");
+  return ok ? rc : PEPCG_ERR_CUDA;
+}
+
+int pepcg_timber_tree(void* ctx) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return PEPCG_ERR_BAD_ARG;
+  c->has_tree = false;  // buffers are kept for the next grow (reused, grow-only)
+  return PEPCG_OK;
+}
+
+int pepcg_stats_get(void* ctx, pepcg_stats* s) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || !s) return PEPCG_ERR_BAD_ARG;
+  c->st.npart = c->n;
+  c->st.nleaf = c->n;
+  c->st.ntwig = c->ntwig;
+  c->st.max_level = c->max_level;
+  c->st.dup_count = c->dup_count;
+  for (int i = 0; i < 9; ++i) c->st.box[i] = c->box[i];
+  *s = c->st;
+  return PEPCG_OK;
+}
+
+int64_t pepcg_num_nodes(void* ctx) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || !c->has_tree) return 0;
+  return c->nnodes;
+}
+
+int pepcg_tree_export(void* ctx, int64_t* key, int32_t* level, int64_t* leaves,
+                      int64_t* descendants, int64_t* parent, int64_t* first_child,
+                      int64_t* next_sibling, double* moments15) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return PEPCG_ERR_BAD_ARG;
+  if (!c->has_tree) {
+    c->err = "no grown tree";
+    return PEPCG_ERR_NO_TREE;
+  }
+  cudaSetDevice(c->device);
+  return export_tree(c, key, level, leaves, descendants, parent, first_child, next_sibling,
+                     moments15);
+}
+
+int pepcg_direct(void* ctx, int64_t ntest, const int64_t* tidx, double* ex, double* ey,
+                 double* ez, double* pot) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || ntest < 0 || !tidx || !ex || !ey || !ez || !pot) return PEPCG_ERR_BAD_ARG;
+  if (!c->has_tree) {
+    c->err = "no grown tree";
+    return PEPCG_ERR_NO_TREE;
+  }
+  if (ntest == 0) return PEPCG_OK;
+  for (int64_t i = 0; i < ntest; ++i)
+    if (tidx[i] < 0 || tidx[i] >= c->n) {
+      c->err = "pepcg_direct: target index out of range";
+      return PEPCG_ERR_BAD_ARG;
+    }
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  if (!ensure(c, c->tgt, 4 * ntest, "direct") || !ensure(c, c->tkeys, ntest, "direct idx"))
+    return PEPCG_ERR_OOM;
+  if (!cuda_ok(c, cudaMemcpyAsync(c->tkeys.p, tidx, ntest * 8, cudaMemcpyHostToDevice, s), "H2D"))
+    return PEPCG_ERR_CUDA;
+  double* b = c->tgt.p;
+  int rc = direct_device(c, ntest, c->tkeys.p, b, b + ntest, b + 2 * ntest, b + 3 * ntest);
+  if (rc) return rc;
+  double* hout[4] = {ex, ey, ez, pot};
+  bool ok = true;
+  for (int k = 0; k < 4; ++k)
+    ok = ok && cuda_ok(c, cudaMemcpyAsync(hout[k], b + k * ntest, ntest * 8, cudaMemcpyDeviceToHost, s), "D2H");
+  ok = ok && cuda_ok(c, cudaStreamSynchronize(s), "direct");
+  return ok ? PEPCG_OK : PEPCG_ERR_CUDA;
+}
+
+int pepcg_lattice(void* ctx, int64_t nt, const double* tx, const double* ty, const double* tz,
+                  double* ex, double* ey, double* ez, double* pot) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || nt < 0 || !tx || !ty || !tz || !ex || !ey || !ez || !pot) return PEPCG_ERR_BAD_ARG;
+  if (!c->far_field) {
+    c->err = "pepcg_lattice: context is not periodic with far field";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  if (!c->has_tree) {
+    c->err = "no grown tree (the lattice expansion is formed at grow)";
+    return PEPCG_ERR_NO_TREE;
+  }
+  if (nt == 0) return PEPCG_OK;
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  if (!ensure(c, c->tgt, 7 * nt, "lattice")) return PEPCG_ERR_OOM;
+  double* b = c->tgt.p;
+  const double* hin[3] = {tx, ty, tz};
+  bool ok = true;
+  for (int k = 0; k < 3; ++k)
+    ok = ok && cuda_ok(c, cudaMemcpyAsync(b + k * nt, hin[k], nt * 8, cudaMemcpyHostToDevice, s), "H2D");
+  if (!ok) return PEPCG_ERR_CUDA;
+  int rc = lattice_add(c, nt, b, b + nt, b + 2 * nt, b + 3 * nt, b + 4 * nt, b + 5 * nt, b + 6 * nt, true);
+  if (rc) return rc;
+  double* hout[4] = {ex, ey, ez, pot};
+  for (int k = 0; k < 4; ++k)
+    ok = ok && cuda_ok(c, cudaMemcpyAsync(hout[k], b + (3 + k) * nt, nt * 8, cudaMemcpyDeviceToHost, s), "D2H");
+  ok = ok && cuda_ok(c, cudaStreamSynchronize(s), "lattice");
+  return ok ? PEPCG_OK : PEPCG_ERR_CUDA;
+}
+
+}  // extern "C"

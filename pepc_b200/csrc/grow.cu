@@ -1,0 +1,867 @@
+// grow.cu -- pepc_grow_tree on the device (sm_100a):
+//   bounding box -> space-filling-curve keys -> LSD radix sort of (key, index)
+//   -> permutation of the particle payload -> duplicate-key fix -> octree from
+//   the sorted keys -> upward multipole pass.
+// Reference: tree_grow (src/treecode/lpepcsrc/module_tree_grow.f90:37-138).
+// Compiled with --fmad=false: the FP64 arithmetic below must equal a plain
+// IEEE evaluation of the reference's expressions.
+
+#include "internal.cuh"
+
+namespace pepcg {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// ---------------------------------------------------------------------------
+// Bounding box: box_create (module_box.f90:48-93)
+// ---------------------------------------------------------------------------
+__global__ void k_bbox_partial(int64_t n, const double* __restrict__ x,
+                               const double* __restrict__ y, const double* __restrict__ z,
+                               double* __restrict__ part, uint32_t* status) {
+  double lo[3] = {INFINITY, INFINITY, INFINITY};
+  double hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  bool bad = false;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double v[3] = {x[i], y[i], z[i]};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      bad |= !isfinite(v[d]);
+      lo[d] = fmin(lo[d], v[d]);
+      hi[d] = fmax(hi[d], v[d]);
+    }
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(status, ST_NONFINITE);
+  __shared__ double s[6][kThreads / 32];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+      hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+    }
+  }
+  int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    for (int d = 0; d < 3; ++d) {
+      s[d][w] = lo[d];
+      s[3 + d][w] = hi[d];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double r = s[threadIdx.x][0];
+    for (int k = 1; k < kThreads / 32; ++k)
+      r = threadIdx.x < 3 ? fmin(r, s[threadIdx.x][k]) : fmax(r, s[threadIdx.x][k]);
+    part[blockIdx.x * 6 + threadIdx.x] = r;
+  }
+}
+
+// final reduction + margin (module_box.f90:71-84) + boxlength2 (module_tree.f90:196-201)
+__global__ void k_bbox_final(int nparts, const double* __restrict__ part, int cubic,
+                             double* __restrict__ box) {
+  if (threadIdx.x != 0) return;
+  double lo[3], hi[3];
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = part[d];
+    hi[d] = part[3 + d];
+  }
+  for (int b = 1; b < nparts; ++b)
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = fmin(lo[d], part[b * 6 + d]);
+      hi[d] = fmax(hi[d], part[b * 6 + 3 + d]);
+    }
+  if (cubic) {
+    double l = fmin(lo[0], fmin(lo[1], lo[2])), h = fmax(hi[0], fmax(hi[1], hi[2]));
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = l;
+      hi[d] = h;
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    double s = hi[d] - lo[d];
+    double mn = lo[d] - s / 10000.0;
+    double mx = hi[d] + s / 10000.0;
+    box[d] = mn;
+    box[3 + d] = mx;
+    box[6 + d] = mx - mn;
+  }
+  double b0 = fmax(box[6], fmax(box[7], box[8]));
+  double bl = b0 * b0;
+  box[9] = bl;
+  for (int l = 1; l <= kMaxLevel; ++l) {
+    bl = bl / 4.0;
+    box[9 + l] = bl;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Keys: compute_particle_keys (module_spacefilling.f90:224-257) with
+// intcoord_to_key_hilbert3D (:380-440) or the 3D Morton interleave.
+// ---------------------------------------------------------------------------
+__constant__ int8_t c_CI3[8] = {0, 1, 3, 2, 7, 6, 4, 5};  // :389
+__constant__ int8_t c_G3x[8] = {5, 6, 0, 5, 5, 0, 6, 5};  // :390 exchange
+__constant__ int8_t c_G3r[8] = {0, 0, 0, 5, 0, 0, 6, 5};  // :390 reverse
+
+__device__ __forceinline__ uint64_t hilbert3d(int64_t i0, int64_t i1, int64_t i2) {
+  int64_t it[3] = {i0, i1, i2};
+  uint64_t key = 1;
+#pragma unroll 1
+  for (int i = kMaxLevel - 1; i >= 0; --i) {
+    int cval = (int)((((it[2] >> i) & 1) << 2) | (((it[1] >> i) & 1) << 1) | ((it[0] >> i) & 1));
+    const int64_t lowmask = (int64_t(1) << i) - 1;
+    it[0] &= lowmask;
+    it[1] &= lowmask;
+    it[2] &= lowmask;
+    int h = c_CI3[cval];
+    int ex = c_G3x[h], rv = c_G3r[h];
+    key = (key << 3) | (uint64_t)h;
+    if (ex == 5) {
+      int64_t t = it[0]; it[0] = it[2]; it[2] = t;
+    } else if (ex == 6) {
+      int64_t t = it[1]; it[1] = it[2]; it[2] = t;
+    }
+    if (rv & 1) it[0] = (~it[0]) & lowmask;
+    if (rv & 2) it[1] = (~it[1]) & lowmask;
+    if (rv & 4) it[2] = (~it[2]) & lowmask;
+  }
+  return key;
+}
+
+__device__ __forceinline__ uint64_t morton3d(int64_t i0, int64_t i1, int64_t i2) {
+  uint64_t key = 1;
+#pragma unroll 4
+  for (int i = kMaxLevel - 1; i >= 0; --i)
+    key = (key << 3) | (uint64_t)((((i2 >> i) & 1) << 2) | (((i1 >> i) & 1) << 1) | ((i0 >> i) & 1));
+  return key;
+}
+
+__global__ void k_keys(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                       const double* __restrict__ z, const double* __restrict__ box, int curve,
+                       uint64_t* __restrict__ keys, int32_t* __restrict__ idx) {
+  __shared__ double sb[6];
+  if (threadIdx.x < 3) {
+    sb[threadIdx.x] = box[threadIdx.x];
+    // s = boxsize / 2**maxlevel (module_spacefilling.f90:238), exact
+    sb[3 + threadIdx.x] = box[6 + threadIdx.x] / 1048576.0;
+  }
+  __syncthreads();
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    // coord_to_intcoord_with_refinement_length (:218): int() truncates
+    int64_t i0 = __double2ll_rz((x[i] - sb[0]) / sb[3]);
+    int64_t i1 = __double2ll_rz((y[i] - sb[1]) / sb[4]);
+    int64_t i2 = __double2ll_rz((z[i] - sb[2]) / sb[5]);
+    keys[i] = curve == PEPCG_CURVE_MORTON ? morton3d(i0, i1, i2) : hilbert3d(i0, i1, i2);
+    idx[i] = (int32_t)i;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// LSD radix sort of (uint64 key, int32 index), 8 passes of 8 bits, stable.
+// Pass = per-block digit histogram -> exclusive scan over (digit, block) ->
+// stable scatter (warp match + block prefix per 256-key row).
+// ---------------------------------------------------------------------------
+constexpr int kSortRows = 16;                       // rows of 256 keys per block
+constexpr int kSortChunk = kSortRows * kThreads;    // 4096 keys per block
+
+__global__ void k_sort_hist(int64_t n, const uint64_t* __restrict__ keys, int shift,
+                            uint32_t* __restrict__ hist, int nblocks) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  int64_t base = (int64_t)blockIdx.x * kSortChunk;
+  for (int r = 0; r < kSortRows; ++r) {
+    int64_t i = base + r * kThreads + threadIdx.x;
+    if (i < n) atomicAdd(&h[(keys[i] >> shift) & 255u], 1u);
+  }
+  __syncthreads();
+  hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void k_sort_scatter(int64_t n, const uint64_t* __restrict__ kin,
+                               const int32_t* __restrict__ vin, uint64_t* __restrict__ kout,
+                               int32_t* __restrict__ vout, int shift,
+                               const uint32_t* __restrict__ offs, int nblocks) {
+  __shared__ uint32_t running[256];
+  __shared__ uint32_t wcnt[kThreads / 32][257];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  running[threadIdx.x] = offs[(int64_t)threadIdx.x * nblocks + blockIdx.x];
+  for (int w = 0; w < kThreads / 32; ++w) wcnt[w][threadIdx.x] = 0;
+  if (threadIdx.x < kThreads / 32) wcnt[threadIdx.x][256] = 0;
+  __syncthreads();
+  const unsigned lt = (1u << lane) - 1u;
+  int64_t base = (int64_t)blockIdx.x * kSortChunk;
+  for (int r = 0; r < kSortRows; ++r) {
+    int64_t i = base + r * kThreads + threadIdx.x;
+    bool valid = i < n;
+    uint64_t k = valid ? kin[i] : 0;
+    int32_t v = valid ? vin[i] : 0;
+    int d = valid ? (int)((k >> shift) & 255u) : 256;
+    unsigned peers = __match_any_sync(0xffffffffu, d);
+    int lrank = __popc(peers & lt);
+    int leader = __ffs(peers) - 1;
+    if (lane == leader) wcnt[warp][d] = __popc(peers);
+    __syncthreads();
+    {  // exclusive prefix over warps for digit threadIdx.x
+      int b = threadIdx.x;
+      uint32_t run = running[b];
+#pragma unroll
+      for (int w = 0; w < kThreads / 32; ++w) {
+        uint32_t t = wcnt[w][b];
+        wcnt[w][b] = run;
+        run += t;
+      }
+      running[b] = run;
+    }
+    __syncthreads();
+    if (valid) {
+      uint32_t dst = wcnt[warp][d] + lrank;
+      kout[dst] = k;
+      vout[dst] = v;
+    }
+    __syncthreads();
+    if (lane == leader) wcnt[warp][d] = 0;
+    // wcnt of digits not present in this warp were overwritten by the prefix
+    // pass; clear the whole row owned by this thread's digit for the next row
+    for (int w = 0; w < kThreads / 32; ++w) wcnt[w][threadIdx.x] = 0;
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Exclusive scans (uint32 / int32): reduce per block, scan block sums, apply.
+// ---------------------------------------------------------------------------
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kThreads * kScanItems;  // 2048
+
+template <class T>
+__device__ __forceinline__ T block_exclusive_scan(T v, T* smem, T& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) smem[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    T s = lane < kThreads / 32 ? smem[lane] : T(0);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      T y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < kThreads / 32) smem[lane] = s;
+  }
+  __syncthreads();
+  T wpre = warp > 0 ? smem[warp - 1] : T(0);
+  total = smem[kThreads / 32 - 1];
+  __syncthreads();
+  return wpre + x - v;
+}
+
+template <class T>
+__global__ void k_scan_reduce(const T* __restrict__ in, int64_t n, T* __restrict__ bsum) {
+  __shared__ T sm[32];
+  int64_t base = (int64_t)blockIdx.x * kScanTile;
+  T s = 0;
+  for (int k = 0; k < kScanItems; ++k) {
+    int64_t i = base + (int64_t)threadIdx.x * kScanItems + k;
+    if (i < n) s += in[i];
+  }
+  T tot;
+  block_exclusive_scan<T>(s, sm, tot);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+}
+
+template <class T>
+__global__ void k_scan_blocks(T* __restrict__ bsum, int64_t nb) {
+  // single block: sequential over tiles of kThreads
+  __shared__ T sm[32];
+  T carry = 0;
+  for (int64_t b0 = 0; b0 < nb; b0 += kThreads) {
+    int64_t i = b0 + threadIdx.x;
+    T v = i < nb ? bsum[i] : T(0);
+    T tot;
+    T ex = block_exclusive_scan<T>(v, sm, tot);
+    if (i < nb) bsum[i] = carry + ex;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) bsum[nb] = carry;
+}
+
+template <class T>
+__global__ void k_scan_apply(const T* __restrict__ in, int64_t n, const T* __restrict__ bsum,
+                             T* __restrict__ out) {
+  __shared__ T sm[32];
+  int64_t base = (int64_t)blockIdx.x * kScanTile;
+  T v[kScanItems];
+  T s = 0;
+  for (int k = 0; k < kScanItems; ++k) {
+    int64_t i = base + (int64_t)threadIdx.x * kScanItems + k;
+    v[k] = i < n ? in[i] : T(0);
+    s += v[k];
+  }
+  T tot;
+  T ex = block_exclusive_scan<T>(s, sm, tot) + bsum[blockIdx.x];
+  for (int k = 0; k < kScanItems; ++k) {
+    int64_t i = base + (int64_t)threadIdx.x * kScanItems + k;
+    if (i < n) out[i] = ex;
+    ex += v[k];
+  }
+}
+
+template <class T>
+void exclusive_scan(const T* in, T* out, int64_t n, T* tmp, cudaStream_t s) {
+  int64_t nb = (n + kScanTile - 1) / kScanTile;
+  k_scan_reduce<T><<<(unsigned)nb, kThreads, 0, s>>>(in, n, tmp);
+  k_scan_blocks<T><<<1, kThreads, 0, s>>>(tmp, nb);
+  k_scan_apply<T><<<(unsigned)nb, kThreads, 0, s>>>(in, n, tmp, out);
+}
+
+// ---------------------------------------------------------------------------
+// Permute the payload into key order, flag duplicates (module_domains.f90:199-234)
+// ---------------------------------------------------------------------------
+__global__ void k_permute(int64_t n, const uint64_t* __restrict__ skey,
+                          const int32_t* __restrict__ sval, const double* __restrict__ x,
+                          const double* __restrict__ y, const double* __restrict__ z,
+                          const double* __restrict__ q, double* __restrict__ xo,
+                          double* __restrict__ yo, double* __restrict__ zo,
+                          double* __restrict__ qo, int64_t* __restrict__ ko,
+                          int64_t* __restrict__ korig, int32_t* __restrict__ perm,
+                          unsigned long long* dupcount, int32_t* duplist, int dupcap) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int32_t j = sval[i];
+    uint64_t k = skey[i];
+    xo[i] = x[j];
+    yo[i] = y[j];
+    zo[i] = z[j];
+    qo[i] = q[j];
+    ko[i] = (int64_t)k;
+    korig[i] = (int64_t)k;
+    perm[i] = j;
+    if (i + 1 < n && skey[i + 1] == k) {
+      unsigned long long slot = atomicAdd(dupcount, 1ull);
+      if (slot < (unsigned long long)dupcap) duplist[slot] = (int32_t)i;
+    }
+  }
+}
+
+// key_to_intcoord_hilbert, module_spacefilling.f90:501-565
+__device__ void key_to_intcoord_hilbert(int64_t key, int64_t ic[3]) {
+  const int C3[8] = {0, 1, 3, 2, 6, 7, 5, 4};
+  int lev = (63 - __clzll((unsigned long long)key)) / 3;
+  ic[0] = ic[1] = ic[2] = 0;
+  for (int i = 0; i < lev; ++i) {
+    int h = (int)((key >> (3 * i)) & 7);
+    int cval = C3[h], rev = c_G3r[h], exch = c_G3x[h];
+    if (i > 0) {
+      for (int j = 0; j < 3; ++j)
+        if ((rev >> j) & 1) ic[j] = (~ic[j]) & ((int64_t(1) << i) - 1);
+      for (int j = 0; j < 2; ++j) {
+        if (!((exch >> j) & 1)) continue;
+        for (int k = j + 1; k < 3; ++k)
+          if ((exch >> k) & 1) {
+            int64_t t = ic[j]; ic[j] = ic[k]; ic[k] = t;
+          }
+      }
+    }
+    for (int j = 0; j < 3; ++j) ic[j] |= (int64_t)((cval >> j) & 1) << i;
+  }
+  for (int j = 0; j < 3; ++j) ic[j] <<= (kMaxLevel - lev);
+}
+
+__device__ void key_to_intcoord_morton(int64_t key, int64_t ic[3]) {
+  int lev = (63 - __clzll((unsigned long long)key)) / 3;
+  ic[0] = ic[1] = ic[2] = 0;
+  for (int i = 0; i < lev; ++i)
+    for (int j = 0; j < 3; ++j) ic[j] |= ((key >> (3 * i + j)) & 1) << i;
+  for (int j = 0; j < 3; ++j) ic[j] <<= (kMaxLevel - lev);
+}
+
+// Duplicate-key fix, module_domains.f90:268-307, executed in the reference's
+// sequential order by one thread over the (rare) duplicate positions.  Keys
+// that changed get new coordinates from key_to_coord (module_spacefilling.f90:445-471).
+__global__ void k_dupfix(int64_t n, int64_t* __restrict__ key, const int64_t* __restrict__ korig,
+                         double* __restrict__ x, double* __restrict__ y, double* __restrict__ z,
+                         const unsigned long long* __restrict__ dupcount,
+                         int32_t* __restrict__ duplist, int dupcap, const double* __restrict__ box,
+                         int curve, uint32_t* status) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  unsigned long long nd = *dupcount;
+  if (nd == 0) return;
+  if (nd > (unsigned long long)dupcap) {
+    atomicOr(status, ST_DUP_OVERFLOW);
+    return;
+  }
+  int m = (int)nd;
+  for (int a = 1; a < m; ++a) {  // the atomic append is unordered: insertion sort
+    int32_t v = duplist[a];
+    int b = a - 1;
+    while (b >= 0 && duplist[b] > v) {
+      duplist[b + 1] = duplist[b];
+      --b;
+    }
+    duplist[b + 1] = v;
+  }
+  // key_diffs(i) = key(i+1) - key(i), and key_diffs(npnew) = 1 (last rank)
+  auto kd = [&](int64_t i) -> int64_t { return (i >= n - 1) ? 1 : key[i + 1] - key[i]; };
+  int64_t lo_changed = n, hi_changed = -1;
+  for (int a = 0; a < m; ++a) {
+    int64_t i = duplist[a];
+    if (kd(i) >= 1) continue;
+    int64_t jmax = (n - 1 - i) > (i + 1) ? (n - 1 - i) : (i + 1);
+    for (int64_t j = 1; j <= jmax; ++j) {
+      int64_t dn = i - j < 0 ? 0 : i - j;
+      int64_t up = (i + j < n - 2) ? i + j : n - 2;
+      if (kd(dn) > 1) {
+        for (int64_t t = (i - j + 1 < 0 ? 0 : i - j + 1); t <= i; ++t) key[t] -= 1;
+        lo_changed = min(lo_changed, i - j + 1 < 0 ? (int64_t)0 : i - j + 1);
+        hi_changed = max(hi_changed, i);
+        break;
+      } else if (up >= 0 && kd(up) > 1) {
+        int64_t top = (i + j < n - 1) ? i + j : n - 1;
+        for (int64_t t = i + 1; t <= top; ++t) key[t] += 1;
+        lo_changed = min(lo_changed, i + 1);
+        hi_changed = max(hi_changed, top);
+        break;
+      }
+    }
+  }
+  for (int64_t i = lo_changed; i <= hi_changed; ++i) {
+    if (key[i] == korig[i]) continue;
+    int64_t ic[3];
+    if (curve == PEPCG_CURVE_MORTON) key_to_intcoord_morton(key[i], ic);
+    else key_to_intcoord_hilbert(key[i], ic);
+    double c[3];
+    for (int d = 0; d < 3; ++d) {
+      double s = box[6 + d] / 1048576.0;
+      c[d] = ((double)ic[d] + 0.5) * s + box[d];
+    }
+    x[i] = c[0];
+    y[i] = c[1];
+    z[i] = c[2];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Octree from sorted, distinct keys.
+// LCP(i, i+1) = number of leading octal digits shared (excluding the
+// placeholder).  Particle i has its leaf at level
+//   lev_i = max(LCP(i-1, i), LCP(i, i+1)) + 1
+// (a twig exists for every prefix shared by >= 2 particles and a leaf holds
+// one particle, module_tree_grow.f90:646-691), starts the nodes of levels
+// LCP(i-1,i)+1 .. lev_i and ends the nodes of levels LCP(i,i+1)+1 .. lev_i.
+// Forward-preorder index (the reference's insertion order) of the node that
+// particle s starts at level l: S_s + (l - LCP(s-1,s) - 1).  Postorder index
+// of the node that particle e ends at level l: E_e + (lev_e - l); the walk
+// order RPO is the reverse of the postorder.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int lcp_keys(uint64_t a, uint64_t b) {
+  uint64_t d = a ^ b;
+  if (d == 0) return kMaxLevel;  // identical: unsplittable
+  int h = 63 - __clzll((unsigned long long)d);
+  return (kMaxLevel - 1) - h / 3;
+}
+
+__global__ void k_node_counts(int64_t n, const int64_t* __restrict__ key,
+                              int8_t* __restrict__ lev, int8_t* __restrict__ lcpn,
+                              int32_t* __restrict__ cstart, int32_t* __restrict__ cend,
+                              uint32_t* status, int* maxlev) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t k = (uint64_t)key[i];
+    int lp = i > 0 ? lcp_keys((uint64_t)key[i - 1], k) : -1;
+    int ln = i + 1 < n ? lcp_keys(k, (uint64_t)key[i + 1]) : -1;
+    int l = (lp > ln ? lp : ln) + 1;
+    if (l > kMaxLevel) {  // "no more levels", module_tree_grow.f90:671-675
+      atomicOr(status, ST_MAXLEVEL);
+      l = kMaxLevel;
+    }
+    lev[i] = (int8_t)l;
+    lcpn[i] = (int8_t)ln;
+    if (l > 0) atomicMax(maxlev, l);
+    cstart[i] = l - (lp + 1) + 1;
+    cend[i] = l - ln;
+  }
+}
+
+__device__ __forceinline__ int64_t group_end(const int64_t* __restrict__ key, int64_t n,
+                                             int64_t from, uint64_t prefix, int sh) {
+  // largest j >= from with key[j] >> sh == prefix (key[from] is known to match)
+  int64_t step = 1, lo = from;
+  while (lo + step < n && ((uint64_t)key[lo + step] >> sh) == prefix) {
+    lo += step;
+    step <<= 1;
+  }
+  int64_t hi = lo + step < n ? lo + step : n;  // exclusive bound, key[hi] mismatches or hi == n
+  while (hi - lo > 1) {
+    int64_t mid = lo + (hi - lo) / 2;
+    if (((uint64_t)key[mid] >> sh) == prefix) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void k_build_nodes(int64_t n, int64_t M, const int64_t* __restrict__ key,
+                              const int8_t* __restrict__ lev, const int8_t* __restrict__ lcpn,
+                              const int32_t* __restrict__ S, const int32_t* __restrict__ E,
+                              const double* __restrict__ x, const double* __restrict__ y,
+                              const double* __restrict__ z, const double* __restrict__ q,
+                              double4* __restrict__ nc4, int2* __restrict__ meta,
+                              int32_t* __restrict__ fpo2rpo, int32_t* __restrict__ rpo2fpo,
+                              int32_t* __restrict__ first_part, int32_t* __restrict__ nleaves,
+                              int64_t* __restrict__ nkey) {
+  for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < n;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t ks = (uint64_t)key[s];
+    const int ls = lev[s];
+    const int Ls = s > 0 ? lcpn[s - 1] + 1 : 0;
+    const int64_t Ss = S[s];
+    int64_t e = s;
+    for (int l = ls; l >= Ls; --l) {
+      const int sh = 3 * (kMaxLevel - l);
+      const uint64_t prefix = ks >> sh;
+      if (l < ls) e = group_end(key, n, e, prefix, sh);
+      const int64_t fpo = Ss + (l - Ls);
+      const int le = lev[e];
+      const int64_t rpo = M - 1 - ((int64_t)E[e] + (le - l));
+      const int64_t next_fpo = (e + 1 < n) ? (int64_t)S[e + 1] : M;
+      const int64_t size = next_fpo - fpo;
+      const bool leaf = (l == ls);
+      meta[rpo] = make_int2((int32_t)(rpo + size), l | (leaf ? kLeafFlag : 0));
+      fpo2rpo[fpo] = (int32_t)rpo;
+      rpo2fpo[rpo] = (int32_t)fpo;
+      first_part[rpo] = (int32_t)s;
+      nleaves[rpo] = (int32_t)(e - s + 1);
+      nkey[rpo] = (int64_t)prefix;
+      if (leaf) nc4[rpo] = make_double4(x[s], y[s], z[s], q[s]);
+    }
+  }
+}
+
+// links: parent / number of children (twigs) and key-order traversal pointers
+__global__ void k_link(int64_t M, const int2* __restrict__ meta,
+                       const int32_t* __restrict__ rpo2fpo, const int32_t* __restrict__ fpo2rpo,
+                       int2* __restrict__ fwd, int32_t* __restrict__ parent,
+                       int32_t* __restrict__ nchild, int32_t* __restrict__ upcnt) {
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < M;
+       u += (int64_t)gridDim.x * blockDim.x) {
+    int2 mu = meta[u];
+    const bool leaf = (mu.y & kLeafFlag) != 0;
+    const int64_t size = (int64_t)mu.x - u;
+    const int64_t f = rpo2fpo[u];
+    int first = leaf ? (int)M : fpo2rpo[f + 1];
+    int after = (f + size >= M) ? (int)M : fpo2rpo[f + size];
+    fwd[u] = make_int2(first, after);
+    upcnt[u] = 0;
+    if (u == 0) parent[0] = -1;
+    if (!leaf) {
+      int cnt = 0;
+      for (int64_t c = u + 1; c < mu.x; c = meta[c].x) {
+        parent[c] = (int32_t)u;
+        ++cnt;
+      }
+      nchild[u] = cnt;
+    } else {
+      nchild[u] = 0;
+    }
+  }
+}
+
+// Upward pass: tree_node_update_from_children / shift_multipoles_up
+// (module_tree_grow.f90:762-821, coulomb/module_interaction_specific.f90:84-140).
+// One thread per leaf climbs; the last child to arrive at a parent (atomic
+// counter) computes the parent from all its children in key order.
+__device__ __forceinline__ void load_child(const double4* nc4, const int2* meta,
+                                           const double* mom, const double2* aux, int64_t c,
+                                           Moments& m) {
+  const double2* p2 = reinterpret_cast<const double2*>(&nc4[c]);
+  double2 a0 = __ldcg(p2), a1 = __ldcg(p2 + 1);
+  m.coc[0] = a0.x;
+  m.coc[1] = a0.y;
+  m.coc[2] = a1.x;
+  m.q = a1.y;
+  int2 mc = __ldcg(&meta[c]);
+  if (mc.y & kLeafFlag) {  // multipole_from_particle, specific.f90:67-79
+    m.absq = fabs(a1.y);
+    for (int k = 0; k < 9; ++k) m.m[k] = 0.0;
+    m.bmax = 0.0;
+  } else {
+    double2 b = __ldcg(&aux[c]);
+    m.absq = b.x;
+    m.bmax = b.y;
+    for (int k = 0; k < 9; ++k) m.m[k] = __ldcg(&mom[9 * c + k]);
+  }
+}
+
+__global__ void k_upward(int64_t M, const int2* __restrict__ meta, const int32_t* parent,
+                         const int32_t* __restrict__ nchild, int32_t* upcnt, double4* nc4,
+                         double* mom, double2* aux) {
+  for (int64_t u0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u0 < M;
+       u0 += (int64_t)gridDim.x * blockDim.x) {
+    int2 m0 = meta[u0];
+    if (!(m0.y & kLeafFlag)) continue;
+    int64_t u = parent[u0];
+    while (u >= 0) {
+      __threadfence();
+      int old = atomicAdd(&upcnt[u], 1);
+      if (old != nchild[u] - 1) break;
+      __threadfence();
+      // gather children: RPO chain is last..first child; store reversed
+      int64_t ch[8];
+      int nc = 0;
+      int2 mu = __ldcg(&meta[u]);
+      for (int64_t c = u + 1; c < mu.x && nc < 8; c = __ldcg(&meta[c]).x) ch[nc++] = c;
+      Moments cm[8];
+      for (int k = 0; k < nc; ++k) load_child(nc4, meta, mom, aux, ch[nc - 1 - k], cm[k]);
+      Moments p;
+      shift_up64(cm, nc, p);
+      double2* o2 = reinterpret_cast<double2*>(&nc4[u]);
+      __stcg(o2, make_double2(p.coc[0], p.coc[1]));
+      __stcg(o2 + 1, make_double2(p.coc[2], p.q));
+      __stcg(&aux[u], make_double2(p.absq, p.bmax));
+      for (int k = 0; k < 9; ++k) __stcg(&mom[9 * u + k], p.m[k]);
+      u = parent[u];
+    }
+  }
+}
+
+// FP32 copy of the twig moments for the mixed walk
+__global__ void k_mom32(int64_t M, const int2* __restrict__ meta, const double* __restrict__ mom,
+                        float* __restrict__ mom32) {
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < M;
+       u += (int64_t)gridDim.x * blockDim.x) {
+    if (meta[u].y & kLeafFlag) continue;
+    for (int k = 0; k < 9; ++k) mom32[12 * u + k] = (float)mom[9 * u + k];
+  }
+}
+
+inline unsigned grid_for(int64_t n, int threads = kThreads) {
+  int64_t b = (n + threads - 1) / threads;
+  if (b > 148 * 64) b = 148 * 64;
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
+}  // namespace
+
+void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp,
+                        cudaStream_t s) {
+  exclusive_scan<int32_t>(in, out, n, tmp, s);
+}
+
+int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const double* dz,
+                const double* dq) {
+  cudaStream_t s = c->stream;
+  c->has_tree = false;
+  if (n < 2) {
+    c->err = "pepcg_grow_tree: need at least 2 particles (module_domains.f90:187)";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  if (n > (int64_t)INT32_MAX / 4) {
+    c->err = "pepcg_grow_tree: too many particles for 32-bit node indices";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  const int64_t nblk_sort = (n + kSortChunk - 1) / kSortChunk;
+  const int dupcap = 1 << 20;
+  if (!ensure(c, c->x, n, "x") || !ensure(c, c->y, n, "y") || !ensure(c, c->z, n, "z") ||
+      !ensure(c, c->q, n, "q") || !ensure(c, c->key, n, "key") || !ensure(c, c->perm, n, "perm") ||
+      !ensure(c, c->skey, n, "skey") || !ensure(c, c->skey_alt, n, "skey_alt") ||
+      !ensure(c, c->sval, n, "sval") || !ensure(c, c->sval_alt, n, "sval_alt") ||
+      !ensure(c, c->hist, 256 * nblk_sort + 1, "hist") ||
+      !ensure(c, c->scan_tmp, 2 * ((256 * nblk_sort + n) / 2048 + 64), "scan_tmp") ||
+      !ensure(c, c->orig_key, n, "orig_key") || !ensure(c, c->dup_list, dupcap, "dup_list") ||
+      !ensure(c, c->lev, n, "lev") || !ensure(c, c->lcpn, n, "lcpn") ||
+      !ensure(c, c->cstart, n, "cstart") || !ensure(c, c->cend, n, "cend") ||
+      !ensure(c, c->sstart, n, "sstart") || !ensure(c, c->send, n, "send"))
+    return PEPCG_ERR_OOM;
+
+  if (!cuda_ok(c, cudaMemsetAsync(c->d_status, 0, sizeof(uint32_t), s), "memset status") ||
+      !cuda_ok(c, cudaMemsetAsync(c->d_small, 0, 8 * sizeof(unsigned long long), s), "memset"))
+    return PEPCG_ERR_CUDA;
+
+  cudaEventRecord(c->ev[0], s);
+  // box
+  const int nbb = 296;
+  double* part = c->d_part;  // 6 * nbb doubles
+  k_bbox_partial<<<nbb, kThreads, 0, s>>>(n, dx, dy, dz, part, c->d_status);
+  k_bbox_final<<<1, 32, 0, s>>>(nbb, part, c->prm.force_cubic_domain, c->d_box);
+  // keys
+  k_keys<<<grid_for(n), kThreads, 0, s>>>(n, dx, dy, dz, c->d_box, c->prm.curve, c->skey.p,
+                                          c->sval.p);
+  cudaEventRecord(c->ev[1], s);
+  // sort: 8 LSD passes of 8 bits
+  uint64_t* kin = c->skey.p;
+  uint64_t* kout = c->skey_alt.p;
+  int32_t* vin = c->sval.p;
+  int32_t* vout = c->sval_alt.p;
+  const int nb = (int)nblk_sort;
+  for (int pass = 0; pass < 8; ++pass) {
+    const int shift = 8 * pass;
+    k_sort_hist<<<nb, kThreads, 0, s>>>(n, kin, shift, c->hist.p, nb);
+    exclusive_scan<uint32_t>(c->hist.p, c->hist.p, 256 * (int64_t)nb,
+                             reinterpret_cast<uint32_t*>(c->scan_tmp.p), s);
+    k_sort_scatter<<<nb, kThreads, 0, s>>>(n, kin, vin, kout, vout, shift, c->hist.p, nb);
+    std::swap(kin, kout);
+    std::swap(vin, vout);
+  }
+  // after an even number of passes the result is back in skey / sval
+  k_permute<<<grid_for(n), kThreads, 0, s>>>(n, kin, vin, dx, dy, dz, dq, c->x.p, c->y.p, c->z.p,
+                                             c->q.p, c->key.p, c->orig_key.p, c->perm.p,
+                                             c->d_small, c->dup_list.p, dupcap);
+  k_dupfix<<<1, 32, 0, s>>>(n, c->key.p, c->orig_key.p, c->x.p, c->y.p, c->z.p, c->d_small,
+                            c->dup_list.p, dupcap, c->d_box, c->prm.curve, c->d_status);
+  cudaEventRecord(c->ev[2], s);
+  // tree
+  k_node_counts<<<grid_for(n), kThreads, 0, s>>>(n, c->key.p, c->lev.p, c->lcpn.p, c->cstart.p,
+                                                  c->cend.p, c->d_status,
+                                                  reinterpret_cast<int*>(c->d_small + 2));
+  exclusive_scan<int32_t>(c->cstart.p, c->sstart.p, n, c->scan_tmp.p, s);
+  exclusive_scan<int32_t>(c->cend.p, c->send.p, n, c->scan_tmp.p + (n / 2048 + 32), s);
+  // total number of nodes M and the box go to the host (the grid sizes below need M)
+  int32_t last[2];
+  int32_t lastc;
+  if (!cuda_ok(c, cudaMemcpyAsync(&last[0], c->sstart.p + (n - 1), 4, cudaMemcpyDeviceToHost, s),
+               "M") ||
+      !cuda_ok(c, cudaMemcpyAsync(&lastc, c->cstart.p + (n - 1), 4, cudaMemcpyDeviceToHost, s),
+               "M") ||
+      !cuda_ok(c, cudaMemcpyAsync(c->box, c->d_box, 9 * sizeof(double), cudaMemcpyDeviceToHost, s),
+               "box") ||
+      !cuda_ok(c, cudaMemcpyAsync(c->boxlength2, c->d_box + 9, 21 * sizeof(double),
+                                  cudaMemcpyDeviceToHost, s), "box") ||
+      !cuda_ok(c, cudaMemcpyAsync(&c->dup_count, c->d_small, 8, cudaMemcpyDeviceToHost, s), "dup"))
+    return PEPCG_ERR_CUDA;
+  uint32_t st = 0;
+  if (!cuda_ok(c, cudaMemcpyAsync(&st, c->d_status, 4, cudaMemcpyDeviceToHost, s), "status") ||
+      !cuda_ok(c, cudaStreamSynchronize(s), "grow (keys/sort)"))
+    return PEPCG_ERR_CUDA;
+  if (st) return status_to_code(c, st);
+  const int64_t M = (int64_t)last[0] + lastc;
+  // every particle starts at most kMaxLevel + 1 nodes
+  if (M < 2 || M > (int64_t)(kMaxLevel + 1) * n || M >= (int64_t)INT32_MAX) {
+    c->err = "node count out of range";
+    return PEPCG_ERR_NODE_POOL;
+  }
+  if (!ensure(c, c->nc4, M, "nc4") || !ensure(c, c->meta, M, "meta") ||
+      !ensure(c, c->fwd, M, "fwd") || !ensure(c, c->mom, 9 * M, "mom") ||
+      !ensure(c, c->aux, M, "aux") || !ensure(c, c->mom32, 12 * M, "mom32") ||
+      !ensure(c, c->parent, M, "parent") || !ensure(c, c->nchild, M, "nchild") ||
+      !ensure(c, c->upcnt, M, "upcnt") || !ensure(c, c->first_part, M, "first_part") ||
+      !ensure(c, c->nleaves, M, "nleaves") || !ensure(c, c->fpo2rpo, M, "fpo2rpo") ||
+      !ensure(c, c->rpo2fpo, M, "rpo2fpo") || !ensure(c, c->nkey, M, "nkey"))
+    return PEPCG_ERR_OOM;
+  k_build_nodes<<<grid_for(n), kThreads, 0, s>>>(n, M, c->key.p, c->lev.p, c->lcpn.p, c->sstart.p,
+                                                  c->send.p, c->x.p, c->y.p, c->z.p, c->q.p,
+                                                  c->nc4.p, c->meta.p, c->fpo2rpo.p, c->rpo2fpo.p,
+                                                  c->first_part.p, c->nleaves.p, c->nkey.p);
+  k_link<<<grid_for(M), kThreads, 0, s>>>(M, c->meta.p, c->rpo2fpo.p, c->fpo2rpo.p, c->fwd.p,
+                                          c->parent.p, c->nchild.p, c->upcnt.p);
+  cudaEventRecord(c->ev[3], s);
+  k_upward<<<grid_for(M), kThreads, 0, s>>>(M, c->meta.p, c->parent.p, c->nchild.p, c->upcnt.p,
+                                            c->nc4.p, c->mom.p, c->aux.p);
+  k_mom32<<<grid_for(M), kThreads, 0, s>>>(M, c->meta.p, c->mom.p, c->mom32.p);
+  cudaEventRecord(c->ev[4], s);
+  if (!cuda_ok(c, cudaGetLastError(), "grow kernels")) return PEPCG_ERR_CUDA;
+  c->n = n;
+  c->nnodes = M;
+  c->ntwig = M - n;
+  int maxl = 0;
+  cudaMemcpyAsync(&maxl, c->d_small + 2, 4, cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  c->max_level = maxl;
+  c->has_tree = true;
+  return PEPCG_OK;
+}
+
+// Tree export in the reference's insertion (forward preorder) order.
+namespace {
+__global__ void k_export(int64_t M, const int32_t* __restrict__ fpo2rpo,
+                         const int32_t* __restrict__ rpo2fpo, const int2* __restrict__ meta,
+                         const int2* __restrict__ fwd, const int32_t* __restrict__ parent,
+                         const int64_t* __restrict__ nkey, const double4* __restrict__ nc4,
+                         const double* __restrict__ mom, const double2* __restrict__ aux,
+                         int64_t* okey, int32_t* olevel, int64_t* oleaves, int64_t* odesc,
+                         int64_t* oparent, int64_t* ofirst, int64_t* onext, double* omom,
+                         const int32_t* __restrict__ first_part, int64_t n) {
+  for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < M;
+       f += (int64_t)gridDim.x * blockDim.x) {
+    int64_t u = fpo2rpo[f];
+    int2 mu = meta[u];
+    const bool leaf = mu.y & kLeafFlag;
+    const int64_t size = (int64_t)mu.x - u;
+    okey[f] = nkey[u];
+    olevel[f] = mu.y & 0xff;
+    oleaves[f] = 0;  // filled below from the particle range
+    odesc[f] = size - 1;
+    oparent[f] = parent[u] < 0 ? -1 : rpo2fpo[parent[u]];
+    ofirst[f] = leaf ? -1 : f + 1;
+    // next sibling: the node after the subtree in forward preorder, if it has the same parent
+    int64_t after = f + size;
+    int64_t nxt = -1;
+    if (after < M) {
+      int64_t ua = fpo2rpo[after];
+      if (parent[ua] == parent[u]) nxt = after;
+    }
+    onext[f] = nxt;
+    double4 a = nc4[u];
+    double* o = omom + 15 * f;
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+    if (leaf) {
+      o[4] = fabs(a.w);
+      for (int k = 5; k < 15; ++k) o[k] = 0.0;
+    } else {
+      double2 b = aux[u];
+      o[4] = b.x;
+      for (int k = 0; k < 9; ++k) o[5 + k] = mom[9 * u + k];
+      o[14] = b.y;
+    }
+    // leaves = particles in the node's range: from the first particle of this
+    // node to the first particle of the node after the subtree
+    int64_t p0 = first_part[u];
+    int64_t p1 = after < M ? (int64_t)first_part[fpo2rpo[after]] : n;
+    oleaves[f] = p1 - p0;
+  }
+}
+}  // namespace
+
+int export_tree(Ctx* c, int64_t* key, int32_t* level, int64_t* leaves, int64_t* desc,
+                int64_t* parent, int64_t* first_child, int64_t* next_sibling, double* mom15) {
+  const int64_t M = c->nnodes;
+  cudaStream_t s = c->stream;
+  size_t bytes = M * (8 * 6 + 4 + 15 * 8);
+  char* d = nullptr;
+  if (!cuda_ok(c, cudaMallocAsync((void**)&d, bytes, s), "export alloc")) return PEPCG_ERR_OOM;
+  int64_t* dk = (int64_t*)d;
+  int64_t* dl = dk + M;
+  int64_t* dd = dl + M;
+  int64_t* dp = dd + M;
+  int64_t* df = dp + M;
+  int64_t* dn = df + M;
+  double* dm = (double*)(dn + M);
+  int32_t* dlev = (int32_t*)(dm + 15 * M);
+  k_export<<<grid_for(M), kThreads, 0, s>>>(M, c->fpo2rpo.p, c->rpo2fpo.p, c->meta.p, c->fwd.p,
+                                            c->parent.p, c->nkey.p, c->nc4.p, c->mom.p, c->aux.p,
+                                            dk, dlev, dl, dd, dp, df, dn, dm, c->first_part.p, c->n);
+  bool ok = true;
+  auto cp = [&](void* h, const void* dv, size_t b) {
+    if (h) ok = ok && cuda_ok(c, cudaMemcpyAsync(h, dv, b, cudaMemcpyDeviceToHost, s), "export");
+  };
+  cp(key, dk, 8 * M);
+  cp(level, dlev, 4 * M);
+  cp(leaves, dl, 8 * M);
+  cp(desc, dd, 8 * M);
+  cp(parent, dp, 8 * M);
+  cp(first_child, df, 8 * M);
+  cp(next_sibling, dn, 8 * M);
+  cp(mom15, dm, 8 * 15 * M);
+  cudaFreeAsync(d, s);
+  if (!ok || !cuda_ok(c, cudaStreamSynchronize(s), "export")) return PEPCG_ERR_CUDA;
+  return PEPCG_OK;
+}
+
+}  // namespace pepcg

@@ -1,0 +1,274 @@
+// internal.cuh -- shared declarations of libpepcg (sm_100a).
+//
+// Data layout in HBM (all device arrays owned by Ctx):
+//   particles, key order, SoA FP64: x y z q, keys (int64), perm (int32: key
+//     order -> caller order)
+//   nodes, "reverse preorder" (RPO) order: the depth-first preorder of the
+//     octree whose children are visited from the LAST key-ordered child to
+//     the first.  In that order the per-target LIFO walk of the reference
+//     (module_tree_walk_pthreads.f90:604-687: pop last pushed child first) is
+//     a forward scan: open a node -> u + 1, accept/leaf -> skip[u].
+//       nc4[u]   = (coc x, coc y, coc z, charge)           FP64, every node
+//       meta[u]  = (skip, level | leaf flag << 8)          int32 x 2
+//       fwd[u]   = (first child in key order, next node after the subtree in
+//                   key-order preorder)                     int32 x 2
+//       mom[u]   = twig moments (dip x3, quad xx yy zz, xy yz zx) FP64 x 9
+//       aux[u]   = (abs_charge, bmax)                      FP64 x 2 (twigs)
+//       mom32[u] = the 9 moments in FP32 (mixed walk)
+//     rpo2fpo / fpo2rpo map RPO to the reference's node order (forward
+//     preorder = insertion order of module_tree_grow.f90:623-696).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/pepcg.h"
+
+namespace pepcg {
+
+constexpr int kMaxLevel = 20;    // treevars.f90:55 for idim = 3, 64-bit keys
+constexpr int kLeafFlag = 1 << 8;
+
+// device status word bits (set by kernels, read by the host after a launch)
+enum : uint32_t {
+  ST_OK = 0,
+  ST_MAXLEVEL = 1u << 0,
+  ST_INCOMPLETE = 1u << 1,
+  ST_TIMEOUT = 1u << 2,
+  ST_NONFINITE = 1u << 3,
+  ST_DUP_OVERFLOW = 1u << 4,
+  ST_NOT_NEUTRAL = 1u << 5,
+};
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t cap = 0;  // elements
+};
+
+struct Walk;
+
+struct Ctx {
+  pepcg_params prm;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+
+  int64_t n = 0;       // particles in the tree
+  int64_t nnodes = 0;  // M
+  int64_t ntwig = 0;
+  bool has_tree = false;
+
+  // particles (key order)
+  DBuf<double> x, y, z, q;
+  DBuf<int64_t> key;
+  DBuf<int32_t> perm;
+  // grow scratch
+  DBuf<double> in_x, in_y, in_z, in_q;  // staging for host inputs
+  DBuf<uint64_t> skey, skey_alt;
+  DBuf<int32_t> sval, sval_alt;
+  DBuf<uint32_t> hist;
+  DBuf<int64_t> orig_key;               // sorted keys before the duplicate fix
+  DBuf<int32_t> dup_list;
+  DBuf<int8_t> lev, lcpn;
+  DBuf<int32_t> cstart, cend, sstart, send;
+  DBuf<int32_t> scan_tmp;
+  // nodes (RPO)
+  DBuf<double4> nc4;
+  DBuf<int2> meta;
+  DBuf<int2> fwd;
+  DBuf<double> mom;   // 9 * nnodes, node-major
+  DBuf<double2> aux;
+  DBuf<float> mom32;  // 12 * nnodes (coc-relative moments in FP32, padded)
+  DBuf<int32_t> parent, nchild, upcnt, first_part, nleaves;
+  DBuf<int32_t> fpo2rpo, rpo2fpo;
+  DBuf<int64_t> nkey;
+  // walk scratch
+  DBuf<int32_t> tiles;        // PER_TILE tile boundaries
+  DBuf<unsigned long long> counters;  // interaction counters
+  DBuf<double> tgt;           // staging for host targets / results
+  DBuf<int64_t> tkeys;
+  // small device state: box (9), boxlength2 (21), status word, dup count ...
+  double* d_box = nullptr;    // [0..8] box, [9..29] boxlength2
+  uint32_t* d_status = nullptr;
+  unsigned long long* d_small = nullptr;  // [0] dup count, [1] nnodes, [2] tile count, ...
+  double box[9];
+  double boxlength2[kMaxLevel + 1];
+  int max_level = 0;
+  int64_t dup_count = 0;
+
+  // periodic lattice state
+  bool periodic = false, far_field = false;
+  int nboxes = 1;
+  double vbox[3 * 125];      // lattice vectors of the near-field boxes, central last
+  double* d_vbox = nullptr;   // the same on the device
+  double* d_part = nullptr;   // bbox partials (6 * 296)
+  double2* d_mlattice = nullptr;  // 861 complex
+  double2* d_omega = nullptr;     // 231 complex
+  double2* d_mu = nullptr;        // 861 complex
+  double* d_fmm_aux = nullptr;    // box dipole (3), quad trace, fict (4 x 4), nfict, ...
+  double* d_factorial = nullptr;  // 0..80
+
+  // statistics
+  pepcg_stats st{};
+  cudaEvent_t ev[8];
+
+  int32_t* nleaves_ptr() { return nleaves.p; }
+};
+
+// ---- helpers implemented in api.cu ----
+bool cuda_ok(Ctx* c, cudaError_t e, const char* what);
+template <class T>
+bool ensure(Ctx* c, DBuf<T>& b, size_t n, const char* what);
+int status_to_code(Ctx* c, uint32_t st);
+
+// ---- grow.cu ----
+int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const double* dz,
+                const double* dq);
+int export_tree(Ctx* c, int64_t* key, int32_t* level, int64_t* leaves, int64_t* desc,
+                int64_t* parent, int64_t* first_child, int64_t* next_sibling, double* mom15);
+// device scan helper (exclusive, int32), returns the total through *total (device)
+void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp,
+                        cudaStream_t s);
+
+// ---- walk_plain.cu / walk_mixed.cu ----
+// tiles of keyed targets that are not the grown particles (host recursion,
+// module_tree_walk_simple.f90:168-211); writes (first, count) pairs
+int host_tiles(Ctx* c, int64_t nt, const int64_t* d_tkeys, int T, int2* d_tiles, int64_t* ntiles);
+int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
+                    const int64_t* tkeys, bool self, double* ex, double* ey, double* ez,
+                    double* pot, double* work);
+
+// ---- lattice.cu ----
+int lattice_prepare(Ctx* c);
+int lattice_timestep(Ctx* c);
+int lattice_add(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
+                double* ex, double* ey, double* ez, double* pot, bool overwrite);
+
+// ---- direct.cu ----
+int direct_device(Ctx* c, int64_t ntest, const int64_t* d_tidx, double* ex, double* ey,
+                  double* ez, double* pot);
+
+// ---- scalar.cu ----
+// (C entry points only)
+
+}  // namespace pepcg
+
+// ---------------------------------------------------------------------------
+// Device arithmetic shared by the kernels (restatements of the reference
+// backend, operation order as written in the Fortran source).  The FP64
+// translation units are compiled with --fmad=false so that these are
+// bit-identical to a non-contracted IEEE evaluation.
+// ---------------------------------------------------------------------------
+namespace pepcg {
+
+// calc_force_coulomb_3D_direct, coulomb/module_coulomb_kernels.f90:242-257
+__host__ __device__ __forceinline__ void force_leaf64(double q, double dx, double dy, double dz,
+                                                      double dist2, double& ex, double& ey,
+                                                      double& ez, double& phi) {
+  double r = sqrt(dist2);
+  double rd = 1.0 / r;
+  double rd3charge = ((q * rd) * rd) * rd;
+  phi = q * rd;
+  ex = rd3charge * dx;
+  ey = rd3charge * dy;
+  ez = rd3charge * dz;
+}
+
+// calc_force_coulomb_3D, coulomb/module_coulomb_kernels.f90:60-145.
+// m = (dip x, dip y, dip z, quad xx, yy, zz, xy, yz, zx)
+__host__ __device__ __forceinline__ void force_twig64(double q, const double* m, double dx,
+                                                      double dy, double dz, double dist2,
+                                                      double& ex, double& ey, double& ez,
+                                                      double& phi) {
+  const double r = sqrt(dist2);
+  const double rd = 1.0 / r;
+  const double rd2 = rd * rd;
+  const double rd3 = rd * rd2;
+  const double rd5 = rd3 * rd2;
+  const double rd7 = rd5 * rd2;
+  const double dx2 = dx * dx, dy2 = dy * dy, dz2 = dz * dz;
+  const double fdx = ((3.0 * dx2) * rd5) - rd3;
+  const double fdy = ((3.0 * dy2) * rd5) - rd3;
+  const double fdz = ((3.0 * dz2) * rd5) - rd3;
+  const double fdxy = ((3.0 * dx) * dy) * rd5;
+  const double fdyz = ((3.0 * dy) * dz) * rd5;
+  const double fdxz = ((3.0 * dx) * dz) * rd5;
+  const double m2rd5 = 2.0 * rd5;
+  const double m5rd7 = 5.0 * rd7;
+  const double pre1 = ((m5rd7 * dx) * dy) * dz;
+  const double pre2x = (m5rd7 * dx2) - rd5;
+  const double pre2y = (m5rd7 * dy2) - rd5;
+  const double pre2z = (m5rd7 * dz2) - rd5;
+  const double d1 = m[0], d2 = m[1], d3 = m[2];
+  const double q1 = m[3], q2 = m[4], q3 = m[5], qxy = m[6], qyz = m[7], qzx = m[8];
+  const double preQx = pre2x * q1;
+  const double preQy = pre2y * q2;
+  const double preQz = pre2z * q3;
+  phi = (((((((q * rd) - (((dx * d1) + (dy * d2)) + (dz * d3)) * rd3) + fdx * q1) + fdy * q2) +
+           fdz * q3) + fdxy * qxy) + fdyz * qyz) + fdxz * qzx;
+  ex = (((q * dx) * rd3) - (((fdx * d1) + (fdxy * d2)) + (fdxz * d3))) +
+       3.0 * ((((dx * ((((pre2x - m2rd5) * q1) + preQy) + preQz)) + ((dy * pre2x) * qxy)) +
+               ((dz * pre2x) * qzx)) + (pre1 * qyz));
+  ey = (((q * dy) * rd3) - (((fdy * d2) + (fdxy * d1)) + (fdyz * d3))) +
+       3.0 * ((((dy * ((((pre2y - m2rd5) * q2) + preQx) + preQz)) + ((dx * pre2y) * qxy)) +
+               ((dz * pre2y) * qyz)) + (pre1 * qzx));
+  ez = (((q * dz) * rd3) - (((fdz * d3) + (fdyz * d2)) + (fdxz * d1))) +
+       3.0 * ((((dz * ((((pre2z - m2rd5) * q3) + preQy) + preQx)) + ((dx * pre2z) * qzx)) +
+               ((dy * pre2z) * qyz)) + (pre1 * qxy));
+}
+
+// shift_multipoles_up, coulomb/module_interaction_specific.f90:84-140.
+// Children in key order; each child c gives coc (3), charge, abs_charge,
+// moments m (9) and bmax.  Output: coc, charge, abs_charge, m, bmax.
+struct Moments {
+  double coc[3];
+  double q, absq;
+  double m[9];
+  double bmax;
+};
+
+__host__ __device__ __forceinline__ void shift_up64(const Moments* ch, int nc, Moments& p) {
+  double charge = 0.0, absq = 0.0;
+  for (int j = 0; j < nc; ++j) charge = charge + ch[j].q;
+  for (int j = 0; j < nc; ++j) absq = absq + ch[j].absq;
+  double coc[3] = {0.0, 0.0, 0.0};
+  if (absq != 0.0) {
+    for (int j = 0; j < nc; ++j)
+      for (int d = 0; d < 3; ++d) coc[d] = coc[d] + ch[j].coc[d] * ch[j].absq;
+    for (int d = 0; d < 3; ++d) coc[d] = coc[d] / absq;
+  } else {
+    for (int j = 0; j < nc; ++j)
+      for (int d = 0; d < 3; ++d) coc[d] = coc[d] + ch[j].coc[d];
+    for (int d = 0; d < 3; ++d) coc[d] = coc[d] / (double)nc;
+  }
+  double dip[3] = {0, 0, 0}, quad[3] = {0, 0, 0}, xy = 0, yz = 0, zx = 0;
+  for (int j = 0; j < nc; ++j) {
+    const Moments& c = ch[j];
+    double s[3];
+    for (int d = 0; d < 3; ++d) s[d] = coc[d] - c.coc[d];
+    for (int d = 0; d < 3; ++d) dip[d] = (dip[d] + c.m[d]) + c.q * s[d];
+    for (int d = 0; d < 3; ++d)
+      quad[d] = ((quad[d] + c.m[3 + d]) + c.m[d] * s[d]) + (0.5 * c.q) * (s[d] * s[d]);
+    xy = (((xy + c.m[6]) + c.m[0] * s[1]) + c.m[1] * s[0]) + (c.q * s[0]) * s[1];
+    yz = (((yz + c.m[7]) + c.m[1] * s[2]) + c.m[2] * s[1]) + (c.q * s[1]) * s[2];
+    zx = (((zx + c.m[8]) + c.m[2] * s[0]) + c.m[0] * s[2]) + (c.q * s[2]) * s[0];
+  }
+  double bmax = 0.0;
+  for (int j = 0; j < nc; ++j) {
+    double a = coc[0] - ch[j].coc[0], b = coc[1] - ch[j].coc[1], d = coc[2] - ch[j].coc[2];
+    double v = sqrt((a * a + b * b) + d * d) + ch[j].bmax;
+    if (j == 0 || v > bmax) bmax = v;
+  }
+  for (int d = 0; d < 3; ++d) p.coc[d] = coc[d];
+  p.q = charge;
+  p.absq = absq;
+  p.m[0] = dip[0]; p.m[1] = dip[1]; p.m[2] = dip[2];
+  p.m[3] = quad[0]; p.m[4] = quad[1]; p.m[5] = quad[2];
+  p.m[6] = xy; p.m[7] = yz; p.m[8] = zx;
+  p.bmax = bmax;
+}
+
+}  // namespace pepcg

@@ -1,0 +1,586 @@
+// lattice.cu -- periodic far-lattice term of the Coulomb backend
+// (interaction_specific/coulomb/module_fmm_framework.f90) on the device.
+//
+//  prepare  (fmm_framework_prepare, :100-126): lattice coefficients MLattice by
+//           the iteration of calc_lattice_coefficients (:154-213).  For a
+//           unit-cube lattice the reference loads a table that was produced by
+//           that same iteration at Lmax_multipole = 50 (:253-259); running it
+//           at 50 here reproduces the table (to ~1e-14) and the first
+//           Lmax_taylor = 40 orders are kept.
+//  timestep (fmm_framework_timestep, :132-149): box dipole and quadrupole
+//           trace, the central box's multipole expansion omega_tilde (l <= 20,
+//           fictitious charges included) and mu_cent = M2L(MLattice, omega).
+//  add      (fmm_sum_lattice_force, :766-826): per target, O(l <= 20) at the
+//           target, L2L to l <= 1, E and phi, then the extrinsic correction.
+// Expansions use the flat layout tblinv(l, m) = l(l+1)/2 + m, m >= 0.
+// Compiled with --fmad=false.
+
+#include <cmath>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace pepcg {
+namespace {
+
+constexpr int kLM = 20;                    // Lmax_multipole
+constexpr int kLT = 40;                    // Lmax_taylor
+constexpr int kLenM = 231;
+constexpr int kLenT = 861;
+constexpr int kLMTable = 50;               // unit-cube table order
+constexpr int kMaxIter = 32;
+
+__device__ __forceinline__ int tblinv(int l, int m) { return l * (l + 1) / 2 + m; }
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// tbl, :838-854
+__device__ __forceinline__ double2 tbl(const double2* A, int l, int m, int lmax) {
+  if (l > lmax || abs(m) > l) return make_double2(0.0, 0.0);
+  double2 t = A[tblinv(l, abs(m))];
+  if (m < 0) {
+    double s = (m & 1) ? -1.0 : 1.0;
+    t = make_double2(s * t.x, -s * t.y);
+  }
+  return t;
+}
+
+// LegendreP, :1196-1242
+__device__ double legendre_p(int l, int m, double x) {
+  double pll = 0.0, pmm = 1.0;
+  if (m > 0) {
+    double somx2 = sqrt((1.0 - x) * (1.0 + x));
+    double fact = 1.0;
+    for (int i = 1; i <= m; ++i) {
+      pmm = (-pmm * fact) * somx2;
+      fact = fact + 2.0;
+    }
+  }
+  double r;
+  if (l == m) {
+    r = pmm;
+  } else {
+    double pmmp1 = (x * (2.0 * m + 1.0)) * pmm;
+    if (l == m + 1) {
+      r = pmmp1;
+    } else {
+      for (int ll = m + 2; ll <= l; ++ll) {
+        pll = ((x * (2.0 * ll - 1.0)) * pmmp1 - ((double)(ll + m) - 1.0) * pmm) / (double)(ll - m);
+        pmm = pmmp1;
+        pmmp1 = pll;
+      }
+      r = pll;
+    }
+  }
+  return ((m & 1) ? -1.0 : 1.0) * r;
+}
+
+// cartesian_to_spherical, :1083-1103 -> (r, cos theta, phi)
+__device__ __forceinline__ void cart2sph(double cx, double cy, double cz, double s[3]) {
+  s[0] = sqrt((cx * cx + cy * cy) + cz * cz);
+  s[1] = (s[0] == 0.0) ? 1.0 : cz / s[0];
+  s[2] = (cx == 0.0 && cy == 0.0) ? 0.0 : atan2(cy, cx);
+}
+
+// OMultipole, :695-714 (fact = factorial table)
+__device__ __forceinline__ double2 omultipole(int l, int m, const double s[3], const double* fact) {
+  double ph = (double)m * s[2];
+  double sn, cs;
+  sincos(ph, &sn, &cs);
+  double pt = legendre_p(l, m, s[1]) / fact[l + m];
+  double a = (s[0] > 0.0 || l > 0) ? pow(s[0], (double)l) * pt : pt;
+  return make_double2(a * cs, a * -sn);
+}
+
+// MTaylor, :720-733
+__device__ __forceinline__ double2 mtaylor(int l, int m, const double s[3], const double* fact) {
+  double ph = (double)m * s[2];
+  double sn, cs;
+  sincos(ph, &sn, &cs);
+  double p2 = legendre_p(l, m, s[1]) * fact[l - m];
+  double a = (1.0 / pow(s[0], (double)(l + 1))) * p2;
+  return make_double2(a * cs, a * sn);
+}
+
+// sort_abs, :1321-1367 (heap sort by magnitude) on a strided global slice
+__device__ void sort_abs(double* a, int n) {
+  auto sift = [&](int l, int r) {
+    double v = a[l - 1];
+    int jold = l, j = l + l;
+    for (;;) {
+      if (j > r) break;
+      if (j < r && fabs(a[j - 1]) < fabs(a[j])) j = j + 1;
+      if (fabs(v) >= fabs(a[j - 1])) break;
+      a[jold - 1] = a[j - 1];
+      jold = j;
+      j = j + j;
+    }
+    a[jold - 1] = v;
+  };
+  for (int i = n / 2; i >= 1; --i) sift(i, n);
+  for (int i = n; i >= 2; --i) {
+    double t = a[0];
+    a[0] = a[i - 1];
+    a[i - 1] = t;
+    sift(1, i - 1);
+  }
+}
+
+// MstarFunc, :1005-1036: one thread per (l, m), l <= lm
+__global__ void k_mstar(int lm, int nb, const double* __restrict__ vbox, const double* fact,
+                        double* scratch, double2* __restrict__ mstar) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  int len = lm * (lm + 1) / 2 + lm + 1;
+  if (idx >= len) return;
+  int l = (int)((sqrt(8.0 * idx + 1.0) - 1.0) / 2.0);
+  while (l * (l + 1) / 2 > idx) --l;
+  while ((l + 1) * (l + 2) / 2 <= idx) ++l;
+  int m = idx - l * (l + 1) / 2;
+  double* rp = scratch + (int64_t)idx * 2 * nb;
+  double* ip = rp + nb;
+  for (int i = 0; i < nb; ++i) {
+    double s[3];
+    cart2sph(-vbox[3 * i], -vbox[3 * i + 1], -vbox[3 * i + 2], s);
+    double2 t = omultipole(l, m, s, fact);
+    rp[i] = t.x;
+    ip[i] = t.y;
+  }
+  sort_abs(rp, nb);
+  sort_abs(ip, nb);
+  double r = 0.0, im = 0.0;
+  for (int i = 0; i < nb; ++i) {
+    r = r + rp[i];
+    im = im + ip[i];
+  }
+  mstar[idx] = make_double2(r, im);
+}
+
+// LstarFunc, :1042-1077: one thread per (l, m), l <= lt
+__global__ void k_lstar(int lt, int nb, int ws, const double* __restrict__ vbox, const double* fact,
+                        double* scratch, double2* __restrict__ lstar) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  int len = lt * (lt + 1) / 2 + lt + 1;
+  if (idx >= len) return;
+  int l = (int)((sqrt(8.0 * idx + 1.0) - 1.0) / 2.0);
+  while (l * (l + 1) / 2 > idx) --l;
+  while ((l + 1) * (l + 2) / 2 <= idx) ++l;
+  int m = idx - l * (l + 1) / 2;
+  const int cnt = nb * (nb - 1);
+  double* rp = scratch + (int64_t)idx * 2 * cnt;
+  double* ip = rp + cnt;
+  int k = 0;
+  const double f = (double)(2 * ws + 1);
+  for (int i = 0; i < nb - 1; ++i)
+    for (int ii = 0; ii < nb; ++ii) {
+      double s[3];
+      cart2sph(f * vbox[3 * i] + vbox[3 * ii], f * vbox[3 * i + 1] + vbox[3 * ii + 1],
+               f * vbox[3 * i + 2] + vbox[3 * ii + 2], s);
+      double2 t = mtaylor(l, m, s, fact);
+      rp[k] = t.x;
+      ip[k] = t.y;
+      ++k;
+    }
+  sort_abs(rp, cnt);
+  sort_abs(ip, cnt);
+  double r = 0.0, im = 0.0;
+  for (int i = 0; i < cnt; ++i) {
+    r = r + rp[i];
+    im = im + ip[i];
+  }
+  lstar[idx] = make_double2(r, im);
+}
+
+// one step of calc_lattice_coefficients: ML_new = M2L(UL(ML), Mstar) + Lstar
+// (UL, :982-999; M2L, :912-937); scp[l] = (2 ws + 1)**(l + 1)
+__global__ void k_lattice_iter(int lt, int lm, const double2* __restrict__ ML,
+                               const double2* __restrict__ mstar, const double2* __restrict__ lstar,
+                               const double* __restrict__ scp, double2* __restrict__ out) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  int len = lt * (lt + 1) / 2 + lt + 1;
+  if (idx >= len) return;
+  int l = (int)((sqrt(8.0 * idx + 1.0) - 1.0) / 2.0);
+  while (l * (l + 1) / 2 > idx) --l;
+  while ((l + 1) * (l + 2) / 2 <= idx) ++l;
+  int m = idx - l * (l + 1) / 2;
+  double2 t = make_double2(0.0, 0.0);
+  for (int j = 0; j <= lt; ++j) {
+    const double sg = (j & 1) ? -1.0 : 1.0;
+    for (int k = -j; k <= j; ++k) {
+      const int ll = j + l, mm = k + m;
+      double2 a = make_double2(0.0, 0.0);
+      if (ll <= lt && abs(mm) <= ll) {
+        double2 v = ML[tblinv(ll, abs(mm))];
+        const double d = scp[ll];
+        v = make_double2(v.x / d, v.y / d);  // UL
+        if (mm < 0) {
+          const double s = (mm & 1) ? -1.0 : 1.0;
+          v = make_double2(s * v.x, -s * v.y);
+        }
+        a = v;
+      }
+      double2 b = tbl(mstar, j, k, lm);
+      t = cadd(t, cmul(make_double2(sg * a.x, sg * a.y), b));
+    }
+  }
+  out[idx] = cadd(t, lstar[idx]);
+}
+
+// keep the first Lmax_taylor orders of a table of order lt
+__global__ void k_truncate(const double2* __restrict__ src, double2* __restrict__ dst) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx < kLenT) dst[idx] = src[idx];
+}
+
+// box dipole and quadrupole trace (calc_box_dipole, :605-630): block partials
+__global__ void k_box_dipole(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                             const double* __restrict__ z, const double* __restrict__ q,
+                             double cx, double cy, double cz, double* __restrict__ part) {
+  double a[4] = {0, 0, 0, 0};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double r0 = x[i] - cx, r1 = y[i] - cy, r2 = z[i] - cz;
+    a[0] = a[0] + q[i] * r0;
+    a[1] = a[1] + q[i] * r1;
+    a[2] = a[2] + q[i] * r2;
+    a[3] = a[3] + q[i] * ((r0 * r0 + r1 * r1) + r2 * r2);
+  }
+  __shared__ double sm[4][8];
+  for (int c = 0; c < 4; ++c) {
+    double v = a[c];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sm[c][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double v = 0;
+    for (int w = 0; w < 8; ++w) v += sm[threadIdx.x][w];
+    part[4 * blockIdx.x + threadIdx.x] = v;
+  }
+}
+
+// omega_tilde partials (calc_omega_tilde, :514-596): one thread per (l, m),
+// each block sums a contiguous chunk of particles
+constexpr int kOmChunk = 1024;
+__global__ void __launch_bounds__(256) k_omega_partial(int64_t n, const double* __restrict__ x,
+                                                       const double* __restrict__ y,
+                                                       const double* __restrict__ z,
+                                                       const double* __restrict__ q, double cx,
+                                                       double cy, double cz, const double* fact,
+                                                       double2* __restrict__ part) {
+  __shared__ double sp[kOmChunk][4];
+  const int64_t base = (int64_t)blockIdx.x * kOmChunk;
+  const int cnt = (int)min((int64_t)kOmChunk, n - base);
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+    double s[3];
+    cart2sph(x[base + i] - cx, y[base + i] - cy, z[base + i] - cz, s);
+    sp[i][0] = s[0];
+    sp[i][1] = s[1];
+    sp[i][2] = s[2];
+    sp[i][3] = q[base + i];
+  }
+  __syncthreads();
+  const int idx = threadIdx.x;
+  if (idx >= kLenM) return;
+  int l = 0;
+  while ((l + 1) * (l + 2) / 2 <= idx) ++l;
+  const int m = idx - l * (l + 1) / 2;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int i = 0; i < cnt; ++i) {
+    double s[3] = {sp[i][0], sp[i][1], sp[i][2]};
+    double2 o = omultipole(l, m, s, fact);
+    acc = cadd(acc, make_double2(sp[i][3] * o.x, sp[i][3] * o.y));
+  }
+  part[(int64_t)blockIdx.x * kLenM + idx] = acc;
+}
+
+// sum the partials in block order, add the fictitious charges (:536-559),
+// remove a net monopole (:570-573), then mu_cent = M2L(MLattice, omega)
+__global__ void k_omega_final(int nparts, const double2* __restrict__ part, const double* aux,
+                              double cx, double cy, double cz, const double* fact,
+                              double2* __restrict__ omega, uint32_t* status) {
+  const int idx = threadIdx.x;
+  __shared__ double s_fict[4][4];
+  __shared__ int s_nf;
+  if (idx == 0) {
+    s_nf = (int)aux[4];
+    for (int p = 0; p < s_nf; ++p)
+      for (int k = 0; k < 4; ++k) s_fict[p][k] = aux[8 + 4 * p + k];
+  }
+  __syncthreads();
+  if (idx >= kLenM) return;
+  int l = 0;
+  while ((l + 1) * (l + 2) / 2 <= idx) ++l;
+  const int m = idx - l * (l + 1) / 2;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int b = 0; b < nparts; ++b) acc = cadd(acc, part[(int64_t)b * kLenM + idx]);
+  for (int p = 0; p < s_nf; ++p) {
+    double s[3];
+    cart2sph(s_fict[p][0] - cx, s_fict[p][1] - cy, s_fict[p][2] - cz, s);
+    double2 o = omultipole(l, m, s, fact);
+    acc = cadd(acc, make_double2(s_fict[p][3] * o.x, s_fict[p][3] * o.y));
+  }
+  if (idx == 0 && hypot(acc.x, acc.y) > 0.0) {
+    acc = make_double2(0.0, 0.0);
+    atomicOr(status, ST_NOT_NEUTRAL);
+  }
+  omega[idx] = acc;
+}
+
+__global__ void k_mu_cent(const double2* __restrict__ ML, const double2* __restrict__ omega,
+                          double2* __restrict__ mu) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= kLenT) return;
+  int l = 0;
+  while ((l + 1) * (l + 2) / 2 <= idx) ++l;
+  int m = idx - l * (l + 1) / 2;
+  double2 t = make_double2(0.0, 0.0);
+  for (int j = 0; j <= kLT; ++j) {
+    const double sg = (j & 1) ? -1.0 : 1.0;
+    for (int k = -j; k <= j; ++k) {
+      double2 a = tbl(ML, j + l, k + m, kLT);
+      t = cadd(t, cmul(make_double2(sg * a.x, sg * a.y), tbl(omega, j, k, kLM)));
+    }
+  }
+  mu[idx] = t;
+}
+
+// fictitious charges from the box dipole (single thread; :540-552)
+__global__ void k_fict(int nbp, const double* __restrict__ part, double* aux, int p0, int p1,
+                       int p2, const double* lat, const double* origin, int corr) {
+  if (threadIdx.x != 0) return;
+  double a[4] = {0, 0, 0, 0};
+  for (int b = 0; b < nbp; ++b)
+    for (int c = 0; c < 4; ++c) a[c] += part[4 * b + c];
+  for (int c = 0; c < 4; ++c) aux[c] = a[c];
+  int nf = 0;
+  if (corr == 2) {
+    int per[3] = {p0, p1, p2};
+    double sum = 0.0;
+    for (int p = 0; p < 3; ++p) {
+      if (!per[p]) continue;
+      const double* L = lat + 3 * p;
+      for (int d = 0; d < 3; ++d) aux[8 + 4 * nf + d] = origin[d] + L[d];
+      aux[8 + 4 * nf + 3] = -a[p] / sqrt((L[0] * L[0] + L[1] * L[1]) + L[2] * L[2]);
+      ++nf;
+    }
+    for (int p = 0; p < nf; ++p) sum = sum + aux[8 + 4 * p + 3];
+    for (int d = 0; d < 3; ++d) aux[8 + 4 * nf + d] = origin[d];
+    aux[8 + 4 * nf + 3] = -sum;
+    ++nf;
+  }
+  aux[4] = nf;
+}
+
+// fmm_sum_lattice_force per target (:766-826)
+__global__ void __launch_bounds__(128) k_lattice_force(
+    int64_t nt, const double* __restrict__ tx, const double* __restrict__ ty,
+    const double* __restrict__ tz, const double2* __restrict__ mu, const double* __restrict__ aux,
+    const double* __restrict__ vbox, int nbox, double cx, double cy, double cz, double volume,
+    int corr, const double* fact, double* ex, double* ey, double* ez, double* pot, int overwrite) {
+  __shared__ double2 s_mu[kLenM];  // only j <= Lmax_multipole entries are read by L2L
+  __shared__ double s_aux[32];
+  __shared__ double s_vb[3 * 125];
+  __shared__ double s_fact[2 * kLM + 1];
+  for (int i = threadIdx.x; i < kLenM; i += blockDim.x) s_mu[i] = mu[i];
+  for (int i = threadIdx.x; i < 32; i += blockDim.x) s_aux[i] = aux[i];
+  for (int i = threadIdx.x; i < 3 * nbox; i += blockDim.x) s_vb[i] = vbox[i];
+  for (int i = threadIdx.x; i <= 2 * kLM; i += blockDim.x) s_fact[i] = fact[i];
+  __syncthreads();
+  const double pi = acos(-1.0);
+  const double prefact = (2.0 * pi) / (3.0 * volume);
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nt;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const double px = tx[t], py = ty[t], pz = tz[t];
+    const double R0 = px - cx, R1 = py - cy, R2 = pz - cz;
+    double s[3];
+    cart2sph(R0, R1, R2, s);
+    double2 OR[kLenM];
+    for (int l = 0; l <= kLM; ++l)
+      for (int m = 0; m <= l; ++m) OR[tblinv(l, m)] = omultipole(l, m, s, s_fact);
+    double2 ms[3];
+    for (int l = 0; l <= 1; ++l)
+      for (int m = 0; m <= l; ++m) {  // L2L, :943-976 with max_l = 1
+        double2 acc = make_double2(0.0, 0.0);
+        for (int j = l; j <= kLM; ++j)
+          for (int k = -j; k <= j; ++k) {
+            const int a = j - l, b = k - m;
+            double2 o = make_double2(0.0, 0.0);
+            if (abs(b) <= a) {
+              o = OR[tblinv(a, abs(b))];
+              if (b < 0) {
+                const double sg = (b & 1) ? -1.0 : 1.0;
+                o = make_double2(sg * o.x, -sg * o.y);
+              }
+            }
+            acc = cadd(acc, cmul(o, tbl(s_mu, j, k, kLM)));
+          }
+        ms[tblinv(l, m)] = acc;
+      }
+    double e0 = -ms[2].x, e1 = -ms[2].y, e2 = -ms[1].x, ph = ms[0].x;
+    if (corr == 1) {
+      e0 = e0 + (2.0 * prefact) * s_aux[0];
+      e1 = e1 + (2.0 * prefact) * s_aux[1];
+      e2 = e2 + (2.0 * prefact) * s_aux[2];
+      double rd = (R0 * s_aux[0] + R1 * s_aux[1]) + R2 * s_aux[2];
+      ph = (ph - (2.0 * prefact) * rd) + prefact * s_aux[3];
+    } else if (corr == 2) {
+      const int nf = (int)s_aux[4];
+      for (int p = 0; p < nf; ++p) {
+        const double fx = s_aux[8 + 4 * p], fy = s_aux[9 + 4 * p], fz = s_aux[10 + 4 * p];
+        const double fq = s_aux[11 + 4 * p];
+        for (int ib = 0; ib < nbox; ++ib) {
+          const double d0 = (px - s_vb[3 * ib]) - fx, d1 = (py - s_vb[3 * ib + 1]) - fy,
+                       d2 = (pz - s_vb[3 * ib + 2]) - fz;
+          double gx, gy, gz, gp;
+          force_leaf64(fq, d0, d1, d2, (d0 * d0 + d1 * d1) + d2 * d2, gx, gy, gz, gp);
+          e0 = e0 + gx;
+          e1 = e1 + gy;
+          e2 = e2 + gz;
+          ph = ph + gp;
+        }
+      }
+    }
+    if (overwrite) {
+      ex[t] = e0; ey[t] = e1; ez[t] = e2; pot[t] = ph;
+    } else {
+      ex[t] += e0; ey[t] += e1; ez[t] += e2; pot[t] += ph;
+    }
+  }
+}
+
+double host_factorial(int n) {  // factorial, :1247-1314 (the exact values to 24!, gamma above)
+  static const double f[25] = {1.0, 1.0, 2.0, 6.0, 24.0, 120.0, 720.0, 5040.0, 40320.0,
+                               362880.0, 3628800.0, 39916800.0, 479001600.0, 6227020800.0,
+                               87178291200.0, 1307674368000.0, 20922789888000.0,
+                               355687428096000.0, 6402373705728000.0, 121645100408832000.0,
+                               2432902008176640000.0, 51090942171709440000.0,
+                               1124000727777607680000.0, 25852016738884976640000.0,
+                               620448401733239439360000.0};
+  if (n <= 24) return f[n];
+  return std::tgamma((double)(n + 1));
+}
+
+bool unit_cube(const pepcg_params& p) {  // system_is_unit_cube, module_mirror_boxes.f90:248-255
+  auto nsq = [](const double* v) { return (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]; };
+  bool axes = p.t_lattice_1[0] > 0 && p.t_lattice_1[1] == 0 && p.t_lattice_1[2] == 0 &&
+              p.t_lattice_2[0] == 0 && p.t_lattice_2[1] > 0 && p.t_lattice_2[2] == 0 &&
+              p.t_lattice_3[0] == 0 && p.t_lattice_3[1] == 0 && p.t_lattice_3[2] > 0;
+  return axes && nsq(p.t_lattice_1) == 1.0 && nsq(p.t_lattice_2) == 1.0 && nsq(p.t_lattice_3) == 1.0;
+}
+
+}  // namespace
+
+int lattice_prepare(Ctx* c) {
+  const pepcg_params& p = c->prm;
+  cudaStream_t s = c->stream;
+  const int lm = unit_cube(p) ? kLMTable : kLM;
+  const int lt = 2 * lm;
+  const int lenm = lm * (lm + 1) / 2 + lm + 1, lent = lt * (lt + 1) / 2 + lt + 1;
+  const int nb = c->nboxes, ws = p.mirror_box_layers;
+  // factorials (exact to 24!, gamma above, as the reference) and (2 ws + 1)**(l + 1)
+  std::vector<double> hf(2 * lt + 2), hs(lt + 1);
+  for (int i = 0; i < (int)hf.size(); ++i) hf[i] = host_factorial(i);
+  for (int l = 0; l <= lt; ++l) hs[l] = std::pow((double)(2 * ws + 1), (double)(l + 1));
+  double2 *mstar = nullptr, *lstar = nullptr, *ml0 = nullptr, *ml1 = nullptr;
+  double *scratch = nullptr, *d_scp = nullptr;
+  const int64_t cnt = (int64_t)nb * (nb - 1);
+  const size_t scratch_n = (size_t)lent * 2 * (cnt > nb ? cnt : nb);
+  bool ok = cuda_ok(c, cudaMalloc((void**)&c->d_factorial, hf.size() * 8), "fmm") &&
+            cuda_ok(c, cudaMalloc((void**)&c->d_mlattice, kLenT * 16), "fmm") &&
+            cuda_ok(c, cudaMalloc((void**)&c->d_omega, kLenM * 16), "fmm") &&
+            cuda_ok(c, cudaMalloc((void**)&c->d_mu, kLenT * 16), "fmm") &&
+            cuda_ok(c, cudaMalloc((void**)&c->d_fmm_aux, 64 * 8), "fmm") &&
+            cuda_ok(c, cudaMalloc((void**)&mstar, lenm * 16), "fmm") &&
+            cuda_ok(c, cudaMalloc((void**)&lstar, lent * 16), "fmm") &&
+            cuda_ok(c, cudaMalloc((void**)&ml0, lent * 16), "fmm") &&
+            cuda_ok(c, cudaMalloc((void**)&ml1, lent * 16), "fmm") &&
+            cuda_ok(c, cudaMalloc((void**)&d_scp, (lt + 1) * 8), "fmm") &&
+            cuda_ok(c, cudaMalloc((void**)&scratch, scratch_n * 8), "fmm scratch");
+  if (ok) {
+    cudaMemcpyAsync(c->d_factorial, hf.data(), hf.size() * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_scp, hs.data(), hs.size() * 8, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(c->d_fmm_aux, 0, 64 * 8, s);
+    k_mstar<<<(lenm + 63) / 64, 64, 0, s>>>(lm, nb, c->d_vbox, c->d_factorial, scratch, mstar);
+    k_lstar<<<(lent + 63) / 64, 64, 0, s>>>(lt, nb, ws, c->d_vbox, c->d_factorial, scratch, lstar);
+    cudaMemcpyAsync(ml0, lstar, lent * 16, cudaMemcpyDeviceToDevice, s);
+    for (int it = 0; it < kMaxIter; ++it) {
+      k_lattice_iter<<<(lent + 127) / 128, 128, 0, s>>>(lt, lm, ml0, mstar, lstar, d_scp, ml1);
+      std::swap(ml0, ml1);
+    }
+    k_truncate<<<(kLenT + 127) / 128, 128, 0, s>>>(ml0, c->d_mlattice);
+    ok = cuda_ok(c, cudaGetLastError(), "lattice coefficients") &&
+         cuda_ok(c, cudaStreamSynchronize(s), "lattice coefficients");
+  }
+  for (void* q : {(void*)mstar, (void*)lstar, (void*)ml0, (void*)ml1, (void*)scratch, (void*)d_scp})
+    if (q) cudaFree(q);
+  return ok ? PEPCG_OK : PEPCG_ERR_CUDA;
+}
+
+int lattice_timestep(Ctx* c) {
+  const pepcg_params& p = c->prm;
+  cudaStream_t s = c->stream;
+  const double cx = 0.5 * ((p.t_lattice_1[0] + p.t_lattice_2[0]) + p.t_lattice_3[0]) + p.lattice_origin[0];
+  const double cy = 0.5 * ((p.t_lattice_1[1] + p.t_lattice_2[1]) + p.t_lattice_3[1]) + p.lattice_origin[1];
+  const double cz = 0.5 * ((p.t_lattice_1[2] + p.t_lattice_2[2]) + p.t_lattice_3[2]) + p.lattice_origin[2];
+  const int64_t n = c->n;
+  const int nbp = 148;
+  const int64_t nom = (n + kOmChunk - 1) / kOmChunk;
+  double* part = nullptr;
+  double2* opart = nullptr;
+  double* d_lat = nullptr;
+  bool ok = cuda_ok(c, cudaMallocAsync((void**)&part, 4 * nbp * 8, s), "fmm") &&
+            cuda_ok(c, cudaMallocAsync((void**)&opart, nom * kLenM * 16, s), "fmm") &&
+            cuda_ok(c, cudaMallocAsync((void**)&d_lat, 12 * 8, s), "fmm");
+  if (!ok) return PEPCG_ERR_OOM;
+  double lat[12];
+  for (int d = 0; d < 3; ++d) {
+    lat[d] = p.t_lattice_1[d];
+    lat[3 + d] = p.t_lattice_2[d];
+    lat[6 + d] = p.t_lattice_3[d];
+    lat[9 + d] = p.lattice_origin[d];
+  }
+  cudaMemcpyAsync(d_lat, lat, 12 * 8, cudaMemcpyHostToDevice, s);
+  cudaMemsetAsync(c->d_status, 0, 4, s);
+  k_box_dipole<<<nbp, 256, 0, s>>>(n, c->x.p, c->y.p, c->z.p, c->q.p, cx, cy, cz, part);
+  k_fict<<<1, 32, 0, s>>>(nbp, part, c->d_fmm_aux, p.periodicity[0], p.periodicity[1],
+                         p.periodicity[2], d_lat, d_lat + 9, p.fmm_extrinsic_correction);
+  k_omega_partial<<<(unsigned)nom, 256, 0, s>>>(n, c->x.p, c->y.p, c->z.p, c->q.p, cx, cy, cz,
+                                                c->d_factorial, opart);
+  k_omega_final<<<1, 256, 0, s>>>((int)nom, opart, c->d_fmm_aux, cx, cy, cz, c->d_factorial,
+                                  c->d_omega, c->d_status);
+  k_mu_cent<<<(kLenT + 127) / 128, 128, 0, s>>>(c->d_mlattice, c->d_omega, c->d_mu);
+  uint32_t st = 0;
+  ok = cuda_ok(c, cudaGetLastError(), "lattice timestep") &&
+       cuda_ok(c, cudaMemcpyAsync(&st, c->d_status, 4, cudaMemcpyDeviceToHost, s), "status");
+  cudaFreeAsync(part, s);
+  cudaFreeAsync(opart, s);
+  cudaFreeAsync(d_lat, s);
+  ok = ok && cuda_ok(c, cudaStreamSynchronize(s), "lattice timestep");
+  if (!ok) return PEPCG_ERR_CUDA;
+  return st ? status_to_code(c, st) : PEPCG_OK;
+}
+
+int lattice_add(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
+                double* ex, double* ey, double* ez, double* pot, bool overwrite) {
+  const pepcg_params& p = c->prm;
+  cudaStream_t s = c->stream;
+  const double cx = 0.5 * ((p.t_lattice_1[0] + p.t_lattice_2[0]) + p.t_lattice_3[0]) + p.lattice_origin[0];
+  const double cy = 0.5 * ((p.t_lattice_1[1] + p.t_lattice_2[1]) + p.t_lattice_3[1]) + p.lattice_origin[1];
+  const double cz = 0.5 * ((p.t_lattice_1[2] + p.t_lattice_2[2]) + p.t_lattice_3[2]) + p.lattice_origin[2];
+  const double* a = p.t_lattice_1;
+  const double* b = p.t_lattice_2;
+  const double* cc = p.t_lattice_3;
+  double cr[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+  const double volume = std::fabs((cr[0] * cc[0] + cr[1] * cc[1]) + cr[2] * cc[2]);
+  unsigned blocks = (unsigned)((nt + 127) / 128);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_lattice_force<<<blocks, 128, 0, s>>>(nt, tx, ty, tz, c->d_mu, c->d_fmm_aux, c->d_vbox, c->nboxes,
+                                         cx, cy, cz, volume, p.fmm_extrinsic_correction,
+                                         c->d_factorial, ex, ey, ez, pot, overwrite ? 1 : 0);
+  return cuda_ok(c, cudaGetLastError(), "lattice force") ? PEPCG_OK : PEPCG_ERR_CUDA;
+}
+
+}  // namespace pepcg

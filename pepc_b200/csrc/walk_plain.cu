@@ -1,0 +1,354 @@
+// walk_plain.cu -- FP64 tree walks (the drop-in "plain" form) and the
+// traversal orchestration of pepc_traverse_tree.
+//
+// Two semantics, both exact:
+//  * per target (module_tree_walk_pthreads.f90:558-765): every target keeps
+//    its own next-node index in the RPO node order; a warp of 32 key-ordered
+//    targets processes, at each step, the smallest next index among its lanes
+//    (all lanes that wait for that node evaluate it together, the node data is
+//    loaded once).  Each lane sees exactly its own LIFO sequence, so its
+//    interaction list, order and counts equal the reference's.
+//  * per tile (module_tree_walk_simple.f90:256-384): a warp holds one tile of
+//    <= 32 targets; a twig is opened if any target fails the MAC, children are
+//    visited first to last (key order) through the fwd pointers.
+// Compiled with --fmad=false: results are bit-identical to the oracle.
+
+#include "internal.cuh"
+
+namespace pepcg {
+
+__device__ unsigned int g_bucket_counter;
+
+namespace {
+
+constexpr int kWalkThreads = 128;
+
+struct WalkArgs {
+  int64_t nt;
+  const double* tx;
+  const double* ty;
+  const double* tz;
+  const double4* nc4;
+  const int2* meta;
+  const int2* fwd;
+  const double* mom;
+  const int32_t* nleaves;
+  const double* bl2;   // boxlength2[0..20]
+  const double* vbox;  // 3 * nbox
+  int nbox;
+  double theta2, eps2;
+  int32_t M;
+  int64_t npart;
+  double* ex;
+  double* ey;
+  double* ez;
+  double* pot;
+  double* work;
+  unsigned long long* counters;  // [0] leaf, [1] twig, [2] mac
+  uint32_t* status;
+  // per tile
+  const int2* tiles;  // (first target, count)
+  int64_t ntiles;
+};
+
+__device__ __forceinline__ void warp_add_counters(unsigned long long* ctr, unsigned long long a,
+                                                  unsigned long long b, unsigned long long c) {
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&ctr[0], a);
+    atomicAdd(&ctr[1], b);
+    atomicAdd(&ctr[2], c);
+  }
+}
+
+__global__ void __launch_bounds__(kWalkThreads) k_walk_target64(WalkArgs A) {
+  __shared__ double s_bl2[kMaxLevel + 1];
+  __shared__ double s_vb[3 * 125];
+  for (int i = threadIdx.x; i <= kMaxLevel; i += blockDim.x) s_bl2[i] = A.bl2[i];
+  for (int i = threadIdx.x; i < 3 * A.nbox; i += blockDim.x) s_vb[i] = A.vbox[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const unsigned M = (unsigned)A.M;
+  unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
+  for (;;) {
+    unsigned b = 0;
+    if (lane == 0) b = atomicAdd(&g_bucket_counter, 1u);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    if ((int64_t)b * 32 >= A.nt) break;
+    const int64_t t = (int64_t)b * 32 + lane;
+    const bool valid = t < A.nt;
+    double px = 0, py = 0, pz = 0, e0 = 0, e1 = 0, e2 = 0, ph = 0, w = 0;
+    if (valid) {
+      px = A.tx[t]; py = A.ty[t]; pz = A.tz[t];
+      e0 = A.ex[t]; e1 = A.ey[t]; e2 = A.ez[t]; ph = A.pot[t]; w = A.work[t];
+    }
+    bool complete = true;
+    for (int ib = 0; ib < A.nbox; ++ib) {
+      // shifted_particle_position = x - vbox (module_tree_walk_pthreads.f90:595)
+      const double sx = px - s_vb[3 * ib], sy = py - s_vb[3 * ib + 1], sz = pz - s_vb[3 * ib + 2];
+      // the root is never evaluated: the walk starts with its children (:601)
+      unsigned next = valid ? 1u : M;
+      int64_t partner = 0;
+      for (;;) {
+        const unsigned u = __reduce_min_sync(0xffffffffu, next);
+        if (u >= M) break;
+        if (next != u) continue;
+        const double4 a = A.nc4[u];
+        const int2 mu = A.meta[u];
+        const double dx = sx - a.x, dy = sy - a.y, dz = sz - a.z;
+        const double dist2 = (dx * dx + dy * dy) + dz * dz;
+        if (mu.y & kLeafFlag) {
+          partner += 1;
+          w += 1.0;
+          ++c_leaf;
+          if (dist2 > 0.0) {
+            double fx, fy, fz, fp;
+            force_leaf64(a.w, dx, dy, dz, dist2 + A.eps2, fx, fy, fz, fp);
+            e0 += fx; e1 += fy; e2 += fz; ph += fp;
+          }
+          next = u + 1;
+        } else {
+          ++c_mac;
+          if (A.theta2 * dist2 > s_bl2[mu.y & 0xff]) {
+            partner += A.nleaves[u];
+            double m[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) m[k] = A.mom[9 * (int64_t)u + k];
+            double fx, fy, fz, fp;
+            force_twig64(a.w, m, dx, dy, dz, dist2 + A.eps2, fx, fy, fz, fp);
+            e0 += fx; e1 += fy; e2 += fz; ph += fp;
+            ++c_twig;
+            w += 1.0;
+            next = (unsigned)mu.x;
+          } else {
+            next = u + 1;
+          }
+        }
+      }
+      if (valid && partner != A.npart) complete = false;
+    }
+    if (valid) {
+      A.ex[t] = e0; A.ey[t] = e1; A.ez[t] = e2; A.pot[t] = ph; A.work[t] = w;
+    }
+    if (__any_sync(0xffffffffu, !complete) && lane == 0) atomicOr(A.status, ST_INCOMPLETE);
+  }
+  warp_add_counters(A.counters, c_leaf, c_twig, c_mac);
+}
+
+__global__ void __launch_bounds__(kWalkThreads) k_walk_tile64(WalkArgs A) {
+  __shared__ double s_bl2[kMaxLevel + 1];
+  __shared__ double s_vb[3 * 125];
+  for (int i = threadIdx.x; i <= kMaxLevel; i += blockDim.x) s_bl2[i] = A.bl2[i];
+  for (int i = threadIdx.x; i < 3 * A.nbox; i += blockDim.x) s_vb[i] = A.vbox[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const unsigned M = (unsigned)A.M;
+  unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
+  for (;;) {
+    unsigned b = 0;
+    if (lane == 0) b = atomicAdd(&g_bucket_counter, 1u);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    if ((int64_t)b >= A.ntiles) break;
+    const int2 tl = A.tiles[b];
+    const bool valid = lane < tl.y;
+    const int64_t t = (int64_t)tl.x + lane;
+    double px = 0, py = 0, pz = 0, e0 = 0, e1 = 0, e2 = 0, ph = 0, w = 0;
+    if (valid) {
+      px = A.tx[t]; py = A.ty[t]; pz = A.tz[t];
+      e0 = A.ex[t]; e1 = A.ey[t]; e2 = A.ez[t]; ph = A.pot[t]; w = A.work[t];
+    }
+    bool complete = true;
+    for (int ib = 0; ib < A.nbox; ++ib) {
+      const double vx = s_vb[3 * ib], vy = s_vb[3 * ib + 1], vz = s_vb[3 * ib + 2];
+      unsigned u = 0;  // tree_walk_single_aux starts at the root (:286)
+      int64_t partner = 0;
+      while (u < M) {
+        const double4 a = A.nc4[u];
+        const int2 mu = A.meta[u];
+        const int2 fw = A.fwd[u];
+        // d = (x - vbox) - coc (module_tree_walk_simple.f90:328,345)
+        const double dx = (px - vx) - a.x, dy = (py - vy) - a.y, dz = (pz - vz) - a.z;
+        const double dist2 = (dx * dx + dy * dy) + dz * dz;
+        if (mu.y & kLeafFlag) {
+          partner += 1;
+          if (valid) {
+            w += 1.0;
+            ++c_leaf;
+            if (dist2 > 0.0) {
+              double fx, fy, fz, fp;
+              force_leaf64(a.w, dx, dy, dz, dist2 + A.eps2, fx, fy, fz, fp);
+              e0 += fx; e1 += fy; e2 += fz; ph += fp;
+            }
+          }
+          u = (unsigned)fw.y;
+        } else {
+          const bool ok = !valid || (A.theta2 * dist2 > s_bl2[mu.y & 0xff]);
+          const unsigned fail = __ballot_sync(0xffffffffu, !ok);
+          // MAC evaluations stop at the first failing target (:343-370)
+          const int first_fail = fail ? __ffs(fail) - 1 : 32;
+          if (valid && lane <= first_fail) ++c_mac;
+          if (fail == 0) {
+            partner += A.nleaves[u];
+            if (valid) {
+              double m[9];
+#pragma unroll
+              for (int k = 0; k < 9; ++k) m[k] = A.mom[9 * (int64_t)u + k];
+              double fx, fy, fz, fp;
+              force_twig64(a.w, m, dx, dy, dz, dist2 + A.eps2, fx, fy, fz, fp);
+              e0 += fx; e1 += fy; e2 += fz; ph += fp;
+              w += 1.0;
+              ++c_twig;
+            }
+            u = (unsigned)fw.y;
+          } else {
+            u = (unsigned)fw.x;
+          }
+        }
+      }
+      if (partner != A.npart) complete = false;
+    }
+    if (valid) {
+      A.ex[t] = e0; A.ey[t] = e1; A.ez[t] = e2; A.pot[t] = ph; A.work[t] = w;
+    }
+    if (!complete && lane == 0) atomicOr(A.status, ST_INCOMPLETE);
+  }
+  warp_add_counters(A.counters, c_leaf, c_twig, c_mac);
+}
+
+// Tiles of the grown particles: tree nodes with <= T leaves whose parent has
+// more than T (the key-prefix split of tree_walk_init_aux,
+// module_tree_walk_simple.f90:168-211, is exactly this set of nodes).
+__global__ void k_tiles_from_tree(int32_t M, int T, const int32_t* __restrict__ nleaves,
+                                  const int32_t* __restrict__ parent,
+                                  const int32_t* __restrict__ first_part, int2* tiles,
+                                  unsigned int* ntiles) {
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < M;
+       u += (int64_t)gridDim.x * blockDim.x) {
+    int lv = nleaves[u];
+    int p = parent[u];
+    if (lv <= T && (p < 0 || nleaves[p] > T)) {
+      unsigned slot = atomicAdd(ntiles, 1u);
+      tiles[slot] = make_int2(first_part[u], lv);
+    }
+  }
+}
+
+__global__ void k_same_keys(int64_t n, const int64_t* __restrict__ a, const int64_t* __restrict__ b,
+                            unsigned int* differ) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    if (a[i] != b[i]) atomicOr(differ, 1u);
+}
+
+__global__ void k_reset_counter() { g_bucket_counter = 0; }
+
+}  // namespace
+
+int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
+                    const int64_t* tkeys, bool self, double* ex, double* ey, double* ez,
+                    double* pot, double* work) {
+  if (!c->has_tree) {
+    c->err = "traverse called without a grown tree";
+    return PEPCG_ERR_NO_TREE;
+  }
+  if (nt <= 0) return PEPCG_OK;
+  cudaStream_t s = c->stream;
+  const int walk = c->prm.walk;
+  if (!cuda_ok(c, cudaMemsetAsync(c->counters.p, 0, 4 * sizeof(unsigned long long), s), "ctr") ||
+      !cuda_ok(c, cudaMemsetAsync(c->d_status, 0, 4, s), "status"))
+    return PEPCG_ERR_CUDA;
+  int64_t ntiles = 0;
+  if (walk == PEPCG_WALK_PER_TILE) {
+    const int T = c->prm.tile_size < 1 ? 1 : (c->prm.tile_size > 32 ? 32 : c->prm.tile_size);
+    bool from_tree = self;
+    if (!self && tkeys && nt == c->n) {
+      unsigned int* d_diff = reinterpret_cast<unsigned int*>(c->d_small + 4);
+      unsigned int h_diff = 1;
+      cudaMemsetAsync(d_diff, 0, 4, s);
+      k_same_keys<<<296, 256, 0, s>>>(nt, tkeys, c->key.p, d_diff);
+      if (!cuda_ok(c, cudaMemcpyAsync(&h_diff, d_diff, 4, cudaMemcpyDeviceToHost, s), "tiles") ||
+          !cuda_ok(c, cudaStreamSynchronize(s), "tiles"))
+        return PEPCG_ERR_CUDA;
+      from_tree = (h_diff == 0);
+    }
+    if (!ensure(c, c->tiles, 2 * (nt + 1), "tiles")) return PEPCG_ERR_OOM;
+    int2* d_tiles = reinterpret_cast<int2*>(c->tiles.p);
+    if (from_tree) {
+      unsigned int* d_nt = reinterpret_cast<unsigned int*>(c->d_small + 5);
+      unsigned int h_nt = 0;
+      cudaMemsetAsync(d_nt, 0, 4, s);
+      k_tiles_from_tree<<<296, 256, 0, s>>>((int32_t)c->nnodes, T, c->nleaves_ptr(), c->parent.p,
+                                            c->first_part.p, d_tiles, d_nt);
+      if (!cuda_ok(c, cudaMemcpyAsync(&h_nt, d_nt, 4, cudaMemcpyDeviceToHost, s), "tiles") ||
+          !cuda_ok(c, cudaStreamSynchronize(s), "tiles"))
+        return PEPCG_ERR_CUDA;
+      ntiles = h_nt;
+    } else {
+      int rc = host_tiles(c, nt, tkeys, T, d_tiles, &ntiles);
+      if (rc) return rc;
+    }
+  }
+  cudaEventRecord(c->ev[5], s);
+  WalkArgs A;
+  A.nt = nt;
+  A.tx = tx; A.ty = ty; A.tz = tz;
+  A.nc4 = c->nc4.p;
+  A.meta = c->meta.p;
+  A.fwd = c->fwd.p;
+  A.mom = c->mom.p;
+  A.nleaves = c->nleaves_ptr();
+  A.bl2 = c->d_box + 9;
+  A.vbox = c->d_vbox;
+  A.nbox = c->nboxes;
+  A.theta2 = c->prm.theta2;
+  A.eps2 = c->prm.eps2;
+  A.M = (int32_t)c->nnodes;
+  A.npart = c->n;
+  A.ex = ex; A.ey = ey; A.ez = ez; A.pot = pot; A.work = work;
+  A.counters = c->counters.p;
+  A.status = c->d_status;
+  A.tiles = reinterpret_cast<const int2*>(c->tiles.p);
+  A.ntiles = ntiles;
+  k_reset_counter<<<1, 1, 0, s>>>();
+  const int blocks = 148 * 8;
+  if (c->prm.precision == PEPCG_PRECISION_PLAIN) {
+    if (walk == PEPCG_WALK_PER_TARGET || walk == PEPCG_WALK_GROUP)
+      k_walk_target64<<<blocks, kWalkThreads, 0, s>>>(A);
+    else
+      k_walk_tile64<<<blocks, kWalkThreads, 0, s>>>(A);
+  } else {
+    c->err = "mixed precision walk not built yet";
+    return PEPCG_ERR_UNSUPPORTED;
+  }
+  if (!cuda_ok(c, cudaGetLastError(), "walk launch")) return PEPCG_ERR_CUDA;
+  cudaEventRecord(c->ev[6], s);
+  if (c->far_field) {
+    int rc = lattice_add(c, nt, tx, ty, tz, ex, ey, ez, pot, false);
+    if (rc) return rc;
+  }
+  cudaEventRecord(c->ev[7], s);
+  unsigned long long ctr[4];
+  uint32_t st = 0;
+  if (!cuda_ok(c, cudaMemcpyAsync(ctr, c->counters.p, 4 * sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, s), "counters") ||
+      !cuda_ok(c, cudaMemcpyAsync(&st, c->d_status, 4, cudaMemcpyDeviceToHost, s), "status") ||
+      !cuda_ok(c, cudaStreamSynchronize(s), "walk"))
+    return PEPCG_ERR_CUDA;
+  c->st.leaf_interactions = (int64_t)ctr[0];
+  c->st.twig_interactions = (int64_t)ctr[1];
+  c->st.interactions = (int64_t)(ctr[0] + ctr[1]);
+  c->st.mac_evaluations = (int64_t)ctr[2];
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev[5], c->ev[6]);
+  c->st.t_walk_ms = ms;
+  cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]);
+  c->st.t_lattice_ms = ms;
+  if (st) return status_to_code(c, st);
+  return PEPCG_OK;
+}
+
+}  // namespace pepcg
