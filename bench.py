@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Headline benchmark: particle force evaluations per second of the tree code
+(grow + traverse) on a clustered 4M-particle Plummer sphere.
+
+Workload (the 4M clustered-gravity configuration): N = 4,194,304 equal charges
+q = +1/N (gravity differs only by the sign of E), Plummer sphere with scale
+radius 1 truncated at r = 20, seeded (numpy PCG64, seed 3), eps = 1e-3,
+theta = 0.4, quadrupole, Hilbert keys, open boundaries.  Synthetic data.
+
+One step = clear the results, grow the tree (bounding box, keys, sort, tree,
+multipoles) and evaluate E and phi on every particle (the traversal), with the
+particles already in HBM.  The timed form is the mixed-precision group walk;
+the plain FP64 per-target walk (the drop-in form) is timed beside it.
+
+Prints one JSON line (rank 0).  --impl reference times the CPU restatement
+of the reference algorithm (the oracle) on the host cores instead.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle force evals/s at 4M, mixed vs FP64 GPU walk, at ≤1e-4 median force err"
+UNIT = "force evals/s"
+FLOPS_TWIG = 144  # counted from coulomb/module_coulomb_kernels.f90:60-145 + delta, dist2, MAC, sums
+FLOPS_LEAF = 22   # counted from module_coulomb_kernels.f90:242-257 + delta, dist2, sums
+SMS = 148
+
+
+def plummer(n, seed=3, rmax=20.0):
+    """Plummer sphere, a = 1: r = (u^(-2/3) - 1)^(-1/2), resampled above rmax."""
+    rng = np.random.default_rng(seed)
+    r = np.empty(0)
+    while r.size < n:
+        u = rng.random(2 * n)
+        with np.errstate(divide="ignore"):
+            rr = 1.0 / np.sqrt(u ** (-2.0 / 3.0) - 1.0)
+        r = np.concatenate([r, rr[np.isfinite(rr) & (rr <= rmax)]])
+    r = r[:n]
+    v = rng.standard_normal((n, 3))
+    v /= np.linalg.norm(v, axis=1)[:, None]
+    p = v * r[:, None]
+    return (np.ascontiguousarray(p[:, 0]), np.ascontiguousarray(p[:, 1]),
+            np.ascontiguousarray(p[:, 2]), np.full(n, 1.0 / n))
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (200 ms period)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([s.strip() for s in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            for k, nm in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(x, y, z, q, theta2, eps2, sample, threads, seed=11):
+    """The oracle (CPU restatement of the reference path) on the host cores:
+    grow of all N, traverse of a random sample of targets, scaled to N."""
+    from oracle import oracle as O
+    n = len(x)
+    orc = O.Oracle(theta2=theta2, eps2=eps2, walk=0, num_threads=threads)
+    t0 = time.perf_counter()
+    g = orc.grow_tree(x, y, z, q)
+    t1 = time.perf_counter()
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(n, min(sample, n), replace=False))
+    orc.traverse_tree(g["x"][idx], g["y"][idx], g["z"][idx])
+    t2 = time.perf_counter()
+    orc.close()
+    t_full = (t1 - t0) + (t2 - t1) * n / len(idx)
+    return {"value": n / t_full, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"grow of all {n} particles ({t1 - t0:.2f} s) + per-target walk of "
+                      f"{len(idx)} random targets ({t2 - t1:.2f} s), scaled to {n} targets",
+            "t_grow_s": t1 - t0, "t_walk_sample_s": t2 - t1}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    x, y, z, q = plummer(args.n)
+    threads = os.cpu_count() or 1
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(x, y, z, q, args.theta ** 2, args.eps ** 2, args.cpu_sample, threads,
+                          seed=100 + i)
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": args.n / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": workload_name(args), "implementation":
+                       "CPU restatement of the reference tree code (oracle, per-target walk), "
+                       "all host threads; the reference itself needs gfortran + MPI, absent here"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_name(args):
+    return (f"Plummer sphere N={args.n} (a=1, r<=20, q=1/N), theta={args.theta}, "
+            f"eps={args.eps}, quadrupole, Hilbert keys, open boundaries")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=4194304)
+    ap.add_argument("--theta", type=float, default=0.4)
+    ap.add_argument("--eps", type=float, default=1e-3)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "plain"])
+    ap.add_argument("--walk", default="group", choices=["group", "target", "tile"])
+    ap.add_argument("--ntest", type=int, default=8192)
+    ap.add_argument("--cpu-sample", type=int, default=32768)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    assert args.warmup >= 3, "at least 3 warm-up steps"
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import pepc_b200 as P
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    x, y, z, q = plummer(args.n)
+    n = args.n
+    dev = torch.device("cuda", local)
+    tx, ty, tz, tq = (torch.from_numpy(a).to(dev) for a in (x, y, z, q))
+    out = [torch.zeros(n, dtype=torch.float64, device=dev) for _ in range(5)]
+    stream = torch.cuda.current_stream()
+    walk = {"group": P.WALK_GROUP, "target": P.WALK_PER_TARGET, "tile": P.WALK_PER_TILE}[args.walk]
+    prec = P.PRECISION_MIXED if args.precision == "mixed" else P.PRECISION_PLAIN
+    tc = P.TreeCode(theta2=args.theta ** 2, eps2=args.eps ** 2, precision=prec, walk=walk,
+                    device=local)
+    tc.set_stream(stream.cuda_stream)
+
+    def step(t):
+        for o in out:
+            o.zero_()
+        t.grow_tree_device(tx, ty, tz, tq)
+        t.traverse_self_device(*out)
+
+    def timed(t, steps, warmup, clocks=None):
+        for _ in range(warmup):
+            step(t)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = P.kernel_launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ctx = Clocks(local) if clocks else None
+        if ctx:
+            ctx.__enter__()
+        e0.record(stream)
+        for _ in range(steps):
+            step(t)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if ctx:
+            ctx.__exit__()
+        if dist:
+            dist.barrier()
+        ms = e0.elapsed_time(e1) / steps
+        launches = (P.kernel_launches() - l0)
+        if dist:
+            tt = torch.tensor([ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+        return ms, launches, (ctx.summary() if ctx else None)
+
+    ms, launches, clk = timed(tc, args.steps, args.warmup, clocks=True)
+    st = tc.stats()
+    value = n * world / (ms * 1e-3)
+
+    # accuracy of this step's result against an FP64 direct sum on sampled targets
+    rng = np.random.default_rng(33)
+    tidx = np.sort(rng.choice(n, args.ntest, replace=False))
+    E = torch.stack(out[:3]).cpu().numpy()[:, tidx]
+    d = tc.direct(tidx)
+    Ed = np.stack([d["ex"], d["ey"], d["ez"]])
+    rel = np.linalg.norm(E - Ed, axis=0) / np.linalg.norm(Ed, axis=0)
+    prel = np.abs(out[3].cpu().numpy()[tidx] - d["pot"]) / np.abs(d["pot"])
+
+    # roofline of the dominant kernel (the walk)
+    f_mhz = clk["sm_mhz"] if clk and clk["sm_mhz"] else 1965.0
+    lanes = 128 if prec == P.PRECISION_MIXED else 64  # FP32 / FP64 lanes per SM
+    peak = SMS * lanes * 2 * f_mhz * 1e6 / 1e12
+    flops = FLOPS_TWIG * st["twig_interactions"] + FLOPS_LEAF * st["leaf_interactions"]
+    achieved = flops / (st["t_walk_ms"] * 1e-3) / 1e12
+    roof = {"bound": "fp32-core" if prec == P.PRECISION_MIXED else "fp64-core",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": None,
+            "kernel": "walk", "kernel_ms": st["t_walk_ms"],
+            "peak_source": f"{SMS} SMs x {lanes} lanes x 2 flop/FMA x median SM clock under load "
+                           f"({f_mhz:.0f} MHz); no measured CUDA-core peak in MEASURED_PEAKS.json",
+            "flops_per_launch": flops,
+            "interactions": {"twig": st["twig_interactions"], "leaf": st["leaf_interactions"]}}
+    phases = {k: st[k] for k in ("t_keys_ms", "t_sort_ms", "t_tree_ms", "t_upward_ms",
+                                 "t_walk_ms", "t_lattice_ms")}
+
+    # the plain FP64 drop-in form (per-target walk) on the same input
+    plain = None
+    if not args.no_plain:
+        tp = P.TreeCode(theta2=args.theta ** 2, eps2=args.eps ** 2, precision=P.PRECISION_PLAIN,
+                        walk=P.WALK_PER_TARGET, device=local)
+        tp.set_stream(stream.cuda_stream)
+        pms, _, _ = timed(tp, max(1, min(args.steps, 3)), 3)
+        pst = tp.stats()
+        Ep = torch.stack(out[:3]).cpu().numpy()[:, tidx]
+        prel_p = np.linalg.norm(Ep - Ed, axis=0) / np.linalg.norm(Ed, axis=0)
+        pflops = FLOPS_TWIG * pst["twig_interactions"] + FLOPS_LEAF * pst["leaf_interactions"]
+        plain = {"value": n * world / (pms * 1e-3), "ms_per_step": pms,
+                 "walk_ms": pst["t_walk_ms"], "interactions": pst["interactions"],
+                 "walk_tflops": pflops / (pst["t_walk_ms"] * 1e-3) / 1e12,
+                 "force_err_median": float(np.median(prel_p)),
+                 "force_err_p99": float(np.percentile(prel_p, 99))}
+        tp.close()
+
+    # end to end through the host API (pinned host buffers, copies inside the timed region)
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+        hx, hy, hz, hq = pin(x), pin(y), pin(z), pin(q)
+        hk = torch.zeros(n, dtype=torch.int64).pin_memory().numpy()
+        hp = torch.zeros(n, dtype=torch.int64).pin_memory().numpy()
+        hxo, hyo, hzo = (torch.zeros(n, dtype=torch.float64).pin_memory().numpy() for _ in range(3))
+        res = [torch.zeros(n, dtype=torch.float64).pin_memory().numpy() for _ in range(5)]
+        import ctypes as C
+        L = P.lib()
+        dp = lambda a: a.ctypes.data_as(P.D)  # noqa: E731
+        ipp = lambda a: a.ctypes.data_as(P.I64)  # noqa: E731
+
+        def host_step():
+            for r_ in res:
+                r_.fill(0.0)
+            tc._check(L.pepcg_grow_tree(tc._h, n, dp(hx), dp(hy), dp(hz), dp(hq), ipp(hk), ipp(hp),
+                                        dp(hxo), dp(hyo), dp(hzo)))
+            tc._check(L.pepcg_traverse_tree(tc._h, n, dp(hxo), dp(hyo), dp(hzo), ipp(hk),
+                                            *[dp(r_) for r_ in res]))
+
+        for _ in range(3):
+            host_step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ksteps = max(1, min(args.steps, 3))
+        e0.record(stream)
+        for _ in range(ksteps):
+            host_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1) / ksteps
+        if dist:
+            tt = torch.tensor([ems], device=dev, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ems = float(tt.item())
+        # grow: x y z q in; key, perm (int32), x y z out.  traverse: x y z, key,
+        # e(3) pot work in; e(3) pot work out
+        h2d = n * (4 * 8) + n * (3 * 8 + 8 + 5 * 8)
+        d2h = n * (8 + 4 + 3 * 8) + n * (5 * 8)
+        e2e = {"value": n * world / (ems * 1e-3), "unit": UNIT, "ms_per_step": ems,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "api": "pepcg_grow_tree + pepcg_traverse_tree (host arrays, pinned)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(x, y, z, q, args.theta ** 2, args.eps ** 2, args.cpu_sample,
+                           os.cpu_count() or 1)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 interactions + f64 offsets/sums" if prec == P.PRECISION_MIXED else "f64",
+        "data": "synthetic",
+        "config": {"workload": workload_name(args), "precision": args.precision,
+                   "walk": args.walk, "parallelism": "replicas only" if world > 1 else "single GPU",
+                   "l2": "inputs (128 MB) and tree (~0.7 GB) exceed the 126 MB L2; no flush",
+                   "step": "zero results + grow (box, keys, sort, tree, multipoles) + traverse"},
+        "force_err": {"median": float(np.median(rel)), "p99": float(np.percentile(rel, 99)),
+                      "pot_median": float(np.median(prel)), "ntest": args.ntest,
+                      "against": "FP64 direct sum (pepcg_direct)"},
+        "roofline": roof, "phases_ms": phases, "gpu_launches": launches,
+        "clocks": clk, "e2e": e2e, "plain": plain,
+        "mixed_over_plain": (value / plain["value"]) if plain else None,
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    tc.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

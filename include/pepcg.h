@@ -156,6 +156,15 @@ int pepcg_traverse_tree_device(void* ctx, int64_t nt, const double* d_tx, const 
 int pepcg_traverse_self_device(void* ctx, double* d_ex, double* d_ey, double* d_ez,
                                double* d_pot, double* d_work);
 
+/* Launch all of this context's work on the caller's CUDA stream (a
+ * cudaStream_t of the context's device), or on a private stream when NULL.
+ * Lets a caller that owns a stream (e.g. a framework's current stream) order
+ * and time the library's kernels with its own events.  No reference
+ * counterpart: the reference has no device streams. */
+int pepcg_set_stream(void* ctx, void* stream);
+/* Total number of kernels this library has launched in the process. */
+long long pepcg_kernel_launches(void);
+
 /* replaces pepc_timber_tree (module_pepc.f90:538 -> module_libpepc_main.f90:129-148) */
 int pepcg_timber_tree(void* ctx);
 int pepcg_stats_get(void* ctx, pepcg_stats* s);

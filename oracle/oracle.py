@@ -71,6 +71,8 @@ def lib():
         L.orc_lattice.argtypes = [C.c_void_p, C.c_int64, D, D, D, D, D, D, D]
         L.orc_lattice.restype = C.c_int
         L.orc_fmm_lattice_coefficients.argtypes = [C.POINTER(OrcParams), D]
+        L.orc_set_lattice_coefficients.argtypes = [C.c_void_p, D]
+        L.orc_set_lattice_coefficients.restype = C.c_int
         _LIB = L
     return _LIB
 
@@ -163,6 +165,15 @@ def par_rand(iseed, n):
     return out
 
 
+def reference_lattice_table(gold):
+    """The reference's pretabulated unit-cube MLattice (l <= 40) from the golden fixture."""
+    ml = np.zeros(861, dtype=np.complex128)
+    for l, m, v in zip(gold["lattice_l"], gold["lattice_m"], gold["lattice_v"]):
+        if l <= 40:
+            ml[l * (l + 1) // 2 + m] = v
+    return ml
+
+
 def lattice_coefficients(p):
     out = np.zeros(2 * 861)
     lib().orc_fmm_lattice_coefficients(C.byref(p), dp(out))
@@ -246,6 +257,12 @@ class Oracle:
         if rc != 0:
             raise RuntimeError(f"orc_direct failed: {rc}")
         return dict(ex=ex, ey=ey, ez=ez, pot=pt)
+
+    def set_lattice_coefficients(self, ml):
+        ml = np.asarray(ml, dtype=np.complex128)
+        buf = np.ascontiguousarray(np.stack([ml.real, ml.imag], axis=1).reshape(-1))
+        if lib().orc_set_lattice_coefficients(self.h, dp(buf)) != 0:
+            raise RuntimeError("not a periodic context")
 
     def lattice(self, x, y, z):
         n = len(x)

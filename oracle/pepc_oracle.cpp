@@ -372,6 +372,7 @@ void orc_fmm_destroy(OrcFmm* f);
 void orc_fmm_timestep(OrcFmm* f, int64_t n, const double* x, const double* y, const double* z,
                       const double* q);
 void orc_fmm_sum_lattice_force(const OrcFmm* f, const double pos[3], double e[3], double* phi);
+void orc_fmm_set_mlattice(OrcFmm* f, const double* re_im);
 
 // ---------------------------------------------------------------------------
 // Whole-path context
@@ -948,6 +949,15 @@ int orc_direct(orc_ctx* c, int64_t ntest, const int64_t* tidx, double* ex, doubl
     }
     ex[j] = e[0]; ey[j] = e[1]; ez[j] = e[2]; pot[j] = ph;
   });
+  return 0;
+}
+
+// Install lattice coefficients (861 complex, interleaved re/im), e.g. the
+// reference's pretabulated unit-cube table (load_lattice_coefficients,
+// module_fmm_framework.f90:260-508).  Must be called before grow.
+int orc_set_lattice_coefficients(orc_ctx* c, const double* re_im) {
+  if (!c->fmm) return -1;
+  orc_fmm_set_mlattice(c->fmm, re_im);
   return 0;
 }
 

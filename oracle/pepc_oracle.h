@@ -91,6 +91,8 @@ void orc_counters(const orc_ctx* c, int64_t out[2]);
  * mirror boxes and, if periodic with far field, the lattice term. */
 int orc_direct(orc_ctx* c, int64_t ntest, const int64_t* tidx, double* ex, double* ey,
                double* ez, double* pot);
+/* install lattice coefficients (861 complex as interleaved re, im) before grow */
+int orc_set_lattice_coefficients(orc_ctx* c, const double* re_im);
 /* periodic lattice term alone for arbitrary positions (fmm_sum_lattice_force) */
 int orc_lattice(orc_ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                 double* ex, double* ey, double* ez, double* pot);

@@ -382,6 +382,10 @@ void orc_fmm_sum_lattice_force(const OrcFmm* f, const double pos[3], double e[3]
   *phi = ph;
 }
 
+void orc_fmm_set_mlattice(OrcFmm* f, const double* re_im) {
+  for (int i = 0; i < kLenT; ++i) f->mlattice[i] = {re_im[2 * i], re_im[2 * i + 1]};
+}
+
 extern "C" {
 // Lattice coefficients (MLattice) for inspection: 861 complex values as
 // interleaved (re, im), layout tblinv(l, m).

@@ -111,6 +111,7 @@ EXPORTS = [
     "pepcg_traverse_self_device", "pepcg_timber_tree", "pepcg_stats_get", "pepcg_num_nodes",
     "pepcg_tree_export", "pepcg_direct", "pepcg_lattice", "pepcg_multipole_from_particle",
     "pepcg_shift_multipoles_up", "pepcg_force_with_leaf", "pepcg_force_with_twig", "pepcg_mac",
+    "pepcg_set_stream", "pepcg_kernel_launches",
 ]
 
 _LIB = None
@@ -139,6 +140,9 @@ def lib():
     L.pepcg_traverse_tree_device.argtypes = [VP, C.c_int64, VP, VP, VP, VP, VP, VP, VP, VP, VP]
     L.pepcg_traverse_self_device.argtypes = [VP, VP, VP, VP, VP, VP]
     L.pepcg_timber_tree.argtypes = [VP]
+    L.pepcg_set_stream.argtypes = [VP, VP]
+    L.pepcg_kernel_launches.argtypes = []
+    L.pepcg_kernel_launches.restype = C.c_longlong
     L.pepcg_stats_get.argtypes = [VP, C.POINTER(Stats)]
     L.pepcg_num_nodes.argtypes = [VP]
     L.pepcg_num_nodes.restype = C.c_int64
@@ -202,6 +206,7 @@ class TreeCode:
 
     def __init__(self, **params):
         self._h = C.c_void_p()
+        self.last_status = PEPCG_OK
         self.params = make_params(**params)
         rc = lib().pepcg_create(C.byref(self._h), C.byref(self.params))
         if rc != PEPCG_OK:
@@ -209,6 +214,7 @@ class TreeCode:
 
     # -- helpers
     def _check(self, rc, allow_warn=True):
+        self.last_status = rc
         if rc == PEPCG_OK or (allow_warn and rc == PEPCG_WARN_NOT_NEUTRAL):
             return rc
         raise PepcgError(rc, lib().pepcg_last_error(self._h).decode())
@@ -279,6 +285,10 @@ class TreeCode:
         return self._check(lib().pepcg_get_particles_device(
             self._h, _tptr(key), _tptr(perm), _tptr(x), _tptr(y), _tptr(z), _tptr(q)))
 
+    def set_stream(self, stream_ptr):
+        """Launch on an external cudaStream_t (int pointer), or a private stream for None."""
+        self._check(lib().pepcg_set_stream(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
     # -- diagnostics
     def stats(self):
         s = Stats()
@@ -346,6 +356,10 @@ def force_with_twig(node, delta, dist2, eps2):
     _chk(lib().pepcg_force_with_twig(_dp(_f64(node)), _dp(_f64(delta)), float(dist2), float(eps2),
                                      _dp(e), _dp(phi)))
     return e, phi[0]
+
+
+def kernel_launches():
+    return int(lib().pepcg_kernel_launches())
 
 
 def mac(theta2, dist2, boxlength2):

@@ -16,6 +16,7 @@
 namespace pepcg {
 
 static thread_local std::string g_static_err;
+std::atomic<long long> g_launches{0};
 
 bool cuda_ok(Ctx* c, cudaError_t e, const char* what) {
   if (e == cudaSuccess) return true;
@@ -289,6 +290,7 @@ int pepcg_create(void** out, const pepcg_params* p) {
     delete c;
     return PEPCG_ERR_CUDA;
   }
+  c->own_stream = true;
   for (int i = 0; i < 8; ++i) cudaEventCreate(&c->ev[i]);
   bool ok = cuda_ok(nullptr, cudaMalloc((void**)&c->d_box, 64 * sizeof(double)), "box") &&
             cuda_ok(nullptr, cudaMalloc((void**)&c->d_status, 16), "status") &&
@@ -342,7 +344,7 @@ int pepcg_destroy(void* ctx) {
     if (p) cudaFree(p);
   for (int i = 0; i < 8; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
-  if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
   delete c;
   return PEPCG_OK;
 }
@@ -509,6 +511,27 @@ int pepcg_traverse_tree(void* ctx, int64_t nt, const double* tx, const double* t
   ok = ok && cuda_ok(c, cudaStreamSynchronize(s), "traverse");
   return ok ? rc : PEPCG_ERR_CUDA;
 }
+
+int pepcg_set_stream(void* ctx, void* stream) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return PEPCG_ERR_BAD_ARG;
+  cudaSetDevice(c->device);
+  if (!cuda_ok(c, cudaStreamSynchronize(c->stream), "set stream")) return PEPCG_ERR_CUDA;
+  if (c->own_stream) {
+    cudaStreamDestroy(c->stream);
+    c->own_stream = false;
+  }
+  if (stream == nullptr) {
+    if (!cuda_ok(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream"))
+      return PEPCG_ERR_CUDA;
+    c->own_stream = true;
+  } else {
+    c->stream = static_cast<cudaStream_t>(stream);
+  }
+  return PEPCG_OK;
+}
+
+long long pepcg_kernel_launches(void) { return g_launches.load(); }
 
 int pepcg_timber_tree(void* ctx) {
   Ctx* c = as_ctx(ctx);

@@ -97,6 +97,7 @@ int direct_device(Ctx* c, int64_t ntest, const int64_t* d_tidx, double* ex, doub
                   double* ez, double* pot) {
   cudaStream_t s = c->stream;
   const int64_t nb = (ntest + kTB - 1) / kTB;
+  COUNT_LAUNCH();
   k_direct<<<(unsigned)nb, kDThreads, 0, s>>>(ntest, d_tidx, c->n, c->x.p, c->y.p, c->z.p, c->q.p,
                                               c->d_vbox, c->nboxes, c->prm.eps2, ex, ey, ez, pot);
   if (!cuda_ok(c, cudaGetLastError(), "direct launch")) return PEPCG_ERR_CUDA;
@@ -104,6 +105,7 @@ int direct_device(Ctx* c, int64_t ntest, const int64_t* d_tidx, double* ex, doub
     double* pos = nullptr;
     if (!cuda_ok(c, cudaMallocAsync((void**)&pos, 3 * ntest * sizeof(double), s), "direct pos"))
       return PEPCG_ERR_OOM;
+    COUNT_LAUNCH();
     k_gather_pos<<<148, 256, 0, s>>>(ntest, d_tidx, c->x.p, c->y.p, c->z.p, pos);
     int rc = lattice_add(c, ntest, pos, pos + ntest, pos + 2 * ntest, ex, ey, ez, pot, false);
     cudaFreeAsync(pos, s);

@@ -317,8 +317,11 @@ __global__ void k_scan_apply(const T* __restrict__ in, int64_t n, const T* __res
 template <class T>
 void exclusive_scan(const T* in, T* out, int64_t n, T* tmp, cudaStream_t s) {
   int64_t nb = (n + kScanTile - 1) / kScanTile;
+  COUNT_LAUNCH();
   k_scan_reduce<T><<<(unsigned)nb, kThreads, 0, s>>>(in, n, tmp);
+  COUNT_LAUNCH();
   k_scan_blocks<T><<<1, kThreads, 0, s>>>(tmp, nb);
+  COUNT_LAUNCH();
   k_scan_apply<T><<<(unsigned)nb, kThreads, 0, s>>>(in, n, tmp, out);
 }
 
@@ -631,13 +634,18 @@ __global__ void k_upward(int64_t M, const int2* __restrict__ meta, const int32_t
   }
 }
 
-// FP32 copy of the twig moments for the mixed walk
+// FP32 copy of the twig moments for the mixed walk, packed as three float4:
+// (px, py, pz, qxx), (qyy, qzz, qxy/2, qyz/2), (qzx/2, qxx+qyy+qzz, charge, 0)
 __global__ void k_mom32(int64_t M, const int2* __restrict__ meta, const double* __restrict__ mom,
-                        float* __restrict__ mom32) {
+                        const double4* __restrict__ nc4, float4* __restrict__ mom32) {
   for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < M;
        u += (int64_t)gridDim.x * blockDim.x) {
     if (meta[u].y & kLeafFlag) continue;
-    for (int k = 0; k < 9; ++k) mom32[12 * u + k] = (float)mom[9 * u + k];
+    const double* m = mom + 9 * u;
+    const double q = nc4[u].w;
+    mom32[3 * u] = make_float4((float)m[0], (float)m[1], (float)m[2], (float)m[3]);
+    mom32[3 * u + 1] = make_float4((float)m[4], (float)m[5], (float)(0.5 * m[6]), (float)(0.5 * m[7]));
+    mom32[3 * u + 2] = make_float4((float)(0.5 * m[8]), (float)((m[3] + m[4]) + m[5]), (float)q, 0.f);
   }
 }
 
@@ -689,9 +697,12 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
   // box
   const int nbb = 296;
   double* part = c->d_part;  // 6 * nbb doubles
+  COUNT_LAUNCH();
   k_bbox_partial<<<nbb, kThreads, 0, s>>>(n, dx, dy, dz, part, c->d_status);
+  COUNT_LAUNCH();
   k_bbox_final<<<1, 32, 0, s>>>(nbb, part, c->prm.force_cubic_domain, c->d_box);
   // keys
+  COUNT_LAUNCH();
   k_keys<<<grid_for(n), kThreads, 0, s>>>(n, dx, dy, dz, c->d_box, c->prm.curve, c->skey.p,
                                           c->sval.p);
   cudaEventRecord(c->ev[1], s);
@@ -703,21 +714,26 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
   const int nb = (int)nblk_sort;
   for (int pass = 0; pass < 8; ++pass) {
     const int shift = 8 * pass;
+    COUNT_LAUNCH();
     k_sort_hist<<<nb, kThreads, 0, s>>>(n, kin, shift, c->hist.p, nb);
     exclusive_scan<uint32_t>(c->hist.p, c->hist.p, 256 * (int64_t)nb,
                              reinterpret_cast<uint32_t*>(c->scan_tmp.p), s);
+    COUNT_LAUNCH();
     k_sort_scatter<<<nb, kThreads, 0, s>>>(n, kin, vin, kout, vout, shift, c->hist.p, nb);
     std::swap(kin, kout);
     std::swap(vin, vout);
   }
   // after an even number of passes the result is back in skey / sval
+  COUNT_LAUNCH();
   k_permute<<<grid_for(n), kThreads, 0, s>>>(n, kin, vin, dx, dy, dz, dq, c->x.p, c->y.p, c->z.p,
                                              c->q.p, c->key.p, c->orig_key.p, c->perm.p,
                                              c->d_small, c->dup_list.p, dupcap);
+  COUNT_LAUNCH();
   k_dupfix<<<1, 32, 0, s>>>(n, c->key.p, c->orig_key.p, c->x.p, c->y.p, c->z.p, c->d_small,
                             c->dup_list.p, dupcap, c->d_box, c->prm.curve, c->d_status);
   cudaEventRecord(c->ev[2], s);
   // tree
+  COUNT_LAUNCH();
   k_node_counts<<<grid_for(n), kThreads, 0, s>>>(n, c->key.p, c->lev.p, c->lcpn.p, c->cstart.p,
                                                   c->cend.p, c->d_status,
                                                   reinterpret_cast<int*>(c->d_small + 2));
@@ -755,16 +771,21 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
       !ensure(c, c->nleaves, M, "nleaves") || !ensure(c, c->fpo2rpo, M, "fpo2rpo") ||
       !ensure(c, c->rpo2fpo, M, "rpo2fpo") || !ensure(c, c->nkey, M, "nkey"))
     return PEPCG_ERR_OOM;
+  COUNT_LAUNCH();
   k_build_nodes<<<grid_for(n), kThreads, 0, s>>>(n, M, c->key.p, c->lev.p, c->lcpn.p, c->sstart.p,
                                                   c->send.p, c->x.p, c->y.p, c->z.p, c->q.p,
                                                   c->nc4.p, c->meta.p, c->fpo2rpo.p, c->rpo2fpo.p,
                                                   c->first_part.p, c->nleaves.p, c->nkey.p);
+  COUNT_LAUNCH();
   k_link<<<grid_for(M), kThreads, 0, s>>>(M, c->meta.p, c->rpo2fpo.p, c->fpo2rpo.p, c->fwd.p,
                                           c->parent.p, c->nchild.p, c->upcnt.p);
   cudaEventRecord(c->ev[3], s);
+  COUNT_LAUNCH();
   k_upward<<<grid_for(M), kThreads, 0, s>>>(M, c->meta.p, c->parent.p, c->nchild.p, c->upcnt.p,
                                             c->nc4.p, c->mom.p, c->aux.p);
-  k_mom32<<<grid_for(M), kThreads, 0, s>>>(M, c->meta.p, c->mom.p, c->mom32.p);
+  COUNT_LAUNCH();
+  k_mom32<<<grid_for(M), kThreads, 0, s>>>(M, c->meta.p, c->mom.p, c->nc4.p,
+                                           reinterpret_cast<float4*>(c->mom32.p));
   cudaEventRecord(c->ev[4], s);
   if (!cuda_ok(c, cudaGetLastError(), "grow kernels")) return PEPCG_ERR_CUDA;
   c->n = n;
@@ -844,6 +865,7 @@ int export_tree(Ctx* c, int64_t* key, int32_t* level, int64_t* leaves, int64_t* 
   int64_t* dn = df + M;
   double* dm = (double*)(dn + M);
   int32_t* dlev = (int32_t*)(dm + 15 * M);
+  COUNT_LAUNCH();
   k_export<<<grid_for(M), kThreads, 0, s>>>(M, c->fpo2rpo.p, c->rpo2fpo.p, c->meta.p, c->fwd.p,
                                             c->parent.p, c->nkey.p, c->nc4.p, c->mom.p, c->aux.p,
                                             dk, dlev, dl, dd, dp, df, dn, dm, c->first_part.p, c->n);

@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 
 #include "../../include/pepcg.h"
@@ -29,6 +30,11 @@
 namespace pepcg {
 
 constexpr int kMaxLevel = 20;    // treevars.f90:55 for idim = 3, 64-bit keys
+
+// number of kernels this library has launched (process-wide, for the record
+// of GPU work per call)
+extern std::atomic<long long> g_launches;
+#define COUNT_LAUNCH() (::pepcg::g_launches.fetch_add(1, std::memory_order_relaxed))
 constexpr int kLeafFlag = 1 << 8;
 
 // device status word bits (set by kernels, read by the host after a launch)
@@ -54,6 +60,7 @@ struct Ctx {
   pepcg_params prm;
   int device = 0;
   cudaStream_t stream = nullptr;
+  bool own_stream = false;
   std::string err;
 
   int64_t n = 0;       // particles in the tree

@@ -503,13 +503,17 @@ int lattice_prepare(Ctx* c) {
     cudaMemcpyAsync(c->d_factorial, hf.data(), hf.size() * 8, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d_scp, hs.data(), hs.size() * 8, cudaMemcpyHostToDevice, s);
     cudaMemsetAsync(c->d_fmm_aux, 0, 64 * 8, s);
+    COUNT_LAUNCH();
     k_mstar<<<(lenm + 63) / 64, 64, 0, s>>>(lm, nb, c->d_vbox, c->d_factorial, scratch, mstar);
+    COUNT_LAUNCH();
     k_lstar<<<(lent + 63) / 64, 64, 0, s>>>(lt, nb, ws, c->d_vbox, c->d_factorial, scratch, lstar);
     cudaMemcpyAsync(ml0, lstar, lent * 16, cudaMemcpyDeviceToDevice, s);
     for (int it = 0; it < kMaxIter; ++it) {
+      COUNT_LAUNCH();
       k_lattice_iter<<<(lent + 127) / 128, 128, 0, s>>>(lt, lm, ml0, mstar, lstar, d_scp, ml1);
       std::swap(ml0, ml1);
     }
+    COUNT_LAUNCH();
     k_truncate<<<(kLenT + 127) / 128, 128, 0, s>>>(ml0, c->d_mlattice);
     ok = cuda_ok(c, cudaGetLastError(), "lattice coefficients") &&
          cuda_ok(c, cudaStreamSynchronize(s), "lattice coefficients");
@@ -544,13 +548,18 @@ int lattice_timestep(Ctx* c) {
   }
   cudaMemcpyAsync(d_lat, lat, 12 * 8, cudaMemcpyHostToDevice, s);
   cudaMemsetAsync(c->d_status, 0, 4, s);
+  COUNT_LAUNCH();
   k_box_dipole<<<nbp, 256, 0, s>>>(n, c->x.p, c->y.p, c->z.p, c->q.p, cx, cy, cz, part);
+  COUNT_LAUNCH();
   k_fict<<<1, 32, 0, s>>>(nbp, part, c->d_fmm_aux, p.periodicity[0], p.periodicity[1],
                          p.periodicity[2], d_lat, d_lat + 9, p.fmm_extrinsic_correction);
+  COUNT_LAUNCH();
   k_omega_partial<<<(unsigned)nom, 256, 0, s>>>(n, c->x.p, c->y.p, c->z.p, c->q.p, cx, cy, cz,
                                                 c->d_factorial, opart);
+  COUNT_LAUNCH();
   k_omega_final<<<1, 256, 0, s>>>((int)nom, opart, c->d_fmm_aux, cx, cy, cz, c->d_factorial,
                                   c->d_omega, c->d_status);
+  COUNT_LAUNCH();
   k_mu_cent<<<(kLenT + 127) / 128, 128, 0, s>>>(c->d_mlattice, c->d_omega, c->d_mu);
   uint32_t st = 0;
   ok = cuda_ok(c, cudaGetLastError(), "lattice timestep") &&
@@ -577,6 +586,7 @@ int lattice_add(Ctx* c, int64_t nt, const double* tx, const double* ty, const do
   const double volume = std::fabs((cr[0] * cc[0] + cr[1] * cc[1]) + cr[2] * cc[2]);
   unsigned blocks = (unsigned)((nt + 127) / 128);
   if (blocks > 148 * 16) blocks = 148 * 16;
+  COUNT_LAUNCH();
   k_lattice_force<<<blocks, 128, 0, s>>>(nt, tx, ty, tz, c->d_mu, c->d_fmm_aux, c->d_vbox, c->nboxes,
                                          cx, cy, cz, volume, p.fmm_extrinsic_correction,
                                          c->d_factorial, ex, ey, ez, pot, overwrite ? 1 : 0);

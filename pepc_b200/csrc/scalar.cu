@@ -54,6 +54,7 @@ int run_scalar(int op, const double* in, int nin_doubles, int nchild, double* ou
     return PEPCG_ERR_CUDA;
   }
   cudaMemcpy(d, in, nin_doubles * sizeof(double), cudaMemcpyHostToDevice);
+  COUNT_LAUNCH();
   k_scalar<<<1, 32>>>(op, d, nchild, d + nin_doubles);
   cudaError_t e = cudaMemcpy(out, d + nin_doubles, nout * sizeof(double), cudaMemcpyDeviceToHost);
   cudaFree(d);

@@ -152,8 +152,10 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_tile64(WalkArgs A) {
     unsigned b = 0;
     if (lane == 0) b = atomicAdd(&g_bucket_counter, 1u);
     b = __shfl_sync(0xffffffffu, b, 0);
-    if ((int64_t)b >= A.ntiles) break;
-    const int2 tl = A.tiles[b];
+    const int64_t nbk = A.tiles ? A.ntiles : (A.nt + 31) / 32;
+    if ((int64_t)b >= nbk) break;
+    const int2 tl = A.tiles ? A.tiles[b]
+                            : make_int2((int)((int64_t)b * 32), (int)min((int64_t)32, A.nt - (int64_t)b * 32));
     const bool valid = lane < tl.y;
     const int64_t t = (int64_t)tl.x + lane;
     double px = 0, py = 0, pz = 0, e0 = 0, e1 = 0, e2 = 0, ph = 0, w = 0;
@@ -248,6 +250,10 @@ __global__ void k_reset_counter() { g_bucket_counter = 0; }
 
 }  // namespace
 
+int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
+                      double* ex, double* ey, double* ez, double* pot, double* work,
+                      const int2* tiles, int64_t ntiles, bool per_target);
+
 int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                     const int64_t* tkeys, bool self, double* ex, double* ey, double* ez,
                     double* pot, double* work) {
@@ -269,6 +275,7 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
       unsigned int* d_diff = reinterpret_cast<unsigned int*>(c->d_small + 4);
       unsigned int h_diff = 1;
       cudaMemsetAsync(d_diff, 0, 4, s);
+      COUNT_LAUNCH();
       k_same_keys<<<296, 256, 0, s>>>(nt, tkeys, c->key.p, d_diff);
       if (!cuda_ok(c, cudaMemcpyAsync(&h_diff, d_diff, 4, cudaMemcpyDeviceToHost, s), "tiles") ||
           !cuda_ok(c, cudaStreamSynchronize(s), "tiles"))
@@ -281,6 +288,7 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
       unsigned int* d_nt = reinterpret_cast<unsigned int*>(c->d_small + 5);
       unsigned int h_nt = 0;
       cudaMemsetAsync(d_nt, 0, 4, s);
+      COUNT_LAUNCH();
       k_tiles_from_tree<<<296, 256, 0, s>>>((int32_t)c->nnodes, T, c->nleaves_ptr(), c->parent.p,
                                             c->first_part.p, d_tiles, d_nt);
       if (!cuda_ok(c, cudaMemcpyAsync(&h_nt, d_nt, 4, cudaMemcpyDeviceToHost, s), "tiles") ||
@@ -313,16 +321,22 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
   A.status = c->d_status;
   A.tiles = reinterpret_cast<const int2*>(c->tiles.p);
   A.ntiles = ntiles;
+  COUNT_LAUNCH();
   k_reset_counter<<<1, 1, 0, s>>>();
   const int blocks = 148 * 8;
   if (c->prm.precision == PEPCG_PRECISION_PLAIN) {
-    if (walk == PEPCG_WALK_PER_TARGET || walk == PEPCG_WALK_GROUP)
+    COUNT_LAUNCH();
+    if (walk == PEPCG_WALK_PER_TARGET) {
       k_walk_target64<<<blocks, kWalkThreads, 0, s>>>(A);
-    else
+    } else {
+      if (walk == PEPCG_WALK_GROUP) A.tiles = nullptr;
       k_walk_tile64<<<blocks, kWalkThreads, 0, s>>>(A);
+    }
   } else {
-    c->err = "mixed precision walk not built yet";
-    return PEPCG_ERR_UNSUPPORTED;
+    int rc = launch_walk_mixed(c, nt, tx, ty, tz, ex, ey, ez, pot, work,
+                               walk == PEPCG_WALK_PER_TILE ? A.tiles : nullptr, ntiles,
+                               walk == PEPCG_WALK_PER_TARGET);
+    if (rc) return rc;
   }
   if (!cuda_ok(c, cudaGetLastError(), "walk launch")) return PEPCG_ERR_CUDA;
   cudaEventRecord(c->ev[6], s);

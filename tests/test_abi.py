@@ -18,7 +18,7 @@ def declared_symbols():
             continue
         txt = open(os.path.join(ROOT, "include", name)).read()
         txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-        for m in re.finditer(r"\b(?:int|void|const char\*|int64_t)\s+\**(pepcg_\w+)\s*\(", txt):
+        for m in re.finditer(r"\b(?:int|void|const char\*|int64_t|long long)\s+\**(pepcg_\w+)\s*\(", txt):
             syms.add(m.group(1))
     return syms
 

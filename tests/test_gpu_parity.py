@@ -9,32 +9,9 @@ import pytest
 
 import pepc_b200 as P
 from oracle import oracle as O
+from tests.datasets import cube, plummer
 
 pytestmark = pytest.mark.gpu
-
-
-def cube(n, seed, charges="alt"):
-    rng = np.random.default_rng(seed)
-    x, y, z = rng.random(n), rng.random(n), rng.random(n)
-    if charges == "alt":
-        q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
-    else:
-        q = rng.standard_normal(n)
-    return x, y, z, q
-
-
-def plummer(n, seed):
-    rng = np.random.default_rng(seed)
-    r = np.empty(0)
-    while r.size < n:
-        u = rng.random(2 * n)
-        rr = 1.0 / np.sqrt(u ** (-2.0 / 3.0) - 1.0)
-        r = np.concatenate([r, rr[rr <= 20.0]])
-    r = r[:n]
-    v = rng.standard_normal((n, 3))
-    v /= np.linalg.norm(v, axis=1)[:, None]
-    p = v * r[:, None]
-    return p[:, 0].copy(), p[:, 1].copy(), p[:, 2].copy(), np.full(n, 1.0 / n)
 
 
 def grow_both(x, y, z, q, **kw):

@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
+from tests.datasets import rocksalt
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden", "reference_pins.npz")
 
@@ -113,3 +114,17 @@ def test_tree_invariants_and_walk_limits():
         idx = np.arange(0, n, 97)
         rel = np.abs(r["ex"][idx] - d["ex"]) / np.abs(d["ex"]).max()
         assert rel.max() < 1e-12
+
+
+def test_oracle_madelung_constant(gold):
+    # rock-salt lattice in the periodic unit cube, all near-field boxes summed
+    # directly (theta = 0) plus the reference's far-lattice term with its
+    # pretabulated coefficients: -<q phi> r0 is the Madelung constant of NaCl
+    n = 8
+    x, y, z, q = rocksalt(n)
+    orc = O.Oracle(theta2=0.0, eps2=0.0, periodicity=(1, 1, 1), num_threads=4)
+    orc.set_lattice_coefficients(O.reference_lattice_table(gold))
+    g = orc.grow_tree(x, y, z, q)
+    r = orc.traverse_tree(g["x"], g["y"], g["z"])
+    m_est = -np.mean(g["q"] * r["pot"]) / n
+    assert abs(m_est - 1.7475645946331822) < 1e-8
