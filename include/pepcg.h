@@ -195,6 +195,22 @@ int pepcg_direct(void* ctx, int64_t ntest, const int64_t* tidx, double* ex, doub
 int pepcg_lattice(void* ctx, int64_t nt, const double* tx, const double* ty, const double* tz,
                   double* ex, double* ey, double* ez, double* pot);
 
+/*
+ * pepcg_sort_keys_noalloc -- sorts n non-negative 64-bit keys (ascending,
+ * stable: equal keys keep their input order) and returns the sorted keys and
+ * the 0-based input index of each sorted key, all device pointers, enqueued
+ * on `stream` (a cudaStream_t of the current device, or NULL).  It allocates
+ * nothing: for callers that cannot call cudaMalloc, its scratch is a static
+ * device array of the library (about 24.3 MB per device, held until exit),
+ * which limits n to 1,048,576; larger n returns PEPCG_ERR_BAD_ARG.  The first
+ * call on a device looks up that array's address (make it before any stream
+ * capture); calls that overlap on the GPU race on the shared array.  The
+ * order equals the key order of pepcg_grow_tree's key_out / perm_out.
+ * No counterpart in the reference.
+ */
+int pepcg_sort_keys_noalloc(int64_t n, const int64_t* d_keys_in, int64_t* d_keys_out,
+                            int64_t* d_perm_out, void* stream);
+
 /* ---- scalar backend entry points (evaluated by the same device code the
  * walk uses; one tiny launch per call, for shims and unit tests) ---- */
 /* multipole_from_particle, coulomb/module_interaction_specific.f90:67-79 */

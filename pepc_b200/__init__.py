@@ -111,7 +111,7 @@ EXPORTS = [
     "pepcg_traverse_self_device", "pepcg_timber_tree", "pepcg_stats_get", "pepcg_num_nodes",
     "pepcg_tree_export", "pepcg_direct", "pepcg_lattice", "pepcg_multipole_from_particle",
     "pepcg_shift_multipoles_up", "pepcg_force_with_leaf", "pepcg_force_with_twig", "pepcg_mac",
-    "pepcg_set_stream", "pepcg_kernel_launches",
+    "pepcg_set_stream", "pepcg_kernel_launches", "pepcg_sort_keys_noalloc",
 ]
 
 _LIB = None
@@ -141,6 +141,7 @@ def lib():
     L.pepcg_traverse_self_device.argtypes = [VP, VP, VP, VP, VP, VP]
     L.pepcg_timber_tree.argtypes = [VP]
     L.pepcg_set_stream.argtypes = [VP, VP]
+    L.pepcg_sort_keys_noalloc.argtypes = [C.c_int64, VP, VP, VP, VP]
     L.pepcg_kernel_launches.argtypes = []
     L.pepcg_kernel_launches.restype = C.c_longlong
     L.pepcg_stats_get.argtypes = [VP, C.POINTER(Stats)]

@@ -18,6 +18,8 @@ namespace pepcg {
 static thread_local std::string g_static_err;
 std::atomic<long long> g_launches{0};
 
+void set_static_error(const std::string& msg) { g_static_err = msg; }
+
 bool cuda_ok(Ctx* c, cudaError_t e, const char* what) {
   if (e == cudaSuccess) return true;
   std::string msg = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";

@@ -6,6 +6,9 @@
 // Compiled with --fmad=false: the FP64 arithmetic below must equal a plain
 // IEEE evaluation of the reference's expressions.
 
+#include <mutex>
+#include <string>
+
 #include "internal.cuh"
 
 namespace pepcg {
@@ -887,3 +890,137 @@ int export_tree(Ctx* c, int64_t* key, int32_t* level, int64_t* leaves, int64_t* 
 }
 
 }  // namespace pepcg
+
+// ---------------------------------------------------------------------------
+// Allocation-free key sort.
+//
+// Some callers cannot allocate device memory at the time they need the sort:
+// a Fortran or C frontend that runs inside another code's memory pool with
+// cudaMalloc forbidden, code that must not change the device's memory
+// footprint between steps, or a caller that runs where allocating would
+// synchronise the device.  pepcg_sort_keys_noalloc serves them: it runs the
+// same LSD radix sort passes as pepcg_grow_tree (k_sort_hist /
+// k_sort_scatter / the exclusive scans above) with every scratch buffer taken
+// from the file-scope array below, and never calls cudaMalloc, cudaFree or an
+// allocating library routine.
+//
+// Limits and sharing:
+//  * at most kNoAllocMaxKeys keys per call (larger n is rejected);
+//  * the array lives on every GPU that loads this library until the process
+//    exits (about 24.3 MB per device);
+//  * all calls share the array, and it keeps the last call's contents; every
+//    scratch word a call reads is written by that same call first, so nothing
+//    needs clearing, but calls that overlap on the GPU (two streams, two host
+//    threads, or a call issued before the previous one finished) race on it;
+//  * the first call on a device looks up the array's device address with
+//    cudaGetSymbolAddress (host code only holds a host-side stand-in for the
+//    symbol); make that first call before any stream capture on the device.
+// ---------------------------------------------------------------------------
+namespace pepcg {
+namespace {
+
+constexpr int64_t kNoAllocMaxKeys = int64_t(1) << 20;
+constexpr int64_t kNoAllocBlocks = kNoAllocMaxKeys / kSortChunk;  // 256
+// byte offsets inside the scratch array
+constexpr size_t kNaKeysA = 0;
+constexpr size_t kNaKeysB = kNaKeysA + 8 * kNoAllocMaxKeys;
+constexpr size_t kNaValsA = kNaKeysB + 8 * kNoAllocMaxKeys;
+constexpr size_t kNaValsB = kNaValsA + 4 * kNoAllocMaxKeys;
+constexpr size_t kNaHist = kNaValsB + 4 * kNoAllocMaxKeys;
+constexpr size_t kNaHistBytes = ((4 * (256 * kNoAllocBlocks + 1) + 255) / 256) * 256;
+constexpr size_t kNaScan = kNaHist + kNaHistBytes;
+constexpr size_t kNaScanBytes = 4 * 1024;
+constexpr size_t kNaBytes = kNaScan + kNaScanBytes;
+
+static __device__ __align__(256) unsigned char g_sort_scratch[kNaBytes];
+
+__global__ void k_noalloc_load(int64_t n, const int64_t* __restrict__ in, uint64_t* __restrict__ k,
+                               int32_t* __restrict__ v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    k[i] = (uint64_t)in[i];
+    v[i] = (int32_t)i;
+  }
+}
+
+__global__ void k_noalloc_store(int64_t n, const uint64_t* __restrict__ k,
+                                const int32_t* __restrict__ v, int64_t* __restrict__ kout,
+                                int64_t* __restrict__ pout) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    kout[i] = (int64_t)k[i];
+    pout[i] = (int64_t)v[i];
+  }
+}
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[64] = {};
+
+}  // namespace
+}  // namespace pepcg
+
+extern "C" int pepcg_sort_keys_noalloc(int64_t n, const int64_t* d_keys_in, int64_t* d_keys_out,
+                                       int64_t* d_perm_out, void* stream) {
+  using namespace pepcg;
+  if (n < 0 || n > kNoAllocMaxKeys) {
+    set_static_error("pepcg_sort_keys_noalloc: n = " + std::to_string(n) +
+                     " is outside 0.." + std::to_string(kNoAllocMaxKeys) +
+                     " (the size of the library's static sort scratch)");
+    return PEPCG_ERR_BAD_ARG;
+  }
+  if (n == 0) return PEPCG_OK;
+  if (!d_keys_in || !d_keys_out || !d_perm_out) {
+    set_static_error("pepcg_sort_keys_noalloc: null pointer");
+    return PEPCG_ERR_BAD_ARG;
+  }
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 64) {
+    set_static_error(std::string("pepcg_sort_keys_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
+    return PEPCG_ERR_CUDA;
+  }
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_sort_scratch);
+      if (e != cudaSuccess || p == nullptr) {
+        set_static_error(std::string("pepcg_sort_keys_noalloc: cudaGetSymbolAddress: ") +
+                         cudaGetErrorString(e));
+        return PEPCG_ERR_CUDA;
+      }
+      g_noalloc_ptr[dev] = p;
+    }
+    base = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  uint64_t* kin = reinterpret_cast<uint64_t*>(base + kNaKeysA);
+  uint64_t* kout = reinterpret_cast<uint64_t*>(base + kNaKeysB);
+  int32_t* vin = reinterpret_cast<int32_t*>(base + kNaValsA);
+  int32_t* vout = reinterpret_cast<int32_t*>(base + kNaValsB);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(base + kNaHist);
+  uint32_t* tmp = reinterpret_cast<uint32_t*>(base + kNaScan);
+  const int nb = (int)((n + kSortChunk - 1) / kSortChunk);
+  COUNT_LAUNCH();
+  k_noalloc_load<<<grid_for(n), kThreads, 0, s>>>(n, d_keys_in, kin, vin);
+  for (int pass = 0; pass < 8; ++pass) {
+    const int shift = 8 * pass;
+    COUNT_LAUNCH();
+    k_sort_hist<<<nb, kThreads, 0, s>>>(n, kin, shift, hist, nb);
+    g_launches.fetch_add(3, std::memory_order_relaxed);
+    exclusive_scan<uint32_t>(hist, hist, 256 * (int64_t)nb, tmp, s);
+    COUNT_LAUNCH();
+    k_sort_scatter<<<nb, kThreads, 0, s>>>(n, kin, vin, kout, vout, shift, hist, nb);
+    std::swap(kin, kout);
+    std::swap(vin, vout);
+  }
+  COUNT_LAUNCH();
+  k_noalloc_store<<<grid_for(n), kThreads, 0, s>>>(n, kin, vin, d_keys_out, d_perm_out);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_static_error(std::string("pepcg_sort_keys_noalloc: launch: ") + cudaGetErrorString(e));
+    return PEPCG_ERR_CUDA;
+  }
+  return PEPCG_OK;
+}

@@ -127,6 +127,8 @@ struct Ctx {
 
 // ---- helpers implemented in api.cu ----
 bool cuda_ok(Ctx* c, cudaError_t e, const char* what);
+// error text for entry points without a context (pepcg_last_error(NULL))
+void set_static_error(const std::string& msg);
 template <class T>
 bool ensure(Ctx* c, DBuf<T>& b, size_t n, const char* what);
 int status_to_code(Ctx* c, uint32_t st);
