@@ -197,7 +197,10 @@ def main():
     dev = torch.device("cuda", local)
     tx, ty, tz, tq = (torch.from_numpy(a).to(dev) for a in (x, y, z, q))
     out = [torch.zeros(n, dtype=torch.float64, device=dev) for _ in range(5)]
-    stream = torch.cuda.current_stream()
+    # a dedicated stream, current for torch as well, so the CUDA events that
+    # time the steps sit on the stream the library launches on
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
     walk = {"group": P.WALK_GROUP, "target": P.WALK_PER_TARGET, "tile": P.WALK_PER_TILE}[args.walk]
     prec = P.PRECISION_MIXED if args.precision == "mixed" else P.PRECISION_PLAIN
     tc = P.TreeCode(theta2=args.theta ** 2, eps2=args.eps ** 2, precision=prec, walk=walk,

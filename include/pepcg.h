@@ -156,8 +156,29 @@ int pepcg_traverse_tree_device(void* ctx, int64_t nt, const double* d_tx, const 
 int pepcg_traverse_self_device(void* ctx, double* d_ex, double* d_ey, double* d_ez,
                                double* d_pot, double* d_work);
 
+/*
+ * pepcg_traverse_adjoint -- the adjoint of pepcg_traverse_tree (no reference
+ * counterpart; the reference has no differentiation).  Given dL/dE (three
+ * arrays) and dL/dphi at nt targets, returns dL/dq and dL/dx, dL/dy, dL/dz of
+ * the grown particles in the caller's ORIGINAL order (overwrites; arrays of
+ * length npart).  The interaction lists are recomputed with the context's walk
+ * semantics and held fixed (MAC decisions and keys are piecewise constant).
+ * FP64.  Open boundaries only: a periodic far field returns
+ * PEPCG_ERR_UNSUPPORTED.
+ */
+int pepcg_traverse_adjoint(void* ctx, int64_t nt, const double* tx, const double* ty,
+                           const double* tz, const double* dLdEx, const double* dLdEy,
+                           const double* dLdEz, const double* dLdphi, double* dLdq, double* dLdx,
+                           double* dLdy, double* dLdz);
+/* Same with device arrays. */
+int pepcg_traverse_adjoint_device(void* ctx, int64_t nt, const double* d_tx, const double* d_ty,
+                                  const double* d_tz, const double* d_gex, const double* d_gey,
+                                  const double* d_gez, const double* d_gphi, double* d_dq,
+                                  double* d_dx, double* d_dy, double* d_dz);
+
 /* Launch all of this context's work on the caller's CUDA stream (a
- * cudaStream_t of the context's device), or on a private stream when NULL.
+ * cudaStream_t of the context's device), or on a private non-blocking stream
+ * when NULL (so the legacy default stream is selected with cudaStreamLegacy).
  * Lets a caller that owns a stream (e.g. a framework's current stream) order
  * and time the library's kernels with its own events.  No reference
  * counterpart: the reference has no device streams. */

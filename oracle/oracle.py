@@ -72,6 +72,10 @@ def lib():
         L.orc_lattice.restype = C.c_int
         L.orc_fmm_lattice_coefficients.argtypes = [C.POINTER(OrcParams), D]
         L.orc_set_lattice_coefficients.argtypes = [C.c_void_p, D]
+        L.orc_traverse_adjoint.argtypes = [C.c_void_p, C.c_int64, D, D, D, D, D, D, D, D, D, D, D]
+        L.orc_traverse_adjoint.restype = C.c_int
+        L.orc_direct_adjoint.argtypes = [C.c_void_p, C.c_int64, D, D, D, D, D, D, D, D, D, D, D]
+        L.orc_direct_adjoint.restype = C.c_int
         L.orc_set_lattice_coefficients.restype = C.c_int
         _LIB = L
     return _LIB
@@ -257,6 +261,17 @@ class Oracle:
         if rc != 0:
             raise RuntimeError(f"orc_direct failed: {rc}")
         return dict(ex=ex, ey=ey, ez=ez, pot=pt)
+
+    def traverse_adjoint(self, x, y, z, gE, gphi, npart, direct=False):
+        """dL/dq, dL/dx (original particle order) of sum_t gphi phi_t + gE.E_t."""
+        nt = len(x)
+        args = [f64(v) for v in (x, y, z, gE[0], gE[1], gE[2], gphi)]
+        out = [np.zeros(npart) for _ in range(4)]
+        fn = lib().orc_direct_adjoint if direct else lib().orc_traverse_adjoint
+        rc = fn(self.h, nt, *[dp(a) for a in args], *[dp(o) for o in out])
+        if rc != 0:
+            raise RuntimeError(f"adjoint failed: {rc}")
+        return dict(q=out[0], x=out[1], y=out[2], z=out[3])
 
     def set_lattice_coefficients(self, ml):
         ml = np.asarray(ml, dtype=np.complex128)

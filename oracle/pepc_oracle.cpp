@@ -614,6 +614,156 @@ void parallel_for(int64_t n, int nthreads, F&& f) {
   for (auto& t : th) t.join();
 }
 
+
+// ---------------------------------------------------------------------------
+// Adjoint of the walk (checker for pepcg_traverse_adjoint; the reference has
+// no adjoint).  Writing the twig potential as
+//   phi = q D0 + p_k D1_k + sum_{kl in xx,yy,zz,xy,yz,zx} Q_kl D2_kl
+// with D the Cartesian derivative tensors of 1/r (r^2 = |d|^2 + eps^2) --
+// which is exactly calc_force_coulomb_3D (module_coulomb_kernels.f90:60-145)
+// -- one target-node pair with dL/dphi = gphi, dL/dE = gE contributes
+//   qbar += gphi D0 - gE.D1,  pbar_k += gphi D1_k - gE_i D2_ik,
+//   Qbar_kl += gphi D2_kl - gE_i D3_ikl,  cocbar += gphi E + H gE
+// (E = -grad phi, H = the Hessian of phi).  The interaction lists are held
+// fixed (the MAC and the keys are piecewise constant).
+// ---------------------------------------------------------------------------
+struct Tens {
+  double d[3], R[5];
+  void set(const double dd[3], double eps2) {
+    d[0] = dd[0]; d[1] = dd[1]; d[2] = dd[2];
+    const double r2 = ((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]) + eps2;
+    const double r0 = 1.0 / std::sqrt(r2);
+    const double r02 = r0 * r0;
+    R[0] = r0;
+    R[1] = R[0] * r02;
+    R[2] = R[1] * r02;
+    R[3] = R[2] * r02;
+    R[4] = R[3] * r02;
+  }
+  static double dl(int i, int j) { return i == j ? 1.0 : 0.0; }
+  double D1(int i) const { return -d[i] * R[1]; }
+  double D2(int i, int j) const { return 3.0 * d[i] * d[j] * R[2] - dl(i, j) * R[1]; }
+  double D3(int i, int j, int k) const {
+    return -15.0 * d[i] * d[j] * d[k] * R[3] +
+           3.0 * R[2] * (dl(i, j) * d[k] + dl(i, k) * d[j] + dl(j, k) * d[i]);
+  }
+  double D4(int i, int j, int k, int l) const {
+    return 105.0 * d[i] * d[j] * d[k] * d[l] * R[4] -
+           15.0 * R[3] *
+               (dl(i, j) * d[k] * d[l] + dl(i, k) * d[j] * d[l] + dl(i, l) * d[j] * d[k] +
+                dl(j, k) * d[i] * d[l] + dl(j, l) * d[i] * d[k] + dl(k, l) * d[i] * d[j]) +
+           3.0 * R[2] * (dl(i, j) * dl(k, l) + dl(i, k) * dl(j, l) + dl(i, l) * dl(j, k));
+  }
+};
+
+const int kQK[6] = {0, 1, 2, 0, 1, 2};  // moment order xx yy zz xy yz zx
+const int kQL[6] = {0, 1, 2, 1, 2, 0};
+
+struct Adj {
+  double q = 0, p[3] = {0, 0, 0}, Q[6] = {0, 0, 0, 0, 0, 0}, c[3] = {0, 0, 0}, A = 0;
+};
+
+void twig_adjoint(const double* m, const double d[3], double eps2, double gphi, const double gE[3],
+                  Adj& a) {
+  Tens T;
+  T.set(d, eps2);
+  const double q = m[M_Q];
+  const double p[3] = {m[M_DX], m[M_DY], m[M_DZ]};
+  const double Q[6] = {m[M_QXX], m[M_QYY], m[M_QZZ], m[M_XY], m[M_YZ], m[M_ZX]};
+  a.q += gphi * T.R[0];
+  for (int i = 0; i < 3; ++i) a.q -= gE[i] * T.D1(i);
+  for (int k = 0; k < 3; ++k) {
+    double v = gphi * T.D1(k);
+    for (int i = 0; i < 3; ++i) v -= gE[i] * T.D2(i, k);
+    a.p[k] += v;
+  }
+  for (int s = 0; s < 6; ++s) {
+    double v = gphi * T.D2(kQK[s], kQL[s]);
+    for (int i = 0; i < 3; ++i) v -= gE[i] * T.D3(i, kQK[s], kQL[s]);
+    a.Q[s] += v;
+  }
+  for (int j = 0; j < 3; ++j) {
+    double E = q * T.D1(j);
+    for (int k = 0; k < 3; ++k) E += p[k] * T.D2(j, k);
+    for (int s = 0; s < 6; ++s) E += Q[s] * T.D3(j, kQK[s], kQL[s]);
+    E = -E;
+    double hg = 0.0;
+    for (int i = 0; i < 3; ++i) {
+      double H = q * T.D2(i, j);
+      for (int k = 0; k < 3; ++k) H += p[k] * T.D3(i, j, k);
+      for (int s = 0; s < 6; ++s) H += Q[s] * T.D4(i, j, kQK[s], kQL[s]);
+      hg += H * gE[i];
+    }
+    a.c[j] += gphi * E + hg;
+  }
+}
+
+void leaf_adjoint(double q, const double d[3], double eps2, double gphi, const double gE[3],
+                  Adj& a) {
+  Tens T;
+  T.set(d, eps2);
+  a.q += gphi * T.R[0];
+  for (int i = 0; i < 3; ++i) a.q -= gE[i] * T.D1(i);
+  for (int j = 0; j < 3; ++j) {
+    const double E = -q * T.D1(j);
+    double hg = 0.0;
+    for (int i = 0; i < 3; ++i) hg += q * T.D2(i, j) * gE[i];
+    a.c[j] += gphi * E + hg;
+  }
+}
+
+inline double sgn(double v) { return (double)((v > 0.0) - (v < 0.0)); }
+
+// transpose of shift_multipoles_up (coulomb/module_interaction_specific.f90:84-140)
+// for one parent: adds to the children's adjoints (children in key order)
+void shift_up_adjoint(const double* par, const double* const* ch, int nc, const Adj& pa, Adj* ca) {
+  const double A = par[M_ABSQ];
+  double s[8][3];
+  for (int c = 0; c < nc; ++c)
+    for (int d = 0; d < 3; ++d) s[c][d] = par[M_COCX + d] - ch[c][M_COCX + d];
+  double cocbar[3] = {pa.c[0], pa.c[1], pa.c[2]};
+  for (int c = 0; c < nc; ++c) {
+    const double* m = ch[c];
+    const double qc = m[M_Q];
+    const double pc[3] = {m[M_DX], m[M_DY], m[M_DZ]};
+    const double* sc = s[c];
+    double sbar[3] = {0, 0, 0};
+    for (int i = 0; i < 3; ++i) sbar[i] += pa.p[i] * qc;                        // dip
+    for (int i = 0; i < 3; ++i) sbar[i] += pa.Q[i] * (pc[i] + qc * sc[i]);      // quad diag
+    sbar[0] += pa.Q[3] * (pc[1] + qc * sc[1]); sbar[1] += pa.Q[3] * (pc[0] + qc * sc[0]);  // xy
+    sbar[1] += pa.Q[4] * (pc[2] + qc * sc[2]); sbar[2] += pa.Q[4] * (pc[1] + qc * sc[1]);  // yz
+    sbar[2] += pa.Q[5] * (pc[0] + qc * sc[0]); sbar[0] += pa.Q[5] * (pc[2] + qc * sc[2]);  // zx
+    Adj& a = ca[c];
+    a.q += pa.q;
+    for (int i = 0; i < 3; ++i) a.q += pa.p[i] * sc[i] + pa.Q[i] * 0.5 * sc[i] * sc[i];
+    a.q += pa.Q[3] * sc[0] * sc[1] + pa.Q[4] * sc[1] * sc[2] + pa.Q[5] * sc[2] * sc[0];
+    for (int i = 0; i < 3; ++i) a.p[i] += pa.p[i] + pa.Q[i] * sc[i];
+    a.p[0] += pa.Q[3] * sc[1] + pa.Q[5] * sc[2];
+    a.p[1] += pa.Q[3] * sc[0] + pa.Q[4] * sc[2];
+    a.p[2] += pa.Q[4] * sc[1] + pa.Q[5] * sc[0];
+    for (int k = 0; k < 6; ++k) a.Q[k] += pa.Q[k];
+    for (int i = 0; i < 3; ++i) {
+      a.c[i] -= sbar[i];  // s_c = coc - coc_c
+      cocbar[i] += sbar[i];
+    }
+    a.A += pa.A;  // abs_charge = sum of the children's abs_charge
+  }
+  for (int c = 0; c < nc; ++c) {
+    Adj& a = ca[c];
+    if (A != 0.0) {
+      const double w = ch[c][M_ABSQ] / A;
+      double g = 0.0;
+      for (int i = 0; i < 3; ++i) {
+        a.c[i] += cocbar[i] * w;
+        g += cocbar[i] * (ch[c][M_COCX + i] - par[M_COCX + i]);
+      }
+      a.A += g / A;
+    } else {
+      for (int i = 0; i < 3; ++i) a.c[i] += cocbar[i] / (double)nc;
+    }
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -969,6 +1119,111 @@ int orc_lattice(orc_ctx* c, int64_t nt, const double* tx, const double* ty, cons
     orc_fmm_sum_lattice_force(c->fmm, pos, e, &ph);
     ex[i] = e[0]; ey[i] = e[1]; ez[i] = e[2]; pot[i] = ph;
   }
+  return 0;
+}
+
+
+// Adjoint of the per-target walk (module_tree_walk_pthreads.f90 semantics):
+// dL/dq and dL/dx of the grown particles, in the caller's original order.
+// Open boundaries only (returns -5 with a periodic far field).
+int orc_traverse_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double* ty,
+                         const double* tz, const double* gex, const double* gey,
+                         const double* gez, const double* gphi, double* dLdq, double* dLdx,
+                         double* dLdy, double* dLdz) {
+  if (c->fmm) return -5;
+  auto boxes = neighbour_boxes(c->p);
+  const int64_t M = (int64_t)c->nodes.size();
+  std::vector<Adj> adj(M);
+  std::vector<int64_t> todo;
+  for (int64_t i = 0; i < nt; ++i) {
+    const double gE[3] = {gex[i], gey[i], gez[i]};
+    for (auto& bx : boxes) {
+      double vb[3];
+      lattice_vect(c->p, bx, vb);
+      const double sh[3] = {tx[i] - vb[0], ty[i] - vb[1], tz[i] - vb[2]};
+      todo.clear();
+      for (int64_t ch = c->nodes[c->root].first_child; ch != kNodeInvalid; ch = c->nodes[ch].next_sibling)
+        todo.push_back(ch);
+      while (!todo.empty()) {
+        int64_t ni = todo.back();
+        todo.pop_back();
+        const Node& nd = c->nodes[ni];
+        const double d[3] = {sh[0] - nd.m[M_COCX], sh[1] - nd.m[M_COCY], sh[2] - nd.m[M_COCZ]};
+        const double dist2 = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2];
+        if (nd.descendants == 0) {
+          if (dist2 > 0.0) leaf_adjoint(nd.m[M_Q], d, c->p.eps2, gphi[i], gE, adj[ni]);
+        } else if (c->p.theta2 * dist2 > c->boxlength2[nd.level]) {
+          twig_adjoint(nd.m, d, c->p.eps2, gphi[i], gE, adj[ni]);
+        } else {
+          for (int64_t ch = nd.first_child; ch != kNodeInvalid; ch = c->nodes[ch].next_sibling)
+            todo.push_back(ch);
+        }
+      }
+    }
+  }
+  // preorder (insertion order) visits every parent before its children
+  for (int64_t ni = 0; ni < M; ++ni) {
+    const Node& nd = c->nodes[ni];
+    if (nd.descendants == 0) continue;
+    const double* chm[8];
+    int64_t chi[8];
+    int nc = 0;
+    for (int64_t ch = nd.first_child; ch != kNodeInvalid; ch = c->nodes[ch].next_sibling) {
+      chm[nc] = c->nodes[ch].m;
+      chi[nc] = ch;
+      ++nc;
+    }
+    Adj ca[8];
+    shift_up_adjoint(nd.m, chm, nc, adj[ni], ca);
+    for (int k = 0; k < nc; ++k) {
+      Adj& a = adj[chi[k]];
+      a.q += ca[k].q;
+      for (int j = 0; j < 3; ++j) { a.p[j] += ca[k].p[j]; a.c[j] += ca[k].c[j]; }
+      for (int j = 0; j < 6; ++j) a.Q[j] += ca[k].Q[j];
+      a.A += ca[k].A;
+    }
+  }
+  for (int64_t ni = 0; ni < M; ++ni) {
+    const Node& nd = c->nodes[ni];
+    if (nd.descendants != 0) continue;
+    const int64_t ip = nd.particle;
+    const int64_t io = c->perm[ip];
+    const Adj& a = adj[ni];
+    dLdq[io] = a.q + a.A * sgn(c->q[ip]);
+    dLdx[io] = a.c[0];
+    dLdy[io] = a.c[1];
+    dLdz[io] = a.c[2];
+  }
+  return 0;
+}
+
+// FP64 direct-sum gradient of sum_t (gphi phi_t + gE . E_t) over the grown
+// particles (no tree), in the caller's original order.
+int orc_direct_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double* ty,
+                       const double* tz, const double* gex, const double* gey, const double* gez,
+                       const double* gphi, double* dLdq, double* dLdx, double* dLdy, double* dLdz) {
+  auto boxes = neighbour_boxes(c->p);
+  const int64_t n = c->n;
+  int nth = std::max(1, c->p.num_threads);
+  parallel_for(n, nth, [&](int64_t j, int) {
+    Adj a;
+    for (int64_t i = 0; i < nt; ++i) {
+      const double gE[3] = {gex[i], gey[i], gez[i]};
+      for (auto& bx : boxes) {
+        double vb[3];
+        lattice_vect(c->p, bx, vb);
+        const double d[3] = {(tx[i] - vb[0]) - c->x[j], (ty[i] - vb[1]) - c->y[j],
+                             (tz[i] - vb[2]) - c->z[j]};
+        if (d[0] == 0.0 && d[1] == 0.0 && d[2] == 0.0) continue;
+        leaf_adjoint(c->q[j], d, c->p.eps2, gphi[i], gE, a);
+      }
+    }
+    const int64_t io = c->perm[j];
+    dLdq[io] = a.q;
+    dLdx[io] = a.c[0];
+    dLdy[io] = a.c[1];
+    dLdz[io] = a.c[2];
+  });
   return 0;
 }
 

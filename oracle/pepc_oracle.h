@@ -91,6 +91,17 @@ void orc_counters(const orc_ctx* c, int64_t out[2]);
  * mirror boxes and, if periodic with far field, the lattice term. */
 int orc_direct(orc_ctx* c, int64_t ntest, const int64_t* tidx, double* ex, double* ey,
                double* ez, double* pot);
+/* adjoint of the per-target walk with fixed interaction lists: dL/dq, dL/dx
+ * of the grown particles (original order) for given dL/dE (gex..) and dL/dphi
+ * at nt targets; open boundaries only (returns -5 otherwise) */
+int orc_traverse_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double* ty,
+                         const double* tz, const double* gex, const double* gey,
+                         const double* gez, const double* gphi, double* dLdq, double* dLdx,
+                         double* dLdy, double* dLdz);
+/* the same gradient by FP64 direct summation (no tree) */
+int orc_direct_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double* ty,
+                       const double* tz, const double* gex, const double* gey, const double* gez,
+                       const double* gphi, double* dLdq, double* dLdx, double* dLdy, double* dLdz);
 /* install lattice coefficients (861 complex as interleaved re, im) before grow */
 int orc_set_lattice_coefficients(orc_ctx* c, const double* re_im);
 /* periodic lattice term alone for arbitrary positions (fmm_sum_lattice_force) */

@@ -112,6 +112,7 @@ EXPORTS = [
     "pepcg_tree_export", "pepcg_direct", "pepcg_lattice", "pepcg_multipole_from_particle",
     "pepcg_shift_multipoles_up", "pepcg_force_with_leaf", "pepcg_force_with_twig", "pepcg_mac",
     "pepcg_set_stream", "pepcg_kernel_launches", "pepcg_sort_keys_noalloc",
+    "pepcg_traverse_adjoint", "pepcg_traverse_adjoint_device",
 ]
 
 _LIB = None
@@ -142,6 +143,8 @@ def lib():
     L.pepcg_timber_tree.argtypes = [VP]
     L.pepcg_set_stream.argtypes = [VP, VP]
     L.pepcg_sort_keys_noalloc.argtypes = [C.c_int64, VP, VP, VP, VP]
+    L.pepcg_traverse_adjoint.argtypes = [VP, C.c_int64, D, D, D, D, D, D, D, D, D, D, D]
+    L.pepcg_traverse_adjoint_device.argtypes = [VP, C.c_int64] + [VP] * 11
     L.pepcg_kernel_launches.argtypes = []
     L.pepcg_kernel_launches.restype = C.c_longlong
     L.pepcg_stats_get.argtypes = [VP, C.POINTER(Stats)]
@@ -287,8 +290,17 @@ class TreeCode:
             self._h, _tptr(key), _tptr(perm), _tptr(x), _tptr(y), _tptr(z), _tptr(q)))
 
     def set_stream(self, stream_ptr):
-        """Launch on an external cudaStream_t (int pointer), or a private stream for None."""
-        self._check(lib().pepcg_set_stream(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
+        """Launch on an external cudaStream_t (int handle, e.g. torch's
+        ``Stream.cuda_stream``); 0 is the legacy default stream (passed on as
+        cudaStreamLegacy, since NULL asks the library for a private stream);
+        None selects a private stream."""
+        if stream_ptr is None:
+            h = None
+        elif stream_ptr == 0:
+            h = C.c_void_p(1)  # cudaStreamLegacy
+        else:
+            h = C.c_void_p(stream_ptr)
+        self._check(lib().pepcg_set_stream(self._h, h))
 
     # -- diagnostics
     def stats(self):
@@ -314,6 +326,21 @@ class TreeCode:
         ex, ey, ez, pt = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(n)
         self._check(lib().pepcg_direct(self._h, n, _ip(tidx), _dp(ex), _dp(ey), _dp(ez), _dp(pt)))
         return dict(ex=ex, ey=ey, ez=ez, pot=pt)
+
+    def traverse_adjoint(self, x, y, z, dLdE, dLdphi, npart):
+        """dL/dq, dL/dx of the grown particles (caller's original order) for
+        dL/dE = (3 arrays) and dL/dphi at the targets x, y, z."""
+        nt = len(x)
+        args = [_f64(v) for v in (x, y, z, dLdE[0], dLdE[1], dLdE[2], dLdphi)]
+        out = [np.zeros(npart) for _ in range(4)]
+        self._check(lib().pepcg_traverse_adjoint(self._h, nt, *[_dp(a) for a in args],
+                                                 *[_dp(o) for o in out]))
+        return dict(q=out[0], x=out[1], y=out[2], z=out[3])
+
+    def traverse_adjoint_device(self, x, y, z, dLdE, dLdphi, dq, dx, dy, dz):
+        """traverse_adjoint on torch CUDA float64 tensors; dq..dz are overwritten."""
+        ptrs = [_tptr(t) for t in (x, y, z, dLdE[0], dLdE[1], dLdE[2], dLdphi, dq, dx, dy, dz)]
+        return self._check(lib().pepcg_traverse_adjoint_device(self._h, x.numel(), *ptrs))
 
     def lattice(self, x, y, z):
         n = len(x)

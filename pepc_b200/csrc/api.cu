@@ -58,6 +58,7 @@ template bool ensure<unsigned long long>(Ctx*, DBuf<unsigned long long>&, size_t
 template bool ensure<double4>(Ctx*, DBuf<double4>&, size_t, const char*);
 template bool ensure<double2>(Ctx*, DBuf<double2>&, size_t, const char*);
 template bool ensure<int2>(Ctx*, DBuf<int2>&, size_t, const char*);
+template bool ensure<int4>(Ctx*, DBuf<int4>&, size_t, const char*);
 
 template <class T>
 static void release(DBuf<T>& b) {
@@ -338,7 +339,8 @@ int pepcg_destroy(void* ctx) {
   release(c->nc4); release(c->meta); release(c->fwd); release(c->mom); release(c->aux);
   release(c->mom32);
   release(c->parent); release(c->nchild); release(c->upcnt); release(c->first_part);
-  release(c->nleaves); release(c->fpo2rpo); release(c->rpo2fpo); release(c->nkey);
+  release(c->nleaves); release(c->child8); release(c->wstack); release(c->leafnode);
+  release(c->adj); release(c->fpo2rpo); release(c->rpo2fpo); release(c->nkey);
   release(c->tiles); release(c->counters); release(c->tgt); release(c->tkeys);
   for (void* p : {(void*)c->d_box, (void*)c->d_status, (void*)c->d_small, (void*)c->d_vbox,
                   (void*)c->d_part, (void*)c->d_mlattice, (void*)c->d_omega, (void*)c->d_mu,
@@ -382,15 +384,7 @@ int pepcg_grow_tree_device(void* ctx, int64_t n, const double* d_x, const double
     rc = lattice_timestep(c);
     if (rc && rc != PEPCG_WARN_NOT_NEUTRAL) return rc;
   }
-  float ms = 0;
-  cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
-  c->st.t_keys_ms = ms;
-  cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]);
-  c->st.t_sort_ms = ms;
-  cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
-  c->st.t_tree_ms = ms;
-  cudaEventElapsedTime(&ms, c->ev[3], c->ev[4]);
-  c->st.t_upward_ms = ms;
+  c->grow_times_pending = true;  // read the phase events later, without a sync here
   return rc;
 }
 
@@ -535,6 +529,51 @@ int pepcg_set_stream(void* ctx, void* stream) {
 
 long long pepcg_kernel_launches(void) { return g_launches.load(); }
 
+int pepcg_traverse_adjoint_device(void* ctx, int64_t nt, const double* d_tx, const double* d_ty,
+                                  const double* d_tz, const double* d_gex, const double* d_gey,
+                                  const double* d_gez, const double* d_gphi, double* d_dq,
+                                  double* d_dx, double* d_dy, double* d_dz) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || nt < 0 || !d_tx || !d_ty || !d_tz || !d_gex || !d_gey || !d_gez || !d_gphi || !d_dq ||
+      !d_dx || !d_dy || !d_dz)
+    return PEPCG_ERR_BAD_ARG;
+  cudaSetDevice(c->device);
+  return adjoint_device(c, nt, d_tx, d_ty, d_tz, d_gex, d_gey, d_gez, d_gphi, d_dq, d_dx, d_dy, d_dz);
+}
+
+int pepcg_traverse_adjoint(void* ctx, int64_t nt, const double* tx, const double* ty,
+                           const double* tz, const double* dLdEx, const double* dLdEy,
+                           const double* dLdEz, const double* dLdphi, double* dLdq, double* dLdx,
+                           double* dLdy, double* dLdz) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || nt < 0 || !tx || !ty || !tz || !dLdEx || !dLdEy || !dLdEz || !dLdphi || !dLdq ||
+      !dLdx || !dLdy || !dLdz)
+    return PEPCG_ERR_BAD_ARG;
+  if (!c->has_tree) {
+    c->err = "no grown tree";
+    return PEPCG_ERR_NO_TREE;
+  }
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  const int64_t n = c->n;
+  if (!ensure(c, c->tgt, 7 * nt + 4 * n, "adjoint staging")) return PEPCG_ERR_OOM;
+  double* b = c->tgt.p;
+  const double* hin[7] = {tx, ty, tz, dLdEx, dLdEy, dLdEz, dLdphi};
+  bool ok = true;
+  for (int k = 0; k < 7; ++k)
+    ok = ok && cuda_ok(c, cudaMemcpyAsync(b + k * nt, hin[k], nt * 8, cudaMemcpyHostToDevice, s), "H2D");
+  if (!ok) return PEPCG_ERR_CUDA;
+  double* o = b + 7 * nt;
+  int rc = adjoint_device(c, nt, b, b + nt, b + 2 * nt, b + 3 * nt, b + 4 * nt, b + 5 * nt,
+                          b + 6 * nt, o, o + n, o + 2 * n, o + 3 * n);
+  if (rc) return rc;
+  double* hout[4] = {dLdq, dLdx, dLdy, dLdz};
+  for (int k = 0; k < 4; ++k)
+    ok = ok && cuda_ok(c, cudaMemcpyAsync(hout[k], o + k * n, n * 8, cudaMemcpyDeviceToHost, s), "D2H");
+  ok = ok && cuda_ok(c, cudaStreamSynchronize(s), "adjoint");
+  return ok ? PEPCG_OK : PEPCG_ERR_CUDA;
+}
+
 int pepcg_timber_tree(void* ctx) {
   Ctx* c = as_ctx(ctx);
   if (!c) return PEPCG_ERR_BAD_ARG;
@@ -545,6 +584,14 @@ int pepcg_timber_tree(void* ctx) {
 int pepcg_stats_get(void* ctx, pepcg_stats* s) {
   Ctx* c = as_ctx(ctx);
   if (!c || !s) return PEPCG_ERR_BAD_ARG;
+  if (c->grow_times_pending && cudaEventSynchronize(c->ev[4]) == cudaSuccess) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]) == cudaSuccess) c->st.t_keys_ms = ms;
+    if (cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]) == cudaSuccess) c->st.t_sort_ms = ms;
+    if (cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]) == cudaSuccess) c->st.t_tree_ms = ms;
+    if (cudaEventElapsedTime(&ms, c->ev[3], c->ev[4]) == cudaSuccess) c->st.t_upward_ms = ms;
+    c->grow_times_pending = false;
+  }
   c->st.npart = c->n;
   c->st.nleaf = c->n;
   c->st.ntwig = c->ntwig;

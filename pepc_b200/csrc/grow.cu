@@ -7,6 +7,7 @@
 // IEEE evaluation of the reference's expressions.
 
 #include <mutex>
+#include <utility>
 #include <string>
 
 #include "internal.cuh"
@@ -64,17 +65,19 @@ __global__ void k_bbox_partial(int64_t n, const double* __restrict__ x,
 // final reduction + margin (module_box.f90:71-84) + boxlength2 (module_tree.f90:196-201)
 __global__ void k_bbox_final(int nparts, const double* __restrict__ part, int cubic,
                              double* __restrict__ box) {
-  if (threadIdx.x != 0) return;
-  double lo[3], hi[3];
-  for (int d = 0; d < 3; ++d) {
-    lo[d] = part[d];
-    hi[d] = part[3 + d];
-  }
-  for (int b = 1; b < nparts; ++b)
+  const int lane = threadIdx.x;  // one warp
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int b = lane; b < nparts; b += 32)
     for (int d = 0; d < 3; ++d) {
       lo[d] = fmin(lo[d], part[b * 6 + d]);
       hi[d] = fmax(hi[d], part[b * 6 + 3 + d]);
     }
+  for (int d = 0; d < 3; ++d)
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+      hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+    }
+  if (lane != 0) return;
   if (cubic) {
     double l = fmin(lo[0], fmin(lo[1], lo[2])), h = fmax(hi[0], fmax(hi[1], hi[2]));
     for (int d = 0; d < 3; ++d) {
@@ -140,23 +143,56 @@ __device__ __forceinline__ uint64_t morton3d(int64_t i0, int64_t i1, int64_t i2)
   return key;
 }
 
+// The reference's Hilbert recursion (module_spacefilling.f90:380-440) keeps
+// three transformed coordinates; every exchange / reverse step permutes and
+// complements their remaining bits, so the transform applied so far is a
+// signed permutation of the axes (at most 48 states).  HilbertTable holds, for
+// every (state, raw octant of the original coordinates), the key digit and the
+// next state, built on the host by running the reference's own exchange and
+// reverse rules (hilbert_table() below); one lookup per level then reproduces
+// the reference's key bit for bit.
+struct HilbertTable {
+  uint16_t e[48 * 8];  // digit | next_state << 3
+};
+
 __global__ void k_keys(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
                        const double* __restrict__ z, const double* __restrict__ box, int curve,
-                       uint64_t* __restrict__ keys, int32_t* __restrict__ idx) {
+                       HilbertTable tab, uint64_t* __restrict__ keys, int32_t* __restrict__ idx) {
   __shared__ double sb[6];
+  __shared__ uint16_t st[48 * 8];
   if (threadIdx.x < 3) {
     sb[threadIdx.x] = box[threadIdx.x];
     // s = boxsize / 2**maxlevel (module_spacefilling.f90:238), exact
     sb[3 + threadIdx.x] = box[6 + threadIdx.x] / 1048576.0;
   }
+  for (int i = threadIdx.x; i < 48 * 8; i += blockDim.x) st[i] = tab.e[i];
   __syncthreads();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     // coord_to_intcoord_with_refinement_length (:218): int() truncates
-    int64_t i0 = __double2ll_rz((x[i] - sb[0]) / sb[3]);
-    int64_t i1 = __double2ll_rz((y[i] - sb[1]) / sb[4]);
-    int64_t i2 = __double2ll_rz((z[i] - sb[2]) / sb[5]);
-    keys[i] = curve == PEPCG_CURVE_MORTON ? morton3d(i0, i1, i2) : hilbert3d(i0, i1, i2);
+    const int64_t i0 = __double2ll_rz((x[i] - sb[0]) / sb[3]);
+    const int64_t i1 = __double2ll_rz((y[i] - sb[1]) / sb[4]);
+    const int64_t i2 = __double2ll_rz((z[i] - sb[2]) / sb[5]);
+    uint64_t key;
+    if (curve == PEPCG_CURVE_MORTON) {
+      key = morton3d(i0, i1, i2);
+    } else {
+      const unsigned a = (unsigned)i0, b = (unsigned)i1, c = (unsigned)i2;
+      unsigned state = 0;
+      unsigned hi = 1, lo = 0;  // key = hi:lo, placeholder bit first
+      uint64_t k = 1;
+#pragma unroll
+      for (int l = kMaxLevel - 1; l >= 0; --l) {
+        const unsigned o = (((c >> l) & 1u) << 2) | (((b >> l) & 1u) << 1) | ((a >> l) & 1u);
+        const unsigned ent = st[state * 8 + o];
+        k = (k << 3) | (ent & 7u);
+        state = ent >> 3;
+      }
+      (void)hi;
+      (void)lo;
+      key = k;
+    }
+    keys[i] = key;
     idx[i] = (int32_t)i;
   }
 }
@@ -521,7 +557,7 @@ __global__ void k_build_nodes(int64_t n, int64_t M, const int64_t* __restrict__ 
                               double4* __restrict__ nc4, int2* __restrict__ meta,
                               int32_t* __restrict__ fpo2rpo, int32_t* __restrict__ rpo2fpo,
                               int32_t* __restrict__ first_part, int32_t* __restrict__ nleaves,
-                              int64_t* __restrict__ nkey) {
+                              int64_t* __restrict__ nkey, int32_t* __restrict__ leafnode) {
   for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < n;
        s += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t ks = (uint64_t)key[s];
@@ -545,7 +581,10 @@ __global__ void k_build_nodes(int64_t n, int64_t M, const int64_t* __restrict__ 
       first_part[rpo] = (int32_t)s;
       nleaves[rpo] = (int32_t)(e - s + 1);
       nkey[rpo] = (int64_t)prefix;
-      if (leaf) nc4[rpo] = make_double4(x[s], y[s], z[s], q[s]);
+      if (leaf) {
+        nc4[rpo] = make_double4(x[s], y[s], z[s], q[s]);
+        leafnode[s] = (int32_t)rpo;
+      }
     }
   }
 }
@@ -554,7 +593,8 @@ __global__ void k_build_nodes(int64_t n, int64_t M, const int64_t* __restrict__ 
 __global__ void k_link(int64_t M, const int2* __restrict__ meta,
                        const int32_t* __restrict__ rpo2fpo, const int32_t* __restrict__ fpo2rpo,
                        int2* __restrict__ fwd, int32_t* __restrict__ parent,
-                       int32_t* __restrict__ nchild, int32_t* __restrict__ upcnt) {
+                       int32_t* __restrict__ nchild, int32_t* __restrict__ upcnt,
+                       int4* __restrict__ child8) {
   for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < M;
        u += (int64_t)gridDim.x * blockDim.x) {
     int2 mu = meta[u];
@@ -568,11 +608,15 @@ __global__ void k_link(int64_t M, const int2* __restrict__ meta,
     if (u == 0) parent[0] = -1;
     if (!leaf) {
       int cnt = 0;
+      int ch[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
       for (int64_t c = u + 1; c < mu.x; c = meta[c].x) {
         parent[c] = (int32_t)u;
+        if (cnt < 8) ch[cnt] = (int)c;
         ++cnt;
       }
       nchild[u] = cnt;
+      child8[2 * u] = make_int4(ch[0], ch[1], ch[2], ch[3]);
+      child8[2 * u + 1] = make_int4(ch[4], ch[5], ch[6], ch[7]);
     } else {
       nchild[u] = 0;
     }
@@ -637,6 +681,90 @@ __global__ void k_upward(int64_t M, const int2* __restrict__ meta, const int32_t
   }
 }
 
+// Level-synchronous variant of the upward pass: one launch per level, deepest
+// first; one thread per twig of that level computes it from its children (in
+// key order: the RPO chain u+1, skip.. lists them last to first).  No fences,
+// no atomics; every child of a level-L twig was finished by an earlier launch.
+__global__ void __launch_bounds__(256) k_upward_level(int64_t M, int level,
+                                                      const int2* __restrict__ meta,
+                                                      double4* __restrict__ nc4,
+                                                      double* __restrict__ mom,
+                                                      double2* __restrict__ aux) {
+  // shift_up64 streamed over the children (key order = reverse RPO chain):
+  // the same additions in the same order, with the child data re-read from
+  // L1 on every pass instead of held in registers
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < M;
+       u += (int64_t)gridDim.x * blockDim.x) {
+    const int2 mu = meta[u];
+    if ((mu.y & kLeafFlag) || (mu.y & 0xff) != level) continue;
+    int ch[8];
+    int nc = 0;
+    for (int64_t c = u + 1; c < mu.x && nc < 8; c = meta[c].x) ch[nc++] = (int)c;
+    auto absq_of = [&](int c, double q) {
+      return (meta[c].y & kLeafFlag) ? fabs(q) : aux[c].x;
+    };
+    double charge = 0.0, absq = 0.0;
+    for (int k = nc - 1; k >= 0; --k) charge = charge + nc4[ch[k]].w;
+    for (int k = nc - 1; k >= 0; --k) absq = absq + absq_of(ch[k], nc4[ch[k]].w);
+    double cx = 0.0, cy = 0.0, cz = 0.0;
+    if (absq != 0.0) {
+      for (int k = nc - 1; k >= 0; --k) {
+        const double4 a = nc4[ch[k]];
+        const double w = absq_of(ch[k], a.w);
+        cx = cx + a.x * w;
+        cy = cy + a.y * w;
+        cz = cz + a.z * w;
+      }
+      cx = cx / absq;
+      cy = cy / absq;
+      cz = cz / absq;
+    } else {
+      for (int k = nc - 1; k >= 0; --k) {
+        const double4 a = nc4[ch[k]];
+        cx = cx + a.x;
+        cy = cy + a.y;
+        cz = cz + a.z;
+      }
+      cx = cx / (double)nc;
+      cy = cy / (double)nc;
+      cz = cz / (double)nc;
+    }
+    double d0 = 0, d1 = 0, d2 = 0, q0 = 0, q1 = 0, q2 = 0, xy = 0, yz = 0, zx = 0;
+    for (int k = nc - 1; k >= 0; --k) {
+      const int c = ch[k];
+      const double4 a = nc4[c];
+      const bool leafc = (meta[c].y & kLeafFlag) != 0;
+      double m[9];
+#pragma unroll
+      for (int j = 0; j < 9; ++j) m[j] = leafc ? 0.0 : mom[9 * (int64_t)c + j];
+      const double s0 = cx - a.x, s1 = cy - a.y, s2 = cz - a.z;
+      const double q = a.w;
+      d0 = (d0 + m[0]) + q * s0;
+      d1 = (d1 + m[1]) + q * s1;
+      d2 = (d2 + m[2]) + q * s2;
+      q0 = ((q0 + m[3]) + m[0] * s0) + (0.5 * q) * (s0 * s0);
+      q1 = ((q1 + m[4]) + m[1] * s1) + (0.5 * q) * (s1 * s1);
+      q2 = ((q2 + m[5]) + m[2] * s2) + (0.5 * q) * (s2 * s2);
+      xy = (((xy + m[6]) + m[0] * s1) + m[1] * s0) + (q * s0) * s1;
+      yz = (((yz + m[7]) + m[1] * s2) + m[2] * s1) + (q * s1) * s2;
+      zx = (((zx + m[8]) + m[2] * s0) + m[0] * s2) + (q * s2) * s0;
+    }
+    double bmax = 0.0;
+    for (int k = nc - 1; k >= 0; --k) {
+      const int c = ch[k];
+      const double4 a = nc4[c];
+      const double bc = (meta[c].y & kLeafFlag) ? 0.0 : aux[c].y;
+      const double e0 = cx - a.x, e1 = cy - a.y, e2 = cz - a.z;
+      const double v = sqrt((e0 * e0 + e1 * e1) + e2 * e2) + bc;
+      if (k == nc - 1 || v > bmax) bmax = v;
+    }
+    nc4[u] = make_double4(cx, cy, cz, charge);
+    aux[u] = make_double2(absq, bmax);
+    double* o = mom + 9 * u;
+    o[0] = d0; o[1] = d1; o[2] = d2; o[3] = q0; o[4] = q1; o[5] = q2; o[6] = xy; o[7] = yz; o[8] = zx;
+  }
+}
+
 // FP32 copy of the twig moments for the mixed walk, packed as three float4:
 // (px, py, pz, qxx), (qyy, qzz, qxy/2, qyz/2), (qzx/2, qxx+qyy+qzz, charge, 0)
 __global__ void k_mom32(int64_t M, const int2* __restrict__ meta, const double* __restrict__ mom,
@@ -650,6 +778,45 @@ __global__ void k_mom32(int64_t M, const int2* __restrict__ meta, const double* 
     mom32[3 * u + 1] = make_float4((float)m[4], (float)m[5], (float)(0.5 * m[6]), (float)(0.5 * m[7]));
     mom32[3 * u + 2] = make_float4((float)(0.5 * m[8]), (float)((m[3] + m[4]) + m[5]), (float)q, 0.f);
   }
+}
+
+// The reference's exchange / reverse rules (module_spacefilling.f90:389-438)
+// applied to a (permutation, flip) state: slot j of the transformed
+// coordinates holds original axis perm[j], complemented when flip bit j is set.
+HilbertTable hilbert_table() {
+  static const int CI3[8] = {0, 1, 3, 2, 7, 6, 4, 5};
+  static const int G3x[8] = {5, 6, 0, 5, 5, 0, 6, 5};
+  static const int G3r[8] = {0, 0, 0, 5, 0, 0, 6, 5};
+  static const int perms[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+  auto pidx = [&](const int* p) {
+    for (int k = 0; k < 6; ++k)
+      if (perms[k][0] == p[0] && perms[k][1] == p[1] && perms[k][2] == p[2]) return k;
+    return 0;
+  };
+  HilbertTable t{};
+  for (int pi = 0; pi < 6; ++pi)
+    for (int f = 0; f < 8; ++f)
+      for (int o = 0; o < 8; ++o) {
+        const int r[3] = {o & 1, (o >> 1) & 1, (o >> 2) & 1};
+        int b[3];
+        for (int j = 0; j < 3; ++j) b[j] = r[perms[pi][j]] ^ ((f >> j) & 1);
+        const int cval = (b[2] << 2) | (b[1] << 1) | b[0];
+        const int h = CI3[cval];
+        int p2[3] = {perms[pi][0], perms[pi][1], perms[pi][2]};
+        int fl[3] = {f & 1, (f >> 1) & 1, (f >> 2) & 1};
+        if (G3x[h] == 5) {
+          std::swap(p2[0], p2[2]);
+          std::swap(fl[0], fl[2]);
+        } else if (G3x[h] == 6) {
+          std::swap(p2[1], p2[2]);
+          std::swap(fl[1], fl[2]);
+        }
+        for (int j = 0; j < 3; ++j) fl[j] ^= (G3r[h] >> j) & 1;
+        const int nf = fl[0] | (fl[1] << 1) | (fl[2] << 2);
+        const int ns = pidx(p2) * 8 + nf;
+        t.e[(pi * 8 + f) * 8 + o] = (uint16_t)(h | (ns << 3));
+      }
+  return t;
 }
 
 inline unsigned grid_for(int64_t n, int threads = kThreads) {
@@ -689,7 +856,8 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
       !ensure(c, c->orig_key, n, "orig_key") || !ensure(c, c->dup_list, dupcap, "dup_list") ||
       !ensure(c, c->lev, n, "lev") || !ensure(c, c->lcpn, n, "lcpn") ||
       !ensure(c, c->cstart, n, "cstart") || !ensure(c, c->cend, n, "cend") ||
-      !ensure(c, c->sstart, n, "sstart") || !ensure(c, c->send, n, "send"))
+      !ensure(c, c->sstart, n, "sstart") || !ensure(c, c->send, n, "send") ||
+      !ensure(c, c->leafnode, n, "leafnode"))
     return PEPCG_ERR_OOM;
 
   if (!cuda_ok(c, cudaMemsetAsync(c->d_status, 0, sizeof(uint32_t), s), "memset status") ||
@@ -706,7 +874,8 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
   k_bbox_final<<<1, 32, 0, s>>>(nbb, part, c->prm.force_cubic_domain, c->d_box);
   // keys
   COUNT_LAUNCH();
-  k_keys<<<grid_for(n), kThreads, 0, s>>>(n, dx, dy, dz, c->d_box, c->prm.curve, c->skey.p,
+  static const HilbertTable htab = hilbert_table();
+  k_keys<<<grid_for(n), kThreads, 0, s>>>(n, dx, dy, dz, c->d_box, c->prm.curve, htab, c->skey.p,
                                           c->sval.p);
   cudaEventRecord(c->ev[1], s);
   // sort: 8 LSD passes of 8 bits
@@ -753,7 +922,8 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
                "box") ||
       !cuda_ok(c, cudaMemcpyAsync(c->boxlength2, c->d_box + 9, 21 * sizeof(double),
                                   cudaMemcpyDeviceToHost, s), "box") ||
-      !cuda_ok(c, cudaMemcpyAsync(&c->dup_count, c->d_small, 8, cudaMemcpyDeviceToHost, s), "dup"))
+      !cuda_ok(c, cudaMemcpyAsync(&c->dup_count, c->d_small, 8, cudaMemcpyDeviceToHost, s), "dup") ||
+      !cuda_ok(c, cudaMemcpyAsync(&c->max_level, c->d_small + 2, 4, cudaMemcpyDeviceToHost, s), "maxlev"))
     return PEPCG_ERR_CUDA;
   uint32_t st = 0;
   if (!cuda_ok(c, cudaMemcpyAsync(&st, c->d_status, 4, cudaMemcpyDeviceToHost, s), "status") ||
@@ -772,20 +942,27 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
       !ensure(c, c->parent, M, "parent") || !ensure(c, c->nchild, M, "nchild") ||
       !ensure(c, c->upcnt, M, "upcnt") || !ensure(c, c->first_part, M, "first_part") ||
       !ensure(c, c->nleaves, M, "nleaves") || !ensure(c, c->fpo2rpo, M, "fpo2rpo") ||
-      !ensure(c, c->rpo2fpo, M, "rpo2fpo") || !ensure(c, c->nkey, M, "nkey"))
+      !ensure(c, c->rpo2fpo, M, "rpo2fpo") || !ensure(c, c->nkey, M, "nkey") ||
+      !ensure(c, c->child8, 2 * M, "child8"))
     return PEPCG_ERR_OOM;
   COUNT_LAUNCH();
   k_build_nodes<<<grid_for(n), kThreads, 0, s>>>(n, M, c->key.p, c->lev.p, c->lcpn.p, c->sstart.p,
                                                   c->send.p, c->x.p, c->y.p, c->z.p, c->q.p,
                                                   c->nc4.p, c->meta.p, c->fpo2rpo.p, c->rpo2fpo.p,
-                                                  c->first_part.p, c->nleaves.p, c->nkey.p);
+                                                  c->first_part.p, c->nleaves.p, c->nkey.p,
+                                                  c->leafnode.p);
   COUNT_LAUNCH();
   k_link<<<grid_for(M), kThreads, 0, s>>>(M, c->meta.p, c->rpo2fpo.p, c->fpo2rpo.p, c->fwd.p,
-                                          c->parent.p, c->nchild.p, c->upcnt.p);
+                                          c->parent.p, c->nchild.p, c->upcnt.p, c->child8.p);
   cudaEventRecord(c->ev[3], s);
-  COUNT_LAUNCH();
-  k_upward<<<grid_for(M), kThreads, 0, s>>>(M, c->meta.p, c->parent.p, c->nchild.p, c->upcnt.p,
-                                            c->nc4.p, c->mom.p, c->aux.p);
+  // the deepest twig level is one above the deepest leaf level
+  {
+    const int maxlev = c->max_level;
+    for (int L = maxlev - 1; L >= 0; --L) {
+      COUNT_LAUNCH();
+      k_upward_level<<<grid_for(M), kThreads, 0, s>>>(M, L, c->meta.p, c->nc4.p, c->mom.p, c->aux.p);
+    }
+  }
   COUNT_LAUNCH();
   k_mom32<<<grid_for(M), kThreads, 0, s>>>(M, c->meta.p, c->mom.p, c->nc4.p,
                                            reinterpret_cast<float4*>(c->mom32.p));
@@ -794,10 +971,7 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
   c->n = n;
   c->nnodes = M;
   c->ntwig = M - n;
-  int maxl = 0;
-  cudaMemcpyAsync(&maxl, c->d_small + 2, 4, cudaMemcpyDeviceToHost, s);
-  cudaStreamSynchronize(s);
-  c->max_level = maxl;
+
   c->has_tree = true;
   return PEPCG_OK;
 }

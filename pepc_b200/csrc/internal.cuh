@@ -90,6 +90,10 @@ struct Ctx {
   DBuf<double2> aux;
   DBuf<float> mom32;  // 12 * nnodes (coc-relative moments in FP32, padded)
   DBuf<int32_t> parent, nchild, upcnt, first_part, nleaves;
+  DBuf<int4> child8;  // up to 8 children (RPO indices) per twig, as 2 x int4
+  DBuf<int32_t> wstack;  // per-warp traversal stacks of the wide group walk
+  DBuf<int32_t> leafnode;  // key-ordered particle -> RPO index of its leaf
+  DBuf<double> adj;        // adjoint records, 16 doubles per node
   DBuf<int32_t> fpo2rpo, rpo2fpo;
   DBuf<int64_t> nkey;
   // walk scratch
@@ -121,6 +125,7 @@ struct Ctx {
   // statistics
   pepcg_stats st{};
   cudaEvent_t ev[8];
+  bool grow_times_pending = false;
 
   int32_t* nleaves_ptr() { return nleaves.p; }
 };
@@ -149,6 +154,11 @@ int host_tiles(Ctx* c, int64_t nt, const int64_t* d_tkeys, int T, int2* d_tiles,
 int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                     const int64_t* tkeys, bool self, double* ex, double* ey, double* ez,
                     double* pot, double* work);
+
+// ---- adjoint.cu ----
+int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
+                   const double* gex, const double* gey, const double* gez, const double* gphi,
+                   double* dq, double* dx, double* dy, double* dz);
 
 // ---- lattice.cu ----
 int lattice_prepare(Ctx* c);

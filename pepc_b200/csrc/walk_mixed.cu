@@ -50,6 +50,7 @@ struct MixArgs {
   int nbox;
   float theta2;
   float eps2;
+  double theta2_64;
   int32_t M;
   int64_t npart;
   double* ex;
@@ -208,6 +209,385 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_group_mixed(MixArgs A) {
   warp_add3(A.counters, c_leaf, c_twig, c_mac);
 }
 
+// Group walk in two phases per warp.
+//  Phase A (traversal): the warp walks the RPO node order; at a twig every
+//    lane evaluates the Barnes-Hut MAC in FP64 and the twig is accepted only if
+//    all lanes pass (module_tree_walk_simple.f90:343-382 semantics).  Accepted
+//    twigs and reached leaves are appended to per-warp shared-memory lists.
+//  Phase B (evaluation): the listed nodes are staged 32 at a time, lane k
+//    loading node k's record (independent loads, one latency per batch), and
+//    every lane then evaluates all staged nodes from broadcast shared-memory
+//    reads.  Each batch's FP32 sums are added to the FP64 accumulators.
+constexpr int kListCap = 128;
+struct __align__(16) Staged {
+  double cx, cy, cz, q;  // coc (FP64) and charge
+  float4 m0, m1, m2;     // FP32 moments (twigs)
+};
+
+__global__ void __launch_bounds__(kMixThreads) k_walk_group_mixed_ab(MixArgs A) {
+  __shared__ double s_bl2[kMaxLevel + 1];
+  __shared__ double s_vb[3 * 125];
+  __shared__ int s_tw[kMixThreads / 32][kListCap];
+  __shared__ int s_lf[kMixThreads / 32][kListCap];
+  __shared__ Staged s_st[kMixThreads / 32][32];
+  for (int i = threadIdx.x; i <= kMaxLevel; i += blockDim.x) s_bl2[i] = A.bl2[i];
+  for (int i = threadIdx.x; i < 3 * A.nbox; i += blockDim.x) s_vb[i] = A.vbox[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int* tw = s_tw[w];
+  int* lf = s_lf[w];
+  Staged* st = s_st[w];
+  const unsigned M = (unsigned)A.M;
+  const double theta2 = (double)A.theta2_64;
+  const int64_t nbuckets = A.tiles ? A.ntiles : (A.nt + 31) / 32;
+  unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
+  for (;;) {
+    unsigned b = 0;
+    if (lane == 0) b = atomicAdd(&g_bucket_counter_mixed, 1u);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    if ((int64_t)b >= nbuckets) break;
+    int64_t t0;
+    int cnt;
+    if (A.tiles) {
+      const int2 tl = A.tiles[b];
+      t0 = tl.x;
+      cnt = tl.y;
+    } else {
+      t0 = (int64_t)b * 32;
+      cnt = (int)min((int64_t)32, A.nt - t0);
+    }
+    const bool valid = lane < cnt;
+    const int64_t t = t0 + lane;
+    double px = 0, py = 0, pz = 0;
+    double E0 = 0, E1 = 0, E2 = 0, PH = 0, W = 0;
+    if (valid) {
+      px = A.tx[t]; py = A.ty[t]; pz = A.tz[t];
+      E0 = A.ex[t]; E1 = A.ey[t]; E2 = A.ez[t]; PH = A.pot[t]; W = A.work[t];
+    }
+    bool complete = true;
+    for (int ib = 0; ib < A.nbox; ++ib) {
+      const double sx = px - s_vb[3 * ib], sy = py - s_vb[3 * ib + 1], sz = pz - s_vb[3 * ib + 2];
+      int64_t partner = 0;
+      unsigned u = 0;
+      while (u < M) {
+        // ---- phase A: fill the lists
+        int nt_ = 0, nl_ = 0;
+        while (u < M && nt_ < kListCap && nl_ < kListCap) {
+          const double4 a = A.nc4[u];
+          const int2 mu = A.meta[u];
+          if (mu.y & kLeafFlag) {
+            if (lane == 0) lf[nl_] = (int)u;
+            ++nl_;
+            partner += 1;
+            u = u + 1;
+          } else {
+            const double dx = sx - a.x, dy = sy - a.y, dz = sz - a.z;
+            const double d2 = (dx * dx + dy * dy) + dz * dz;
+            const bool ok = !valid || (theta2 * d2 > s_bl2[mu.y & 0xff]);
+            const unsigned fail = __ballot_sync(0xffffffffu, !ok);
+            const int first_fail = fail ? __ffs(fail) - 1 : 32;
+            if (valid && lane <= first_fail) ++c_mac;
+            if (fail == 0) {
+              if (lane == 0) tw[nt_] = (int)u;
+              ++nt_;
+              partner += A.nleaves[u];
+              u = (unsigned)mu.x;
+            } else {
+              u = u + 1;
+            }
+          }
+        }
+        __syncwarp();
+        W += (double)(nt_ + nl_);
+        // ---- phase B: twigs
+        for (int base = 0; base < nt_; base += 32) {
+          const int k = base + lane;
+          if (k < nt_) {
+            const int nd = tw[k];
+            const double4 a = A.nc4[nd];
+            Staged sv;
+            sv.cx = a.x; sv.cy = a.y; sv.cz = a.z; sv.q = a.w;
+            sv.m0 = A.mom32[3 * (int64_t)nd];
+            sv.m1 = A.mom32[3 * (int64_t)nd + 1];
+            sv.m2 = A.mom32[3 * (int64_t)nd + 2];
+            st[lane] = sv;
+          }
+          __syncwarp();
+          const int cntb = min(32, nt_ - base);
+          float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
+          if (valid) {
+            for (int j = 0; j < cntb; ++j) {
+              const double cx = st[j].cx, cy = st[j].cy, cz = st[j].cz;
+              const float dx = (float)(sx - cx), dy = (float)(sy - cy), dz = (float)(sz - cz);
+              twig32(st[j].m0, st[j].m1, st[j].m2, dx, dy, dz, A.eps2, ax, ay, az, ap);
+            }
+            c_twig += (unsigned)cntb;
+          }
+          E0 += (double)ax; E1 += (double)ay; E2 += (double)az; PH += (double)ap;
+          __syncwarp();
+        }
+        // ---- phase B: leaves
+        for (int base = 0; base < nl_; base += 32) {
+          const int k = base + lane;
+          if (k < nl_) {
+            const double4 a = A.nc4[lf[k]];
+            st[lane].cx = a.x; st[lane].cy = a.y; st[lane].cz = a.z; st[lane].q = a.w;
+          }
+          __syncwarp();
+          const int cntb = min(32, nl_ - base);
+          float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
+          if (valid) {
+            for (int j = 0; j < cntb; ++j) {
+              const double dx64 = sx - st[j].cx, dy64 = sy - st[j].cy, dz64 = sz - st[j].cz;
+              if (dx64 == 0.0 && dy64 == 0.0 && dz64 == 0.0) continue;  // self
+              leaf32((float)st[j].q, (float)dx64, (float)dy64, (float)dz64, A.eps2, ax, ay, az, ap);
+              ++c_leaf;
+            }
+          }
+          E0 += (double)ax; E1 += (double)ay; E2 += (double)az; PH += (double)ap;
+          __syncwarp();
+        }
+      }
+      if (partner != A.npart) complete = false;
+    }
+    if (valid) {
+      A.ex[t] = E0; A.ey[t] = E1; A.ez[t] = E2; A.pot[t] = PH; A.work[t] = W;
+    }
+    if (!complete && lane == 0) atomicOr(A.status, ST_INCOMPLETE);
+  }
+  warp_add3(A.counters, c_leaf, c_twig, c_mac);
+}
+
+// Group walk with a wide traversal (the default GROUP kernel).
+// The warp's 32 targets form the group; the traversal pops up to 32 nodes
+// from a per-warp LIFO stack (global memory) and lane k decides node k:
+//   leaf   -> queued for direct evaluation,
+//   twig   -> accepted if every target of the group passes the Barnes-Hut MAC
+//             (module_tree_walk_simple.f90:343-382 semantics), else its
+//             children (child8 table) are pushed.
+// The MAC uses the targets' offsets from the group centre in FP32; a bounding
+// sphere of the group gives a quick accept / quick open before the per-target
+// loop.  Queued twigs and leaves are evaluated 32 at a time from a shared
+// staging area (lane k loads node k, then every lane reads all of them), so
+// node loads never sit on the per-interaction dependency chain.
+// Stack bound: a pop takes <= 32 entries and pushes <= 8 per node, so the
+// stack never holds more than (kMaxLevel + 1) * 8 * 32 entries; kStackCap
+// leaves a margin and an overflow sets ST_INCOMPLETE instead of writing past it.
+constexpr int kStackCap = 8192;
+constexpr int kWW = kMixThreads / 32;  // warps per block
+
+__device__ __forceinline__ int warp_excl_scan(int v, int lane, int& total) {
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  total = __shfl_sync(0xffffffffu, x, 31);
+  return x - v;
+}
+
+__global__ void __launch_bounds__(kMixThreads) k_walk_group_wide(MixArgs A, int* __restrict__ gstack,
+                                                                 const int4* __restrict__ child8,
+                                                                 const int* __restrict__ nchild) {
+  __shared__ float s_bl2[kMaxLevel + 1];
+  __shared__ double s_vb[3 * 125];
+  __shared__ float4 s_t[kWW][32];
+  __shared__ int s_tw[kWW][64];
+  __shared__ int s_lf[kWW][64];
+  __shared__ Staged s_st[kWW][32];
+  for (int i = threadIdx.x; i <= kMaxLevel; i += blockDim.x) s_bl2[i] = (float)A.bl2[i];
+  for (int i = threadIdx.x; i < 3 * A.nbox; i += blockDim.x) s_vb[i] = A.vbox[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  int* stack = gstack + (int64_t)(blockIdx.x * kWW + w) * kStackCap;
+  float4* tt = s_t[w];
+  int* tw = s_tw[w];
+  int* lf = s_lf[w];
+  Staged* st = s_st[w];
+  const float theta2 = A.theta2;
+  const int64_t nbuckets = A.tiles ? A.ntiles : (A.nt + 31) / 32;
+  unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
+  for (;;) {
+    unsigned b = 0;
+    if (lane == 0) b = atomicAdd(&g_bucket_counter_mixed, 1u);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    if ((int64_t)b >= nbuckets) break;
+    int64_t t0;
+    int cnt;
+    if (A.tiles) {
+      const int2 tl = A.tiles[b];
+      t0 = tl.x;
+      cnt = tl.y;
+    } else {
+      t0 = (int64_t)b * 32;
+      cnt = (int)min((int64_t)32, A.nt - t0);
+    }
+    const bool valid = lane < cnt;
+    const int64_t t = t0 + lane;
+    double px = 0, py = 0, pz = 0;
+    double E0 = 0, E1 = 0, E2 = 0, PH = 0, W = 0;
+    if (valid) {
+      px = A.tx[t]; py = A.ty[t]; pz = A.tz[t];
+      E0 = A.ex[t]; E1 = A.ey[t]; E2 = A.ez[t]; PH = A.pot[t]; W = A.work[t];
+    }
+    // group centre (FP64) and the targets' offsets from it (FP32)
+    double lo[3] = {valid ? px : INFINITY, valid ? py : INFINITY, valid ? pz : INFINITY};
+    double hi[3] = {valid ? px : -INFINITY, valid ? py : -INFINITY, valid ? pz : -INFINITY};
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      for (int o = 16; o > 0; o >>= 1) {
+        lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+        hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+      }
+    const double g0x = 0.5 * (lo[0] + hi[0]), g0y = 0.5 * (lo[1] + hi[1]), g0z = 0.5 * (lo[2] + hi[2]);
+    const float rx = (float)(px - g0x), ry = (float)(py - g0y), rz = (float)(pz - g0z);
+    float rg = valid ? sqrtf(rx * rx + ry * ry + rz * rz) : 0.f;
+    for (int o = 16; o > 0; o >>= 1) rg = fmaxf(rg, __shfl_xor_sync(0xffffffffu, rg, o));
+    rg = rg * 1.0001f + 1e-30f;  // the sphere must contain every target after rounding
+    tt[lane] = make_float4(rx, ry, rz, valid ? 1.f : 0.f);
+    __syncwarp();
+    bool complete = true;
+    for (int ib = 0; ib < A.nbox; ++ib) {
+      const double vx = s_vb[3 * ib], vy = s_vb[3 * ib + 1], vz = s_vb[3 * ib + 2];
+      const double sx = px - vx, sy = py - vy, sz = pz - vz;
+      const double gx = g0x - vx, gy = g0y - vy, gz = g0z - vz;
+      int64_t partner = 0;
+      int nT = 0, nL = 0;
+      int top = 1;
+      if (lane == 0) stack[0] = 0;  // the root (walk_simple starts at the root, :286)
+      __syncwarp();
+      // evaluates the first n queued twigs / leaves and removes them
+      auto flush_twigs = [&](int n) {
+        if (lane < n) {
+          const int nd = tw[lane];
+          const double4 a = A.nc4[nd];
+          Staged sv;
+          sv.cx = a.x; sv.cy = a.y; sv.cz = a.z; sv.q = a.w;
+          sv.m0 = A.mom32[3 * (int64_t)nd];
+          sv.m1 = A.mom32[3 * (int64_t)nd + 1];
+          sv.m2 = A.mom32[3 * (int64_t)nd + 2];
+          st[lane] = sv;
+        }
+        __syncwarp();
+        if (valid) {
+          float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
+          for (int j = 0; j < n; ++j) {
+            const float dx = (float)(sx - st[j].cx), dy = (float)(sy - st[j].cy),
+                        dz = (float)(sz - st[j].cz);
+            twig32(st[j].m0, st[j].m1, st[j].m2, dx, dy, dz, A.eps2, ax, ay, az, ap);
+          }
+          E0 += (double)ax; E1 += (double)ay; E2 += (double)az; PH += (double)ap;
+          c_twig += (unsigned)n;
+        }
+        W += (double)n;
+        __syncwarp();
+        if (lane + n < nT) tw[lane] = tw[lane + n];
+        nT -= n;
+        __syncwarp();
+      };
+      auto flush_leaves = [&](int n) {
+        if (lane < n) {
+          const double4 a = A.nc4[lf[lane]];
+          st[lane].cx = a.x; st[lane].cy = a.y; st[lane].cz = a.z; st[lane].q = a.w;
+        }
+        __syncwarp();
+        if (valid) {
+          float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
+          for (int j = 0; j < n; ++j) {
+            const double dx64 = sx - st[j].cx, dy64 = sy - st[j].cy, dz64 = sz - st[j].cz;
+            if (dx64 == 0.0 && dy64 == 0.0 && dz64 == 0.0) continue;  // self
+            leaf32((float)st[j].q, (float)dx64, (float)dy64, (float)dz64, A.eps2, ax, ay, az, ap);
+            ++c_leaf;
+          }
+          E0 += (double)ax; E1 += (double)ay; E2 += (double)az; PH += (double)ap;
+        }
+        W += (double)n;
+        __syncwarp();
+        if (lane + n < nL) lf[lane] = lf[lane + n];
+        nL -= n;
+        __syncwarp();
+      };
+      while (top > 0) {
+        const int take = top < 32 ? top : 32;
+        top -= take;
+        const int node = lane < take ? stack[top + lane] : -1;
+        __syncwarp();
+        bool isleaf = false, accept = false, open = false;
+        int nleaf_acc = 0;
+        if (node >= 0) {
+          const double4 a = A.nc4[node];
+          const int2 mu = A.meta[node];
+          if (mu.y & kLeafFlag) {
+            isleaf = true;
+          } else {
+            const float cx = (float)(a.x - gx), cy = (float)(a.y - gy), cz = (float)(a.z - gz);
+            const float bl = s_bl2[mu.y & 0xff];
+            const float dc = sqrtf(cx * cx + cy * cy + cz * cz);
+            const float dmin = dc - rg, dmax = dc + rg;
+            if (dmin > 0.f && theta2 * (dmin * dmin) > bl) {
+              accept = true;  // every target is farther than dmin
+              c_mac += 1;
+            } else if (!(theta2 * (dmax * dmax) > bl)) {
+              open = true;    // no target can pass
+              c_mac += 1;
+            } else {
+              accept = true;
+              for (int j = 0; j < 32; ++j) {
+                const float4 q4 = tt[j];
+                if (q4.w == 0.f) continue;
+                const float dx = q4.x - cx, dy = q4.y - cy, dz = q4.z - cz;
+                ++c_mac;
+                if (!(theta2 * fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > bl)) {
+                  accept = false;
+                  break;
+                }
+              }
+              open = !accept;
+            }
+            if (accept) nleaf_acc = A.nleaves[node];
+          }
+        }
+        const unsigned lb = __ballot_sync(0xffffffffu, isleaf);
+        const unsigned ab = __ballot_sync(0xffffffffu, accept);
+        if (isleaf) lf[nL + __popc(lb & lt)] = node;
+        if (accept) tw[nT + __popc(ab & lt)] = node;
+        nL += __popc(lb);
+        nT += __popc(ab);
+        int pl = nleaf_acc;
+        for (int o = 16; o > 0; o >>= 1) pl += __shfl_xor_sync(0xffffffffu, pl, o);
+        partner += (int64_t)pl + __popc(lb);
+        // push the children of opened twigs
+        const int nch = open ? min(8, nchild[node]) : 0;
+        int total;
+        const int off = warp_excl_scan(nch, lane, total);
+        if (top + total > kStackCap) {
+          complete = false;  // cannot happen within the bound above
+          break;
+        }
+        if (nch > 0) {
+          const int4 c0 = child8[2 * (int64_t)node], c1 = child8[2 * (int64_t)node + 1];
+          const int cc[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+          for (int k = 0; k < nch; ++k) stack[top + off + k] = cc[k];
+        }
+        top += total;
+        __syncwarp();
+        if (nT >= 32) flush_twigs(32);
+        if (nL >= 32) flush_leaves(32);
+      }
+      if (nT > 0) flush_twigs(nT);
+      if (nL > 0) flush_leaves(nL);
+      if (partner != A.npart) complete = false;
+    }
+    if (valid) {
+      A.ex[t] = E0; A.ey[t] = E1; A.ez[t] = E2; A.pot[t] = PH; A.work[t] = W;
+    }
+    if (__any_sync(0xffffffffu, !complete) && lane == 0) atomicOr(A.status, ST_INCOMPLETE);
+  }
+  warp_add3(A.counters, c_leaf, c_twig, c_mac);
+}
+
 // per-target semantics (module_tree_walk_pthreads.f90:558-765) with FP32
 // interactions; the MAC is evaluated on the FP32 offsets
 __global__ void __launch_bounds__(kMixThreads) k_walk_target_mixed(MixArgs A) {
@@ -294,6 +674,7 @@ __global__ void k_reset_mixed() { g_bucket_counter_mixed = 0; }
 int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                       double* ex, double* ey, double* ez, double* pot, double* work,
                       const int2* tiles, int64_t ntiles, bool per_target) {
+  const int blocks = 148 * 8;
   MixArgs A;
   A.nt = nt;
   A.tx = tx; A.ty = ty; A.tz = tz;
@@ -305,6 +686,7 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
   A.vbox = c->d_vbox;
   A.nbox = c->nboxes;
   A.theta2 = (float)c->prm.theta2;
+  A.theta2_64 = c->prm.theta2;
   A.eps2 = (float)c->prm.eps2;
   A.M = (int32_t)c->nnodes;
   A.npart = c->n;
@@ -317,10 +699,16 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
   COUNT_LAUNCH();
   k_reset_mixed<<<1, 1, 0, s>>>();
   COUNT_LAUNCH();
-  if (per_target)
-    k_walk_target_mixed<<<148 * 8, kMixThreads, 0, s>>>(A);
-  else
-    k_walk_group_mixed<<<148 * 8, kMixThreads, 0, s>>>(A);
+  if (per_target) {
+    k_walk_target_mixed<<<blocks, kMixThreads, 0, s>>>(A);
+  } else if (c->prm.reserved[0] == 1) {
+    k_walk_group_mixed<<<blocks, kMixThreads, 0, s>>>(A);
+  } else if (c->prm.reserved[0] == 2) {
+    k_walk_group_mixed_ab<<<blocks, kMixThreads, 0, s>>>(A);
+  } else {
+    if (!ensure(c, c->wstack, (size_t)blocks * kWW * kStackCap, "walk stacks")) return PEPCG_ERR_OOM;
+    k_walk_group_wide<<<blocks, kMixThreads, 0, s>>>(A, c->wstack.p, c->child8.p, c->nchild.p);
+  }
   return cuda_ok(c, cudaGetLastError(), "mixed walk launch") ? PEPCG_OK : PEPCG_ERR_CUDA;
 }
 

@@ -357,10 +357,8 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
   c->st.interactions = (int64_t)(ctr[0] + ctr[1]);
   c->st.mac_evaluations = (int64_t)ctr[2];
   float ms = 0;
-  cudaEventElapsedTime(&ms, c->ev[5], c->ev[6]);
-  c->st.t_walk_ms = ms;
-  cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]);
-  c->st.t_lattice_ms = ms;
+  if (cudaEventElapsedTime(&ms, c->ev[5], c->ev[6]) == cudaSuccess) c->st.t_walk_ms = ms;
+  if (cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]) == cudaSuccess) c->st.t_lattice_ms = ms;
   if (st) return status_to_code(c, st);
   return PEPCG_OK;
 }

@@ -1,0 +1,208 @@
+"""GPU: the adjoint walk (pepcg_traverse_adjoint) -- dL/dq and dL/dx of the
+sources for dL/dE and dL/dphi given at the targets.
+
+Checks, all in FP64:
+  * against the oracle's adjoint (same walk semantics, fixed lists):
+    relative 1e-9 of the gradient's scale (atomic summation order differs);
+  * against central finite differences of the GPU forward pass (h = 1e-6,
+    the whole grow + traverse re-run per point): relative 1e-5, allowing a
+    coordinate whose perturbation flips a MAC decision or a key;
+  * the adjoint configuration -- 262,144 sources U[0,1)^3 with q ~ N(0,1),
+    4,096 probes U[0.25,0.75]^3, L = sum (phi - phi_target)^2 with
+    phi_target from a second charge set, theta = 0.4, eps = 1e-3 -- against
+    the FP64 direct-sum gradient (tree-code accuracy) and FD on 64 random
+    coordinates."""
+import numpy as np
+import pytest
+import torch
+
+import pepc_b200 as P
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def forward_L(x, y, z, q, tx, ty, tz, gphi, gE, **kw):
+    tc = P.TreeCode(precision=P.PRECISION_PLAIN, **kw)
+    tc.pepc_grow_tree(x, y, z, q)
+    r = tc.pepc_traverse_tree(tx, ty, tz)
+    tc.close()
+    return float(np.sum(gphi * r["pot"] + gE[0] * r["ex"] + gE[1] * r["ey"] + gE[2] * r["ez"]))
+
+
+def problem(n, nt, seed):
+    rng = np.random.default_rng(seed)
+    x, y, z = rng.random(n), rng.random(n), rng.random(n)
+    q = rng.standard_normal(n)
+    tx, ty, tz = (0.25 + 0.5 * rng.random(nt) for _ in range(3))
+    gphi = rng.standard_normal(nt)
+    gE = [rng.standard_normal(nt) for _ in range(3)]
+    return x, y, z, q, tx, ty, tz, gphi, gE, rng
+
+
+@pytest.mark.parametrize("walk", [P.WALK_PER_TARGET, P.WALK_GROUP])
+def test_adjoint_matches_oracle_and_fd(gpu, walk):
+    x, y, z, q, tx, ty, tz, gphi, gE, rng = problem(3000, 70, 71)
+    kw = dict(theta2=0.16, eps2=1e-3, walk=walk)
+    tc = P.TreeCode(precision=P.PRECISION_PLAIN, **kw)
+    tc.pepc_grow_tree(x, y, z, q)
+    g = tc.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
+    if walk == P.WALK_PER_TARGET:
+        orc = O.Oracle(theta2=0.16, eps2=1e-3, walk=0)
+        orc.grow_tree(x, y, z, q)
+        go = orc.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
+        for k in ("q", "x", "y", "z"):
+            scale = np.abs(go[k]).max()
+            assert np.abs(g[k] - go[k]).max() <= 1e-9 * scale, k
+    h = 1e-6
+    bad = 0
+    for trial in range(16):
+        j = int(rng.integers(len(x)))
+        key = "xyzq"[trial % 4]
+        arrs = {"x": x, "y": y, "z": z, "q": q}
+        plus = {k: v.copy() for k, v in arrs.items()}
+        minus = {k: v.copy() for k, v in arrs.items()}
+        plus[key][j] += h
+        minus[key][j] -= h
+        fd = (forward_L(plus["x"], plus["y"], plus["z"], plus["q"], tx, ty, tz, gphi, gE, **kw) -
+              forward_L(minus["x"], minus["y"], minus["z"], minus["q"], tx, ty, tz, gphi, gE, **kw)) / (2 * h)
+        an = g[key][j]
+        if abs(fd - an) > 1e-5 * max(abs(fd), abs(an), 1e-8):
+            bad += 1
+    assert bad <= 1
+
+
+def test_adjoint_configuration_against_direct_and_fd(gpu):
+    n, nt = 262144, 4096
+    rng = np.random.default_rng(4)
+    x, y, z = rng.random(n), rng.random(n), rng.random(n)
+    q = np.random.default_rng(41).standard_normal(n)
+    prng = np.random.default_rng(42)
+    tx, ty, tz = (0.25 + 0.5 * prng.random(nt) for _ in range(3))
+    q_t = np.random.default_rng(43).standard_normal(n)
+    kw = dict(theta2=0.16, eps2=1e-6, walk=P.WALK_PER_TARGET)
+    # phi_target: the potential of the second charge set at the probes
+    tt = P.TreeCode(precision=P.PRECISION_PLAIN, **kw)
+    tt.pepc_grow_tree(x, y, z, q_t)
+    phi_t = tt.pepc_traverse_tree(tx, ty, tz)["pot"]
+    tt.close()
+    tc = P.TreeCode(precision=P.PRECISION_PLAIN, **kw)
+    tc.pepc_grow_tree(x, y, z, q)
+    phi = tc.pepc_traverse_tree(tx, ty, tz)["pot"]
+    gphi = 2.0 * (phi - phi_t)
+    zero = [np.zeros(nt)] * 3
+    g = tc.traverse_adjoint(tx, ty, tz, zero, gphi, n)
+    # FP64 direct-sum gradient (no tree), oracle
+    orc = O.Oracle(theta2=0.16, eps2=1e-6, walk=0, num_threads=16)
+    orc.grow_tree(x, y, z, q)
+    gd = orc.traverse_adjoint(tx, ty, tz, zero, gphi, n, direct=True)
+    for k in ("q", "x"):
+        rel = np.abs(g[k] - gd[k]) / np.abs(gd[k]).max()
+        assert np.median(rel) < 1e-3, (k, np.median(rel))
+    # central differences of L = sum (phi - phi_t)^2 on 64 random coordinates
+    def L(xx, yy, zz, qq):
+        t = P.TreeCode(precision=P.PRECISION_PLAIN, **kw)
+        t.pepc_grow_tree(xx, yy, zz, qq)
+        p = t.pepc_traverse_tree(tx, ty, tz)["pot"]
+        t.close()
+        return float(np.sum((p - phi_t) ** 2))
+    h = 1e-6
+    crng = np.random.default_rng(44)
+    bad = 0
+    for trial in range(64):
+        j = int(crng.integers(n))
+        key = "xyzq"[int(crng.integers(4))]
+        arrs = {"x": x, "y": y, "z": z, "q": q}
+        plus = {k: (v.copy() if k == key else v) for k, v in arrs.items()}
+        minus = {k: (v.copy() if k == key else v) for k, v in arrs.items()}
+        plus[key][j] += h
+        minus[key][j] -= h
+        fd = (L(plus["x"], plus["y"], plus["z"], plus["q"]) -
+              L(minus["x"], minus["y"], minus["z"], minus["q"])) / (2 * h)
+        an = g[key][j]
+        if abs(fd - an) > 1e-4 * max(abs(fd), abs(an)) + 1e-9:
+            bad += 1
+    assert bad <= 3, bad
+
+
+class TreeField(torch.autograd.Function):
+    """phi, E at fixed probes as a function of the sources (x, y, z, q), with
+    the backward pass through pepcg_traverse_adjoint_device.  Test harness
+    only: the library itself has no torch dependency."""
+
+    @staticmethod
+    def forward(ctx, x, y, z, q, probes, tc):
+        tc.grow_tree_device(x, y, z, q)
+        tx, ty, tz = probes
+        out = [torch.zeros_like(tx) for _ in range(5)]
+        tc.traverse_tree_device(tx, ty, tz, *out)
+        ctx.tc, ctx.probes, ctx.n = tc, probes, x.numel()
+        return out[3], out[0], out[1], out[2]
+
+    @staticmethod
+    def backward(ctx, gphi, gex, gey, gez):
+        tx, ty, tz = ctx.probes
+        dev = tx.device
+        g = [torch.zeros(ctx.n, dtype=torch.float64, device=dev) for _ in range(4)]
+        z = torch.zeros_like(tx)
+        gphi = gphi.contiguous() if gphi is not None else z
+        gE = [a.contiguous() if a is not None else z for a in (gex, gey, gez)]
+        ctx.tc.traverse_adjoint_device(tx, ty, tz, gE, gphi, *g)
+        return g[1], g[2], g[3], g[0], None, None
+
+
+def direct_grad_torch(x, y, z, q, tx, ty, tz, gphi, chunk=256):
+    """FP64 direct-sum dL/dq, dL/dx for dL/dphi = gphi (torch, chunked)."""
+    dq = torch.zeros_like(q)
+    dx, dy, dz = torch.zeros_like(x), torch.zeros_like(x), torch.zeros_like(x)
+    for s in range(0, tx.numel(), chunk):
+        e = slice(s, s + chunk)
+        rx = tx[e, None] - x[None, :]
+        ry = ty[e, None] - y[None, :]
+        rz = tz[e, None] - z[None, :]
+        rinv = torch.rsqrt(rx * rx + ry * ry + rz * rz + 1e-6)
+        g = gphi[e, None]
+        dq += (g * rinv).sum(0)
+        w = g * q[None, :] * rinv ** 3
+        dx += (w * rx).sum(0)
+        dy += (w * ry).sum(0)
+        dz += (w * rz).sum(0)
+    return dq, dx, dy, dz
+
+
+def test_autograd_harness_against_torch_direct_gradient(gpu):
+    """L = sum (phi - phi_t)^2 through torch.autograd with the adjoint as the
+    backward; the gradient is compared with the FP64 direct-sum gradient in
+    torch (tree accuracy at theta = 0.4)."""
+    dev = torch.device("cuda", 0)
+    n, nt = 65536, 1024
+    rng = np.random.default_rng(8)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    x, y, z = (T(rng.random(n)) for _ in range(3))
+    q = T(rng.standard_normal(n))
+    probes = tuple(T(0.25 + 0.5 * rng.random(nt)) for _ in range(3))
+    phi_t = T(rng.standard_normal(nt))
+    tc = P.TreeCode(theta2=0.16, eps2=1e-6, precision=P.PRECISION_PLAIN, walk=P.WALK_GROUP)
+    tc.set_stream(torch.cuda.current_stream().cuda_stream)
+    leaves = [a.clone().requires_grad_(True) for a in (x, y, z, q)]
+    phi, ex, ey, ez = TreeField.apply(*leaves, probes, tc)
+    L = ((phi - phi_t) ** 2).sum()
+    L.backward()
+    gphi = 2.0 * (phi.detach() - phi_t)
+    dq, dx, dy, dz = direct_grad_torch(x, y, z, q, *probes, gphi)
+    for name, a, b in (("q", leaves[3].grad, dq), ("x", leaves[0].grad, dx),
+                       ("y", leaves[1].grad, dy), ("z", leaves[2].grad, dz)):
+        rel = ((a - b).abs() / b.abs().max()).cpu().numpy()
+        assert np.median(rel) < 1e-3, (name, np.median(rel))
+    tc.close()
+
+
+def test_adjoint_rejects_periodic_far_field(gpu):
+    rng = np.random.default_rng(5)
+    x, y, z = rng.random(200), rng.random(200), rng.random(200)
+    q = np.where(np.arange(200) % 2 == 0, 1.0, -1.0)
+    tc = P.TreeCode(periodicity=(1, 1, 1))
+    tc.pepc_grow_tree(x, y, z, q)
+    with pytest.raises(P.PepcgError) as ei:
+        tc.traverse_adjoint(x[:5], y[:5], z[:5], [np.zeros(5)] * 3, np.ones(5), 200)
+    assert ei.value.code == P.PEPCG_ERR_UNSUPPORTED

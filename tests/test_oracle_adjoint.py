@@ -1,0 +1,83 @@
+"""CPU: the oracle's adjoint walk (orc_traverse_adjoint) and direct-sum
+gradient (orc_direct_adjoint) against central finite differences.
+
+The tree adjoint is the exact derivative of the tree-code fields with the
+interaction lists held fixed, so FD of the oracle's forward walk agrees with
+it to FD accuracy wherever a perturbation flips no MAC decision; the direct
+gradient is checked against FD of a numpy direct sum."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+
+def _problem(n, nt, seed):
+    rng = np.random.default_rng(seed)
+    x, y, z = rng.random(n), rng.random(n), rng.random(n)
+    q = rng.standard_normal(n)
+    tx, ty, tz = (0.25 + 0.5 * rng.random(nt) for _ in range(3))
+    gphi = rng.standard_normal(nt)
+    gE = [rng.standard_normal(nt) for _ in range(3)]
+    return x, y, z, q, tx, ty, tz, gphi, gE, rng
+
+
+def _L_tree(arrs, t, gphi, gE, **kw):
+    o = O.Oracle(**kw)
+    o.grow_tree(arrs["x"], arrs["y"], arrs["z"], arrs["q"])
+    r = o.traverse_tree(*t)
+    o.close()
+    return float(np.sum(gphi * r["pot"] + gE[0] * r["ex"] + gE[1] * r["ey"] + gE[2] * r["ez"]))
+
+
+def _L_direct(arrs, t, gphi, gE, eps2):
+    dx = t[0][:, None] - arrs["x"][None, :]
+    dy = t[1][:, None] - arrs["y"][None, :]
+    dz = t[2][:, None] - arrs["z"][None, :]
+    r2 = dx * dx + dy * dy + dz * dz + eps2
+    rinv = 1.0 / np.sqrt(r2)
+    r3 = rinv ** 3
+    q = arrs["q"][None, :]
+    pot = np.sum(q * rinv, axis=1)
+    ex, ey, ez = (np.sum(q * d * r3, axis=1) for d in (dx, dy, dz))
+    return float(np.sum(gphi * pot + gE[0] * ex + gE[1] * ey + gE[2] * ez))
+
+
+@pytest.mark.parametrize("direct", [False, True])
+def test_oracle_adjoint_against_fd(direct):
+    x, y, z, q, tx, ty, tz, gphi, gE, rng = _problem(600, 24, 13)
+    kw = dict(theta2=0.16, eps2=1e-3, walk=0)
+    o = O.Oracle(**kw)
+    o.grow_tree(x, y, z, q)
+    g = o.traverse_adjoint(tx, ty, tz, gE, gphi, len(x), direct=direct)
+    o.close()
+    t = (tx, ty, tz)
+    h = 1e-6
+    bad = 0
+    for trial in range(24):
+        j = int(rng.integers(len(x)))
+        key = "xyzq"[trial % 4]
+        arrs = {"x": x, "y": y, "z": z, "q": q}
+        plus = {k: (v.copy() if k == key else v) for k, v in arrs.items()}
+        minus = {k: (v.copy() if k == key else v) for k, v in arrs.items()}
+        plus[key][j] += h
+        minus[key][j] -= h
+        if direct:
+            fd = (_L_direct(plus, t, gphi, gE, 1e-3) - _L_direct(minus, t, gphi, gE, 1e-3)) / (2 * h)
+        else:
+            fd = (_L_tree(plus, t, gphi, gE, **kw) - _L_tree(minus, t, gphi, gE, **kw)) / (2 * h)
+        an = g[key][j]
+        if abs(fd - an) > 1e-5 * max(abs(fd), abs(an), 1e-6):
+            bad += 1
+    assert bad <= (0 if direct else 1), bad
+
+
+def test_oracle_adjoint_close_to_direct_gradient():
+    x, y, z, q, tx, ty, tz, gphi, gE, _ = _problem(2000, 32, 17)
+    o = O.Oracle(theta2=0.16, eps2=1e-3, walk=0)
+    o.grow_tree(x, y, z, q)
+    gt = o.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
+    gd = o.traverse_adjoint(tx, ty, tz, gE, gphi, len(x), direct=True)
+    o.close()
+    for k in ("q", "x", "y", "z"):
+        rel = np.abs(gt[k] - gd[k]) / np.abs(gd[k]).max()
+        assert np.median(rel) < 1e-3, (k, np.median(rel))
