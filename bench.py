@@ -31,6 +31,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "particle force evals/s at 4M, mixed vs FP64 GPU walk, at ≤1e-4 median force err"
 UNIT = "force evals/s"
+# DRAM bytes per particle of one mixed group-walk launch (ncu, Plummer N = 1,048,576,
+# theta = 0.4: 344.5 MB read + 54.6 MB written; profiles/k_walk_group_wide_plummer1M.md),
+# scaled by the particle count: the tree the walk re-reads grows with N
+WALK_DRAM_BYTES_PER_PARTICLE = (344.5e6 + 54.6e6) / 1048576
 FLOPS_TWIG = 144  # counted from coulomb/module_coulomb_kernels.f90:60-145 + delta, dist2, MAC, sums
 FLOPS_LEAF = 22   # counted from module_coulomb_kernels.f90:242-257 + delta, dist2, sums
 SMS = 148
@@ -151,6 +155,161 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def uniform_sphere(n, seed=2):
+    """Uniform in the unit sphere: radius u^(1/3), isotropic direction."""
+    rng = np.random.default_rng(seed)
+    r = rng.random(n) ** (1.0 / 3.0)
+    v = rng.standard_normal((n, 3))
+    v /= np.linalg.norm(v, axis=1)[:, None]
+    p = v * r[:, None]
+    return tuple(np.ascontiguousarray(p[:, k]) for k in range(3))
+
+
+def rocksalt(n):
+    """Rock-salt lattice: sites (i + 1/2)/n of the unit cube, q = (-1)^(i+j+k)."""
+    i, j, k = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    return (((i + 0.5) / n).ravel(), ((j + 0.5) / n).ravel(), ((k + 0.5) / n).ravel(),
+            ((-1.0) ** (i + j + k)).ravel())
+
+
+def event_ms(torch, stream, fn):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_explosion(args, P, torch, dev, stream):
+    """Coulomb explosion: N = 1,048,576 uniform in the unit sphere (seed 2), q = m = 1/N,
+    eps = 1e-3, theta = 0.3, Hilbert keys; 10 kick-drift steps, dt = 1e-3, in the
+    pepc-mini pusher form (v += dt q/m E; x += dt v, module_helper.f90:205-222).
+    Each precision runs its own trajectory from the same start; the force error is
+    measured against the FP64 direct sum on 4,096 sampled targets (seed 22) at the
+    first and the last step."""
+    n = args.n if args.n != 4194304 else 1048576
+    x0, y0, z0 = uniform_sphere(n)
+    dt, nsteps = 1e-3, 10
+    res = {}
+    final = {}
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    for name, prec, walk in (("mixed", P.PRECISION_MIXED, P.WALK_GROUP),
+                             ("plain", P.PRECISION_PLAIN, P.WALK_PER_TARGET)):
+        q = torch.full((n,), 1.0 / n, dtype=torch.float64, device=dev)
+        zeros = lambda: torch.zeros(n, dtype=torch.float64, device=dev)  # noqa: E731
+        st = {"x": T(x0), "y": T(y0), "z": T(z0), "q": q, "m": q.clone(),
+              "vx": zeros(), "vy": zeros(), "vz": zeros()}
+        tc = P.TreeCode(theta2=0.09, eps2=1e-6, precision=prec, walk=walk)
+        tc.set_stream(stream.cuda_stream)
+        key = torch.empty(n, dtype=torch.int64, device=dev)
+        perm = torch.empty(n, dtype=torch.int64, device=dev)
+        xs, ys, zs, qs = (torch.empty(n, dtype=torch.float64, device=dev) for _ in range(4))
+        out = [zeros() for _ in range(5)]
+
+        def step():
+            tc.grow_tree_device(st["x"], st["y"], st["z"], st["q"])
+            tc.particles_device(key, perm, xs, ys, zs, qs)  # key order, like pepc-mini
+            for o in out:
+                o.zero_()
+            tc.traverse_self_device(*out)
+            m_s = st["m"][perm]
+            f = dt * qs / m_s
+            nvx = st["vx"][perm] + f * out[0]
+            nvy = st["vy"][perm] + f * out[1]
+            nvz = st["vz"][perm] + f * out[2]
+            st.update(x=xs + dt * nvx, y=ys + dt * nvy, z=zs + dt * nvz, q=qs.clone(), m=m_s,
+                      vx=nvx, vy=nvy, vz=nvz)
+
+        def error():
+            # the field just computed, at the positions before the push (key order)
+            idx = np.sort(np.random.default_rng(22).choice(n, 4096, replace=False))
+            d = tc.direct(idx)
+            E = torch.stack(out[:3]).cpu().numpy()[:, idx]
+            Ed = np.stack([d["ex"], d["ey"], d["ez"]])
+            rel = np.linalg.norm(E - Ed, axis=0) / np.linalg.norm(Ed, axis=0)
+            return float(np.median(rel)), float(np.percentile(rel, 99))
+
+        ms, errs = [], []
+        for k in range(nsteps):
+            ms.append(event_ms(torch, stream, step))
+            if k in (0, nsteps - 1):
+                errs.append(error())
+        res[name] = {"ms_per_step_median": statistics.median(ms), "ms_first": ms[0],
+                     "value": n / (statistics.median(ms) * 1e-3),
+                     "walk_ms_last": tc.stats()["t_walk_ms"],
+                     "force_err_first": {"median": errs[0][0], "p99": errs[0][1]},
+                     "force_err_last": {"median": errs[1][0], "p99": errs[1][1]}}
+        final[name] = st
+        tc.close()
+    # the two trajectories hold their particles in different orders (each is
+    # re-sorted by key every step), so they are compared through the mean radius
+    rm = {k: float(torch.sqrt(v["x"] ** 2 + v["y"] ** 2 + v["z"] ** 2).mean())
+          for k, v in final.items()}
+    line = {"workload": f"Coulomb explosion N={n} uniform sphere, q=m=1/N, eps=1e-3, theta=0.3, "
+                        f"10 kick-drift steps dt=1e-3", "unit": UNIT, "mixed": res["mixed"],
+            "plain": res["plain"],
+            "mixed_over_plain": res["mixed"]["value"] / res["plain"]["value"],
+            "mean_radius_after": rm,
+            "step": "grow + key-order gather + traverse + push, inputs resident in HBM"}
+    print(json.dumps(line), flush=True)
+
+
+def run_madelung(args, P, torch, dev, stream):
+    """Periodic rock-salt lattice, FMM far-lattice term, eps = 0, theta = 0.3,
+    one mirror-box layer: the Madelung constant at n = 64 (262,144 ions), then
+    n = 80 (512,000 ions) perturbed by N(0, 1e-3) (seed 5), wrapped into the
+    box, timed for the mixed group walk and the plain per-target walk."""
+    out_line = {"workload": "rock-salt lattice, periodic, FMM lattice, eps=0, theta=0.3"}
+    x, y, z, q = rocksalt(64)
+    tc = P.TreeCode(theta2=0.09, eps2=0.0, periodicity=(1, 1, 1), walk=P.WALK_PER_TARGET)
+    g = tc.pepc_grow_tree(x, y, z, q)
+    r = tc.pepc_traverse_tree(g.x, g.y, g.z)
+    tc.close()
+    m_est = -float(np.mean(q[g.perm] * r["pot"])) / 64
+    out_line["madelung_n64"] = {"estimate": m_est, "reference": 1.747565,
+                                "abs_err": abs(m_est - 1.7475645946331822)}
+    n = 80
+    x, y, z, q = rocksalt(n)
+    rng = np.random.default_rng(5)
+    x, y, z = ((a + rng.normal(0.0, 1e-3, a.size)) % 1.0 for a in (x, y, z))
+    N = x.size
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    tx, ty, tz, tq = T(x), T(y), T(z), T(q)
+    out = [torch.zeros(N, dtype=torch.float64, device=dev) for _ in range(5)]
+    E_mixed = None
+    for name, prec, walk in (("mixed", P.PRECISION_MIXED, P.WALK_GROUP),
+                             ("plain", P.PRECISION_PLAIN, P.WALK_PER_TARGET)):
+        tc = P.TreeCode(theta2=0.09, eps2=0.0, periodicity=(1, 1, 1), precision=prec, walk=walk)
+        tc.set_stream(stream.cuda_stream)
+
+        def step():
+            for o in out:
+                o.zero_()
+            tc.grow_tree_device(tx, ty, tz, tq)
+            tc.traverse_self_device(*out)
+
+        for _ in range(3):
+            step()
+        ms = statistics.median(event_ms(torch, stream, step) for _ in range(3))
+        st = tc.stats()
+        out_line[name] = {"ms_per_step": ms, "value": N / (ms * 1e-3), "walk_ms": st["t_walk_ms"],
+                          "lattice_ms": st["t_lattice_ms"], "interactions": st["interactions"]}
+        if E_mixed is None:
+            E_mixed = torch.stack(out[:3]).clone()
+        else:
+            E_plain = torch.stack(out[:3])
+            rel = (torch.linalg.norm(E_mixed - E_plain, dim=0) /
+                   torch.linalg.norm(E_plain, dim=0)).cpu().numpy()
+            out_line["mixed_vs_plain_rel_E"] = {"median": float(np.median(rel)),
+                                                "p99": float(np.percentile(rel, 99))}
+        tc.close()
+    out_line["n_timed"] = N
+    out_line["mixed_over_plain"] = out_line["mixed"]["value"] / out_line["plain"]["value"]
+    print(json.dumps(out_line), flush=True)
+
+
 def workload_name(args):
     return (f"Plummer sphere N={args.n} (a=1, r<=20, q=1/N), theta={args.theta}, "
             f"eps={args.eps}, quadrupole, Hilbert keys, open boundaries")
@@ -172,6 +331,9 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="plummer", choices=["plummer", "explosion", "madelung"],
+                    help="plummer: the headline line; explosion / madelung: the other "
+                         "configurations, one descriptive JSON line each")
     args = ap.parse_args()
     assert args.warmup >= 3, "at least 3 warm-up steps"
 
@@ -191,6 +353,13 @@ def main():
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    if args.workload != "plummer":
+        dev = torch.device("cuda", local)
+        stream = torch.cuda.Stream(device=dev)
+        torch.cuda.set_stream(stream)
+        (run_explosion if args.workload == "explosion" else run_madelung)(args, P, torch, dev, stream)
+        return
 
     x, y, z, q = plummer(args.n)
     n = args.n
@@ -263,7 +432,11 @@ def main():
     achieved = flops / (st["t_walk_ms"] * 1e-3) / 1e12
     roof = {"bound": "fp32-core" if prec == P.PRECISION_MIXED else "fp64-core",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "traffic": None,
+            "traffic": (WALK_DRAM_BYTES_PER_PARTICLE * n
+                        if prec == P.PRECISION_MIXED and args.walk == "group" and args.theta == 0.4
+                        else None),
+            "traffic_source": "ncu dram__bytes_read+write of one launch at N=1,048,576, scaled by "
+                              "N (mixed group walk, theta 0.4 only; null otherwise)",
             "kernel": "walk", "kernel_ms": st["t_walk_ms"],
             "peak_source": f"{SMS} SMs x {lanes} lanes x 2 flop/FMA x median SM clock under load "
                            f"({f_mhz:.0f} MHz); no measured CUDA-core peak in MEASURED_PEAKS.json",
@@ -353,6 +526,8 @@ def main():
         "force_err": {"median": float(np.median(rel)), "p99": float(np.percentile(rel, 99)),
                       "pot_median": float(np.median(prel)), "ntest": args.ntest,
                       "against": "FP64 direct sum (pepcg_direct)"},
+        "walk_only": {"value": n * world / (st["t_walk_ms"] * 1e-3), "unit": UNIT,
+                      "ms": st["t_walk_ms"]},
         "roofline": roof, "phases_ms": phases, "gpu_launches": launches,
         "clocks": clk, "e2e": e2e, "plain": plain,
         "mixed_over_plain": (value / plain["value"]) if plain else None,

@@ -7,149 +7,182 @@
 // construction (coulomb/module_interaction_specific.f90:84-140), with the
 // interaction lists held fixed (the MAC and the keys are piecewise constant).
 //
-// Writing the twig potential as
-//   phi = q D0 + p_k D1_k + sum_{kl in xx,yy,zz,xy,yz,zx} Q_kl D2_kl,
-// D the Cartesian derivative tensors of 1/r with r^2 = |d|^2 + eps^2, one
-// target-node pair (dL/dphi = gphi, dL/dE = gE) contributes
-//   qbar += gphi D0 - gE.D1,   pbar_k += gphi D1_k - gE_i D2_ik,
-//   Qbar_kl += gphi D2_kl - gE_i D3_ikl,   cocbar += gphi E + H gE,
-// where E = -grad phi and H the Hessian of phi (D4 enters only through gE).
 // Pass 1 (walk): the lists are recomputed exactly as in the forward walk;
-//   the contributions of a warp's targets to a node are reduced across the
-//   warp and added to the node's adjoint (14 doubles) with atomics.
+//   each target-node pair contributes to the node's adjoint record
+//   (q, p, Q, coc, abs_charge); the contributions of a warp's targets to a
+//   node are reduced across the warp and added with FP64 atomics.
 // Pass 2 (top-down, one launch per level): the transpose of
 //   shift_multipoles_up moves every twig's adjoint to its children,
 //   including the dependence of the centre of charge on the children's
 //   positions and abs_charge weights; a node has one parent, so no atomics.
 // Pass 3: the leaves' adjoints become dL/dq (plus abs_charge adjoint times
 //   sign(q)) and dL/dx in the caller's original particle order.
-// Compiled with --fmad=false.
+
+#include <algorithm>
 
 #include "internal.cuh"
 
 namespace pepcg {
 
 __device__ unsigned int g_bucket_counter_adj;
+__device__ unsigned long long g_item_counter_adj;
 
 namespace {
 
 constexpr int kAdjThreads = 128;
 constexpr int kNA = 16;  // adjoint record: q, p(3), Q(6), coc(3), A, pad(2)
+// per-target walk: up to this many contributing lanes add their records directly
+constexpr int kDirectLanes = 2;
 
-struct Tens {
-  double d[3], R[5];
-  __device__ __forceinline__ void set(double dx, double dy, double dz, double eps2) {
-    d[0] = dx; d[1] = dy; d[2] = dz;
-    const double r2 = ((dx * dx + dy * dy) + dz * dz) + eps2;
-    const double r0 = 1.0 / sqrt(r2);
-    const double r02 = r0 * r0;
-    R[0] = r0;
-    R[1] = R[0] * r02;
-    R[2] = R[1] * r02;
-    R[3] = R[2] * r02;
-    R[4] = R[3] * r02;
-  }
-  __device__ __forceinline__ static double dl(int i, int j) { return i == j ? 1.0 : 0.0; }
-  __device__ __forceinline__ double D1(int i) const { return -d[i] * R[1]; }
-  __device__ __forceinline__ double D2(int i, int j) const {
-    return 3.0 * d[i] * d[j] * R[2] - dl(i, j) * R[1];
-  }
-  __device__ __forceinline__ double D3(int i, int j, int k) const {
-    return -15.0 * d[i] * d[j] * d[k] * R[3] +
-           3.0 * R[2] * (dl(i, j) * d[k] + dl(i, k) * d[j] + dl(j, k) * d[i]);
-  }
-  __device__ __forceinline__ double D4(int i, int j, int k, int l) const {
-    return 105.0 * d[i] * d[j] * d[k] * d[l] * R[4] -
-           15.0 * R[3] *
-               (dl(i, j) * d[k] * d[l] + dl(i, k) * d[j] * d[l] + dl(i, l) * d[j] * d[k] +
-                dl(j, k) * d[i] * d[l] + dl(j, l) * d[i] * d[k] + dl(k, l) * d[i] * d[j]) +
-           3.0 * R[2] * (dl(i, j) * dl(k, l) + dl(i, k) * dl(j, l) + dl(i, l) * dl(j, k));
-  }
-};
-
-__constant__ int c_QK[6] = {0, 1, 2, 0, 1, 2};  // moment order xx yy zz xy yz zx
-__constant__ int c_QL[6] = {0, 1, 2, 1, 2, 0};
-
-// a[0] q, a[1..3] p, a[4..9] Q, a[10..12] coc, a[13] abs_charge
+// Closed forms of the contractions.  With r^2 = |d|^2 + eps^2 and
+// R_n = r^-(2n+1), the derivative tensors of 1/r are
+//   D1_i = -d_i R1,   D2_ij = 3 d_i d_j R2 - delta_ij R1,
+//   D3_ijk = -15 d_i d_j d_k R3 + 3 R2 (delta_ij d_k + delta_ik d_j + delta_jk d_i),
+//   D4_ijkl = 105 d_i d_j d_k d_l R4 - 15 R3 (six delta d d terms) + 3 R2 (three delta delta terms).
+// The twig potential is phi = q R0 + p.D1 + M:D2 with M the quadrupole
+// matrix (diagonal qxx qyy qzz, off-diagonal halves of qxy qyz qzx), so with
+// g = dL/dE, a = g.d, pd = p.d, dMd = d.M.d, tr = trace M:
+//   qbar  += gphi R0 + a R1
+//   pbar  += -gphi R1 d - 3 a R2 d + R1 g
+//   Mbar  += gphi D2 + 15 a R3 d d^T - 3 R2 (g d^T + d g^T + a I)
+//   cocbar += gphi E + H g, with E = -grad phi the forward field and
+//   H g = q (3 a R2 d - R1 g)
+//       + 3 R2 (pd g + (g.p) d + a p) - 15 a pd R3 d
+//       + 105 R4 a dMd d - 15 R3 (dMd g + 2 (g.M.d) d + 2 a M d + a tr d) + 3 R2 (tr g + 2 M g).
+// The stored quadrupole slots take dphi/dq_kl = D2_kl (an off-diagonal
+// q_kl = 2 M_kl enters twice through M).
+// a[0] q, a[1..3] p, a[4..9] Q (xx yy zz xy yz zx), a[10..12] coc, a[13] abs_charge
 template <bool kWithE>
-__device__ __forceinline__ void twig_adj(double q, const double* m, double dx, double dy,
-                                         double dz, double eps2, double gphi, const double gE[3],
-                                         double a[14]) {
-  Tens T;
-  T.set(dx, dy, dz, eps2);
+__host__ __device__ __forceinline__ void twig_adj(double q, const double* m, double dx, double dy,
+                                                  double dz, double eps2, double gphi,
+                                                  const double gE[3], double a[14]) {
+  const double r2 = ((dx * dx + dy * dy) + dz * dz) + eps2;
+  const double R0 = 1.0 / sqrt(r2);
+  const double i2 = R0 * R0;
+  const double R1 = R0 * i2, R2 = R1 * i2, R3 = R2 * i2;
+  const double d[3] = {dx, dy, dz};
   const double p[3] = {m[0], m[1], m[2]};
-  const double Q[6] = {m[3], m[4], m[5], m[6], m[7], m[8]};
-  a[0] += gphi * T.R[0];
-  if (kWithE)
+  const double Mx[3] = {m[3], 0.5 * m[6], 0.5 * m[8]};
+  const double My[3] = {0.5 * m[6], m[4], 0.5 * m[7]};
+  const double Mz[3] = {0.5 * m[8], 0.5 * m[7], m[5]};
+  const double Md[3] = {Mx[0] * dx + Mx[1] * dy + Mx[2] * dz, My[0] * dx + My[1] * dy + My[2] * dz,
+                        Mz[0] * dx + Mz[1] * dy + Mz[2] * dz};
+  const double dMd = dx * Md[0] + dy * Md[1] + dz * Md[2];
+  const double tr = m[3] + m[4] + m[5];
+  const double pd = p[0] * dx + p[1] * dy + p[2] * dz;
+  // forward field E = d [q R1 - 3 pd R2 + 15 dMd R3 - 3 tr R2] + p R1 - 6 R2 M d
+  const double ce = q * R1 - 3.0 * pd * R2 + 15.0 * dMd * R3 - 3.0 * tr * R2;
+  a[0] += gphi * R0;
 #pragma unroll
-    for (int i = 0; i < 3; ++i) a[0] -= gE[i] * T.D1(i);
+  for (int k = 0; k < 3; ++k) a[1 + k] -= gphi * R1 * d[k];
+  a[4] += gphi * (3.0 * dx * dx * R2 - R1);
+  a[5] += gphi * (3.0 * dy * dy * R2 - R1);
+  a[6] += gphi * (3.0 * dz * dz * R2 - R1);
+  a[7] += gphi * (3.0 * dx * dy * R2);
+  a[8] += gphi * (3.0 * dy * dz * R2);
+  a[9] += gphi * (3.0 * dz * dx * R2);
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    double v = gphi * T.D1(k);
-    if (kWithE)
+  for (int j = 0; j < 3; ++j) a[10 + j] += gphi * (ce * d[j] + p[j] * R1 - 6.0 * R2 * Md[j]);
+  if (kWithE) {
+    const double R4 = R3 * i2;
+    const double g[3] = {gE[0], gE[1], gE[2]};
+    const double ga = g[0] * dx + g[1] * dy + g[2] * dz;
+    const double gp = g[0] * p[0] + g[1] * p[1] + g[2] * p[2];
+    const double Mg[3] = {Mx[0] * g[0] + Mx[1] * g[1] + Mx[2] * g[2],
+                          My[0] * g[0] + My[1] * g[1] + My[2] * g[2],
+                          Mz[0] * g[0] + Mz[1] * g[1] + Mz[2] * g[2]};
+    const double gMd = g[0] * Md[0] + g[1] * Md[1] + g[2] * Md[2];
+    a[0] += ga * R1;
 #pragma unroll
-      for (int i = 0; i < 3; ++i) v -= gE[i] * T.D2(i, k);
-    a[1 + k] += v;
-  }
+    for (int k = 0; k < 3; ++k) a[1 + k] += R1 * g[k] - 3.0 * ga * R2 * d[k];
+    // -g_i D3_ikl = 15 a R3 d_k d_l - 3 R2 (g_k d_l + g_l d_k + delta_kl a)
+    const double a15 = 15.0 * ga * R3, r3 = 3.0 * R2;
+    a[4] += a15 * dx * dx - r3 * (2.0 * g[0] * dx + ga);
+    a[5] += a15 * dy * dy - r3 * (2.0 * g[1] * dy + ga);
+    a[6] += a15 * dz * dz - r3 * (2.0 * g[2] * dz + ga);
+    a[7] += a15 * dx * dy - r3 * (g[0] * dy + g[1] * dx);
+    a[8] += a15 * dy * dz - r3 * (g[1] * dz + g[2] * dy);
+    a[9] += a15 * dz * dx - r3 * (g[2] * dx + g[0] * dz);
+    const double cd = 3.0 * q * ga * R2 - 15.0 * ga * pd * R3 + r3 * gp + 105.0 * R4 * ga * dMd -
+                      15.0 * R3 * (2.0 * gMd + ga * tr);
+    const double cg = -q * R1 + r3 * pd - 15.0 * R3 * dMd + r3 * tr;
 #pragma unroll
-  for (int s = 0; s < 6; ++s) {
-    double v = gphi * T.D2(c_QK[s], c_QL[s]);
-    if (kWithE)
-#pragma unroll
-      for (int i = 0; i < 3; ++i) v -= gE[i] * T.D3(i, c_QK[s], c_QL[s]);
-    a[4 + s] += v;
-  }
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    double E = q * T.D1(j);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) E += p[k] * T.D2(j, k);
-#pragma unroll
-    for (int s = 0; s < 6; ++s) E += Q[s] * T.D3(j, c_QK[s], c_QL[s]);
-    E = -E;
-    double hg = 0.0;
-    if (kWithE) {
-#pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        double H = q * T.D2(i, j);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) H += p[k] * T.D3(i, j, k);
-#pragma unroll
-        for (int s = 0; s < 6; ++s) H += Q[s] * T.D4(i, j, c_QK[s], c_QL[s]);
-        hg += H * gE[i];
-      }
-    }
-    a[10 + j] += gphi * E + hg;
-  }
-}
-
-__device__ __forceinline__ void leaf_adj(double q, double dx, double dy, double dz, double eps2,
-                                         double gphi, const double gE[3], double a[14]) {
-  Tens T;
-  T.set(dx, dy, dz, eps2);
-  a[0] += gphi * T.R[0];
-#pragma unroll
-  for (int i = 0; i < 3; ++i) a[0] -= gE[i] * T.D1(i);
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    const double E = -q * T.D1(j);
-    double hg = 0.0;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) hg += q * T.D2(i, j) * gE[i];
-    a[10 + j] += gphi * E + hg;
+    for (int j = 0; j < 3; ++j)
+      a[10 + j] += cd * d[j] + cg * g[j] + r3 * ga * p[j] - 30.0 * R3 * ga * Md[j] + 6.0 * R2 * Mg[j];
   }
 }
 
-// warp-reduce the lanes' contributions and add them to the node's adjoint
+__host__ __device__ __forceinline__ void leaf_adj(double q, double dx, double dy, double dz,
+                                                  double eps2, double gphi, const double gE[3],
+                                                  double a[14]) {
+  const double r2 = ((dx * dx + dy * dy) + dz * dz) + eps2;
+  const double R0 = 1.0 / sqrt(r2);
+  const double R1 = R0 * R0 * R0, R2 = R1 * R0 * R0;
+  const double ga = gE[0] * dx + gE[1] * dy + gE[2] * dz;
+  a[0] += gphi * R0 + ga * R1;
+  const double cd = q * (gphi * R1 + 3.0 * ga * R2);
+  a[10] += cd * dx - q * R1 * gE[0];
+  a[11] += cd * dy - q * R1 * gE[1];
+  a[12] += cd * dz - q * R1 * gE[2];
+}
+
+// warp-reduce the lanes' contributions and add them to the node's adjoint:
+// a leaf's record has charge and position terms only (a[0], a[10..12]), a
+// twig's everything but the abs_charge slot, which only the downward pass fills
+__device__ __forceinline__ void reduce_add(double* __restrict__ dst, double& v, int lane) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (lane == 0 && v != 0.0) atomicAdd(dst, v);
+  v = 0.0;
+}
+
 __device__ __forceinline__ void flush_node(double* __restrict__ adj, unsigned u, double a[14],
-                                           int lane) {
+                                           int lane, bool leaf) {
+  double* d = adj + (int64_t)kNA * u;
+  reduce_add(d, a[0], lane);
+  if (!leaf) {
 #pragma unroll
-  for (int k = 0; k < 14; ++k) {
-    double v = a[k];
+    for (int k = 1; k < 10; ++k) reduce_add(d + k, a[k], lane);
+  }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0 && v != 0.0) atomicAdd(&adj[(int64_t)kNA * u + k], v);
-    a[k] = 0.0;
+  for (int k = 10; k < 13; ++k) reduce_add(d + k, a[k], lane);
+}
+
+// two twigs at once: after one exchange across the half-warps, lanes 0-15
+// hold partial sums for twig p and lanes 16-31 for twig q, so the remaining
+// four reduction steps serve both (13 + 4 x 13 shuffles for two twigs
+// instead of 2 x 5 x 13)
+__device__ __forceinline__ void flush_pair(double* __restrict__ adj, unsigned up, double P[14],
+                                           unsigned uq, double Q[14], int lane) {
+  const bool lo = lane < 16;
+  double* d = adj + (int64_t)kNA * (lo ? up : uq);
+#pragma unroll
+  for (int k = 0; k < 13; ++k) {
+    const double send = lo ? Q[k] : P[k];
+    double keep = lo ? P[k] : Q[k];
+    keep += __shfl_xor_sync(0xffffffffu, send, 16);
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) keep += __shfl_xor_sync(0xffffffffu, keep, o);
+    if ((lane & 15) == 0 && keep != 0.0) atomicAdd(d + k, keep);
+    P[k] = 0.0;
+    Q[k] = 0.0;
+  }
+}
+
+// a twig's contributions wait in `pend` for a second twig to share the flush
+__device__ __forceinline__ void flush_twig_paired(double* __restrict__ adj, unsigned u,
+                                                  double a[14], unsigned& pend_u, double pend[14],
+                                                  unsigned none, int lane) {
+  if (pend_u == none) {
+#pragma unroll
+    for (int k = 0; k < 13; ++k) {
+      pend[k] = a[k];
+      a[k] = 0.0;
+    }
+    pend_u = u;
+  } else {
+    flush_pair(adj, pend_u, pend, u, a, lane);
+    pend_u = none;
   }
 }
 
@@ -174,9 +207,21 @@ struct AdjArgs {
   double* adj;
   const int2* tiles;  // per tile: (first, count); nullptr: per-target semantics
   int64_t ntiles;
+  // per-target work split (k_adj_target): the nsub twigs on split_level
+  int split_level;
+  int nsub;
+  const int32_t* sublist;
+  const int32_t* parent;
 };
 
-// per-target semantics: the min-next-index schedule of k_walk_target64
+// per-target semantics: the min-next-index schedule of k_walk_target64.
+// With few targets the walk of a 32-target bucket is cut into work items so
+// that enough warps run: item 0 covers the nodes above the split level (and
+// the leaves on it) and skips the twigs on it; item k >= 1 covers the subtree
+// of the k-th twig S on the split level for the lanes that reach S, i.e.
+// whose walk opened every ancestor of S below the root.  The union of the
+// items is exactly each target's interaction list; only the order of the
+// (atomic) adjoint sums changes.
 template <bool kWithE>
 __global__ void __launch_bounds__(kAdjThreads) k_adj_target(AdjArgs A) {
   __shared__ double s_bl2[kMaxLevel + 1];
@@ -186,12 +231,16 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_target(AdjArgs A) {
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const unsigned M = (unsigned)A.M;
+  const int64_t per = 1 + (int64_t)A.nsub;
+  const int64_t nitems = (A.nt + 31) / 32 * per;
   for (;;) {
-    unsigned b = 0;
-    if (lane == 0) b = atomicAdd(&g_bucket_counter_adj, 1u);
-    b = __shfl_sync(0xffffffffu, b, 0);
-    if ((int64_t)b * 32 >= A.nt) break;
-    const int64_t t = (int64_t)b * 32 + lane;
+    unsigned long long item = 0;
+    if (lane == 0) item = atomicAdd(&g_item_counter_adj, 1ull);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if ((int64_t)item >= nitems) break;
+    const int64_t b = (int64_t)item / per;
+    const int sub = (int)((int64_t)item % per);
+    const int64_t t = b * 32 + lane;
     const bool valid = t < A.nt;
     double px = 0, py = 0, pz = 0, gp = 0, gE[3] = {0, 0, 0};
     if (valid) {
@@ -201,33 +250,72 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_target(AdjArgs A) {
     }
     for (int ib = 0; ib < A.nbox; ++ib) {
       const double sx = px - s_vb[3 * ib], sy = py - s_vb[3 * ib + 1], sz = pz - s_vb[3 * ib + 2];
-      unsigned next = valid ? 1u : M;
-      double a[14];
+      unsigned next = valid ? 1u : M, end = M;
+      if (sub > 0) {
+        const int S = A.sublist[sub - 1];
+        end = (unsigned)A.meta[S].x;
+        bool reach = valid;
+        for (int p = A.parent[S]; p > 0; p = A.parent[p]) {
+          const double4 pn = A.nc4[p];
+          const double dx = sx - pn.x, dy = sy - pn.y, dz = sz - pn.z;
+          const double dist2 = (dx * dx + dy * dy) + dz * dz;
+          if (A.theta2 * dist2 > s_bl2[A.meta[p].y & 0xff]) reach = false;  // accepted above S
+        }
+        next = reach ? (unsigned)S : end;
+      }
+      double a[14], pend[14];
 #pragma unroll
-      for (int k = 0; k < 14; ++k) a[k] = 0.0;
+      for (int k = 0; k < 14; ++k) a[k] = pend[k] = 0.0;
+      unsigned pend_u = M;
       for (;;) {
         const unsigned u = __reduce_min_sync(0xffffffffu, next);
-        if (u >= M) break;
+        if (u >= end) break;
         const double4 nd = A.nc4[u];
         const int2 mu = A.meta[u];
+        const bool leaf = (mu.y & kLeafFlag) != 0;  // the same node for every lane
+        if (sub == 0 && A.nsub > 0 && !leaf && (mu.y & 0xff) == A.split_level) {
+          if (next == u) next = (unsigned)mu.x;  // the subtree items cover it
+          continue;
+        }
+        bool contrib = false;
         if (next == u) {
           const double dx = sx - nd.x, dy = sy - nd.y, dz = sz - nd.z;
           const double dist2 = (dx * dx + dy * dy) + dz * dz;
-          if (mu.y & kLeafFlag) {
-            if (dist2 > 0.0) leaf_adj(nd.w, dx, dy, dz, A.eps2, gp, gE, a);
+          if (leaf) {
+            if (dist2 > 0.0) {
+              leaf_adj(nd.w, dx, dy, dz, A.eps2, gp, gE, a);
+              contrib = true;
+            }
             next = u + 1;
           } else if (A.theta2 * dist2 > s_bl2[mu.y & 0xff]) {
             double m[9];
 #pragma unroll
             for (int k = 0; k < 9; ++k) m[k] = A.mom[9 * (int64_t)u + k];
             twig_adj<kWithE>(nd.w, m, dx, dy, dz, A.eps2, gp, gE, a);
+            contrib = true;
             next = (unsigned)mu.x;
           } else {
             next = u + 1;
           }
         }
-        flush_node(A.adj, u, a, lane);
+        const unsigned cm = __ballot_sync(0xffffffffu, contrib);
+        if (cm != 0u && __popc(cm) <= kDirectLanes) {
+          // few contributors: each adds its own record, no warp reduction
+          if (contrib) {
+            double* d = A.adj + (int64_t)kNA * u;
+#pragma unroll
+            for (int k = 0; k < 13; ++k) {
+              if ((leaf && k >= 1 && k < 10) || a[k] == 0.0) continue;
+              atomicAdd(d + k, a[k]);
+              a[k] = 0.0;
+            }
+          }
+        } else if (cm != 0u) {
+          if (leaf) flush_node(A.adj, u, a, lane, true);
+          else flush_twig_paired(A.adj, u, a, pend_u, pend, M, lane);
+        }
       }
+      if (pend_u != M) flush_node(A.adj, pend_u, pend, lane, false);
     }
   }
 }
@@ -260,9 +348,10 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_group(AdjArgs A) {
     }
     for (int ib = 0; ib < A.nbox; ++ib) {
       const double vx = s_vb[3 * ib], vy = s_vb[3 * ib + 1], vz = s_vb[3 * ib + 2];
-      double a[14];
+      double a[14], pend[14];
 #pragma unroll
-      for (int k = 0; k < 14; ++k) a[k] = 0.0;
+      for (int k = 0; k < 14; ++k) a[k] = pend[k] = 0.0;
+      unsigned pend_u = M;
       unsigned u = 0;
       while (u < M) {
         const double4 nd = A.nc4[u];
@@ -272,7 +361,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_group(AdjArgs A) {
         const double dist2 = (dx * dx + dy * dy) + dz * dz;
         if (mu.y & kLeafFlag) {
           if (valid && dist2 > 0.0) leaf_adj(nd.w, dx, dy, dz, A.eps2, gp, gE, a);
-          flush_node(A.adj, u, a, lane);
+          flush_node(A.adj, u, a, lane, true);
           u = (unsigned)fw.y;
         } else {
           const bool ok = !valid || (A.theta2 * dist2 > s_bl2[mu.y & 0xff]);
@@ -283,25 +372,31 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_group(AdjArgs A) {
               for (int k = 0; k < 9; ++k) m[k] = A.mom[9 * (int64_t)u + k];
               twig_adj<kWithE>(nd.w, m, dx, dy, dz, A.eps2, gp, gE, a);
             }
-            flush_node(A.adj, u, a, lane);
+            flush_twig_paired(A.adj, u, a, pend_u, pend, M, lane);
             u = (unsigned)fw.y;
           } else {
             u = (unsigned)fw.x;
           }
         }
       }
+      if (pend_u != M) flush_node(A.adj, pend_u, pend, lane, false);
     }
   }
 }
 
-// transpose of shift_multipoles_up for the twigs of one level (top-down)
-__global__ void k_adj_down_level(int64_t M, int level, const int2* __restrict__ meta,
+// transpose of shift_multipoles_up for the twigs of one level (top-down);
+// the twigs of a level come from the per-level lists built by the grow
+__global__ void k_adj_down_level(int level, const int32_t* __restrict__ lvl,
+                                 const int32_t* __restrict__ twiglist,
+                                 const int2* __restrict__ meta,
                                  const double4* __restrict__ nc4, const double* __restrict__ mom,
                                  const double2* __restrict__ aux, double* __restrict__ adj) {
-  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < M;
-       u += (int64_t)gridDim.x * blockDim.x) {
+  int base = 0;
+  for (int l = 0; l < level; ++l) base += lvl[l];
+  const int cnt = lvl[level];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+    const int64_t u = twiglist[base + i];
     const int2 mu = meta[u];
-    if ((mu.y & kLeafFlag) || (mu.y & 0xff) != level) continue;
     const double4 pc = nc4[u];
     const double A = aux[u].x;
     const double* pa = adj + kNA * u;
@@ -385,7 +480,10 @@ __global__ void k_adj_out(int64_t n, const int32_t* __restrict__ leafnode,
   }
 }
 
-__global__ void k_reset_adj() { g_bucket_counter_adj = 0; }
+__global__ void k_reset_adj() {
+  g_bucket_counter_adj = 0;
+  g_item_counter_adj = 0;
+}
 
 __global__ void k_any_nonzero(int64_t n, const double* a, const double* b, const double* c,
                               unsigned int* flag) {
@@ -441,7 +539,25 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
   A.adj = c->adj.p;
   A.tiles = nullptr;
   A.ntiles = 0;
+  A.split_level = 0;
+  A.nsub = 0;
+  A.sublist = nullptr;
+  A.parent = c->parent.p;
   const bool per_target = (c->prm.walk == PEPCG_WALK_PER_TARGET);
+  if (per_target) {
+    // split the per-target walk until about 16 warps per SM have work
+    const int64_t nb = (nt + 31) / 32;
+    const int64_t want = 148 * 16;
+    int base = 0;
+    for (int L = 0; L <= 4 && L < c->max_level && nb * (1 + A.nsub) < want; ++L) {
+      if (L >= 1 && c->lvl_host[L] > 0) {
+        A.split_level = L;
+        A.nsub = c->lvl_host[L];
+        A.sublist = c->twiglist.p + base;
+      }
+      base += c->lvl_host[L];
+    }
+  }
   if (!per_target) {
     // the same tiles as the forward walk of these targets
     if (!ensure(c, c->tiles, 2 * (nt + 32), "tiles")) return PEPCG_ERR_OOM;
@@ -475,8 +591,12 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
   }
   const unsigned g = (unsigned)((M + 255) / 256 > 148 * 16 ? 148 * 16 : (M + 255) / 256);
   for (int L = 0; L < c->max_level; ++L) {
+    const int64_t cnt = c->lvl_host[L];
+    if (cnt <= 0) continue;
+    const unsigned gl = (unsigned)std::min<int64_t>((cnt + 255) / 256, 148 * 16);
     COUNT_LAUNCH();
-    k_adj_down_level<<<g, 256, 0, s>>>(M, L, c->meta.p, c->nc4.p, c->mom.p, c->aux.p, c->adj.p);
+    k_adj_down_level<<<gl, 256, 0, s>>>(L, c->lvlcnt.p, c->twiglist.p, c->meta.p, c->nc4.p,
+                                        c->mom.p, c->aux.p, c->adj.p);
   }
   COUNT_LAUNCH();
   k_adj_out<<<g, 256, 0, s>>>(c->n, c->leafnode.p, c->perm.p, c->q.p, c->adj.p, dq, dx, dy, dz);

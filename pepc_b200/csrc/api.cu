@@ -338,7 +338,7 @@ int pepcg_destroy(void* ctx) {
   release(c->scan_tmp);
   release(c->nc4); release(c->meta); release(c->fwd); release(c->mom); release(c->aux);
   release(c->mom32);
-  release(c->parent); release(c->nchild); release(c->upcnt); release(c->first_part);
+  release(c->parent); release(c->nchild); release(c->twiglist); release(c->lvlcnt); release(c->first_part);
   release(c->nleaves); release(c->child8); release(c->wstack); release(c->leafnode);
   release(c->adj); release(c->fpo2rpo); release(c->rpo2fpo); release(c->nkey);
   release(c->tiles); release(c->counters); release(c->tgt); release(c->tkeys);

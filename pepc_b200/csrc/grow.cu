@@ -6,6 +6,7 @@
 // Compiled with --fmad=false: the FP64 arithmetic below must equal a plain
 // IEEE evaluation of the reference's expressions.
 
+#include <algorithm>
 #include <mutex>
 #include <utility>
 #include <string>
@@ -510,10 +511,16 @@ __device__ __forceinline__ int lcp_keys(uint64_t a, uint64_t b) {
   return (kMaxLevel - 1) - h / 3;
 }
 
+// Particle i starts the nodes of levels lp+1 .. l (l its leaf level); the
+// ones below l are twigs (they also hold particle i+1), so the twigs of each
+// level are counted here too (lvl[0..20]).
 __global__ void k_node_counts(int64_t n, const int64_t* __restrict__ key,
                               int8_t* __restrict__ lev, int8_t* __restrict__ lcpn,
                               int32_t* __restrict__ cstart, int32_t* __restrict__ cend,
-                              uint32_t* status, int* maxlev) {
+                              uint32_t* status, int* maxlev, int32_t* __restrict__ lvl) {
+  __shared__ int h[kMaxLevel + 1];
+  if (threadIdx.x <= kMaxLevel) h[threadIdx.x] = 0;
+  __syncthreads();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     uint64_t k = (uint64_t)key[i];
@@ -529,7 +536,10 @@ __global__ void k_node_counts(int64_t n, const int64_t* __restrict__ key,
     if (l > 0) atomicMax(maxlev, l);
     cstart[i] = l - (lp + 1) + 1;
     cend[i] = l - ln;
+    for (int L = lp + 1; L < l; ++L) atomicAdd(&h[L], 1);
   }
+  __syncthreads();
+  if (threadIdx.x <= kMaxLevel && h[threadIdx.x]) atomicAdd(&lvl[threadIdx.x], h[threadIdx.x]);
 }
 
 __device__ __forceinline__ int64_t group_end(const int64_t* __restrict__ key, int64_t n,
@@ -593,8 +603,7 @@ __global__ void k_build_nodes(int64_t n, int64_t M, const int64_t* __restrict__ 
 __global__ void k_link(int64_t M, const int2* __restrict__ meta,
                        const int32_t* __restrict__ rpo2fpo, const int32_t* __restrict__ fpo2rpo,
                        int2* __restrict__ fwd, int32_t* __restrict__ parent,
-                       int32_t* __restrict__ nchild, int32_t* __restrict__ upcnt,
-                       int4* __restrict__ child8) {
+                       int32_t* __restrict__ nchild, int4* __restrict__ child8) {
   for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < M;
        u += (int64_t)gridDim.x * blockDim.x) {
     int2 mu = meta[u];
@@ -604,7 +613,6 @@ __global__ void k_link(int64_t M, const int2* __restrict__ meta,
     int first = leaf ? (int)M : fpo2rpo[f + 1];
     int after = (f + size >= M) ? (int)M : fpo2rpo[f + size];
     fwd[u] = make_int2(first, after);
-    upcnt[u] = 0;
     if (u == 0) parent[0] = -1;
     if (!leaf) {
       int cnt = 0;
@@ -623,122 +631,141 @@ __global__ void k_link(int64_t M, const int2* __restrict__ meta,
   }
 }
 
-// Upward pass: tree_node_update_from_children / shift_multipoles_up
-// (module_tree_grow.f90:762-821, coulomb/module_interaction_specific.f90:84-140).
-// One thread per leaf climbs; the last child to arrive at a parent (atomic
-// counter) computes the parent from all its children in key order.
-__device__ __forceinline__ void load_child(const double4* nc4, const int2* meta,
-                                           const double* mom, const double2* aux, int64_t c,
-                                           Moments& m) {
-  const double2* p2 = reinterpret_cast<const double2*>(&nc4[c]);
-  double2 a0 = __ldcg(p2), a1 = __ldcg(p2 + 1);
-  m.coc[0] = a0.x;
-  m.coc[1] = a0.y;
-  m.coc[2] = a1.x;
-  m.q = a1.y;
-  int2 mc = __ldcg(&meta[c]);
-  if (mc.y & kLeafFlag) {  // multipole_from_particle, specific.f90:67-79
-    m.absq = fabs(a1.y);
-    for (int k = 0; k < 9; ++k) m.m[k] = 0.0;
-    m.bmax = 0.0;
-  } else {
-    double2 b = __ldcg(&aux[c]);
-    m.absq = b.x;
-    m.bmax = b.y;
-    for (int k = 0; k < 9; ++k) m.m[k] = __ldcg(&mom[9 * c + k]);
-  }
+// Twigs grouped by level for the upward pass and the adjoint's downward pass.
+// lvl[0..31] counts the twigs of each level (k_node_counts), lvl[32..63] are
+// fill counters; twiglist holds, level after level, the RPO indices of that
+// level's twigs (in no particular order).
+__device__ __forceinline__ int level_base(const int32_t* lvl, int level) {
+  int b = 0;
+  for (int l = 0; l < level; ++l) b += lvl[l];
+  return b;
 }
 
-__global__ void k_upward(int64_t M, const int2* __restrict__ meta, const int32_t* parent,
-                         const int32_t* __restrict__ nchild, int32_t* upcnt, double4* nc4,
-                         double* mom, double2* aux) {
-  for (int64_t u0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u0 < M;
-       u0 += (int64_t)gridDim.x * blockDim.x) {
-    int2 m0 = meta[u0];
-    if (!(m0.y & kLeafFlag)) continue;
-    int64_t u = parent[u0];
-    while (u >= 0) {
-      __threadfence();
-      int old = atomicAdd(&upcnt[u], 1);
-      if (old != nchild[u] - 1) break;
-      __threadfence();
-      // gather children: RPO chain is last..first child; store reversed
-      int64_t ch[8];
-      int nc = 0;
-      int2 mu = __ldcg(&meta[u]);
-      for (int64_t c = u + 1; c < mu.x && nc < 8; c = __ldcg(&meta[c]).x) ch[nc++] = c;
-      Moments cm[8];
-      for (int k = 0; k < nc; ++k) load_child(nc4, meta, mom, aux, ch[nc - 1 - k], cm[k]);
-      Moments p;
-      shift_up64(cm, nc, p);
-      double2* o2 = reinterpret_cast<double2*>(&nc4[u]);
-      __stcg(o2, make_double2(p.coc[0], p.coc[1]));
-      __stcg(o2 + 1, make_double2(p.coc[2], p.q));
-      __stcg(&aux[u], make_double2(p.absq, p.bmax));
-      for (int k = 0; k < 9; ++k) __stcg(&mom[9 * u + k], p.m[k]);
-      u = parent[u];
-    }
-  }
-}
-
-// Level-synchronous variant of the upward pass: one launch per level, deepest
-// first; one thread per twig of that level computes it from its children (in
-// key order: the RPO chain u+1, skip.. lists them last to first).  No fences,
-// no atomics; every child of a level-L twig was finished by an earlier launch.
-__global__ void __launch_bounds__(256) k_upward_level(int64_t M, int level,
-                                                      const int2* __restrict__ meta,
-                                                      double4* __restrict__ nc4,
-                                                      double* __restrict__ mom,
-                                                      double2* __restrict__ aux) {
-  // shift_up64 streamed over the children (key order = reverse RPO chain):
-  // the same additions in the same order, with the child data re-read from
-  // L1 on every pass instead of held in registers
-  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < M;
-       u += (int64_t)gridDim.x * blockDim.x) {
+__global__ void __launch_bounds__(256) k_level_scatter(int64_t M, const int2* __restrict__ meta,
+                                                       int32_t* __restrict__ lvl,
+                                                       int32_t* __restrict__ twiglist) {
+  __shared__ int h[kMaxLevel + 1], base[kMaxLevel + 1];
+  if (threadIdx.x <= kMaxLevel) h[threadIdx.x] = 0;
+  __syncthreads();
+  const int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int L = -1, local = 0;
+  if (u < M) {
     const int2 mu = meta[u];
-    if ((mu.y & kLeafFlag) || (mu.y & 0xff) != level) continue;
-    int ch[8];
-    int nc = 0;
-    for (int64_t c = u + 1; c < mu.x && nc < 8; c = meta[c].x) ch[nc++] = (int)c;
-    auto absq_of = [&](int c, double q) {
-      return (meta[c].y & kLeafFlag) ? fabs(q) : aux[c].x;
-    };
-    double charge = 0.0, absq = 0.0;
-    for (int k = nc - 1; k >= 0; --k) charge = charge + nc4[ch[k]].w;
-    for (int k = nc - 1; k >= 0; --k) absq = absq + absq_of(ch[k], nc4[ch[k]].w);
-    double cx = 0.0, cy = 0.0, cz = 0.0;
-    if (absq != 0.0) {
-      for (int k = nc - 1; k >= 0; --k) {
-        const double4 a = nc4[ch[k]];
-        const double w = absq_of(ch[k], a.w);
-        cx = cx + a.x * w;
-        cy = cy + a.y * w;
-        cz = cz + a.z * w;
-      }
-      cx = cx / absq;
-      cy = cy / absq;
-      cz = cz / absq;
-    } else {
-      for (int k = nc - 1; k >= 0; --k) {
-        const double4 a = nc4[ch[k]];
-        cx = cx + a.x;
-        cy = cy + a.y;
-        cz = cz + a.z;
-      }
-      cx = cx / (double)nc;
-      cy = cy / (double)nc;
-      cz = cz / (double)nc;
+    if (!(mu.y & kLeafFlag)) {
+      L = mu.y & 0xff;
+      local = atomicAdd(&h[L], 1);
     }
-    double d0 = 0, d1 = 0, d2 = 0, q0 = 0, q1 = 0, q2 = 0, xy = 0, yz = 0, zx = 0;
-    for (int k = nc - 1; k >= 0; --k) {
-      const int c = ch[k];
-      const double4 a = nc4[c];
-      const bool leafc = (meta[c].y & kLeafFlag) != 0;
+  }
+  __syncthreads();
+  if (threadIdx.x <= kMaxLevel) {
+    const int l = threadIdx.x;
+    base[l] = h[l] ? level_base(lvl, l) + atomicAdd(&lvl[32 + l], h[l]) : 0;
+  }
+  __syncthreads();
+  if (L >= 0) twiglist[base[L] + local] = (int32_t)u;
+}
+
+// Upward pass: tree_node_update_from_children / shift_multipoles_up
+// (module_tree_grow.f90:762-821, coulomb/module_interaction_specific.f90:84-140),
+// level-synchronous: one launch per level, deepest first; one thread per twig
+// of that level computes it from its children in key order (child8 lists
+// them last to first, like the RPO chain).  No fences, no atomics; every child
+// of a level-L twig was finished by an earlier launch.  shift_up64's
+// additions in its order.  kPreload loads every child's centre, charge and
+// abs_charge in one round (for the small top levels, which are
+// latency-bound); otherwise each pass re-reads them from L1 (for the large
+// levels, which want occupancy).
+template <bool kPreload>
+__device__ __forceinline__ void upward_twig(int64_t u, const int2* __restrict__ meta,
+                                            const int4* __restrict__ child8,
+                                            const int32_t* __restrict__ nchild,
+                                            double4* __restrict__ nc4, double* __restrict__ mom,
+                                            double2* __restrict__ aux, float4* __restrict__ mom32) {
+  const int4 c0 = child8[2 * u], c1 = child8[2 * u + 1];
+  const int ch[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+  const int nc = min(8, nchild[u]);
+  double4 ca[8];
+  double2 cb[8];  // (abs_charge, bmax); a leaf's are (|q|, 0)
+  bool cl[8];
+  auto child = [&](int k, double4& a4, double2& b2, bool& leaf) {
+    if (kPreload) {
+      a4 = ca[k]; b2 = cb[k]; leaf = cl[k];
+    } else {
+      a4 = nc4[ch[k]];
+      leaf = (meta[ch[k]].y & kLeafFlag) != 0;
+      b2 = leaf ? make_double2(fabs(a4.w), 0.0) : aux[ch[k]];
+    }
+  };
+  if (kPreload) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (k < nc) {
+        ca[k] = nc4[ch[k]];
+        cl[k] = (meta[ch[k]].y & kLeafFlag) != 0;
+        cb[k] = cl[k] ? make_double2(fabs(ca[k].w), 0.0) : aux[ch[k]];
+      }
+    }
+  }
+  // every sum runs over the children in key order (k = nc-1 .. 0)
+  double charge = 0.0, absq = 0.0;
+#pragma unroll
+  for (int k = 7; k >= 0; --k) {
+    if (k < nc) {
+      double4 a4; double2 b2; bool lf;
+      child(k, a4, b2, lf);
+      charge = charge + a4.w;
+    }
+  }
+#pragma unroll
+  for (int k = 7; k >= 0; --k) {
+    if (k < nc) {
+      double4 a4; double2 b2; bool lf;
+      child(k, a4, b2, lf);
+      absq = absq + b2.x;
+    }
+  }
+  double cx = 0.0, cy = 0.0, cz = 0.0;
+  if (absq != 0.0) {
+#pragma unroll
+    for (int k = 7; k >= 0; --k) {
+      if (k < nc) {
+        double4 a4; double2 b2; bool lf;
+        child(k, a4, b2, lf);
+        cx = cx + a4.x * b2.x;
+        cy = cy + a4.y * b2.x;
+        cz = cz + a4.z * b2.x;
+      }
+    }
+    cx = cx / absq;
+    cy = cy / absq;
+    cz = cz / absq;
+  } else {
+#pragma unroll
+    for (int k = 7; k >= 0; --k) {
+      if (k < nc) {
+        double4 a4; double2 b2; bool lf;
+        child(k, a4, b2, lf);
+        cx = cx + a4.x;
+        cy = cy + a4.y;
+        cz = cz + a4.z;
+      }
+    }
+    cx = cx / (double)nc;
+    cy = cy / (double)nc;
+    cz = cz / (double)nc;
+  }
+  double d0 = 0, d1 = 0, d2 = 0, q0 = 0, q1 = 0, q2 = 0, xy = 0, yz = 0, zx = 0;
+#pragma unroll
+  for (int k = 7; k >= 0; --k) {
+    if (k < nc) {
+      double4 a4; double2 b2; bool lf;
+      child(k, a4, b2, lf);
+      const int64_t c = ch[k];
       double m[9];
 #pragma unroll
-      for (int j = 0; j < 9; ++j) m[j] = leafc ? 0.0 : mom[9 * (int64_t)c + j];
-      const double s0 = cx - a.x, s1 = cy - a.y, s2 = cz - a.z;
-      const double q = a.w;
+      for (int j = 0; j < 9; ++j) m[j] = lf ? 0.0 : mom[9 * c + j];
+      const double s0 = cx - a4.x, s1 = cy - a4.y, s2 = cz - a4.z;
+      const double q = a4.w;
       d0 = (d0 + m[0]) + q * s0;
       d1 = (d1 + m[1]) + q * s1;
       d2 = (d2 + m[2]) + q * s2;
@@ -749,35 +776,45 @@ __global__ void __launch_bounds__(256) k_upward_level(int64_t M, int level,
       yz = (((yz + m[7]) + m[1] * s2) + m[2] * s1) + (q * s1) * s2;
       zx = (((zx + m[8]) + m[2] * s0) + m[0] * s2) + (q * s2) * s0;
     }
-    double bmax = 0.0;
-    for (int k = nc - 1; k >= 0; --k) {
-      const int c = ch[k];
-      const double4 a = nc4[c];
-      const double bc = (meta[c].y & kLeafFlag) ? 0.0 : aux[c].y;
-      const double e0 = cx - a.x, e1 = cy - a.y, e2 = cz - a.z;
-      const double v = sqrt((e0 * e0 + e1 * e1) + e2 * e2) + bc;
+  }
+  double bmax = 0.0;
+#pragma unroll
+  for (int k = 7; k >= 0; --k) {
+    if (k < nc) {
+      double4 a4; double2 b2; bool lf;
+      child(k, a4, b2, lf);
+      const double e0 = cx - a4.x, e1 = cy - a4.y, e2 = cz - a4.z;
+      const double v = sqrt((e0 * e0 + e1 * e1) + e2 * e2) + b2.y;
       if (k == nc - 1 || v > bmax) bmax = v;
     }
-    nc4[u] = make_double4(cx, cy, cz, charge);
-    aux[u] = make_double2(absq, bmax);
-    double* o = mom + 9 * u;
-    o[0] = d0; o[1] = d1; o[2] = d2; o[3] = q0; o[4] = q1; o[5] = q2; o[6] = xy; o[7] = yz; o[8] = zx;
   }
+  nc4[u] = make_double4(cx, cy, cz, charge);
+  aux[u] = make_double2(absq, bmax);
+  double* o = mom + 9 * u;
+  o[0] = d0; o[1] = d1; o[2] = d2; o[3] = q0; o[4] = q1; o[5] = q2; o[6] = xy; o[7] = yz; o[8] = zx;
+  // FP32 copy for the mixed walk, the quadrupole matrix M (off-diagonals
+  // halved) scaled by 3: (px, py, pz, 3qxx), (3qyy, 3qzz, 1.5qxy, 1.5qyz),
+  // (1.5qzx, qxx+qyy+qzz, charge, 0)
+  mom32[3 * u] = make_float4((float)d0, (float)d1, (float)d2, (float)(3.0 * q0));
+  mom32[3 * u + 1] =
+      make_float4((float)(3.0 * q1), (float)(3.0 * q2), (float)(1.5 * xy), (float)(1.5 * yz));
+  mom32[3 * u + 2] = make_float4((float)(1.5 * zx), (float)((q0 + q1) + q2), (float)charge, 0.f);
 }
 
-// FP32 copy of the twig moments for the mixed walk, packed as three float4:
-// (px, py, pz, qxx), (qyy, qzz, qxy/2, qyz/2), (qzx/2, qxx+qyy+qzz, charge, 0)
-__global__ void k_mom32(int64_t M, const int2* __restrict__ meta, const double* __restrict__ mom,
-                        const double4* __restrict__ nc4, float4* __restrict__ mom32) {
-  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < M;
-       u += (int64_t)gridDim.x * blockDim.x) {
-    if (meta[u].y & kLeafFlag) continue;
-    const double* m = mom + 9 * u;
-    const double q = nc4[u].w;
-    mom32[3 * u] = make_float4((float)m[0], (float)m[1], (float)m[2], (float)m[3]);
-    mom32[3 * u + 1] = make_float4((float)m[4], (float)m[5], (float)(0.5 * m[6]), (float)(0.5 * m[7]));
-    mom32[3 * u + 2] = make_float4((float)(0.5 * m[8]), (float)((m[3] + m[4]) + m[5]), (float)q, 0.f);
-  }
+template <bool kPreload>
+__global__ void __launch_bounds__(256) k_upward_level(int level, const int32_t* __restrict__ lvl,
+                                                      const int32_t* __restrict__ twiglist,
+                                                      const int2* __restrict__ meta,
+                                                      const int4* __restrict__ child8,
+                                                      const int32_t* __restrict__ nchild,
+                                                      double4* __restrict__ nc4,
+                                                      double* __restrict__ mom,
+                                                      double2* __restrict__ aux,
+                                                      float4* __restrict__ mom32) {
+  const int cnt = lvl[level];
+  const int32_t* list = twiglist + level_base(lvl, level);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x)
+    upward_twig<kPreload>(list[i], meta, child8, nchild, nc4, mom, aux, mom32);
 }
 
 // The reference's exchange / reverse rules (module_spacefilling.f90:389-438)
@@ -857,11 +894,12 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
       !ensure(c, c->lev, n, "lev") || !ensure(c, c->lcpn, n, "lcpn") ||
       !ensure(c, c->cstart, n, "cstart") || !ensure(c, c->cend, n, "cend") ||
       !ensure(c, c->sstart, n, "sstart") || !ensure(c, c->send, n, "send") ||
-      !ensure(c, c->leafnode, n, "leafnode"))
+      !ensure(c, c->leafnode, n, "leafnode") || !ensure(c, c->lvlcnt, 64, "lvlcnt"))
     return PEPCG_ERR_OOM;
 
   if (!cuda_ok(c, cudaMemsetAsync(c->d_status, 0, sizeof(uint32_t), s), "memset status") ||
-      !cuda_ok(c, cudaMemsetAsync(c->d_small, 0, 8 * sizeof(unsigned long long), s), "memset"))
+      !cuda_ok(c, cudaMemsetAsync(c->d_small, 0, 8 * sizeof(unsigned long long), s), "memset") ||
+      !cuda_ok(c, cudaMemsetAsync(c->lvlcnt.p, 0, 64 * sizeof(int32_t), s), "memset lvl"))
     return PEPCG_ERR_CUDA;
 
   cudaEventRecord(c->ev[0], s);
@@ -908,7 +946,8 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
   COUNT_LAUNCH();
   k_node_counts<<<grid_for(n), kThreads, 0, s>>>(n, c->key.p, c->lev.p, c->lcpn.p, c->cstart.p,
                                                   c->cend.p, c->d_status,
-                                                  reinterpret_cast<int*>(c->d_small + 2));
+                                                  reinterpret_cast<int*>(c->d_small + 2),
+                                                  c->lvlcnt.p);
   exclusive_scan<int32_t>(c->cstart.p, c->sstart.p, n, c->scan_tmp.p, s);
   exclusive_scan<int32_t>(c->cend.p, c->send.p, n, c->scan_tmp.p + (n / 2048 + 32), s);
   // total number of nodes M and the box go to the host (the grid sizes below need M)
@@ -923,7 +962,9 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
       !cuda_ok(c, cudaMemcpyAsync(c->boxlength2, c->d_box + 9, 21 * sizeof(double),
                                   cudaMemcpyDeviceToHost, s), "box") ||
       !cuda_ok(c, cudaMemcpyAsync(&c->dup_count, c->d_small, 8, cudaMemcpyDeviceToHost, s), "dup") ||
-      !cuda_ok(c, cudaMemcpyAsync(&c->max_level, c->d_small + 2, 4, cudaMemcpyDeviceToHost, s), "maxlev"))
+      !cuda_ok(c, cudaMemcpyAsync(&c->max_level, c->d_small + 2, 4, cudaMemcpyDeviceToHost, s), "maxlev") ||
+      !cuda_ok(c, cudaMemcpyAsync(c->lvl_host, c->lvlcnt.p, sizeof(c->lvl_host),
+                                  cudaMemcpyDeviceToHost, s), "levels"))
     return PEPCG_ERR_CUDA;
   uint32_t st = 0;
   if (!cuda_ok(c, cudaMemcpyAsync(&st, c->d_status, 4, cudaMemcpyDeviceToHost, s), "status") ||
@@ -940,7 +981,7 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
       !ensure(c, c->fwd, M, "fwd") || !ensure(c, c->mom, 9 * M, "mom") ||
       !ensure(c, c->aux, M, "aux") || !ensure(c, c->mom32, 12 * M, "mom32") ||
       !ensure(c, c->parent, M, "parent") || !ensure(c, c->nchild, M, "nchild") ||
-      !ensure(c, c->upcnt, M, "upcnt") || !ensure(c, c->first_part, M, "first_part") ||
+      !ensure(c, c->twiglist, M, "twiglist") || !ensure(c, c->first_part, M, "first_part") ||
       !ensure(c, c->nleaves, M, "nleaves") || !ensure(c, c->fpo2rpo, M, "fpo2rpo") ||
       !ensure(c, c->rpo2fpo, M, "rpo2fpo") || !ensure(c, c->nkey, M, "nkey") ||
       !ensure(c, c->child8, 2 * M, "child8"))
@@ -953,19 +994,29 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
                                                   c->leafnode.p);
   COUNT_LAUNCH();
   k_link<<<grid_for(M), kThreads, 0, s>>>(M, c->meta.p, c->rpo2fpo.p, c->fpo2rpo.p, c->fwd.p,
-                                          c->parent.p, c->nchild.p, c->upcnt.p, c->child8.p);
+                                          c->parent.p, c->nchild.p, c->child8.p);
   cudaEventRecord(c->ev[3], s);
-  // the deepest twig level is one above the deepest leaf level
+  // twigs by level, then one launch per level, sized by the level's twig
+  // count; the deepest twig level is one above the deepest leaf level
   {
-    const int maxlev = c->max_level;
-    for (int L = maxlev - 1; L >= 0; --L) {
+    const unsigned gM = (unsigned)((M + kThreads - 1) / kThreads);
+    COUNT_LAUNCH();
+    k_level_scatter<<<gM, kThreads, 0, s>>>(M, c->meta.p, c->lvlcnt.p, c->twiglist.p);
+    float4* m32 = reinterpret_cast<float4*>(c->mom32.p);
+    for (int L = c->max_level - 1; L >= 0; --L) {
+      const int64_t cnt = c->lvl_host[L];
+      if (cnt <= 0) continue;
       COUNT_LAUNCH();
-      k_upward_level<<<grid_for(M), kThreads, 0, s>>>(M, L, c->meta.p, c->nc4.p, c->mom.p, c->aux.p);
+      if (cnt < 148 * kThreads)  // under one thread per SM slot: latency-bound
+        k_upward_level<true><<<grid_for(cnt), kThreads, 0, s>>>(
+            L, c->lvlcnt.p, c->twiglist.p, c->meta.p, c->child8.p, c->nchild.p, c->nc4.p,
+            c->mom.p, c->aux.p, m32);
+      else
+        k_upward_level<false><<<grid_for(cnt), kThreads, 0, s>>>(
+            L, c->lvlcnt.p, c->twiglist.p, c->meta.p, c->child8.p, c->nchild.p, c->nc4.p,
+            c->mom.p, c->aux.p, m32);
     }
   }
-  COUNT_LAUNCH();
-  k_mom32<<<grid_for(M), kThreads, 0, s>>>(M, c->meta.p, c->mom.p, c->nc4.p,
-                                           reinterpret_cast<float4*>(c->mom32.p));
   cudaEventRecord(c->ev[4], s);
   if (!cuda_ok(c, cudaGetLastError(), "grow kernels")) return PEPCG_ERR_CUDA;
   c->n = n;

@@ -89,7 +89,10 @@ struct Ctx {
   DBuf<double> mom;   // 9 * nnodes, node-major
   DBuf<double2> aux;
   DBuf<float> mom32;  // 12 * nnodes (coc-relative moments in FP32, padded)
-  DBuf<int32_t> parent, nchild, upcnt, first_part, nleaves;
+  DBuf<int32_t> parent, nchild, first_part, nleaves;
+  DBuf<int32_t> twiglist;  // twig RPO indices grouped by level (upward and adjoint passes)
+  DBuf<int32_t> lvlcnt;    // [0, 32) twigs per level, [32, 64) fill counters
+  int32_t lvl_host[kMaxLevel + 1] = {0};  // twigs per level of the grown tree
   DBuf<int4> child8;  // up to 8 children (RPO indices) per twig, as 2 x int4
   DBuf<int32_t> wstack;  // per-warp traversal stacks of the wide group walk
   DBuf<int32_t> leafnode;  // key-ordered particle -> RPO index of its leaf

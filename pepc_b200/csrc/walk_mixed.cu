@@ -1,11 +1,19 @@
 // walk_mixed.cu -- the mixed-precision walks.
 //
-// Precision contract: the target-minus-node offset is formed in FP64 and
-// rounded to FP32; the interaction (monopole + dipole + quadrupole, Plummer
-// softened) is evaluated in FP32 with rsqrt; each target sums its FP32
-// contributions over chunks of kChunk walk steps and adds every chunk sum to
-// FP64 accumulators.  Node moments are computed in FP64 by the upward pass
-// and rounded to FP32 once per grow (k_mom32 in grow.cu).
+// Precision contract.  Every interaction offset is formed in FP64 from the
+// FP64 positions and then rounded to FP32; the interaction (monopole + dipole
+// + quadrupole, Plummer softened) is evaluated in FP32 with rsqrt; per target
+// the FP32 sums of each batch of <= 32 interactions are added to FP64
+// accumulators; node moments are computed in FP64 by the upward pass and
+// rounded to FP32 once per grow (k_upward_level in grow.cu).
+//  * Group walk: the offsets of the target and of the node centre from the
+//    group centre g (the centre of the 32 targets' bounding box) are each
+//    formed in FP64 and rounded once; the interaction offset is their FP32
+//    difference.  Against the FP64 offset rounded once, the extra error is at
+//    most 2u (|t - g| + |d|) with u = 2^-24: 2u (1 + r_g/|d|) relative, r_g
+//    the group radius.  A leaf whose FP32 offset is exactly zero is re-tested
+//    in FP64, so the self test is the reference's dist2 == 0.
+//  * Per-target walk: target minus node centre in FP64, then rounded.
 //
 // The FP32 twig interaction is the reference's quadrupole kernel
 // (coulomb/module_coulomb_kernels.f90:60-145) rewritten in the equivalent
@@ -14,16 +22,7 @@
 //   E   = d [q/r^3 - 3 (d.p)/r^5 + 15 (d.M.d)/r^7 - 3 tr(Q)/r^5] + p/r^3 - 6 (M.d)/r^5
 // with M = [[qxx, qxy/2, qzx/2], [qxy/2, qyy, qyz/2], [qzx/2, qyz/2, qzz]]
 // (expanding the reference's fdx.. / pre2x.. terms gives exactly these
-// polynomials), which needs ~45 FP32 operations instead of ~130.
-//
-// Walks:
-//  * group / per tile: a warp holds one tile of targets (32 key-consecutive
-//    targets in GROUP mode, the reference's <= tile_size key-prefix tiles in
-//    PER_TILE mode) and visits nodes in the RPO order; a twig is accepted
-//    only if every target passes the MAC (module_tree_walk_simple.f90:343-382
-//    semantics), so accepted interactions are warp-uniform.
-//  * per target: the same min-next-index schedule as the FP64 per-target walk
-//    (module_tree_walk_pthreads.f90 semantics) with FP32 interactions.
+// polynomials), which needs ~42 FP32 operations instead of ~130.
 
 #include "internal.cuh"
 
@@ -50,7 +49,6 @@ struct MixArgs {
   int nbox;
   float theta2;
   float eps2;
-  double theta2_64;
   int32_t M;
   int64_t npart;
   double* ex;
@@ -76,7 +74,11 @@ __device__ __forceinline__ void leaf32(float q, float dx, float dy, float dz, fl
   az = fmaf(qr3, dz, az);
 }
 
-// m0 = (px, py, pz, qxx), m1 = (qyy, qzz, qxy/2, qyz/2), m2 = (qzx/2, tr, q, 0)
+// m0 = (px, py, pz, 3qxx), m1 = (3qyy, 3qzz, 1.5qxy, 1.5qyz), m2 = (1.5qzx, tr, q, -),
+// i.e. 3M with M the quadrupole matrix with halved off-diagonals; with
+// A = d.p + tr and B = d.(3M).d:
+//   phi += q/r + B/r^5 - A/r^3
+//   E   += d [q/r^3 + (5B/r^2 - 3A)/r^5] + p/r^3 - 2 (3M d)/r^5
 __device__ __forceinline__ void twig32(float4 m0, float4 m1, float4 m2, float dx, float dy,
                                        float dz, float eps2, float& ax, float& ay, float& az,
                                        float& ap) {
@@ -85,20 +87,20 @@ __device__ __forceinline__ void twig32(float4 m0, float4 m1, float4 m2, float dx
   const float ri2 = ri * ri;
   const float rd3 = ri * ri2;
   const float rd5 = rd3 * ri2;
-  const float rd7 = rd5 * ri2;
-  const float q = m2.z, tr = m2.y;
-  const float dp = fmaf(dx, m0.x, fmaf(dy, m0.y, dz * m0.z));
+  const float q = m2.z;
+  const float A = fmaf(dx, m0.x, fmaf(dy, m0.y, fmaf(dz, m0.z, m2.y)));
   const float vx = fmaf(m0.w, dx, fmaf(m1.z, dy, m2.x * dz));
   const float vy = fmaf(m1.z, dx, fmaf(m1.x, dy, m1.w * dz));
   const float vz = fmaf(m2.x, dx, fmaf(m1.w, dy, m1.y * dz));
-  const float dqd = fmaf(dx, vx, fmaf(dy, vy, dz * vz));
-  // phi = q/r - dp/r^3 + 3 dQd/r^5 - tr/r^3
-  ap += fmaf(q, ri, fmaf(3.0f * dqd, rd5, -(dp + tr) * rd3));
-  const float c = fmaf(q, rd3, fmaf(15.0f * dqd, rd7, -3.0f * (dp + tr) * rd5));
-  const float s6 = 6.0f * rd5;
-  ax = fmaf(c, dx, fmaf(rd3, m0.x, fmaf(-s6, vx, ax)));
-  ay = fmaf(c, dy, fmaf(rd3, m0.y, fmaf(-s6, vy, ay)));
-  az = fmaf(c, dz, fmaf(rd3, m0.z, fmaf(-s6, vz, az)));
+  const float B = fmaf(dx, vx, fmaf(dy, vy, dz * vz));
+  ap = fmaf(q, ri, ap);
+  ap = fmaf(B, rd5, ap);
+  ap = fmaf(-A, rd3, ap);
+  const float c = fmaf(q, rd3, rd5 * fmaf(5.0f * B, ri2, -3.0f * A));
+  const float s2 = -2.0f * rd5;
+  ax = fmaf(c, dx, fmaf(rd3, m0.x, fmaf(s2, vx, ax)));
+  ay = fmaf(c, dy, fmaf(rd3, m0.y, fmaf(s2, vy, ay)));
+  az = fmaf(c, dz, fmaf(rd3, m0.z, fmaf(s2, vz, az)));
 }
 
 __device__ __forceinline__ void warp_add3(unsigned long long* ctr, unsigned long long a,
@@ -115,266 +117,30 @@ __device__ __forceinline__ void warp_add3(unsigned long long* ctr, unsigned long
   }
 }
 
-__global__ void __launch_bounds__(kMixThreads) k_walk_group_mixed(MixArgs A) {
-  __shared__ float s_bl2[kMaxLevel + 1];
-  __shared__ double s_vb[3 * 125];
-  for (int i = threadIdx.x; i <= kMaxLevel; i += blockDim.x) s_bl2[i] = (float)A.bl2[i];
-  for (int i = threadIdx.x; i < 3 * A.nbox; i += blockDim.x) s_vb[i] = A.vbox[i];
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const unsigned M = (unsigned)A.M;
-  const int64_t nbuckets = A.tiles ? A.ntiles : (A.nt + 31) / 32;
-  unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
-  for (;;) {
-    unsigned b = 0;
-    if (lane == 0) b = atomicAdd(&g_bucket_counter_mixed, 1u);
-    b = __shfl_sync(0xffffffffu, b, 0);
-    if ((int64_t)b >= nbuckets) break;
-    int64_t t0;
-    int cnt;
-    if (A.tiles) {
-      const int2 tl = A.tiles[b];
-      t0 = tl.x;
-      cnt = tl.y;
-    } else {
-      t0 = (int64_t)b * 32;
-      cnt = (int)min((int64_t)32, A.nt - t0);
-    }
-    const bool valid = lane < cnt;
-    const int64_t t = t0 + lane;
-    double px = 0, py = 0, pz = 0;
-    double E0 = 0, E1 = 0, E2 = 0, PH = 0, W = 0;
-    if (valid) {
-      px = A.tx[t]; py = A.ty[t]; pz = A.tz[t];
-      E0 = A.ex[t]; E1 = A.ey[t]; E2 = A.ez[t]; PH = A.pot[t]; W = A.work[t];
-    }
-    bool complete = true;
-    for (int ib = 0; ib < A.nbox; ++ib) {
-      const double sx = px - s_vb[3 * ib], sy = py - s_vb[3 * ib + 1], sz = pz - s_vb[3 * ib + 2];
-      float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
-      int steps = 0;
-      int64_t partner = 0;
-      unsigned nint = 0;
-      unsigned u = 0;
-      while (u < M) {
-        const double4 a = A.nc4[u];
-        const int2 mu = A.meta[u];
-        const double dx64 = sx - a.x, dy64 = sy - a.y, dz64 = sz - a.z;
-        const float dx = (float)dx64, dy = (float)dy64, dz = (float)dz64;
-        if (mu.y & kLeafFlag) {
-          partner += 1;
-          ++nint;
-          const bool self = (dx64 == 0.0 && dy64 == 0.0 && dz64 == 0.0);
-          if (valid && !self) {
-            leaf32((float)a.w, dx, dy, dz, A.eps2, ax, ay, az, ap);
-            ++c_leaf;
-          }
-          u = u + 1;
-        } else {
-          const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          const bool ok = !valid || (A.theta2 * r2 > s_bl2[mu.y & 0xff]);
-          const unsigned fail = __ballot_sync(0xffffffffu, !ok);
-          // MAC evaluations stop at the first failing target (walk_simple :343-370)
-          const int first_fail = fail ? __ffs(fail) - 1 : 32;
-          if (valid && lane <= first_fail) ++c_mac;
-          if (fail == 0) {
-            partner += A.nleaves[u];
-            ++nint;
-            const float4 m0 = A.mom32[3 * (int64_t)u], m1 = A.mom32[3 * (int64_t)u + 1],
-                         m2 = A.mom32[3 * (int64_t)u + 2];
-            if (valid) {
-              twig32(m0, m1, m2, dx, dy, dz, A.eps2, ax, ay, az, ap);
-              ++c_twig;
-            }
-            u = (unsigned)mu.x;
-          } else {
-            u = u + 1;
-          }
-        }
-        if (++steps == kChunk) {  // flush the FP32 chunk sums into FP64
-          E0 += (double)ax; E1 += (double)ay; E2 += (double)az; PH += (double)ap;
-          ax = ay = az = ap = 0.f;
-          steps = 0;
-        }
-      }
-      E0 += (double)ax; E1 += (double)ay; E2 += (double)az; PH += (double)ap;
-      W += (double)nint;
-      if (partner != A.npart) complete = false;
-    }
-    if (valid) {
-      A.ex[t] = E0; A.ey[t] = E1; A.ez[t] = E2; A.pot[t] = PH; A.work[t] = W;
-    }
-    if (!complete && lane == 0) atomicOr(A.status, ST_INCOMPLETE);
-  }
-  warp_add3(A.counters, c_leaf, c_twig, c_mac);
-}
-
-// Group walk in two phases per warp.
-//  Phase A (traversal): the warp walks the RPO node order; at a twig every
-//    lane evaluates the Barnes-Hut MAC in FP64 and the twig is accepted only if
-//    all lanes pass (module_tree_walk_simple.f90:343-382 semantics).  Accepted
-//    twigs and reached leaves are appended to per-warp shared-memory lists.
-//  Phase B (evaluation): the listed nodes are staged 32 at a time, lane k
-//    loading node k's record (independent loads, one latency per batch), and
-//    every lane then evaluates all staged nodes from broadcast shared-memory
-//    reads.  Each batch's FP32 sums are added to the FP64 accumulators.
-constexpr int kListCap = 128;
-struct __align__(16) Staged {
-  double cx, cy, cz, q;  // coc (FP64) and charge
-  float4 m0, m1, m2;     // FP32 moments (twigs)
-};
-
-__global__ void __launch_bounds__(kMixThreads) k_walk_group_mixed_ab(MixArgs A) {
-  __shared__ double s_bl2[kMaxLevel + 1];
-  __shared__ double s_vb[3 * 125];
-  __shared__ int s_tw[kMixThreads / 32][kListCap];
-  __shared__ int s_lf[kMixThreads / 32][kListCap];
-  __shared__ Staged s_st[kMixThreads / 32][32];
-  for (int i = threadIdx.x; i <= kMaxLevel; i += blockDim.x) s_bl2[i] = A.bl2[i];
-  for (int i = threadIdx.x; i < 3 * A.nbox; i += blockDim.x) s_vb[i] = A.vbox[i];
-  __syncthreads();
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int* tw = s_tw[w];
-  int* lf = s_lf[w];
-  Staged* st = s_st[w];
-  const unsigned M = (unsigned)A.M;
-  const double theta2 = (double)A.theta2_64;
-  const int64_t nbuckets = A.tiles ? A.ntiles : (A.nt + 31) / 32;
-  unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
-  for (;;) {
-    unsigned b = 0;
-    if (lane == 0) b = atomicAdd(&g_bucket_counter_mixed, 1u);
-    b = __shfl_sync(0xffffffffu, b, 0);
-    if ((int64_t)b >= nbuckets) break;
-    int64_t t0;
-    int cnt;
-    if (A.tiles) {
-      const int2 tl = A.tiles[b];
-      t0 = tl.x;
-      cnt = tl.y;
-    } else {
-      t0 = (int64_t)b * 32;
-      cnt = (int)min((int64_t)32, A.nt - t0);
-    }
-    const bool valid = lane < cnt;
-    const int64_t t = t0 + lane;
-    double px = 0, py = 0, pz = 0;
-    double E0 = 0, E1 = 0, E2 = 0, PH = 0, W = 0;
-    if (valid) {
-      px = A.tx[t]; py = A.ty[t]; pz = A.tz[t];
-      E0 = A.ex[t]; E1 = A.ey[t]; E2 = A.ez[t]; PH = A.pot[t]; W = A.work[t];
-    }
-    bool complete = true;
-    for (int ib = 0; ib < A.nbox; ++ib) {
-      const double sx = px - s_vb[3 * ib], sy = py - s_vb[3 * ib + 1], sz = pz - s_vb[3 * ib + 2];
-      int64_t partner = 0;
-      unsigned u = 0;
-      while (u < M) {
-        // ---- phase A: fill the lists
-        int nt_ = 0, nl_ = 0;
-        while (u < M && nt_ < kListCap && nl_ < kListCap) {
-          const double4 a = A.nc4[u];
-          const int2 mu = A.meta[u];
-          if (mu.y & kLeafFlag) {
-            if (lane == 0) lf[nl_] = (int)u;
-            ++nl_;
-            partner += 1;
-            u = u + 1;
-          } else {
-            const double dx = sx - a.x, dy = sy - a.y, dz = sz - a.z;
-            const double d2 = (dx * dx + dy * dy) + dz * dz;
-            const bool ok = !valid || (theta2 * d2 > s_bl2[mu.y & 0xff]);
-            const unsigned fail = __ballot_sync(0xffffffffu, !ok);
-            const int first_fail = fail ? __ffs(fail) - 1 : 32;
-            if (valid && lane <= first_fail) ++c_mac;
-            if (fail == 0) {
-              if (lane == 0) tw[nt_] = (int)u;
-              ++nt_;
-              partner += A.nleaves[u];
-              u = (unsigned)mu.x;
-            } else {
-              u = u + 1;
-            }
-          }
-        }
-        __syncwarp();
-        W += (double)(nt_ + nl_);
-        // ---- phase B: twigs
-        for (int base = 0; base < nt_; base += 32) {
-          const int k = base + lane;
-          if (k < nt_) {
-            const int nd = tw[k];
-            const double4 a = A.nc4[nd];
-            Staged sv;
-            sv.cx = a.x; sv.cy = a.y; sv.cz = a.z; sv.q = a.w;
-            sv.m0 = A.mom32[3 * (int64_t)nd];
-            sv.m1 = A.mom32[3 * (int64_t)nd + 1];
-            sv.m2 = A.mom32[3 * (int64_t)nd + 2];
-            st[lane] = sv;
-          }
-          __syncwarp();
-          const int cntb = min(32, nt_ - base);
-          float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
-          if (valid) {
-            for (int j = 0; j < cntb; ++j) {
-              const double cx = st[j].cx, cy = st[j].cy, cz = st[j].cz;
-              const float dx = (float)(sx - cx), dy = (float)(sy - cy), dz = (float)(sz - cz);
-              twig32(st[j].m0, st[j].m1, st[j].m2, dx, dy, dz, A.eps2, ax, ay, az, ap);
-            }
-            c_twig += (unsigned)cntb;
-          }
-          E0 += (double)ax; E1 += (double)ay; E2 += (double)az; PH += (double)ap;
-          __syncwarp();
-        }
-        // ---- phase B: leaves
-        for (int base = 0; base < nl_; base += 32) {
-          const int k = base + lane;
-          if (k < nl_) {
-            const double4 a = A.nc4[lf[k]];
-            st[lane].cx = a.x; st[lane].cy = a.y; st[lane].cz = a.z; st[lane].q = a.w;
-          }
-          __syncwarp();
-          const int cntb = min(32, nl_ - base);
-          float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
-          if (valid) {
-            for (int j = 0; j < cntb; ++j) {
-              const double dx64 = sx - st[j].cx, dy64 = sy - st[j].cy, dz64 = sz - st[j].cz;
-              if (dx64 == 0.0 && dy64 == 0.0 && dz64 == 0.0) continue;  // self
-              leaf32((float)st[j].q, (float)dx64, (float)dy64, (float)dz64, A.eps2, ax, ay, az, ap);
-              ++c_leaf;
-            }
-          }
-          E0 += (double)ax; E1 += (double)ay; E2 += (double)az; PH += (double)ap;
-          __syncwarp();
-        }
-      }
-      if (partner != A.npart) complete = false;
-    }
-    if (valid) {
-      A.ex[t] = E0; A.ey[t] = E1; A.ez[t] = E2; A.pot[t] = PH; A.work[t] = W;
-    }
-    if (!complete && lane == 0) atomicOr(A.status, ST_INCOMPLETE);
-  }
-  warp_add3(A.counters, c_leaf, c_twig, c_mac);
-}
-
-// Group walk with a wide traversal (the default GROUP kernel).
-// The warp's 32 targets form the group; the traversal pops up to 32 nodes
-// from a per-warp LIFO stack (global memory) and lane k decides node k:
-//   leaf   -> queued for direct evaluation,
-//   twig   -> accepted if every target of the group passes the Barnes-Hut MAC
-//             (module_tree_walk_simple.f90:343-382 semantics), else its
-//             children (child8 table) are pushed.
-// The MAC uses the targets' offsets from the group centre in FP32; a bounding
-// sphere of the group gives a quick accept / quick open before the per-target
-// loop.  Queued twigs and leaves are evaluated 32 at a time from a shared
-// staging area (lane k loads node k, then every lane reads all of them), so
-// node loads never sit on the per-interaction dependency chain.
+// Group walk (GROUP and PER_TILE modes): per-tile semantics
+// (module_tree_walk_simple.f90:256-384) -- a twig is accepted only if every
+// target of the warp's group passes the Barnes-Hut MAC, else it is opened --
+// with a wide traversal.  The traversal pops up to 32 nodes from a per-warp
+// LIFO stack (global memory) and lane k decides node k:
+//   leaf -> queued for evaluation;
+//   twig -> the group's bounding sphere decides most nodes at once (every
+//           target farther than the MAC distance: accept; none: open); the
+//           rest get the exact test one node at a time across the warp
+//           (lane = target, a ballot of the failures); opened twigs push
+//           their children (child8 table).
+// A popped node's centre, level, leaf count and child table are loaded in
+// one round.  The MAC is evaluated on the FP32 group-centred offsets, and
+// the same offsets go straight into the node's staging record: accepted
+// twigs and leaves are written into per-warp ring buffers in shared memory
+// at decision time (the twig moments by cp.async), so a batch of 32 is
+// evaluated without a load on its critical path; every lane then reads all
+// staged records by broadcast.
 // Stack bound: a pop takes <= 32 entries and pushes <= 8 per node, so the
 // stack never holds more than (kMaxLevel + 1) * 8 * 32 entries; kStackCap
 // leaves a margin and an overflow sets ST_INCOMPLETE instead of writing past it.
 constexpr int kStackCap = 8192;
 constexpr int kWW = kMixThreads / 32;  // warps per block
+constexpr int kRing = 64;              // staging ring (<= 31 pending + 32 new)
 
 __device__ __forceinline__ int warp_excl_scan(int v, int lane, int& total) {
   int x = v;
@@ -387,25 +153,40 @@ __device__ __forceinline__ int warp_excl_scan(int v, int lane, int& total) {
   return x - v;
 }
 
-__global__ void __launch_bounds__(kMixThreads) k_walk_group_wide(MixArgs A, int* __restrict__ gstack,
-                                                                 const int4* __restrict__ child8,
-                                                                 const int* __restrict__ nchild) {
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+struct __align__(16) StagedTwig {
+  float4 c;   // (coc - g) rounded from FP64, charge
+  float4 m0;  // px py pz 3qxx
+  float4 m1;  // 3qyy 3qzz 1.5qxy 1.5qyz
+  float4 m2;  // 1.5qzx, trace, charge, -
+};
+struct __align__(16) StagedLeaf {
+  float4 c;          // (x - g) rounded from FP64, charge
+  double x, y, z;    // FP64 position, for the exact self test
+};
+
+__global__ void __launch_bounds__(kMixThreads, 5)
+    k_walk_group_wide(MixArgs A, int* __restrict__ gstack, const int4* __restrict__ child8,
+                      const int* __restrict__ nchild) {
   __shared__ float s_bl2[kMaxLevel + 1];
   __shared__ double s_vb[3 * 125];
-  __shared__ float4 s_t[kWW][32];
-  __shared__ int s_tw[kWW][64];
-  __shared__ int s_lf[kWW][64];
-  __shared__ Staged s_st[kWW][32];
+  __shared__ StagedTwig s_tw[kWW][kRing];
+  __shared__ StagedLeaf s_lf[kWW][kRing];
   for (int i = threadIdx.x; i <= kMaxLevel; i += blockDim.x) s_bl2[i] = (float)A.bl2[i];
   for (int i = threadIdx.x; i < 3 * A.nbox; i += blockDim.x) s_vb[i] = A.vbox[i];
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
   int* stack = gstack + (int64_t)(blockIdx.x * kWW + w) * kStackCap;
-  float4* tt = s_t[w];
-  int* tw = s_tw[w];
-  int* lf = s_lf[w];
-  Staged* st = s_st[w];
+  StagedTwig* stw = s_tw[w];
+  StagedLeaf* stl = s_lf[w];
   const float theta2 = A.theta2;
   const int64_t nbuckets = A.tiles ? A.ntiles : (A.nt + 31) / 32;
   unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
@@ -425,6 +206,7 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_group_wide(MixArgs A, int*
       cnt = (int)min((int64_t)32, A.nt - t0);
     }
     const bool valid = lane < cnt;
+    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
     const int64_t t = t0 + lane;
     double px = 0, py = 0, pz = 0;
     double E0 = 0, E1 = 0, E2 = 0, PH = 0, W = 0;
@@ -446,66 +228,59 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_group_wide(MixArgs A, int*
     float rg = valid ? sqrtf(rx * rx + ry * ry + rz * rz) : 0.f;
     for (int o = 16; o > 0; o >>= 1) rg = fmaxf(rg, __shfl_xor_sync(0xffffffffu, rg, o));
     rg = rg * 1.0001f + 1e-30f;  // the sphere must contain every target after rounding
-    tt[lane] = make_float4(rx, ry, rz, valid ? 1.f : 0.f);
-    __syncwarp();
     bool complete = true;
     for (int ib = 0; ib < A.nbox; ++ib) {
       const double vx = s_vb[3 * ib], vy = s_vb[3 * ib + 1], vz = s_vb[3 * ib + 2];
       const double sx = px - vx, sy = py - vy, sz = pz - vz;
       const double gx = g0x - vx, gy = g0y - vy, gz = g0z - vz;
-      int64_t partner = 0;
-      int nT = 0, nL = 0;
+      int64_t partner = 0;  // leaves covered by this lane's nodes (summed over the warp at the end)
+      int nT = 0, hT = 0, nL = 0, hL = 0;  // ring counts and heads
       int top = 1;
       if (lane == 0) stack[0] = 0;  // the root (walk_simple starts at the root, :286)
       __syncwarp();
-      // evaluates the first n queued twigs / leaves and removes them
+      // evaluates the n staged twigs / leaves at the ring heads
       auto flush_twigs = [&](int n) {
-        if (lane < n) {
-          const int nd = tw[lane];
-          const double4 a = A.nc4[nd];
-          Staged sv;
-          sv.cx = a.x; sv.cy = a.y; sv.cz = a.z; sv.q = a.w;
-          sv.m0 = A.mom32[3 * (int64_t)nd];
-          sv.m1 = A.mom32[3 * (int64_t)nd + 1];
-          sv.m2 = A.mom32[3 * (int64_t)nd + 2];
-          st[lane] = sv;
-        }
+        cp_async_wait_all();
         __syncwarp();
         if (valid) {
           float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
+#pragma unroll 4
           for (int j = 0; j < n; ++j) {
-            const float dx = (float)(sx - st[j].cx), dy = (float)(sy - st[j].cy),
-                        dz = (float)(sz - st[j].cz);
-            twig32(st[j].m0, st[j].m1, st[j].m2, dx, dy, dz, A.eps2, ax, ay, az, ap);
+            const StagedTwig& r = stw[(hT + j) & (kRing - 1)];
+            const float4 c = r.c;
+            twig32(r.m0, r.m1, r.m2, rx - c.x, ry - c.y, rz - c.z, A.eps2, ax, ay, az, ap);
           }
           E0 += (double)ax; E1 += (double)ay; E2 += (double)az; PH += (double)ap;
           c_twig += (unsigned)n;
         }
         W += (double)n;
-        __syncwarp();
-        if (lane + n < nT) tw[lane] = tw[lane + n];
+        hT = (hT + n) & (kRing - 1);
         nT -= n;
         __syncwarp();
       };
       auto flush_leaves = [&](int n) {
-        if (lane < n) {
-          const double4 a = A.nc4[lf[lane]];
-          st[lane].cx = a.x; st[lane].cy = a.y; st[lane].cz = a.z; st[lane].q = a.w;
-        }
         __syncwarp();
         if (valid) {
           float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
+#pragma unroll 4
           for (int j = 0; j < n; ++j) {
-            const double dx64 = sx - st[j].cx, dy64 = sy - st[j].cy, dz64 = sz - st[j].cz;
-            if (dx64 == 0.0 && dy64 == 0.0 && dz64 == 0.0) continue;  // self
-            leaf32((float)st[j].q, (float)dx64, (float)dy64, (float)dz64, A.eps2, ax, ay, az, ap);
+            const StagedLeaf& r = stl[(hL + j) & (kRing - 1)];
+            const float4 c = r.c;
+            float dx = rx - c.x, dy = ry - c.y, dz = rz - c.z;
+            if (dx == 0.f && dy == 0.f && dz == 0.f) {
+              // self (dist2 == 0 in FP64) or two points closer than the FP32
+              // resolution at the group scale: decide and evaluate in FP64
+              const double ex = sx - r.x, ey = sy - r.y, ez = sz - r.z;
+              if (ex == 0.0 && ey == 0.0 && ez == 0.0) continue;
+              dx = (float)ex; dy = (float)ey; dz = (float)ez;
+            }
+            leaf32(c.w, dx, dy, dz, A.eps2, ax, ay, az, ap);
             ++c_leaf;
           }
           E0 += (double)ax; E1 += (double)ay; E2 += (double)az; PH += (double)ap;
         }
         W += (double)n;
-        __syncwarp();
-        if (lane + n < nL) lf[lane] = lf[lane + n];
+        hL = (hL + n) & (kRing - 1);
         nL -= n;
         __syncwarp();
       };
@@ -514,16 +289,24 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_group_wide(MixArgs A, int*
         top -= take;
         const int node = lane < take ? stack[top + lane] : -1;
         __syncwarp();
-        bool isleaf = false, accept = false, open = false;
-        int nleaf_acc = 0;
+        bool isleaf = false, accept = false, open = false, amb = false;
+        float cx = 0.f, cy = 0.f, cz = 0.f, bl = 0.f;
+        double4 a = make_double4(0, 0, 0, 0);
+        int nlv = 0, nch = 0;
+        int4 c0 = make_int4(0, 0, 0, 0), c1 = c0;
         if (node >= 0) {
-          const double4 a = A.nc4[node];
+          // one round of loads: what accept, open and leaf each need
+          a = A.nc4[node];
           const int2 mu = A.meta[node];
+          nlv = A.nleaves[node];
+          nch = nchild[node];
+          c0 = child8[2 * (int64_t)node];
+          c1 = child8[2 * (int64_t)node + 1];
+          cx = (float)(a.x - gx); cy = (float)(a.y - gy); cz = (float)(a.z - gz);
           if (mu.y & kLeafFlag) {
             isleaf = true;
           } else {
-            const float cx = (float)(a.x - gx), cy = (float)(a.y - gy), cz = (float)(a.z - gz);
-            const float bl = s_bl2[mu.y & 0xff];
+            bl = s_bl2[mu.y & 0xff];
             const float dc = sqrtf(cx * cx + cy * cy + cz * cz);
             const float dmin = dc - rg, dmax = dc + rg;
             if (dmin > 0.f && theta2 * (dmin * dmin) > bl) {
@@ -533,43 +316,67 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_group_wide(MixArgs A, int*
               open = true;    // no target can pass
               c_mac += 1;
             } else {
-              accept = true;
-              for (int j = 0; j < 32; ++j) {
-                const float4 q4 = tt[j];
-                if (q4.w == 0.f) continue;
-                const float dx = q4.x - cx, dy = q4.y - cy, dz = q4.z - cz;
-                ++c_mac;
-                if (!(theta2 * fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > bl)) {
-                  accept = false;
-                  break;
-                }
-              }
-              open = !accept;
+              amb = true;
             }
-            if (accept) nleaf_acc = A.nleaves[node];
+          }
+        }
+        // the exact MAC for the undecided nodes, one node at a time across
+        // the targets (lane = target): accepted iff no target fails
+        unsigned am = __ballot_sync(0xffffffffu, amb);
+        while (am) {
+          const int j = __ffs(am) - 1;
+          am &= am - 1;
+          const float ux = __shfl_sync(0xffffffffu, cx, j);
+          const float uy = __shfl_sync(0xffffffffu, cy, j);
+          const float uz = __shfl_sync(0xffffffffu, cz, j);
+          const float ub = __shfl_sync(0xffffffffu, bl, j);
+          const float dx = rx - ux, dy = ry - uy, dz = rz - uz;
+          const bool fail = valid && !(theta2 * fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > ub);
+          const unsigned f = __ballot_sync(0xffffffffu, fail);
+          if (lane == j) {
+            accept = (f == 0);
+            open = !accept;
+            // MAC evaluations up to the first failing target, in target order
+            c_mac += (unsigned)__popc(f ? (vmask & ((2u << (__ffs(f) - 1)) - 1u)) : vmask);
           }
         }
         const unsigned lb = __ballot_sync(0xffffffffu, isleaf);
         const unsigned ab = __ballot_sync(0xffffffffu, accept);
-        if (isleaf) lf[nL + __popc(lb & lt)] = node;
-        if (accept) tw[nT + __popc(ab & lt)] = node;
+        if (isleaf) {
+          StagedLeaf& r = stl[(hL + nL + __popc(lb & lt)) & (kRing - 1)];
+          r.c = make_float4(cx, cy, cz, (float)a.w);
+          r.x = a.x; r.y = a.y; r.z = a.z;
+          partner += 1;
+        }
+        if (accept) {
+          StagedTwig& r = stw[(hT + nT + __popc(ab & lt)) & (kRing - 1)];
+          r.c = make_float4(cx, cy, cz, (float)a.w);
+          const float4* m = A.mom32 + 3 * (int64_t)node;
+          cp_async16(&r.m0, m);
+          cp_async16(&r.m1, m + 1);
+          cp_async16(&r.m2, m + 2);
+          partner += nlv;
+        }
         nL += __popc(lb);
         nT += __popc(ab);
-        int pl = nleaf_acc;
-        for (int o = 16; o > 0; o >>= 1) pl += __shfl_xor_sync(0xffffffffu, pl, o);
-        partner += (int64_t)pl + __popc(lb);
         // push the children of opened twigs
-        const int nch = open ? min(8, nchild[node]) : 0;
+        const int npush = open ? min(8, nch) : 0;
         int total;
-        const int off = warp_excl_scan(nch, lane, total);
+        const int off = warp_excl_scan(npush, lane, total);
         if (top + total > kStackCap) {
           complete = false;  // cannot happen within the bound above
           break;
         }
-        if (nch > 0) {
-          const int4 c0 = child8[2 * (int64_t)node], c1 = child8[2 * (int64_t)node + 1];
-          const int cc[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-          for (int k = 0; k < nch; ++k) stack[top + off + k] = cc[k];
+        if (npush > 0) {
+          int* dst = stack + top + off;
+          dst[0] = c0.x;
+          if (npush > 1) dst[1] = c0.y;
+          if (npush > 2) dst[2] = c0.z;
+          if (npush > 3) dst[3] = c0.w;
+          if (npush > 4) dst[4] = c1.x;
+          if (npush > 5) dst[5] = c1.y;
+          if (npush > 6) dst[6] = c1.z;
+          if (npush > 7) dst[7] = c1.w;
         }
         top += total;
         __syncwarp();
@@ -578,6 +385,7 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_group_wide(MixArgs A, int*
       }
       if (nT > 0) flush_twigs(nT);
       if (nL > 0) flush_leaves(nL);
+      for (int o = 16; o > 0; o >>= 1) partner += __shfl_xor_sync(0xffffffffu, partner, o);
       if (partner != A.npart) complete = false;
     }
     if (valid) {
@@ -585,6 +393,7 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_group_wide(MixArgs A, int*
     }
     if (__any_sync(0xffffffffu, !complete) && lane == 0) atomicOr(A.status, ST_INCOMPLETE);
   }
+  cp_async_wait_all();
   warp_add3(A.counters, c_leaf, c_twig, c_mac);
 }
 
@@ -674,7 +483,6 @@ __global__ void k_reset_mixed() { g_bucket_counter_mixed = 0; }
 int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                       double* ex, double* ey, double* ez, double* pot, double* work,
                       const int2* tiles, int64_t ntiles, bool per_target) {
-  const int blocks = 148 * 8;
   MixArgs A;
   A.nt = nt;
   A.tx = tx; A.ty = ty; A.tz = tz;
@@ -686,7 +494,6 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
   A.vbox = c->d_vbox;
   A.nbox = c->nboxes;
   A.theta2 = (float)c->prm.theta2;
-  A.theta2_64 = c->prm.theta2;
   A.eps2 = (float)c->prm.eps2;
   A.M = (int32_t)c->nnodes;
   A.npart = c->n;
@@ -700,14 +507,13 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
   k_reset_mixed<<<1, 1, 0, s>>>();
   COUNT_LAUNCH();
   if (per_target) {
-    k_walk_target_mixed<<<blocks, kMixThreads, 0, s>>>(A);
-  } else if (c->prm.reserved[0] == 1) {
-    k_walk_group_mixed<<<blocks, kMixThreads, 0, s>>>(A);
-  } else if (c->prm.reserved[0] == 2) {
-    k_walk_group_mixed_ab<<<blocks, kMixThreads, 0, s>>>(A);
+    k_walk_target_mixed<<<148 * 8, kMixThreads, 0, s>>>(A);
   } else {
-    if (!ensure(c, c->wstack, (size_t)blocks * kWW * kStackCap, "walk stacks")) return PEPCG_ERR_OOM;
-    k_walk_group_wide<<<blocks, kMixThreads, 0, s>>>(A, c->wstack.p, c->child8.p, c->nchild.p);
+    // 5 resident blocks per SM (launch bounds: 96 registers, 31.8 KB shared
+    // memory each); the grid is exactly one wave
+    const int gblocks = 148 * 5;
+    if (!ensure(c, c->wstack, (size_t)gblocks * kWW * kStackCap, "walk stacks")) return PEPCG_ERR_OOM;
+    k_walk_group_wide<<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p, c->child8.p, c->nchild.p);
   }
   return cuda_ok(c, cudaGetLastError(), "mixed walk launch") ? PEPCG_OK : PEPCG_ERR_CUDA;
 }
