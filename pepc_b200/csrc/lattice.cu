@@ -261,39 +261,80 @@ __global__ void k_box_dipole(int64_t n, const double* __restrict__ x, const doub
   }
 }
 
-// omega_tilde partials (calc_omega_tilde, :514-596): one thread per (l, m),
-// each block sums a contiguous chunk of particles
+// omega_tilde partials (calc_omega_tilde, :514-596).  Lane m (< 21) of each
+// warp takes the order m of every harmonic of its particles: LegendreP's
+// recurrence (:1196-1242) runs once up through l = 20, giving P_l^m for every
+// l >= m in the same operations as a separate call per l; r^l is carried by
+// multiplication and e^{-i m phi} comes from one sincos.  Each block sums a
+// contiguous chunk of particles (warp partials added in shared memory).
 constexpr int kOmChunk = 1024;
+constexpr int kOmWarps = 8;
 __global__ void __launch_bounds__(256) k_omega_partial(int64_t n, const double* __restrict__ x,
                                                        const double* __restrict__ y,
                                                        const double* __restrict__ z,
                                                        const double* __restrict__ q, double cx,
                                                        double cy, double cz, const double* fact,
                                                        double2* __restrict__ part) {
-  __shared__ double sp[kOmChunk][4];
+  __shared__ double2 s_acc[kOmWarps][kLenM];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int m = lane;
   const int64_t base = (int64_t)blockIdx.x * kOmChunk;
   const int cnt = (int)min((int64_t)kOmChunk, n - base);
-  for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-    double s[3];
-    cart2sph(x[base + i] - cx, y[base + i] - cy, z[base + i] - cz, s);
-    sp[i][0] = s[0];
-    sp[i][1] = s[1];
-    sp[i][2] = s[2];
-    sp[i][3] = q[base + i];
+  double2 acc[kLM + 1];
+#pragma unroll
+  for (int l = 0; l <= kLM; ++l) acc[l] = make_double2(0.0, 0.0);
+  if (m <= kLM) {
+    for (int i = w; i < cnt; i += kOmWarps) {
+      double sph[3];
+      cart2sph(x[base + i] - cx, y[base + i] - cy, z[base + i] - cz, sph);
+      const double qi = q[base + i];
+      const double xc = sph[1];
+      double sn, cs;
+      sincos((double)m * sph[2], &sn, &cs);
+      const double sg = (m & 1) ? -1.0 : 1.0;
+      double pmm = 1.0;
+      if (m > 0) {
+        const double somx2 = sqrt((1.0 - xc) * (1.0 + xc));
+        double f = 1.0;
+        for (int k = 1; k <= m; ++k) {
+          pmm = (-pmm * f) * somx2;
+          f = f + 2.0;
+        }
+      }
+      double pmmp1 = 0.0, rl = 1.0;
+#pragma unroll
+      for (int l = 0; l <= kLM; ++l) {
+        if (l >= m) {
+          double P;
+          if (l == m) {
+            P = pmm;
+          } else if (l == m + 1) {
+            pmmp1 = (xc * (2.0 * m + 1.0)) * pmm;
+            P = pmmp1;
+          } else {
+            const double pll =
+                ((xc * (2.0 * l - 1.0)) * pmmp1 - ((double)(l + m) - 1.0) * pmm) / (double)(l - m);
+            pmm = pmmp1;
+            pmmp1 = pll;
+            P = pll;
+          }
+          const double pt = (sg * P) / fact[l + m];
+          const double amp = (sph[0] > 0.0 || l > 0) ? rl * pt : pt;
+          acc[l] = cadd(acc[l], make_double2(qi * (amp * cs), qi * (amp * -sn)));
+        }
+        rl = rl * sph[0];
+      }
+    }
   }
+#pragma unroll
+  for (int l = 0; l <= kLM; ++l)
+    if (m <= l) s_acc[w][tblinv(l, m)] = acc[l];
   __syncthreads();
-  const int idx = threadIdx.x;
-  if (idx >= kLenM) return;
-  int l = 0;
-  while ((l + 1) * (l + 2) / 2 <= idx) ++l;
-  const int m = idx - l * (l + 1) / 2;
-  double2 acc = make_double2(0.0, 0.0);
-  for (int i = 0; i < cnt; ++i) {
-    double s[3] = {sp[i][0], sp[i][1], sp[i][2]};
-    double2 o = omultipole(l, m, s, fact);
-    acc = cadd(acc, make_double2(sp[i][3] * o.x, sp[i][3] * o.y));
+  for (int idx = threadIdx.x; idx < kLenM; idx += blockDim.x) {
+    double2 t = s_acc[0][idx];
+    for (int ww = 1; ww < kOmWarps; ++ww) t = cadd(t, s_acc[ww][idx]);
+    part[(int64_t)blockIdx.x * kLenM + idx] = t;
   }
-  part[(int64_t)blockIdx.x * kLenM + idx] = acc;
 }
 
 // sum the partials in block order, add the fictitious charges (:536-559),
@@ -397,28 +438,58 @@ __global__ void __launch_bounds__(128) k_lattice_force(
     const double R0 = px - cx, R1 = py - cy, R2 = pz - cz;
     double s[3];
     cart2sph(R0, R1, R2, s);
-    double2 OR[kLenM];
-    for (int l = 0; l <= kLM; ++l)
-      for (int m = 0; m <= l; ++m) OR[tblinv(l, m)] = omultipole(l, m, s, s_fact);
-    double2 ms[3];
-    for (int l = 0; l <= 1; ++l)
-      for (int m = 0; m <= l; ++m) {  // L2L, :943-976 with max_l = 1
-        double2 acc = make_double2(0.0, 0.0);
-        for (int j = l; j <= kLM; ++j)
-          for (int k = -j; k <= j; ++k) {
-            const int a = j - l, b = k - m;
-            double2 o = make_double2(0.0, 0.0);
-            if (abs(b) <= a) {
-              o = OR[tblinv(a, abs(b))];
-              if (b < 0) {
-                const double sg = (b & 1) ? -1.0 : 1.0;
-                o = make_double2(sg * o.x, -sg * o.y);
-              }
-            }
-            acc = cadd(acc, cmul(o, tbl(s_mu, j, k, kLM)));
-          }
-        ms[tblinv(l, m)] = acc;
+    // O_R(a, b) at the target (OMultipole, :695-714) times mu, L2L to l <= 1
+    // (:943-976 with max_l = 1): output (l, m') collects O_R(a, b) mu(a + l,
+    // b + m') over |b| <= a <= 20.  The harmonics are generated order by
+    // order: for each m, one sincos, LegendreP's recurrence through a = 20
+    // and r^a by multiplication, and O_R(a, -m) = (-1)^m conj(O_R(a, m)).
+    double2 ms[3] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+    for (int m = 0; m <= kLM; ++m) {
+      double sn, cs;
+      sincos((double)m * s[2], &sn, &cs);
+      const double sg = (m & 1) ? -1.0 : 1.0;
+      const double xc = s[1];
+      double pmm = 1.0;
+      if (m > 0) {
+        const double somx2 = sqrt((1.0 - xc) * (1.0 + xc));
+        double f = 1.0;
+        for (int k = 1; k <= m; ++k) {
+          pmm = (-pmm * f) * somx2;
+          f = f + 2.0;
+        }
       }
+      double rl = 1.0;
+      for (int k = 0; k < m; ++k) rl = rl * s[0];
+      double pmmp1 = 0.0;
+      for (int a = m; a <= kLM; ++a) {
+        double P;
+        if (a == m) {
+          P = pmm;
+        } else if (a == m + 1) {
+          pmmp1 = (xc * (2.0 * m + 1.0)) * pmm;
+          P = pmmp1;
+        } else {
+          const double pll =
+              ((xc * (2.0 * a - 1.0)) * pmmp1 - ((double)(a + m) - 1.0) * pmm) / (double)(a - m);
+          pmm = pmmp1;
+          pmmp1 = pll;
+          P = pll;
+        }
+        const double pt = (sg * P) / s_fact[a + m];
+        const double amp = (s[0] > 0.0 || a > 0) ? rl * pt : pt;
+        rl = rl * s[0];
+        const double2 o = make_double2(amp * cs, amp * -sn);
+        ms[0] = cadd(ms[0], cmul(o, tbl(s_mu, a, m, kLM)));
+        ms[1] = cadd(ms[1], cmul(o, tbl(s_mu, a + 1, m, kLM)));
+        ms[2] = cadd(ms[2], cmul(o, tbl(s_mu, a + 1, m + 1, kLM)));
+        if (m > 0) {
+          const double2 on = make_double2(sg * o.x, -sg * o.y);
+          ms[0] = cadd(ms[0], cmul(on, tbl(s_mu, a, -m, kLM)));
+          ms[1] = cadd(ms[1], cmul(on, tbl(s_mu, a + 1, -m, kLM)));
+          ms[2] = cadd(ms[2], cmul(on, tbl(s_mu, a + 1, -m + 1, kLM)));
+        }
+      }
+    }
     double e0 = -ms[2].x, e1 = -ms[2].y, e2 = -ms[1].x, ph = ms[0].x;
     if (corr == 1) {
       e0 = e0 + (2.0 * prefact) * s_aux[0];

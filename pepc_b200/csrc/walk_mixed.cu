@@ -244,11 +244,19 @@ __global__ void __launch_bounds__(kMixThreads, 5)
         __syncwarp();
         if (valid) {
           float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
+          // the batch is at most two contiguous runs of the ring
+          const int n1 = min(n, kRing - hT);
+          const StagedTwig* r = stw + hT;
 #pragma unroll 4
-          for (int j = 0; j < n; ++j) {
-            const StagedTwig& r = stw[(hT + j) & (kRing - 1)];
-            const float4 c = r.c;
-            twig32(r.m0, r.m1, r.m2, rx - c.x, ry - c.y, rz - c.z, A.eps2, ax, ay, az, ap);
+          for (int j = 0; j < n1; ++j) {
+            const float4 c = r[j].c;
+            twig32(r[j].m0, r[j].m1, r[j].m2, rx - c.x, ry - c.y, rz - c.z, A.eps2, ax, ay, az, ap);
+          }
+#pragma unroll 4
+          for (int j = 0; j < n - n1; ++j) {
+            const float4 c = stw[j].c;
+            twig32(stw[j].m0, stw[j].m1, stw[j].m2, rx - c.x, ry - c.y, rz - c.z, A.eps2, ax, ay,
+                   az, ap);
           }
           E0 += (double)ax; E1 += (double)ay; E2 += (double)az; PH += (double)ap;
           c_twig += (unsigned)n;
