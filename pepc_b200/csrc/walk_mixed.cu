@@ -270,21 +270,26 @@ __global__ void __launch_bounds__(kMixThreads, 5)
         __syncwarp();
         if (valid) {
           float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
-#pragma unroll 4
-          for (int j = 0; j < n; ++j) {
-            const StagedLeaf& r = stl[(hL + j) & (kRing - 1)];
+          auto leaf = [&](const StagedLeaf& r) {
             const float4 c = r.c;
             float dx = rx - c.x, dy = ry - c.y, dz = rz - c.z;
             if (dx == 0.f && dy == 0.f && dz == 0.f) {
               // self (dist2 == 0 in FP64) or two points closer than the FP32
               // resolution at the group scale: decide and evaluate in FP64
               const double ex = sx - r.x, ey = sy - r.y, ez = sz - r.z;
-              if (ex == 0.0 && ey == 0.0 && ez == 0.0) continue;
+              if (ex == 0.0 && ey == 0.0 && ez == 0.0) return;
               dx = (float)ex; dy = (float)ey; dz = (float)ez;
             }
             leaf32(c.w, dx, dy, dz, A.eps2, ax, ay, az, ap);
             ++c_leaf;
-          }
+          };
+          // the batch is at most two contiguous runs of the ring
+          const int n1 = min(n, kRing - hL);
+          const StagedLeaf* r = stl + hL;
+#pragma unroll 4
+          for (int j = 0; j < n1; ++j) leaf(r[j]);
+#pragma unroll 4
+          for (int j = 0; j < n - n1; ++j) leaf(stl[j]);
           E0 += (double)ax; E1 += (double)ay; E2 += (double)az; PH += (double)ap;
         }
         W += (double)n;
