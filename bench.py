@@ -155,6 +155,22 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(ms, dist, device):
+    """The slowest rank's time: every rank's replica must finish for the job's step
+    to end.  `dist` is torch.distributed (or None for one rank)."""
+    if not dist:
+        return ms
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(n_per_rank, world, ms):
+    """Whole-job force evaluations per second: every rank's N over the slowest time."""
+    return n_per_rank * world / (ms * 1e-3)
+
+
 def uniform_sphere(n, seed=2):
     """Uniform in the unit sphere: radius u^(1/3), isotropic direction."""
     rng = np.random.default_rng(seed)
@@ -404,15 +420,12 @@ def main():
             dist.barrier()
         ms = e0.elapsed_time(e1) / steps
         launches = (P.kernel_launches() - l0)
-        if dist:
-            tt = torch.tensor([ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ms = float(tt.item())
+        ms = max_over_ranks(ms, dist, dev)
         return ms, launches, (ctx.summary() if ctx else None)
 
     ms, launches, clk = timed(tc, args.steps, args.warmup, clocks=True)
     st = tc.stats()
-    value = n * world / (ms * 1e-3)
+    value = job_rate(n, world, ms)
 
     # accuracy of this step's result against an FP64 direct sum on sampled targets
     rng = np.random.default_rng(33)
@@ -495,10 +508,7 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1) / ksteps
-        if dist:
-            tt = torch.tensor([ems], device=dev, dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ems = float(tt.item())
+        ems = max_over_ranks(ems, dist, dev)
         # grow: x y z q in; key, perm (int32), x y z out.  traverse: x y z, key,
         # e(3) pot work in; e(3) pot work out
         h2d = n * (4 * 8) + n * (3 * 8 + 8 + 5 * 8)

@@ -84,3 +84,24 @@ def test_mixed_group_periodic_matches_plain(gpu):
     # alternating charges cancel, so FP32 rounding shows more than for equal charges
     assert np.median(diff) < 2e-5, np.median(diff)
     assert np.mean(rm["work"] == rp["work"]) > 0.99
+
+
+def test_mixed_group_ragged_buckets_and_duplicates(gpu):
+    # N not a multiple of 32 (a partial last bucket) and coincident positions
+    # (the duplicate-key fix moves them apart by less than the FP32 resolution
+    # at the group scale, so the walk's exact FP64 self test is exercised)
+    rng = np.random.default_rng(45)
+    n = 4099
+    x, y, z = rng.random(n), rng.random(n), rng.random(n)
+    dup = rng.choice(n, 200, replace=False)
+    x[dup[:100]], y[dup[:100]], z[dup[:100]] = x[dup[100:]], y[dup[100:]], z[dup[100:]]
+    q = rng.standard_normal(n)
+    kw = dict(theta2=0.25, eps2=1e-4, walk=P.WALK_GROUP)
+    tp, gp, rp = run(x, y, z, q, precision=P.PRECISION_PLAIN, **kw)
+    tm, gm, rm = run(x, y, z, q, precision=P.PRECISION_MIXED, **kw)
+    assert np.array_equal(gp.key, gm.key)
+    idx = np.arange(n)
+    diff = relerr(rm, {"ex": rp["ex"], "ey": rp["ey"], "ez": rp["ez"]}, idx)
+    assert np.median(diff) < 2e-5, np.median(diff)
+    assert np.all(np.isfinite(rm["pot"]))
+    assert np.mean(rm["work"] == rp["work"]) > 0.99
