@@ -176,6 +176,32 @@ int pepcg_traverse_adjoint_device(void* ctx, int64_t nt, const double* d_tx, con
                                   const double* d_gez, const double* d_gphi, double* d_dq,
                                   double* d_dx, double* d_dy, double* d_dz);
 
+/*
+ * The frontend's time step around the path, on device arrays and the
+ * context's stream, so particles can stay on the GPU between steps.  These
+ * replace loops of the pepc-mini frontend rather than library routines:
+ *   pepcg_push_particles_device       push_particles (frontends/pepc-mini/
+ *     module_helper.f90:205-222): v += dt q/m E, then x += dt v (in place);
+ *   pepcg_apply_external_field_device apply_external_field (:321-334):
+ *     E_z += ez_ext, pot -= z ez_ext (in place);
+ *   pepcg_constrain_periodic_device   constrain_periodic (module_mirror_boxes.f90:
+ *     177-218): positions wrapped into the context's lattice cell along its
+ *     periodic directions (in place);
+ *   pepcg_gather_device               out[i] = in[perm[i]] with the last grow's
+ *     permutation (n of that grow), to carry per-particle state such as
+ *     velocity or mass into key order as the reference's domain_decompose
+ *     (module_domains.f90:158-319) moves whole particle records; in != out.
+ * Results are the reference expressions in their order, bit for bit.
+ */
+int pepcg_push_particles_device(void* ctx, int64_t n, double dt, const double* d_q,
+                                const double* d_m, const double* d_ex, const double* d_ey,
+                                const double* d_ez, double* d_vx, double* d_vy, double* d_vz,
+                                double* d_x, double* d_y, double* d_z);
+int pepcg_apply_external_field_device(void* ctx, int64_t n, double ez_ext, const double* d_z,
+                                      double* d_ez, double* d_pot);
+int pepcg_constrain_periodic_device(void* ctx, int64_t n, double* d_x, double* d_y, double* d_z);
+int pepcg_gather_device(void* ctx, const double* d_in, double* d_out);
+
 /* Launch all of this context's work on the caller's CUDA stream (a
  * cudaStream_t of the context's device), or on a private non-blocking stream
  * when NULL (so the legacy default stream is selected with cudaStreamLegacy).

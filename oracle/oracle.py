@@ -77,6 +77,9 @@ def lib():
         L.orc_direct_adjoint.argtypes = [C.c_void_p, C.c_int64, D, D, D, D, D, D, D, D, D, D, D]
         L.orc_direct_adjoint.restype = C.c_int
         L.orc_set_lattice_coefficients.restype = C.c_int
+        L.orc_push_particles.argtypes = [C.c_int64, C.c_double] + [D] * 11
+        L.orc_apply_external_field.argtypes = [C.c_int64, C.c_double, D, D, D]
+        L.orc_constrain_periodic.argtypes = [C.POINTER(OrcParams), C.c_int64, D, D, D]
         _LIB = L
     return _LIB
 
@@ -287,3 +290,23 @@ class Oracle:
         if rc != 0:
             raise RuntimeError("lattice term needs a periodic context")
         return dict(ex=ex, ey=ey, ez=ez, pot=pt)
+
+
+def push_particles(dt, q, m, e, v, x):
+    """pepc-mini push_particles on numpy arrays (v, x updated in place)."""
+    args = [f64(a) for a in (q, m, *e)]
+    for a in (*v, *x):
+        assert a.dtype == np.float64 and a.flags.c_contiguous
+    lib().orc_push_particles(len(q), dt, *[dp(a) for a in args],
+                             *[dp(a) for a in (*v, *x)])
+
+
+def apply_external_field(ez_ext, z, ez, pot):
+    lib().orc_apply_external_field(len(z), ez_ext, dp(f64(z)), dp(ez), dp(pot))
+
+
+def constrain_periodic(x, y, z, **kw):
+    """constrain_periodic with the lattice of params(**kw); x, y, z in place."""
+    p = params(**kw)
+    lib().orc_constrain_periodic(C.byref(p), len(x), dp(x), dp(y), dp(z))
+

@@ -1228,3 +1228,103 @@ int orc_direct_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double* t
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The frontend's time step around the path.  Test infrastructure: restates
+// pepc-mini's push_particles / apply_external_field (module_helper.f90:205-222,
+// :321-334) and constrain_periodic (module_mirror_boxes.f90:177-218) with
+// inverse3 / det3 / det2f (module_math_tools.f90:55-150).
+// ---------------------------------------------------------------------------
+namespace {
+// Fortran MODULO for reals, as fmod with the sign moved to the divisor's
+double fortran_modulo(double a, double p) {
+  double r = std::fmod(a, p);
+  if (r != 0.0 && ((r < 0.0) != (p < 0.0))) r = r + p;
+  return r;
+}
+
+void lattice_inverse(const orc_params* p, double L[3][3], double Li[3][3]) {
+  for (int j = 0; j < 3; ++j) {
+    L[0][j] = p->t_lattice_1[j];
+    L[1][j] = p->t_lattice_2[j];
+    L[2][j] = p->t_lattice_3[j];
+  }
+  // m(i, j) = L[i-1][j-1]
+  auto m = [&](int i, int j) { return L[i - 1][j - 1]; };
+  const double det = m(1, 1) * m(2, 2) * m(3, 3) + m(1, 2) * m(2, 3) * m(3, 1) +
+                     m(1, 3) * m(2, 1) * m(3, 2) - m(1, 3) * m(2, 2) * m(3, 1) -
+                     m(1, 2) * m(2, 1) * m(3, 3) - m(1, 1) * m(2, 3) * m(3, 2);
+  auto d2 = [](double a, double b, double c, double d) { return a * d - b * c; };
+  // column-major reshape of the nine 2x2 determinants
+  Li[0][0] = d2(m(2, 2), m(3, 2), m(2, 3), m(3, 3)) / det;
+  Li[1][0] = d2(m(2, 3), m(3, 3), m(2, 1), m(3, 1)) / det;
+  Li[2][0] = d2(m(2, 1), m(3, 1), m(2, 2), m(3, 2)) / det;
+  Li[0][1] = d2(m(1, 3), m(3, 3), m(1, 2), m(3, 2)) / det;
+  Li[1][1] = d2(m(1, 1), m(3, 1), m(1, 3), m(3, 3)) / det;
+  Li[2][1] = d2(m(1, 2), m(3, 2), m(1, 1), m(3, 1)) / det;
+  Li[0][2] = d2(m(1, 2), m(2, 2), m(1, 3), m(2, 3)) / det;
+  Li[1][2] = d2(m(1, 3), m(2, 3), m(1, 1), m(2, 1)) / det;
+  Li[2][2] = d2(m(1, 1), m(2, 1), m(1, 2), m(2, 2)) / det;
+}
+}  // namespace
+
+extern "C" {
+
+void orc_push_particles(int64_t n, double dt, const double* q, const double* m, const double* ex,
+                        const double* ey, const double* ez, double* vx, double* vy, double* vz,
+                        double* x, double* y, double* z) {
+  const double fact = dt;
+  for (int64_t i = 0; i < n; ++i) {
+    const double f = fact * q[i] / m[i];
+    vx[i] = vx[i] + f * ex[i];
+    vy[i] = vy[i] + f * ey[i];
+    vz[i] = vz[i] + f * ez[i];
+    x[i] = x[i] + dt * vx[i];
+    y[i] = y[i] + dt * vy[i];
+    z[i] = z[i] + dt * vz[i];
+  }
+}
+
+void orc_apply_external_field(int64_t n, double ez_ext, const double* z, double* ez, double* pot) {
+  for (int64_t i = 0; i < n; ++i) {
+    ez[i] = ez[i] + ez_ext;
+    pot[i] = pot[i] - z[i] * ez_ext;
+  }
+}
+
+void orc_constrain_periodic(const orc_params* p, int64_t n, double* x, double* y, double* z) {
+  const double* o = p->lattice_origin;
+  const bool simple = p->t_lattice_1[0] > 0.0 && p->t_lattice_1[1] == 0.0 &&
+                      p->t_lattice_1[2] == 0.0 && p->t_lattice_2[0] == 0.0 &&
+                      p->t_lattice_2[1] > 0.0 && p->t_lattice_2[2] == 0.0 &&
+                      p->t_lattice_3[0] == 0.0 && p->t_lattice_3[1] == 0.0 &&
+                      p->t_lattice_3[2] > 0.0;
+  double L[3][3], Li[3][3];
+  lattice_inverse(p, L, Li);
+  double* c[3] = {x, y, z};
+  for (int64_t i = 0; i < n; ++i) {
+    if (simple) {
+      const double walls[3] = {p->t_lattice_1[0], p->t_lattice_2[1], p->t_lattice_3[2]};
+      for (int d = 0; d < 3; ++d)
+        if (p->periodicity[d]) c[d][i] = fortran_modulo(c[d][i] - o[d], walls[d]) + o[d];
+    } else {
+      const double v[3] = {x[i] - o[0], y[i] - o[1], z[i] - o[2]};
+      double lc[3];
+      bool out = false;
+      for (int j = 0; j < 3; ++j) {
+        lc[j] = (v[0] * Li[0][j] + v[1] * Li[1][j]) + v[2] * Li[2][j];
+        if (lc[j] > 1.0 || lc[j] < 0.0) out = true;
+      }
+      if (out) {
+        for (int j = 0; j < 3; ++j) lc[j] = fortran_modulo(lc[j], 1.0);
+        for (int j = 0; j < 3; ++j) {
+          const double r = ((lc[0] * L[0][j] + lc[1] * L[1][j]) + lc[2] * L[2][j]) + o[j];
+          if (p->periodicity[j]) c[j][i] = r;
+        }
+      }
+    }
+  }
+}
+
+}  // extern "C"
+

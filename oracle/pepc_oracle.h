@@ -108,6 +108,16 @@ int orc_set_lattice_coefficients(orc_ctx* c, const double* re_im);
 int orc_lattice(orc_ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                 double* ex, double* ey, double* ez, double* pot);
 
+/* ---- the frontend's time step around the path (pepc-mini, module_helper.f90) ---- */
+/* push_particles (:205-222): v += dt q/m E, then x += dt v */
+void orc_push_particles(int64_t n, double dt, const double* q, const double* m, const double* ex,
+                        const double* ey, const double* ez, double* vx, double* vy, double* vz,
+                        double* x, double* y, double* z);
+/* apply_external_field (:321-334): E_z += ez_ext, pot -= z ez_ext */
+void orc_apply_external_field(int64_t n, double ez_ext, const double* z, double* ez, double* pot);
+/* constrain_periodic (module_mirror_boxes.f90:177-218) with the parameters' lattice */
+void orc_constrain_periodic(const orc_params* p, int64_t n, double* x, double* y, double* z);
+
 #ifdef __cplusplus
 }
 #endif

@@ -113,6 +113,8 @@ EXPORTS = [
     "pepcg_shift_multipoles_up", "pepcg_force_with_leaf", "pepcg_force_with_twig", "pepcg_mac",
     "pepcg_set_stream", "pepcg_kernel_launches", "pepcg_sort_keys_noalloc",
     "pepcg_traverse_adjoint", "pepcg_traverse_adjoint_device",
+    "pepcg_push_particles_device", "pepcg_apply_external_field_device",
+    "pepcg_constrain_periodic_device", "pepcg_gather_device",
 ]
 
 _LIB = None
@@ -145,6 +147,10 @@ def lib():
     L.pepcg_sort_keys_noalloc.argtypes = [C.c_int64, VP, VP, VP, VP]
     L.pepcg_traverse_adjoint.argtypes = [VP, C.c_int64, D, D, D, D, D, D, D, D, D, D, D]
     L.pepcg_traverse_adjoint_device.argtypes = [VP, C.c_int64] + [VP] * 11
+    L.pepcg_push_particles_device.argtypes = [VP, C.c_int64, C.c_double] + [VP] * 11
+    L.pepcg_apply_external_field_device.argtypes = [VP, C.c_int64, C.c_double, VP, VP, VP]
+    L.pepcg_constrain_periodic_device.argtypes = [VP, C.c_int64, VP, VP, VP]
+    L.pepcg_gather_device.argtypes = [VP, VP, VP]
     L.pepcg_kernel_launches.argtypes = []
     L.pepcg_kernel_launches.restype = C.c_longlong
     L.pepcg_stats_get.argtypes = [VP, C.POINTER(Stats)]
@@ -288,6 +294,25 @@ class TreeCode:
     def particles_device(self, key, perm, x, y, z, q):
         return self._check(lib().pepcg_get_particles_device(
             self._h, _tptr(key), _tptr(perm), _tptr(x), _tptr(y), _tptr(z), _tptr(q)))
+
+    # -- the frontend's time step on device arrays (module_helper.f90:205-222, :321-334;
+    #    module_mirror_boxes.f90:177-218)
+    def push_particles_device(self, dt, q, m, e, v, x):
+        """v += dt q/m E, then x += dt v; e, v, x are (x, y, z) triples of tensors."""
+        ptrs = [_tptr(t) for t in (q, m, *e, *v, *x)]
+        return self._check(lib().pepcg_push_particles_device(self._h, q.numel(), float(dt), *ptrs))
+
+    def apply_external_field_device(self, ez_ext, z, ez, pot):
+        return self._check(lib().pepcg_apply_external_field_device(
+            self._h, z.numel(), float(ez_ext), _tptr(z), _tptr(ez), _tptr(pot)))
+
+    def constrain_periodic_device(self, x, y, z):
+        return self._check(lib().pepcg_constrain_periodic_device(self._h, x.numel(), _tptr(x),
+                                                                 _tptr(y), _tptr(z)))
+
+    def gather_device(self, src, dst):
+        """dst[i] = src[perm[i]] with the last grow's permutation (key order)."""
+        return self._check(lib().pepcg_gather_device(self._h, _tptr(src), _tptr(dst)))
 
     def set_stream(self, stream_ptr):
         """Launch on an external cudaStream_t (int handle, e.g. torch's

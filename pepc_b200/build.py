@@ -22,7 +22,7 @@ LIB = os.path.join(HERE, "libpepcg.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-Xptxas", "-v"] + ARCH
-EXACT_FP64 = {"grow.cu", "walk_plain.cu", "direct.cu", "scalar.cu", "lattice.cu"}
+EXACT_FP64 = {"grow.cu", "walk_plain.cu", "direct.cu", "scalar.cu", "lattice.cu", "timeloop.cu"}
 
 
 def nvcc():

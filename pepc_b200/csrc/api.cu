@@ -413,12 +413,11 @@ int pepcg_grow_tree(void* ctx, int64_t n, const double* x, const double* y, cons
   if (key_out)
     ok = ok && cuda_ok(c, cudaMemcpyAsync(key_out, c->key.p, n * 8, cudaMemcpyDeviceToHost, s), "D2H key");
   if (perm_out) {
-    std::vector<int32_t> p32(n);
-    ok = ok && cuda_ok(c, cudaMemcpyAsync(p32.data(), c->perm.p, n * 4, cudaMemcpyDeviceToHost, s),
-                       "D2H perm") &&
-         cuda_ok(c, cudaStreamSynchronize(s), "D2H perm");
-    if (ok)
-      for (int64_t i = 0; i < n; ++i) perm_out[i] = p32[i];
+    // widened to 64 bits on the device (scratch: the target-key buffer)
+    if (!ensure(c, c->tkeys, n, "perm")) return PEPCG_ERR_OOM;
+    ok = ok && widen_perm_device(c, c->tkeys.p) == PEPCG_OK &&
+         cuda_ok(c, cudaMemcpyAsync(perm_out, c->tkeys.p, n * 8, cudaMemcpyDeviceToHost, s),
+                 "D2H perm");
   }
   if (x_out) ok = ok && cuda_ok(c, cudaMemcpyAsync(x_out, c->x.p, n * 8, cudaMemcpyDeviceToHost, s), "D2H x");
   if (y_out) ok = ok && cuda_ok(c, cudaMemcpyAsync(y_out, c->y.p, n * 8, cudaMemcpyDeviceToHost, s), "D2H y");
@@ -445,14 +444,7 @@ int pepcg_get_particles_device(void* ctx, int64_t* d_key, int64_t* d_perm, doubl
   if (d_y) ok = ok && cuda_ok(c, cudaMemcpyAsync(d_y, c->y.p, n * 8, cudaMemcpyDeviceToDevice, s), "y");
   if (d_z) ok = ok && cuda_ok(c, cudaMemcpyAsync(d_z, c->z.p, n * 8, cudaMemcpyDeviceToDevice, s), "z");
   if (d_q) ok = ok && cuda_ok(c, cudaMemcpyAsync(d_q, c->q.p, n * 8, cudaMemcpyDeviceToDevice, s), "q");
-  if (d_perm) {
-    std::vector<int32_t> p32(n);
-    std::vector<int64_t> p64(n);
-    ok = ok && cuda_ok(c, cudaMemcpyAsync(p32.data(), c->perm.p, n * 4, cudaMemcpyDeviceToHost, s), "perm") &&
-         cuda_ok(c, cudaStreamSynchronize(s), "perm");
-    for (int64_t i = 0; ok && i < n; ++i) p64[i] = p32[i];
-    ok = ok && cuda_ok(c, cudaMemcpyAsync(d_perm, p64.data(), n * 8, cudaMemcpyHostToDevice, s), "perm");
-  }
+  if (d_perm && ok) ok = widen_perm_device(c, d_perm) == PEPCG_OK;
   ok = ok && cuda_ok(c, cudaStreamSynchronize(s), "get particles");
   return ok ? PEPCG_OK : PEPCG_ERR_CUDA;
 }
@@ -682,6 +674,51 @@ int pepcg_lattice(void* ctx, int64_t nt, const double* tx, const double* ty, con
     ok = ok && cuda_ok(c, cudaMemcpyAsync(hout[k], b + (3 + k) * nt, nt * 8, cudaMemcpyDeviceToHost, s), "D2H");
   ok = ok && cuda_ok(c, cudaStreamSynchronize(s), "lattice");
   return ok ? PEPCG_OK : PEPCG_ERR_CUDA;
+}
+
+
+int pepcg_push_particles_device(void* ctx, int64_t n, double dt, const double* d_q,
+                                const double* d_m, const double* d_ex, const double* d_ey,
+                                const double* d_ez, double* d_vx, double* d_vy, double* d_vz,
+                                double* d_x, double* d_y, double* d_z) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || n < 0 || (n > 0 && (!d_q || !d_m || !d_ex || !d_ey || !d_ez || !d_vx || !d_vy ||
+                                !d_vz || !d_x || !d_y || !d_z)))
+    return PEPCG_ERR_BAD_ARG;
+  if (n == 0) return PEPCG_OK;
+  cudaSetDevice(c->device);
+  return push_device(c, n, dt, d_q, d_m, d_ex, d_ey, d_ez, d_vx, d_vy, d_vz, d_x, d_y, d_z);
+}
+
+int pepcg_apply_external_field_device(void* ctx, int64_t n, double ez_ext, const double* d_z,
+                                      double* d_ez, double* d_pot) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || n < 0 || (n > 0 && (!d_z || !d_ez || !d_pot))) return PEPCG_ERR_BAD_ARG;
+  if (n == 0) return PEPCG_OK;
+  cudaSetDevice(c->device);
+  return external_field_device(c, n, ez_ext, d_z, d_ez, d_pot);
+}
+
+int pepcg_constrain_periodic_device(void* ctx, int64_t n, double* d_x, double* d_y, double* d_z) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || n < 0 || (n > 0 && (!d_x || !d_y || !d_z))) return PEPCG_ERR_BAD_ARG;
+  if (n == 0) return PEPCG_OK;
+  cudaSetDevice(c->device);
+  return wrap_device(c, n, d_x, d_y, d_z);
+}
+
+int pepcg_gather_device(void* ctx, const double* d_in, double* d_out) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || !d_in || !d_out || d_in == d_out) {
+    if (c) c->err = "pepcg_gather_device: distinct input and output arrays are required";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  if (!c->has_tree) {
+    c->err = "pepcg_gather_device: no grown tree (the permutation comes from the last grow)";
+    return PEPCG_ERR_NO_TREE;
+  }
+  cudaSetDevice(c->device);
+  return gather_device(c, d_in, d_out);
 }
 
 }  // extern "C"

@@ -166,6 +166,15 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
 // ---- lattice.cu ----
 int lattice_prepare(Ctx* c);
 int lattice_timestep(Ctx* c);
+// timeloop.cu
+int push_device(Ctx* c, int64_t n, double dt, const double* q, const double* m, const double* ex,
+                const double* ey, const double* ez, double* vx, double* vy, double* vz, double* x,
+                double* y, double* z);
+int external_field_device(Ctx* c, int64_t n, double ez_ext, const double* z, double* ez,
+                          double* pot);
+int wrap_device(Ctx* c, int64_t n, double* x, double* y, double* z);
+int gather_device(Ctx* c, const double* in, double* out);
+int widen_perm_device(Ctx* c, int64_t* out);
 int lattice_add(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                 double* ex, double* ey, double* ez, double* pot, bool overwrite);
 

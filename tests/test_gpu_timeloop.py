@@ -1,0 +1,127 @@
+"""GPU: the device time-step pieces (push, external field, periodic wrap,
+key-order gather) bit for bit against the oracle's restatement of the
+pepc-mini frontend, and a device-resident multi-step loop against the same
+loop on the oracle."""
+import numpy as np
+import pytest
+import torch
+
+import pepc_b200 as P
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda", 0)
+
+
+def T(a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(DEV)
+
+
+def H(t):
+    return t.cpu().numpy()
+
+
+def test_push_and_field_bitwise(gpu):
+    rng = np.random.default_rng(71)
+    n = 5000
+    q, m = rng.standard_normal(n), rng.random(n) + 0.5
+    e = [rng.standard_normal(n) for _ in range(3)]
+    v = [rng.standard_normal(n) for _ in range(3)]
+    x = [rng.random(n) for _ in range(3)]
+    dv, dx = [T(a) for a in v], [T(a) for a in x]
+    tc = P.TreeCode()
+    tc.push_particles_device(1e-3, T(q), T(m), [T(a) for a in e], dv, dx)
+    O.push_particles(1e-3, q, m, e, v, x)
+    for a, b in zip(dv + dx, v + x):
+        assert np.array_equal(H(a), b)
+    ez, pot = rng.standard_normal(n), rng.standard_normal(n)
+    dez, dpot = T(ez), T(pot)
+    tc.apply_external_field_device(0.3, dx[2], dez, dpot)
+    O.apply_external_field(0.3, x[2], ez, pot)
+    assert np.array_equal(H(dez), ez) and np.array_equal(H(dpot), pot)
+    tc.close()
+
+
+@pytest.mark.parametrize("lattice", ["principal", "skewed"])
+def test_wrap_bitwise(gpu, lattice):
+    rng = np.random.default_rng(72)
+    n = 5000
+    c = [rng.uniform(-2.0, 3.0, n) for _ in range(3)]
+    if lattice == "principal":
+        kw = dict(periodicity=(1, 0, 1), t_lattice_1=(2.0, 0.0, 0.0), t_lattice_2=(0.0, 1.0, 0.0),
+                  t_lattice_3=(0.0, 0.0, 0.5), lattice_origin=(0.1, -0.2, 0.0))
+    else:
+        kw = dict(periodicity=(1, 1, 1), t_lattice_1=(1.0, 0.0, 0.0), t_lattice_2=(0.5, 1.0, 0.0),
+                  t_lattice_3=(0.0, 0.3, 1.0), include_far_field_if_periodic=0)
+    dc = [T(a) for a in c]
+    tc = P.TreeCode(**kw)
+    tc.constrain_periodic_device(*dc)
+    O.constrain_periodic(*c, **kw)
+    for a, b in zip(dc, c):
+        assert np.array_equal(H(a), b)
+    tc.close()
+
+
+def test_gather_follows_the_grow(gpu):
+    rng = np.random.default_rng(73)
+    n = 3000
+    x, y, z, q = rng.random(n), rng.random(n), rng.random(n), rng.standard_normal(n)
+    tc = P.TreeCode()
+    g = tc.pepc_grow_tree(x, y, z, q)
+    v = rng.standard_normal(n)
+    out = torch.empty(n, dtype=torch.float64, device=DEV)
+    tc.gather_device(T(v), out)
+    assert np.array_equal(H(out), v[g.perm])
+    with pytest.raises(P.PepcgError):
+        src = T(v)
+        tc.gather_device(src, src)
+    tc.close()
+
+
+def test_device_resident_steps_match_the_oracle_loop(gpu):
+    # periodic (mirror boxes, no far field: bit-exact walks), three kick-drift
+    # steps with the wrap; the particle state follows each grow's key order
+    rng = np.random.default_rng(74)
+    n = 2000
+    kw = dict(theta2=0.25, eps2=1e-4, periodicity=(1, 1, 1), include_far_field_if_periodic=0)
+    x, y, z = rng.random(n), rng.random(n), rng.random(n)
+    q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
+    m = np.full(n, 1.0)
+    dt = 2e-4
+    # oracle loop on numpy
+    ox, oy, oz, oq, om = x.copy(), y.copy(), z.copy(), q.copy(), m.copy()
+    ov = [np.zeros(n) for _ in range(3)]
+    orc = O.Oracle(walk=0, **kw)
+    for _ in range(3):
+        g = orc.grow_tree(ox, oy, oz, oq)
+        p = g["perm"]
+        ox, oy, oz, oq, om = g["x"].copy(), g["y"].copy(), g["z"].copy(), oq[p], om[p]
+        ov = [a[p] for a in ov]
+        r = orc.traverse_tree(ox, oy, oz, keys=g["key"])
+        pos = [ox, oy, oz]
+        O.push_particles(dt, oq, om, [r["ex"], r["ey"], r["ez"]], ov, pos)
+        O.constrain_periodic(*pos, **kw)
+    # device loop
+    tc = P.TreeCode(walk=P.WALK_PER_TARGET, **kw)
+    tc.set_stream(torch.cuda.current_stream().cuda_stream)
+    dx, dy, dz, dq, dm = T(x), T(y), T(z), T(q), T(m)
+    dv = [torch.zeros(n, dtype=torch.float64, device=DEV) for _ in range(3)]
+    key = torch.empty(n, dtype=torch.int64, device=DEV)
+    for _ in range(3):
+        tc.grow_tree_device(dx, dy, dz, dq)
+        nx, ny, nz, nq = (torch.empty(n, dtype=torch.float64, device=DEV) for _ in range(4))
+        tc.particles_device(key, torch.empty(n, dtype=torch.int64, device=DEV), nx, ny, nz, nq)
+        nm = torch.empty_like(dm)
+        tc.gather_device(dm, nm)
+        nv = [torch.empty_like(a) for a in dv]
+        for a, b in zip(dv, nv):
+            tc.gather_device(a, b)
+        dx, dy, dz, dq, dm, dv = nx, ny, nz, nq, nm, nv
+        out = [torch.zeros(n, dtype=torch.float64, device=DEV) for _ in range(5)]
+        tc.traverse_self_device(*out)
+        tc.push_particles_device(dt, dq, dm, out[:3], dv, [dx, dy, dz])
+        tc.constrain_periodic_device(dx, dy, dz)
+    torch.cuda.synchronize()
+    for a, b in zip([dx, dy, dz] + dv, [ox, oy, oz] + ov):
+        assert np.array_equal(H(a), b)
+    tc.close()
