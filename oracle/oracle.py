@@ -34,6 +34,7 @@ class OrcParams(C.Structure):
         ("t_lattice_3", C.c_double * 3),
         ("lattice_origin", C.c_double * 3),
         ("num_threads", C.c_int32),
+        ("mac_select", C.c_int32),
     ]
 
 

@@ -403,6 +403,21 @@ struct orc_ctx {
   }
 };
 
+// mac (coulomb/module_interaction_specific.f90:256-275): Barnes-Hut, Bmax
+// (min(bmax^2, 3 boxlength2)), or no acceptance at all (the N^2 code)
+static bool mac_pass(const orc_ctx* c, const Node& nd, double dist2) {
+  const double bl2 = c->boxlength2[nd.level];
+  switch (c->p.mac_select) {
+    case 0:
+      return c->p.theta2 * dist2 > bl2;
+    case 1:
+      return c->p.theta2 * dist2 > std::min(nd.m[M_BMAX] * nd.m[M_BMAX], 3.0 * bl2);
+    default:
+      return false;
+  }
+}
+
+
 namespace {
 
 // tree_node_create_from_particle, module_tree_grow.f90:702-734
@@ -488,7 +503,7 @@ int64_t walk_pthreads(const orc_ctx* c, const double xt[3], const double vbox[3]
   for (int64_t ch = c->nodes[c->root].first_child; ch != kNodeInvalid;
        ch = c->nodes[ch].next_sibling)
     todo.push_back(ch);
-  const double eps2 = c->p.eps2, theta2 = c->p.theta2;
+  const double eps2 = c->p.eps2;
   while (!todo.empty()) {
     int64_t ni = todo.back();
     todo.pop_back();
@@ -508,7 +523,7 @@ int64_t walk_pthreads(const orc_ctx* c, const double xt[3], const double vbox[3]
       cnt.inter += 1;
     } else {
       cnt.mac += 1;
-      if (theta2 * dist2 > c->boxlength2[nd.level]) {  // mac, :635 / specific.f90:267
+      if (mac_pass(c, nd, dist2)) {  // mac, :635 / specific.f90:256-275
         partner += nd.leaves;
         double ee[3], ph;
         force_twig(nd.m, d, dist2 + eps2, ee, ph);  // specific.f90:373
@@ -530,7 +545,7 @@ void walk_simple_aux(const orc_ctx* c, int64_t ni, int np, const double (*xs)[3]
                      const double vbox[3], double (*e)[3], double* pot, double* work,
                      int64_t& partner, Counters& cnt) {
   const Node& nd = c->nodes[ni];
-  const double eps2 = c->p.eps2, theta2 = c->p.theta2;
+  const double eps2 = c->p.eps2;
   double d[32][3], d2[32];
   if (nd.descendants == 0) {
     partner += 1;
@@ -552,7 +567,7 @@ void walk_simple_aux(const orc_ctx* c, int64_t ni, int np, const double (*xs)[3]
     cnt.mac += 1;
     for (int k = 0; k < 3; ++k) d[ip][k] = (xs[ip][k] - vbox[k]) - nd.m[M_COCX + k];
     d2[ip] = (d[ip][0] * d[ip][0] + d[ip][1] * d[ip][1]) + d[ip][2] * d[ip][2];
-    if (!(theta2 * d2[ip] > c->boxlength2[nd.level])) {  // MAC fails for this target: resolve
+    if (!mac_pass(c, nd, d2[ip])) {  // MAC fails for this target: resolve
       for (int64_t ch = nd.first_child; ch != kNodeInvalid; ch = c->nodes[ch].next_sibling)
         walk_simple_aux(c, ch, np, xs, vbox, e, pot, work, partner, cnt);
       return;
@@ -1152,7 +1167,7 @@ int orc_traverse_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double*
         const double dist2 = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2];
         if (nd.descendants == 0) {
           if (dist2 > 0.0) leaf_adjoint(nd.m[M_Q], d, c->p.eps2, gphi[i], gE, adj[ni]);
-        } else if (c->p.theta2 * dist2 > c->boxlength2[nd.level]) {
+        } else if (mac_pass(c, nd, dist2)) {
           twig_adjoint(nd.m, d, c->p.eps2, gphi[i], gE, adj[ni]);
         } else {
           for (int64_t ch = nd.first_child; ch != kNodeInvalid; ch = c->nodes[ch].next_sibling)

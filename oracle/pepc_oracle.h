@@ -36,6 +36,7 @@ typedef struct orc_params {
   double t_lattice_1[3], t_lattice_2[3], t_lattice_3[3];
   double lattice_origin[3];
   int32_t num_threads;      /* host threads for the walk (1 = serial) */
+  int32_t mac_select;       /* 0 Barnes-Hut, 1 Bmax, other: no acceptance (N^2) */
 } orc_params;
 
 void orc_params_default(orc_params* p);

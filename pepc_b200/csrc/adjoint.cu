@@ -200,6 +200,7 @@ struct AdjArgs {
   const int2* fwd;
   const double* mom;
   const double* bl2;
+  const double* macb;  // per-twig MAC threshold, or nullptr: bl2 of the level (Barnes-Hut)
   const double* vbox;
   int nbox;
   double theta2, eps2;
@@ -259,7 +260,8 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_target(AdjArgs A) {
           const double4 pn = A.nc4[p];
           const double dx = sx - pn.x, dy = sy - pn.y, dz = sz - pn.z;
           const double dist2 = (dx * dx + dy * dy) + dz * dz;
-          if (A.theta2 * dist2 > s_bl2[A.meta[p].y & 0xff]) reach = false;  // accepted above S
+          const double thr = A.macb ? A.macb[p] : s_bl2[A.meta[p].y & 0xff];
+          if (A.theta2 * dist2 > thr) reach = false;  // accepted above S
         }
         next = reach ? (unsigned)S : end;
       }
@@ -287,7 +289,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_target(AdjArgs A) {
               contrib = true;
             }
             next = u + 1;
-          } else if (A.theta2 * dist2 > s_bl2[mu.y & 0xff]) {
+          } else if (A.theta2 * dist2 > (A.macb ? A.macb[u] : s_bl2[mu.y & 0xff])) {
             double m[9];
 #pragma unroll
             for (int k = 0; k < 9; ++k) m[k] = A.mom[9 * (int64_t)u + k];
@@ -364,7 +366,8 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_group(AdjArgs A) {
           flush_node(A.adj, u, a, lane, true);
           u = (unsigned)fw.y;
         } else {
-          const bool ok = !valid || (A.theta2 * dist2 > s_bl2[mu.y & 0xff]);
+          const bool ok =
+              !valid || (A.theta2 * dist2 > (A.macb ? A.macb[u] : s_bl2[mu.y & 0xff]));
           if (__all_sync(0xffffffffu, ok)) {
             if (valid) {
               double m[9];
@@ -531,6 +534,10 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
   A.fwd = c->fwd.p;
   A.mom = c->mom.p;
   A.bl2 = c->d_box + 9;
+  {
+    int rc = prepare_mac(c, &A.macb);
+    if (rc) return rc;
+  }
   A.vbox = c->d_vbox;
   A.nbox = c->nboxes;
   A.theta2 = c->prm.theta2;

@@ -137,9 +137,9 @@ static int check_params(Ctx* c, const pepcg_params* p) {
     c->err = "only force_law = 3 (3D Coulomb) is supported";
     return PEPCG_ERR_UNSUPPORTED;
   }
-  if (p->mac_select != 0) {
-    c->err = "only mac_select = 0 (Barnes-Hut) is supported";
-    return PEPCG_ERR_UNSUPPORTED;
+  if (p->mac_select < 0) {
+    c->err = "mac_select must be 0 (Barnes-Hut), 1 (Bmax) or another positive value (no acceptance, N^2)";
+    return PEPCG_ERR_BAD_ARG;
   }
   if (p->curve != PEPCG_CURVE_HILBERT && p->curve != PEPCG_CURVE_MORTON) {
     c->err = "curve must be PEPCG_CURVE_HILBERT or PEPCG_CURVE_MORTON";
@@ -338,7 +338,7 @@ int pepcg_destroy(void* ctx) {
   release(c->scan_tmp);
   release(c->nc4); release(c->meta); release(c->fwd); release(c->mom); release(c->aux);
   release(c->mom32);
-  release(c->parent); release(c->nchild); release(c->twiglist); release(c->lvlcnt); release(c->first_part);
+  release(c->parent); release(c->nchild); release(c->twiglist); release(c->lvlcnt); release(c->macb); release(c->first_part);
   release(c->nleaves); release(c->child8); release(c->wstack); release(c->leafnode);
   release(c->adj); release(c->fpo2rpo); release(c->rpo2fpo); release(c->nkey);
   release(c->tiles); release(c->counters); release(c->tgt); release(c->tkeys);

@@ -92,6 +92,7 @@ struct Ctx {
   DBuf<int32_t> parent, nchild, first_part, nleaves;
   DBuf<int32_t> twiglist;  // twig RPO indices grouped by level (upward and adjoint passes)
   DBuf<int32_t> lvlcnt;    // [0, 32) twigs per level, [32, 64) fill counters
+  DBuf<double> macb;       // per-twig MAC threshold for mac_select != 0
   int32_t lvl_host[kMaxLevel + 1] = {0};  // twigs per level of the grown tree
   DBuf<int4> child8;  // up to 8 children (RPO indices) per twig, as 2 x int4
   DBuf<int32_t> wstack;  // per-warp traversal stacks of the wide group walk
@@ -166,6 +167,8 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
 // ---- lattice.cu ----
 int lattice_prepare(Ctx* c);
 int lattice_timestep(Ctx* c);
+// walk_plain.cu: per-twig MAC thresholds for mac_select != 0 (nullptr for Barnes-Hut)
+int prepare_mac(Ctx* c, const double** macb);
 // timeloop.cu
 int push_device(Ctx* c, int64_t n, double dt, const double* q, const double* m, const double* ex,
                 const double* ey, const double* ez, double* vx, double* vy, double* vz, double* x,

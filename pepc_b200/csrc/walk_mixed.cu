@@ -45,6 +45,7 @@ struct MixArgs {
   const float4* mom32;  // 3 float4 per node
   const int32_t* nleaves;
   const double* bl2;
+  const double* macb;  // per-twig MAC threshold, or nullptr: bl2 of the level (Barnes-Hut)
   const double* vbox;
   int nbox;
   float theta2;
@@ -319,7 +320,7 @@ __global__ void __launch_bounds__(kMixThreads, 5)
           if (mu.y & kLeafFlag) {
             isleaf = true;
           } else {
-            bl = s_bl2[mu.y & 0xff];
+            bl = A.macb ? (float)A.macb[node] : s_bl2[mu.y & 0xff];
             const float dc = sqrtf(cx * cx + cy * cy + cz * cz);
             const float dmin = dc - rg, dmax = dc + rg;
             if (dmin > 0.f && theta2 * (dmin * dmin) > bl) {
@@ -459,7 +460,7 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_target_mixed(MixArgs A) {
           } else {
             ++c_mac;
             const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            if (A.theta2 * r2 > s_bl2[mu.y & 0xff]) {
+            if (A.theta2 * r2 > (A.macb ? (float)A.macb[u] : s_bl2[mu.y & 0xff])) {
               partner += A.nleaves[u];
               const float4 m0 = A.mom32[3 * (int64_t)u], m1 = A.mom32[3 * (int64_t)u + 1],
                            m2 = A.mom32[3 * (int64_t)u + 2];
@@ -504,6 +505,10 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
   A.mom32 = reinterpret_cast<const float4*>(c->mom32.p);
   A.nleaves = c->nleaves.p;
   A.bl2 = c->d_box + 9;
+  {
+    int rc = prepare_mac(c, &A.macb);
+    if (rc) return rc;
+  }
   A.vbox = c->d_vbox;
   A.nbox = c->nboxes;
   A.theta2 = (float)c->prm.theta2;

@@ -34,6 +34,7 @@ struct WalkArgs {
   const double* mom;
   const int32_t* nleaves;
   const double* bl2;   // boxlength2[0..20]
+  const double* macb;  // per-twig MAC threshold, or nullptr: bl2 of the level (Barnes-Hut)
   const double* vbox;  // 3 * nbox
   int nbox;
   double theta2, eps2;
@@ -113,7 +114,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_target64(WalkArgs A) {
           next = u + 1;
         } else {
           ++c_mac;
-          if (A.theta2 * dist2 > s_bl2[mu.y & 0xff]) {
+          if (A.theta2 * dist2 > (A.macb ? A.macb[u] : s_bl2[mu.y & 0xff])) {
             partner += A.nleaves[u];
             double m[9];
 #pragma unroll
@@ -188,7 +189,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_tile64(WalkArgs A) {
           }
           u = (unsigned)fw.y;
         } else {
-          const bool ok = !valid || (A.theta2 * dist2 > s_bl2[mu.y & 0xff]);
+          const bool ok =
+              !valid || (A.theta2 * dist2 > (A.macb ? A.macb[u] : s_bl2[mu.y & 0xff]));
           const unsigned fail = __ballot_sync(0xffffffffu, !ok);
           // MAC evaluations stop at the first failing target (:343-370)
           const int first_fail = fail ? __ffs(fail) - 1 : 32;
@@ -248,11 +250,45 @@ __global__ void k_same_keys(int64_t n, const int64_t* __restrict__ a, const int6
 
 __global__ void k_reset_counter() { g_bucket_counter = 0; }
 
+// mac (coulomb/module_interaction_specific.f90:256-275) for mac_select != 0,
+// as a per-twig threshold t with "accept iff theta2 dist2 > t": the Bmax MAC
+// has t = min(bmax^2, 3 boxlength2(level)); any other selection accepts
+// nothing (the N^2 code), t = +inf.
+__global__ void k_mac_thresholds(int64_t M, int mode, const int2* __restrict__ meta,
+                                 const double2* __restrict__ aux, const double* __restrict__ bl2,
+                                 double* __restrict__ macb) {
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < M;
+       u += (int64_t)gridDim.x * blockDim.x) {
+    const int2 mu = meta[u];
+    if (mu.y & kLeafFlag) continue;
+    if (mode == 1) {
+      const double bmax = aux[u].y;
+      macb[u] = fmin(bmax * bmax, 3.0 * bl2[mu.y & 0xff]);
+    } else {
+      macb[u] = INFINITY;
+    }
+  }
+}
+
 }  // namespace
 
 int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                       double* ex, double* ey, double* ez, double* pot, double* work,
                       const int2* tiles, int64_t ntiles, bool per_target);
+
+int prepare_mac(Ctx* c, const double** macb) {
+  *macb = nullptr;
+  if (c->prm.mac_select == 0) return PEPCG_OK;
+  const int64_t M = c->nnodes;
+  if (!ensure(c, c->macb, M, "mac thresholds")) return PEPCG_ERR_OOM;
+  COUNT_LAUNCH();
+  const unsigned g = (unsigned)((M + 255) / 256 > 148 * 16 ? 148 * 16 : (M + 255) / 256);
+  k_mac_thresholds<<<g, 256, 0, c->stream>>>(M, c->prm.mac_select, c->meta.p, c->aux.p,
+                                             c->d_box + 9, c->macb.p);
+  if (!cuda_ok(c, cudaGetLastError(), "mac thresholds")) return PEPCG_ERR_CUDA;
+  *macb = c->macb.p;
+  return PEPCG_OK;
+}
 
 int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                     const int64_t* tkeys, bool self, double* ex, double* ey, double* ez,
@@ -310,6 +346,10 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
   A.mom = c->mom.p;
   A.nleaves = c->nleaves_ptr();
   A.bl2 = c->d_box + 9;
+  {
+    int rc = prepare_mac(c, &A.macb);
+    if (rc) return rc;
+  }
   A.vbox = c->d_vbox;
   A.nbox = c->nboxes;
   A.theta2 = c->prm.theta2;

@@ -40,15 +40,16 @@ def problem(n, nt, seed):
     return x, y, z, q, tx, ty, tz, gphi, gE, rng
 
 
-@pytest.mark.parametrize("walk", [P.WALK_PER_TARGET, P.WALK_GROUP])
-def test_adjoint_matches_oracle_and_fd(gpu, walk):
+@pytest.mark.parametrize("walk,mac", [(P.WALK_PER_TARGET, 0), (P.WALK_GROUP, 0),
+                                      (P.WALK_PER_TARGET, 1)])
+def test_adjoint_matches_oracle_and_fd(gpu, walk, mac):
     x, y, z, q, tx, ty, tz, gphi, gE, rng = problem(3000, 70, 71)
-    kw = dict(theta2=0.16, eps2=1e-3, walk=walk)
+    kw = dict(theta2=0.16, eps2=1e-3, walk=walk, mac_select=mac)
     tc = P.TreeCode(precision=P.PRECISION_PLAIN, **kw)
     tc.pepc_grow_tree(x, y, z, q)
     g = tc.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
     if walk == P.WALK_PER_TARGET:
-        orc = O.Oracle(theta2=0.16, eps2=1e-3, walk=0)
+        orc = O.Oracle(theta2=0.16, eps2=1e-3, walk=0, mac_select=mac)
         orc.grow_tree(x, y, z, q)
         go = orc.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
         for k in ("q", "x", "y", "z"):

@@ -105,3 +105,18 @@ def test_mixed_group_ragged_buckets_and_duplicates(gpu):
     assert np.median(diff) < 2e-5, np.median(diff)
     assert np.all(np.isfinite(rm["pot"]))
     assert np.mean(rm["work"] == rp["work"]) > 0.99
+
+
+def test_mixed_group_bmax_mac_matches_plain(gpu):
+    x, y, z, q = plummer(30000, 46)
+    kw = dict(theta2=0.36, eps2=1e-6, walk=P.WALK_GROUP, mac_select=1)
+    tp, _, rp = run(x, y, z, q, precision=P.PRECISION_PLAIN, **kw)
+    tm, _, rm = run(x, y, z, q, precision=P.PRECISION_MIXED, **kw)
+    idx = np.arange(0, 30000, 7)
+    diff = relerr(rm, {"ex": rp["ex"][idx], "ey": rp["ey"][idx], "ez": rp["ez"][idx]}, idx)
+    assert np.median(diff) < 2e-6, np.median(diff)
+    assert np.mean(rm["work"] == rp["work"]) > 0.99
+    # the Bmax MAC is the stricter one here: more interactions than Barnes-Hut
+    _, _, rb = run(x, y, z, q, precision=P.PRECISION_MIXED, theta2=0.36, eps2=1e-6,
+                   walk=P.WALK_GROUP)
+    assert rm["work"].sum() != rb["work"].sum()

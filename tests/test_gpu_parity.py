@@ -17,7 +17,8 @@ pytestmark = pytest.mark.gpu
 def grow_both(x, y, z, q, **kw):
     tc = P.TreeCode(**kw)
     okw = {k: v for k, v in kw.items() if k in ("theta2", "eps2", "curve", "tile_size",
-                                                  "periodicity", "force_cubic_domain")}
+                                                  "periodicity", "force_cubic_domain",
+                                                  "mac_select")}
     if "walk" in kw:
         okw["walk"] = 0 if kw["walk"] == P.WALK_PER_TARGET else 1
     orc = O.Oracle(num_threads=8, **okw)
@@ -101,6 +102,24 @@ def test_walk_per_tile_bit_exact(gpu, tile):
         assert np.array_equal(r[k], ro[k]), k
     assert tc.stats()["interactions"] == orc.counters()["interactions"]
     assert tc.stats()["mac_evaluations"] == orc.counters()["mac_evaluations"]
+
+
+@pytest.mark.parametrize("walk", [P.WALK_PER_TARGET, P.WALK_PER_TILE])
+@pytest.mark.parametrize("mac", [1, 2])
+def test_walk_other_macs_bit_exact(gpu, walk, mac):
+    # mac_select 1: Bmax MAC, min(bmax^2, 3 boxlength2); 2: nothing accepted
+    # (every target sees every particle, the N^2 code)
+    n = 6000 if mac == 1 else 1500
+    x, y, z, q = plummer(n, 25)
+    tc, orc, g, go = grow_both(x, y, z, q, theta2=0.36, eps2=1e-6, walk=walk, mac_select=mac)
+    r = tc.pepc_traverse_tree(g.x, g.y, g.z, keys=g.key)
+    ro = orc.traverse_tree(go["x"], go["y"], go["z"], keys=go["key"])
+    for k in ("ex", "ey", "ez", "pot", "work"):
+        assert np.array_equal(r[k], ro[k]), k
+    assert tc.stats()["interactions"] == orc.counters()["interactions"]
+    if mac == 2:
+        assert np.all(r["work"] == n)  # every leaf, the self interaction included
+        assert tc.stats()["twig_interactions"] == 0
 
 
 def test_walk_accumulates_and_foreign_targets(gpu):
