@@ -69,7 +69,7 @@ extern "C" {
 typedef struct pepcg_params {
   double theta2;                 /* square of the BH opening angle [0.36] */
   double eps2;                   /* Plummer softening squared [0.0] */
-  int32_t force_law;             /* 3 = 3D Coulomb (only value supported) [3] */
+  int32_t force_law;             /* 3 3D Coulomb, 2 2D Coulomb, 4 Lennard-Jones (plain form) [3] */
   int32_t mac_select;            /* 0 Barnes-Hut, 1 Bmax, other > 0: no acceptance (N^2) [0] */
   int32_t curve;                 /* PEPCG_CURVE_* [HILBERT] */
   int32_t precision;             /* PEPCG_PRECISION_* [PLAIN] */

@@ -35,6 +35,7 @@ class OrcParams(C.Structure):
         ("lattice_origin", C.c_double * 3),
         ("num_threads", C.c_int32),
         ("mac_select", C.c_int32),
+        ("force_law", C.c_int32),
     ]
 
 

@@ -330,6 +330,85 @@ inline void force_twig(const double* t, const double d[3], double dist2, double 
                     + ((dx * pre2z) * t[M_ZX])) + ((dy * pre2z) * t[M_YZ])) + (pre1 * t[M_XY]));
 }
 
+// calc_force_coulomb_2D_direct, coulomb/module_coulomb_kernels.f90:267-279
+// (d2 = dx^2 + dy^2 + eps2)
+inline void force_leaf_2d(const double* t, const double d[3], double d2, double e[3],
+                          double& phi) {
+  phi = -((0.5 * t[M_Q]) * std::log(d2));
+  const double rd2charge = t[M_Q] / d2;
+  e[0] = rd2charge * d[0];
+  e[1] = rd2charge * d[1];
+  e[2] = 0.0;
+}
+
+// calc_force_coulomb_2D, coulomb/module_coulomb_kernels.f90:155-195
+inline void force_twig_2d(const double* t, const double d[3], double d2, double e[3],
+                          double& phi) {
+  const double dx = d[0], dy = d[1];
+  const double rd2 = 1.0 / d2, rd4 = rd2 * rd2, rd6 = rd4 * rd2;
+  const double dx2 = dx * dx, dy2 = dy * dy, dx3 = dx2 * dx, dy3 = dy2 * dy;
+  const double q = t[M_Q], p1 = t[M_DX], p2 = t[M_DY];
+  const double q1 = t[M_QXX], q2 = t[M_QYY], qxy = t[M_XY];
+  phi = ((((-((0.5 * q) * std::log(d2))) - ((dx * p1) + (dy * p2)) * rd2) +
+          q1 * (((2.0 * dx2) * rd4) - rd2)) +
+         q2 * (((2.0 * dy2) * rd4) - rd2)) +
+        (((2.0 * qxy) * dx) * dy) * rd4;
+  e[0] = (((((q * dx) * rd2 - p1 * (((2.0 * dx2) * rd4) - rd2)) - (((p2 * 2.0) * dx) * dy) * rd4) +
+           q1 * (((8.0 * dx3) * rd6) - ((6.0 * dx) * rd4))) +
+          q2 * ((((8.0 * dx) * dy2) * rd6) - ((2.0 * dx) * rd4))) +
+         qxy * ((((8.0 * dx2) * dy) * rd6) - ((2.0 * dy) * rd4));
+  e[1] = (((((q * dy) * rd2 - p2 * (((2.0 * dy2) * rd4) - rd2)) - (((p1 * 2.0) * dx) * dy) * rd4) +
+           q2 * (((8.0 * dy3) * rd6) - ((6.0 * dy) * rd4))) +
+          q1 * ((((8.0 * dy) * dx2) * rd6) - ((2.0 * dy) * rd4))) +
+         qxy * ((((8.0 * dy2) * dx) * rd6) - ((2.0 * dx) * rd4));
+  e[2] = 0.0;
+}
+
+// calc_force_LJ, coulomb/module_coulomb_kernels.f90:204-235 (r2 unsoftened,
+// aii2 = eps2; the same for leaves and twigs)
+inline void force_lj(const double d[3], double r2, double aii2, double e[3], double& phi) {
+  const double epsc2 = 0.8 * aii2;
+  const double aii2_r2 = (r2 > epsc2) ? aii2 / r2 : aii2 / epsc2;
+  const double aii4_r4 = aii2_r2 * aii2_r2;
+  const double flj = 2.0 * (aii4_r4 * aii4_r4) - aii4_r4;
+  phi = 0.0;
+  const double r = std::sqrt(r2);
+  const double fljrd = flj / r;
+  e[0] = d[0] * fljrd;
+  e[1] = d[1] * fljrd;
+  e[2] = d[2] * fljrd;
+}
+
+// calc_force_per_interaction_with_leaf / _with_twig
+// (coulomb/module_interaction_specific.f90:314-387): the force law's kernel
+// for an unsoftened |delta|^2
+inline void law_leaf(int law, const double* t, const double d[3], double dist2, double eps2,
+                     double e[3], double& phi) {
+  switch (law) {
+    case 2:
+      force_leaf_2d(t, d, (d[0] * d[0] + d[1] * d[1]) + eps2, e, phi);
+      break;
+    case 4:
+      force_lj(d, dist2, eps2, e, phi);
+      break;
+    default:
+      force_leaf(t, d, dist2 + eps2, e, phi);
+  }
+}
+inline void law_twig(int law, const double* t, const double d[3], double dist2, double eps2,
+                     double e[3], double& phi) {
+  switch (law) {
+    case 2:
+      force_twig_2d(t, d, (d[0] * d[0] + d[1] * d[1]) + eps2, e, phi);
+      break;
+    case 4:
+      force_lj(d, dist2, eps2, e, phi);
+      break;
+    default:
+      force_twig(t, d, dist2 + eps2, e, phi);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Mirror boxes (treecode/lpepcsrc/module_mirror_boxes.f90:73-156)
 // ---------------------------------------------------------------------------
@@ -516,7 +595,7 @@ int64_t walk_pthreads(const orc_ctx* c, const double xt[3], const double vbox[3]
       work += 1.0;
       if (dist2 > 0.0) {
         double ee[3], ph;
-        force_leaf(nd.m, d, dist2 + eps2, ee, ph);  // coulomb/...specific.f90:333
+        law_leaf(c->p.force_law, nd.m, d, dist2, eps2, ee, ph);  // coulomb/...specific.f90:327-337
         e[0] += ee[0]; e[1] += ee[1]; e[2] += ee[2];
         pot += ph;
       }
@@ -526,7 +605,7 @@ int64_t walk_pthreads(const orc_ctx* c, const double xt[3], const double vbox[3]
       if (mac_pass(c, nd, dist2)) {  // mac, :635 / specific.f90:256-275
         partner += nd.leaves;
         double ee[3], ph;
-        force_twig(nd.m, d, dist2 + eps2, ee, ph);  // specific.f90:373
+        law_twig(c->p.force_law, nd.m, d, dist2, eps2, ee, ph);  // specific.f90:368-380
         e[0] += ee[0]; e[1] += ee[1]; e[2] += ee[2];
         pot += ph;
         cnt.inter += 1;
@@ -556,7 +635,7 @@ void walk_simple_aux(const orc_ctx* c, int64_t ni, int np, const double (*xs)[3]
       work[ip] += 1.0;
       if (d2[ip] > 0.0) {
         double ee[3], ph;
-        force_leaf(nd.m, d[ip], d2[ip] + eps2, ee, ph);
+        law_leaf(c->p.force_law, nd.m, d[ip], d2[ip], eps2, ee, ph);
         e[ip][0] += ee[0]; e[ip][1] += ee[1]; e[ip][2] += ee[2];
         pot[ip] += ph;
       }
@@ -578,7 +657,7 @@ void walk_simple_aux(const orc_ctx* c, int64_t ni, int np, const double (*xs)[3]
     cnt.inter += 1;
     work[ip] += 1.0;
     double ee[3], ph;
-    force_twig(nd.m, d[ip], d2[ip] + eps2, ee, ph);
+    law_twig(c->p.force_law, nd.m, d[ip], d2[ip], eps2, ee, ph);
     e[ip][0] += ee[0]; e[ip][1] += ee[1]; e[ip][2] += ee[2];
     pot[ip] += ph;
   }
@@ -797,6 +876,7 @@ void orc_params_default(orc_params* p) {
   p->t_lattice_2[1] = 1.0;
   p->t_lattice_3[2] = 1.0;
   p->num_threads = 1;
+  p->force_law = 3;   // coulomb/module_interaction_specific.f90:35
 }
 
 void orc_box_create(int64_t n, const double* x, const double* y, const double* z,
@@ -1102,7 +1182,7 @@ int orc_direct(orc_ctx* c, int64_t ntest, const int64_t* tidx, double* ex, doubl
         if (ib + 1 == boxes.size() && tj == i) continue;  // self, :119-124
         double dist2 = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2];
         double ee[3], pp;
-        force_leaf(m, d, dist2 + c->p.eps2, ee, pp);
+        law_leaf(c->p.force_law, m, d, dist2, c->p.eps2, ee, pp);
         e[0] += ee[0]; e[1] += ee[1]; e[2] += ee[2];
         ph += pp;
       }

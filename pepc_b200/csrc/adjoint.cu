@@ -514,6 +514,10 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
     c->err = "adjoint of the periodic far-lattice term is not implemented";
     return PEPCG_ERR_UNSUPPORTED;
   }
+  if (c->prm.force_law != 3) {
+    c->err = "the adjoint walk differentiates the 3D Coulomb law only (force_law = 3)";
+    return PEPCG_ERR_UNSUPPORTED;
+  }
   cudaStream_t s = c->stream;
   const int64_t M = c->nnodes;
   if (!ensure(c, c->adj, (size_t)kNA * M, "adjoint")) return PEPCG_ERR_OOM;

@@ -133,8 +133,12 @@ static void prepare_boxes(Ctx* c) {
 }
 
 static int check_params(Ctx* c, const pepcg_params* p) {
-  if (p->force_law != 3) {
-    c->err = "only force_law = 3 (3D Coulomb) is supported";
+  if (p->force_law != 2 && p->force_law != 3 && p->force_law != 4) {
+    c->err = "force_law must be 3 (3D Coulomb), 2 (2D Coulomb) or 4 (Lennard-Jones); 5 (Kelbg) is not built";
+    return PEPCG_ERR_UNSUPPORTED;
+  }
+  if (p->force_law != 3 && p->precision != PEPCG_PRECISION_PLAIN) {
+    c->err = "the mixed-precision walks evaluate the 3D Coulomb law only (force_law = 3)";
     return PEPCG_ERR_UNSUPPORTED;
   }
   if (p->mac_select < 0) {

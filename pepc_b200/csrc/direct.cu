@@ -15,6 +15,7 @@ namespace {
 constexpr int kTB = 8;
 constexpr int kDThreads = 256;
 
+template <int kLaw>
 __global__ void __launch_bounds__(kDThreads)
 k_direct(int64_t ntest, const int64_t* __restrict__ tidx, int64_t n, const double* __restrict__ x,
          const double* __restrict__ y, const double* __restrict__ z, const double* __restrict__ q,
@@ -49,7 +50,7 @@ k_direct(int64_t ntest, const int64_t* __restrict__ tidx, int64_t n, const doubl
         const double dx = (tx[k] - vx) - xs, dy = (ty[k] - vy) - ys, dz = (tz[k] - vz) - zs;
         const double dist2 = (dx * dx + dy * dy) + dz * dz;
         double fx, fy, fz, fp;
-        force_leaf64(qs, dx, dy, dz, dist2 + eps2, fx, fy, fz, fp);
+        law_leaf64<kLaw>(qs, dx, dy, dz, dist2, eps2, fx, fy, fz, fp);
         acc[k][0] += fx;
         acc[k][1] += fy;
         acc[k][2] += fz;
@@ -98,8 +99,9 @@ int direct_device(Ctx* c, int64_t ntest, const int64_t* d_tidx, double* ex, doub
   cudaStream_t s = c->stream;
   const int64_t nb = (ntest + kTB - 1) / kTB;
   COUNT_LAUNCH();
-  k_direct<<<(unsigned)nb, kDThreads, 0, s>>>(ntest, d_tidx, c->n, c->x.p, c->y.p, c->z.p, c->q.p,
-                                              c->d_vbox, c->nboxes, c->prm.eps2, ex, ey, ez, pot);
+  auto kern = c->prm.force_law == 2 ? k_direct<2> : (c->prm.force_law == 4 ? k_direct<4> : k_direct<3>);
+  kern<<<(unsigned)nb, kDThreads, 0, s>>>(ntest, d_tidx, c->n, c->x.p, c->y.p, c->z.p, c->q.p,
+                                          c->d_vbox, c->nboxes, c->prm.eps2, ex, ey, ez, pot);
   if (!cuda_ok(c, cudaGetLastError(), "direct launch")) return PEPCG_ERR_CUDA;
   if (c->far_field) {
     double* pos = nullptr;

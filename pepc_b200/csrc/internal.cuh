@@ -305,4 +305,75 @@ __host__ __device__ __forceinline__ void shift_up64(const Moments* ch, int nc, M
   p.bmax = bmax;
 }
 
+// calc_force_coulomb_2D_direct, coulomb/module_coulomb_kernels.f90:267-279
+// (d2 = dx^2 + dy^2 + eps2; E_z = 0)
+__host__ __device__ __forceinline__ void force_leaf_2d64(double q, double dx, double dy, double d2,
+                                                         double& ex, double& ey, double& ez,
+                                                         double& phi) {
+  phi = -((0.5 * q) * log(d2));
+  const double rd2charge = q / d2;
+  ex = rd2charge * dx;
+  ey = rd2charge * dy;
+  ez = 0.0;
+}
+
+// calc_force_coulomb_2D, coulomb/module_coulomb_kernels.f90:155-195
+__host__ __device__ __forceinline__ void force_twig_2d64(double q, const double* m, double dx,
+                                                         double dy, double d2, double& ex,
+                                                         double& ey, double& ez, double& phi) {
+  const double rd2 = 1.0 / d2, rd4 = rd2 * rd2, rd6 = rd4 * rd2;
+  const double dx2 = dx * dx, dy2 = dy * dy, dx3 = dx2 * dx, dy3 = dy2 * dy;
+  const double p1 = m[0], p2 = m[1], q1 = m[3], q2 = m[4], qxy = m[6];
+  phi = ((((-((0.5 * q) * log(d2))) - ((dx * p1) + (dy * p2)) * rd2) +
+          q1 * (((2.0 * dx2) * rd4) - rd2)) +
+         q2 * (((2.0 * dy2) * rd4) - rd2)) +
+        (((2.0 * qxy) * dx) * dy) * rd4;
+  ex = (((((q * dx) * rd2 - p1 * (((2.0 * dx2) * rd4) - rd2)) - (((p2 * 2.0) * dx) * dy) * rd4) +
+         q1 * (((8.0 * dx3) * rd6) - ((6.0 * dx) * rd4))) +
+        q2 * ((((8.0 * dx) * dy2) * rd6) - ((2.0 * dx) * rd4))) +
+       qxy * ((((8.0 * dx2) * dy) * rd6) - ((2.0 * dy) * rd4));
+  ey = (((((q * dy) * rd2 - p2 * (((2.0 * dy2) * rd4) - rd2)) - (((p1 * 2.0) * dx) * dy) * rd4) +
+         q2 * (((8.0 * dy3) * rd6) - ((6.0 * dy) * rd4))) +
+        q1 * ((((8.0 * dy) * dx2) * rd6) - ((2.0 * dy) * rd4))) +
+       qxy * ((((8.0 * dy2) * dx) * rd6) - ((2.0 * dx) * rd4));
+  ez = 0.0;
+}
+
+// calc_force_LJ, coulomb/module_coulomb_kernels.f90:204-235 (r2 unsoftened,
+// aii2 = eps2; leaves and twigs alike, phi = 0)
+__host__ __device__ __forceinline__ void force_lj64(double dx, double dy, double dz, double r2,
+                                                    double aii2, double& ex, double& ey,
+                                                    double& ez, double& phi) {
+  const double epsc2 = 0.8 * aii2;
+  const double aii2_r2 = (r2 > epsc2) ? aii2 / r2 : aii2 / epsc2;
+  const double aii4_r4 = aii2_r2 * aii2_r2;
+  const double flj = 2.0 * (aii4_r4 * aii4_r4) - aii4_r4;
+  phi = 0.0;
+  const double fljrd = flj / sqrt(r2);
+  ex = dx * fljrd;
+  ey = dy * fljrd;
+  ez = dz * fljrd;
+}
+
+// calc_force_per_interaction_with_leaf / _with_twig
+// (coulomb/module_interaction_specific.f90:314-387) for force_law kLaw
+// (3: 3D Coulomb, 2: 2D Coulomb, 4: Lennard-Jones); dist2 is unsoftened
+template <int kLaw>
+__host__ __device__ __forceinline__ void law_leaf64(double q, double dx, double dy, double dz,
+                                                    double dist2, double eps2, double& ex,
+                                                    double& ey, double& ez, double& phi) {
+  if (kLaw == 2) force_leaf_2d64(q, dx, dy, (dx * dx + dy * dy) + eps2, ex, ey, ez, phi);
+  else if (kLaw == 4) force_lj64(dx, dy, dz, dist2, eps2, ex, ey, ez, phi);
+  else force_leaf64(q, dx, dy, dz, dist2 + eps2, ex, ey, ez, phi);
+}
+template <int kLaw>
+__host__ __device__ __forceinline__ void law_twig64(double q, const double* m, double dx,
+                                                    double dy, double dz, double dist2,
+                                                    double eps2, double& ex, double& ey,
+                                                    double& ez, double& phi) {
+  if (kLaw == 2) force_twig_2d64(q, m, dx, dy, (dx * dx + dy * dy) + eps2, ex, ey, ez, phi);
+  else if (kLaw == 4) force_lj64(dx, dy, dz, dist2, eps2, ex, ey, ez, phi);
+  else force_twig64(q, m, dx, dy, dz, dist2 + eps2, ex, ey, ez, phi);
+}
+
 }  // namespace pepcg

@@ -66,6 +66,7 @@ __device__ __forceinline__ void warp_add_counters(unsigned long long* ctr, unsig
   }
 }
 
+template <int kLaw>
 __global__ void __launch_bounds__(kWalkThreads) k_walk_target64(WalkArgs A) {
   __shared__ double s_bl2[kMaxLevel + 1];
   __shared__ double s_vb[3 * 125];
@@ -108,7 +109,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_target64(WalkArgs A) {
           ++c_leaf;
           if (dist2 > 0.0) {
             double fx, fy, fz, fp;
-            force_leaf64(a.w, dx, dy, dz, dist2 + A.eps2, fx, fy, fz, fp);
+            law_leaf64<kLaw>(a.w, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp);
             e0 += fx; e1 += fy; e2 += fz; ph += fp;
           }
           next = u + 1;
@@ -120,7 +121,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_target64(WalkArgs A) {
 #pragma unroll
             for (int k = 0; k < 9; ++k) m[k] = A.mom[9 * (int64_t)u + k];
             double fx, fy, fz, fp;
-            force_twig64(a.w, m, dx, dy, dz, dist2 + A.eps2, fx, fy, fz, fp);
+            law_twig64<kLaw>(a.w, m, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp);
             e0 += fx; e1 += fy; e2 += fz; ph += fp;
             ++c_twig;
             w += 1.0;
@@ -140,6 +141,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_target64(WalkArgs A) {
   warp_add_counters(A.counters, c_leaf, c_twig, c_mac);
 }
 
+template <int kLaw>
 __global__ void __launch_bounds__(kWalkThreads) k_walk_tile64(WalkArgs A) {
   __shared__ double s_bl2[kMaxLevel + 1];
   __shared__ double s_vb[3 * 125];
@@ -183,7 +185,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_tile64(WalkArgs A) {
             ++c_leaf;
             if (dist2 > 0.0) {
               double fx, fy, fz, fp;
-              force_leaf64(a.w, dx, dy, dz, dist2 + A.eps2, fx, fy, fz, fp);
+              law_leaf64<kLaw>(a.w, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp);
               e0 += fx; e1 += fy; e2 += fz; ph += fp;
             }
           }
@@ -202,7 +204,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_tile64(WalkArgs A) {
 #pragma unroll
               for (int k = 0; k < 9; ++k) m[k] = A.mom[9 * (int64_t)u + k];
               double fx, fy, fz, fp;
-              force_twig64(a.w, m, dx, dy, dz, dist2 + A.eps2, fx, fy, fz, fp);
+              law_twig64<kLaw>(a.w, m, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp);
               e0 += fx; e1 += fy; e2 += fz; ph += fp;
               w += 1.0;
               ++c_twig;
@@ -366,11 +368,16 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
   const int blocks = 148 * 8;
   if (c->prm.precision == PEPCG_PRECISION_PLAIN) {
     COUNT_LAUNCH();
+    const int law = c->prm.force_law;
     if (walk == PEPCG_WALK_PER_TARGET) {
-      k_walk_target64<<<blocks, kWalkThreads, 0, s>>>(A);
+      if (law == 2) k_walk_target64<2><<<blocks, kWalkThreads, 0, s>>>(A);
+      else if (law == 4) k_walk_target64<4><<<blocks, kWalkThreads, 0, s>>>(A);
+      else k_walk_target64<3><<<blocks, kWalkThreads, 0, s>>>(A);
     } else {
       if (walk == PEPCG_WALK_GROUP) A.tiles = nullptr;
-      k_walk_tile64<<<blocks, kWalkThreads, 0, s>>>(A);
+      if (law == 2) k_walk_tile64<2><<<blocks, kWalkThreads, 0, s>>>(A);
+      else if (law == 4) k_walk_tile64<4><<<blocks, kWalkThreads, 0, s>>>(A);
+      else k_walk_tile64<3><<<blocks, kWalkThreads, 0, s>>>(A);
     }
   } else {
     int rc = launch_walk_mixed(c, nt, tx, ty, tz, ex, ey, ez, pot, work,

@@ -18,7 +18,7 @@ def grow_both(x, y, z, q, **kw):
     tc = P.TreeCode(**kw)
     okw = {k: v for k, v in kw.items() if k in ("theta2", "eps2", "curve", "tile_size",
                                                   "periodicity", "force_cubic_domain",
-                                                  "mac_select")}
+                                                  "mac_select", "force_law")}
     if "walk" in kw:
         okw["walk"] = 0 if kw["walk"] == P.WALK_PER_TARGET else 1
     orc = O.Oracle(num_threads=8, **okw)
@@ -122,6 +122,32 @@ def test_walk_other_macs_bit_exact(gpu, walk, mac):
         assert tc.stats()["twig_interactions"] == 0
 
 
+@pytest.mark.parametrize("walk", [P.WALK_PER_TARGET, P.WALK_PER_TILE])
+@pytest.mark.parametrize("law", [2, 4])
+def test_walk_other_force_laws(gpu, walk, law):
+    # force_law 2 (2D Coulomb: log potential, quadrupole in x, y) and 4
+    # (Lennard-Jones quiet-start force); the walk is unchanged.  LJ uses only
+    # + - * / sqrt, so it is bit-exact; the 2D law calls log, whose last bit
+    # may differ between CUDA and the host library
+    x, y, z, q = cube(6000, 26, charges="gauss")
+    tc, orc, g, go = grow_both(x, y, z, q, theta2=0.25, eps2=1e-4, walk=walk, force_law=law)
+    r = tc.pepc_traverse_tree(g.x, g.y, g.z, keys=g.key)
+    ro = orc.traverse_tree(go["x"], go["y"], go["z"], keys=go["key"])
+    assert np.array_equal(r["work"], ro["work"])
+    assert np.all(r["ez"] == 0.0) if law == 2 else np.all(r["pot"] == 0.0)
+    for k in ("ex", "ey", "ez", "pot"):
+        if law == 4:
+            assert np.array_equal(r[k], ro[k]), k
+        else:
+            scale = np.abs(ro[k]).max() + 1e-300
+            assert np.abs(r[k] - ro[k]).max() <= 1e-13 * scale, k
+    d = tc.direct(np.arange(0, 6000, 97))
+    do = orc.direct(np.arange(0, 6000, 97))
+    for k in ("ex", "ey", "ez", "pot"):
+        scale = np.abs(do[k]).max() + 1e-300
+        assert np.abs(d[k] - do[k]).max() <= 1e-12 * scale, k
+
+
 def test_walk_accumulates_and_foreign_targets(gpu):
     x, y, z, q = plummer(15000, 23)
     tc, orc, g, go = grow_both(x, y, z, q, theta2=0.25, eps2=1e-6, walk=P.WALK_PER_TARGET)
@@ -204,5 +230,9 @@ def test_errors_are_reported(gpu):
     with pytest.raises(P.PepcgError) as ei:
         tc2.pepc_traverse_tree([0.1], [0.1], [0.1])
     assert ei.value.code == P.PEPCG_ERR_NO_TREE
-    with pytest.raises(P.PepcgError):
-        P.TreeCode(force_law=2)
+    with pytest.raises(P.PepcgError) as ei:
+        P.TreeCode(force_law=5)  # Kelbg is not built
+    assert ei.value.code == P.PEPCG_ERR_UNSUPPORTED
+    with pytest.raises(P.PepcgError) as ei:
+        P.TreeCode(force_law=2, precision=P.PRECISION_MIXED)
+    assert ei.value.code == P.PEPCG_ERR_UNSUPPORTED
