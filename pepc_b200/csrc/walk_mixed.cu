@@ -248,12 +248,12 @@ __global__ void __launch_bounds__(kMixThreads, 5)
           // the batch is at most two contiguous runs of the ring
           const int n1 = min(n, kRing - hT);
           const StagedTwig* r = stw + hT;
-#pragma unroll 4
+#pragma unroll 16
           for (int j = 0; j < n1; ++j) {
             const float4 c = r[j].c;
             twig32(r[j].m0, r[j].m1, r[j].m2, rx - c.x, ry - c.y, rz - c.z, A.eps2, ax, ay, az, ap);
           }
-#pragma unroll 4
+#pragma unroll 8
           for (int j = 0; j < n - n1; ++j) {
             const float4 c = stw[j].c;
             twig32(stw[j].m0, stw[j].m1, stw[j].m2, rx - c.x, ry - c.y, rz - c.z, A.eps2, ax, ay,
@@ -287,7 +287,7 @@ __global__ void __launch_bounds__(kMixThreads, 5)
           // the batch is at most two contiguous runs of the ring
           const int n1 = min(n, kRing - hL);
           const StagedLeaf* r = stl + hL;
-#pragma unroll 4
+#pragma unroll 8
           for (int j = 0; j < n1; ++j) leaf(r[j]);
 #pragma unroll 4
           for (int j = 0; j < n - n1; ++j) leaf(stl[j]);
