@@ -426,6 +426,7 @@ def main():
 
     ms, launches, clk = timed(tc, args.steps, args.warmup, clocks=True)
     st = tc.stats()
+    fields_dev = (out[0].cpu().numpy(), out[3].cpu().numpy())  # for the host-path check
     value = job_rate(n, world, ms)
 
     # accuracy of this step's result against an FP64 direct sum on sampled targets
@@ -490,9 +491,11 @@ def main():
         dp = lambda a: a.ctypes.data_as(P.D)  # noqa: E731
         ipp = lambda a: a.ctypes.data_as(P.I64)  # noqa: E731
 
+        # the frontend's results clear folded into the traverse: the old values
+        # are not uploaded, the fields come back in full
+        tc.set_params(overwrite_results=1)
+
         def host_step():
-            for r_ in res:
-                r_.fill(0.0)
             tc._check(L.pepcg_grow_tree(tc._h, n, dp(hx), dp(hy), dp(hz), dp(hq), ipp(hk), ipp(hp),
                                         dp(hxo), dp(hyo), dp(hzo)))
             tc._check(L.pepcg_traverse_tree(tc._h, n, dp(hxo), dp(hyo), dp(hzo), ipp(hk),
@@ -510,13 +513,17 @@ def main():
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1) / ksteps
         ems = max_over_ranks(ems, dist, dev)
-        # grow: x y z q in; key, perm, x y z out.  traverse: x y z, key,
-        # e(3) pot work in; e(3) pot work out
-        h2d = n * (4 * 8) + n * (3 * 8 + 8 + 5 * 8)
+        tc.set_params(overwrite_results=0)
+        # the host path's fields against the device path's (same walk, same input)
+        same = bool(np.array_equal(res[0], fields_dev[0]) and np.array_equal(res[3], fields_dev[1]))
+        # grow: x y z q in; key, perm, x y z out.  traverse: x y z, key in;
+        # e(3) pot work out
+        h2d = n * (4 * 8) + n * (3 * 8 + 8)
         d2h = n * (8 + 8 + 3 * 8) + n * (5 * 8)
         e2e = {"value": n * world / (ems * 1e-3), "unit": UNIT, "ms_per_step": ems,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "api": "pepcg_grow_tree + pepcg_traverse_tree (host arrays, pinned)"}
+               "api": "pepcg_grow_tree + pepcg_traverse_tree (host arrays, pinned; "
+                      "overwrite_results = 1)", "fields_equal_device_path": same}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

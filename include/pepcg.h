@@ -85,7 +85,11 @@ typedef struct pepcg_params {
   double t_lattice_3[3];         /* [0,0,1] */
   double lattice_origin[3];      /* [0,0,0] */
   int32_t device;                /* CUDA device ordinal [0] */
-  int32_t reserved[7];
+  int32_t overwrite_results;     /* pepcg_traverse_tree: 0 = add to ex..work (+=, like
+                                    particle%results) [0]; 1 = overwrite them (the frontend's
+                                    results clear and the traverse in one call, with no
+                                    upload of the old values) */
+  int32_t reserved[6];
 } pepcg_params;
 
 /* Statistics of the last grow/traverse (module_tree.f90:622-699,

@@ -71,7 +71,8 @@ class Params(C.Structure):
         ("t_lattice_3", C.c_double * 3),
         ("lattice_origin", C.c_double * 3),
         ("device", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("overwrite_results", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 

@@ -489,9 +489,13 @@ int pepcg_traverse_tree(void* ctx, int64_t nt, const double* tx, const double* t
   cudaStream_t s = c->stream;
   double* b = c->tgt.p;
   const double* hin[8] = {tx, ty, tz, ex, ey, ez, pot, work};
+  // with overwrite_results the old values are not uploaded: the walk adds to zeros
+  const int nin = c->prm.overwrite_results ? 3 : 8;
   bool ok = true;
-  for (int k = 0; k < 8; ++k)
+  for (int k = 0; k < nin; ++k)
     ok = ok && cuda_ok(c, cudaMemcpyAsync(b + k * nt, hin[k], nt * 8, cudaMemcpyHostToDevice, s), "H2D");
+  if (nin == 3)
+    ok = ok && cuda_ok(c, cudaMemsetAsync(b + 3 * nt, 0, 5 * nt * 8, s), "clear results");
   if (tkeys) ok = ok && cuda_ok(c, cudaMemcpyAsync(c->tkeys.p, tkeys, nt * 8, cudaMemcpyHostToDevice, s), "H2D");
   if (!ok) return PEPCG_ERR_CUDA;
   int rc = traverse_device(c, nt, b, b + nt, b + 2 * nt, tkeys ? c->tkeys.p : nullptr, false,

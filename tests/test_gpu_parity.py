@@ -148,6 +148,20 @@ def test_walk_other_force_laws(gpu, walk, law):
         assert np.abs(d[k] - do[k]).max() <= 1e-12 * scale, k
 
 
+def test_overwrite_results(gpu):
+    # overwrite_results = 1: the old contents of ex..work are ignored, as if
+    # the frontend had cleared them before the traverse
+    x, y, z, q = cube(3000, 27)
+    tc, orc, g, go = grow_both(x, y, z, q, theta2=0.25, eps2=1e-4, walk=P.WALK_PER_TARGET)
+    r0 = tc.pepc_traverse_tree(g.x, g.y, g.z, keys=g.key)
+    tc.set_params(overwrite_results=1)
+    junk = [np.full(3000, 7.0) for _ in range(3)]
+    r1 = tc.pepc_traverse_tree(g.x, g.y, g.z, keys=g.key, e=junk, pot=np.full(3000, 5.0),
+                               work=np.full(3000, 3.0))
+    for k in ("ex", "ey", "ez", "pot", "work"):
+        assert np.array_equal(r0[k], r1[k]), k
+
+
 def test_walk_accumulates_and_foreign_targets(gpu):
     x, y, z, q = plummer(15000, 23)
     tc, orc, g, go = grow_both(x, y, z, q, theta2=0.25, eps2=1e-6, walk=P.WALK_PER_TARGET)
