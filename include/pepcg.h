@@ -206,6 +206,22 @@ int pepcg_apply_external_field_device(void* ctx, int64_t n, double ez_ext, const
 int pepcg_constrain_periodic_device(void* ctx, int64_t n, double* d_x, double* d_y, double* d_z);
 int pepcg_gather_device(void* ctx, const double* d_in, double* d_out);
 
+/*
+ * Sharding the targets of the grown particles over ranks (one GPU each, the
+ * tree replicated), and the way back to the caller's order.  No reference
+ * entry points: they stand for the MPI domain split of the particles
+ * (module_domains.f90) and domain_restore (:372-408).
+ *   pepcg_traverse_range_device  the fields on the grown particles [t0, t1) of
+ *     the key order, written to arrays of length t1 - t0 (accumulates like
+ *     pepcg_traverse_self_device); ranges that start at multiples of 32 give
+ *     exactly the single-call result in every walk mode;
+ *   pepcg_restore_device         out[perm[i]] = in[i]: a key-ordered array back
+ *     to the order of the last grow's input (in != out).
+ */
+int pepcg_traverse_range_device(void* ctx, int64_t t0, int64_t t1, double* d_ex, double* d_ey,
+                                double* d_ez, double* d_pot, double* d_work);
+int pepcg_restore_device(void* ctx, const double* d_in, double* d_out);
+
 /* Launch all of this context's work on the caller's CUDA stream (a
  * cudaStream_t of the context's device), or on a private non-blocking stream
  * when NULL (so the legacy default stream is selected with cudaStreamLegacy).

@@ -116,6 +116,7 @@ EXPORTS = [
     "pepcg_traverse_adjoint", "pepcg_traverse_adjoint_device",
     "pepcg_push_particles_device", "pepcg_apply_external_field_device",
     "pepcg_constrain_periodic_device", "pepcg_gather_device",
+    "pepcg_traverse_range_device", "pepcg_restore_device",
 ]
 
 _LIB = None
@@ -152,6 +153,8 @@ def lib():
     L.pepcg_apply_external_field_device.argtypes = [VP, C.c_int64, C.c_double, VP, VP, VP]
     L.pepcg_constrain_periodic_device.argtypes = [VP, C.c_int64, VP, VP, VP]
     L.pepcg_gather_device.argtypes = [VP, VP, VP]
+    L.pepcg_traverse_range_device.argtypes = [VP, C.c_int64, C.c_int64, VP, VP, VP, VP, VP]
+    L.pepcg_restore_device.argtypes = [VP, VP, VP]
     L.pepcg_kernel_launches.argtypes = []
     L.pepcg_kernel_launches.restype = C.c_longlong
     L.pepcg_stats_get.argtypes = [VP, C.POINTER(Stats)]
@@ -315,6 +318,15 @@ class TreeCode:
         """dst[i] = src[perm[i]] with the last grow's permutation (key order)."""
         return self._check(lib().pepcg_gather_device(self._h, _tptr(src), _tptr(dst)))
 
+    def traverse_range_device(self, t0, t1, ex, ey, ez, pot, work):
+        """Fields on the grown particles [t0, t1) of the key order (one rank's share)."""
+        return self._check(lib().pepcg_traverse_range_device(
+            self._h, int(t0), int(t1), _tptr(ex), _tptr(ey), _tptr(ez), _tptr(pot), _tptr(work)))
+
+    def restore_device(self, src, dst):
+        """dst[perm[i]] = src[i]: a key-ordered array back to the last grow's input order."""
+        return self._check(lib().pepcg_restore_device(self._h, _tptr(src), _tptr(dst)))
+
     def set_stream(self, stream_ptr):
         """Launch on an external cudaStream_t (int handle, e.g. torch's
         ``Stream.cuda_stream``); 0 is the legacy default stream (passed on as
@@ -420,3 +432,16 @@ def mac(theta2, dist2, boxlength2):
     a = C.c_int32(0)
     _chk(lib().pepcg_mac(float(theta2), float(dist2), float(boxlength2), C.byref(a)))
     return bool(a.value)
+
+
+def shard_range(n, rank, world, align=32):
+    """[t0, t1) of the key-ordered targets for one of `world` ranks: contiguous,
+    disjoint, covering [0, n), with every boundary a multiple of `align` so each
+    rank's 32-target groups are the single-GPU ones."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("need 0 <= rank < world")
+    blocks = (n + align - 1) // align
+    b0 = blocks * rank // world
+    b1 = blocks * (rank + 1) // world
+    return min(n, b0 * align), min(n, b1 * align)
+

@@ -476,6 +476,42 @@ int pepcg_traverse_self_device(void* ctx, double* d_ex, double* d_ey, double* d_
                          d_work);
 }
 
+int pepcg_traverse_range_device(void* ctx, int64_t t0, int64_t t1, double* d_ex, double* d_ey,
+                                double* d_ez, double* d_pot, double* d_work) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || !d_ex || !d_ey || !d_ez || !d_pot || !d_work) return PEPCG_ERR_BAD_ARG;
+  if (!c->has_tree) {
+    c->err = "no grown tree";
+    return PEPCG_ERR_NO_TREE;
+  }
+  if (t0 < 0 || t1 < t0 || t1 > c->n) {
+    c->err = "pepcg_traverse_range_device: need 0 <= t0 <= t1 <= n";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  if (t0 == t1) return PEPCG_OK;
+  cudaSetDevice(c->device);
+  if (t0 == 0 && t1 == c->n)
+    return traverse_device(c, c->n, c->x.p, c->y.p, c->z.p, c->key.p, true, d_ex, d_ey, d_ez,
+                           d_pot, d_work);
+  // the range's own keys give the per-tile walk its tiles, as a rank's local keys would
+  return traverse_device(c, t1 - t0, c->x.p + t0, c->y.p + t0, c->z.p + t0, c->key.p + t0, false,
+                         d_ex, d_ey, d_ez, d_pot, d_work);
+}
+
+int pepcg_restore_device(void* ctx, const double* d_in, double* d_out) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || !d_in || !d_out || d_in == d_out) {
+    if (c) c->err = "pepcg_restore_device: distinct input and output arrays are required";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  if (!c->has_tree) {
+    c->err = "pepcg_restore_device: no grown tree (the permutation comes from the last grow)";
+    return PEPCG_ERR_NO_TREE;
+  }
+  cudaSetDevice(c->device);
+  return restore_device(c, d_in, d_out);
+}
+
 int pepcg_traverse_tree(void* ctx, int64_t nt, const double* tx, const double* ty,
                         const double* tz, const int64_t* tkeys, double* ex, double* ey,
                         double* ez, double* pot, double* work) {

@@ -177,6 +177,7 @@ int external_field_device(Ctx* c, int64_t n, double ez_ext, const double* z, dou
                           double* pot);
 int wrap_device(Ctx* c, int64_t n, double* x, double* y, double* z);
 int gather_device(Ctx* c, const double* in, double* out);
+int restore_device(Ctx* c, const double* in, double* out);
 int widen_perm_device(Ctx* c, int64_t* out);
 int lattice_add(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                 double* ex, double* ey, double* ez, double* pot, bool overwrite);

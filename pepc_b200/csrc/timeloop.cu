@@ -10,7 +10,9 @@
 //               (inverse3, module_math_tools.f90:114-150);
 //   gather      out[i] = in[perm[i]]: carries per-particle state (velocity,
 //               mass, ...) into the key order of the last grow, as the
-//               reference's domain_decompose moves whole particle records.
+//               reference's domain_decompose moves whole particle records;
+//   restore     out[perm[i]] = in[i]: the way back to the input order
+//               (domain_restore, module_domains.f90:372-408).
 // Compiled with --fmad=false, so every result is the reference expression in
 // its order, rounded once per operation.
 
@@ -98,6 +100,13 @@ __global__ void k_gather(int64_t n, const int32_t* __restrict__ perm, const doub
     out[i] = in[perm[i]];
 }
 
+__global__ void k_scatter(int64_t n, const int32_t* __restrict__ perm, const double* __restrict__ in,
+                          double* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[perm[i]] = in[i];
+}
+
 __global__ void k_widen(int64_t n, const int32_t* __restrict__ in, int64_t* __restrict__ out) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
@@ -166,6 +175,12 @@ int gather_device(Ctx* c, const double* in, double* out) {
   COUNT_LAUNCH();
   k_gather<<<grid_of(c->n), kTL, 0, c->stream>>>(c->n, c->perm.p, in, out);
   return cuda_ok(c, cudaGetLastError(), "gather") ? PEPCG_OK : PEPCG_ERR_CUDA;
+}
+
+int restore_device(Ctx* c, const double* in, double* out) {
+  COUNT_LAUNCH();
+  k_scatter<<<grid_of(c->n), kTL, 0, c->stream>>>(c->n, c->perm.p, in, out);
+  return cuda_ok(c, cudaGetLastError(), "restore") ? PEPCG_OK : PEPCG_ERR_CUDA;
 }
 
 int widen_perm_device(Ctx* c, int64_t* out) {

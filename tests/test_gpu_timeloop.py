@@ -125,3 +125,57 @@ def test_device_resident_steps_match_the_oracle_loop(gpu):
     for a, b in zip([dx, dy, dz] + dv, [ox, oy, oz] + ov):
         assert np.array_equal(H(a), b)
     tc.close()
+
+
+@pytest.mark.parametrize("walk", [P.WALK_PER_TARGET, P.WALK_GROUP])
+@pytest.mark.parametrize("precision", [P.PRECISION_PLAIN, P.PRECISION_MIXED])
+def test_sharded_targets_equal_one_call(gpu, walk, precision):
+    # three ranks' shares of the key-ordered targets, each walked alone, give
+    # the single-call fields bit for bit (shares start at multiples of 32)
+    rng = np.random.default_rng(75)
+    n = 10007
+    x, y, z, q = rng.random(n), rng.random(n), rng.random(n), rng.standard_normal(n)
+    tc = P.TreeCode(theta2=0.25, eps2=1e-4, walk=walk, precision=precision)
+    tc.grow_tree_device(T(x), T(y), T(z), T(q))
+    full = [torch.zeros(n, dtype=torch.float64, device=DEV) for _ in range(5)]
+    tc.traverse_self_device(*full)
+    parts = [torch.zeros(n, dtype=torch.float64, device=DEV) for _ in range(5)]
+    for r in range(3):
+        t0, t1 = P.shard_range(n, r, 3)
+        tc.traverse_range_device(t0, t1, *[p[t0:t1] for p in parts])
+    for a, b in zip(full, parts):
+        assert torch.equal(a, b)
+    tc.close()
+
+
+def test_sharded_tiles_follow_the_range_keys(gpu):
+    # per-tile semantics on a share: tiles come from the share's own keys, as
+    # they would from a rank's local keys; checked against the oracle
+    rng = np.random.default_rng(76)
+    n = 6000
+    x, y, z, q = rng.random(n), rng.random(n), rng.random(n), rng.standard_normal(n)
+    tc = P.TreeCode(theta2=0.25, eps2=1e-4, walk=P.WALK_PER_TILE)
+    g = tc.pepc_grow_tree(x, y, z, q)
+    orc = O.Oracle(theta2=0.25, eps2=1e-4, walk=1)
+    go = orc.grow_tree(x, y, z, q)
+    t0, t1 = P.shard_range(n, 1, 2)
+    out = [torch.zeros(t1 - t0, dtype=torch.float64, device=DEV) for _ in range(5)]
+    tc.traverse_range_device(t0, t1, *out)
+    ro = orc.traverse_tree(go["x"][t0:t1], go["y"][t0:t1], go["z"][t0:t1], keys=go["key"][t0:t1])
+    for k, a in zip(("ex", "ey", "ez", "pot", "work"), out):
+        assert np.array_equal(H(a), ro[k]), k
+    tc.close()
+
+
+def test_restore_undoes_gather(gpu):
+    rng = np.random.default_rng(77)
+    n = 4000
+    x, y, z, q = rng.random(n), rng.random(n), rng.random(n), rng.standard_normal(n)
+    tc = P.TreeCode()
+    tc.pepc_grow_tree(x, y, z, q)
+    v = T(rng.standard_normal(n))
+    a, b = torch.empty_like(v), torch.empty_like(v)
+    tc.gather_device(v, a)
+    tc.restore_device(a, b)
+    assert torch.equal(b, v)
+    tc.close()

@@ -1,6 +1,8 @@
-"""CPU, two processes over gloo: the replica timing of bench.py -- each rank
-runs its own copy of the workload, the step time is the slowest rank's, and
-the job's rate counts every rank's particles."""
+"""CPU, two processes over gloo: the multi-rank host logic.  The replica
+timing of bench.py (each rank runs its own copy of the workload, the step
+time is the slowest rank's, the job's rate counts every rank's particles),
+and the target shares of pepc_b200.shard_range (contiguous, disjoint,
+covering, 32-aligned), gathered across the ranks."""
 import os
 import socket
 
@@ -10,6 +12,7 @@ import torch.distributed as dist
 import torch.multiprocessing as mp
 
 import bench
+import pepc_b200
 
 
 def _free_port():
@@ -42,6 +45,35 @@ def test_replicas_take_the_slowest_rank():
     m, rate = out[0]
     assert m == 15.0
     assert rate == pytest.approx(1000 * 2 / 15e-3)
+
+
+def _share_worker(rank, world, port, n, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        t0, t1 = pepc_b200.shard_range(n, rank, world)
+        mine = torch.tensor([t0, t1], dtype=torch.int64)
+        every = [torch.zeros(2, dtype=torch.int64) for _ in range(world)]
+        dist.all_gather(every, mine)
+        out[rank] = [tuple(int(v) for v in e) for e in every]
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("n", [10007, 64, 5])
+def test_target_shares_cover_the_particles(n):
+    world = 2
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.start_processes(_share_worker, args=(world, _free_port(), n, out), nprocs=world,
+                       join=True, start_method="spawn")
+    shares = out[0]
+    assert out[1] == shares
+    assert shares[0][0] == 0 and shares[-1][1] == n
+    for (a0, a1), (b0, b1) in zip(shares, shares[1:]):
+        assert a1 == b0 and a0 <= a1
+    assert all(t0 % 32 == 0 for t0, _ in shares)
 
 
 def test_single_rank_needs_no_process_group():
