@@ -69,7 +69,8 @@ extern "C" {
 typedef struct pepcg_params {
   double theta2;                 /* square of the BH opening angle [0.36] */
   double eps2;                   /* Plummer softening squared [0.0] */
-  int32_t force_law;             /* 3 3D Coulomb, 2 2D Coulomb, 4 Lennard-Jones (plain form) [3] */
+  int32_t force_law;             /* 3 3D Coulomb, 2 2D Coulomb, 4 Lennard-Jones, 5 Kelbg
+                                    (2, 4, 5: plain form) [3] */
   int32_t mac_select;            /* 0 Barnes-Hut, 1 Bmax, other > 0: no acceptance (N^2) [0] */
   int32_t curve;                 /* PEPCG_CURVE_* [HILBERT] */
   int32_t precision;             /* PEPCG_PRECISION_* [PLAIN] */
@@ -89,7 +90,8 @@ typedef struct pepcg_params {
                                     particle%results) [0]; 1 = overwrite them (the frontend's
                                     results clear and the traverse in one call, with no
                                     upload of the old values) */
-  int32_t reserved[6];
+  double kelbg_invsqrttemp;      /* force_law 5: 1/sqrt(temperature) (specific.f90:40) [0] */
+  int32_t reserved[4];
 } pepcg_params;
 
 /* Statistics of the last grow/traverse (module_tree.f90:622-699,

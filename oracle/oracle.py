@@ -36,6 +36,7 @@ class OrcParams(C.Structure):
         ("num_threads", C.c_int32),
         ("mac_select", C.c_int32),
         ("force_law", C.c_int32),
+        ("kelbg_invsqrttemp", C.c_double),
     ]
 
 

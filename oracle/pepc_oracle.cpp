@@ -382,14 +382,39 @@ inline void force_lj(const double d[3], double r2, double aii2, double e[3], dou
 // calc_force_per_interaction_with_leaf / _with_twig
 // (coulomb/module_interaction_specific.f90:314-387): the force law's kernel
 // for an unsoftened |delta|^2
+// calc_force_kelbg_3D_direct, coulomb/module_coulomb_kernels.f90:286-325
+// (tq: the target's charge; dist2 unsoftened)
+inline void force_kelbg(double tq, const double* t, const double d[3], double dist2, double kinv,
+                        double e[3], double& phi) {
+  const double q = t[M_Q];
+  double lambda;
+  if (tq * q < 0.0) lambda = 1.00027227 * kinv;      // e-i
+  else if (q > 0.0) lambda = 0.03300355 * kinv;      // i-i
+  else lambda = 1.41421356 * kinv;                   // e-e
+  const double sqrtpi = std::sqrt(std::acos(-1.0));
+  const double r = std::sqrt(dist2);
+  const double rd = 1.0 / r;
+  const double rd3 = (rd * rd) * rd;
+  const double rol = r / lambda;
+  const double ome = 1.0 - std::exp(-(rol * rol));
+  phi = (q * rd) * (ome + (sqrtpi * rol) * (1.0 - std::erf(rol)));
+  const double fprefac = (q * rd3) * ome;
+  e[0] = fprefac * d[0];
+  e[1] = fprefac * d[1];
+  e[2] = fprefac * d[2];
+}
+
 inline void law_leaf(int law, const double* t, const double d[3], double dist2, double eps2,
-                     double e[3], double& phi) {
+                     double e[3], double& phi, double tq = 0.0, double kinv = 0.0) {
   switch (law) {
     case 2:
       force_leaf_2d(t, d, (d[0] * d[0] + d[1] * d[1]) + eps2, e, phi);
       break;
     case 4:
       force_lj(d, dist2, eps2, e, phi);
+      break;
+    case 5:
+      force_kelbg(tq, t, d, dist2, kinv, e, phi);
       break;
     default:
       force_leaf(t, d, dist2 + eps2, e, phi);
@@ -403,6 +428,9 @@ inline void law_twig(int law, const double* t, const double d[3], double dist2, 
       break;
     case 4:
       force_lj(d, dist2, eps2, e, phi);
+      break;
+    case 5:  // multipole expansion with Coulomb, unsoftened (specific.f90:375-378)
+      force_twig(t, d, dist2, e, phi);
       break;
     default:
       force_twig(t, d, dist2 + eps2, e, phi);
@@ -575,7 +603,8 @@ struct Counters {
 // root (:601 parses it once and pushes the root's children); the todo list is
 // a LIFO stack.  Returns the number of partner leaves (completeness check :452).
 int64_t walk_pthreads(const orc_ctx* c, const double xt[3], const double vbox[3], double e[3],
-                      double& pot, double& work, Counters& cnt, std::vector<int64_t>& todo) {
+                      double& pot, double& work, Counters& cnt, std::vector<int64_t>& todo,
+                      double tq) {
   const double shifted[3] = {xt[0] - vbox[0], xt[1] - vbox[1], xt[2] - vbox[2]};  // :595
   int64_t partner = 0;
   todo.clear();
@@ -595,7 +624,7 @@ int64_t walk_pthreads(const orc_ctx* c, const double xt[3], const double vbox[3]
       work += 1.0;
       if (dist2 > 0.0) {
         double ee[3], ph;
-        law_leaf(c->p.force_law, nd.m, d, dist2, eps2, ee, ph);  // coulomb/...specific.f90:327-337
+        law_leaf(c->p.force_law, nd.m, d, dist2, eps2, ee, ph, tq, c->p.kelbg_invsqrttemp);  // specific.f90:327-343
         e[0] += ee[0]; e[1] += ee[1]; e[2] += ee[2];
         pot += ph;
       }
@@ -622,7 +651,7 @@ int64_t walk_pthreads(const orc_ctx* c, const double xt[3], const double vbox[3]
 // tree_walk_single_aux, treecode/lpepcsrc/module_tree_walk_simple.f90:301-384
 void walk_simple_aux(const orc_ctx* c, int64_t ni, int np, const double (*xs)[3],
                      const double vbox[3], double (*e)[3], double* pot, double* work,
-                     int64_t& partner, Counters& cnt) {
+                     int64_t& partner, Counters& cnt, const double* tqs) {
   const Node& nd = c->nodes[ni];
   const double eps2 = c->p.eps2;
   double d[32][3], d2[32];
@@ -635,7 +664,7 @@ void walk_simple_aux(const orc_ctx* c, int64_t ni, int np, const double (*xs)[3]
       work[ip] += 1.0;
       if (d2[ip] > 0.0) {
         double ee[3], ph;
-        law_leaf(c->p.force_law, nd.m, d[ip], d2[ip], eps2, ee, ph);
+        law_leaf(c->p.force_law, nd.m, d[ip], d2[ip], eps2, ee, ph, tqs[ip], c->p.kelbg_invsqrttemp);
         e[ip][0] += ee[0]; e[ip][1] += ee[1]; e[ip][2] += ee[2];
         pot[ip] += ph;
       }
@@ -648,7 +677,7 @@ void walk_simple_aux(const orc_ctx* c, int64_t ni, int np, const double (*xs)[3]
     d2[ip] = (d[ip][0] * d[ip][0] + d[ip][1] * d[ip][1]) + d[ip][2] * d[ip][2];
     if (!mac_pass(c, nd, d2[ip])) {  // MAC fails for this target: resolve
       for (int64_t ch = nd.first_child; ch != kNodeInvalid; ch = c->nodes[ch].next_sibling)
-        walk_simple_aux(c, ch, np, xs, vbox, e, pot, work, partner, cnt);
+        walk_simple_aux(c, ch, np, xs, vbox, e, pot, work, partner, cnt, tqs);
       return;
     }
   }
@@ -1070,6 +1099,13 @@ int orc_traverse_tree(orc_ctx* c, int64_t nt, const double* tx, const double* ty
   int nth = std::max(1, c->p.num_threads);
   std::vector<Counters> cnt(nth);
   std::atomic<int> bad{0};
+  // the Kelbg law needs each target's charge: the targets must be the grown
+  // particles in key order
+  const double* tq = nullptr;
+  if (c->p.force_law == 5) {
+    if (nt != c->n) return -6;
+    tq = c->q.data();
+  }
   // libpepc_traverse_tree, module_libpepc_main.f90:161-200: one walk per box,
   // central box last, then the per-particle lattice term.
   if (c->p.walk == 0) {
@@ -1081,7 +1117,7 @@ int orc_traverse_tree(orc_ctx* c, int64_t nt, const double* tx, const double* ty
       for (auto& bx : boxes) {
         double vb[3];
         lattice_vect(c->p, bx, vb);
-        int64_t partner = walk_pthreads(c, xt, vb, e, ph, w, cnt[t], todo);
+        int64_t partner = walk_pthreads(c, xt, vb, e, ph, w, cnt[t], todo, tq ? tq[i] : 0.0);
         if (partner != c->n) bad.store(1);
       }
       ex[i] = e[0]; ey[i] = e[1]; ez[i] = e[2]; pot[i] = ph; work[i] = w;
@@ -1097,8 +1133,9 @@ int orc_traverse_tree(orc_ctx* c, int64_t nt, const double* tx, const double* ty
     }
     parallel_for((int64_t)tiles.size(), nth, [&](int64_t it, int t) {
       int64_t lo = tiles[it].first, np = tiles[it].second - tiles[it].first;
-      double xs[32][3], e[32][3], ph[32], w[32];
+      double xs[32][3], e[32][3], ph[32], w[32], qs[32];
       for (int k = 0; k < np; ++k) {
+        qs[k] = tq ? tq[lo + k] : 0.0;
         xs[k][0] = tx[lo + k]; xs[k][1] = ty[lo + k]; xs[k][2] = tz[lo + k];
         e[k][0] = ex[lo + k]; e[k][1] = ey[lo + k]; e[k][2] = ez[lo + k];
         ph[k] = pot[lo + k]; w[k] = work[lo + k];
@@ -1107,7 +1144,7 @@ int orc_traverse_tree(orc_ctx* c, int64_t nt, const double* tx, const double* ty
         double vb[3];
         lattice_vect(c->p, bx, vb);
         int64_t partner = 0;
-        walk_simple_aux(c, c->root, (int)np, xs, vb, e, ph, w, partner, cnt[t]);
+        walk_simple_aux(c, c->root, (int)np, xs, vb, e, ph, w, partner, cnt[t], qs);
         if (partner != c->n) bad.store(1);
       }
       for (int k = 0; k < np; ++k) {
@@ -1182,7 +1219,7 @@ int orc_direct(orc_ctx* c, int64_t ntest, const int64_t* tidx, double* ex, doubl
         if (ib + 1 == boxes.size() && tj == i) continue;  // self, :119-124
         double dist2 = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2];
         double ee[3], pp;
-        law_leaf(c->p.force_law, m, d, dist2, c->p.eps2, ee, pp);
+        law_leaf(c->p.force_law, m, d, dist2, c->p.eps2, ee, pp, c->q[tj], c->p.kelbg_invsqrttemp);
         e[0] += ee[0]; e[1] += ee[1]; e[2] += ee[2];
         ph += pp;
       }

@@ -37,7 +37,8 @@ typedef struct orc_params {
   double lattice_origin[3];
   int32_t num_threads;      /* host threads for the walk (1 = serial) */
   int32_t mac_select;       /* 0 Barnes-Hut, 1 Bmax, other: no acceptance (N^2) */
-  int32_t force_law;        /* 3 3D Coulomb, 2 2D Coulomb, 4 Lennard-Jones */
+  int32_t force_law;        /* 3 3D Coulomb, 2 2D Coulomb, 4 Lennard-Jones, 5 Kelbg */
+  double kelbg_invsqrttemp; /* Kelbg: 1/sqrt(temperature) [0] */
 } orc_params;
 
 void orc_params_default(orc_params* p);

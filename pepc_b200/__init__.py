@@ -72,7 +72,8 @@ class Params(C.Structure):
         ("lattice_origin", C.c_double * 3),
         ("device", C.c_int32),
         ("overwrite_results", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("kelbg_invsqrttemp", C.c_double),
+        ("reserved", C.c_int32 * 4),
     ]
 
 

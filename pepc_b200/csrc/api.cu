@@ -133,8 +133,8 @@ static void prepare_boxes(Ctx* c) {
 }
 
 static int check_params(Ctx* c, const pepcg_params* p) {
-  if (p->force_law != 2 && p->force_law != 3 && p->force_law != 4) {
-    c->err = "force_law must be 3 (3D Coulomb), 2 (2D Coulomb) or 4 (Lennard-Jones); 5 (Kelbg) is not built";
+  if (p->force_law < 2 || p->force_law > 5) {
+    c->err = "force_law must be 3 (3D Coulomb), 2 (2D Coulomb), 4 (Lennard-Jones) or 5 (Kelbg)";
     return PEPCG_ERR_UNSUPPORTED;
   }
   if (p->force_law != 3 && p->precision != PEPCG_PRECISION_PLAIN) {
@@ -460,7 +460,9 @@ int pepcg_traverse_tree_device(void* ctx, int64_t nt, const double* d_tx, const 
   if (!c || nt < 0 || !d_tx || !d_ty || !d_tz || !d_ex || !d_ey || !d_ez || !d_pot || !d_work)
     return PEPCG_ERR_BAD_ARG;
   cudaSetDevice(c->device);
-  return traverse_device(c, nt, d_tx, d_ty, d_tz, d_tkeys, false, d_ex, d_ey, d_ez, d_pot, d_work);
+  const double* tq = c->prm.force_law == 5 ? grown_charges_if_same(c, nt, d_tkeys) : nullptr;
+  return traverse_device(c, nt, d_tx, d_ty, d_tz, d_tkeys, false, d_ex, d_ey, d_ez, d_pot, d_work,
+                         tq);
 }
 
 int pepcg_traverse_self_device(void* ctx, double* d_ex, double* d_ey, double* d_ez,
@@ -473,7 +475,7 @@ int pepcg_traverse_self_device(void* ctx, double* d_ex, double* d_ey, double* d_
   }
   cudaSetDevice(c->device);
   return traverse_device(c, c->n, c->x.p, c->y.p, c->z.p, c->key.p, true, d_ex, d_ey, d_ez, d_pot,
-                         d_work);
+                         d_work, c->q.p);
 }
 
 int pepcg_traverse_range_device(void* ctx, int64_t t0, int64_t t1, double* d_ex, double* d_ey,
@@ -492,10 +494,10 @@ int pepcg_traverse_range_device(void* ctx, int64_t t0, int64_t t1, double* d_ex,
   cudaSetDevice(c->device);
   if (t0 == 0 && t1 == c->n)
     return traverse_device(c, c->n, c->x.p, c->y.p, c->z.p, c->key.p, true, d_ex, d_ey, d_ez,
-                           d_pot, d_work);
+                           d_pot, d_work, c->q.p);
   // the range's own keys give the per-tile walk its tiles, as a rank's local keys would
   return traverse_device(c, t1 - t0, c->x.p + t0, c->y.p + t0, c->z.p + t0, c->key.p + t0, false,
-                         d_ex, d_ey, d_ez, d_pot, d_work);
+                         d_ex, d_ey, d_ez, d_pot, d_work, c->q.p + t0);
 }
 
 int pepcg_restore_device(void* ctx, const double* d_in, double* d_out) {
@@ -534,8 +536,10 @@ int pepcg_traverse_tree(void* ctx, int64_t nt, const double* tx, const double* t
     ok = ok && cuda_ok(c, cudaMemsetAsync(b + 3 * nt, 0, 5 * nt * 8, s), "clear results");
   if (tkeys) ok = ok && cuda_ok(c, cudaMemcpyAsync(c->tkeys.p, tkeys, nt * 8, cudaMemcpyHostToDevice, s), "H2D");
   if (!ok) return PEPCG_ERR_CUDA;
+  const double* tq =
+      c->prm.force_law == 5 ? grown_charges_if_same(c, nt, tkeys ? c->tkeys.p : nullptr) : nullptr;
   int rc = traverse_device(c, nt, b, b + nt, b + 2 * nt, tkeys ? c->tkeys.p : nullptr, false,
-                           b + 3 * nt, b + 4 * nt, b + 5 * nt, b + 6 * nt, b + 7 * nt);
+                           b + 3 * nt, b + 4 * nt, b + 5 * nt, b + 6 * nt, b + 7 * nt, tq);
   if (rc && rc != PEPCG_WARN_NOT_NEUTRAL) return rc;
   double* hout[5] = {ex, ey, ez, pot, work};
   for (int k = 0; k < 5; ++k)

@@ -7,6 +7,8 @@
 // reference's sequential loop, so results agree to rounding, not bitwise).
 // Compiled with --fmad=false.
 
+#include <cmath>
+
 #include "internal.cuh"
 
 namespace pepcg {
@@ -19,15 +21,16 @@ template <int kLaw>
 __global__ void __launch_bounds__(kDThreads)
 k_direct(int64_t ntest, const int64_t* __restrict__ tidx, int64_t n, const double* __restrict__ x,
          const double* __restrict__ y, const double* __restrict__ z, const double* __restrict__ q,
-         const double* __restrict__ vbox, int nbox, double eps2, double* __restrict__ ex,
-         double* __restrict__ ey, double* __restrict__ ez, double* __restrict__ pot) {
+         const double* __restrict__ vbox, int nbox, double eps2, double kinv, double sqrtpi,
+         double* __restrict__ ex, double* __restrict__ ey, double* __restrict__ ez,
+         double* __restrict__ pot) {
   __shared__ double s_vb[3 * 125];
   __shared__ double red[kDThreads / 32][kTB * 4];
   for (int i = threadIdx.x; i < 3 * nbox; i += blockDim.x) s_vb[i] = vbox[i];
   __syncthreads();
   const int64_t t0 = (int64_t)blockIdx.x * kTB;
   int64_t tj[kTB];
-  double tx[kTB], ty[kTB], tz[kTB];
+  double tx[kTB], ty[kTB], tz[kTB], tq[kTB];
   double acc[kTB][4];
 #pragma unroll
   for (int k = 0; k < kTB; ++k) {
@@ -37,6 +40,7 @@ k_direct(int64_t ntest, const int64_t* __restrict__ tidx, int64_t n, const doubl
     tx[k] = x[jj];
     ty[k] = y[jj];
     tz[k] = z[jj];
+    tq[k] = q[jj];
     acc[k][0] = acc[k][1] = acc[k][2] = acc[k][3] = 0.0;
   }
   for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
@@ -50,7 +54,8 @@ k_direct(int64_t ntest, const int64_t* __restrict__ tidx, int64_t n, const doubl
         const double dx = (tx[k] - vx) - xs, dy = (ty[k] - vy) - ys, dz = (tz[k] - vz) - zs;
         const double dist2 = (dx * dx + dy * dy) + dz * dz;
         double fx, fy, fz, fp;
-        law_leaf64<kLaw>(qs, dx, dy, dz, dist2, eps2, fx, fy, fz, fp);
+        law_leaf64<kLaw>(qs, dx, dy, dz, dist2, eps2, fx, fy, fz, fp,
+                         KelbgArgs{tq[k], kinv, sqrtpi});
         acc[k][0] += fx;
         acc[k][1] += fy;
         acc[k][2] += fz;
@@ -99,9 +104,12 @@ int direct_device(Ctx* c, int64_t ntest, const int64_t* d_tidx, double* ex, doub
   cudaStream_t s = c->stream;
   const int64_t nb = (ntest + kTB - 1) / kTB;
   COUNT_LAUNCH();
-  auto kern = c->prm.force_law == 2 ? k_direct<2> : (c->prm.force_law == 4 ? k_direct<4> : k_direct<3>);
+  const int law = c->prm.force_law;
+  auto kern = law == 2 ? k_direct<2> : law == 4 ? k_direct<4> : law == 5 ? k_direct<5> : k_direct<3>;
   kern<<<(unsigned)nb, kDThreads, 0, s>>>(ntest, d_tidx, c->n, c->x.p, c->y.p, c->z.p, c->q.p,
-                                          c->d_vbox, c->nboxes, c->prm.eps2, ex, ey, ez, pot);
+                                          c->d_vbox, c->nboxes, c->prm.eps2,
+                                          c->prm.kelbg_invsqrttemp, std::sqrt(std::acos(-1.0)), ex,
+                                          ey, ez, pot);
   if (!cuda_ok(c, cudaGetLastError(), "direct launch")) return PEPCG_ERR_CUDA;
   if (c->far_field) {
     double* pos = nullptr;

@@ -155,9 +155,11 @@ void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp
 // tiles of keyed targets that are not the grown particles (host recursion,
 // module_tree_walk_simple.f90:168-211); writes (first, count) pairs
 int host_tiles(Ctx* c, int64_t nt, const int64_t* d_tkeys, int T, int2* d_tiles, int64_t* ntiles);
+// tq: the targets' charges when they are grown particles (the Kelbg law needs
+// them), else nullptr
 int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                     const int64_t* tkeys, bool self, double* ex, double* ey, double* ez,
-                    double* pot, double* work);
+                    double* pot, double* work, const double* tq = nullptr);
 
 // ---- adjoint.cu ----
 int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
@@ -169,6 +171,9 @@ int lattice_prepare(Ctx* c);
 int lattice_timestep(Ctx* c);
 // walk_plain.cu: per-twig MAC thresholds for mac_select != 0 (nullptr for Barnes-Hut)
 int prepare_mac(Ctx* c, const double** macb);
+// the grown particles' charges when the targets are exactly the grown
+// particles in key order (same keys), else nullptr
+const double* grown_charges_if_same(Ctx* c, int64_t nt, const int64_t* d_tkeys);
 // timeloop.cu
 int push_device(Ctx* c, int64_t n, double dt, const double* q, const double* m, const double* ex,
                 const double* ey, const double* ez, double* vx, double* vy, double* vz, double* x,
@@ -356,15 +361,44 @@ __host__ __device__ __forceinline__ void force_lj64(double dx, double dy, double
   ez = dz * fljrd;
 }
 
+// calc_force_kelbg_3D_direct, coulomb/module_coulomb_kernels.f90:286-325:
+// tq the target's charge, kinv = kelbg_invsqrttemp, sqrtpi = sqrt(acos(-1));
+// dist2 unsoftened
+struct KelbgArgs {
+  double tq, kinv, sqrtpi;
+};
+__host__ __device__ __forceinline__ void force_kelbg64(double q, double dx, double dy, double dz,
+                                                       double dist2, const KelbgArgs& k,
+                                                       double& ex, double& ey, double& ez,
+                                                       double& phi) {
+  double lambda;
+  if (k.tq * q < 0.0) lambda = 1.00027227 * k.kinv;  // e-i
+  else if (q > 0.0) lambda = 0.03300355 * k.kinv;    // i-i
+  else lambda = 1.41421356 * k.kinv;                 // e-e
+  const double r = sqrt(dist2);
+  const double rd = 1.0 / r;
+  const double rd3 = (rd * rd) * rd;
+  const double rol = r / lambda;
+  const double ome = 1.0 - exp(-(rol * rol));
+  phi = (q * rd) * (ome + (k.sqrtpi * rol) * (1.0 - erf(rol)));
+  const double fprefac = (q * rd3) * ome;
+  ex = fprefac * dx;
+  ey = fprefac * dy;
+  ez = fprefac * dz;
+}
+
 // calc_force_per_interaction_with_leaf / _with_twig
 // (coulomb/module_interaction_specific.f90:314-387) for force_law kLaw
-// (3: 3D Coulomb, 2: 2D Coulomb, 4: Lennard-Jones); dist2 is unsoftened
+// (3: 3D Coulomb, 2: 2D Coulomb, 4: Lennard-Jones, 5: Kelbg leaves with
+// unsoftened Coulomb twigs); dist2 is unsoftened
 template <int kLaw>
 __host__ __device__ __forceinline__ void law_leaf64(double q, double dx, double dy, double dz,
                                                     double dist2, double eps2, double& ex,
-                                                    double& ey, double& ez, double& phi) {
+                                                    double& ey, double& ez, double& phi,
+                                                    const KelbgArgs& kel = KelbgArgs{0, 0, 0}) {
   if (kLaw == 2) force_leaf_2d64(q, dx, dy, (dx * dx + dy * dy) + eps2, ex, ey, ez, phi);
   else if (kLaw == 4) force_lj64(dx, dy, dz, dist2, eps2, ex, ey, ez, phi);
+  else if (kLaw == 5) force_kelbg64(q, dx, dy, dz, dist2, kel, ex, ey, ez, phi);
   else force_leaf64(q, dx, dy, dz, dist2 + eps2, ex, ey, ez, phi);
 }
 template <int kLaw>
@@ -374,6 +408,7 @@ __host__ __device__ __forceinline__ void law_twig64(double q, const double* m, d
                                                     double& ez, double& phi) {
   if (kLaw == 2) force_twig_2d64(q, m, dx, dy, (dx * dx + dy * dy) + eps2, ex, ey, ez, phi);
   else if (kLaw == 4) force_lj64(dx, dy, dz, dist2, eps2, ex, ey, ez, phi);
+  else if (kLaw == 5) force_twig64(q, m, dx, dy, dz, dist2, ex, ey, ez, phi);
   else force_twig64(q, m, dx, dy, dz, dist2 + eps2, ex, ey, ez, phi);
 }
 

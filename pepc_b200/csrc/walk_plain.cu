@@ -13,6 +13,8 @@
 //    visited first to last (key order) through the fwd pointers.
 // Compiled with --fmad=false: results are bit-identical to the oracle.
 
+#include <cmath>
+
 #include "internal.cuh"
 
 namespace pepcg {
@@ -35,6 +37,8 @@ struct WalkArgs {
   const int32_t* nleaves;
   const double* bl2;   // boxlength2[0..20]
   const double* macb;  // per-twig MAC threshold, or nullptr: bl2 of the level (Barnes-Hut)
+  const double* tq;    // force_law 5: the targets' charges
+  double kinv, sqrtpi;  // force_law 5: kelbg_invsqrttemp, sqrt(acos(-1))
   const double* vbox;  // 3 * nbox
   int nbox;
   double theta2, eps2;
@@ -84,8 +88,10 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_target64(WalkArgs A) {
     const int64_t t = (int64_t)b * 32 + lane;
     const bool valid = t < A.nt;
     double px = 0, py = 0, pz = 0, e0 = 0, e1 = 0, e2 = 0, ph = 0, w = 0;
+    KelbgArgs kel{0.0, A.kinv, A.sqrtpi};
     if (valid) {
       px = A.tx[t]; py = A.ty[t]; pz = A.tz[t];
+      if (kLaw == 5) kel.tq = A.tq[t];
       e0 = A.ex[t]; e1 = A.ey[t]; e2 = A.ez[t]; ph = A.pot[t]; w = A.work[t];
     }
     bool complete = true;
@@ -109,7 +115,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_target64(WalkArgs A) {
           ++c_leaf;
           if (dist2 > 0.0) {
             double fx, fy, fz, fp;
-            law_leaf64<kLaw>(a.w, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp);
+            law_leaf64<kLaw>(a.w, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp, kel);
             e0 += fx; e1 += fy; e2 += fz; ph += fp;
           }
           next = u + 1;
@@ -162,8 +168,10 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_tile64(WalkArgs A) {
     const bool valid = lane < tl.y;
     const int64_t t = (int64_t)tl.x + lane;
     double px = 0, py = 0, pz = 0, e0 = 0, e1 = 0, e2 = 0, ph = 0, w = 0;
+    KelbgArgs kel{0.0, A.kinv, A.sqrtpi};
     if (valid) {
       px = A.tx[t]; py = A.ty[t]; pz = A.tz[t];
+      if (kLaw == 5) kel.tq = A.tq[t];
       e0 = A.ex[t]; e1 = A.ey[t]; e2 = A.ez[t]; ph = A.pot[t]; w = A.work[t];
     }
     bool complete = true;
@@ -185,7 +193,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_tile64(WalkArgs A) {
             ++c_leaf;
             if (dist2 > 0.0) {
               double fx, fy, fz, fp;
-              law_leaf64<kLaw>(a.w, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp);
+              law_leaf64<kLaw>(a.w, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp, kel);
               e0 += fx; e1 += fy; e2 += fz; ph += fp;
             }
           }
@@ -278,6 +286,19 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
                       double* ex, double* ey, double* ez, double* pot, double* work,
                       const int2* tiles, int64_t ntiles, bool per_target);
 
+const double* grown_charges_if_same(Ctx* c, int64_t nt, const int64_t* d_tkeys) {
+  if (!d_tkeys || nt != c->n) return nullptr;
+  unsigned int* d_diff = reinterpret_cast<unsigned int*>(c->d_small + 7);
+  unsigned int h_diff = 1;
+  cudaMemsetAsync(d_diff, 0, 4, c->stream);
+  COUNT_LAUNCH();
+  k_same_keys<<<296, 256, 0, c->stream>>>(nt, d_tkeys, c->key.p, d_diff);
+  if (!cuda_ok(c, cudaMemcpyAsync(&h_diff, d_diff, 4, cudaMemcpyDeviceToHost, c->stream), "keys") ||
+      !cuda_ok(c, cudaStreamSynchronize(c->stream), "keys"))
+    return nullptr;
+  return h_diff == 0 ? c->q.p : nullptr;
+}
+
 int prepare_mac(Ctx* c, const double** macb) {
   *macb = nullptr;
   if (c->prm.mac_select == 0) return PEPCG_OK;
@@ -294,12 +315,18 @@ int prepare_mac(Ctx* c, const double** macb) {
 
 int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                     const int64_t* tkeys, bool self, double* ex, double* ey, double* ez,
-                    double* pot, double* work) {
+                    double* pot, double* work, const double* tq) {
   if (!c->has_tree) {
     c->err = "traverse called without a grown tree";
     return PEPCG_ERR_NO_TREE;
   }
   if (nt <= 0) return PEPCG_OK;
+  if (c->prm.force_law == 5 && !tq) {
+    c->err = "force_law 5 (Kelbg) needs the targets' charges: traverse the grown particles "
+             "(pepcg_traverse_self_device, pepcg_traverse_range_device, or pepcg_traverse_tree "
+             "with the grown keys)";
+    return PEPCG_ERR_UNSUPPORTED;
+  }
   cudaStream_t s = c->stream;
   const int walk = c->prm.walk;
   if (!cuda_ok(c, cudaMemsetAsync(c->counters.p, 0, 4 * sizeof(unsigned long long), s), "ctr") ||
@@ -363,6 +390,9 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
   A.status = c->d_status;
   A.tiles = reinterpret_cast<const int2*>(c->tiles.p);
   A.ntiles = ntiles;
+  A.tq = tq;
+  A.kinv = c->prm.kelbg_invsqrttemp;
+  A.sqrtpi = std::sqrt(std::acos(-1.0));
   COUNT_LAUNCH();
   k_reset_counter<<<1, 1, 0, s>>>();
   const int blocks = 148 * 8;
@@ -372,11 +402,13 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
     if (walk == PEPCG_WALK_PER_TARGET) {
       if (law == 2) k_walk_target64<2><<<blocks, kWalkThreads, 0, s>>>(A);
       else if (law == 4) k_walk_target64<4><<<blocks, kWalkThreads, 0, s>>>(A);
+      else if (law == 5) k_walk_target64<5><<<blocks, kWalkThreads, 0, s>>>(A);
       else k_walk_target64<3><<<blocks, kWalkThreads, 0, s>>>(A);
     } else {
       if (walk == PEPCG_WALK_GROUP) A.tiles = nullptr;
       if (law == 2) k_walk_tile64<2><<<blocks, kWalkThreads, 0, s>>>(A);
       else if (law == 4) k_walk_tile64<4><<<blocks, kWalkThreads, 0, s>>>(A);
+      else if (law == 5) k_walk_tile64<5><<<blocks, kWalkThreads, 0, s>>>(A);
       else k_walk_tile64<3><<<blocks, kWalkThreads, 0, s>>>(A);
     }
   } else {

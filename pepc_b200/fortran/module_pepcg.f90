@@ -29,7 +29,8 @@ module module_pepcg
       real(c_double) :: t_lattice_1(3), t_lattice_2(3), t_lattice_3(3), lattice_origin(3)
       integer(c_int32_t) :: device
       integer(c_int32_t) :: overwrite_results
-      integer(c_int32_t) :: reserved(6)
+      real(c_double) :: kelbg_invsqrttemp
+      integer(c_int32_t) :: reserved(4)
    end type
 
    interface

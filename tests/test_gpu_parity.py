@@ -18,7 +18,8 @@ def grow_both(x, y, z, q, **kw):
     tc = P.TreeCode(**kw)
     okw = {k: v for k, v in kw.items() if k in ("theta2", "eps2", "curve", "tile_size",
                                                   "periodicity", "force_cubic_domain",
-                                                  "mac_select", "force_law")}
+                                                  "mac_select", "force_law",
+                                                  "kelbg_invsqrttemp")}
     if "walk" in kw:
         okw["walk"] = 0 if kw["walk"] == P.WALK_PER_TARGET else 1
     orc = O.Oracle(num_threads=8, **okw)
@@ -148,6 +149,30 @@ def test_walk_other_force_laws(gpu, walk, law):
         assert np.abs(d[k] - do[k]).max() <= 1e-12 * scale, k
 
 
+@pytest.mark.parametrize("walk", [P.WALK_PER_TARGET, P.WALK_PER_TILE])
+def test_walk_kelbg(gpu, walk):
+    # force_law 5: Kelbg leaves (erf / exp; lambda from the target's and the
+    # source's charges) and unsoftened Coulomb twigs; the targets must be the
+    # grown particles, whose charges the library knows
+    x, y, z, q = cube(5000, 28)  # +1 / -1 alternating: e-i, i-i and e-e pairs
+    kw = dict(theta2=0.25, eps2=1e-4, walk=walk, force_law=5, kelbg_invsqrttemp=20.0)
+    tc, orc, g, go = grow_both(x, y, z, q, **kw)
+    r = tc.pepc_traverse_tree(g.x, g.y, g.z, keys=g.key)
+    ro = orc.traverse_tree(go["x"], go["y"], go["z"], keys=go["key"])
+    assert np.array_equal(r["work"], ro["work"])
+    for k in ("ex", "ey", "ez", "pot"):
+        scale = np.abs(ro[k]).max()
+        assert np.abs(r[k] - ro[k]).max() <= 1e-13 * scale, k
+    d = tc.direct(np.arange(0, 5000, 61))
+    do = orc.direct(np.arange(0, 5000, 61))
+    for k in ("ex", "ey", "ez", "pot"):
+        scale = np.abs(do[k]).max()
+        assert np.abs(d[k] - do[k]).max() <= 1e-12 * scale, k
+    with pytest.raises(P.PepcgError) as ei:  # foreign targets: their charges are unknown
+        tc.pepc_traverse_tree(np.array([0.5]), np.array([0.5]), np.array([0.5]))
+    assert ei.value.code == P.PEPCG_ERR_UNSUPPORTED
+
+
 def test_overwrite_results(gpu):
     # overwrite_results = 1: the old contents of ex..work are ignored, as if
     # the frontend had cleared them before the traverse
@@ -245,7 +270,7 @@ def test_errors_are_reported(gpu):
         tc2.pepc_traverse_tree([0.1], [0.1], [0.1])
     assert ei.value.code == P.PEPCG_ERR_NO_TREE
     with pytest.raises(P.PepcgError) as ei:
-        P.TreeCode(force_law=5)  # Kelbg is not built
+        P.TreeCode(force_law=6)
     assert ei.value.code == P.PEPCG_ERR_UNSUPPORTED
     with pytest.raises(P.PepcgError) as ei:
         P.TreeCode(force_law=2, precision=P.PRECISION_MIXED)
