@@ -155,6 +155,32 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def hbm_peak_gbs():
+    """The measured copy bandwidth of this pool's B200s, else the fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def grow_roofline(st, n):
+    """Achieved HBM bandwidth of the grow phases from their algorithmic bytes:
+    bounding box 24 B and keys 32 B per particle; sort 24 B (one read and
+    write of key + index) plus the permutation 64 B per particle; tree build
+    8 B per particle + 40 B per node; upward pass 240 B per twig."""
+    peak, src = hbm_peak_gbs()
+    nodes = st["nleaf"] + st["ntwig"]
+    phases = {"keys": (st["t_keys_ms"], 56 * n), "sort": (st["t_sort_ms"], 88 * n),
+              "tree": (st["t_tree_ms"], 8 * n + 40 * nodes),
+              "upward": (st["t_upward_ms"], 240 * st["ntwig"])}
+    out = {"peak_gbs": peak, "peak_source": src}
+    for k, (ms, b) in phases.items():
+        gbs = b / (ms * 1e-3) / 1e9 if ms > 0 else None
+        out[k] = {"bytes": b, "ms": ms, "gbs": gbs, "frac": (gbs / peak) if gbs else None}
+    return out
+
+
 def max_over_ranks(ms, dist, device):
     """The slowest rank's time: every rank's replica must finish for the job's step
     to end.  `dist` is torch.distributed (or None for one rank)."""
@@ -458,6 +484,7 @@ def main():
             "interactions": {"twig": st["twig_interactions"], "leaf": st["leaf_interactions"]}}
     phases = {k: st[k] for k in ("t_keys_ms", "t_sort_ms", "t_tree_ms", "t_upward_ms",
                                  "t_walk_ms", "t_lattice_ms")}
+    grow_roof = grow_roofline(st, n)
 
     # the plain FP64 drop-in form (per-target walk) on the same input
     plain = None
@@ -545,7 +572,8 @@ def main():
                       "against": "FP64 direct sum (pepcg_direct)"},
         "walk_only": {"value": n * world / (st["t_walk_ms"] * 1e-3), "unit": UNIT,
                       "ms": st["t_walk_ms"]},
-        "roofline": roof, "phases_ms": phases, "gpu_launches": launches,
+        "roofline": roof, "phases_ms": phases, "grow_roofline": grow_roof,
+        "gpu_launches": launches,
         "clocks": clk, "e2e": e2e, "plain": plain,
         "mixed_over_plain": (value / plain["value"]) if plain else None,
         "cpu_baseline": cpu,
