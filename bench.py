@@ -543,9 +543,10 @@ def main():
         tc.set_params(overwrite_results=0)
         # the host path's fields against the device path's (same walk, same input)
         same = bool(np.array_equal(res[0], fields_dev[0]) and np.array_equal(res[3], fields_dev[1]))
-        # grow: x y z q in; key, perm, x y z out.  traverse: x y z, key in;
-        # e(3) pot work out
-        h2d = n * (4 * 8) + n * (3 * 8 + 8)
+        # grow: x y z q in; key, perm, x y z out.  traverse: x y z in (the
+        # group walk does not read the keys, so they are not uploaded); e(3)
+        # pot work out
+        h2d = n * (4 * 8) + n * (3 * 8)
         d2h = n * (8 + 8 + 3 * 8) + n * (5 * 8)
         e2e = {"value": n * world / (ems * 1e-3), "unit": UNIT, "ms_per_step": ems,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

@@ -352,6 +352,15 @@ int pepcg_destroy(void* ctx) {
     if (p) cudaFree(p);
   for (int i = 0; i < 8; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  for (int i = 0; i < Ctx::kMaxChunks; ++i) {
+    if (c->ready[i]) cudaEventDestroy(c->ready[i]);
+    if (c->done[i]) cudaEventDestroy(c->done[i]);
+  }
+  for (cudaStream_t t : {c->h2d, c->d2h})
+    if (t) {
+      cudaStreamSynchronize(t);
+      cudaStreamDestroy(t);
+    }
   if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
   delete c;
   return PEPCG_OK;
@@ -375,6 +384,26 @@ int pepcg_set_params(void* ctx, const pepcg_params* p) {
   }
   c->prm = *p;
   return PEPCG_OK;
+}
+
+// The copy streams and chunk events of the host-array entry points, created on
+// first use.
+static bool copy_streams(Ctx* c) {
+  if (c->h2d) return true;
+  bool ok = cuda_ok(c, cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking), "copy stream") &&
+            cuda_ok(c, cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking), "copy stream");
+  for (int i = 0; ok && i < Ctx::kMaxChunks; ++i)
+    ok = cuda_ok(c, cudaEventCreateWithFlags(&c->ready[i], cudaEventDisableTiming), "event") &&
+         cuda_ok(c, cudaEventCreateWithFlags(&c->done[i], cudaEventDisableTiming), "event");
+  return ok;
+}
+
+// Waits for both copy streams (they may hold transfers of caller arrays) and
+// folds their status into ok.
+static bool drain_copies(Ctx* c, bool ok) {
+  for (cudaStream_t t : {c->h2d, c->d2h})
+    if (t) ok = cuda_ok(c, cudaStreamSynchronize(t), "copy stream") && ok;
+  return ok;
 }
 
 int pepcg_grow_tree_device(void* ctx, int64_t n, const double* d_x, const double* d_y,
@@ -413,21 +442,27 @@ int pepcg_grow_tree(void* ctx, int64_t n, const double* x, const double* y, cons
     return PEPCG_ERR_CUDA;
   int rc = pepcg_grow_tree_device(c, n, c->in_x.p, c->in_y.p, c->in_z.p, c->in_q.p);
   if (rc && rc != PEPCG_WARN_NOT_NEUTRAL) return rc;
-  bool ok = true;
+  // The outputs are final once the duplicate fix has run (event 2, before the
+  // tree build): copy them back on the device-to-host stream while the tree
+  // build and the upward pass run on the context stream.  The call returns
+  // when the copies are done; the rest of the grow stays stream-ordered
+  // before the next call's work.
+  if (!copy_streams(c)) return PEPCG_ERR_CUDA;
+  cudaStream_t t = c->d2h;
+  bool ok = cuda_ok(c, cudaStreamWaitEvent(t, c->ev[2], 0), "grow outputs");
   if (key_out)
-    ok = ok && cuda_ok(c, cudaMemcpyAsync(key_out, c->key.p, n * 8, cudaMemcpyDeviceToHost, s), "D2H key");
+    ok = ok && cuda_ok(c, cudaMemcpyAsync(key_out, c->key.p, n * 8, cudaMemcpyDeviceToHost, t), "D2H key");
   if (perm_out) {
     // widened to 64 bits on the device (scratch: the target-key buffer)
-    if (!ensure(c, c->tkeys, n, "perm")) return PEPCG_ERR_OOM;
-    ok = ok && widen_perm_device(c, c->tkeys.p) == PEPCG_OK &&
-         cuda_ok(c, cudaMemcpyAsync(perm_out, c->tkeys.p, n * 8, cudaMemcpyDeviceToHost, s),
+    if (!ensure(c, c->tkeys, n, "perm")) return drain_copies(c, false), PEPCG_ERR_OOM;
+    ok = ok && widen_perm_device(c, c->tkeys.p, t) == PEPCG_OK &&
+         cuda_ok(c, cudaMemcpyAsync(perm_out, c->tkeys.p, n * 8, cudaMemcpyDeviceToHost, t),
                  "D2H perm");
   }
-  if (x_out) ok = ok && cuda_ok(c, cudaMemcpyAsync(x_out, c->x.p, n * 8, cudaMemcpyDeviceToHost, s), "D2H x");
-  if (y_out) ok = ok && cuda_ok(c, cudaMemcpyAsync(y_out, c->y.p, n * 8, cudaMemcpyDeviceToHost, s), "D2H y");
-  if (z_out) ok = ok && cuda_ok(c, cudaMemcpyAsync(z_out, c->z.p, n * 8, cudaMemcpyDeviceToHost, s), "D2H z");
-  ok = ok && cuda_ok(c, cudaStreamSynchronize(s), "grow");
-  if (!ok) return PEPCG_ERR_CUDA;
+  if (x_out) ok = ok && cuda_ok(c, cudaMemcpyAsync(x_out, c->x.p, n * 8, cudaMemcpyDeviceToHost, t), "D2H x");
+  if (y_out) ok = ok && cuda_ok(c, cudaMemcpyAsync(y_out, c->y.p, n * 8, cudaMemcpyDeviceToHost, t), "D2H y");
+  if (z_out) ok = ok && cuda_ok(c, cudaMemcpyAsync(z_out, c->z.p, n * 8, cudaMemcpyDeviceToHost, t), "D2H z");
+  if (!drain_copies(c, ok)) return PEPCG_ERR_CUDA;
   return rc;
 }
 
@@ -514,6 +549,10 @@ int pepcg_restore_device(void* ctx, const double* d_in, double* d_out) {
   return restore_device(c, d_in, d_out);
 }
 
+// Host targets at least this many are walked in chunks, overlapping the
+// uploads and downloads with the walk.
+constexpr int64_t kChunkedTargets = 1 << 18;
+
 int pepcg_traverse_tree(void* ctx, int64_t nt, const double* tx, const double* ty,
                         const double* tz, const int64_t* tkeys, double* ex, double* ey,
                         double* ez, double* pot, double* work) {
@@ -522,26 +561,71 @@ int pepcg_traverse_tree(void* ctx, int64_t nt, const double* tx, const double* t
     return PEPCG_ERR_BAD_ARG;
   if (nt == 0) return PEPCG_OK;
   cudaSetDevice(c->device);
-  if (!ensure(c, c->tgt, 8 * nt, "targets") || (tkeys && !ensure(c, c->tkeys, nt, "tkeys")))
+  // the keys steer only the per-tile walk's tiles and the Kelbg law's charges
+  const bool keys_used = tkeys && (c->prm.walk == PEPCG_WALK_PER_TILE || c->prm.force_law == 5);
+  if (!ensure(c, c->tgt, 8 * nt, "targets") || (keys_used && !ensure(c, c->tkeys, nt, "tkeys")))
     return PEPCG_ERR_OOM;
   cudaStream_t s = c->stream;
   double* b = c->tgt.p;
   const double* hin[8] = {tx, ty, tz, ex, ey, ez, pot, work};
+  double* hout[5] = {ex, ey, ez, pot, work};
   // with overwrite_results the old values are not uploaded: the walk adds to zeros
   const int nin = c->prm.overwrite_results ? 3 : 8;
+  const bool chunked = nt >= kChunkedTargets && !keys_used && c->prm.walk != PEPCG_WALK_PER_TILE &&
+                       !c->far_field && c->has_tree;
+  if (chunked) {
+    // three chunks, small ones first and last: the walk starts after 1/16 of
+    // the upload and only 1/16 of the download trails it
+    if (!copy_streams(c)) return PEPCG_ERR_CUDA;
+    const int nch = 3;
+    auto al = [](int64_t v) { return v & ~(int64_t)31; };
+    const int64_t bounds[nch + 1] = {0, al(nt / 16), al(nt - nt / 16), nt};
+    bool ok = true;
+    for (int k = 0; k < nch; ++k) {
+      const int64_t t0 = bounds[k], len = bounds[k + 1] - bounds[k];
+      for (int a = 0; a < nin && len > 0; ++a)
+        ok = ok && cuda_ok(c, cudaMemcpyAsync(b + a * nt + t0, hin[a] + t0, len * 8,
+                                              cudaMemcpyHostToDevice, c->h2d), "H2D");
+      ok = ok && cuda_ok(c, cudaEventRecord(c->ready[k], c->h2d), "event");
+    }
+    if (nin == 3)
+      ok = ok && cuda_ok(c, cudaMemsetAsync(b + 3 * nt, 0, 5 * nt * 8, s), "clear results");
+    if (!ok) return drain_copies(c, false), PEPCG_ERR_CUDA;
+    ChunkPlan plan;
+    plan.nchunks = nch;
+    plan.bounds = bounds;
+    plan.ready = c->ready;
+    plan.done = c->done;
+    plan.before_sync = [&]() {
+      bool okd = true;
+      for (int k = 0; k < nch; ++k) {
+        const int64_t t0 = bounds[k], len = bounds[k + 1] - bounds[k];
+        okd = okd && cuda_ok(c, cudaStreamWaitEvent(c->d2h, c->done[k], 0), "chunk wait");
+        for (int r = 0; r < 5 && len > 0; ++r)
+          okd = okd && cuda_ok(c, cudaMemcpyAsync(hout[r] + t0, b + (3 + r) * nt + t0, len * 8,
+                                                  cudaMemcpyDeviceToHost, c->d2h), "D2H");
+      }
+      return okd;
+    };
+    int rc = traverse_device(c, nt, b, b + nt, b + 2 * nt, nullptr, false, b + 3 * nt,
+                             b + 4 * nt, b + 5 * nt, b + 6 * nt, b + 7 * nt, nullptr, &plan);
+    const bool drained = drain_copies(c, true);
+    if (rc && rc != PEPCG_WARN_NOT_NEUTRAL) return rc;
+    return drained ? rc : PEPCG_ERR_CUDA;
+  }
   bool ok = true;
   for (int k = 0; k < nin; ++k)
     ok = ok && cuda_ok(c, cudaMemcpyAsync(b + k * nt, hin[k], nt * 8, cudaMemcpyHostToDevice, s), "H2D");
   if (nin == 3)
     ok = ok && cuda_ok(c, cudaMemsetAsync(b + 3 * nt, 0, 5 * nt * 8, s), "clear results");
-  if (tkeys) ok = ok && cuda_ok(c, cudaMemcpyAsync(c->tkeys.p, tkeys, nt * 8, cudaMemcpyHostToDevice, s), "H2D");
+  if (keys_used)
+    ok = ok && cuda_ok(c, cudaMemcpyAsync(c->tkeys.p, tkeys, nt * 8, cudaMemcpyHostToDevice, s), "H2D");
   if (!ok) return PEPCG_ERR_CUDA;
   const double* tq =
-      c->prm.force_law == 5 ? grown_charges_if_same(c, nt, tkeys ? c->tkeys.p : nullptr) : nullptr;
-  int rc = traverse_device(c, nt, b, b + nt, b + 2 * nt, tkeys ? c->tkeys.p : nullptr, false,
+      c->prm.force_law == 5 ? grown_charges_if_same(c, nt, keys_used ? c->tkeys.p : nullptr) : nullptr;
+  int rc = traverse_device(c, nt, b, b + nt, b + 2 * nt, keys_used ? c->tkeys.p : nullptr, false,
                            b + 3 * nt, b + 4 * nt, b + 5 * nt, b + 6 * nt, b + 7 * nt, tq);
   if (rc && rc != PEPCG_WARN_NOT_NEUTRAL) return rc;
-  double* hout[5] = {ex, ey, ez, pot, work};
   for (int k = 0; k < 5; ++k)
     ok = ok && cuda_ok(c, cudaMemcpyAsync(hout[k], b + (3 + k) * nt, nt * 8, cudaMemcpyDeviceToHost, s), "D2H");
   ok = ok && cuda_ok(c, cudaStreamSynchronize(s), "traverse");

@@ -23,6 +23,7 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <functional>
 #include <string>
 
 #include "../../include/pepcg.h"
@@ -131,6 +132,13 @@ struct Ctx {
   cudaEvent_t ev[8];
   bool grow_times_pending = false;
 
+  // host-transfer overlap (the host-array entry points): one stream per copy
+  // direction and untimed events that order chunks across the streams;
+  // created on first use
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  static constexpr int kMaxChunks = 8;
+  cudaEvent_t ready[kMaxChunks] = {}, done[kMaxChunks] = {};
+
   int32_t* nleaves_ptr() { return nleaves.p; }
 };
 
@@ -157,9 +165,25 @@ void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp
 int host_tiles(Ctx* c, int64_t nt, const int64_t* d_tkeys, int T, int2* d_tiles, int64_t* ntiles);
 // tq: the targets' charges when they are grown particles (the Kelbg law needs
 // them), else nullptr
+//
+// plan (optional) splits the walk into consecutive target ranges so that host
+// transfers overlap it: chunk k is launched after the context stream waits on
+// ready[k] (when set), done[k] is recorded on the context stream after it, and
+// before_sync runs once every chunk is enqueued, before the call waits for
+// the walk.  Only the per-target and group walks without the periodic far
+// field are split (their per-target results do not depend on the split when
+// the interior bounds are multiples of 32).
+struct ChunkPlan {
+  int nchunks = 1;
+  const int64_t* bounds = nullptr;  // nchunks + 1 target offsets
+  const cudaEvent_t* ready = nullptr;
+  const cudaEvent_t* done = nullptr;
+  std::function<bool()> before_sync;
+};
 int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                     const int64_t* tkeys, bool self, double* ex, double* ey, double* ez,
-                    double* pot, double* work, const double* tq = nullptr);
+                    double* pot, double* work, const double* tq = nullptr,
+                    const ChunkPlan* plan = nullptr);
 
 // ---- adjoint.cu ----
 int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
@@ -183,7 +207,7 @@ int external_field_device(Ctx* c, int64_t n, double ez_ext, const double* z, dou
 int wrap_device(Ctx* c, int64_t n, double* x, double* y, double* z);
 int gather_device(Ctx* c, const double* in, double* out);
 int restore_device(Ctx* c, const double* in, double* out);
-int widen_perm_device(Ctx* c, int64_t* out);
+int widen_perm_device(Ctx* c, int64_t* out, cudaStream_t st = nullptr);  // null: c->stream
 int lattice_add(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                 double* ex, double* ey, double* ez, double* pot, bool overwrite);
 

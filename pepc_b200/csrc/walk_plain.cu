@@ -315,7 +315,7 @@ int prepare_mac(Ctx* c, const double** macb) {
 
 int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                     const int64_t* tkeys, bool self, double* ex, double* ey, double* ez,
-                    double* pot, double* work, const double* tq) {
+                    double* pot, double* work, const double* tq, const ChunkPlan* plan) {
   if (!c->has_tree) {
     c->err = "traverse called without a grown tree";
     return PEPCG_ERR_NO_TREE;
@@ -365,10 +365,18 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
       if (rc) return rc;
     }
   }
-  cudaEventRecord(c->ev[5], s);
+  const int nchunks = plan ? plan->nchunks : 1;
+  if (nchunks > 1) {
+    bool ok = walk != PEPCG_WALK_PER_TILE && !c->far_field && nchunks <= Ctx::kMaxChunks &&
+              plan->bounds[0] == 0 && plan->bounds[nchunks] == nt;
+    for (int k = 1; ok && k < nchunks; ++k)
+      ok = plan->bounds[k] % 32 == 0 && plan->bounds[k] >= plan->bounds[k - 1];
+    if (!ok) {
+      c->err = "traverse: invalid chunk plan";
+      return PEPCG_ERR_BAD_ARG;
+    }
+  }
   WalkArgs A;
-  A.nt = nt;
-  A.tx = tx; A.ty = ty; A.tz = tz;
   A.nc4 = c->nc4.p;
   A.meta = c->meta.p;
   A.fwd = c->fwd.p;
@@ -385,45 +393,58 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
   A.eps2 = c->prm.eps2;
   A.M = (int32_t)c->nnodes;
   A.npart = c->n;
-  A.ex = ex; A.ey = ey; A.ez = ez; A.pot = pot; A.work = work;
   A.counters = c->counters.p;
   A.status = c->d_status;
   A.tiles = reinterpret_cast<const int2*>(c->tiles.p);
   A.ntiles = ntiles;
-  A.tq = tq;
   A.kinv = c->prm.kelbg_invsqrttemp;
   A.sqrtpi = std::sqrt(std::acos(-1.0));
-  COUNT_LAUNCH();
-  k_reset_counter<<<1, 1, 0, s>>>();
   const int blocks = 148 * 8;
-  if (c->prm.precision == PEPCG_PRECISION_PLAIN) {
-    COUNT_LAUNCH();
-    const int law = c->prm.force_law;
-    if (walk == PEPCG_WALK_PER_TARGET) {
-      if (law == 2) k_walk_target64<2><<<blocks, kWalkThreads, 0, s>>>(A);
-      else if (law == 4) k_walk_target64<4><<<blocks, kWalkThreads, 0, s>>>(A);
-      else if (law == 5) k_walk_target64<5><<<blocks, kWalkThreads, 0, s>>>(A);
-      else k_walk_target64<3><<<blocks, kWalkThreads, 0, s>>>(A);
-    } else {
-      if (walk == PEPCG_WALK_GROUP) A.tiles = nullptr;
-      if (law == 2) k_walk_tile64<2><<<blocks, kWalkThreads, 0, s>>>(A);
-      else if (law == 4) k_walk_tile64<4><<<blocks, kWalkThreads, 0, s>>>(A);
-      else if (law == 5) k_walk_tile64<5><<<blocks, kWalkThreads, 0, s>>>(A);
-      else k_walk_tile64<3><<<blocks, kWalkThreads, 0, s>>>(A);
+  for (int k = 0; k < nchunks; ++k) {
+    const int64_t t0 = nchunks > 1 ? plan->bounds[k] : 0;
+    const int64_t t1 = nchunks > 1 ? plan->bounds[k + 1] : nt;
+    if (plan && plan->ready && !cuda_ok(c, cudaStreamWaitEvent(s, plan->ready[k], 0), "chunk wait"))
+      return PEPCG_ERR_CUDA;
+    if (k == 0) cudaEventRecord(c->ev[5], s);
+    if (t1 > t0) {
+      A.nt = t1 - t0;
+      A.tx = tx + t0; A.ty = ty + t0; A.tz = tz + t0;
+      A.ex = ex + t0; A.ey = ey + t0; A.ez = ez + t0; A.pot = pot + t0; A.work = work + t0;
+      A.tq = tq ? tq + t0 : nullptr;
+      COUNT_LAUNCH();
+      k_reset_counter<<<1, 1, 0, s>>>();
+      if (c->prm.precision == PEPCG_PRECISION_PLAIN) {
+        COUNT_LAUNCH();
+        const int law = c->prm.force_law;
+        if (walk == PEPCG_WALK_PER_TARGET) {
+          if (law == 2) k_walk_target64<2><<<blocks, kWalkThreads, 0, s>>>(A);
+          else if (law == 4) k_walk_target64<4><<<blocks, kWalkThreads, 0, s>>>(A);
+          else if (law == 5) k_walk_target64<5><<<blocks, kWalkThreads, 0, s>>>(A);
+          else k_walk_target64<3><<<blocks, kWalkThreads, 0, s>>>(A);
+        } else {
+          if (walk == PEPCG_WALK_GROUP) A.tiles = nullptr;
+          if (law == 2) k_walk_tile64<2><<<blocks, kWalkThreads, 0, s>>>(A);
+          else if (law == 4) k_walk_tile64<4><<<blocks, kWalkThreads, 0, s>>>(A);
+          else if (law == 5) k_walk_tile64<5><<<blocks, kWalkThreads, 0, s>>>(A);
+          else k_walk_tile64<3><<<blocks, kWalkThreads, 0, s>>>(A);
+        }
+      } else {
+        int rc = launch_walk_mixed(c, t1 - t0, A.tx, A.ty, A.tz, A.ex, A.ey, A.ez, A.pot, A.work,
+                                   walk == PEPCG_WALK_PER_TILE ? A.tiles : nullptr, ntiles,
+                                   walk == PEPCG_WALK_PER_TARGET);
+        if (rc) return rc;
+      }
+      if (!cuda_ok(c, cudaGetLastError(), "walk launch")) return PEPCG_ERR_CUDA;
     }
-  } else {
-    int rc = launch_walk_mixed(c, nt, tx, ty, tz, ex, ey, ez, pot, work,
-                               walk == PEPCG_WALK_PER_TILE ? A.tiles : nullptr, ntiles,
-                               walk == PEPCG_WALK_PER_TARGET);
-    if (rc) return rc;
+    if (plan && plan->done) cudaEventRecord(plan->done[k], s);
   }
-  if (!cuda_ok(c, cudaGetLastError(), "walk launch")) return PEPCG_ERR_CUDA;
   cudaEventRecord(c->ev[6], s);
   if (c->far_field) {
     int rc = lattice_add(c, nt, tx, ty, tz, ex, ey, ez, pot, false);
     if (rc) return rc;
   }
   cudaEventRecord(c->ev[7], s);
+  if (plan && plan->before_sync && !plan->before_sync()) return PEPCG_ERR_CUDA;
   unsigned long long ctr[4];
   uint32_t st = 0;
   if (!cuda_ok(c, cudaMemcpyAsync(ctr, c->counters.p, 4 * sizeof(unsigned long long),
