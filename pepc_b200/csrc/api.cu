@@ -335,14 +335,14 @@ int pepcg_destroy(void* ctx) {
   release(c->x); release(c->y); release(c->z); release(c->q);
   release(c->key); release(c->perm);
   release(c->in_x); release(c->in_y); release(c->in_z); release(c->in_q);
-  release(c->skey); release(c->skey_alt); release(c->sval); release(c->sval_alt);
+  release(c->packed); release(c->skey); release(c->skey_alt); release(c->sval); release(c->sval_alt);
   release(c->hist); release(c->orig_key); release(c->dup_list);
   release(c->lev); release(c->lcpn);
   release(c->cstart); release(c->cend); release(c->sstart); release(c->send);
   release(c->scan_tmp);
   release(c->nc4); release(c->meta); release(c->fwd); release(c->mom); release(c->aux);
   release(c->mom32);
-  release(c->parent); release(c->nchild); release(c->twiglist); release(c->lvlcnt); release(c->macb); release(c->first_part);
+  release(c->parent); release(c->nchild); release(c->twiglist); release(c->lvlcnt); release(c->lvlblk); release(c->macb); release(c->first_part);
   release(c->nleaves); release(c->child8); release(c->wstack); release(c->leafnode);
   release(c->adj); release(c->fpo2rpo); release(c->rpo2fpo); release(c->nkey);
   release(c->tiles); release(c->counters); release(c->tgt); release(c->tkeys);

@@ -156,24 +156,46 @@ struct HilbertTable {
   uint16_t e[48 * 8];  // digit | next_state << 3
 };
 
+// int((v - lo) / s), coord_to_intcoord_with_refinement_length
+// (module_spacefilling.f90:218).  The quotient is formed by multiplying with
+// the rounded reciprocal rs wherever that cannot change the integer part: the
+// product p is within 1.5 * 2^-52 * p of the correctly rounded quotient, so
+// their floors agree unless an integer lies within that distance of p; the
+// test below leaves a margin (2^-50 * p) and otherwise divides.  The
+// difference v - lo is positive (the box has a margin), so the floor is the
+// truncation.
+__device__ __forceinline__ int64_t quantise(double v, double lo, double s, double rs) {
+  const double d = v - lo;
+  const double p = d * rs;
+  const double f = floor(p);
+  const double tol = p * 0x1p-50;
+  if (p >= 0.0 && p - f > tol && (f + 1.0) - p > tol) return (int64_t)f;
+  return __double2ll_rz(d / s);
+}
+
 __global__ void k_keys(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
-                       const double* __restrict__ z, const double* __restrict__ box, int curve,
-                       HilbertTable tab, uint64_t* __restrict__ keys, int32_t* __restrict__ idx) {
-  __shared__ double sb[6];
+                       const double* __restrict__ z, const double* __restrict__ q,
+                       const double* __restrict__ box, int curve, HilbertTable tab,
+                       uint64_t* __restrict__ keys, int32_t* __restrict__ idx,
+                       double4* __restrict__ packed) {
+  __shared__ double sb[9];
   __shared__ uint16_t st[48 * 8];
   if (threadIdx.x < 3) {
     sb[threadIdx.x] = box[threadIdx.x];
     // s = boxsize / 2**maxlevel (module_spacefilling.f90:238), exact
     sb[3 + threadIdx.x] = box[6 + threadIdx.x] / 1048576.0;
+    sb[6 + threadIdx.x] = 1.0 / sb[3 + threadIdx.x];
   }
   for (int i = threadIdx.x; i < 48 * 8; i += blockDim.x) st[i] = tab.e[i];
   __syncthreads();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    // coord_to_intcoord_with_refinement_length (:218): int() truncates
-    const int64_t i0 = __double2ll_rz((x[i] - sb[0]) / sb[3]);
-    const int64_t i1 = __double2ll_rz((y[i] - sb[1]) / sb[4]);
-    const int64_t i2 = __double2ll_rz((z[i] - sb[2]) / sb[5]);
+    const double xi = x[i], yi = y[i], zi = z[i];
+    // the particle, packed in input order for the permutation's gather
+    packed[i] = make_double4(xi, yi, zi, q[i]);
+    const int64_t i0 = quantise(xi, sb[0], sb[3], sb[6]);
+    const int64_t i1 = quantise(yi, sb[1], sb[4], sb[7]);
+    const int64_t i2 = quantise(zi, sb[2], sb[5], sb[8]);
     uint64_t key;
     if (curve == PEPCG_CURVE_MORTON) {
       key = morton3d(i0, i1, i2);
@@ -220,54 +242,118 @@ __global__ void k_sort_hist(int64_t n, const uint64_t* __restrict__ keys, int sh
   hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
-__global__ void k_sort_scatter(int64_t n, const uint64_t* __restrict__ kin,
-                               const int32_t* __restrict__ vin, uint64_t* __restrict__ kout,
-                               int32_t* __restrict__ vout, int shift,
-                               const uint32_t* __restrict__ offs, int nblocks) {
-  __shared__ uint32_t running[256];
-  __shared__ uint32_t wcnt[kThreads / 32][257];
+// Stable scatter of one 4096-key tile.  Warp w owns the tile's keys
+// [512 w, 512 w + 512) and reads them in one round (16 per lane, coalesced);
+// it ranks them among themselves by digit, in order (warp match, the digit's
+// running count in shared memory, updated by the peers' leader), with no
+// block barrier; the per-digit counts are then prefixed over the warps, which
+// keeps the ranks stable, and over the digits, which gives each digit's run
+// in the tile.  The tile is sorted by digit in shared memory and written out
+// in that order, so that consecutive threads store consecutive addresses of a
+// digit's run in the output (the run of digit d of tile b starts at
+// offs[d * nblocks + b]).
+constexpr int kWarpsSort = kThreads / 32;
+constexpr int kPerWarp = kSortChunk / kWarpsSort;  // 512 keys
+constexpr int kScatterSmem = kSortChunk * 8 + kSortChunk * 4 + 2 * 256 * 4 + kWarpsSort * 256 * 4;
+
+__global__ void __launch_bounds__(kThreads) k_sort_scatter(int64_t n, const uint64_t* __restrict__ kin,
+                                                           const int32_t* __restrict__ vin,
+                                                           uint64_t* __restrict__ kout,
+                                                           int32_t* __restrict__ vout, int shift,
+                                                           const uint32_t* __restrict__ offs,
+                                                           int nblocks) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint64_t* sk = reinterpret_cast<uint64_t*>(smem);
+  int32_t* sv = reinterpret_cast<int32_t*>(sk + kSortChunk);
+  uint32_t* lstart = reinterpret_cast<uint32_t*>(sv + kSortChunk);  // tile-local run starts
+  uint32_t* gbase = lstart + 256;                                   // output run starts
+  uint32_t(*wcnt)[256] = reinterpret_cast<uint32_t(*)[256]>(gbase + 256);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  running[threadIdx.x] = offs[(int64_t)threadIdx.x * nblocks + blockIdx.x];
-  for (int w = 0; w < kThreads / 32; ++w) wcnt[w][threadIdx.x] = 0;
-  if (threadIdx.x < kThreads / 32) wcnt[threadIdx.x][256] = 0;
-  __syncthreads();
   const unsigned lt = (1u << lane) - 1u;
-  int64_t base = (int64_t)blockIdx.x * kSortChunk;
-  for (int r = 0; r < kSortRows; ++r) {
-    int64_t i = base + r * kThreads + threadIdx.x;
-    bool valid = i < n;
-    uint64_t k = valid ? kin[i] : 0;
-    int32_t v = valid ? vin[i] : 0;
-    int d = valid ? (int)((k >> shift) & 255u) : 256;
-    unsigned peers = __match_any_sync(0xffffffffu, d);
-    int lrank = __popc(peers & lt);
-    int leader = __ffs(peers) - 1;
-    if (lane == leader) wcnt[warp][d] = __popc(peers);
-    __syncthreads();
-    {  // exclusive prefix over warps for digit threadIdx.x
-      int b = threadIdx.x;
-      uint32_t run = running[b];
+  const int64_t base = (int64_t)blockIdx.x * kSortChunk;
+  const int cnt = (int)min((int64_t)kSortChunk, n - base);
+  gbase[threadIdx.x] = offs[(int64_t)threadIdx.x * nblocks + blockIdx.x];
+  for (int w = 0; w < kWarpsSort; ++w) wcnt[w][threadIdx.x] = 0;
+  uint64_t kr[kPerWarp / 32];
+  int32_t vr[kPerWarp / 32];
 #pragma unroll
-      for (int w = 0; w < kThreads / 32; ++w) {
-        uint32_t t = wcnt[w][b];
-        wcnt[w][b] = run;
-        run += t;
-      }
-      running[b] = run;
-    }
-    __syncthreads();
-    if (valid) {
-      uint32_t dst = wcnt[warp][d] + lrank;
-      kout[dst] = k;
-      vout[dst] = v;
-    }
-    __syncthreads();
-    if (lane == leader) wcnt[warp][d] = 0;
-    // wcnt of digits not present in this warp were overwritten by the prefix
-    // pass; clear the whole row owned by this thread's digit for the next row
-    for (int w = 0; w < kThreads / 32; ++w) wcnt[w][threadIdx.x] = 0;
-    __syncthreads();
+  for (int j = 0; j < kPerWarp / 32; ++j) {
+    const int i = warp * kPerWarp + j * 32 + lane;
+    kr[j] = i < cnt ? kin[base + i] : 0;
+    vr[j] = i < cnt ? vin[base + i] : 0;
   }
+  __syncthreads();
+  int rk[kPerWarp / 32];
+  uint32_t* my = wcnt[warp];
+#pragma unroll
+  for (int j = 0; j < kPerWarp / 32; ++j) {
+    const bool valid = warp * kPerWarp + j * 32 + lane < cnt;
+    const int d = (int)((kr[j] >> shift) & 255u);
+    const unsigned peers = __match_any_sync(0xffffffffu, valid ? d : 256);
+    const int leader = __ffs(peers) - 1;
+    uint32_t c0 = 0;
+    if (valid && lane == leader) c0 = my[d];
+    c0 = __shfl_sync(0xffffffffu, c0, leader);
+    rk[j] = (int)c0 + __popc(peers & lt);
+    if (valid && lane == leader) my[d] = c0 + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  {  // digit threadIdx.x: prefix over the warps, then the tile's run starts
+    const int b = threadIdx.x;
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < kWarpsSort; ++w) {
+      const uint32_t t = wcnt[w][b];
+      wcnt[w][b] = run;
+      run += t;
+    }
+    uint32_t x = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    __shared__ uint32_t wtot[kWarpsSort];
+    if (lane == 31) wtot[warp] = x;
+    __syncthreads();
+    uint32_t pre = 0;
+    for (int w = 0; w < warp; ++w) pre += wtot[w];
+    lstart[b] = pre + x - run;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < kPerWarp / 32; ++j) {
+    if (warp * kPerWarp + j * 32 + lane < cnt) {
+      const int d = (int)((kr[j] >> shift) & 255u);
+      const int pos = (int)(lstart[d] + wcnt[warp][d]) + rk[j];
+      sk[pos] = kr[j];
+      sv[pos] = vr[j];
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < cnt; i += kThreads) {
+    const uint64_t k = sk[i];
+    const int d = (int)((k >> shift) & 255u);
+    const uint32_t dst = gbase[d] + (uint32_t)(i - (int)lstart[d]);
+    kout[dst] = k;
+    vout[dst] = sv[i];
+  }
+}
+
+// k_sort_scatter needs more than the default 48 KB of dynamic shared memory
+void sort_scatter(int64_t n, const uint64_t* kin, const int32_t* vin, uint64_t* kout,
+                  int32_t* vout, int shift, const uint32_t* offs, int nblocks, cudaStream_t s) {
+  static thread_local int configured_device = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (configured_device != dev) {
+    cudaFuncSetAttribute(k_sort_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, kScatterSmem);
+    configured_device = dev;
+  }
+  COUNT_LAUNCH();
+  k_sort_scatter<<<nblocks, kThreads, kScatterSmem, s>>>(n, kin, vin, kout, vout, shift, offs,
+                                                          nblocks);
 }
 
 // ---------------------------------------------------------------------------
@@ -368,22 +454,24 @@ void exclusive_scan(const T* in, T* out, int64_t n, T* tmp, cudaStream_t s) {
 // ---------------------------------------------------------------------------
 // Permute the payload into key order, flag duplicates (module_domains.f90:199-234)
 // ---------------------------------------------------------------------------
+// Particles into key order: one 32-byte gather per particle from the packed
+// copy that k_keys wrote.
 __global__ void k_permute(int64_t n, const uint64_t* __restrict__ skey,
-                          const int32_t* __restrict__ sval, const double* __restrict__ x,
-                          const double* __restrict__ y, const double* __restrict__ z,
-                          const double* __restrict__ q, double* __restrict__ xo,
-                          double* __restrict__ yo, double* __restrict__ zo,
-                          double* __restrict__ qo, int64_t* __restrict__ ko,
-                          int64_t* __restrict__ korig, int32_t* __restrict__ perm,
-                          unsigned long long* dupcount, int32_t* duplist, int dupcap) {
+                          const int32_t* __restrict__ sval, const double4* __restrict__ packed,
+                          double* __restrict__ xo, double* __restrict__ yo,
+                          double* __restrict__ zo, double* __restrict__ qo,
+                          int64_t* __restrict__ ko, int64_t* __restrict__ korig,
+                          int32_t* __restrict__ perm, unsigned long long* dupcount,
+                          int32_t* duplist, int dupcap) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     int32_t j = sval[i];
     uint64_t k = skey[i];
-    xo[i] = x[j];
-    yo[i] = y[j];
-    zo[i] = z[j];
-    qo[i] = q[j];
+    const double4 p = packed[j];
+    xo[i] = p.x;
+    yo[i] = p.y;
+    zo[i] = p.z;
+    qo[i] = p.w;
     ko[i] = (int64_t)k;
     korig[i] = (int64_t)k;
     perm[i] = j;
@@ -632,189 +720,193 @@ __global__ void k_link(int64_t M, const int2* __restrict__ meta,
 }
 
 // Twigs grouped by level for the upward pass and the adjoint's downward pass.
-// lvl[0..31] counts the twigs of each level (k_node_counts), lvl[32..63] are
-// fill counters; twiglist holds, level after level, the RPO indices of that
-// level's twigs (in no particular order).
+// lvl[0..20] counts the twigs of each level (k_node_counts); twiglist holds,
+// level after level, the RPO indices of that level's twigs in increasing
+// order, so that neighbouring threads of a level's launch read neighbouring
+// subtrees.  Built from per-block counts of each level's twigs, an exclusive
+// scan over (level, block) in level-major order -- level L then starts after
+// all twigs above it, level_base below -- and a stable scatter.
 __device__ __forceinline__ int level_base(const int32_t* lvl, int level) {
   int b = 0;
   for (int l = 0; l < level; ++l) b += lvl[l];
   return b;
 }
 
-__global__ void __launch_bounds__(256) k_level_scatter(int64_t M, const int2* __restrict__ meta,
-                                                       int32_t* __restrict__ lvl,
-                                                       int32_t* __restrict__ twiglist) {
-  __shared__ int h[kMaxLevel + 1], base[kMaxLevel + 1];
+__global__ void __launch_bounds__(256) k_level_count(int64_t M, const int2* __restrict__ meta,
+                                                     int32_t* __restrict__ bcnt, int nblk) {
+  __shared__ int h[kMaxLevel + 1];
   if (threadIdx.x <= kMaxLevel) h[threadIdx.x] = 0;
   __syncthreads();
   const int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  int L = -1, local = 0;
   if (u < M) {
     const int2 mu = meta[u];
-    if (!(mu.y & kLeafFlag)) {
-      L = mu.y & 0xff;
-      local = atomicAdd(&h[L], 1);
+    if (!(mu.y & kLeafFlag)) atomicAdd(&h[mu.y & 0xff], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x <= kMaxLevel) bcnt[(int64_t)threadIdx.x * nblk + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(256) k_level_scatter(int64_t M, const int2* __restrict__ meta,
+                                                       const int32_t* __restrict__ bofs, int nblk,
+                                                       int32_t* __restrict__ twiglist) {
+  __shared__ int wc[256 / 32][kMaxLevel + 1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x < (256 / 32) * (kMaxLevel + 1)) (&wc[0][0])[threadIdx.x] = 0;
+  const int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int L = -1;
+  if (u < M) {
+    const int2 mu = meta[u];
+    if (!(mu.y & kLeafFlag)) L = mu.y & 0xff;
+  }
+  const unsigned peers = __match_any_sync(0xffffffffu, L);
+  const int lrank = __popc(peers & ((1u << lane) - 1u));
+  __syncthreads();
+  if (L >= 0 && lane == __ffs(peers) - 1) wc[warp][L] = __popc(peers);
+  __syncthreads();
+  if (threadIdx.x <= kMaxLevel) {  // exclusive prefix over the warps, level threadIdx.x
+    int run = 0;
+    for (int w = 0; w < 256 / 32; ++w) {
+      const int t = wc[w][threadIdx.x];
+      wc[w][threadIdx.x] = run;
+      run += t;
     }
   }
   __syncthreads();
-  if (threadIdx.x <= kMaxLevel) {
-    const int l = threadIdx.x;
-    base[l] = h[l] ? level_base(lvl, l) + atomicAdd(&lvl[32 + l], h[l]) : 0;
-  }
-  __syncthreads();
-  if (L >= 0) twiglist[base[L] + local] = (int32_t)u;
+  if (L >= 0) twiglist[bofs[(int64_t)L * nblk + blockIdx.x] + wc[warp][L] + lrank] = (int32_t)u;
 }
 
 // Upward pass: tree_node_update_from_children / shift_multipoles_up
 // (module_tree_grow.f90:762-821, coulomb/module_interaction_specific.f90:84-140),
-// level-synchronous: one launch per level, deepest first; one thread per twig
-// of that level computes it from its children in key order (child8 lists
-// them last to first, like the RPO chain).  No fences, no atomics; every child
-// of a level-L twig was finished by an earlier launch.  shift_up64's
-// additions in its order.  kPreload loads every child's centre, charge and
-// abs_charge in one round (for the small top levels, which are
-// latency-bound); otherwise each pass re-reads them from L1 (for the large
-// levels, which want occupancy).
-template <bool kPreload>
-__device__ __forceinline__ void upward_twig(int64_t u, const int2* __restrict__ meta,
-                                            const int4* __restrict__ child8,
-                                            const int32_t* __restrict__ nchild,
-                                            double4* __restrict__ nc4, double* __restrict__ mom,
-                                            double2* __restrict__ aux, float4* __restrict__ mom32) {
-  const int4 c0 = child8[2 * u], c1 = child8[2 * u + 1];
-  const int ch[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-  const int nc = min(8, nchild[u]);
-  double4 ca[8];
-  double2 cb[8];  // (abs_charge, bmax); a leaf's are (|q|, 0)
-  bool cl[8];
-  auto child = [&](int k, double4& a4, double2& b2, bool& leaf) {
-    if (kPreload) {
-      a4 = ca[k]; b2 = cb[k]; leaf = cl[k];
-    } else {
-      a4 = nc4[ch[k]];
-      leaf = (meta[ch[k]].y & kLeafFlag) != 0;
-      b2 = leaf ? make_double2(fabs(a4.w), 0.0) : aux[ch[k]];
-    }
-  };
-  if (kPreload) {
+// level-synchronous: one launch per level, deepest first; every child of a
+// level-L twig was finished by an earlier launch, so there are no fences and
+// no atomics.  One thread per twig; every sum runs over the children in key
+// order (child8 lists them last to first, like the RPO chain, so k runs
+// nc-1 .. 0) with the reference's operations in its order (no contraction:
+// this file is compiled with --fmad=false).
+//
+// Memory: a twig's children form its RPO subtree range in order, so child k
+// is a leaf exactly when the next child (or the subtree's end, for the last
+// one) starts right after it -- no load of the child's own record.  All child
+// data is then requested in one round: centres and charges (and the twig
+// children's abs_charge / bmax) into registers, the twig children's 9
+// moments into this thread's slice of shared memory by cp.async, which
+// costs no registers.  A twig thus waits for three memory latencies.
+constexpr int kUpThreads = 128;
+constexpr int kUpSmem = kUpThreads * 8 * 9 * 8;  // 9 moments of up to 8 children per thread
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+__global__ void __launch_bounds__(kUpThreads) k_upward_level(int level, const int32_t* __restrict__ lvl,
+                                                             const int32_t* __restrict__ twiglist,
+                                                             const int2* __restrict__ meta,
+                                                             const int4* __restrict__ child8,
+                                                             const int32_t* __restrict__ nchild,
+                                                             double4* __restrict__ nc4,
+                                                             double* __restrict__ mom,
+                                                             double2* __restrict__ aux,
+                                                             float4* __restrict__ mom32) {
+  extern __shared__ double s_up[];
+  double* sm = s_up + threadIdx.x * 72;
+  const int cnt = lvl[level];
+  const int32_t* list = twiglist + level_base(lvl, level);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+    const int64_t u = list[i];
+    const int4 c0 = child8[2 * u], c1 = child8[2 * u + 1];
+    const int nc = min(8, nchild[u]);
+    const int end = meta[u].x;
+    const int ch[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+    bool lf[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) lf[k] = k < nc && (k + 1 < nc ? ch[k + 1] : end) == ch[k] + 1;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (k < nc && !lf[k]) {
+        const double* src = mom + 9 * (int64_t)ch[k];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) cp_async8(sm + 9 * k + j, src + j);
+      }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    double4 ca[8];
+    double2 cb[8];  // (abs_charge, bmax); a leaf's are (|q|, 0)
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       if (k < nc) {
         ca[k] = nc4[ch[k]];
-        cl[k] = (meta[ch[k]].y & kLeafFlag) != 0;
-        cb[k] = cl[k] ? make_double2(fabs(ca[k].w), 0.0) : aux[ch[k]];
+        cb[k] = lf[k] ? make_double2(fabs(ca[k].w), 0.0) : aux[ch[k]];
       }
     }
-  }
-  // every sum runs over the children in key order (k = nc-1 .. 0)
-  double charge = 0.0, absq = 0.0;
+    double charge = 0.0, absq = 0.0;
 #pragma unroll
-  for (int k = 7; k >= 0; --k) {
-    if (k < nc) {
-      double4 a4; double2 b2; bool lf;
-      child(k, a4, b2, lf);
-      charge = charge + a4.w;
-    }
-  }
+    for (int k = 7; k >= 0; --k)
+      if (k < nc) charge = charge + ca[k].w;
 #pragma unroll
-  for (int k = 7; k >= 0; --k) {
-    if (k < nc) {
-      double4 a4; double2 b2; bool lf;
-      child(k, a4, b2, lf);
-      absq = absq + b2.x;
+    for (int k = 7; k >= 0; --k)
+      if (k < nc) absq = absq + cb[k].x;
+    double cx = 0.0, cy = 0.0, cz = 0.0;
+    if (absq != 0.0) {
+#pragma unroll
+      for (int k = 7; k >= 0; --k) {
+        if (k < nc) {
+          cx = cx + ca[k].x * cb[k].x;
+          cy = cy + ca[k].y * cb[k].x;
+          cz = cz + ca[k].z * cb[k].x;
+        }
+      }
+      cx = cx / absq;
+      cy = cy / absq;
+      cz = cz / absq;
+    } else {
+#pragma unroll
+      for (int k = 7; k >= 0; --k) {
+        if (k < nc) {
+          cx = cx + ca[k].x;
+          cy = cy + ca[k].y;
+          cz = cz + ca[k].z;
+        }
+      }
+      cx = cx / (double)nc;
+      cy = cy / (double)nc;
+      cz = cz / (double)nc;
     }
-  }
-  double cx = 0.0, cy = 0.0, cz = 0.0;
-  if (absq != 0.0) {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    double d0 = 0, d1 = 0, d2 = 0, q0 = 0, q1 = 0, q2 = 0, xy = 0, yz = 0, zx = 0;
+    double bmax = 0.0;
 #pragma unroll
     for (int k = 7; k >= 0; --k) {
       if (k < nc) {
-        double4 a4; double2 b2; bool lf;
-        child(k, a4, b2, lf);
-        cx = cx + a4.x * b2.x;
-        cy = cy + a4.y * b2.x;
-        cz = cz + a4.z * b2.x;
+        double m[9];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) m[j] = lf[k] ? 0.0 : sm[9 * k + j];
+        const double s0 = cx - ca[k].x, s1 = cy - ca[k].y, s2 = cz - ca[k].z;
+        const double q = ca[k].w;
+        d0 = (d0 + m[0]) + q * s0;
+        d1 = (d1 + m[1]) + q * s1;
+        d2 = (d2 + m[2]) + q * s2;
+        q0 = ((q0 + m[3]) + m[0] * s0) + (0.5 * q) * (s0 * s0);
+        q1 = ((q1 + m[4]) + m[1] * s1) + (0.5 * q) * (s1 * s1);
+        q2 = ((q2 + m[5]) + m[2] * s2) + (0.5 * q) * (s2 * s2);
+        xy = (((xy + m[6]) + m[0] * s1) + m[1] * s0) + (q * s0) * s1;
+        yz = (((yz + m[7]) + m[1] * s2) + m[2] * s1) + (q * s1) * s2;
+        zx = (((zx + m[8]) + m[2] * s0) + m[0] * s2) + (q * s2) * s0;
+        const double v = sqrt((s0 * s0 + s1 * s1) + s2 * s2) + cb[k].y;
+        if (k == nc - 1 || v > bmax) bmax = v;
       }
     }
-    cx = cx / absq;
-    cy = cy / absq;
-    cz = cz / absq;
-  } else {
-#pragma unroll
-    for (int k = 7; k >= 0; --k) {
-      if (k < nc) {
-        double4 a4; double2 b2; bool lf;
-        child(k, a4, b2, lf);
-        cx = cx + a4.x;
-        cy = cy + a4.y;
-        cz = cz + a4.z;
-      }
-    }
-    cx = cx / (double)nc;
-    cy = cy / (double)nc;
-    cz = cz / (double)nc;
+    nc4[u] = make_double4(cx, cy, cz, charge);
+    aux[u] = make_double2(absq, bmax);
+    double* o = mom + 9 * u;
+    o[0] = d0; o[1] = d1; o[2] = d2; o[3] = q0; o[4] = q1; o[5] = q2; o[6] = xy; o[7] = yz; o[8] = zx;
+    // FP32 copy for the mixed walk, the quadrupole matrix M (off-diagonals
+    // halved) scaled by 3: (px, py, pz, 3qxx), (3qyy, 3qzz, 1.5qxy, 1.5qyz),
+    // (1.5qzx, qxx+qyy+qzz, charge, 0)
+    mom32[3 * u] = make_float4((float)d0, (float)d1, (float)d2, (float)(3.0 * q0));
+    mom32[3 * u + 1] =
+        make_float4((float)(3.0 * q1), (float)(3.0 * q2), (float)(1.5 * xy), (float)(1.5 * yz));
+    mom32[3 * u + 2] = make_float4((float)(1.5 * zx), (float)((q0 + q1) + q2), (float)charge, 0.f);
   }
-  double d0 = 0, d1 = 0, d2 = 0, q0 = 0, q1 = 0, q2 = 0, xy = 0, yz = 0, zx = 0;
-#pragma unroll
-  for (int k = 7; k >= 0; --k) {
-    if (k < nc) {
-      double4 a4; double2 b2; bool lf;
-      child(k, a4, b2, lf);
-      const int64_t c = ch[k];
-      double m[9];
-#pragma unroll
-      for (int j = 0; j < 9; ++j) m[j] = lf ? 0.0 : mom[9 * c + j];
-      const double s0 = cx - a4.x, s1 = cy - a4.y, s2 = cz - a4.z;
-      const double q = a4.w;
-      d0 = (d0 + m[0]) + q * s0;
-      d1 = (d1 + m[1]) + q * s1;
-      d2 = (d2 + m[2]) + q * s2;
-      q0 = ((q0 + m[3]) + m[0] * s0) + (0.5 * q) * (s0 * s0);
-      q1 = ((q1 + m[4]) + m[1] * s1) + (0.5 * q) * (s1 * s1);
-      q2 = ((q2 + m[5]) + m[2] * s2) + (0.5 * q) * (s2 * s2);
-      xy = (((xy + m[6]) + m[0] * s1) + m[1] * s0) + (q * s0) * s1;
-      yz = (((yz + m[7]) + m[1] * s2) + m[2] * s1) + (q * s1) * s2;
-      zx = (((zx + m[8]) + m[2] * s0) + m[0] * s2) + (q * s2) * s0;
-    }
-  }
-  double bmax = 0.0;
-#pragma unroll
-  for (int k = 7; k >= 0; --k) {
-    if (k < nc) {
-      double4 a4; double2 b2; bool lf;
-      child(k, a4, b2, lf);
-      const double e0 = cx - a4.x, e1 = cy - a4.y, e2 = cz - a4.z;
-      const double v = sqrt((e0 * e0 + e1 * e1) + e2 * e2) + b2.y;
-      if (k == nc - 1 || v > bmax) bmax = v;
-    }
-  }
-  nc4[u] = make_double4(cx, cy, cz, charge);
-  aux[u] = make_double2(absq, bmax);
-  double* o = mom + 9 * u;
-  o[0] = d0; o[1] = d1; o[2] = d2; o[3] = q0; o[4] = q1; o[5] = q2; o[6] = xy; o[7] = yz; o[8] = zx;
-  // FP32 copy for the mixed walk, the quadrupole matrix M (off-diagonals
-  // halved) scaled by 3: (px, py, pz, 3qxx), (3qyy, 3qzz, 1.5qxy, 1.5qyz),
-  // (1.5qzx, qxx+qyy+qzz, charge, 0)
-  mom32[3 * u] = make_float4((float)d0, (float)d1, (float)d2, (float)(3.0 * q0));
-  mom32[3 * u + 1] =
-      make_float4((float)(3.0 * q1), (float)(3.0 * q2), (float)(1.5 * xy), (float)(1.5 * yz));
-  mom32[3 * u + 2] = make_float4((float)(1.5 * zx), (float)((q0 + q1) + q2), (float)charge, 0.f);
-}
-
-template <bool kPreload>
-__global__ void __launch_bounds__(256) k_upward_level(int level, const int32_t* __restrict__ lvl,
-                                                      const int32_t* __restrict__ twiglist,
-                                                      const int2* __restrict__ meta,
-                                                      const int4* __restrict__ child8,
-                                                      const int32_t* __restrict__ nchild,
-                                                      double4* __restrict__ nc4,
-                                                      double* __restrict__ mom,
-                                                      double2* __restrict__ aux,
-                                                      float4* __restrict__ mom32) {
-  const int cnt = lvl[level];
-  const int32_t* list = twiglist + level_base(lvl, level);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x)
-    upward_twig<kPreload>(list[i], meta, child8, nchild, nc4, mom, aux, mom32);
 }
 
 // The reference's exchange / reverse rules (module_spacefilling.f90:389-438)
@@ -894,7 +986,8 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
       !ensure(c, c->lev, n, "lev") || !ensure(c, c->lcpn, n, "lcpn") ||
       !ensure(c, c->cstart, n, "cstart") || !ensure(c, c->cend, n, "cend") ||
       !ensure(c, c->sstart, n, "sstart") || !ensure(c, c->send, n, "send") ||
-      !ensure(c, c->leafnode, n, "leafnode") || !ensure(c, c->lvlcnt, 64, "lvlcnt"))
+      !ensure(c, c->leafnode, n, "leafnode") || !ensure(c, c->lvlcnt, 64, "lvlcnt") ||
+      !ensure(c, c->packed, n, "packed"))
     return PEPCG_ERR_OOM;
 
   if (!cuda_ok(c, cudaMemsetAsync(c->d_status, 0, sizeof(uint32_t), s), "memset status") ||
@@ -913,8 +1006,8 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
   // keys
   COUNT_LAUNCH();
   static const HilbertTable htab = hilbert_table();
-  k_keys<<<grid_for(n), kThreads, 0, s>>>(n, dx, dy, dz, c->d_box, c->prm.curve, htab, c->skey.p,
-                                          c->sval.p);
+  k_keys<<<grid_for(n), kThreads, 0, s>>>(n, dx, dy, dz, dq, c->d_box, c->prm.curve, htab,
+                                          c->skey.p, c->sval.p, c->packed.p);
   cudaEventRecord(c->ev[1], s);
   // sort: 8 LSD passes of 8 bits
   uint64_t* kin = c->skey.p;
@@ -928,14 +1021,13 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
     k_sort_hist<<<nb, kThreads, 0, s>>>(n, kin, shift, c->hist.p, nb);
     exclusive_scan<uint32_t>(c->hist.p, c->hist.p, 256 * (int64_t)nb,
                              reinterpret_cast<uint32_t*>(c->scan_tmp.p), s);
-    COUNT_LAUNCH();
-    k_sort_scatter<<<nb, kThreads, 0, s>>>(n, kin, vin, kout, vout, shift, c->hist.p, nb);
+    sort_scatter(n, kin, vin, kout, vout, shift, c->hist.p, nb, s);
     std::swap(kin, kout);
     std::swap(vin, vout);
   }
   // after an even number of passes the result is back in skey / sval
   COUNT_LAUNCH();
-  k_permute<<<grid_for(n), kThreads, 0, s>>>(n, kin, vin, dx, dy, dz, dq, c->x.p, c->y.p, c->z.p,
+  k_permute<<<grid_for(n), kThreads, 0, s>>>(n, kin, vin, c->packed.p, c->x.p, c->y.p, c->z.p,
                                              c->q.p, c->key.p, c->orig_key.p, c->perm.p,
                                              c->d_small, c->dup_list.p, dupcap);
   COUNT_LAUNCH();
@@ -1001,20 +1093,21 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
   {
     const unsigned gM = (unsigned)((M + kThreads - 1) / kThreads);
     COUNT_LAUNCH();
-    k_level_scatter<<<gM, kThreads, 0, s>>>(M, c->meta.p, c->lvlcnt.p, c->twiglist.p);
+    if (!ensure(c, c->lvlblk, (size_t)(kMaxLevel + 1) * gM, "level blocks")) return PEPCG_ERR_OOM;
+    k_level_count<<<gM, kThreads, 0, s>>>(M, c->meta.p, c->lvlblk.p, (int)gM);
+    exclusive_scan<int32_t>(c->lvlblk.p, c->lvlblk.p, (int64_t)(kMaxLevel + 1) * gM,
+                            c->scan_tmp.p, s);
+    COUNT_LAUNCH();
+    k_level_scatter<<<gM, kThreads, 0, s>>>(M, c->meta.p, c->lvlblk.p, (int)gM, c->twiglist.p);
+    cudaFuncSetAttribute(k_upward_level, cudaFuncAttributeMaxDynamicSharedMemorySize, kUpSmem);
     float4* m32 = reinterpret_cast<float4*>(c->mom32.p);
     for (int L = c->max_level - 1; L >= 0; --L) {
       const int64_t cnt = c->lvl_host[L];
       if (cnt <= 0) continue;
       COUNT_LAUNCH();
-      if (cnt < 148 * kThreads)  // under one thread per SM slot: latency-bound
-        k_upward_level<true><<<grid_for(cnt), kThreads, 0, s>>>(
-            L, c->lvlcnt.p, c->twiglist.p, c->meta.p, c->child8.p, c->nchild.p, c->nc4.p,
-            c->mom.p, c->aux.p, m32);
-      else
-        k_upward_level<false><<<grid_for(cnt), kThreads, 0, s>>>(
-            L, c->lvlcnt.p, c->twiglist.p, c->meta.p, c->child8.p, c->nchild.p, c->nc4.p,
-            c->mom.p, c->aux.p, m32);
+      k_upward_level<<<grid_for(cnt, kUpThreads), kUpThreads, kUpSmem, s>>>(
+          L, c->lvlcnt.p, c->twiglist.p, c->meta.p, c->child8.p, c->nchild.p, c->nc4.p, c->mom.p,
+          c->aux.p, m32);
     }
   }
   cudaEventRecord(c->ev[4], s);
@@ -1235,8 +1328,7 @@ extern "C" int pepcg_sort_keys_noalloc(int64_t n, const int64_t* d_keys_in, int6
     k_sort_hist<<<nb, kThreads, 0, s>>>(n, kin, shift, hist, nb);
     g_launches.fetch_add(3, std::memory_order_relaxed);
     exclusive_scan<uint32_t>(hist, hist, 256 * (int64_t)nb, tmp, s);
-    COUNT_LAUNCH();
-    k_sort_scatter<<<nb, kThreads, 0, s>>>(n, kin, vin, kout, vout, shift, hist, nb);
+    sort_scatter(n, kin, vin, kout, vout, shift, hist, nb, s);
     std::swap(kin, kout);
     std::swap(vin, vout);
   }

@@ -75,6 +75,7 @@ struct Ctx {
   DBuf<int32_t> perm;
   // grow scratch
   DBuf<double> in_x, in_y, in_z, in_q;  // staging for host inputs
+  DBuf<double4> packed;                 // (x, y, z, q) in input order, for the permutation
   DBuf<uint64_t> skey, skey_alt;
   DBuf<int32_t> sval, sval_alt;
   DBuf<uint32_t> hist;
@@ -92,7 +93,8 @@ struct Ctx {
   DBuf<float> mom32;  // 12 * nnodes (coc-relative moments in FP32, padded)
   DBuf<int32_t> parent, nchild, first_part, nleaves;
   DBuf<int32_t> twiglist;  // twig RPO indices grouped by level (upward and adjoint passes)
-  DBuf<int32_t> lvlcnt;    // [0, 32) twigs per level, [32, 64) fill counters
+  DBuf<int32_t> lvlcnt;    // [0, 32) twigs per level
+  DBuf<int32_t> lvlblk;    // twigs per (level, block of 256 nodes), then their exclusive scan
   DBuf<double> macb;       // per-twig MAC threshold for mac_select != 0
   int32_t lvl_host[kMaxLevel + 1] = {0};  // twigs per level of the grown tree
   DBuf<int4> child8;  // up to 8 children (RPO indices) per twig, as 2 x int4
