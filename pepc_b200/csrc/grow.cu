@@ -180,6 +180,7 @@ __global__ void k_keys(int64_t n, const double* __restrict__ x, const double* __
                        double4* __restrict__ packed) {
   __shared__ double sb[9];
   __shared__ uint16_t st[48 * 8];
+  __shared__ uint16_t st2[48 * 64];  // two levels per lookup: 6 key bits | next state << 6
   if (threadIdx.x < 3) {
     sb[threadIdx.x] = box[threadIdx.x];
     // s = boxsize / 2**maxlevel (module_spacefilling.f90:238), exact
@@ -187,6 +188,12 @@ __global__ void k_keys(int64_t n, const double* __restrict__ x, const double* __
     sb[6 + threadIdx.x] = 1.0 / sb[3 + threadIdx.x];
   }
   for (int i = threadIdx.x; i < 48 * 8; i += blockDim.x) st[i] = tab.e[i];
+  __syncthreads();
+  for (int t = threadIdx.x; t < 48 * 64; t += blockDim.x) {
+    const unsigned e1 = st[(t >> 6) * 8 + ((t >> 3) & 7)];
+    const unsigned e2 = st[(e1 >> 3) * 8 + (t & 7)];
+    st2[t] = (uint16_t)((((e1 & 7u) << 3) | (e2 & 7u)) | ((e2 >> 3) << 6));
+  }
   __syncthreads();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
@@ -200,19 +207,20 @@ __global__ void k_keys(int64_t n, const double* __restrict__ x, const double* __
     if (curve == PEPCG_CURVE_MORTON) {
       key = morton3d(i0, i1, i2);
     } else {
+      // levels 2p+1 and 2p per lookup, octants (z << 2 | y << 1 | x) of the
+      // upper level in bits 3..5 of the index
       const unsigned a = (unsigned)i0, b = (unsigned)i1, c = (unsigned)i2;
       unsigned state = 0;
-      unsigned hi = 1, lo = 0;  // key = hi:lo, placeholder bit first
-      uint64_t k = 1;
+      uint64_t k = 1;  // the placeholder bit
 #pragma unroll
-      for (int l = kMaxLevel - 1; l >= 0; --l) {
-        const unsigned o = (((c >> l) & 1u) << 2) | (((b >> l) & 1u) << 1) | ((a >> l) & 1u);
-        const unsigned ent = st[state * 8 + o];
-        k = (k << 3) | (ent & 7u);
-        state = ent >> 3;
+      for (int p = kMaxLevel / 2 - 1; p >= 0; --p) {
+        const unsigned ax = (a >> (2 * p)) & 3u, by = (b >> (2 * p)) & 3u, cz = (c >> (2 * p)) & 3u;
+        const unsigned o = ((cz & 2u) << 4) | ((by & 2u) << 3) | ((ax & 2u) << 2) |
+                           ((cz & 1u) << 2) | ((by & 1u) << 1) | (ax & 1u);
+        const unsigned ent = st2[state * 64 + o];
+        k = (k << 6) | (ent & 63u);
+        state = ent >> 6;
       }
-      (void)hi;
-      (void)lo;
       key = k;
     }
     keys[i] = key;
@@ -252,17 +260,24 @@ __global__ void k_sort_hist(int64_t n, const uint64_t* __restrict__ keys, int sh
 // in that order, so that consecutive threads store consecutive addresses of a
 // digit's run in the output (the run of digit d of tile b starts at
 // offs[d * nblocks + b]).
-constexpr int kWarpsSort = kThreads / 32;
-constexpr int kPerWarp = kSortChunk / kWarpsSort;  // 512 keys
+// barrier for the first 256 threads of the block only (the digit lanes)
+__device__ __forceinline__ void named_barrier_256() {
+  asm volatile("bar.sync 1, 256;\n" ::: "memory");
+}
+
+constexpr int kScatterThreads = 512;
+constexpr int kWarpsSort = kScatterThreads / 32;
+constexpr int kPerWarp = kSortChunk / kWarpsSort;  // 256 keys
 constexpr int kScatterSmem = kSortChunk * 8 + kSortChunk * 4 + 2 * 256 * 4 + kWarpsSort * 256 * 4;
 
-__global__ void __launch_bounds__(kThreads) k_sort_scatter(int64_t n, const uint64_t* __restrict__ kin,
+__global__ void __launch_bounds__(kScatterThreads, 2) k_sort_scatter(int64_t n, const uint64_t* __restrict__ kin,
                                                            const int32_t* __restrict__ vin,
                                                            uint64_t* __restrict__ kout,
                                                            int32_t* __restrict__ vout, int shift,
                                                            const uint32_t* __restrict__ offs,
                                                            int nblocks) {
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ uint32_t wtot[8];
   uint64_t* sk = reinterpret_cast<uint64_t*>(smem);
   int32_t* sv = reinterpret_cast<int32_t*>(sk + kSortChunk);
   uint32_t* lstart = reinterpret_cast<uint32_t*>(sv + kSortChunk);  // tile-local run starts
@@ -272,8 +287,8 @@ __global__ void __launch_bounds__(kThreads) k_sort_scatter(int64_t n, const uint
   const unsigned lt = (1u << lane) - 1u;
   const int64_t base = (int64_t)blockIdx.x * kSortChunk;
   const int cnt = (int)min((int64_t)kSortChunk, n - base);
-  gbase[threadIdx.x] = offs[(int64_t)threadIdx.x * nblocks + blockIdx.x];
-  for (int w = 0; w < kWarpsSort; ++w) wcnt[w][threadIdx.x] = 0;
+  if (threadIdx.x < 256) gbase[threadIdx.x] = offs[(int64_t)threadIdx.x * nblocks + blockIdx.x];
+  for (int i = threadIdx.x; i < kWarpsSort * 256; i += kScatterThreads) (&wcnt[0][0])[i] = 0;
   uint64_t kr[kPerWarp / 32];
   int32_t vr[kPerWarp / 32];
 #pragma unroll
@@ -299,7 +314,7 @@ __global__ void __launch_bounds__(kThreads) k_sort_scatter(int64_t n, const uint
     __syncwarp();
   }
   __syncthreads();
-  {  // digit threadIdx.x: prefix over the warps, then the tile's run starts
+  if (threadIdx.x < 256) {  // digit threadIdx.x: prefix over the warps, then the tile's run starts
     const int b = threadIdx.x;
     uint32_t run = 0;
 #pragma unroll
@@ -314,9 +329,8 @@ __global__ void __launch_bounds__(kThreads) k_sort_scatter(int64_t n, const uint
       const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
       if (lane >= o) x += y;
     }
-    __shared__ uint32_t wtot[kWarpsSort];
     if (lane == 31) wtot[warp] = x;
-    __syncthreads();
+    named_barrier_256();
     uint32_t pre = 0;
     for (int w = 0; w < warp; ++w) pre += wtot[w];
     lstart[b] = pre + x - run;
@@ -332,7 +346,7 @@ __global__ void __launch_bounds__(kThreads) k_sort_scatter(int64_t n, const uint
     }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < cnt; i += kThreads) {
+  for (int i = threadIdx.x; i < cnt; i += kScatterThreads) {
     const uint64_t k = sk[i];
     const int d = (int)((k >> shift) & 255u);
     const uint32_t dst = gbase[d] + (uint32_t)(i - (int)lstart[d]);
@@ -352,8 +366,8 @@ void sort_scatter(int64_t n, const uint64_t* kin, const int32_t* vin, uint64_t* 
     configured_device = dev;
   }
   COUNT_LAUNCH();
-  k_sort_scatter<<<nblocks, kThreads, kScatterSmem, s>>>(n, kin, vin, kout, vout, shift, offs,
-                                                          nblocks);
+  k_sort_scatter<<<nblocks, kScatterThreads, kScatterSmem, s>>>(n, kin, vin, kout, vout, shift,
+                                                                 offs, nblocks);
 }
 
 // ---------------------------------------------------------------------------
@@ -1006,7 +1020,7 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
   // keys
   COUNT_LAUNCH();
   static const HilbertTable htab = hilbert_table();
-  k_keys<<<grid_for(n), kThreads, 0, s>>>(n, dx, dy, dz, dq, c->d_box, c->prm.curve, htab,
+  k_keys<<<std::min(grid_for(n), 148u * 8u), kThreads, 0, s>>>(n, dx, dy, dz, dq, c->d_box, c->prm.curve, htab,
                                           c->skey.p, c->sval.p, c->packed.p);
   cudaEventRecord(c->ev[1], s);
   // sort: 8 LSD passes of 8 bits
