@@ -352,6 +352,67 @@ def run_madelung(args, P, torch, dev, stream):
     print(json.dumps(out_line), flush=True)
 
 
+def run_sharded(args, P, torch, dev, stream, dist, rank, world, local):
+    """Target sharding (strong scaling): every rank grows the same tree from the
+    same particles, walks its shard_range share of the key-ordered targets
+    (pepcg_traverse_range_device) and all-gathers the shares' fields
+    (gather_shards), so that every rank ends the step with all N fields.  The
+    step time is the slowest rank's; the job's rate is N per step."""
+    x, y, z, q = plummer(args.n)
+    n = args.n
+    tx, ty, tz, tq = (torch.from_numpy(a).to(dev) for a in (x, y, z, q))
+    t0, t1 = P.shard_range(n, rank, world)
+    share = torch.zeros((5, t1 - t0), dtype=torch.float64, device=dev)
+    walk = {"group": P.WALK_GROUP, "target": P.WALK_PER_TARGET, "tile": P.WALK_PER_TILE}[args.walk]
+    prec = P.PRECISION_MIXED if args.precision == "mixed" else P.PRECISION_PLAIN
+    tc = P.TreeCode(theta2=args.theta ** 2, eps2=args.eps ** 2, precision=prec, walk=walk,
+                    device=local)
+    tc.set_stream(stream.cuda_stream)
+    full = [None]
+
+    def step():
+        share.zero_()
+        tc.grow_tree_device(tx, ty, tz, tq)
+        tc.traverse_range_device(t0, t1, *share)
+        full[0] = P.gather_shards(share, n, rank, world)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = P.kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, dev)
+    launches = P.kernel_launches() - l0
+    # the gathered fields against one single-call traverse of all targets
+    ref = [torch.zeros(n, dtype=torch.float64, device=dev) for _ in range(5)]
+    tc.traverse_self_device(*ref)
+    torch.cuda.synchronize()
+    same = all(bool(torch.equal(full[0][k], ref[k])) for k in range(5))
+    tc.close()
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": n / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32 interactions + f64 offsets/sums" if args.precision == "mixed" else "f64",
+            "data": "synthetic",
+            "config": {"workload": workload_name(args), "precision": args.precision,
+                       "walk": args.walk,
+                       "parallelism": f"target shards over {world} ranks (replicated tree) "
+                                      "+ all-gather of the fields"},
+            "fields_equal_single_call": same, "gpu_launches": launches}), flush=True)
+
+
 def workload_name(args):
     return (f"Plummer sphere N={args.n} (a=1, r<=20, q=1/N), theta={args.theta}, "
             f"eps={args.eps}, quadrupole, Hilbert keys, open boundaries")
@@ -373,6 +434,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="target sharding across the ranks (strong scaling) instead of replicas")
     ap.add_argument("--workload", default="plummer", choices=["plummer", "explosion", "madelung"],
                     help="plummer: the headline line; explosion / madelung: the other "
                          "configurations, one descriptive JSON line each")
@@ -401,6 +464,15 @@ def main():
         stream = torch.cuda.Stream(device=dev)
         torch.cuda.set_stream(stream)
         (run_explosion if args.workload == "explosion" else run_madelung)(args, P, torch, dev, stream)
+        return
+
+    if args.shard:
+        dev = torch.device("cuda", local)
+        stream = torch.cuda.Stream(device=dev)
+        torch.cuda.set_stream(stream)
+        run_sharded(args, P, torch, dev, stream, dist, rank, world, local)
+        if dist:
+            dist.destroy_process_group()
         return
 
     x, y, z, q = plummer(args.n)

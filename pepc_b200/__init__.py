@@ -446,3 +446,32 @@ def shard_range(n, rank, world, align=32):
     b1 = blocks * (rank + 1) // world
     return min(n, b0 * align), min(n, b1 * align)
 
+
+def gather_shards(local, n, rank, world, align=32, group=None):
+    """The exchange of a target-sharded traverse: every rank's share of the
+    key-ordered fields (local: a (k, t1 - t0) tensor of this rank's
+    shard_range share, k fields) gathered on every rank as a (k, n) tensor.
+    The shares are padded to the largest one so that a single all-gather
+    moves them (all_gather_into_tensor over NCCL; a list all-gather where the
+    backend has no tensor form)."""
+    import torch
+    import torch.distributed as dist
+    sizes = [shard_range(n, r, world, align) for r in range(world)]
+    t0, t1 = sizes[rank]
+    if local.dim() != 2 or local.shape[1] != t1 - t0:
+        raise ValueError(f"rank {rank}: local share must be (k, {t1 - t0}), got {tuple(local.shape)}")
+    k = local.shape[0]
+    cap = max(b - a for a, b in sizes)
+    buf = torch.zeros((k, cap), dtype=local.dtype, device=local.device)
+    buf[:, : t1 - t0] = local
+    if world == 1:
+        return buf[:, :n].clone()
+    try:
+        flat = torch.empty((world, k, cap), dtype=local.dtype, device=local.device)
+        dist.all_gather_into_tensor(flat, buf, group=group)
+        parts = [flat[r] for r in range(world)]
+    except (RuntimeError, NotImplementedError):
+        parts = [torch.empty_like(buf) for _ in range(world)]
+        dist.all_gather(parts, buf, group=group)
+    return torch.cat([parts[r][:, : b - a] for r, (a, b) in enumerate(sizes)], dim=1)
+

@@ -241,11 +241,16 @@ __global__ void k_sort_hist(int64_t n, const uint64_t* __restrict__ keys, int sh
   __shared__ uint32_t h[256];
   h[threadIdx.x] = 0;
   __syncthreads();
-  int64_t base = (int64_t)blockIdx.x * kSortChunk;
+  const int64_t base = (int64_t)blockIdx.x * kSortChunk;
+  uint64_t kr[kSortRows];  // every row's key requested before the first count
+#pragma unroll
   for (int r = 0; r < kSortRows; ++r) {
-    int64_t i = base + r * kThreads + threadIdx.x;
-    if (i < n) atomicAdd(&h[(keys[i] >> shift) & 255u], 1u);
+    const int64_t i = base + r * kThreads + threadIdx.x;
+    kr[r] = i < n ? keys[i] : 0;
   }
+#pragma unroll
+  for (int r = 0; r < kSortRows; ++r)
+    if (base + r * kThreads + threadIdx.x < n) atomicAdd(&h[(kr[r] >> shift) & 255u], 1u);
   __syncthreads();
   hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }

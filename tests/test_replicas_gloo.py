@@ -78,3 +78,29 @@ def test_target_shares_cover_the_particles(n):
 
 def test_single_rank_needs_no_process_group():
     assert bench.max_over_ranks(7.0, None, torch.device("cpu")) == 7.0
+
+
+def _gather_worker(rank, world, port, n, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        t0, t1 = pepc_b200.shard_range(n, rank, world)
+        # the "fields" of a share: field f of target t is 10 f + t
+        local = torch.stack([10.0 * f + torch.arange(t0, t1, dtype=torch.float64)
+                             for f in range(5)])
+        full = pepc_b200.gather_shards(local, n, rank, world)
+        out[rank] = full.numpy().tolist()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("n", [1000, 4096, 33])
+def test_gather_shards_rebuilds_the_fields(n):
+    world = 2
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.start_processes(_gather_worker, args=(world, _free_port(), n, out), nprocs=world,
+                       join=True, start_method="spawn")
+    want = [[10.0 * f + t for t in range(n)] for f in range(5)]
+    assert out[0] == want and out[1] == want
