@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_target(AdjArgs A) {
           } else if (A.theta2 * dist2 > (A.macb ? A.macb[u] : s_bl2[mu.y & 0xff])) {
             double m[9];
 #pragma unroll
-            for (int k = 0; k < 9; ++k) m[k] = A.mom[9 * (int64_t)u + k];
+            for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
             twig_adj<kWithE>(nd.w, m, dx, dy, dz, A.eps2, gp, gE, a);
             contrib = true;
             next = (unsigned)mu.x;
@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_group(AdjArgs A) {
             if (valid) {
               double m[9];
 #pragma unroll
-              for (int k = 0; k < 9; ++k) m[k] = A.mom[9 * (int64_t)u + k];
+              for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
               twig_adj<kWithE>(nd.w, m, dx, dy, dz, A.eps2, gp, gE, a);
             }
             flush_twig_paired(A.adj, u, a, pend_u, pend, M, lane);
@@ -393,7 +393,7 @@ __global__ void k_adj_down_level(int level, const int32_t* __restrict__ lvl,
                                  const int32_t* __restrict__ twiglist,
                                  const int2* __restrict__ meta,
                                  const double4* __restrict__ nc4, const double* __restrict__ mom,
-                                 const double2* __restrict__ aux, double* __restrict__ adj) {
+                                 double* __restrict__ adj) {
   int base = 0;
   for (int l = 0; l < level; ++l) base += lvl[l];
   const int cnt = lvl[level];
@@ -401,7 +401,7 @@ __global__ void k_adj_down_level(int level, const int32_t* __restrict__ lvl,
     const int64_t u = twiglist[base + i];
     const int2 mu = meta[u];
     const double4 pc = nc4[u];
-    const double A = aux[u].x;
+    const double A = mom[kMomStride * u + kMomAbs];
     const double* pa = adj + kNA * u;
     const double Pq = pa[0];
     const double Pp[3] = {pa[1], pa[2], pa[3]};
@@ -418,7 +418,7 @@ __global__ void k_adj_down_level(int level, const int32_t* __restrict__ lvl,
       const bool leafc = (meta[c].y & kLeafFlag) != 0;
       double pcv[3] = {0, 0, 0};
       if (!leafc)
-        for (int i = 0; i < 3; ++i) pcv[i] = mom[9 * c + i];
+        for (int i = 0; i < 3; ++i) pcv[i] = mom[kMomStride * c + i];
       const double qc = cc.w;
       const double sc[3] = {pc.x - cc.x, pc.y - cc.y, pc.z - cc.z};
       double sbar[3] = {0, 0, 0};
@@ -449,7 +449,7 @@ __global__ void k_adj_down_level(int level, const int32_t* __restrict__ lvl,
       const bool leafc = (meta[c].y & kLeafFlag) != 0;
       double* a = adj + kNA * c;
       if (A != 0.0) {
-        const double Ac = leafc ? fabs(cc.w) : aux[c].x;
+        const double Ac = leafc ? fabs(cc.w) : mom[kMomStride * c + kMomAbs];
         const double w = Ac / A;
         const double cv[3] = {cc.x, cc.y, cc.z};
         const double pv[3] = {pc.x, pc.y, pc.z};
@@ -607,7 +607,7 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
     const unsigned gl = (unsigned)std::min<int64_t>((cnt + 255) / 256, 148 * 16);
     COUNT_LAUNCH();
     k_adj_down_level<<<gl, 256, 0, s>>>(L, c->lvlcnt.p, c->twiglist.p, c->meta.p, c->nc4.p,
-                                        c->mom.p, c->aux.p, c->adj.p);
+                                        c->mom.p, c->adj.p);
   }
   COUNT_LAUNCH();
   k_adj_out<<<g, 256, 0, s>>>(c->n, c->leafnode.p, c->perm.p, c->q.p, c->adj.p, dq, dx, dy, dz);

@@ -59,6 +59,7 @@ template bool ensure<double4>(Ctx*, DBuf<double4>&, size_t, const char*);
 template bool ensure<double2>(Ctx*, DBuf<double2>&, size_t, const char*);
 template bool ensure<int2>(Ctx*, DBuf<int2>&, size_t, const char*);
 template bool ensure<int4>(Ctx*, DBuf<int4>&, size_t, const char*);
+template bool ensure<LevelRecord>(Ctx*, DBuf<LevelRecord>&, size_t, const char*);
 
 template <class T>
 static void release(DBuf<T>& b) {
@@ -340,9 +341,11 @@ int pepcg_destroy(void* ctx) {
   release(c->lev); release(c->lcpn);
   release(c->cstart); release(c->cend); release(c->sstart); release(c->send);
   release(c->scan_tmp);
-  release(c->nc4); release(c->meta); release(c->fwd); release(c->mom); release(c->aux);
+  release(c->nc4); release(c->meta); release(c->fwd); release(c->mom);
   release(c->mom32);
-  release(c->parent); release(c->nchild); release(c->twiglist); release(c->lvlcnt); release(c->lvlblk); release(c->macb); release(c->first_part);
+  release(c->parent); release(c->nchild); release(c->twiglist); release(c->lvlcnt); release(c->lvlblk);
+  release(c->drec); release(c->dmom);
+  release(c->tinfo); release(c->tcounts); release(c->macb); release(c->first_part);
   release(c->nleaves); release(c->child8); release(c->wstack); release(c->leafnode);
   release(c->adj); release(c->fpo2rpo); release(c->rpo2fpo); release(c->nkey);
   release(c->tiles); release(c->counters); release(c->tgt); release(c->tkeys);

@@ -111,31 +111,6 @@ __constant__ int8_t c_CI3[8] = {0, 1, 3, 2, 7, 6, 4, 5};  // :389
 __constant__ int8_t c_G3x[8] = {5, 6, 0, 5, 5, 0, 6, 5};  // :390 exchange
 __constant__ int8_t c_G3r[8] = {0, 0, 0, 5, 0, 0, 6, 5};  // :390 reverse
 
-__device__ __forceinline__ uint64_t hilbert3d(int64_t i0, int64_t i1, int64_t i2) {
-  int64_t it[3] = {i0, i1, i2};
-  uint64_t key = 1;
-#pragma unroll 1
-  for (int i = kMaxLevel - 1; i >= 0; --i) {
-    int cval = (int)((((it[2] >> i) & 1) << 2) | (((it[1] >> i) & 1) << 1) | ((it[0] >> i) & 1));
-    const int64_t lowmask = (int64_t(1) << i) - 1;
-    it[0] &= lowmask;
-    it[1] &= lowmask;
-    it[2] &= lowmask;
-    int h = c_CI3[cval];
-    int ex = c_G3x[h], rv = c_G3r[h];
-    key = (key << 3) | (uint64_t)h;
-    if (ex == 5) {
-      int64_t t = it[0]; it[0] = it[2]; it[2] = t;
-    } else if (ex == 6) {
-      int64_t t = it[1]; it[1] = it[2]; it[2] = t;
-    }
-    if (rv & 1) it[0] = (~it[0]) & lowmask;
-    if (rv & 2) it[1] = (~it[1]) & lowmask;
-    if (rv & 4) it[2] = (~it[2]) & lowmask;
-  }
-  return key;
-}
-
 __device__ __forceinline__ uint64_t morton3d(int64_t i0, int64_t i1, int64_t i2) {
   uint64_t key = 1;
 #pragma unroll 4
@@ -741,10 +716,17 @@ __global__ void k_link(int64_t M, const int2* __restrict__ meta,
 // Twigs grouped by level for the upward pass and the adjoint's downward pass.
 // lvl[0..20] counts the twigs of each level (k_node_counts); twiglist holds,
 // level after level, the RPO indices of that level's twigs in increasing
-// order, so that neighbouring threads of a level's launch read neighbouring
-// subtrees.  Built from per-block counts of each level's twigs, an exclusive
-// scan over (level, block) in level-major order -- level L then starts after
-// all twigs above it, level_base below -- and a stable scatter.
+// order.  The same ordering of all nodes gives every node a position in the
+// level-ordered records drec (level after level, RPO order within a level).
+// A twig's children are consecutive nodes of the next level in that order (a
+// node of level L+1 between two children would lie inside the first child's
+// subtree), so the upward pass reads a twig's children as one run of the
+// level-ordered records: child slot k (child8 order) sits at the position of
+// slot 0 plus k.
+//
+// Built from per-block counts of each level's twigs and nodes, exclusive
+// scans over (level, block) in level-major order -- level L then starts
+// after everything above it -- and a stable scatter.
 __device__ __forceinline__ int level_base(const int32_t* lvl, int level) {
   int b = 0;
   for (int l = 0; l < level; ++l) b += lvl[l];
@@ -752,36 +734,34 @@ __device__ __forceinline__ int level_base(const int32_t* lvl, int level) {
 }
 
 __global__ void __launch_bounds__(256) k_level_count(int64_t M, const int2* __restrict__ meta,
-                                                     int32_t* __restrict__ bcnt, int nblk) {
-  __shared__ int h[kMaxLevel + 1];
-  if (threadIdx.x <= kMaxLevel) h[threadIdx.x] = 0;
+                                                     int32_t* __restrict__ bcnt_twig,
+                                                     int32_t* __restrict__ bcnt_all, int nblk) {
+  __shared__ int ht[kMaxLevel + 1], ha[kMaxLevel + 1];
+  if (threadIdx.x <= kMaxLevel) ht[threadIdx.x] = ha[threadIdx.x] = 0;
   __syncthreads();
   const int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (u < M) {
     const int2 mu = meta[u];
-    if (!(mu.y & kLeafFlag)) atomicAdd(&h[mu.y & 0xff], 1);
+    atomicAdd(&ha[mu.y & 0xff], 1);
+    if (!(mu.y & kLeafFlag)) atomicAdd(&ht[mu.y & 0xff], 1);
   }
   __syncthreads();
-  if (threadIdx.x <= kMaxLevel) bcnt[(int64_t)threadIdx.x * nblk + blockIdx.x] = h[threadIdx.x];
+  if (threadIdx.x <= kMaxLevel) {
+    bcnt_twig[(int64_t)threadIdx.x * nblk + blockIdx.x] = ht[threadIdx.x];
+    bcnt_all[(int64_t)threadIdx.x * nblk + blockIdx.x] = ha[threadIdx.x];
+  }
 }
 
-__global__ void __launch_bounds__(256) k_level_scatter(int64_t M, const int2* __restrict__ meta,
-                                                       const int32_t* __restrict__ bofs, int nblk,
-                                                       int32_t* __restrict__ twiglist) {
-  __shared__ int wc[256 / 32][kMaxLevel + 1];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x < (256 / 32) * (kMaxLevel + 1)) (&wc[0][0])[threadIdx.x] = 0;
-  const int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  int L = -1;
-  if (u < M) {
-    const int2 mu = meta[u];
-    if (!(mu.y & kLeafFlag)) L = mu.y & 0xff;
-  }
-  const unsigned peers = __match_any_sync(0xffffffffu, L);
+// rank of this lane among the block's lanes with the same key (-1: none),
+// in block order, plus the warp-level prefix held in wc[warp][key]
+__device__ __forceinline__ int block_rank(int key, int warp, int lane, int (*wc)[kMaxLevel + 1]) {
+  const unsigned peers = __match_any_sync(0xffffffffu, key);
   const int lrank = __popc(peers & ((1u << lane) - 1u));
-  __syncthreads();
-  if (L >= 0 && lane == __ffs(peers) - 1) wc[warp][L] = __popc(peers);
-  __syncthreads();
+  if (key >= 0 && lane == __ffs(peers) - 1) wc[warp][key] = __popc(peers);
+  return lrank;
+}
+
+__device__ __forceinline__ void warp_prefix(int (*wc)[kMaxLevel + 1]) {
   if (threadIdx.x <= kMaxLevel) {  // exclusive prefix over the warps, level threadIdx.x
     int run = 0;
     for (int w = 0; w < 256 / 32; ++w) {
@@ -790,26 +770,94 @@ __global__ void __launch_bounds__(256) k_level_scatter(int64_t M, const int2* __
       run += t;
     }
   }
+}
+
+// Also writes every leaf's level-ordered record (centre and charge from nc4,
+// (abs_charge, bmax) = (|q|, 0)), and for the twig at list position P its
+// child count and leaf mask with its own position (tinfo[P]), and its child
+// and twig-child counts (ccnt[P], tcnt[P]).  Scanned over the twig list, the
+// counts give the position of the twig's first child in the level order and
+// of its first twig child in the twig list: every node but the root has one
+// parent, so the scan at P counts the nodes (twigs) of levels 1 .. L and the
+// children of the level-L twigs before P, one short of the position.
+__global__ void __launch_bounds__(256) k_level_scatter(int64_t M, const int2* __restrict__ meta,
+                                                       const int32_t* __restrict__ bofs_twig,
+                                                       const int32_t* __restrict__ bofs_all,
+                                                       int nblk, int32_t* __restrict__ twiglist,
+                                                       const double4* __restrict__ nc4,
+                                                       LevelRecord* __restrict__ drec,
+                                                       const int4* __restrict__ child8,
+                                                       const int32_t* __restrict__ nchild,
+                                                       int2* __restrict__ tinfo,
+                                                       int32_t* __restrict__ ccnt,
+                                                       int32_t* __restrict__ tcnt) {
+  __shared__ int wt[256 / 32][kMaxLevel + 1], wa[256 / 32][kMaxLevel + 1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x < (256 / 32) * (kMaxLevel + 1)) {
+    (&wt[0][0])[threadIdx.x] = 0;
+    (&wa[0][0])[threadIdx.x] = 0;
+  }
+  const int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int L = -1, end = 0;
+  bool leaf = false;
+  if (u < M) {
+    const int2 mu = meta[u];
+    L = mu.y & 0xff;
+    leaf = (mu.y & kLeafFlag) != 0;
+    end = mu.x;
+  }
   __syncthreads();
-  if (L >= 0) twiglist[bofs[(int64_t)L * nblk + blockIdx.x] + wc[warp][L] + lrank] = (int32_t)u;
+  const int rt = block_rank(leaf ? -1 : L, warp, lane, wt);
+  const int ra = block_rank(L, warp, lane, wa);
+  __syncthreads();
+  warp_prefix(wt);
+  warp_prefix(wa);
+  __syncthreads();
+  if (L < 0) return;
+  const int p = bofs_all[(int64_t)L * nblk + blockIdx.x] + wa[warp][L] + ra;
+  if (!leaf) {
+    const int P = bofs_twig[(int64_t)L * nblk + blockIdx.x] + wt[warp][L] + rt;
+    twiglist[P] = (int32_t)u;
+    // child slot k is a leaf when the next child (or the subtree's end)
+    // starts right after it
+    const int4 c0 = child8[2 * u], c1 = child8[2 * u + 1];
+    const int ch[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+    const int nc = min(8, nchild[u]);
+    unsigned lm = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (k < nc && (k + 1 < nc ? ch[k + 1] : end) == ch[k] + 1) lm |= 1u << k;
+    tinfo[P] = make_int2(nc | (int)(lm << 8), p);
+    ccnt[P] = nc;
+    tcnt[P] = nc - __popc(lm);
+  } else {
+    const double4 a = nc4[u];
+    LevelRecord r;
+    r.pos = a;
+    r.ab = make_double2(fabs(a.w), 0.0);
+    r.pad[0] = r.pad[1] = 0;
+    drec[p] = r;
+  }
 }
 
 // Upward pass: tree_node_update_from_children / shift_multipoles_up
 // (module_tree_grow.f90:762-821, coulomb/module_interaction_specific.f90:84-140),
 // level-synchronous: one launch per level, deepest first; every child of a
 // level-L twig was finished by an earlier launch, so there are no fences and
-// no atomics.  One thread per twig; every sum runs over the children in key
-// order (child8 lists them last to first, like the RPO chain, so k runs
-// nc-1 .. 0) with the reference's operations in its order (no contraction:
+// no atomics.  One thread per twig, in the level's RPO order; every sum runs
+// over the children in key order (child slot k = nc-1 .. 0, slot 0 being the
+// last child) with the reference's operations in its order (no contraction:
 // this file is compiled with --fmad=false).
 //
-// Memory: a twig's children form its RPO subtree range in order, so child k
-// is a leaf exactly when the next child (or the subtree's end, for the last
-// one) starts right after it -- no load of the child's own record.  All child
-// data is then requested in one round: centres and charges (and the twig
-// children's abs_charge / bmax) into registers, the twig children's 9
-// moments into this thread's slice of shared memory by cp.async, which
-// costs no registers.  A twig thus waits for three memory latencies.
+// Memory: a twig's own data (twig list, tinfo, scanned counts) is read at
+// its list position; its children's records from the level-ordered copy
+// (drec: consecutive threads read consecutive runs), and its twig children's
+// nine moments from dmom at their twig-list positions, likewise consecutive
+// for consecutive parents.  The moments arrive in this thread's slice of
+// shared memory by cp.async, which costs no registers.  So a twig waits for
+// two memory latencies.  The twig writes its record both to the RPO arrays
+// the walks read (nc4, mom, mom32, all whole sectors) and to the
+// level-ordered copy its parent will read.
 constexpr int kUpThreads = 128;
 constexpr int kUpSmem = kUpThreads * 8 * 9 * 8;  // 9 moments of up to 8 children per thread
 
@@ -818,32 +866,30 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 
-__global__ void __launch_bounds__(kUpThreads) k_upward_level(int level, const int32_t* __restrict__ lvl,
-                                                             const int32_t* __restrict__ twiglist,
-                                                             const int2* __restrict__ meta,
-                                                             const int4* __restrict__ child8,
-                                                             const int32_t* __restrict__ nchild,
-                                                             double4* __restrict__ nc4,
-                                                             double* __restrict__ mom,
-                                                             double2* __restrict__ aux,
-                                                             float4* __restrict__ mom32) {
+__global__ void __launch_bounds__(kUpThreads) k_upward_level(
+    int level, const int32_t* __restrict__ lvl, const int32_t* __restrict__ twiglist,
+    const int2* __restrict__ tinfo, const int32_t* __restrict__ cfirst,
+    const int32_t* __restrict__ tfirst, LevelRecord* __restrict__ drec,
+    double* __restrict__ dmom, double4* __restrict__ nc4, double* __restrict__ mom,
+    float4* __restrict__ mom32) {
   extern __shared__ double s_up[];
   double* sm = s_up + threadIdx.x * 72;
   const int cnt = lvl[level];
-  const int32_t* list = twiglist + level_base(lvl, level);
+  const int base = level_base(lvl, level);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
-    const int64_t u = list[i];
-    const int4 c0 = child8[2 * u], c1 = child8[2 * u + 1];
-    const int nc = min(8, nchild[u]);
-    const int end = meta[u].x;
-    const int ch[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-    bool lf[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) lf[k] = k < nc && (k + 1 < nc ? ch[k + 1] : end) == ch[k] + 1;
+    const int P = base + i;
+    const int64_t u = twiglist[P];
+    const int2 ti = tinfo[P];
+    const int nc = ti.x & 0xff;
+    const unsigned lm = (unsigned)ti.x >> 8;  // leaf children, by slot
+    const int pu = ti.y;
+    const int cs = cfirst[P] + 1;  // level-order position of child slot 0
+    const int ts = tfirst[P] + 1;  // twig-list position of the first twig child
 #pragma unroll
     for (int k = 0; k < 8; ++k)
-      if (k < nc && !lf[k]) {
-        const double* src = mom + 9 * (int64_t)ch[k];
+      if (k < nc && !((lm >> k) & 1u)) {
+        const int64_t tp = ts + __popc(~lm & ((1u << k) - 1u));
+        const double* src = dmom + 9 * tp;
 #pragma unroll
         for (int j = 0; j < 9; ++j) cp_async8(sm + 9 * k + j, src + j);
       }
@@ -853,8 +899,9 @@ __global__ void __launch_bounds__(kUpThreads) k_upward_level(int level, const in
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       if (k < nc) {
-        ca[k] = nc4[ch[k]];
-        cb[k] = lf[k] ? make_double2(fabs(ca[k].w), 0.0) : aux[ch[k]];
+        const LevelRecord& r = drec[cs + k];
+        ca[k] = r.pos;
+        cb[k] = r.ab;
       }
     }
     double charge = 0.0, absq = 0.0;
@@ -898,7 +945,7 @@ __global__ void __launch_bounds__(kUpThreads) k_upward_level(int level, const in
       if (k < nc) {
         double m[9];
 #pragma unroll
-        for (int j = 0; j < 9; ++j) m[j] = lf[k] ? 0.0 : sm[9 * k + j];
+        for (int j = 0; j < 9; ++j) m[j] = ((lm >> k) & 1u) ? 0.0 : sm[9 * k + j];
         const double s0 = cx - ca[k].x, s1 = cy - ca[k].y, s2 = cz - ca[k].z;
         const double q = ca[k].w;
         d0 = (d0 + m[0]) + q * s0;
@@ -914,17 +961,31 @@ __global__ void __launch_bounds__(kUpThreads) k_upward_level(int level, const in
         if (k == nc - 1 || v > bmax) bmax = v;
       }
     }
-    nc4[u] = make_double4(cx, cy, cz, charge);
-    aux[u] = make_double2(absq, bmax);
-    double* o = mom + 9 * u;
-    o[0] = d0; o[1] = d1; o[2] = d2; o[3] = q0; o[4] = q1; o[5] = q2; o[6] = xy; o[7] = yz; o[8] = zx;
+    const double4 c4 = make_double4(cx, cy, cz, charge);
+    nc4[u] = c4;
+    LevelRecord r;
+    r.pos = c4;
+    r.ab = make_double2(absq, bmax);
+    r.pad[0] = r.pad[1] = 0;
+    drec[pu] = r;
+    double2* o = reinterpret_cast<double2*>(mom + kMomStride * u);
+    o[0] = make_double2(d0, d1);
+    o[1] = make_double2(d2, q0);
+    o[2] = make_double2(q1, q2);
+    o[3] = make_double2(xy, yz);
+    o[4] = make_double2(zx, absq);
+    o[5] = make_double2(bmax, 0.0);
+    double* od = dmom + 9 * (int64_t)P;
+    od[0] = d0; od[1] = d1; od[2] = d2; od[3] = q0; od[4] = q1; od[5] = q2;
+    od[6] = xy; od[7] = yz; od[8] = zx;
     // FP32 copy for the mixed walk, the quadrupole matrix M (off-diagonals
     // halved) scaled by 3: (px, py, pz, 3qxx), (3qyy, 3qzz, 1.5qxy, 1.5qyz),
-    // (1.5qzx, qxx+qyy+qzz, charge, 0)
-    mom32[3 * u] = make_float4((float)d0, (float)d1, (float)d2, (float)(3.0 * q0));
-    mom32[3 * u + 1] =
-        make_float4((float)(3.0 * q1), (float)(3.0 * q2), (float)(1.5 * xy), (float)(1.5 * yz));
-    mom32[3 * u + 2] = make_float4((float)(1.5 * zx), (float)((q0 + q1) + q2), (float)charge, 0.f);
+    // (1.5qzx, qxx+qyy+qzz, charge, 0), padded to a whole 64-byte record
+    float4* m4 = mom32 + kMom32Stride * u;
+    m4[0] = make_float4((float)d0, (float)d1, (float)d2, (float)(3.0 * q0));
+    m4[1] = make_float4((float)(3.0 * q1), (float)(3.0 * q2), (float)(1.5 * xy), (float)(1.5 * yz));
+    m4[2] = make_float4((float)(1.5 * zx), (float)((q0 + q1) + q2), (float)charge, 0.f);
+    m4[3] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
 }
 
@@ -1089,8 +1150,8 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
     return PEPCG_ERR_NODE_POOL;
   }
   if (!ensure(c, c->nc4, M, "nc4") || !ensure(c, c->meta, M, "meta") ||
-      !ensure(c, c->fwd, M, "fwd") || !ensure(c, c->mom, 9 * M, "mom") ||
-      !ensure(c, c->aux, M, "aux") || !ensure(c, c->mom32, 12 * M, "mom32") ||
+      !ensure(c, c->fwd, M, "fwd") || !ensure(c, c->mom, kMomStride * M, "mom") ||
+      !ensure(c, c->mom32, 4 * kMom32Stride * M, "mom32") ||
       !ensure(c, c->parent, M, "parent") || !ensure(c, c->nchild, M, "nchild") ||
       !ensure(c, c->twiglist, M, "twiglist") || !ensure(c, c->first_part, M, "first_part") ||
       !ensure(c, c->nleaves, M, "nleaves") || !ensure(c, c->fpo2rpo, M, "fpo2rpo") ||
@@ -1111,13 +1172,26 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
   // count; the deepest twig level is one above the deepest leaf level
   {
     const unsigned gM = (unsigned)((M + kThreads - 1) / kThreads);
+    const size_t nlb = (size_t)(kMaxLevel + 1) * gM;
+    const int64_t ntw = M - n;
+    if (!ensure(c, c->lvlblk, 2 * nlb, "level blocks") ||
+        !ensure(c, c->drec, M, "level records") || !ensure(c, c->dmom, 9 * ntw, "dmom") ||
+        !ensure(c, c->tinfo, ntw, "twig info") || !ensure(c, c->tcounts, 2 * ntw, "twig counts"))
+      return PEPCG_ERR_OOM;
+    int32_t* bt = c->lvlblk.p;
+    int32_t* ba = c->lvlblk.p + nlb;
     COUNT_LAUNCH();
-    if (!ensure(c, c->lvlblk, (size_t)(kMaxLevel + 1) * gM, "level blocks")) return PEPCG_ERR_OOM;
-    k_level_count<<<gM, kThreads, 0, s>>>(M, c->meta.p, c->lvlblk.p, (int)gM);
-    exclusive_scan<int32_t>(c->lvlblk.p, c->lvlblk.p, (int64_t)(kMaxLevel + 1) * gM,
-                            c->scan_tmp.p, s);
+    k_level_count<<<gM, kThreads, 0, s>>>(M, c->meta.p, bt, ba, (int)gM);
+    exclusive_scan<int32_t>(bt, bt, (int64_t)nlb, c->scan_tmp.p, s);
+    exclusive_scan<int32_t>(ba, ba, (int64_t)nlb, c->scan_tmp.p, s);
     COUNT_LAUNCH();
-    k_level_scatter<<<gM, kThreads, 0, s>>>(M, c->meta.p, c->lvlblk.p, (int)gM, c->twiglist.p);
+    int32_t* cc = c->tcounts.p;
+    int32_t* tcn = c->tcounts.p + ntw;
+    k_level_scatter<<<gM, kThreads, 0, s>>>(M, c->meta.p, bt, ba, (int)gM, c->twiglist.p,
+                                            c->nc4.p, c->drec.p, c->child8.p,
+                                            c->nchild.p, c->tinfo.p, cc, tcn);
+    exclusive_scan<int32_t>(cc, cc, ntw, c->scan_tmp.p, s);
+    exclusive_scan<int32_t>(tcn, tcn, ntw, c->scan_tmp.p, s);
     cudaFuncSetAttribute(k_upward_level, cudaFuncAttributeMaxDynamicSharedMemorySize, kUpSmem);
     float4* m32 = reinterpret_cast<float4*>(c->mom32.p);
     for (int L = c->max_level - 1; L >= 0; --L) {
@@ -1125,8 +1199,8 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
       if (cnt <= 0) continue;
       COUNT_LAUNCH();
       k_upward_level<<<grid_for(cnt, kUpThreads), kUpThreads, kUpSmem, s>>>(
-          L, c->lvlcnt.p, c->twiglist.p, c->meta.p, c->child8.p, c->nchild.p, c->nc4.p, c->mom.p,
-          c->aux.p, m32);
+          L, c->lvlcnt.p, c->twiglist.p, c->tinfo.p, cc, tcn, c->drec.p, c->dmom.p, c->nc4.p,
+          c->mom.p, m32);
     }
   }
   cudaEventRecord(c->ev[4], s);
@@ -1145,7 +1219,7 @@ __global__ void k_export(int64_t M, const int32_t* __restrict__ fpo2rpo,
                          const int32_t* __restrict__ rpo2fpo, const int2* __restrict__ meta,
                          const int2* __restrict__ fwd, const int32_t* __restrict__ parent,
                          const int64_t* __restrict__ nkey, const double4* __restrict__ nc4,
-                         const double* __restrict__ mom, const double2* __restrict__ aux,
+                         const double* __restrict__ mom,
                          int64_t* okey, int32_t* olevel, int64_t* oleaves, int64_t* odesc,
                          int64_t* oparent, int64_t* ofirst, int64_t* onext, double* omom,
                          const int32_t* __restrict__ first_part, int64_t n) {
@@ -1176,10 +1250,10 @@ __global__ void k_export(int64_t M, const int32_t* __restrict__ fpo2rpo,
       o[4] = fabs(a.w);
       for (int k = 5; k < 15; ++k) o[k] = 0.0;
     } else {
-      double2 b = aux[u];
-      o[4] = b.x;
-      for (int k = 0; k < 9; ++k) o[5 + k] = mom[9 * u + k];
-      o[14] = b.y;
+      const double* m = mom + kMomStride * u;
+      o[4] = m[kMomAbs];
+      for (int k = 0; k < 9; ++k) o[5 + k] = m[k];
+      o[14] = m[kMomBmax];
     }
     // leaves = particles in the node's range: from the first particle of this
     // node to the first particle of the node after the subtree
@@ -1207,7 +1281,7 @@ int export_tree(Ctx* c, int64_t* key, int32_t* level, int64_t* leaves, int64_t* 
   int32_t* dlev = (int32_t*)(dm + 15 * M);
   COUNT_LAUNCH();
   k_export<<<grid_for(M), kThreads, 0, s>>>(M, c->fpo2rpo.p, c->rpo2fpo.p, c->meta.p, c->fwd.p,
-                                            c->parent.p, c->nkey.p, c->nc4.p, c->mom.p, c->aux.p,
+                                            c->parent.p, c->nkey.p, c->nc4.p, c->mom.p,
                                             dk, dlev, dl, dd, dp, df, dn, dm, c->first_part.p, c->n);
   bool ok = true;
   auto cp = [&](void* h, const void* dv, size_t b) {

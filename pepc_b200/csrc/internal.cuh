@@ -12,9 +12,9 @@
 //       meta[u]  = (skip, level | leaf flag << 8)          int32 x 2
 //       fwd[u]   = (first child in key order, next node after the subtree in
 //                   key-order preorder)                     int32 x 2
-//       mom[u]   = twig moments (dip x3, quad xx yy zz, xy yz zx) FP64 x 9
-//       aux[u]   = (abs_charge, bmax)                      FP64 x 2 (twigs)
-//       mom32[u] = the 9 moments in FP32 (mixed walk)
+//       mom[u]   = twig moments (dip x3, quad xx yy zz, xy yz zx), then
+//                  abs_charge and bmax                      FP64 x 12 (96 B)
+//       mom32[u] = the moments in FP32 (mixed walk)         float4 x 4 (64 B)
 //     rpo2fpo / fpo2rpo map RPO to the reference's node order (forward
 //     preorder = insertion order of module_tree_grow.f90:623-696).
 #pragma once
@@ -57,6 +57,23 @@ struct DBuf {
 
 struct Walk;
 
+// Per-node records are whole 32-byte sectors, so that the upward pass writes
+// no partial sector (a partial sector costs HBM a read-modify-write):
+//   mom  : kMomStride doubles per node, moments [0, 9), abs_charge, bmax, pad
+//   mom32: kMom32Stride float4 per node, the FP32 moments of the mixed walk
+constexpr int kMomStride = 12;
+constexpr int kMomAbs = 9;
+constexpr int kMomBmax = 10;
+constexpr int kMom32Stride = 4;
+
+// The upward pass's level-ordered copy of a node: centre and charge and
+// (abs_charge, bmax), padded to 64 bytes.
+struct __align__(16) LevelRecord {
+  double4 pos;
+  double2 ab;
+  double pad[2];
+};
+
 struct Ctx {
   pepcg_params prm;
   int device = 0;
@@ -88,13 +105,20 @@ struct Ctx {
   DBuf<double4> nc4;
   DBuf<int2> meta;
   DBuf<int2> fwd;
-  DBuf<double> mom;   // 9 * nnodes, node-major
-  DBuf<double2> aux;
-  DBuf<float> mom32;  // 12 * nnodes (coc-relative moments in FP32, padded)
+  // kMomStride doubles per node (96 B, three whole sectors): the 9 moments,
+  // then abs_charge and bmax
+  DBuf<double> mom;
+  DBuf<float> mom32;  // 16 floats per node (64 B): the FP32 moments, padded
   DBuf<int32_t> parent, nchild, first_part, nleaves;
   DBuf<int32_t> twiglist;  // twig RPO indices grouped by level (upward and adjoint passes)
   DBuf<int32_t> lvlcnt;    // [0, 32) twigs per level
-  DBuf<int32_t> lvlblk;    // twigs per (level, block of 256 nodes), then their exclusive scan
+  DBuf<int32_t> lvlblk;    // twigs, then nodes, per (level, block of 256 nodes), scanned
+  // level-ordered copy of the node records for the upward pass: centre /
+  // charge and (abs_charge, bmax); the twigs' moments by twig-list position
+  DBuf<LevelRecord> drec;
+  DBuf<double> dmom;
+  DBuf<int2> tinfo;        // per twig-list position: child count | leaf mask << 8, own position
+  DBuf<int32_t> tcounts;   // per twig-list position: children, then twig children (scanned)
   DBuf<double> macb;       // per-twig MAC threshold for mac_select != 0
   int32_t lvl_host[kMaxLevel + 1] = {0};  // twigs per level of the grown tree
   DBuf<int4> child8;  // up to 8 children (RPO indices) per twig, as 2 x int4

@@ -42,7 +42,7 @@ struct MixArgs {
   const double* tz;
   const double4* nc4;
   const int2* meta;
-  const float4* mom32;  // 3 float4 per node
+  const float4* mom32;  // kMom32Stride float4 per node, the first 3 used
   const int32_t* nleaves;
   const double* bl2;
   const double* macb;  // per-twig MAC threshold, or nullptr: bl2 of the level (Barnes-Hut)
@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(kMixThreads, 5)
         if (accept) {
           StagedTwig& r = stw[(hT + nT + __popc(ab & lt)) & (kRing - 1)];
           r.c = make_float4(cx, cy, cz, (float)a.w);
-          const float4* m = A.mom32 + 3 * (int64_t)node;
+          const float4* m = A.mom32 + kMom32Stride * (int64_t)node;
           cp_async16(&r.m0, m);
           cp_async16(&r.m1, m + 1);
           cp_async16(&r.m2, m + 2);
@@ -462,8 +462,8 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_target_mixed(MixArgs A) {
             const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             if (A.theta2 * r2 > (A.macb ? (float)A.macb[u] : s_bl2[mu.y & 0xff])) {
               partner += A.nleaves[u];
-              const float4 m0 = A.mom32[3 * (int64_t)u], m1 = A.mom32[3 * (int64_t)u + 1],
-                           m2 = A.mom32[3 * (int64_t)u + 2];
+              const float4* mu4 = A.mom32 + kMom32Stride * (int64_t)u;
+              const float4 m0 = mu4[0], m1 = mu4[1], m2 = mu4[2];
               twig32(m0, m1, m2, dx, dy, dz, A.eps2, ax, ay, az, ap);
               ++c_twig;
               W += 1.0;

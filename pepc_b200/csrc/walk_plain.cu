@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_target64(WalkArgs A) {
             partner += A.nleaves[u];
             double m[9];
 #pragma unroll
-            for (int k = 0; k < 9; ++k) m[k] = A.mom[9 * (int64_t)u + k];
+            for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
             double fx, fy, fz, fp;
             law_twig64<kLaw>(a.w, m, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp);
             e0 += fx; e1 += fy; e2 += fz; ph += fp;
@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_tile64(WalkArgs A) {
             if (valid) {
               double m[9];
 #pragma unroll
-              for (int k = 0; k < 9; ++k) m[k] = A.mom[9 * (int64_t)u + k];
+              for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
               double fx, fy, fz, fp;
               law_twig64<kLaw>(a.w, m, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp);
               e0 += fx; e1 += fy; e2 += fz; ph += fp;
@@ -265,14 +265,14 @@ __global__ void k_reset_counter() { g_bucket_counter = 0; }
 // has t = min(bmax^2, 3 boxlength2(level)); any other selection accepts
 // nothing (the N^2 code), t = +inf.
 __global__ void k_mac_thresholds(int64_t M, int mode, const int2* __restrict__ meta,
-                                 const double2* __restrict__ aux, const double* __restrict__ bl2,
+                                 const double* __restrict__ mom, const double* __restrict__ bl2,
                                  double* __restrict__ macb) {
   for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < M;
        u += (int64_t)gridDim.x * blockDim.x) {
     const int2 mu = meta[u];
     if (mu.y & kLeafFlag) continue;
     if (mode == 1) {
-      const double bmax = aux[u].y;
+      const double bmax = mom[kMomStride * u + kMomBmax];
       macb[u] = fmin(bmax * bmax, 3.0 * bl2[mu.y & 0xff]);
     } else {
       macb[u] = INFINITY;
@@ -306,7 +306,7 @@ int prepare_mac(Ctx* c, const double** macb) {
   if (!ensure(c, c->macb, M, "mac thresholds")) return PEPCG_ERR_OOM;
   COUNT_LAUNCH();
   const unsigned g = (unsigned)((M + 255) / 256 > 148 * 16 ? 148 * 16 : (M + 255) / 256);
-  k_mac_thresholds<<<g, 256, 0, c->stream>>>(M, c->prm.mac_select, c->meta.p, c->aux.p,
+  k_mac_thresholds<<<g, 256, 0, c->stream>>>(M, c->prm.mac_select, c->meta.p, c->mom.p,
                                              c->d_box + 9, c->macb.p);
   if (!cuda_ok(c, cudaGetLastError(), "mac thresholds")) return PEPCG_ERR_CUDA;
   *macb = c->macb.p;
