@@ -853,18 +853,12 @@ __global__ void __launch_bounds__(256) k_level_scatter(int64_t M, const int2* __
 // its list position; its children's records from the level-ordered copy
 // (drec: consecutive threads read consecutive runs), and its twig children's
 // nine moments from dmom at their twig-list positions, likewise consecutive
-// for consecutive parents.  The moments arrive in this thread's slice of
-// shared memory by cp.async, which costs no registers.  So a twig waits for
-// two memory latencies.  The twig writes its record both to the RPO arrays
-// the walks read (nc4, mom, mom32, all whole sectors) and to the
-// level-ordered copy its parent will read.
+// for consecutive parents.  The children's records are re-read by each sum
+// (L1 hits) rather than held in registers, which keeps the kernel at 68
+// registers and lets more twigs be in flight per SM.  The twig writes its
+// record both to the RPO arrays the walks read (nc4, mom, mom32, all whole
+// sectors) and to the level-ordered copy its parent will read.
 constexpr int kUpThreads = 128;
-constexpr int kUpSmem = kUpThreads * 8 * 9 * 8;  // 9 moments of up to 8 children per thread
-
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
 
 __global__ void __launch_bounds__(kUpThreads) k_upward_level(
     int level, const int32_t* __restrict__ lvl, const int32_t* __restrict__ twiglist,
@@ -872,8 +866,6 @@ __global__ void __launch_bounds__(kUpThreads) k_upward_level(
     const int32_t* __restrict__ tfirst, LevelRecord* __restrict__ drec,
     double* __restrict__ dmom, double4* __restrict__ nc4, double* __restrict__ mom,
     float4* __restrict__ mom32) {
-  extern __shared__ double s_up[];
-  double* sm = s_up + threadIdx.x * 72;
   const int cnt = lvl[level];
   const int base = level_base(lvl, level);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
@@ -885,40 +877,24 @@ __global__ void __launch_bounds__(kUpThreads) k_upward_level(
     const int pu = ti.y;
     const int cs = cfirst[P] + 1;  // level-order position of child slot 0
     const int ts = tfirst[P] + 1;  // twig-list position of the first twig child
-#pragma unroll
-    for (int k = 0; k < 8; ++k)
-      if (k < nc && !((lm >> k) & 1u)) {
-        const int64_t tp = ts + __popc(~lm & ((1u << k) - 1u));
-        const double* src = dmom + 9 * tp;
-#pragma unroll
-        for (int j = 0; j < 9; ++j) cp_async8(sm + 9 * k + j, src + j);
-      }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    double4 ca[8];
-    double2 cb[8];  // (abs_charge, bmax); a leaf's are (|q|, 0)
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      if (k < nc) {
-        const LevelRecord& r = drec[cs + k];
-        ca[k] = r.pos;
-        cb[k] = r.ab;
-      }
-    }
+    const LevelRecord* rc = drec + cs;
     double charge = 0.0, absq = 0.0;
 #pragma unroll
     for (int k = 7; k >= 0; --k)
-      if (k < nc) charge = charge + ca[k].w;
+      if (k < nc) charge = charge + rc[k].pos.w;
 #pragma unroll
     for (int k = 7; k >= 0; --k)
-      if (k < nc) absq = absq + cb[k].x;
+      if (k < nc) absq = absq + rc[k].ab.x;
     double cx = 0.0, cy = 0.0, cz = 0.0;
     if (absq != 0.0) {
 #pragma unroll
       for (int k = 7; k >= 0; --k) {
         if (k < nc) {
-          cx = cx + ca[k].x * cb[k].x;
-          cy = cy + ca[k].y * cb[k].x;
-          cz = cz + ca[k].z * cb[k].x;
+          const double4 a = rc[k].pos;
+          const double b = rc[k].ab.x;
+          cx = cx + a.x * b;
+          cy = cy + a.y * b;
+          cz = cz + a.z * b;
         }
       }
       cx = cx / absq;
@@ -928,26 +904,29 @@ __global__ void __launch_bounds__(kUpThreads) k_upward_level(
 #pragma unroll
       for (int k = 7; k >= 0; --k) {
         if (k < nc) {
-          cx = cx + ca[k].x;
-          cy = cy + ca[k].y;
-          cz = cz + ca[k].z;
+          const double4 a = rc[k].pos;
+          cx = cx + a.x;
+          cy = cy + a.y;
+          cz = cz + a.z;
         }
       }
       cx = cx / (double)nc;
       cy = cy / (double)nc;
       cz = cz / (double)nc;
     }
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
     double d0 = 0, d1 = 0, d2 = 0, q0 = 0, q1 = 0, q2 = 0, xy = 0, yz = 0, zx = 0;
     double bmax = 0.0;
 #pragma unroll
     for (int k = 7; k >= 0; --k) {
       if (k < nc) {
+        const bool lf = (lm >> k) & 1u;
+        const double* src = dmom + 9 * (int64_t)(ts + __popc(~lm & ((1u << k) - 1u)));
         double m[9];
 #pragma unroll
-        for (int j = 0; j < 9; ++j) m[j] = ((lm >> k) & 1u) ? 0.0 : sm[9 * k + j];
-        const double s0 = cx - ca[k].x, s1 = cy - ca[k].y, s2 = cz - ca[k].z;
-        const double q = ca[k].w;
+        for (int j = 0; j < 9; ++j) m[j] = lf ? 0.0 : src[j];
+        const double4 a = rc[k].pos;
+        const double s0 = cx - a.x, s1 = cy - a.y, s2 = cz - a.z;
+        const double q = a.w;
         d0 = (d0 + m[0]) + q * s0;
         d1 = (d1 + m[1]) + q * s1;
         d2 = (d2 + m[2]) + q * s2;
@@ -957,7 +936,7 @@ __global__ void __launch_bounds__(kUpThreads) k_upward_level(
         xy = (((xy + m[6]) + m[0] * s1) + m[1] * s0) + (q * s0) * s1;
         yz = (((yz + m[7]) + m[1] * s2) + m[2] * s1) + (q * s1) * s2;
         zx = (((zx + m[8]) + m[2] * s0) + m[0] * s2) + (q * s2) * s0;
-        const double v = sqrt((s0 * s0 + s1 * s1) + s2 * s2) + cb[k].y;
+        const double v = sqrt((s0 * s0 + s1 * s1) + s2 * s2) + rc[k].ab.y;
         if (k == nc - 1 || v > bmax) bmax = v;
       }
     }
@@ -1192,13 +1171,12 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
                                             c->nchild.p, c->tinfo.p, cc, tcn);
     exclusive_scan<int32_t>(cc, cc, ntw, c->scan_tmp.p, s);
     exclusive_scan<int32_t>(tcn, tcn, ntw, c->scan_tmp.p, s);
-    cudaFuncSetAttribute(k_upward_level, cudaFuncAttributeMaxDynamicSharedMemorySize, kUpSmem);
     float4* m32 = reinterpret_cast<float4*>(c->mom32.p);
     for (int L = c->max_level - 1; L >= 0; --L) {
       const int64_t cnt = c->lvl_host[L];
       if (cnt <= 0) continue;
       COUNT_LAUNCH();
-      k_upward_level<<<grid_for(cnt, kUpThreads), kUpThreads, kUpSmem, s>>>(
+      k_upward_level<<<grid_for(cnt, kUpThreads), kUpThreads, 0, s>>>(
           L, c->lvlcnt.p, c->twiglist.p, c->tinfo.p, cc, tcn, c->drec.p, c->dmom.p, c->nc4.p,
           c->mom.p, m32);
     }
