@@ -684,7 +684,8 @@ __global__ void k_build_nodes(int64_t n, int64_t M, const int64_t* __restrict__ 
 // links: parent / number of children (twigs) and key-order traversal pointers
 __global__ void k_link(int64_t M, const int2* __restrict__ meta,
                        const int32_t* __restrict__ rpo2fpo, const int32_t* __restrict__ fpo2rpo,
-                       int2* __restrict__ fwd, int32_t* __restrict__ parent,
+                       int2* __restrict__ fwd, int2* __restrict__ fwdf,
+                       int32_t* __restrict__ parent,
                        int32_t* __restrict__ nchild, int4* __restrict__ child8) {
   for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < M;
        u += (int64_t)gridDim.x * blockDim.x) {
@@ -695,6 +696,8 @@ __global__ void k_link(int64_t M, const int2* __restrict__ meta,
     int first = leaf ? (int)M : fpo2rpo[f + 1];
     int after = (f + size >= M) ? (int)M : fpo2rpo[f + size];
     fwd[u] = make_int2(first, after);
+    // the same two nodes as forward-preorder indices, the per-tile walk's visiting order
+    fwdf[u] = make_int2(leaf ? (int)M : (int)(f + 1), (f + size >= M) ? (int)M : (int)(f + size));
     if (u == 0) parent[0] = -1;
     if (!leaf) {
       int cnt = 0;
@@ -1129,7 +1132,8 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
     return PEPCG_ERR_NODE_POOL;
   }
   if (!ensure(c, c->nc4, M, "nc4") || !ensure(c, c->meta, M, "meta") ||
-      !ensure(c, c->fwd, M, "fwd") || !ensure(c, c->mom, kMomStride * M, "mom") ||
+      !ensure(c, c->fwd, M, "fwd") || !ensure(c, c->fwdf, M, "fwdf") ||
+      !ensure(c, c->mom, kMomStride * M, "mom") ||
       !ensure(c, c->mom32, 4 * kMom32Stride * M, "mom32") ||
       !ensure(c, c->parent, M, "parent") || !ensure(c, c->nchild, M, "nchild") ||
       !ensure(c, c->twiglist, M, "twiglist") || !ensure(c, c->first_part, M, "first_part") ||
@@ -1145,6 +1149,7 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
                                                   c->leafnode.p);
   COUNT_LAUNCH();
   k_link<<<grid_for(M), kThreads, 0, s>>>(M, c->meta.p, c->rpo2fpo.p, c->fpo2rpo.p, c->fwd.p,
+                                          c->fwdf.p,
                                           c->parent.p, c->nchild.p, c->child8.p);
   cudaEventRecord(c->ev[3], s);
   // twigs by level, then one launch per level, sized by the level's twig

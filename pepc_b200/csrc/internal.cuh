@@ -105,6 +105,8 @@ struct Ctx {
   DBuf<double4> nc4;
   DBuf<int2> meta;
   DBuf<int2> fwd;
+  DBuf<int2> fwdf;    // fwd's two nodes as forward-preorder indices
+  DBuf<int32_t> tflag;  // per target: the length of the tile that starts there, else 0
   // kMomStride doubles per node (96 B, three whole sectors): the 9 moments,
   // then abs_charge and bmax
   DBuf<double> mom;

@@ -54,6 +54,10 @@ struct WalkArgs {
   // per tile
   const int2* tiles;  // (first target, count)
   int64_t ntiles;
+  // packed per-tile walk
+  const int2* fwdf;     // (first child, next after the subtree) as forward-preorder indices
+  const int32_t* tflag;  // per target: length of the tile starting there, else 0
+  int tile_w;            // window of targets per warp: 33 - tile_size
 };
 
 __device__ __forceinline__ void warp_add_counters(unsigned long long* ctr, unsigned long long a,
@@ -236,6 +240,132 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_tile64(WalkArgs A) {
 // Tiles of the grown particles: tree nodes with <= T leaves whose parent has
 // more than T (the key-prefix split of tree_walk_init_aux,
 // module_tree_walk_simple.f90:168-211, is exactly this set of nodes).
+// Several reference tiles per warp (simple-walk semantics, module_tree_walk_
+// simple.f90:256-385).  Warp k takes the tiles that start in the target
+// window [W k, W k + W), W = 33 - tile_size, so their targets fit the 32
+// lanes.  Every tile walks the tree in forward preorder (children first to
+// last); the warp steps through the union of its tiles' walks in that order:
+// at each step the lanes whose tile stands at the smallest forward-preorder
+// index f evaluate node f together (one load for all of them), and each tile
+// decides accept / open by a ballot over its own lanes.  A lane's sequence of
+// interactions is exactly its tile's, so fields, work and MAC counts equal
+// the one-tile-per-warp walk's.
+template <int kLaw>
+__global__ void __launch_bounds__(kWalkThreads) k_walk_tilepack64(WalkArgs A) {
+  __shared__ double s_bl2[kMaxLevel + 1];
+  __shared__ double s_vb[3 * 125];
+  for (int i = threadIdx.x; i <= kMaxLevel; i += blockDim.x) s_bl2[i] = A.bl2[i];
+  for (int i = threadIdx.x; i < 3 * A.nbox; i += blockDim.x) s_vb[i] = A.vbox[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const unsigned M = (unsigned)A.M;
+  const int W = A.tile_w;
+  const int64_t nwin = (A.nt + W - 1) / W;
+  unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
+  for (;;) {
+    unsigned b = 0;
+    if (lane == 0) b = atomicAdd(&g_bucket_counter, 1u);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    if ((int64_t)b >= nwin) break;
+    const int64_t base = (int64_t)b * W;
+    // tile starts in the window
+    const int fl = (lane < W && base + lane < A.nt) ? A.tflag[base + lane] : 0;
+    const unsigned starts = __ballot_sync(0xffffffffu, fl > 0);
+    if (starts == 0) continue;
+    const int s0 = __ffs(starts) - 1;
+    const int64_t t0 = base + s0;
+    // this lane's target and tile: the last start at or before it within the window
+    const int wl = s0 + lane;
+    const unsigned upto = wl >= 31 ? starts : (starts & ((2u << wl) - 1u));
+    const int sl = 31 - __clz(upto);
+    const int len = __shfl_sync(0xffffffffu, fl, sl);
+    const int64_t t = t0 + lane;
+    const int tl0 = sl - s0;  // first lane of this lane's tile
+    const bool valid = t < A.nt && lane < tl0 + len;
+    const unsigned tmask = valid ? (((len >= 32) ? 0xffffffffu : ((1u << len) - 1u)) << tl0) : 0u;
+    double px = 0, py = 0, pz = 0, e0 = 0, e1 = 0, e2 = 0, ph = 0, w = 0;
+    KelbgArgs kel{0.0, A.kinv, A.sqrtpi};
+    if (valid) {
+      px = A.tx[t]; py = A.ty[t]; pz = A.tz[t];
+      if (kLaw == 5) kel.tq = A.tq[t];
+      e0 = A.ex[t]; e1 = A.ey[t]; e2 = A.ez[t]; ph = A.pot[t]; w = A.work[t];
+    }
+    bool complete = true;
+    for (int ib = 0; ib < A.nbox; ++ib) {
+      const double vx = s_vb[3 * ib], vy = s_vb[3 * ib + 1], vz = s_vb[3 * ib + 2];
+      unsigned u = 0, uf = 0;  // tree_walk_single_aux starts at the root (:286)
+      int64_t partner = 0;
+      for (;;) {
+        const unsigned f = __reduce_min_sync(0xffffffffu, valid ? uf : 0xffffffffu);
+        if (f >= M) break;
+        // the lanes at node f: whole tiles, all at the same node, so they take
+        // the same branch below
+        const unsigned am = __ballot_sync(0xffffffffu, valid && uf == f);
+        if (valid && uf == f) {
+          const double4 a = A.nc4[u];
+          const int2 mu = A.meta[u];
+          const int2 fw = A.fwd[u];
+          const int2 ff = A.fwdf[u];
+          // d = (x - vbox) - coc (module_tree_walk_simple.f90:328,345)
+          const double dx = (px - vx) - a.x, dy = (py - vy) - a.y, dz = (pz - vz) - a.z;
+          const double dist2 = (dx * dx + dy * dy) + dz * dz;
+          if (mu.y & kLeafFlag) {
+            partner += 1;
+            w += 1.0;
+            ++c_leaf;
+            if (dist2 > 0.0) {
+              double fx, fy, fz, fp;
+              law_leaf64<kLaw>(a.w, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp, kel);
+              e0 += fx; e1 += fy; e2 += fz; ph += fp;
+            }
+            u = (unsigned)fw.y;
+            uf = (unsigned)ff.y;
+          } else {
+            const bool ok = A.theta2 * dist2 > (A.macb ? A.macb[u] : s_bl2[mu.y & 0xff]);
+            const unsigned tf = __ballot_sync(am, !ok) & tmask;
+            // MAC evaluations stop at the tile's first failing target (:343-370)
+            const int first_fail = tf ? __ffs(tf) - 1 : 32;
+            if (lane <= first_fail) ++c_mac;
+            if (tf == 0) {
+              partner += A.nleaves[u];
+              double m[9];
+#pragma unroll
+              for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
+              double fx, fy, fz, fp;
+              law_twig64<kLaw>(a.w, m, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp);
+              e0 += fx; e1 += fy; e2 += fz; ph += fp;
+              w += 1.0;
+              ++c_twig;
+              u = (unsigned)fw.y;
+              uf = (unsigned)ff.y;
+            } else {
+              u = (unsigned)fw.x;
+              uf = (unsigned)ff.x;
+            }
+          }
+        }
+        __syncwarp();
+      }
+      if (valid && partner != A.npart) complete = false;
+    }
+    if (valid) {
+      A.ex[t] = e0; A.ey[t] = e1; A.ez[t] = e2; A.pot[t] = ph; A.work[t] = w;
+    }
+    if (__any_sync(0xffffffffu, !complete) && lane == 0) atomicOr(A.status, ST_INCOMPLETE);
+  }
+  warp_add_counters(A.counters, c_leaf, c_twig, c_mac);
+}
+
+// per-target tile lengths from the compact (first, count) list
+__global__ void k_tile_flags(int64_t ntiles, const int2* __restrict__ tiles,
+                             int32_t* __restrict__ tflag) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ntiles;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int2 tl = tiles[i];
+    tflag[tl.x] = tl.y;
+  }
+}
+
 __global__ void k_tiles_from_tree(int32_t M, int T, const int32_t* __restrict__ nleaves,
                                   const int32_t* __restrict__ parent,
                                   const int32_t* __restrict__ first_part, int2* tiles,
@@ -365,6 +495,17 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
       if (rc) return rc;
     }
   }
+  // plain per-tile walk with tiles of <= 16 targets: several tiles per warp
+  const bool packed = walk == PEPCG_WALK_PER_TILE && c->prm.precision == PEPCG_PRECISION_PLAIN &&
+                      c->prm.tile_size <= 16;
+  if (packed) {
+    if (!ensure(c, c->tflag, nt, "tile flags")) return PEPCG_ERR_OOM;
+    if (!cuda_ok(c, cudaMemsetAsync(c->tflag.p, 0, nt * sizeof(int32_t), s), "tile flags"))
+      return PEPCG_ERR_CUDA;
+    COUNT_LAUNCH();
+    k_tile_flags<<<296, 256, 0, s>>>(ntiles, reinterpret_cast<const int2*>(c->tiles.p),
+                                     c->tflag.p);
+  }
   const int nchunks = plan ? plan->nchunks : 1;
   if (nchunks > 1) {
     bool ok = walk != PEPCG_WALK_PER_TILE && !c->far_field && nchunks <= Ctx::kMaxChunks &&
@@ -399,6 +540,9 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
   A.ntiles = ntiles;
   A.kinv = c->prm.kelbg_invsqrttemp;
   A.sqrtpi = std::sqrt(std::acos(-1.0));
+  A.fwdf = c->fwdf.p;
+  A.tflag = c->tflag.p;
+  A.tile_w = 33 - (c->prm.tile_size < 1 ? 1 : c->prm.tile_size);
   const int blocks = 148 * 8;
   for (int k = 0; k < nchunks; ++k) {
     const int64_t t0 = nchunks > 1 ? plan->bounds[k] : 0;
@@ -421,6 +565,11 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
           else if (law == 4) k_walk_target64<4><<<blocks, kWalkThreads, 0, s>>>(A);
           else if (law == 5) k_walk_target64<5><<<blocks, kWalkThreads, 0, s>>>(A);
           else k_walk_target64<3><<<blocks, kWalkThreads, 0, s>>>(A);
+        } else if (packed) {
+          if (law == 2) k_walk_tilepack64<2><<<blocks, kWalkThreads, 0, s>>>(A);
+          else if (law == 4) k_walk_tilepack64<4><<<blocks, kWalkThreads, 0, s>>>(A);
+          else if (law == 5) k_walk_tilepack64<5><<<blocks, kWalkThreads, 0, s>>>(A);
+          else k_walk_tilepack64<3><<<blocks, kWalkThreads, 0, s>>>(A);
         } else {
           if (walk == PEPCG_WALK_GROUP) A.tiles = nullptr;
           if (law == 2) k_walk_tile64<2><<<blocks, kWalkThreads, 0, s>>>(A);
