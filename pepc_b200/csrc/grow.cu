@@ -107,7 +107,6 @@ __global__ void k_bbox_final(int nparts, const double* __restrict__ part, int cu
 // Keys: compute_particle_keys (module_spacefilling.f90:224-257) with
 // intcoord_to_key_hilbert3D (:380-440) or the 3D Morton interleave.
 // ---------------------------------------------------------------------------
-__constant__ int8_t c_CI3[8] = {0, 1, 3, 2, 7, 6, 4, 5};  // :389
 __constant__ int8_t c_G3x[8] = {5, 6, 0, 5, 5, 0, 6, 5};  // :390 exchange
 __constant__ int8_t c_G3r[8] = {0, 0, 0, 5, 0, 0, 6, 5};  // :390 reverse
 
