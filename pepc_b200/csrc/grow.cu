@@ -600,8 +600,11 @@ __global__ void k_node_counts(int64_t n, const int64_t* __restrict__ key,
                               int32_t* __restrict__ cstart, int32_t* __restrict__ cend,
                               uint32_t* status, int* maxlev, int32_t* __restrict__ lvl) {
   __shared__ int h[kMaxLevel + 1];
+  __shared__ int bmax;
   if (threadIdx.x <= kMaxLevel) h[threadIdx.x] = 0;
+  if (threadIdx.x == 0) bmax = 0;
   __syncthreads();
+  int mymax = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     uint64_t k = (uint64_t)key[i];
@@ -614,12 +617,16 @@ __global__ void k_node_counts(int64_t n, const int64_t* __restrict__ key,
     }
     lev[i] = (int8_t)l;
     lcpn[i] = (int8_t)ln;
-    if (l > 0) atomicMax(maxlev, l);
+    mymax = max(mymax, l);
     cstart[i] = l - (lp + 1) + 1;
     cend[i] = l - ln;
     for (int L = lp + 1; L < l; ++L) atomicAdd(&h[L], 1);
   }
+  // the deepest leaf level: one global atomic per block
+  for (int o = 16; o > 0; o >>= 1) mymax = max(mymax, __shfl_xor_sync(0xffffffffu, mymax, o));
+  if ((threadIdx.x & 31) == 0 && mymax > 0) atomicMax(&bmax, mymax);
   __syncthreads();
+  if (threadIdx.x == 0 && bmax > 0) atomicMax(maxlev, bmax);
   if (threadIdx.x <= kMaxLevel && h[threadIdx.x]) atomicAdd(&lvl[threadIdx.x], h[threadIdx.x]);
 }
 
