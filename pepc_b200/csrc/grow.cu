@@ -28,16 +28,29 @@ __global__ void k_bbox_partial(int64_t n, const double* __restrict__ x,
   double lo[3] = {INFINITY, INFINITY, INFINITY};
   double hi[3] = {-INFINITY, -INFINITY, -INFINITY};
   bool bad = false;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    double v[3] = {x[i], y[i], z[i]};
+  auto take = [&](double vx, double vy, double vz) {
+    const double v[3] = {vx, vy, vz};
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       bad |= !isfinite(v[d]);
       lo[d] = fmin(lo[d], v[d]);
       hi[d] = fmax(hi[d], v[d]);
     }
+  };
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  for (; i + 3 * stride < n; i += 4 * stride) {  // four particles' loads in flight
+    double vx[4], vy[4], vz[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      vx[j] = x[i + j * stride];
+      vy[j] = y[i + j * stride];
+      vz[j] = z[i + j * stride];
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) take(vx[j], vy[j], vz[j]);
   }
+  for (; i < n; i += stride) take(x[i], y[i], z[i]);
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(status, ST_NONFINITE);
   __shared__ double s[6][kThreads / 32];
 #pragma unroll
@@ -1065,7 +1078,7 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
 
   cudaEventRecord(c->ev[0], s);
   // box
-  const int nbb = 296;
+  const int nbb = 512;  // the partials buffer holds 6 x 512
   double* part = c->d_part;  // 6 * nbb doubles
   COUNT_LAUNCH();
   k_bbox_partial<<<nbb, kThreads, 0, s>>>(n, dx, dy, dz, part, c->d_status);
