@@ -92,8 +92,9 @@ def test_walk_per_target_bit_exact(gpu, theta2):
     assert st["mac_evaluations"] == c["mac_evaluations"]
 
 
-@pytest.mark.parametrize("tile", [16, 32, 1])
+@pytest.mark.parametrize("tile", [16, 32, 1, 7])
 def test_walk_per_tile_bit_exact(gpu, tile):
+    # tile sizes up to 16 run several tiles per warp (windows of 33 - T targets)
     x, y, z, q = cube(12000, 22, charges="gauss")
     tc, orc, g, go = grow_both(x, y, z, q, theta2=0.16, eps2=1e-6, walk=P.WALK_PER_TILE,
                                tile_size=tile)
