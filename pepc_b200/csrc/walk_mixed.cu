@@ -61,6 +61,11 @@ struct MixArgs {
   uint32_t* status;
   const int2* tiles;  // PER_TILE tiles, or nullptr for GROUP (implicit 32-target buckets)
   int64_t ntiles;
+  // packed per-tile walk
+  const int2* fwd;       // (first child, next after the subtree), RPO indices
+  const int2* fwdf;      // the same as forward-preorder indices
+  const int32_t* tflag;  // per target: length of the tile starting there, else 0
+  int tile_w;            // window of targets per warp: 33 - tile_size
 };
 
 __device__ __forceinline__ void leaf32(float q, float dx, float dy, float dz, float eps2,
@@ -411,6 +416,115 @@ __global__ void __launch_bounds__(kMixThreads, 5)
   warp_add3(A.counters, c_leaf, c_twig, c_mac);
 }
 
+// Simple-walk semantics (module_tree_walk_simple.f90:256-385) with several
+// reference tiles per warp and FP32 interactions: the tiles that start in
+// the target window [W k, W k + W), W = 33 - tile_size, walk the tree
+// together in forward preorder -- at each step the lanes whose tile stands at
+// the smallest forward-preorder index evaluate that node, and each tile
+// decides accept / open by a ballot over its own lanes (the MAC on the FP32
+// offsets, target minus node centre formed in FP64).  Sums as in the
+// per-target mixed walk: FP32 over chunks of kChunk steps, then FP64.
+__global__ void __launch_bounds__(kMixThreads) k_walk_tilepack_mixed(MixArgs A) {
+  __shared__ float s_bl2[kMaxLevel + 1];
+  __shared__ double s_vb[3 * 125];
+  for (int i = threadIdx.x; i <= kMaxLevel; i += blockDim.x) s_bl2[i] = (float)A.bl2[i];
+  for (int i = threadIdx.x; i < 3 * A.nbox; i += blockDim.x) s_vb[i] = A.vbox[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const unsigned M = (unsigned)A.M;
+  const int W = A.tile_w;
+  const int64_t nwin = (A.nt + W - 1) / W;
+  unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
+  for (;;) {
+    unsigned b = 0;
+    if (lane == 0) b = atomicAdd(&g_bucket_counter_mixed, 1u);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    if ((int64_t)b >= nwin) break;
+    const int64_t base = (int64_t)b * W;
+    const int fl = (lane < W && base + lane < A.nt) ? A.tflag[base + lane] : 0;
+    const unsigned starts = __ballot_sync(0xffffffffu, fl > 0);
+    if (starts == 0) continue;
+    const int s0 = __ffs(starts) - 1;
+    const int wl = s0 + lane;
+    const unsigned upto = wl >= 31 ? starts : (starts & ((2u << wl) - 1u));
+    const int sl = 31 - __clz(upto);
+    const int len = __shfl_sync(0xffffffffu, fl, sl);
+    const int64_t t = base + s0 + lane;
+    const int tl0 = sl - s0;  // first lane of this lane's tile
+    const bool valid = t < A.nt && lane < tl0 + len;
+    const unsigned tmask = valid ? (((len >= 32) ? 0xffffffffu : ((1u << len) - 1u)) << tl0) : 0u;
+    double px = 0, py = 0, pz = 0, E0 = 0, E1 = 0, E2 = 0, PH = 0, W8 = 0;
+    if (valid) {
+      px = A.tx[t]; py = A.ty[t]; pz = A.tz[t];
+      E0 = A.ex[t]; E1 = A.ey[t]; E2 = A.ez[t]; PH = A.pot[t]; W8 = A.work[t];
+    }
+    bool complete = true;
+    for (int ib = 0; ib < A.nbox; ++ib) {
+      const double sx = px - s_vb[3 * ib], sy = py - s_vb[3 * ib + 1], sz = pz - s_vb[3 * ib + 2];
+      float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
+      int steps = 0;
+      unsigned u = 0, uf = 0;  // the root
+      int64_t partner = 0;
+      for (;;) {
+        const unsigned f = __reduce_min_sync(0xffffffffu, valid ? uf : 0xffffffffu);
+        if (f >= M) break;
+        // the lanes at node f: whole tiles at the same node
+        const unsigned am = __ballot_sync(0xffffffffu, valid && uf == f);
+        if (valid && uf == f) {
+          const double4 a = A.nc4[u];
+          const int2 mu = A.meta[u];
+          const int2 fw = A.fwd[u];
+          const int2 ff = A.fwdf[u];
+          const double dx64 = sx - a.x, dy64 = sy - a.y, dz64 = sz - a.z;
+          const float dx = (float)dx64, dy = (float)dy64, dz = (float)dz64;
+          if (mu.y & kLeafFlag) {
+            partner += 1;
+            W8 += 1.0;
+            if (!(dx64 == 0.0 && dy64 == 0.0 && dz64 == 0.0)) {
+              leaf32((float)a.w, dx, dy, dz, A.eps2, ax, ay, az, ap);
+              ++c_leaf;
+            }
+            u = (unsigned)fw.y;
+            uf = (unsigned)ff.y;
+          } else {
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const bool ok = A.theta2 * r2 > (A.macb ? (float)A.macb[u] : s_bl2[mu.y & 0xff]);
+            const unsigned tf = __ballot_sync(am, !ok) & tmask;
+            // MAC evaluations stop at the tile's first failing target
+            const int first_fail = tf ? __ffs(tf) - 1 : 32;
+            if (lane <= first_fail) ++c_mac;
+            if (tf == 0) {
+              partner += A.nleaves[u];
+              const float4* mu4 = A.mom32 + kMom32Stride * (int64_t)u;
+              twig32(mu4[0], mu4[1], mu4[2], dx, dy, dz, A.eps2, ax, ay, az, ap);
+              ++c_twig;
+              W8 += 1.0;
+              u = (unsigned)fw.y;
+              uf = (unsigned)ff.y;
+            } else {
+              u = (unsigned)fw.x;
+              uf = (unsigned)ff.x;
+            }
+          }
+          if (++steps == kChunk) {
+            E0 += (double)ax; E1 += (double)ay; E2 += (double)az; PH += (double)ap;
+            ax = ay = az = ap = 0.f;
+            steps = 0;
+          }
+        }
+        __syncwarp();
+      }
+      E0 += (double)ax; E1 += (double)ay; E2 += (double)az; PH += (double)ap;
+      if (valid && partner != A.npart) complete = false;
+    }
+    if (valid) {
+      A.ex[t] = E0; A.ey[t] = E1; A.ez[t] = E2; A.pot[t] = PH; A.work[t] = W8;
+    }
+    if (__any_sync(0xffffffffu, !complete) && lane == 0) atomicOr(A.status, ST_INCOMPLETE);
+  }
+  warp_add3(A.counters, c_leaf, c_twig, c_mac);
+}
+
 // per-target semantics (module_tree_walk_pthreads.f90:558-765) with FP32
 // interactions; the MAC is evaluated on the FP32 offsets
 __global__ void __launch_bounds__(kMixThreads) k_walk_target_mixed(MixArgs A) {
@@ -496,7 +610,8 @@ __global__ void k_reset_mixed() { g_bucket_counter_mixed = 0; }
 
 int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                       double* ex, double* ey, double* ez, double* pot, double* work,
-                      const int2* tiles, int64_t ntiles, bool per_target) {
+                      const int2* tiles, int64_t ntiles, bool per_target,
+                      const int32_t* tflag) {
   MixArgs A;
   A.nt = nt;
   A.tx = tx; A.ty = ty; A.tz = tz;
@@ -520,12 +635,18 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
   A.status = c->d_status;
   A.tiles = tiles;
   A.ntiles = ntiles;
+  A.fwd = c->fwd.p;
+  A.fwdf = c->fwdf.p;
+  A.tflag = tflag;
+  A.tile_w = 33 - (c->prm.tile_size < 1 ? 1 : c->prm.tile_size);
   cudaStream_t s = c->stream;
   COUNT_LAUNCH();
   k_reset_mixed<<<1, 1, 0, s>>>();
   COUNT_LAUNCH();
   if (per_target) {
     k_walk_target_mixed<<<148 * 8, kMixThreads, 0, s>>>(A);
+  } else if (tflag) {
+    k_walk_tilepack_mixed<<<148 * 8, kMixThreads, 0, s>>>(A);
   } else {
     // 5 resident blocks per SM (launch bounds: 96 registers, 31.8 KB shared
     // memory each); the grid is exactly one wave

@@ -414,7 +414,7 @@ __global__ void k_mac_thresholds(int64_t M, int mode, const int2* __restrict__ m
 
 int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                       double* ex, double* ey, double* ez, double* pot, double* work,
-                      const int2* tiles, int64_t ntiles, bool per_target);
+                      const int2* tiles, int64_t ntiles, bool per_target, const int32_t* tflag);
 
 const double* grown_charges_if_same(Ctx* c, int64_t nt, const int64_t* d_tkeys) {
   if (!d_tkeys || nt != c->n) return nullptr;
@@ -495,9 +495,8 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
       if (rc) return rc;
     }
   }
-  // plain per-tile walk with tiles of <= 16 targets: several tiles per warp
-  const bool packed = walk == PEPCG_WALK_PER_TILE && c->prm.precision == PEPCG_PRECISION_PLAIN &&
-                      c->prm.tile_size <= 16;
+  // per-tile walk with tiles of <= 16 targets: several tiles per warp
+  const bool packed = walk == PEPCG_WALK_PER_TILE && c->prm.tile_size <= 16;
   if (packed) {
     if (!ensure(c, c->tflag, nt, "tile flags")) return PEPCG_ERR_OOM;
     if (!cuda_ok(c, cudaMemsetAsync(c->tflag.p, 0, nt * sizeof(int32_t), s), "tile flags"))
@@ -580,7 +579,7 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
       } else {
         int rc = launch_walk_mixed(c, t1 - t0, A.tx, A.ty, A.tz, A.ex, A.ey, A.ez, A.pot, A.work,
                                    walk == PEPCG_WALK_PER_TILE ? A.tiles : nullptr, ntiles,
-                                   walk == PEPCG_WALK_PER_TARGET);
+                                   walk == PEPCG_WALK_PER_TARGET, packed ? c->tflag.p : nullptr);
         if (rc) return rc;
       }
       if (!cuda_ok(c, cudaGetLastError(), "walk launch")) return PEPCG_ERR_CUDA;
