@@ -48,6 +48,22 @@ def test_chunked_host_traverse_equals_device_path(gpu, precision, walk, overwrit
     tc.close()
 
 
+def test_chunked_host_traverse_ragged_count(gpu):
+    """A target count that is not a multiple of 32: the last chunk is ragged."""
+    n = 262144 + 1001
+    rng = np.random.default_rng(19)
+    x, y, z = rng.random(n), rng.random(n), rng.random(n)
+    q = rng.standard_normal(n) / n
+    tc = P.TreeCode(theta2=0.16, eps2=1e-6, precision=P.PRECISION_MIXED, walk=P.WALK_GROUP,
+                    overwrite_results=1)
+    ref = device_fields(tc, x, y, z, q)
+    g = tc.pepc_grow_tree(x, y, z, q)
+    r = tc.pepc_traverse_tree(g.x, g.y, g.z, keys=g.key)
+    for k, name in enumerate(("ex", "ey", "ez", "pot", "work")):
+        assert np.array_equal(r[name], ref[k]), name
+    tc.close()
+
+
 def test_host_grow_outputs_and_a_following_traverse(gpu):
     """Grow returns while the upward pass may still run; the next traverse is
     stream-ordered after it."""
