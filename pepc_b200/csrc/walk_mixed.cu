@@ -471,10 +471,14 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_tilepack_mixed(MixArgs A) 
         // the lanes at node f: whole tiles at the same node
         const unsigned am = __ballot_sync(0xffffffffu, valid && uf == f);
         if (valid && uf == f) {
+          // one round of loads, the moments and leaf count included
           const double4 a = A.nc4[u];
           const int2 mu = A.meta[u];
           const int2 fw = A.fwd[u];
           const int2 ff = A.fwdf[u];
+          const float4* mu4 = A.mom32 + kMom32Stride * (int64_t)u;
+          const float4 m0 = mu4[0], m1 = mu4[1], m2 = mu4[2];
+          const int nlv = A.nleaves[u];
           const double dx64 = sx - a.x, dy64 = sy - a.y, dz64 = sz - a.z;
           const float dx = (float)dx64, dy = (float)dy64, dz = (float)dz64;
           if (mu.y & kLeafFlag) {
@@ -494,9 +498,8 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_tilepack_mixed(MixArgs A) 
             const int first_fail = tf ? __ffs(tf) - 1 : 32;
             if (lane <= first_fail) ++c_mac;
             if (tf == 0) {
-              partner += A.nleaves[u];
-              const float4* mu4 = A.mom32 + kMom32Stride * (int64_t)u;
-              twig32(mu4[0], mu4[1], mu4[2], dx, dy, dz, A.eps2, ax, ay, az, ap);
+              partner += nlv;
+              twig32(m0, m1, m2, dx, dy, dz, A.eps2, ax, ay, az, ap);
               ++c_twig;
               W8 += 1.0;
               u = (unsigned)fw.y;
@@ -559,8 +562,13 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_target_mixed(MixArgs A) {
         const unsigned u = __reduce_min_sync(0xffffffffu, next);
         if (u >= M) break;
         if (next == u) {
+          // one round of loads: the moments and leaf count are requested with
+          // the centre, before the MAC decides whether they are used
           const double4 a = A.nc4[u];
           const int2 mu = A.meta[u];
+          const float4* mu4 = A.mom32 + kMom32Stride * (int64_t)u;
+          const float4 m0 = mu4[0], m1 = mu4[1], m2 = mu4[2];
+          const int nlv = A.nleaves[u];
           const double dx64 = sx - a.x, dy64 = sy - a.y, dz64 = sz - a.z;
           const float dx = (float)dx64, dy = (float)dy64, dz = (float)dz64;
           if (mu.y & kLeafFlag) {
@@ -575,9 +583,7 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_target_mixed(MixArgs A) {
             ++c_mac;
             const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             if (A.theta2 * r2 > (A.macb ? (float)A.macb[u] : s_bl2[mu.y & 0xff])) {
-              partner += A.nleaves[u];
-              const float4* mu4 = A.mom32 + kMom32Stride * (int64_t)u;
-              const float4 m0 = mu4[0], m1 = mu4[1], m2 = mu4[2];
+              partner += nlv;
               twig32(m0, m1, m2, dx, dy, dz, A.eps2, ax, ay, az, ap);
               ++c_twig;
               W += 1.0;
