@@ -353,11 +353,12 @@ def run_madelung(args, P, torch, dev, stream):
 
 
 def run_sharded(args, P, torch, dev, stream, dist, rank, world, local):
-    """Target sharding (strong scaling): every rank grows the same tree from the
-    same particles, walks its shard_range share of the key-ordered targets
-    (pepcg_traverse_range_device) and all-gathers the shares' fields
-    (gather_shards), so that every rank ends the step with all N fields.  The
-    step time is the slowest rank's; the job's rate is N per step."""
+    """Target sharding (strong scaling): rank 0's particles are broadcast, every
+    rank grows the same tree from them, walks its shard_range share of the
+    key-ordered targets (pepcg_traverse_range_device) and all-gathers the
+    shares' fields (gather_shards), so that every rank ends the step with all
+    N fields.  The step time is the slowest rank's; the job's rate is N per
+    step."""
     x, y, z, q = plummer(args.n)
     n = args.n
     tx, ty, tz, tq = (torch.from_numpy(a).to(dev) for a in (x, y, z, q))
@@ -371,6 +372,11 @@ def run_sharded(args, P, torch, dev, stream, dist, rank, world, local):
     full = [None]
 
     def step():
+        # the particles as rank 0 holds them, broadcast to every rank (32 B per
+        # particle over NVLink), then the same grow on every rank
+        if dist:
+            for a in (tx, ty, tz, tq):
+                dist.broadcast(a, src=0)
         share.zero_()
         tc.grow_tree_device(tx, ty, tz, tq)
         tc.traverse_range_device(t0, t1, *share)
@@ -408,8 +414,8 @@ def run_sharded(args, P, torch, dev, stream, dist, rank, world, local):
             "data": "synthetic",
             "config": {"workload": workload_name(args), "precision": args.precision,
                        "walk": args.walk,
-                       "parallelism": f"target shards over {world} ranks (replicated tree) "
-                                      "+ all-gather of the fields"},
+                       "parallelism": f"target shards over {world} ranks: broadcast of the "
+                                      "particles, replicated tree, all-gather of the fields"},
             "fields_equal_single_call": same, "gpu_launches": launches}), flush=True)
 
 
