@@ -242,27 +242,29 @@ __global__ void k_sort_hist(int64_t n, const uint64_t* __restrict__ keys, int sh
   hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
-// Stable scatter of one 4096-key tile.  Warp w owns the tile's keys
-// [512 w, 512 w + 512) and reads them in one round (16 per lane, coalesced);
-// it ranks them among themselves by digit, in order (warp match, the digit's
-// running count in shared memory, updated by the peers' leader), with no
-// block barrier; the per-digit counts are then prefixed over the warps, which
-// keeps the ranks stable, and over the digits, which gives each digit's run
-// in the tile.  The tile is sorted by digit in shared memory and written out
-// in that order, so that consecutive threads store consecutive addresses of a
-// digit's run in the output (the run of digit d of tile b starts at
-// offs[d * nblocks + b]).
 // barrier for the first 256 threads of the block only (the digit lanes)
 __device__ __forceinline__ void named_barrier_256() {
   asm volatile("bar.sync 1, 256;\n" ::: "memory");
 }
 
+// Stable scatter of one 4096-key tile.  Warp w owns the tile's keys
+// [256 w, 256 w + 256) and reads their digits in one round (8 per lane,
+// coalesced); it ranks them among themselves by digit, in order -- the lanes
+// sharing a digit from one ballot per digit bit, the digit's running count in
+// shared memory, updated by the peers' leader -- with no block barrier.  The
+// per-digit counts are then prefixed over the warps, which keeps the ranks
+// stable, and over the digits, which gives each digit's run in the tile.
+// The tile is sorted by digit in shared memory (the keys and indices re-read
+// from global memory, which keeps the kernel at 40 registers and three blocks
+// per SM) and written out in that order, so that consecutive threads store
+// consecutive addresses of a digit's run in the output (the run of digit d of
+// tile b starts at offs[d * nblocks + b]).
 constexpr int kScatterThreads = 512;
 constexpr int kWarpsSort = kScatterThreads / 32;
 constexpr int kPerWarp = kSortChunk / kWarpsSort;  // 256 keys
 constexpr int kScatterSmem = kSortChunk * 8 + kSortChunk * 4 + 2 * 256 * 4 + kWarpsSort * 256 * 4;
 
-__global__ void __launch_bounds__(kScatterThreads, 2) k_sort_scatter(int64_t n, const uint64_t* __restrict__ kin,
+__global__ void __launch_bounds__(kScatterThreads, 3) k_sort_scatter(int64_t n, const uint64_t* __restrict__ kin,
                                                            const int32_t* __restrict__ vin,
                                                            uint64_t* __restrict__ kout,
                                                            int32_t* __restrict__ vout, int shift,
@@ -281,13 +283,11 @@ __global__ void __launch_bounds__(kScatterThreads, 2) k_sort_scatter(int64_t n, 
   const int cnt = (int)min((int64_t)kSortChunk, n - base);
   if (threadIdx.x < 256) gbase[threadIdx.x] = offs[(int64_t)threadIdx.x * nblocks + blockIdx.x];
   for (int i = threadIdx.x; i < kWarpsSort * 256; i += kScatterThreads) (&wcnt[0][0])[i] = 0;
-  uint64_t kr[kPerWarp / 32];
-  int32_t vr[kPerWarp / 32];
+  uint8_t dg[kPerWarp / 32];
 #pragma unroll
   for (int j = 0; j < kPerWarp / 32; ++j) {
     const int i = warp * kPerWarp + j * 32 + lane;
-    kr[j] = i < cnt ? kin[base + i] : 0;
-    vr[j] = i < cnt ? vin[base + i] : 0;
+    dg[j] = i < cnt ? (uint8_t)((kin[base + i] >> shift) & 255u) : 0;
   }
   __syncthreads();
   int rk[kPerWarp / 32];
@@ -295,8 +295,16 @@ __global__ void __launch_bounds__(kScatterThreads, 2) k_sort_scatter(int64_t n, 
 #pragma unroll
   for (int j = 0; j < kPerWarp / 32; ++j) {
     const bool valid = warp * kPerWarp + j * 32 + lane < cnt;
-    const int d = (int)((kr[j] >> shift) & 255u);
-    const unsigned peers = __match_any_sync(0xffffffffu, valid ? d : 256);
+    const int d = dg[j];
+    // the lanes with this lane's digit, from one ballot per digit bit
+    unsigned peers = __ballot_sync(0xffffffffu, valid);
+    if (!valid) peers = ~peers;
+#pragma unroll
+    for (int bit = 0; bit < 8; ++bit) {
+      const bool on = (d >> bit) & 1;
+      const unsigned m = __ballot_sync(0xffffffffu, on);
+      peers &= on ? m : ~m;
+    }
     const int leader = __ffs(peers) - 1;
     uint32_t c0 = 0;
     if (valid && lane == leader) c0 = my[d];
@@ -330,11 +338,12 @@ __global__ void __launch_bounds__(kScatterThreads, 2) k_sort_scatter(int64_t n, 
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < kPerWarp / 32; ++j) {
-    if (warp * kPerWarp + j * 32 + lane < cnt) {
-      const int d = (int)((kr[j] >> shift) & 255u);
+    const int i = warp * kPerWarp + j * 32 + lane;
+    if (i < cnt) {
+      const int d = dg[j];
       const int pos = (int)(lstart[d] + wcnt[warp][d]) + rk[j];
-      sk[pos] = kr[j];
-      sv[pos] = vr[j];
+      sk[pos] = kin[base + i];
+      sv[pos] = vin[base + i];
     }
   }
   __syncthreads();
@@ -777,7 +786,15 @@ __global__ void __launch_bounds__(256) k_level_count(int64_t M, const int2* __re
 // rank of this lane among the block's lanes with the same key (-1: none),
 // in block order, plus the warp-level prefix held in wc[warp][key]
 __device__ __forceinline__ int block_rank(int key, int warp, int lane, int (*wc)[kMaxLevel + 1]) {
-  const unsigned peers = __match_any_sync(0xffffffffu, key);
+  // the lanes with this lane's key (-1 .. 20), from one ballot per bit of key + 1
+  const int kk = key + 1;
+  unsigned peers = 0xffffffffu;
+#pragma unroll
+  for (int bit = 0; bit < 5; ++bit) {
+    const bool on = (kk >> bit) & 1;
+    const unsigned m = __ballot_sync(0xffffffffu, on);
+    peers &= on ? m : ~m;
+  }
   const int lrank = __popc(peers & ((1u << lane) - 1u));
   if (key >= 0 && lane == __ffs(peers) - 1) wc[warp][key] = __popc(peers);
   return lrank;
