@@ -58,7 +58,9 @@ def plummer(n, seed=3, rmax=20.0):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region (200 ms period)."""
+    """nvidia-smi sampling during the timed region (50 ms period).  Entering waits
+    for the sampler's first row (nvidia-smi takes a while to start) and drops
+    it, so that the rows kept are the ones taken while the timed steps run."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -73,10 +75,14 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 5.0:
+                time.sleep(0.01)
+            self.rows = []
         except Exception:
             self.proc = None
         return self
