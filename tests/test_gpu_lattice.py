@@ -97,3 +97,24 @@ def test_not_neutral_is_a_warning(gpu):
     assert tc.last_status == P.PEPCG_WARN_NOT_NEUTRAL
     r = tc.pepc_traverse_tree(x, y, z)
     assert np.all(np.isfinite(r["pot"]))
+
+
+@pytest.mark.parametrize("walk", [P.WALK_PER_TARGET, P.WALK_PER_TILE])
+def test_periodic_near_field_bit_exact(gpu, walk):
+    """The 27-box near field alone (no lattice term) is the walk's arithmetic
+    only, so both plain walks must equal the oracle bit for bit; the per-tile
+    walk packs its 16-target tiles into shared warps."""
+    rng = np.random.default_rng(53)
+    n = 4000
+    x, y, z = rng.random(n), rng.random(n), rng.random(n)
+    q = rng.standard_normal(n)
+    kw = dict(theta2=0.25, eps2=1e-4, periodicity=(1, 1, 1), include_far_field_if_periodic=0)
+    tc = P.TreeCode(walk=walk, **kw)
+    orc = O.Oracle(walk=0 if walk == P.WALK_PER_TARGET else 1, num_threads=8, **kw)
+    g = tc.pepc_grow_tree(x, y, z, q)
+    go = orc.grow_tree(x, y, z, q)
+    r = tc.pepc_traverse_tree(g.x, g.y, g.z, keys=g.key)
+    ro = orc.traverse_tree(go["x"], go["y"], go["z"], keys=go["key"])
+    for k in ("ex", "ey", "ez", "pot", "work"):
+        assert np.array_equal(r[k], ro[k]), k
+    assert tc.stats()["interactions"] == orc.counters()["interactions"]

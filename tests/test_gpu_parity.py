@@ -92,6 +92,18 @@ def test_walk_per_target_bit_exact(gpu, theta2):
     assert st["mac_evaluations"] == c["mac_evaluations"]
 
 
+@pytest.mark.parametrize("walk", [P.WALK_PER_TARGET, P.WALK_PER_TILE])
+def test_walk_morton_keys_bit_exact(gpu, walk):
+    x, y, z, q = plummer(8000, 29)
+    tc, orc, g, go = grow_both(x, y, z, q, theta2=0.25, eps2=1e-4, walk=walk,
+                               curve=P.CURVE_MORTON)
+    assert np.array_equal(g.key, go["key"])
+    r = tc.pepc_traverse_tree(g.x, g.y, g.z, keys=g.key)
+    ro = orc.traverse_tree(go["x"], go["y"], go["z"], keys=go["key"])
+    for k in ("ex", "ey", "ez", "pot", "work"):
+        assert np.array_equal(r[k], ro[k]), k
+
+
 @pytest.mark.parametrize("tile", [16, 32, 1, 7])
 def test_walk_per_tile_bit_exact(gpu, tile):
     # tile sizes up to 16 run several tiles per warp (windows of 33 - T targets)
