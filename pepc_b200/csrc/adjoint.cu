@@ -126,64 +126,39 @@ __host__ __device__ __forceinline__ void leaf_adj(double q, double dx, double dy
   a[12] += cd * dz - q * R1 * gE[2];
 }
 
-// warp-reduce the lanes' contributions and add them to the node's adjoint:
-// a leaf's record has charge and position terms only (a[0], a[10..12]), a
-// twig's everything but the abs_charge slot, which only the downward pass fills
-__device__ __forceinline__ void reduce_add(double* __restrict__ dst, double& v, int lane) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if (lane == 0 && v != 0.0) atomicAdd(dst, v);
-  v = 0.0;
-}
-
-__device__ __forceinline__ void flush_node(double* __restrict__ adj, unsigned u, double a[14],
-                                           int lane, bool leaf) {
-  double* d = adj + (int64_t)kNA * u;
-  reduce_add(d, a[0], lane);
-  if (!leaf) {
-#pragma unroll
-    for (int k = 1; k < 10; ++k) reduce_add(d + k, a[k], lane);
-  }
-#pragma unroll
-  for (int k = 10; k < 13; ++k) reduce_add(d + k, a[k], lane);
-}
-
-// two twigs at once: after one exchange across the half-warps, lanes 0-15
-// hold partial sums for twig p and lanes 16-31 for twig q, so the remaining
-// four reduction steps serve both (13 + 4 x 13 shuffles for two twigs
-// instead of 2 x 5 x 13)
-__device__ __forceinline__ void flush_pair(double* __restrict__ adj, unsigned up, double P[14],
-                                           unsigned uq, double Q[14], int lane) {
-  const bool lo = lane < 16;
-  double* d = adj + (int64_t)kNA * (lo ? up : uq);
+// The warp's records for one node summed through shared memory (a leaf's
+// record has charge and position terms only, a[0] and a[10..12]; a twig's
+// everything but the abs_charge slot, which only the downward pass fills):
+// every lane
+// writes its values into a column of buf (zeros where it did not contribute),
+// then lane k sums row k over the 32 lanes, in lane order with four partial
+// sums, and adds it to the node with one atomic.  13 stores, 32 loads and 35
+// additions per node; a butterfly of warp shuffles needs 13 x 5 double
+// shuffles (measured: the shared-memory form halves the per-target adjoint).
+constexpr int kRedRow = 33;  // padded row: lanes k = 0..12 read distinct banks
+__device__ __forceinline__ void flush_smem(double* __restrict__ adj, unsigned u, double a[14],
+                                           int lane, bool leaf, double* __restrict__ buf) {
 #pragma unroll
   for (int k = 0; k < 13; ++k) {
-    const double send = lo ? Q[k] : P[k];
-    double keep = lo ? P[k] : Q[k];
-    keep += __shfl_xor_sync(0xffffffffu, send, 16);
-#pragma unroll
-    for (int o = 8; o > 0; o >>= 1) keep += __shfl_xor_sync(0xffffffffu, keep, o);
-    if ((lane & 15) == 0 && keep != 0.0) atomicAdd(d + k, keep);
-    P[k] = 0.0;
-    Q[k] = 0.0;
+    if (leaf && k >= 1 && k < 10) continue;
+    buf[k * kRedRow + lane] = a[k];
+    a[k] = 0.0;
   }
-}
-
-// a twig's contributions wait in `pend` for a second twig to share the flush
-__device__ __forceinline__ void flush_twig_paired(double* __restrict__ adj, unsigned u,
-                                                  double a[14], unsigned& pend_u, double pend[14],
-                                                  unsigned none, int lane) {
-  if (pend_u == none) {
+  __syncwarp();
+  if (lane < 13 && !(leaf && lane >= 1 && lane < 10)) {
+    const double* row = buf + lane * kRedRow;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
 #pragma unroll
-    for (int k = 0; k < 13; ++k) {
-      pend[k] = a[k];
-      a[k] = 0.0;
+    for (int j = 0; j < 32; j += 4) {
+      s0 += row[j];
+      s1 += row[j + 1];
+      s2 += row[j + 2];
+      s3 += row[j + 3];
     }
-    pend_u = u;
-  } else {
-    flush_pair(adj, pend_u, pend, u, a, lane);
-    pend_u = none;
+    const double v = (s0 + s1) + (s2 + s3);
+    if (v != 0.0) atomicAdd(adj + (int64_t)kNA * u + lane, v);
   }
+  __syncwarp();
 }
 
 struct AdjArgs {
@@ -227,10 +202,12 @@ template <bool kWithE>
 __global__ void __launch_bounds__(kAdjThreads) k_adj_target(AdjArgs A) {
   __shared__ double s_bl2[kMaxLevel + 1];
   __shared__ double s_vb[3 * 125];
+  __shared__ double s_red[kAdjThreads / 32][13 * kRedRow];  // per warp: flush_smem's rows
   for (int i = threadIdx.x; i <= kMaxLevel; i += blockDim.x) s_bl2[i] = A.bl2[i];
   for (int i = threadIdx.x; i < 3 * A.nbox; i += blockDim.x) s_vb[i] = A.vbox[i];
   __syncthreads();
   const int lane = threadIdx.x & 31;
+  double* sred = s_red[threadIdx.x >> 5];
   const unsigned M = (unsigned)A.M;
   const int64_t per = 1 + (int64_t)A.nsub;
   const int64_t nitems = (A.nt + 31) / 32 * per;
@@ -265,10 +242,9 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_target(AdjArgs A) {
         }
         next = reach ? (unsigned)S : end;
       }
-      double a[14], pend[14];
+      double a[14];
 #pragma unroll
-      for (int k = 0; k < 14; ++k) a[k] = pend[k] = 0.0;
-      unsigned pend_u = M;
+      for (int k = 0; k < 14; ++k) a[k] = 0.0;
       for (;;) {
         const unsigned u = __reduce_min_sync(0xffffffffu, next);
         if (u >= end) break;
@@ -313,11 +289,9 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_target(AdjArgs A) {
             }
           }
         } else if (cm != 0u) {
-          if (leaf) flush_node(A.adj, u, a, lane, true);
-          else flush_twig_paired(A.adj, u, a, pend_u, pend, M, lane);
+          flush_smem(A.adj, u, a, lane, leaf, sred);
         }
       }
-      if (pend_u != M) flush_node(A.adj, pend_u, pend, lane, false);
     }
   }
 }
@@ -328,10 +302,12 @@ template <bool kWithE>
 __global__ void __launch_bounds__(kAdjThreads) k_adj_group(AdjArgs A) {
   __shared__ double s_bl2[kMaxLevel + 1];
   __shared__ double s_vb[3 * 125];
+  __shared__ double s_red[kAdjThreads / 32][13 * kRedRow];  // per warp: flush_smem's rows
   for (int i = threadIdx.x; i <= kMaxLevel; i += blockDim.x) s_bl2[i] = A.bl2[i];
   for (int i = threadIdx.x; i < 3 * A.nbox; i += blockDim.x) s_vb[i] = A.vbox[i];
   __syncthreads();
   const int lane = threadIdx.x & 31;
+  double* sred = s_red[threadIdx.x >> 5];
   const unsigned M = (unsigned)A.M;
   const int64_t nbk = A.ntiles;
   for (;;) {
@@ -350,10 +326,9 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_group(AdjArgs A) {
     }
     for (int ib = 0; ib < A.nbox; ++ib) {
       const double vx = s_vb[3 * ib], vy = s_vb[3 * ib + 1], vz = s_vb[3 * ib + 2];
-      double a[14], pend[14];
+      double a[14];
 #pragma unroll
-      for (int k = 0; k < 14; ++k) a[k] = pend[k] = 0.0;
-      unsigned pend_u = M;
+      for (int k = 0; k < 14; ++k) a[k] = 0.0;
       unsigned u = 0;
       while (u < M) {
         const double4 nd = A.nc4[u];
@@ -363,7 +338,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_group(AdjArgs A) {
         const double dist2 = (dx * dx + dy * dy) + dz * dz;
         if (mu.y & kLeafFlag) {
           if (valid && dist2 > 0.0) leaf_adj(nd.w, dx, dy, dz, A.eps2, gp, gE, a);
-          flush_node(A.adj, u, a, lane, true);
+          flush_smem(A.adj, u, a, lane, true, sred);
           u = (unsigned)fw.y;
         } else {
           const bool ok =
@@ -375,14 +350,14 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_group(AdjArgs A) {
               for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
               twig_adj<kWithE>(nd.w, m, dx, dy, dz, A.eps2, gp, gE, a);
             }
-            flush_twig_paired(A.adj, u, a, pend_u, pend, M, lane);
+            flush_smem(A.adj, u, a, lane, false, sred);
             u = (unsigned)fw.y;
           } else {
             u = (unsigned)fw.x;
           }
         }
       }
-      if (pend_u != M) flush_node(A.adj, pend_u, pend, lane, false);
+
     }
   }
 }
