@@ -62,6 +62,27 @@ def test_grow_parity_clustered(gpu):
     assert np.array_equal(t["moments"], to["moments"])
 
 
+def test_grow_and_walk_deep_chain(gpu):
+    # a tight cluster (spread 1e-6 of the box) under uniform background: long
+    # chains of one-child twigs down to level 19-20, every level list non-empty
+    x, y, z, q = cube(3000, 14, charges="gauss")
+    rng = np.random.default_rng(15)
+    c = np.array([0.3141, 0.5926, 0.5358])
+    for i in range(40):
+        x[i], y[i], z[i] = c + 1e-6 * rng.random(3)
+    tc, orc, g, go = grow_both(x, y, z, q, theta2=0.16, eps2=1e-8, walk=P.WALK_PER_TARGET)
+    assert tc.stats()["max_level"] >= 18
+    assert np.array_equal(g.key, go["key"])
+    t, to = tc.tree(), orc.tree()
+    for k in ("key", "level", "leaves", "descendants", "parent"):
+        assert np.array_equal(t[k], to[k]), k
+    assert np.array_equal(t["moments"], to["moments"])
+    r = tc.pepc_traverse_tree(g.x, g.y, g.z, keys=g.key)
+    ro = orc.traverse_tree(go["x"], go["y"], go["z"], keys=go["key"])
+    for k in ("ex", "ey", "ez", "pot", "work"):
+        assert np.array_equal(r[k], ro[k]), k
+
+
 def test_grow_duplicate_positions(gpu):
     # duplicated positions give identical keys; the duplicate-key fix
     # (module_domains.f90:248-307) shifts keys and moves those particles
