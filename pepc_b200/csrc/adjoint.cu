@@ -24,9 +24,6 @@
 
 namespace pepcg {
 
-__device__ unsigned int g_bucket_counter_adj;
-__device__ unsigned long long g_item_counter_adj;
-
 namespace {
 
 constexpr int kAdjThreads = 128;
@@ -188,6 +185,8 @@ struct AdjArgs {
   int nsub;
   const int32_t* sublist;
   const int32_t* parent;
+  unsigned int* queue;             // bucket counter (k_adj_group), zeroed before the launch
+  unsigned long long* item_queue;  // item counter (k_adj_target), zeroed before the launch
 };
 
 // per-target semantics: the min-next-index schedule of k_walk_target64.
@@ -213,7 +212,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_target(AdjArgs A) {
   const int64_t nitems = (A.nt + 31) / 32 * per;
   for (;;) {
     unsigned long long item = 0;
-    if (lane == 0) item = atomicAdd(&g_item_counter_adj, 1ull);
+    if (lane == 0) item = atomicAdd(A.item_queue, 1ull);
     item = __shfl_sync(0xffffffffu, item, 0);
     if ((int64_t)item >= nitems) break;
     const int64_t b = (int64_t)item / per;
@@ -312,7 +311,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_group(AdjArgs A) {
   const int64_t nbk = A.ntiles;
   for (;;) {
     unsigned b = 0;
-    if (lane == 0) b = atomicAdd(&g_bucket_counter_adj, 1u);
+    if (lane == 0) b = atomicAdd(A.queue, 1u);
     b = __shfl_sync(0xffffffffu, b, 0);
     if ((int64_t)b >= nbk) break;
     const int2 tl = A.tiles[b];
@@ -458,9 +457,9 @@ __global__ void k_adj_out(int64_t n, const int32_t* __restrict__ leafnode,
   }
 }
 
-__global__ void k_reset_adj() {
-  g_bucket_counter_adj = 0;
-  g_item_counter_adj = 0;
+__global__ void k_reset_adj(unsigned int* q, unsigned long long* items) {
+  *q = 0;
+  *items = 0;
 }
 
 __global__ void k_any_nonzero(int64_t n, const double* a, const double* b, const double* c,
@@ -523,6 +522,8 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
   A.eps2 = c->prm.eps2;
   A.M = (int32_t)M;
   A.adj = c->adj.p;
+  A.queue = c->walk_queue();
+  A.item_queue = c->item_queue();
   A.tiles = nullptr;
   A.ntiles = 0;
   A.split_level = 0;
@@ -565,7 +566,7 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
       !cuda_ok(c, cudaStreamSynchronize(s), "flag"))
     return PEPCG_ERR_CUDA;
   COUNT_LAUNCH();
-  k_reset_adj<<<1, 1, 0, s>>>();
+  k_reset_adj<<<1, 1, 0, s>>>(A.queue, A.item_queue);
   COUNT_LAUNCH();
   const int blocks = 148 * 8;
   if (per_target) {

@@ -138,6 +138,7 @@ struct Ctx {
   double* d_box = nullptr;    // [0..8] box, [9..29] boxlength2
   uint32_t* d_status = nullptr;
   unsigned long long* d_small = nullptr;  // [0] dup count, [1] nnodes, [2] tile count, ...
+                                          // [8] walk bucket queue, [9] adjoint item queue
   double box[9];
   double boxlength2[kMaxLevel + 1];
   int max_level = 0;
@@ -168,6 +169,10 @@ struct Ctx {
   cudaEvent_t ready[kMaxChunks] = {}, done[kMaxChunks] = {};
 
   int32_t* nleaves_ptr() { return nleaves.p; }
+  // The persistent walks take buckets from a counter in the context's own
+  // memory, so walks of different contexts may run concurrently on one device.
+  unsigned int* walk_queue() { return reinterpret_cast<unsigned int*>(d_small + 8); }
+  unsigned long long* item_queue() { return d_small + 9; }
 };
 
 // ---- helpers implemented in api.cu ----

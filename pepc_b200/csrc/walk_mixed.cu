@@ -28,8 +28,6 @@
 
 namespace pepcg {
 
-__device__ unsigned int g_bucket_counter_mixed;
-
 namespace {
 
 constexpr int kMixThreads = 128;
@@ -59,6 +57,7 @@ struct MixArgs {
   double* work;
   unsigned long long* counters;
   uint32_t* status;
+  unsigned int* queue;  // bucket counter, zeroed before the launch
   const int2* tiles;  // PER_TILE tiles, or nullptr for GROUP (implicit 32-target buckets)
   int64_t ntiles;
   // packed per-tile walk
@@ -198,7 +197,7 @@ __global__ void __launch_bounds__(kMixThreads, 5)
   unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
   for (;;) {
     unsigned b = 0;
-    if (lane == 0) b = atomicAdd(&g_bucket_counter_mixed, 1u);
+    if (lane == 0) b = atomicAdd(A.queue, 1u);
     b = __shfl_sync(0xffffffffu, b, 0);
     if ((int64_t)b >= nbuckets) break;
     int64_t t0;
@@ -437,7 +436,7 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_tilepack_mixed(MixArgs A) 
   unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
   for (;;) {
     unsigned b = 0;
-    if (lane == 0) b = atomicAdd(&g_bucket_counter_mixed, 1u);
+    if (lane == 0) b = atomicAdd(A.queue, 1u);
     b = __shfl_sync(0xffffffffu, b, 0);
     if ((int64_t)b >= nwin) break;
     const int64_t base = (int64_t)b * W;
@@ -541,7 +540,7 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_target_mixed(MixArgs A) {
   unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
   for (;;) {
     unsigned b = 0;
-    if (lane == 0) b = atomicAdd(&g_bucket_counter_mixed, 1u);
+    if (lane == 0) b = atomicAdd(A.queue, 1u);
     b = __shfl_sync(0xffffffffu, b, 0);
     if ((int64_t)b * 32 >= A.nt) break;
     const int64_t t = (int64_t)b * 32 + lane;
@@ -610,7 +609,7 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_target_mixed(MixArgs A) {
   warp_add3(A.counters, c_leaf, c_twig, c_mac);
 }
 
-__global__ void k_reset_mixed() { g_bucket_counter_mixed = 0; }
+__global__ void k_reset_mixed(unsigned int* q) { *q = 0; }
 
 }  // namespace
 
@@ -639,6 +638,7 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
   A.ex = ex; A.ey = ey; A.ez = ez; A.pot = pot; A.work = work;
   A.counters = c->counters.p;
   A.status = c->d_status;
+  A.queue = c->walk_queue();
   A.tiles = tiles;
   A.ntiles = ntiles;
   A.fwd = c->fwd.p;
@@ -647,7 +647,7 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
   A.tile_w = 33 - (c->prm.tile_size < 1 ? 1 : c->prm.tile_size);
   cudaStream_t s = c->stream;
   COUNT_LAUNCH();
-  k_reset_mixed<<<1, 1, 0, s>>>();
+  k_reset_mixed<<<1, 1, 0, s>>>(A.queue);
   COUNT_LAUNCH();
   if (per_target) {
     k_walk_target_mixed<<<148 * 8, kMixThreads, 0, s>>>(A);

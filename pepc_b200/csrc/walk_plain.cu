@@ -19,8 +19,6 @@
 
 namespace pepcg {
 
-__device__ unsigned int g_bucket_counter;
-
 namespace {
 
 constexpr int kWalkThreads = 128;
@@ -51,6 +49,7 @@ struct WalkArgs {
   double* work;
   unsigned long long* counters;  // [0] leaf, [1] twig, [2] mac
   uint32_t* status;
+  unsigned int* queue;           // bucket counter, zeroed before the launch
   // per tile
   const int2* tiles;  // (first target, count)
   int64_t ntiles;
@@ -86,7 +85,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_target64(WalkArgs A) {
   unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
   for (;;) {
     unsigned b = 0;
-    if (lane == 0) b = atomicAdd(&g_bucket_counter, 1u);
+    if (lane == 0) b = atomicAdd(A.queue, 1u);
     b = __shfl_sync(0xffffffffu, b, 0);
     if ((int64_t)b * 32 >= A.nt) break;
     const int64_t t = (int64_t)b * 32 + lane;
@@ -163,7 +162,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_tile64(WalkArgs A) {
   unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
   for (;;) {
     unsigned b = 0;
-    if (lane == 0) b = atomicAdd(&g_bucket_counter, 1u);
+    if (lane == 0) b = atomicAdd(A.queue, 1u);
     b = __shfl_sync(0xffffffffu, b, 0);
     const int64_t nbk = A.tiles ? A.ntiles : (A.nt + 31) / 32;
     if ((int64_t)b >= nbk) break;
@@ -264,7 +263,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_tilepack64(WalkArgs A) {
   unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
   for (;;) {
     unsigned b = 0;
-    if (lane == 0) b = atomicAdd(&g_bucket_counter, 1u);
+    if (lane == 0) b = atomicAdd(A.queue, 1u);
     b = __shfl_sync(0xffffffffu, b, 0);
     if ((int64_t)b >= nwin) break;
     const int64_t base = (int64_t)b * W;
@@ -388,7 +387,7 @@ __global__ void k_same_keys(int64_t n, const int64_t* __restrict__ a, const int6
     if (a[i] != b[i]) atomicOr(differ, 1u);
 }
 
-__global__ void k_reset_counter() { g_bucket_counter = 0; }
+__global__ void k_reset_counter(unsigned int* q) { *q = 0; }
 
 // mac (coulomb/module_interaction_specific.f90:256-275) for mac_select != 0,
 // as a per-twig threshold t with "accept iff theta2 dist2 > t": the Bmax MAC
@@ -535,6 +534,7 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
   A.npart = c->n;
   A.counters = c->counters.p;
   A.status = c->d_status;
+  A.queue = c->walk_queue();
   A.tiles = reinterpret_cast<const int2*>(c->tiles.p);
   A.ntiles = ntiles;
   A.kinv = c->prm.kelbg_invsqrttemp;
@@ -555,7 +555,7 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
       A.ex = ex + t0; A.ey = ey + t0; A.ez = ez + t0; A.pot = pot + t0; A.work = work + t0;
       A.tq = tq ? tq + t0 : nullptr;
       COUNT_LAUNCH();
-      k_reset_counter<<<1, 1, 0, s>>>();
+      k_reset_counter<<<1, 1, 0, s>>>(A.queue);
       if (c->prm.precision == PEPCG_PRECISION_PLAIN) {
         COUNT_LAUNCH();
         const int law = c->prm.force_law;
