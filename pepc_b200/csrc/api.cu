@@ -359,7 +359,9 @@ int pepcg_destroy(void* ctx) {
     if (c->ready[i]) cudaEventDestroy(c->ready[i]);
     if (c->done[i]) cudaEventDestroy(c->done[i]);
   }
-  for (cudaStream_t t : {c->h2d, c->d2h})
+  for (cudaEvent_t e : {c->fork, c->join})
+    if (e) cudaEventDestroy(e);
+  for (cudaStream_t t : {c->h2d, c->d2h, c->walk2})
     if (t) {
       cudaStreamSynchronize(t);
       cudaStreamDestroy(t);
@@ -394,7 +396,10 @@ int pepcg_set_params(void* ctx, const pepcg_params* p) {
 static bool copy_streams(Ctx* c) {
   if (c->h2d) return true;
   bool ok = cuda_ok(c, cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking), "copy stream") &&
-            cuda_ok(c, cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking), "copy stream");
+            cuda_ok(c, cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking), "copy stream") &&
+            cuda_ok(c, cudaStreamCreateWithFlags(&c->walk2, cudaStreamNonBlocking), "walk stream") &&
+            cuda_ok(c, cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming), "event") &&
+            cuda_ok(c, cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming), "event");
   for (int i = 0; ok && i < Ctx::kMaxChunks; ++i)
     ok = cuda_ok(c, cudaEventCreateWithFlags(&c->ready[i], cudaEventDisableTiming), "event") &&
          cuda_ok(c, cudaEventCreateWithFlags(&c->done[i], cudaEventDisableTiming), "event");

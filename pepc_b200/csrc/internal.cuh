@@ -138,7 +138,8 @@ struct Ctx {
   double* d_box = nullptr;    // [0..8] box, [9..29] boxlength2
   uint32_t* d_status = nullptr;
   unsigned long long* d_small = nullptr;  // [0] dup count, [1] nnodes, [2] tile count, ...
-                                          // [8] walk bucket queue, [9] adjoint item queue
+                                          // [8], [9] walk bucket queues (one per walk
+                                          // stream), [10] adjoint item queue
   double box[9];
   double boxlength2[kMaxLevel + 1];
   int max_level = 0;
@@ -162,17 +163,20 @@ struct Ctx {
   bool grow_times_pending = false;
 
   // host-transfer overlap (the host-array entry points): one stream per copy
-  // direction and untimed events that order chunks across the streams;
-  // created on first use
-  cudaStream_t h2d = nullptr, d2h = nullptr;
+  // direction, untimed events that order chunks across the streams, and a
+  // second walk stream, so that a chunk's walk starts on the SMs that the
+  // previous chunk's last buckets leave idle; created on first use
+  cudaStream_t h2d = nullptr, d2h = nullptr, walk2 = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   static constexpr int kMaxChunks = 8;
   cudaEvent_t ready[kMaxChunks] = {}, done[kMaxChunks] = {};
 
   int32_t* nleaves_ptr() { return nleaves.p; }
   // The persistent walks take buckets from a counter in the context's own
   // memory, so walks of different contexts may run concurrently on one device.
-  unsigned int* walk_queue() { return reinterpret_cast<unsigned int*>(d_small + 8); }
-  unsigned long long* item_queue() { return d_small + 9; }
+  // Slot 0 serves walks on the context stream, slot 1 walks on walk2.
+  unsigned int* walk_queue(int slot = 0) { return reinterpret_cast<unsigned int*>(d_small + 8 + slot); }
+  unsigned long long* item_queue() { return d_small + 10; }
 };
 
 // ---- helpers implemented in api.cu ----

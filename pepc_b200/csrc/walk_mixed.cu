@@ -616,7 +616,7 @@ __global__ void k_reset_mixed(unsigned int* q) { *q = 0; }
 int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                       double* ex, double* ey, double* ez, double* pot, double* work,
                       const int2* tiles, int64_t ntiles, bool per_target,
-                      const int32_t* tflag) {
+                      const int32_t* tflag, cudaStream_t s, int slot) {
   MixArgs A;
   A.nt = nt;
   A.tx = tx; A.ty = ty; A.tz = tz;
@@ -638,14 +638,13 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
   A.ex = ex; A.ey = ey; A.ez = ez; A.pot = pot; A.work = work;
   A.counters = c->counters.p;
   A.status = c->d_status;
-  A.queue = c->walk_queue();
+  A.queue = c->walk_queue(slot);
   A.tiles = tiles;
   A.ntiles = ntiles;
   A.fwd = c->fwd.p;
   A.fwdf = c->fwdf.p;
   A.tflag = tflag;
   A.tile_w = 33 - (c->prm.tile_size < 1 ? 1 : c->prm.tile_size);
-  cudaStream_t s = c->stream;
   COUNT_LAUNCH();
   k_reset_mixed<<<1, 1, 0, s>>>(A.queue);
   COUNT_LAUNCH();
@@ -655,10 +654,13 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
     k_walk_tilepack_mixed<<<148 * 8, kMixThreads, 0, s>>>(A);
   } else {
     // 5 resident blocks per SM (launch bounds: 96 registers, 31.8 KB shared
-    // memory each); the grid is exactly one wave
+    // memory each); the grid is exactly one wave.  One set of stacks per walk
+    // stream.
     const int gblocks = 148 * 5;
-    if (!ensure(c, c->wstack, (size_t)gblocks * kWW * kStackCap, "walk stacks")) return PEPCG_ERR_OOM;
-    k_walk_group_wide<<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p, c->child8.p, c->nchild.p);
+    const size_t per = (size_t)gblocks * kWW * kStackCap;
+    if (!ensure(c, c->wstack, 2 * per, "walk stacks")) return PEPCG_ERR_OOM;
+    k_walk_group_wide<<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p + slot * per, c->child8.p,
+                                                      c->nchild.p);
   }
   return cuda_ok(c, cudaGetLastError(), "mixed walk launch") ? PEPCG_OK : PEPCG_ERR_CUDA;
 }

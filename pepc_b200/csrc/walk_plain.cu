@@ -413,7 +413,8 @@ __global__ void k_mac_thresholds(int64_t M, int mode, const int2* __restrict__ m
 
 int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                       double* ex, double* ey, double* ez, double* pot, double* work,
-                      const int2* tiles, int64_t ntiles, bool per_target, const int32_t* tflag);
+                      const int2* tiles, int64_t ntiles, bool per_target, const int32_t* tflag,
+                      cudaStream_t s, int slot);
 
 const double* grown_charges_if_same(Ctx* c, int64_t nt, const int64_t* d_tkeys) {
   if (!d_tkeys || nt != c->n) return nullptr;
@@ -543,10 +544,19 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
   A.tflag = c->tflag.p;
   A.tile_w = 33 - (c->prm.tile_size < 1 ? 1 : c->prm.tile_size);
   const int blocks = 148 * 8;
+  // chunks alternate between the context stream and walk2, so that each
+  // chunk's walk starts while the previous one finishes its last buckets
+  const bool two = nchunks > 1 && c->walk2;
+  if (two && (!cuda_ok(c, cudaEventRecord(c->fork, s), "fork") ||
+              !cuda_ok(c, cudaStreamWaitEvent(c->walk2, c->fork, 0), "fork")))
+    return PEPCG_ERR_CUDA;
   for (int k = 0; k < nchunks; ++k) {
     const int64_t t0 = nchunks > 1 ? plan->bounds[k] : 0;
     const int64_t t1 = nchunks > 1 ? plan->bounds[k + 1] : nt;
-    if (plan && plan->ready && !cuda_ok(c, cudaStreamWaitEvent(s, plan->ready[k], 0), "chunk wait"))
+    const int slot = two ? (k & 1) : 0;
+    const cudaStream_t sk = slot ? c->walk2 : s;
+    A.queue = c->walk_queue(slot);
+    if (plan && plan->ready && !cuda_ok(c, cudaStreamWaitEvent(sk, plan->ready[k], 0), "chunk wait"))
       return PEPCG_ERR_CUDA;
     if (k == 0) cudaEventRecord(c->ev[5], s);
     if (t1 > t0) {
@@ -555,37 +565,41 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
       A.ex = ex + t0; A.ey = ey + t0; A.ez = ez + t0; A.pot = pot + t0; A.work = work + t0;
       A.tq = tq ? tq + t0 : nullptr;
       COUNT_LAUNCH();
-      k_reset_counter<<<1, 1, 0, s>>>(A.queue);
+      k_reset_counter<<<1, 1, 0, sk>>>(A.queue);
       if (c->prm.precision == PEPCG_PRECISION_PLAIN) {
         COUNT_LAUNCH();
         const int law = c->prm.force_law;
         if (walk == PEPCG_WALK_PER_TARGET) {
-          if (law == 2) k_walk_target64<2><<<blocks, kWalkThreads, 0, s>>>(A);
-          else if (law == 4) k_walk_target64<4><<<blocks, kWalkThreads, 0, s>>>(A);
-          else if (law == 5) k_walk_target64<5><<<blocks, kWalkThreads, 0, s>>>(A);
-          else k_walk_target64<3><<<blocks, kWalkThreads, 0, s>>>(A);
+          if (law == 2) k_walk_target64<2><<<blocks, kWalkThreads, 0, sk>>>(A);
+          else if (law == 4) k_walk_target64<4><<<blocks, kWalkThreads, 0, sk>>>(A);
+          else if (law == 5) k_walk_target64<5><<<blocks, kWalkThreads, 0, sk>>>(A);
+          else k_walk_target64<3><<<blocks, kWalkThreads, 0, sk>>>(A);
         } else if (packed) {
-          if (law == 2) k_walk_tilepack64<2><<<blocks, kWalkThreads, 0, s>>>(A);
-          else if (law == 4) k_walk_tilepack64<4><<<blocks, kWalkThreads, 0, s>>>(A);
-          else if (law == 5) k_walk_tilepack64<5><<<blocks, kWalkThreads, 0, s>>>(A);
-          else k_walk_tilepack64<3><<<blocks, kWalkThreads, 0, s>>>(A);
+          if (law == 2) k_walk_tilepack64<2><<<blocks, kWalkThreads, 0, sk>>>(A);
+          else if (law == 4) k_walk_tilepack64<4><<<blocks, kWalkThreads, 0, sk>>>(A);
+          else if (law == 5) k_walk_tilepack64<5><<<blocks, kWalkThreads, 0, sk>>>(A);
+          else k_walk_tilepack64<3><<<blocks, kWalkThreads, 0, sk>>>(A);
         } else {
           if (walk == PEPCG_WALK_GROUP) A.tiles = nullptr;
-          if (law == 2) k_walk_tile64<2><<<blocks, kWalkThreads, 0, s>>>(A);
-          else if (law == 4) k_walk_tile64<4><<<blocks, kWalkThreads, 0, s>>>(A);
-          else if (law == 5) k_walk_tile64<5><<<blocks, kWalkThreads, 0, s>>>(A);
-          else k_walk_tile64<3><<<blocks, kWalkThreads, 0, s>>>(A);
+          if (law == 2) k_walk_tile64<2><<<blocks, kWalkThreads, 0, sk>>>(A);
+          else if (law == 4) k_walk_tile64<4><<<blocks, kWalkThreads, 0, sk>>>(A);
+          else if (law == 5) k_walk_tile64<5><<<blocks, kWalkThreads, 0, sk>>>(A);
+          else k_walk_tile64<3><<<blocks, kWalkThreads, 0, sk>>>(A);
         }
       } else {
         int rc = launch_walk_mixed(c, t1 - t0, A.tx, A.ty, A.tz, A.ex, A.ey, A.ez, A.pot, A.work,
                                    walk == PEPCG_WALK_PER_TILE ? A.tiles : nullptr, ntiles,
-                                   walk == PEPCG_WALK_PER_TARGET, packed ? c->tflag.p : nullptr);
+                                   walk == PEPCG_WALK_PER_TARGET, packed ? c->tflag.p : nullptr,
+                                   sk, slot);
         if (rc) return rc;
       }
       if (!cuda_ok(c, cudaGetLastError(), "walk launch")) return PEPCG_ERR_CUDA;
     }
-    if (plan && plan->done) cudaEventRecord(plan->done[k], s);
+    if (plan && plan->done) cudaEventRecord(plan->done[k], sk);
   }
+  if (two && (!cuda_ok(c, cudaEventRecord(c->join, c->walk2), "join") ||
+              !cuda_ok(c, cudaStreamWaitEvent(s, c->join, 0), "join")))
+    return PEPCG_ERR_CUDA;
   cudaEventRecord(c->ev[6], s);
   if (c->far_field) {
     int rc = lattice_add(c, nt, tx, ty, tz, ex, ey, ez, pot, false);
