@@ -83,6 +83,32 @@ def test_grow_and_walk_deep_chain(gpu):
         assert np.array_equal(r[k], ro[k]), k
 
 
+@pytest.mark.parametrize("walk", [P.WALK_PER_TARGET, P.WALK_PER_TILE])
+def test_force_cubic_domain_bit_exact(gpu, walk):
+    # an elongated cloud: the cubic domain (module_box.f90:71-74) differs from
+    # the bounding box, so keys, levels and MAC box lengths all change
+    x, y, z, q = cube(6000, 16)
+    x = 4.0 * x - 1.0
+    z = 0.25 * z
+    tc, orc, g, go = grow_both(x, y, z, q, theta2=0.36, eps2=1e-4, force_cubic_domain=1,
+                               walk=walk, tile_size=16)
+    assert np.array_equal(tc.stats()["box"], orc.box())
+    assert np.array_equal(g.key, go["key"])
+    assert np.array_equal(g.perm, go["perm"])
+    t, to = tc.tree(), orc.tree()
+    for k in ("key", "level", "leaves", "parent"):
+        assert np.array_equal(t[k], to[k]), k
+    assert np.array_equal(t["moments"], to["moments"])
+    r = tc.pepc_traverse_tree(g.x, g.y, g.z, keys=g.key)
+    ro = orc.traverse_tree(go["x"], go["y"], go["z"], keys=go["key"])
+    for k in ("ex", "ey", "ez", "pot", "work"):
+        assert np.array_equal(r[k], ro[k]), k
+    # and the box is the cube, not the bounding box
+    tb = P.TreeCode(theta2=0.36, eps2=1e-4)
+    tb.pepc_grow_tree(x, y, z, q)
+    assert not np.array_equal(tb.stats()["box"], tc.stats()["box"])
+
+
 def test_grow_duplicate_positions(gpu):
     # duplicated positions give identical keys; the duplicate-key fix
     # (module_domains.f90:248-307) shifts keys and moves those particles
