@@ -341,7 +341,7 @@ int pepcg_destroy(void* ctx) {
   release(c->lev); release(c->lcpn);
   release(c->cstart); release(c->cend); release(c->sstart); release(c->send);
   release(c->scan_tmp);
-  release(c->nc4); release(c->meta); release(c->fwd); release(c->fwdf); release(c->tflag); release(c->mom);
+  release(c->nc4); release(c->meta); release(c->fwd); release(c->fwdf); release(c->tflag); release(c->tpack); release(c->mom);
   release(c->mom32);
   release(c->parent); release(c->nchild); release(c->twiglist); release(c->lvlcnt); release(c->lvlblk);
   release(c->drec); release(c->dmom);

@@ -107,6 +107,7 @@ struct Ctx {
   DBuf<int2> fwd;
   DBuf<int2> fwdf;    // fwd's two nodes as forward-preorder indices
   DBuf<int32_t> tflag;  // per target: the length of the tile that starts there, else 0
+  DBuf<int32_t> tpack;  // greedy packing of tiles into warps (walk_plain.cu)
   // kMomStride doubles per node (96 B, three whole sectors): the 9 moments,
   // then abs_charge and bmax
   DBuf<double> mom;
@@ -178,6 +179,23 @@ struct Ctx {
   unsigned int* walk_queue(int slot = 0) { return reinterpret_cast<unsigned int*>(d_small + 8 + slot); }
   unsigned long long* item_queue() { return d_small + 10; }
 };
+
+// The lanes of one pack of the packed per-tile walks: pack b holds the whole
+// tiles in targets [pstart[b], pstart[b + 1]), at most 32, and tflag gives
+// each tile's length at its first target.  Returns whether this lane holds a
+// target; tl0 is the lane of its tile's first target and len the tile's length.
+__device__ __forceinline__ bool pack_lane(const int32_t* __restrict__ pstart,
+                                          const int32_t* __restrict__ tflag, int64_t b, int lane,
+                                          int& tl0, int& len) {
+  const int64_t t0 = pstart[b];
+  const int64_t cnt = pstart[b + 1] - t0;
+  const int fl = lane < cnt ? tflag[t0 + lane] : 0;
+  const unsigned starts = __ballot_sync(0xffffffffu, fl > 0);
+  const unsigned upto = lane == 31 ? starts : (starts & ((2u << lane) - 1u));
+  tl0 = upto ? 31 - __clz(upto) : 0;
+  len = __shfl_sync(0xffffffffu, fl, tl0);
+  return (starts & 1u) && lane < cnt && cnt <= 32;
+}
 
 // ---- helpers implemented in api.cu ----
 bool cuda_ok(Ctx* c, cudaError_t e, const char* what);

@@ -64,7 +64,8 @@ struct MixArgs {
   const int2* fwd;       // (first child, next after the subtree), RPO indices
   const int2* fwdf;      // the same as forward-preorder indices
   const int32_t* tflag;  // per target: length of the tile starting there, else 0
-  int tile_w;            // window of targets per warp: 33 - tile_size
+  const int32_t* pstart;  // packed per-tile walk: first target of each pack, then nt
+  const int32_t* npacks;  // the number of packs (device)
 };
 
 __device__ __forceinline__ void leaf32(float q, float dx, float dy, float dz, float eps2,
@@ -416,9 +417,9 @@ __global__ void __launch_bounds__(kMixThreads, 5)
 }
 
 // Simple-walk semantics (module_tree_walk_simple.f90:256-385) with several
-// reference tiles per warp and FP32 interactions: the tiles that start in
-// the target window [W k, W k + W), W = 33 - tile_size, walk the tree
-// together in forward preorder -- at each step the lanes whose tile stands at
+// reference tiles per warp and FP32 interactions: the whole tiles of one
+// pack (at most 32 targets, k_pack_tiles) walk the tree together in forward
+// preorder -- at each step the lanes whose tile stands at
 // the smallest forward-preorder index evaluate that node, and each tile
 // decides accept / open by a ballot over its own lanes (the MAC on the FP32
 // offsets, target minus node centre formed in FP64).  Sums as in the
@@ -431,26 +432,20 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_tilepack_mixed(MixArgs A) 
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const unsigned M = (unsigned)A.M;
-  const int W = A.tile_w;
-  const int64_t nwin = (A.nt + W - 1) / W;
+  const int64_t npk = *A.npacks;
   unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
   for (;;) {
     unsigned b = 0;
     if (lane == 0) b = atomicAdd(A.queue, 1u);
     b = __shfl_sync(0xffffffffu, b, 0);
-    if ((int64_t)b >= nwin) break;
-    const int64_t base = (int64_t)b * W;
-    const int fl = (lane < W && base + lane < A.nt) ? A.tflag[base + lane] : 0;
-    const unsigned starts = __ballot_sync(0xffffffffu, fl > 0);
-    if (starts == 0) continue;
-    const int s0 = __ffs(starts) - 1;
-    const int wl = s0 + lane;
-    const unsigned upto = wl >= 31 ? starts : (starts & ((2u << wl) - 1u));
-    const int sl = 31 - __clz(upto);
-    const int len = __shfl_sync(0xffffffffu, fl, sl);
-    const int64_t t = base + s0 + lane;
-    const int tl0 = sl - s0;  // first lane of this lane's tile
-    const bool valid = t < A.nt && lane < tl0 + len;
+    if ((int64_t)b >= npk) break;
+    int tl0, len;
+    const bool valid = pack_lane(A.pstart, A.tflag, b, lane, tl0, len);
+    if (!__any_sync(0xffffffffu, valid)) {
+      if (lane == 0) atomicOr(A.status, ST_INCOMPLETE);  // a pack must start with a tile
+      continue;
+    }
+    const int64_t t = A.pstart[b] + lane;
     const unsigned tmask = valid ? (((len >= 32) ? 0xffffffffu : ((1u << len) - 1u)) << tl0) : 0u;
     double px = 0, py = 0, pz = 0, E0 = 0, E1 = 0, E2 = 0, PH = 0, W8 = 0;
     if (valid) {
@@ -616,7 +611,8 @@ __global__ void k_reset_mixed(unsigned int* q) { *q = 0; }
 int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                       double* ex, double* ey, double* ez, double* pot, double* work,
                       const int2* tiles, int64_t ntiles, bool per_target,
-                      const int32_t* tflag, cudaStream_t s, int slot) {
+                      const int32_t* tflag, const int32_t* pstart, const int32_t* npacks,
+                      cudaStream_t s, int slot) {
   MixArgs A;
   A.nt = nt;
   A.tx = tx; A.ty = ty; A.tz = tz;
@@ -644,7 +640,8 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
   A.fwd = c->fwd.p;
   A.fwdf = c->fwdf.p;
   A.tflag = tflag;
-  A.tile_w = 33 - (c->prm.tile_size < 1 ? 1 : c->prm.tile_size);
+  A.pstart = pstart;
+  A.npacks = npacks;
   COUNT_LAUNCH();
   k_reset_mixed<<<1, 1, 0, s>>>(A.queue);
   COUNT_LAUNCH();

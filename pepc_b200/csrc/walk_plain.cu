@@ -13,6 +13,7 @@
 //    visited first to last (key order) through the fwd pointers.
 // Compiled with --fmad=false: results are bit-identical to the oracle.
 
+#include <algorithm>
 #include <cmath>
 
 #include "internal.cuh"
@@ -56,7 +57,8 @@ struct WalkArgs {
   // packed per-tile walk
   const int2* fwdf;     // (first child, next after the subtree) as forward-preorder indices
   const int32_t* tflag;  // per target: length of the tile starting there, else 0
-  int tile_w;            // window of targets per warp: 33 - tile_size
+  const int32_t* pstart;  // packed per-tile walk: first target of each pack, then nt
+  const int32_t* npacks;  // the number of packs (device)
 };
 
 __device__ __forceinline__ void warp_add_counters(unsigned long long* ctr, unsigned long long a,
@@ -240,9 +242,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_tile64(WalkArgs A) {
 // more than T (the key-prefix split of tree_walk_init_aux,
 // module_tree_walk_simple.f90:168-211, is exactly this set of nodes).
 // Several reference tiles per warp (simple-walk semantics, module_tree_walk_
-// simple.f90:256-385).  Warp k takes the tiles that start in the target
-// window [W k, W k + W), W = 33 - tile_size, so their targets fit the 32
-// lanes.  Every tile walks the tree in forward preorder (children first to
+// simple.f90:256-385).  Each warp takes one pack of consecutive whole tiles
+// of at most 32 targets (k_pack_tiles).  Every tile walks the tree in forward
+// preorder (children first to
 // last); the warp steps through the union of its tiles' walks in that order:
 // at each step the lanes whose tile stands at the smallest forward-preorder
 // index f evaluate node f together (one load for all of them), and each tile
@@ -258,29 +260,21 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_tilepack64(WalkArgs A) {
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const unsigned M = (unsigned)A.M;
-  const int W = A.tile_w;
-  const int64_t nwin = (A.nt + W - 1) / W;
+  const int64_t npk = *A.npacks;
   unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
   for (;;) {
     unsigned b = 0;
     if (lane == 0) b = atomicAdd(A.queue, 1u);
     b = __shfl_sync(0xffffffffu, b, 0);
-    if ((int64_t)b >= nwin) break;
-    const int64_t base = (int64_t)b * W;
-    // tile starts in the window
-    const int fl = (lane < W && base + lane < A.nt) ? A.tflag[base + lane] : 0;
-    const unsigned starts = __ballot_sync(0xffffffffu, fl > 0);
-    if (starts == 0) continue;
-    const int s0 = __ffs(starts) - 1;
-    const int64_t t0 = base + s0;
-    // this lane's target and tile: the last start at or before it within the window
-    const int wl = s0 + lane;
-    const unsigned upto = wl >= 31 ? starts : (starts & ((2u << wl) - 1u));
-    const int sl = 31 - __clz(upto);
-    const int len = __shfl_sync(0xffffffffu, fl, sl);
+    if ((int64_t)b >= npk) break;
+    int tl0, len;
+    const int64_t t0 = A.pstart[b];
+    const bool valid = pack_lane(A.pstart, A.tflag, b, lane, tl0, len);
+    if (!__any_sync(0xffffffffu, valid)) {
+      if (lane == 0) atomicOr(A.status, ST_INCOMPLETE);  // a pack must start with a tile
+      continue;
+    }
     const int64_t t = t0 + lane;
-    const int tl0 = sl - s0;  // first lane of this lane's tile
-    const bool valid = t < A.nt && lane < tl0 + len;
     const unsigned tmask = valid ? (((len >= 32) ? 0xffffffffu : ((1u << len) - 1u)) << tl0) : 0u;
     double px = 0, py = 0, pz = 0, e0 = 0, e1 = 0, e2 = 0, ph = 0, w = 0;
     KelbgArgs kel{0.0, A.kinv, A.sqrtpi};
@@ -355,6 +349,64 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_tilepack64(WalkArgs A) {
   warp_add_counters(A.counters, c_leaf, c_twig, c_mac);
 }
 
+// Greedy packing of consecutive tiles into warps.  The targets are cut into
+// chunks of kPackChunk, each chunk's bounds moved forward to the next tile
+// start; one warp per chunk steps through its tiles in order and opens a new
+// pack whenever the next tile would not fit the 32 lanes.  Two consecutive
+// packs hold at least 33 targets between them, so a chunk of kPackChunk + 31
+// targets has at most 127 packs (kPackSlots leaves a margin).  The packs are
+// then compacted in chunk order into pstart.
+constexpr int64_t kPackChunk = 2048;
+constexpr int kPackSlots = 256;
+
+// the first tile start at or after p, or nt: a tile holds at most 32
+// targets, so one lies in [p, p + 31]
+__device__ __forceinline__ int64_t first_tile_start(int64_t p, int64_t nt,
+                                                    const int32_t* __restrict__ tflag, int lane) {
+  if (p >= nt) return nt;
+  const int64_t q = p + lane;
+  const unsigned m = __ballot_sync(0xffffffffu, q >= nt || tflag[q] > 0);
+  return m ? min(p + __ffs(m) - 1, nt) : nt;
+}
+
+__global__ void k_pack_tiles(int64_t nt, const int32_t* __restrict__ tflag,
+                             int32_t* __restrict__ raw, int32_t* __restrict__ pcount,
+                             uint32_t* status) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nchunks = (nt + kPackChunk - 1) / kPackChunk;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t ch = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; ch < nchunks;
+       ch += nwarps) {
+    int64_t p = first_tile_start(ch * kPackChunk, nt, tflag, lane);
+    const int64_t e = first_tile_start((ch + 1) * kPackChunk, nt, tflag, lane);
+    int k = 0;
+    while (p < e && k < kPackSlots) {
+      if (lane == 0) raw[ch * kPackSlots + k] = (int32_t)p;
+      ++k;
+      // the pack ends at the last tile start (or e) in [p + 1, p + 32]
+      const int64_t q = p + 1 + lane;
+      const unsigned m = __ballot_sync(0xffffffffu, q <= e && (q == e || tflag[q] > 0));
+      p = m ? p + 1 + (31 - __clz(m)) : e;
+    }
+    if (lane == 0) {
+      if (p < e) atomicOr(status, ST_INCOMPLETE);
+      pcount[ch] = k;
+    }
+  }
+}
+
+__global__ void k_pack_compact(int64_t nt, int64_t nchunks, const int32_t* __restrict__ raw,
+                               const int32_t* __restrict__ pcount, const int32_t* __restrict__ poff,
+                               int32_t* __restrict__ pstart) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nchunks * kPackSlots;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t ch = i / kPackSlots;
+    const int k = (int)(i % kPackSlots);
+    if (k < pcount[ch]) pstart[poff[ch] + k] = raw[i];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) pstart[poff[nchunks]] = (int32_t)nt;
+}
+
 // per-target tile lengths from the compact (first, count) list
 __global__ void k_tile_flags(int64_t ntiles, const int2* __restrict__ tiles,
                              int32_t* __restrict__ tflag) {
@@ -414,7 +466,7 @@ __global__ void k_mac_thresholds(int64_t M, int mode, const int2* __restrict__ m
 int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                       double* ex, double* ey, double* ez, double* pot, double* work,
                       const int2* tiles, int64_t ntiles, bool per_target, const int32_t* tflag,
-                      cudaStream_t s, int slot);
+                      const int32_t* pstart, const int32_t* npacks, cudaStream_t s, int slot);
 
 const double* grown_charges_if_same(Ctx* c, int64_t nt, const int64_t* d_tkeys) {
   if (!d_tkeys || nt != c->n) return nullptr;
@@ -495,8 +547,15 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
       if (rc) return rc;
     }
   }
-  // per-tile walk with tiles of <= 16 targets: several tiles per warp
-  const bool packed = walk == PEPCG_WALK_PER_TILE && c->prm.tile_size <= 16;
+  // per-tile walk: several whole tiles per warp.  Measured at 4M (Plummer,
+  // theta 0.4): the packed FP64 walk beats one tile per warp at every tile
+  // size (32: 318 vs 851 ms); in the mixed form the wide group kernel with
+  // tiles as buckets wins at 32 targets (127 vs 148 ms) and loses at 24
+  // (167 vs 146 ms)
+  const bool packed = walk == PEPCG_WALK_PER_TILE &&
+                      (c->prm.precision == PEPCG_PRECISION_PLAIN || c->prm.tile_size <= 24);
+  const int32_t* pstart = nullptr;
+  const int32_t* npacks = nullptr;
   if (packed) {
     if (!ensure(c, c->tflag, nt, "tile flags")) return PEPCG_ERR_OOM;
     if (!cuda_ok(c, cudaMemsetAsync(c->tflag.p, 0, nt * sizeof(int32_t), s), "tile flags"))
@@ -504,6 +563,28 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
     COUNT_LAUNCH();
     k_tile_flags<<<296, 256, 0, s>>>(ntiles, reinterpret_cast<const int2*>(c->tiles.p),
                                      c->tflag.p);
+    // packs of whole tiles, <= 32 targets each
+    const int64_t nch = (nt + kPackChunk - 1) / kPackChunk;
+    const int64_t ntmp = (nch + 1 + 2047) / 2048 + 1;
+    const int64_t cap = nch * kPackSlots + 1;  // packs + the end; every slot may be used
+    if (!ensure(c, c->tpack, (size_t)(nch * kPackSlots + 2 * (nch + 1) + ntmp + cap), "packs"))
+      return PEPCG_ERR_OOM;
+    int32_t* raw = c->tpack.p;
+    int32_t* pcount = raw + nch * kPackSlots;
+    int32_t* poff = pcount + nch + 1;
+    int32_t* tmp = poff + nch + 1;
+    int32_t* ps = tmp + ntmp;
+    pstart = ps;
+    npacks = poff + nch;
+    if (!cuda_ok(c, cudaMemsetAsync(pcount, 0, (nch + 1) * sizeof(int32_t), s), "packs"))
+      return PEPCG_ERR_CUDA;
+    const unsigned gw = (unsigned)std::min<int64_t>((nch * 32 + 255) / 256, 148 * 8);
+    COUNT_LAUNCH();
+    k_pack_tiles<<<gw, 256, 0, s>>>(nt, c->tflag.p, raw, pcount, c->d_status);
+    exclusive_scan_i32(pcount, poff, nch + 1, tmp, s);
+    const unsigned gc = (unsigned)std::min<int64_t>((nch * kPackSlots + 255) / 256, 148 * 8);
+    COUNT_LAUNCH();
+    k_pack_compact<<<gc, 256, 0, s>>>(nt, nch, raw, pcount, poff, ps);
   }
   const int nchunks = plan ? plan->nchunks : 1;
   if (nchunks > 1) {
@@ -542,7 +623,8 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
   A.sqrtpi = std::sqrt(std::acos(-1.0));
   A.fwdf = c->fwdf.p;
   A.tflag = c->tflag.p;
-  A.tile_w = 33 - (c->prm.tile_size < 1 ? 1 : c->prm.tile_size);
+  A.pstart = pstart;
+  A.npacks = npacks;
   const int blocks = 148 * 8;
   // chunks alternate between the context stream and walk2, so that each
   // chunk's walk starts while the previous one finishes its last buckets
@@ -590,7 +672,7 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
         int rc = launch_walk_mixed(c, t1 - t0, A.tx, A.ty, A.tz, A.ex, A.ey, A.ez, A.pot, A.work,
                                    walk == PEPCG_WALK_PER_TILE ? A.tiles : nullptr, ntiles,
                                    walk == PEPCG_WALK_PER_TARGET, packed ? c->tflag.p : nullptr,
-                                   sk, slot);
+                                   pstart, npacks, sk, slot);
         if (rc) return rc;
       }
       if (!cuda_ok(c, cudaGetLastError(), "walk launch")) return PEPCG_ERR_CUDA;
