@@ -649,7 +649,10 @@ def main():
         "dtype": "f32 interactions + f64 offsets/sums" if prec == P.PRECISION_MIXED else "f64",
         "data": "synthetic",
         "config": {"workload": workload_name(args), "precision": args.precision,
-                   "walk": args.walk, "parallelism": "replicas only" if world > 1 else "single GPU",
+                   "walk": args.walk,
+                   "group_size": (64 if prec == P.PRECISION_MIXED else 32) if args.walk == "group"
+                   else None,
+                   "parallelism": "replicas only" if world > 1 else "single GPU",
                    "l2": "inputs (128 MB) and tree (~0.7 GB) exceed the 126 MB L2; no flush",
                    "step": "zero results + grow (box, keys, sort, tree, multipoles) + traverse"},
         "force_err": {"median": float(np.median(rel)), "p99": float(np.percentile(rel, 99)),

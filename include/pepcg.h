@@ -57,8 +57,9 @@ extern "C" {
 
 #define PEPCG_WALK_PER_TARGET 0 /* module_tree_walk_pthreads semantics (pepc-mini) */
 #define PEPCG_WALK_PER_TILE 1   /* module_tree_walk_simple semantics (pepc-essential) */
-#define PEPCG_WALK_GROUP 2      /* warp-bucket group walk: tiles of 32 key-consecutive
-                                   targets, node lists batched through shared memory */
+#define PEPCG_WALK_GROUP 2      /* warp-bucket group walk: buckets of group_size key-
+                                   consecutive targets, node lists batched through shared
+                                   memory */
 
 /*
  * Parameters: the /libpepc/ and /calc_force_coulomb/ namelist variables that
@@ -91,7 +92,10 @@ typedef struct pepcg_params {
                                     results clear and the traverse in one call, with no
                                     upload of the old values) */
   double kelbg_invsqrttemp;      /* force_law 5: 1/sqrt(temperature) (specific.f90:40) [0] */
-  int32_t reserved[4];
+  int32_t group_size;            /* GROUP walk: targets per bucket, 32 or 64; 0 = 64 for the
+                                    mixed walk and 32 for the plain walk [0].  The adjoint
+                                    supports 32. */
+  int32_t reserved[3];
 } pepcg_params;
 
 /* Statistics of the last grow/traverse (module_tree.f90:622-699,
@@ -215,8 +219,9 @@ int pepcg_gather_device(void* ctx, const double* d_in, double* d_out);
  * (module_domains.f90) and domain_restore (:372-408).
  *   pepcg_traverse_range_device  the fields on the grown particles [t0, t1) of
  *     the key order, written to arrays of length t1 - t0 (accumulates like
- *     pepcg_traverse_self_device); ranges that start at multiples of 32 give
- *     exactly the single-call result in every walk mode;
+ *     pepcg_traverse_self_device); ranges that start at multiples of the group
+ *     walk's bucket (64 covers both sizes) give exactly the single-call result
+ *     in every walk mode;
  *   pepcg_restore_device         out[perm[i]] = in[i]: a key-ordered array back
  *     to the order of the last grow's input (in != out).
  */

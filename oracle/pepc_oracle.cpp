@@ -654,7 +654,7 @@ void walk_simple_aux(const orc_ctx* c, int64_t ni, int np, const double (*xs)[3]
                      int64_t& partner, Counters& cnt, const double* tqs) {
   const Node& nd = c->nodes[ni];
   const double eps2 = c->p.eps2;
-  double d[32][3], d2[32];
+  double d[64][3], d2[64];
   if (nd.descendants == 0) {
     partner += 1;
     for (int ip = 0; ip < np; ++ip) {
@@ -1125,7 +1125,12 @@ int orc_traverse_tree(orc_ctx* c, int64_t nt, const double* tx, const double* ty
   } else {
     std::vector<std::pair<int64_t, int64_t>> tiles;
     int err = 0;
-    if (tkeys == nullptr) {
+    if (c->p.walk == 2) {
+      // the GPU library's group walk: buckets of tile_size (<= 64)
+      // key-consecutive targets with the simple walk's rule
+      const int64_t g = std::min(64, std::max(1, c->p.tile_size));
+      for (int64_t i = 0; i < nt; i += g) tiles.push_back({i, std::min(nt, i + g)});
+    } else if (tkeys == nullptr) {
       for (int64_t i = 0; i < nt; ++i) tiles.push_back({i, i + 1});
     } else {
       make_tiles(tkeys, 0, nt, 1, 0, std::min(32, std::max(1, c->p.tile_size)), tiles, err);
@@ -1133,7 +1138,7 @@ int orc_traverse_tree(orc_ctx* c, int64_t nt, const double* tx, const double* ty
     }
     parallel_for((int64_t)tiles.size(), nth, [&](int64_t it, int t) {
       int64_t lo = tiles[it].first, np = tiles[it].second - tiles[it].first;
-      double xs[32][3], e[32][3], ph[32], w[32], qs[32];
+      double xs[64][3], e[64][3], ph[64], w[64], qs[64];
       for (int k = 0; k < np; ++k) {
         qs[k] = tq ? tq[lo + k] : 0.0;
         xs[k][0] = tx[lo + k]; xs[k][1] = ty[lo + k]; xs[k][2] = tz[lo + k];

@@ -26,7 +26,8 @@ typedef struct orc_params {
   double theta2;            /* square of the BH opening angle (default 0.36) */
   double eps2;              /* Plummer softening squared (default 0) */
   int32_t curve;            /* 0 = Hilbert (reference), 1 = Morton (extra) */
-  int32_t walk;             /* 0 = pthreads (per-target LIFO), 1 = simple (tile) */
+  int32_t walk;             /* 0 = pthreads (per-target LIFO), 1 = simple (tile), 2 = buckets
+                               of tile_size (<= 64) consecutive targets, simple rule */
   int32_t tile_size;        /* simple walk tile size (reference: 16) */
   int32_t force_cubic_domain;
   int32_t periodicity[3];

@@ -73,7 +73,8 @@ class Params(C.Structure):
         ("device", C.c_int32),
         ("overwrite_results", C.c_int32),
         ("kelbg_invsqrttemp", C.c_double),
-        ("reserved", C.c_int32 * 4),
+        ("group_size", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -435,10 +436,10 @@ def mac(theta2, dist2, boxlength2):
     return bool(a.value)
 
 
-def shard_range(n, rank, world, align=32):
+def shard_range(n, rank, world, align=64):
     """[t0, t1) of the key-ordered targets for one of `world` ranks: contiguous,
     disjoint, covering [0, n), with every boundary a multiple of `align` so each
-    rank's 32-target groups are the single-GPU ones."""
+    rank's group-walk buckets (32 or 64 targets) are the single-GPU ones."""
     if world < 1 or not 0 <= rank < world:
         raise ValueError("need 0 <= rank < world")
     blocks = (n + align - 1) // align
@@ -447,7 +448,7 @@ def shard_range(n, rank, world, align=32):
     return min(n, b0 * align), min(n, b1 * align)
 
 
-def gather_shards(local, n, rank, world, align=32, group=None):
+def gather_shards(local, n, rank, world, align=64, group=None):
     """The exchange of a target-sharded traverse: every rank's share of the
     key-ordered fields (local: a (k, t1 - t0) tensor of this rank's
     shard_range share, k fields) gathered on every rank as a (k, n) tensor.

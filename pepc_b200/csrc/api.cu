@@ -166,6 +166,10 @@ static int check_params(Ctx* c, const pepcg_params* p) {
     c->err = "theta2 and eps2 must be >= 0";
     return PEPCG_ERR_BAD_ARG;
   }
+  if (p->group_size != 0 && p->group_size != 32 && p->group_size != 64) {
+    c->err = "group_size must be 0 (automatic), 32 or 64";
+    return PEPCG_ERR_BAD_ARG;
+  }
   if (p->mirror_box_layers < 0 || p->mirror_box_layers > 2) {
     c->err = "mirror_box_layers must be in 0..2";
     return PEPCG_ERR_BAD_ARG;
@@ -586,7 +590,7 @@ int pepcg_traverse_tree(void* ctx, int64_t nt, const double* tx, const double* t
     // the upload and only 1/16 of the download trails it
     if (!copy_streams(c)) return PEPCG_ERR_CUDA;
     const int nch = 3;
-    auto al = [](int64_t v) { return v & ~(int64_t)31; };
+    auto al = [](int64_t v) { return v & ~(int64_t)63; };  // whole group-walk buckets
     const int64_t bounds[nch + 1] = {0, al(nt / 16), al(nt - nt / 16), nt};
     bool ok = true;
     for (int k = 0; k < nch; ++k) {

@@ -175,6 +175,10 @@ struct Ctx {
   int32_t* nleaves_ptr() { return nleaves.p; }
   // The persistent walks take buckets from a counter in the context's own
   // memory, so walks of different contexts may run concurrently on one device.
+  // targets per bucket of the group walk (pepcg_params.group_size, 0 resolved)
+  int group_size() const {
+    return prm.group_size ? prm.group_size : (prm.precision == PEPCG_PRECISION_MIXED ? 64 : 32);
+  }
   // Slot 0 serves walks on the context stream, slot 1 walks on walk2.
   unsigned int* walk_queue(int slot = 0) { return reinterpret_cast<unsigned int*>(d_small + 8 + slot); }
   unsigned long long* item_queue() { return d_small + 10; }

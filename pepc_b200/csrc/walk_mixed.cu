@@ -109,6 +109,34 @@ __device__ __forceinline__ void twig32(float4 m0, float4 m1, float4 m2, float dx
   az = fmaf(rd3, fmaf(t4, dz, fmaf(m2r, vz, m0.z)), az);
 }
 
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+// twig32 for two targets against the same node in packed FP32 (sm_100
+// FFMA2 / FMUL2 / FADD2): each operation evaluates both targets' terms, and
+// the node's moments enter as (m, m) pairs.  Per target the arithmetic is
+// twig32's, operation for operation.
+__device__ __forceinline__ void twig32x2(float4 m0, float4 m1, float4 m2, float2 dx, float2 dy,
+                                         float2 dz, float2 eps2, float2& ax, float2& ay,
+                                         float2& az, float2& ap) {
+  const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
+  const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+  const float2 ri2 = __fmul2_rn(ri, ri);
+  const float2 rd3 = __fmul2_rn(ri, ri2);
+  const float2 q = f2(m2.z);
+  const float2 A = __ffma2_rn(dx, f2(m0.x), __ffma2_rn(dy, f2(m0.y), __ffma2_rn(dz, f2(m0.z), f2(m2.y))));
+  const float2 vx = __ffma2_rn(f2(m0.w), dx, __ffma2_rn(f2(m1.z), dy, __fmul2_rn(f2(m2.x), dz)));
+  const float2 vy = __ffma2_rn(f2(m1.z), dx, __ffma2_rn(f2(m1.x), dy, __fmul2_rn(f2(m1.w), dz)));
+  const float2 vz = __ffma2_rn(f2(m2.x), dx, __ffma2_rn(f2(m1.w), dy, __fmul2_rn(f2(m1.y), dz)));
+  const float2 B = __ffma2_rn(dx, vx, __ffma2_rn(dy, vy, __fmul2_rn(dz, vz)));
+  const float2 t1 = __ffma2_rn(ri2, B, make_float2(-A.x, -A.y));
+  ap = __ffma2_rn(ri, __ffma2_rn(ri2, t1, q), ap);
+  const float2 t4 = __ffma2_rn(ri2, __ffma2_rn(f2(5.0f), t1, __fadd2_rn(A, A)), q);
+  const float2 m2r = __fmul2_rn(f2(-2.0f), ri2);
+  ax = __ffma2_rn(rd3, __ffma2_rn(t4, dx, __ffma2_rn(m2r, vx, f2(m0.x))), ax);
+  ay = __ffma2_rn(rd3, __ffma2_rn(t4, dy, __ffma2_rn(m2r, vy, f2(m0.y))), ay);
+  az = __ffma2_rn(rd3, __ffma2_rn(t4, dz, __ffma2_rn(m2r, vz, f2(m0.z))), az);
+}
+
 __device__ __forceinline__ void warp_add3(unsigned long long* ctr, unsigned long long a,
                                           unsigned long long b, unsigned long long c) {
   for (int o = 16; o > 0; o >>= 1) {
@@ -168,7 +196,7 @@ __device__ __forceinline__ void cp_async_wait_all() {
 }
 
 struct __align__(16) StagedTwig {
-  float4 c;   // (coc - g) rounded from FP64, charge
+  float4 c;   // (coc - g) rounded from FP64 (k_walk_group64: its negation), charge
   float4 m0;  // px py pz 3qxx
   float4 m1;  // 3qyy 3qzz 1.5qxy 1.5qyz
   float4 m2;  // 1.5qzx, trace, charge, -
@@ -416,6 +444,275 @@ __global__ void __launch_bounds__(kMixThreads, 5)
   warp_add3(A.counters, c_leaf, c_twig, c_mac);
 }
 
+// Group walk over buckets of 64 key-consecutive targets (group_size 64), two
+// per lane: lane k holds targets t0 + k and t0 + 32 + k.  The traversal, the
+// MAC rule (a twig is accepted only if all 64 targets pass) and the staging
+// are those of k_walk_group_wide.  Each staged record is read from shared
+// memory once for both of the lane's targets, and the twig interactions of
+// the pair run as packed FP32 (twig32x2).  Twig records store the node's
+// offset from the group centre negated, so that the pair's offsets are one
+// packed add.  Against 32-target buckets the larger group is opened more
+// often (about 9 % more interactions at 4M, theta 0.4); the packed pair
+// arithmetic and the halved traversal per target more than pay for it.
+__global__ void __launch_bounds__(kMixThreads, 5)
+    k_walk_group64(MixArgs A, int* __restrict__ gstack, const int4* __restrict__ child8,
+                   const int* __restrict__ nchild) {
+  __shared__ float s_bl2[kMaxLevel + 1];
+  __shared__ double s_vb[3 * 125];
+  __shared__ StagedTwig s_tw[kWW][kRing];
+  __shared__ StagedLeaf s_lf[kWW][kRing];
+  for (int i = threadIdx.x; i <= kMaxLevel; i += blockDim.x) s_bl2[i] = (float)A.bl2[i];
+  for (int i = threadIdx.x; i < 3 * A.nbox; i += blockDim.x) s_vb[i] = A.vbox[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  int* stack = gstack + (int64_t)(blockIdx.x * kWW + w) * kStackCap;
+  StagedTwig* stw = s_tw[w];
+  StagedLeaf* stl = s_lf[w];
+  const float theta2 = A.theta2;
+  const int64_t nbuckets = (A.nt + 63) / 64;
+  unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
+  for (;;) {
+    unsigned b = 0;
+    if (lane == 0) b = atomicAdd(A.queue, 1u);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    if ((int64_t)b >= nbuckets) break;
+    const int64_t t0 = (int64_t)b * 64;
+    const int cnt = (int)min((int64_t)64, A.nt - t0);
+    const bool v0 = lane < cnt, v1 = lane + 32 < cnt;
+    const unsigned vm0 = __ballot_sync(0xffffffffu, v0), vm1 = __ballot_sync(0xffffffffu, v1);
+    const int64_t ta = t0 + lane, tb = t0 + 32 + lane;
+    double pxa = 0, pya = 0, pza = 0, pxb = 0, pyb = 0, pzb = 0;
+    double Ea0 = 0, Ea1 = 0, Ea2 = 0, PHa = 0, Eb0 = 0, Eb1 = 0, Eb2 = 0, PHb = 0;
+    double W = 0;  // interactions of this call (the same list for all targets)
+    if (v0) {
+      pxa = A.tx[ta]; pya = A.ty[ta]; pza = A.tz[ta];
+      Ea0 = A.ex[ta]; Ea1 = A.ey[ta]; Ea2 = A.ez[ta]; PHa = A.pot[ta];
+    }
+    if (v1) {
+      pxb = A.tx[tb]; pyb = A.ty[tb]; pzb = A.tz[tb];
+      Eb0 = A.ex[tb]; Eb1 = A.ey[tb]; Eb2 = A.ez[tb]; PHb = A.pot[tb];
+    }
+    double lo[3] = {v0 ? pxa : INFINITY, v0 ? pya : INFINITY, v0 ? pza : INFINITY};
+    double hi[3] = {v0 ? pxa : -INFINITY, v0 ? pya : -INFINITY, v0 ? pza : -INFINITY};
+    if (v1) {
+      lo[0] = fmin(lo[0], pxb); lo[1] = fmin(lo[1], pyb); lo[2] = fmin(lo[2], pzb);
+      hi[0] = fmax(hi[0], pxb); hi[1] = fmax(hi[1], pyb); hi[2] = fmax(hi[2], pzb);
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      for (int o = 16; o > 0; o >>= 1) {
+        lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+        hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+      }
+    const double g0x = 0.5 * (lo[0] + hi[0]), g0y = 0.5 * (lo[1] + hi[1]), g0z = 0.5 * (lo[2] + hi[2]);
+    const float rxa = (float)(pxa - g0x), rya = (float)(pya - g0y), rza = (float)(pza - g0z);
+    const float rxb = (float)(pxb - g0x), ryb = (float)(pyb - g0y), rzb = (float)(pzb - g0z);
+    float rg = fmaxf(v0 ? sqrtf(rxa * rxa + rya * rya + rza * rza) : 0.f,
+                     v1 ? sqrtf(rxb * rxb + ryb * ryb + rzb * rzb) : 0.f);
+    for (int o = 16; o > 0; o >>= 1) rg = fmaxf(rg, __shfl_xor_sync(0xffffffffu, rg, o));
+    rg = rg * 1.0001f + 1e-30f;
+    bool complete = true;
+    for (int ib = 0; ib < A.nbox; ++ib) {
+      const double vx = s_vb[3 * ib], vy = s_vb[3 * ib + 1], vz = s_vb[3 * ib + 2];
+      const double gx = g0x - vx, gy = g0y - vy, gz = g0z - vz;
+      int64_t partner = 0;
+      int nT = 0, hT = 0, nL = 0, hL = 0;
+      int top = 1;
+      if (lane == 0) stack[0] = 0;
+      __syncwarp();
+      auto flush_twigs = [&](int n) {
+        cp_async_wait_all();
+        __syncwarp();
+        if (v0) {
+          float2 PX = f2(0.f), PY = f2(0.f), PZ = f2(0.f), PP = f2(0.f);
+          const float2 RX = make_float2(rxa, rxb), RY = make_float2(rya, ryb), RZ = make_float2(rza, rzb);
+          const float2 E2 = f2(A.eps2);
+          const int n1 = min(n, kRing - hT);
+          const StagedTwig* r = stw + hT;
+#pragma unroll 8
+          for (int j = 0; j < n1; ++j) {
+            const float4 c = r[j].c, m0 = r[j].m0, m1 = r[j].m1, m2 = r[j].m2;
+            twig32x2(m0, m1, m2, __fadd2_rn(RX, f2(c.x)), __fadd2_rn(RY, f2(c.y)), __fadd2_rn(RZ, f2(c.z)), E2, PX, PY, PZ, PP);
+          }
+#pragma unroll 4
+          for (int j = 0; j < n - n1; ++j) {
+            const float4 c = stw[j].c, m0 = stw[j].m0, m1 = stw[j].m1, m2 = stw[j].m2;
+            twig32x2(m0, m1, m2, __fadd2_rn(RX, f2(c.x)), __fadd2_rn(RY, f2(c.y)), __fadd2_rn(RZ, f2(c.z)), E2, PX, PY, PZ, PP);
+          }
+          Ea0 += (double)PX.x; Ea1 += (double)PY.x; Ea2 += (double)PZ.x; PHa += (double)PP.x;
+          Eb0 += (double)PX.y; Eb1 += (double)PY.y; Eb2 += (double)PZ.y; PHb += (double)PP.y;
+          c_twig += (unsigned)n * (v1 ? 2u : 1u);
+        }
+        W += (double)n;
+        hT = (hT + n) & (kRing - 1);
+        nT -= n;
+        __syncwarp();
+      };
+      auto flush_leaves = [&](int n) {
+        __syncwarp();
+        if (v0) {
+          float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f, bx = 0.f, by = 0.f, bz = 0.f, bp = 0.f;
+          auto leaf = [&](const StagedLeaf& r) {
+            const float4 c = r.c;
+            float dx = rxa - c.x, dy = rya - c.y, dz = rza - c.z;
+            bool use = true;
+            if (dx == 0.f && dy == 0.f && dz == 0.f) {
+              // self (dist2 == 0 in FP64) or two points closer than the FP32
+              // resolution at the group scale: decide and evaluate in FP64
+              const double ex = (A.tx[ta] - vx) - r.x, ey = (A.ty[ta] - vy) - r.y,
+                           ez = (A.tz[ta] - vz) - r.z;
+              if (ex == 0.0 && ey == 0.0 && ez == 0.0) use = false;
+              dx = (float)ex; dy = (float)ey; dz = (float)ez;
+            }
+            if (use) {
+              leaf32(c.w, dx, dy, dz, A.eps2, ax, ay, az, ap);
+              ++c_leaf;
+            }
+            dx = rxb - c.x; dy = ryb - c.y; dz = rzb - c.z;
+            use = v1;
+            if (v1 && dx == 0.f && dy == 0.f && dz == 0.f) {
+              const double ex = (A.tx[tb] - vx) - r.x, ey = (A.ty[tb] - vy) - r.y,
+                           ez = (A.tz[tb] - vz) - r.z;
+              if (ex == 0.0 && ey == 0.0 && ez == 0.0) use = false;
+              dx = (float)ex; dy = (float)ey; dz = (float)ez;
+            }
+            if (use) {
+              leaf32(c.w, dx, dy, dz, A.eps2, bx, by, bz, bp);
+              ++c_leaf;
+            }
+          };
+          const int n1 = min(n, kRing - hL);
+          const StagedLeaf* r = stl + hL;
+#pragma unroll 4
+          for (int j = 0; j < n1; ++j) leaf(r[j]);
+#pragma unroll 2
+          for (int j = 0; j < n - n1; ++j) leaf(stl[j]);
+          Ea0 += (double)ax; Ea1 += (double)ay; Ea2 += (double)az; PHa += (double)ap;
+          Eb0 += (double)bx; Eb1 += (double)by; Eb2 += (double)bz; PHb += (double)bp;
+        }
+        W += (double)n;
+        hL = (hL + n) & (kRing - 1);
+        nL -= n;
+        __syncwarp();
+      };
+      while (top > 0) {
+        const int take = top < 32 ? top : 32;
+        top -= take;
+        const int node = lane < take ? stack[top + lane] : -1;
+        __syncwarp();
+        bool isleaf = false, accept = false, open = false, amb = false;
+        float cx = 0.f, cy = 0.f, cz = 0.f, bl = 0.f;
+        double4 a = make_double4(0, 0, 0, 0);
+        int nlv = 0, nch = 0;
+        int4 c0 = make_int4(0, 0, 0, 0), c1 = c0;
+        if (node >= 0) {
+          a = A.nc4[node];
+          const int2 mu = A.meta[node];
+          nlv = A.nleaves[node];
+          nch = nchild[node];
+          c0 = child8[2 * (int64_t)node];
+          c1 = child8[2 * (int64_t)node + 1];
+          cx = (float)(a.x - gx); cy = (float)(a.y - gy); cz = (float)(a.z - gz);
+          if (mu.y & kLeafFlag) {
+            isleaf = true;
+          } else {
+            bl = A.macb ? (float)A.macb[node] : s_bl2[mu.y & 0xff];
+            const float dc = sqrtf(cx * cx + cy * cy + cz * cz);
+            const float dmin = dc - rg, dmax = dc + rg;
+            if (dmin > 0.f && theta2 * (dmin * dmin) > bl) {
+              accept = true;
+              c_mac += 1;
+            } else if (!(theta2 * (dmax * dmax) > bl)) {
+              open = true;
+              c_mac += 1;
+            } else {
+              amb = true;
+            }
+          }
+        }
+        unsigned am = __ballot_sync(0xffffffffu, amb);
+        while (am) {
+          const int j = __ffs(am) - 1;
+          am &= am - 1;
+          const float ux = __shfl_sync(0xffffffffu, cx, j);
+          const float uy = __shfl_sync(0xffffffffu, cy, j);
+          const float uz = __shfl_sync(0xffffffffu, cz, j);
+          const float ub = __shfl_sync(0xffffffffu, bl, j);
+          float dx = rxa - ux, dy = rya - uy, dz = rza - uz;
+          const bool fa = v0 && !(theta2 * fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > ub);
+          dx = rxb - ux; dy = ryb - uy; dz = rzb - uz;
+          const bool fb = v1 && !(theta2 * fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > ub);
+          const unsigned f0 = __ballot_sync(0xffffffffu, fa);
+          const unsigned f1 = __ballot_sync(0xffffffffu, fb);
+          if (lane == j) {
+            accept = (f0 | f1) == 0;
+            open = !accept;
+            // MAC evaluations up to the first failing target, in target order
+            c_mac += (unsigned)(f0 ? __popc(vm0 & ((2u << (__ffs(f0) - 1)) - 1u))
+                                   : __popc(vm0) + (f1 ? __popc(vm1 & ((2u << (__ffs(f1) - 1)) - 1u))
+                                                       : __popc(vm1)));
+          }
+        }
+        const unsigned lb = __ballot_sync(0xffffffffu, isleaf);
+        const unsigned ab = __ballot_sync(0xffffffffu, accept);
+        if (isleaf) {
+          StagedLeaf& r = stl[(hL + nL + __popc(lb & lt)) & (kRing - 1)];
+          r.c = make_float4(cx, cy, cz, (float)a.w);
+          r.x = a.x; r.y = a.y; r.z = a.z;
+          partner += 1;
+        }
+        if (accept) {
+          StagedTwig& r = stw[(hT + nT + __popc(ab & lt)) & (kRing - 1)];
+          r.c = make_float4(-cx, -cy, -cz, (float)a.w);
+          const float4* m = A.mom32 + kMom32Stride * (int64_t)node;
+          cp_async16(&r.m0, m);
+          cp_async16(&r.m1, m + 1);
+          cp_async16(&r.m2, m + 2);
+          partner += nlv;
+        }
+        nL += __popc(lb);
+        nT += __popc(ab);
+        const int npush = open ? min(8, nch) : 0;
+        int total;
+        const int off = warp_excl_scan(npush, lane, total);
+        if (top + total > kStackCap) {
+          complete = false;
+          break;
+        }
+        if (npush > 0) {
+          int* dst = stack + top + off;
+          dst[0] = c0.x;
+          if (npush > 1) dst[1] = c0.y;
+          if (npush > 2) dst[2] = c0.z;
+          if (npush > 3) dst[3] = c0.w;
+          if (npush > 4) dst[4] = c1.x;
+          if (npush > 5) dst[5] = c1.y;
+          if (npush > 6) dst[6] = c1.z;
+          if (npush > 7) dst[7] = c1.w;
+        }
+        top += total;
+        __syncwarp();
+        if (nT >= 32) flush_twigs(32);
+        if (nL >= 32) flush_leaves(32);
+      }
+      if (nT > 0) flush_twigs(nT);
+      if (nL > 0) flush_leaves(nL);
+      for (int o = 16; o > 0; o >>= 1) partner += __shfl_xor_sync(0xffffffffu, partner, o);
+      if (partner != A.npart) complete = false;
+    }
+    if (v0) {
+      A.ex[ta] = Ea0; A.ey[ta] = Ea1; A.ez[ta] = Ea2; A.pot[ta] = PHa; A.work[ta] = A.work[ta] + W;
+    }
+    if (v1) {
+      A.ex[tb] = Eb0; A.ey[tb] = Eb1; A.ez[tb] = Eb2; A.pot[tb] = PHb; A.work[tb] = A.work[tb] + W;
+    }
+    if (__any_sync(0xffffffffu, !complete) && lane == 0) atomicOr(A.status, ST_INCOMPLETE);
+  }
+  cp_async_wait_all();
+  warp_add3(A.counters, c_leaf, c_twig, c_mac);
+}
+
 // Simple-walk semantics (module_tree_walk_simple.f90:256-385) with several
 // reference tiles per warp and FP32 interactions: the whole tiles of one
 // pack (at most 32 targets, k_pack_tiles) walk the tree together in forward
@@ -656,8 +953,12 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
     const int gblocks = 148 * 5;
     const size_t per = (size_t)gblocks * kWW * kStackCap;
     if (!ensure(c, c->wstack, 2 * per, "walk stacks")) return PEPCG_ERR_OOM;
-    k_walk_group_wide<<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p + slot * per, c->child8.p,
-                                                      c->nchild.p);
+    if (tiles == nullptr && c->group_size() == 64)
+      k_walk_group64<<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p + slot * per, c->child8.p,
+                                                     c->nchild.p);
+    else
+      k_walk_group_wide<<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p + slot * per, c->child8.p,
+                                                        c->nchild.p);
   }
   return cuda_ok(c, cudaGetLastError(), "mixed walk launch") ? PEPCG_OK : PEPCG_ERR_CUDA;
 }

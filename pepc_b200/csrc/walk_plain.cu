@@ -152,10 +152,17 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_target64(WalkArgs A) {
   warp_add_counters(A.counters, c_leaf, c_twig, c_mac);
 }
 
-template <int kLaw>
-// Six resident blocks per SM: the plain group walk at 4M takes 223 ms against
-// 270 ms at the unbounded 108 registers.
-__global__ void __launch_bounds__(kWalkThreads, 6) k_walk_tile64(WalkArgs A) {
+// One warp per tile (PER_TILE tiles of up to 32 targets) or per group-walk
+// bucket (GROUP: kTPL x 32 key-consecutive targets, kTPL targets per lane,
+// lane k holding targets t0 + k + 32 s).  A twig is accepted only if every
+// target of the tile passes the MAC (module_tree_walk_simple.f90:343-382);
+// children are visited first to last through fwd, so each target's
+// interactions come in the reference's order.
+// Launch bounds: six resident blocks per SM for one target per lane (the
+// plain group walk at 4M takes 223 ms against 270 ms at the unbounded 108
+// registers), four for two.
+template <int kLaw, int kTPL>
+__global__ void __launch_bounds__(kWalkThreads, kTPL == 1 ? 6 : 4) k_walk_tile64(WalkArgs A) {
   __shared__ double s_bl2[kMaxLevel + 1];
   __shared__ double s_vb[3 * 125];
   for (int i = threadIdx.x; i <= kMaxLevel; i += blockDim.x) s_bl2[i] = A.bl2[i];
@@ -163,23 +170,32 @@ __global__ void __launch_bounds__(kWalkThreads, 6) k_walk_tile64(WalkArgs A) {
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const unsigned M = (unsigned)A.M;
+  constexpr int kB = 32 * kTPL;  // GROUP bucket size
   unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
   for (;;) {
     unsigned b = 0;
     if (lane == 0) b = atomicAdd(A.queue, 1u);
     b = __shfl_sync(0xffffffffu, b, 0);
-    const int64_t nbk = A.tiles ? A.ntiles : (A.nt + 31) / 32;
+    const int64_t nbk = A.tiles ? A.ntiles : (A.nt + kB - 1) / kB;
     if ((int64_t)b >= nbk) break;
     const int2 tl = A.tiles ? A.tiles[b]
-                            : make_int2((int)((int64_t)b * 32), (int)min((int64_t)32, A.nt - (int64_t)b * 32));
-    const bool valid = lane < tl.y;
-    const int64_t t = (int64_t)tl.x + lane;
-    double px = 0, py = 0, pz = 0, e0 = 0, e1 = 0, e2 = 0, ph = 0, w = 0;
-    KelbgArgs kel{0.0, A.kinv, A.sqrtpi};
-    if (valid) {
-      px = A.tx[t]; py = A.ty[t]; pz = A.tz[t];
-      if (kLaw == 5) kel.tq = A.tq[t];
-      e0 = A.ex[t]; e1 = A.ey[t]; e2 = A.ez[t]; ph = A.pot[t]; w = A.work[t];
+                            : make_int2((int)((int64_t)b * kB), (int)min((int64_t)kB, A.nt - (int64_t)b * kB));
+    bool valid[kTPL];
+    int64_t t[kTPL];
+    double px[kTPL], py[kTPL], pz[kTPL], e0[kTPL], e1[kTPL], e2[kTPL], ph[kTPL], w[kTPL];
+    KelbgArgs kel[kTPL];
+#pragma unroll
+    for (int s = 0; s < kTPL; ++s) {
+      valid[s] = lane + 32 * s < tl.y;
+      t[s] = (int64_t)tl.x + lane + 32 * s;
+      px[s] = py[s] = pz[s] = e0[s] = e1[s] = e2[s] = ph[s] = w[s] = 0.0;
+      kel[s] = KelbgArgs{0.0, A.kinv, A.sqrtpi};
+      if (valid[s]) {
+        px[s] = A.tx[t[s]]; py[s] = A.ty[t[s]]; pz[s] = A.tz[t[s]];
+        if (kLaw == 5) kel[s].tq = A.tq[t[s]];
+        e0[s] = A.ex[t[s]]; e1[s] = A.ey[t[s]]; e2[s] = A.ez[t[s]]; ph[s] = A.pot[t[s]];
+        w[s] = A.work[t[s]];
+      }
     }
     bool complete = true;
     for (int ib = 0; ib < A.nbox; ++ib) {
@@ -191,39 +207,56 @@ __global__ void __launch_bounds__(kWalkThreads, 6) k_walk_tile64(WalkArgs A) {
         const int2 mu = A.meta[u];
         const int2 fw = A.fwd[u];
         // d = (x - vbox) - coc (module_tree_walk_simple.f90:328,345)
-        const double dx = (px - vx) - a.x, dy = (py - vy) - a.y, dz = (pz - vz) - a.z;
-        const double dist2 = (dx * dx + dy * dy) + dz * dz;
+        double dx[kTPL], dy[kTPL], dz[kTPL], dist2[kTPL];
+#pragma unroll
+        for (int s = 0; s < kTPL; ++s) {
+          dx[s] = (px[s] - vx) - a.x; dy[s] = (py[s] - vy) - a.y; dz[s] = (pz[s] - vz) - a.z;
+          dist2[s] = (dx[s] * dx[s] + dy[s] * dy[s]) + dz[s] * dz[s];
+        }
         if (mu.y & kLeafFlag) {
           partner += 1;
-          if (valid) {
-            w += 1.0;
-            ++c_leaf;
-            if (dist2 > 0.0) {
-              double fx, fy, fz, fp;
-              law_leaf64<kLaw>(a.w, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp, kel);
-              e0 += fx; e1 += fy; e2 += fz; ph += fp;
+#pragma unroll
+          for (int s = 0; s < kTPL; ++s)
+            if (valid[s]) {
+              w[s] += 1.0;
+              ++c_leaf;
+              if (dist2[s] > 0.0) {
+                double fx, fy, fz, fp;
+                law_leaf64<kLaw>(a.w, dx[s], dy[s], dz[s], dist2[s], A.eps2, fx, fy, fz, fp, kel[s]);
+                e0[s] += fx; e1[s] += fy; e2[s] += fz; ph[s] += fp;
+              }
             }
-          }
           u = (unsigned)fw.y;
         } else {
-          const bool ok =
-              !valid || (A.theta2 * dist2 > (A.macb ? A.macb[u] : s_bl2[mu.y & 0xff]));
-          const unsigned fail = __ballot_sync(0xffffffffu, !ok);
-          // MAC evaluations stop at the first failing target (:343-370)
-          const int first_fail = fail ? __ffs(fail) - 1 : 32;
-          if (valid && lane <= first_fail) ++c_mac;
-          if (fail == 0) {
-            partner += A.nleaves[u];
-            if (valid) {
-              double m[9];
+          const double thr = A.macb ? A.macb[u] : s_bl2[mu.y & 0xff];
+          // MAC evaluations stop at the tile's first failing target, in
+          // target order (:343-370)
+          int first_fail = kB;
+          unsigned any_fail = 0;
 #pragma unroll
-              for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
-              double fx, fy, fz, fp;
-              law_twig64<kLaw>(a.w, m, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp);
-              e0 += fx; e1 += fy; e2 += fz; ph += fp;
-              w += 1.0;
-              ++c_twig;
-            }
+          for (int s = 0; s < kTPL; ++s) {
+            const bool ok = !valid[s] || (A.theta2 * dist2[s] > thr);
+            const unsigned fail = __ballot_sync(0xffffffffu, !ok);
+            if (fail && first_fail == kB) first_fail = 32 * s + __ffs(fail) - 1;
+            any_fail |= fail;
+          }
+#pragma unroll
+          for (int s = 0; s < kTPL; ++s)
+            if (valid[s] && lane + 32 * s <= first_fail) ++c_mac;
+          if (any_fail == 0) {
+            partner += A.nleaves[u];
+            double m[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
+#pragma unroll
+            for (int s = 0; s < kTPL; ++s)
+              if (valid[s]) {
+                double fx, fy, fz, fp;
+                law_twig64<kLaw>(a.w, m, dx[s], dy[s], dz[s], dist2[s], A.eps2, fx, fy, fz, fp);
+                e0[s] += fx; e1[s] += fy; e2[s] += fz; ph[s] += fp;
+                w[s] += 1.0;
+                ++c_twig;
+              }
             u = (unsigned)fw.y;
           } else {
             u = (unsigned)fw.x;
@@ -232,9 +265,12 @@ __global__ void __launch_bounds__(kWalkThreads, 6) k_walk_tile64(WalkArgs A) {
       }
       if (partner != A.npart) complete = false;
     }
-    if (valid) {
-      A.ex[t] = e0; A.ey[t] = e1; A.ez[t] = e2; A.pot[t] = ph; A.work[t] = w;
-    }
+#pragma unroll
+    for (int s = 0; s < kTPL; ++s)
+      if (valid[s]) {
+        A.ex[t[s]] = e0[s]; A.ey[t[s]] = e1[s]; A.ez[t[s]] = e2[s]; A.pot[t[s]] = ph[s];
+        A.work[t[s]] = w[s];
+      }
     if (!complete && lane == 0) atomicOr(A.status, ST_INCOMPLETE);
   }
   warp_add_counters(A.counters, c_leaf, c_twig, c_mac);
@@ -595,7 +631,7 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
     bool ok = walk != PEPCG_WALK_PER_TILE && !c->far_field && nchunks <= Ctx::kMaxChunks &&
               plan->bounds[0] == 0 && plan->bounds[nchunks] == nt;
     for (int k = 1; ok && k < nchunks; ++k)
-      ok = plan->bounds[k] % 32 == 0 && plan->bounds[k] >= plan->bounds[k - 1];
+      ok = plan->bounds[k] % c->group_size() == 0 && plan->bounds[k] >= plan->bounds[k - 1];
     if (!ok) {
       c->err = "traverse: invalid chunk plan";
       return PEPCG_ERR_BAD_ARG;
@@ -667,10 +703,17 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
           else k_walk_tilepack64<3><<<blocks, kWalkThreads, 0, sk>>>(A);
         } else {
           if (walk == PEPCG_WALK_GROUP) A.tiles = nullptr;
-          if (law == 2) k_walk_tile64<2><<<blocks, kWalkThreads, 0, sk>>>(A);
-          else if (law == 4) k_walk_tile64<4><<<blocks, kWalkThreads, 0, sk>>>(A);
-          else if (law == 5) k_walk_tile64<5><<<blocks, kWalkThreads, 0, sk>>>(A);
-          else k_walk_tile64<3><<<blocks, kWalkThreads, 0, sk>>>(A);
+          if (walk == PEPCG_WALK_GROUP && c->group_size() == 64) {
+            if (law == 2) k_walk_tile64<2, 2><<<blocks, kWalkThreads, 0, sk>>>(A);
+            else if (law == 4) k_walk_tile64<4, 2><<<blocks, kWalkThreads, 0, sk>>>(A);
+            else if (law == 5) k_walk_tile64<5, 2><<<blocks, kWalkThreads, 0, sk>>>(A);
+            else k_walk_tile64<3, 2><<<blocks, kWalkThreads, 0, sk>>>(A);
+          } else {
+            if (law == 2) k_walk_tile64<2, 1><<<blocks, kWalkThreads, 0, sk>>>(A);
+            else if (law == 4) k_walk_tile64<4, 1><<<blocks, kWalkThreads, 0, sk>>>(A);
+            else if (law == 5) k_walk_tile64<5, 1><<<blocks, kWalkThreads, 0, sk>>>(A);
+            else k_walk_tile64<3, 1><<<blocks, kWalkThreads, 0, sk>>>(A);
+          }
         }
       } else {
         int rc = launch_walk_mixed(c, t1 - t0, A.tx, A.ty, A.tz, A.ex, A.ey, A.ez, A.pot, A.work,

@@ -207,3 +207,13 @@ def test_adjoint_rejects_periodic_far_field(gpu):
     with pytest.raises(P.PepcgError) as ei:
         tc.traverse_adjoint(x[:5], y[:5], z[:5], [np.zeros(5)] * 3, np.ones(5), 200)
     assert ei.value.code == P.PEPCG_ERR_UNSUPPORTED
+
+
+def test_adjoint_rejects_group_of_64(gpu):
+    rng = np.random.default_rng(6)
+    x, y, z, q = rng.random(300), rng.random(300), rng.random(300), rng.standard_normal(300)
+    tc = P.TreeCode(walk=P.WALK_GROUP, group_size=64)
+    tc.pepc_grow_tree(x, y, z, q)
+    with pytest.raises(P.PepcgError) as ei:
+        tc.traverse_adjoint(x[:5], y[:5], z[:5], [np.zeros(5)] * 3, np.ones(5), 300)
+    assert ei.value.code == P.PEPCG_ERR_UNSUPPORTED

@@ -27,10 +27,11 @@ def relerr(r, d, idx):
     return np.linalg.norm(E - Ed, axis=0) / np.linalg.norm(Ed, axis=0)
 
 
-@pytest.mark.parametrize("walk", [P.WALK_GROUP, P.WALK_PER_TARGET, P.WALK_PER_TILE])
-def test_mixed_matches_plain_same_walk(gpu, walk):
+@pytest.mark.parametrize("walk,gs", [(P.WALK_GROUP, 64), (P.WALK_GROUP, 32),
+                                     (P.WALK_PER_TARGET, 0), (P.WALK_PER_TILE, 0)])
+def test_mixed_matches_plain_same_walk(gpu, walk, gs):
     x, y, z, q = plummer(60000, 41)
-    kw = dict(theta2=0.16, eps2=1e-6, walk=walk)
+    kw = dict(theta2=0.16, eps2=1e-6, walk=walk, group_size=gs)
     tp, gp, rp = run(x, y, z, q, precision=P.PRECISION_PLAIN, **kw)
     tm, gm, rm = run(x, y, z, q, precision=P.PRECISION_MIXED, **kw)
     assert np.array_equal(gp.key, gm.key)
@@ -50,7 +51,7 @@ def test_mixed_matches_plain_same_walk(gpu, walk):
 def test_mixed_group_alternating_charges(gpu):
     # +-1 charges: strong cancellation, the hardest case for FP32 sums
     x, y, z, q = cube(40000, 42)
-    kw = dict(theta2=0.09, eps2=1e-4, walk=P.WALK_GROUP)
+    kw = dict(theta2=0.09, eps2=1e-4, walk=P.WALK_GROUP, group_size=64)
     tp, _, rp = run(x, y, z, q, precision=P.PRECISION_PLAIN, **kw)
     tm, _, rm = run(x, y, z, q, precision=P.PRECISION_MIXED, **kw)
     idx = np.arange(0, 40000, 11)
@@ -76,7 +77,7 @@ def test_mixed_group_periodic_matches_plain(gpu):
     n = 20000
     x, y, z = rng.random(n), rng.random(n), rng.random(n)
     q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
-    kw = dict(theta2=0.16, eps2=1e-4, walk=P.WALK_GROUP, periodicity=(1, 1, 1))
+    kw = dict(theta2=0.16, eps2=1e-4, walk=P.WALK_GROUP, periodicity=(1, 1, 1), group_size=64)
     _, _, rp = run(x, y, z, q, precision=P.PRECISION_PLAIN, **kw)
     _, _, rm = run(x, y, z, q, precision=P.PRECISION_MIXED, **kw)
     idx = np.arange(0, n, 7)
@@ -96,7 +97,7 @@ def test_mixed_group_ragged_buckets_and_duplicates(gpu):
     dup = rng.choice(n, 200, replace=False)
     x[dup[:100]], y[dup[:100]], z[dup[:100]] = x[dup[100:]], y[dup[100:]], z[dup[100:]]
     q = rng.standard_normal(n)
-    kw = dict(theta2=0.25, eps2=1e-4, walk=P.WALK_GROUP)
+    kw = dict(theta2=0.25, eps2=1e-4, walk=P.WALK_GROUP, group_size=64)
     tp, gp, rp = run(x, y, z, q, precision=P.PRECISION_PLAIN, **kw)
     tm, gm, rm = run(x, y, z, q, precision=P.PRECISION_MIXED, **kw)
     assert np.array_equal(gp.key, gm.key)
@@ -109,7 +110,7 @@ def test_mixed_group_ragged_buckets_and_duplicates(gpu):
 
 def test_mixed_group_bmax_mac_matches_plain(gpu):
     x, y, z, q = plummer(30000, 46)
-    kw = dict(theta2=0.36, eps2=1e-6, walk=P.WALK_GROUP, mac_select=1)
+    kw = dict(theta2=0.36, eps2=1e-6, walk=P.WALK_GROUP, mac_select=1, group_size=64)
     tp, _, rp = run(x, y, z, q, precision=P.PRECISION_PLAIN, **kw)
     tm, _, rm = run(x, y, z, q, precision=P.PRECISION_MIXED, **kw)
     idx = np.arange(0, 30000, 7)

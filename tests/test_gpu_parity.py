@@ -139,6 +139,23 @@ def test_walk_per_target_bit_exact(gpu, theta2):
     assert st["mac_evaluations"] == c["mac_evaluations"]
 
 
+@pytest.mark.parametrize("gs", [32, 64])
+def test_walk_group_bit_exact(gpu, gs):
+    # the group walk (buckets of gs key-consecutive targets, the simple walk's
+    # rule) against the oracle's bucketed walk; 20,000 targets leave a ragged
+    # last bucket
+    x, y, z, q = plummer(20000, 17)
+    tc = P.TreeCode(theta2=0.16, eps2=1e-6, walk=P.WALK_GROUP, group_size=gs)
+    orc = O.Oracle(theta2=0.16, eps2=1e-6, walk=2, tile_size=gs, num_threads=8)
+    g = tc.pepc_grow_tree(x, y, z, q)
+    go = orc.grow_tree(x, y, z, q)
+    assert np.array_equal(g.key, go["key"])
+    r = tc.pepc_traverse_tree(g.x, g.y, g.z, keys=g.key)
+    ro = orc.traverse_tree(go["x"], go["y"], go["z"], keys=go["key"])
+    for k in ("ex", "ey", "ez", "pot", "work"):
+        assert np.array_equal(r[k], ro[k]), k
+
+
 @pytest.mark.parametrize("walk", [P.WALK_PER_TARGET, P.WALK_PER_TILE])
 def test_walk_morton_keys_bit_exact(gpu, walk):
     x, y, z, q = plummer(8000, 29)
