@@ -552,35 +552,42 @@ __global__ void __launch_bounds__(kMixThreads, 5)
       auto flush_leaves = [&](int n) {
         __syncwarp();
         if (v0) {
-          float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f, bx = 0.f, by = 0.f, bz = 0.f, bp = 0.f;
+          float2 PX = f2(0.f), PY = f2(0.f), PZ = f2(0.f), PP = f2(0.f);
+          const float2 RX = make_float2(rxa, rxb), RY = make_float2(rya, ryb), RZ = make_float2(rza, rzb);
+          const float2 E2 = f2(A.eps2);
+          unsigned nuse = 0;
           auto leaf = [&](const StagedLeaf& r) {
             const float4 c = r.c;
-            float dx = rxa - c.x, dy = rya - c.y, dz = rza - c.z;
-            bool use = true;
-            if (dx == 0.f && dy == 0.f && dz == 0.f) {
+            float2 dx = __fadd2_rn(RX, f2(-c.x)), dy = __fadd2_rn(RY, f2(-c.y)),
+                   dz = __fadd2_rn(RZ, f2(-c.z));
+            const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+            float2 wq = f2(c.w);
+            if (d2.x == 0.f || (v1 && d2.y == 0.f)) {
               // self (dist2 == 0 in FP64) or two points closer than the FP32
               // resolution at the group scale: decide and evaluate in FP64
-              const double ex = (A.tx[ta] - vx) - r.x, ey = (A.ty[ta] - vy) - r.y,
-                           ez = (A.tz[ta] - vz) - r.z;
-              if (ex == 0.0 && ey == 0.0 && ez == 0.0) use = false;
-              dx = (float)ex; dy = (float)ey; dz = (float)ez;
+              if (d2.x == 0.f) {
+                const double ex = (A.tx[ta] - vx) - r.x, ey = (A.ty[ta] - vy) - r.y,
+                             ez = (A.tz[ta] - vz) - r.z;
+                if (ex == 0.0 && ey == 0.0 && ez == 0.0) { wq.x = 0.f; ++nuse; }
+                dx.x = (float)ex; dy.x = (float)ey; dz.x = (float)ez;
+              }
+              if (v1 && d2.y == 0.f) {
+                const double ex = (A.tx[tb] - vx) - r.x, ey = (A.ty[tb] - vy) - r.y,
+                             ez = (A.tz[tb] - vz) - r.z;
+                if (ex == 0.0 && ey == 0.0 && ez == 0.0) { wq.y = 0.f; ++nuse; }
+                dx.y = (float)ex; dy.y = (float)ey; dz.y = (float)ez;
+              }
             }
-            if (use) {
-              leaf32(c.w, dx, dy, dz, A.eps2, ax, ay, az, ap);
-              ++c_leaf;
-            }
-            dx = rxb - c.x; dy = ryb - c.y; dz = rzb - c.z;
-            use = v1;
-            if (v1 && dx == 0.f && dy == 0.f && dz == 0.f) {
-              const double ex = (A.tx[tb] - vx) - r.x, ey = (A.ty[tb] - vy) - r.y,
-                           ez = (A.tz[tb] - vz) - r.z;
-              if (ex == 0.0 && ey == 0.0 && ez == 0.0) use = false;
-              dx = (float)ex; dy = (float)ey; dz = (float)ez;
-            }
-            if (use) {
-              leaf32(c.w, dx, dy, dz, A.eps2, bx, by, bz, bp);
-              ++c_leaf;
-            }
+            // the pair's leaf32 in packed FP32; a self pair enters with charge 0,
+            // and a zero r2 (eps2 = 0) gives no contribution instead of inf
+            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, E2)));
+            const float2 ri = make_float2(r2.x > 0.f ? rsqrtf(r2.x) : 0.f, r2.y > 0.f ? rsqrtf(r2.y) : 0.f);
+            const float2 qr = __fmul2_rn(wq, ri);
+            const float2 qr3 = __fmul2_rn(__fmul2_rn(qr, ri), ri);
+            PP = __fadd2_rn(PP, qr);
+            PX = __ffma2_rn(qr3, dx, PX);
+            PY = __ffma2_rn(qr3, dy, PY);
+            PZ = __ffma2_rn(qr3, dz, PZ);
           };
           const int n1 = min(n, kRing - hL);
           const StagedLeaf* r = stl + hL;
@@ -588,8 +595,9 @@ __global__ void __launch_bounds__(kMixThreads, 5)
           for (int j = 0; j < n1; ++j) leaf(r[j]);
 #pragma unroll 2
           for (int j = 0; j < n - n1; ++j) leaf(stl[j]);
-          Ea0 += (double)ax; Ea1 += (double)ay; Ea2 += (double)az; PHa += (double)ap;
-          Eb0 += (double)bx; Eb1 += (double)by; Eb2 += (double)bz; PHb += (double)bp;
+          Ea0 += (double)PX.x; Ea1 += (double)PY.x; Ea2 += (double)PZ.x; PHa += (double)PP.x;
+          Eb0 += (double)PX.y; Eb1 += (double)PY.y; Eb2 += (double)PZ.y; PHb += (double)PP.y;
+          c_leaf += (unsigned)n * (v1 ? 2u : 1u) - nuse;
         }
         W += (double)n;
         hL = (hL + n) & (kRing - 1);
