@@ -511,7 +511,7 @@ __global__ void __launch_bounds__(kMixThreads, 5)
     float rg = fmaxf(v0 ? sqrtf(rxa * rxa + rya * rya + rza * rza) : 0.f,
                      v1 ? sqrtf(rxb * rxb + ryb * ryb + rzb * rzb) : 0.f);
     for (int o = 16; o > 0; o >>= 1) rg = fmaxf(rg, __shfl_xor_sync(0xffffffffu, rg, o));
-    rg = rg * 1.0001f + 1e-30f;
+    rg = rg * 1.0001f + 1e-30f;  // the sphere must contain every target after rounding
     bool complete = true;
     for (int ib = 0; ib < A.nbox; ++ib) {
       const double vx = s_vb[3 * ib], vy = s_vb[3 * ib + 1], vz = s_vb[3 * ib + 2];
@@ -526,19 +526,24 @@ __global__ void __launch_bounds__(kMixThreads, 5)
         __syncwarp();
         if (v0) {
           float2 PX = f2(0.f), PY = f2(0.f), PZ = f2(0.f), PP = f2(0.f);
-          const float2 RX = make_float2(rxa, rxb), RY = make_float2(rya, ryb), RZ = make_float2(rza, rzb);
+          const float2 RX = make_float2(rxa, rxb), RY = make_float2(rya, ryb),
+                       RZ = make_float2(rza, rzb);
           const float2 E2 = f2(A.eps2);
           const int n1 = min(n, kRing - hT);
           const StagedTwig* r = stw + hT;
 #pragma unroll 8
           for (int j = 0; j < n1; ++j) {
+            // c is the negated offset: one packed add per axis
             const float4 c = r[j].c, m0 = r[j].m0, m1 = r[j].m1, m2 = r[j].m2;
-            twig32x2(m0, m1, m2, __fadd2_rn(RX, f2(c.x)), __fadd2_rn(RY, f2(c.y)), __fadd2_rn(RZ, f2(c.z)), E2, PX, PY, PZ, PP);
+            twig32x2(m0, m1, m2, __fadd2_rn(RX, f2(c.x)), __fadd2_rn(RY, f2(c.y)),
+                     __fadd2_rn(RZ, f2(c.z)), E2, PX, PY, PZ, PP);
           }
 #pragma unroll 4
           for (int j = 0; j < n - n1; ++j) {
+            // c is the negated offset: one packed add per axis
             const float4 c = stw[j].c, m0 = stw[j].m0, m1 = stw[j].m1, m2 = stw[j].m2;
-            twig32x2(m0, m1, m2, __fadd2_rn(RX, f2(c.x)), __fadd2_rn(RY, f2(c.y)), __fadd2_rn(RZ, f2(c.z)), E2, PX, PY, PZ, PP);
+            twig32x2(m0, m1, m2, __fadd2_rn(RX, f2(c.x)), __fadd2_rn(RY, f2(c.y)),
+                     __fadd2_rn(RZ, f2(c.z)), E2, PX, PY, PZ, PP);
           }
           Ea0 += (double)PX.x; Ea1 += (double)PY.x; Ea2 += (double)PZ.x; PHa += (double)PP.x;
           Eb0 += (double)PX.y; Eb1 += (double)PY.y; Eb2 += (double)PZ.y; PHb += (double)PP.y;
@@ -553,7 +558,8 @@ __global__ void __launch_bounds__(kMixThreads, 5)
         __syncwarp();
         if (v0) {
           float2 PX = f2(0.f), PY = f2(0.f), PZ = f2(0.f), PP = f2(0.f);
-          const float2 RX = make_float2(rxa, rxb), RY = make_float2(rya, ryb), RZ = make_float2(rza, rzb);
+          const float2 RX = make_float2(rxa, rxb), RY = make_float2(rya, ryb),
+                       RZ = make_float2(rza, rzb);
           const float2 E2 = f2(A.eps2);
           unsigned nuse = 0;
           auto leaf = [&](const StagedLeaf& r) {
