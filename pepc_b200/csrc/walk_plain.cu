@@ -589,7 +589,7 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
   }
   // per-tile walk: several whole tiles per warp.  Measured at 4M (Plummer,
   // theta 0.4): the packed FP64 walk beats one tile per warp at every tile
-  // size (32: 318 vs 851 ms); in the mixed form the wide group kernel with
+  // size (32: 278 vs 851 ms); in the mixed form the wide group kernel with
   // tiles as buckets wins at 32 targets (127 vs 148 ms) and loses at 24
   // (167 vs 146 ms)
   const bool packed = walk == PEPCG_WALK_PER_TILE &&
