@@ -270,16 +270,37 @@ int pepcg_lattice(void* ctx, int64_t nt, const double* tx, const double* ty, con
                   double* ex, double* ey, double* ez, double* pot);
 
 /*
- * pepcg_sort_keys_noalloc -- sorts n non-negative 64-bit keys (ascending,
+ * pepcg_sort_keys -- replaces the local key sort of domain_decompose
+ * (module_domains.f90:182, slsort_keys -> sl_pepc/mpi_pepckeys.c:151-167 ->
+ * pepckeys_sort_radix, sort_radix.c:122-151) at one rank: sorts n keys
+ * (host arrays) and returns the sorted keys and the 0-based input index of
+ * each sorted key (slsort_keys' indxl, minus one).  Keys are ordered as
+ * unsigned 64-bit values, as the reference's radix sort orders them (PEPC's
+ * keys are non-negative).  Equal keys come out in the order the reference's
+ * in-place MSD radix sort leaves them, which is the order pepcg_grow_tree
+ * gives to particles with equal keys.  Either output may be NULL.
+ */
+int pepcg_sort_keys(void* ctx, int64_t n, const int64_t* keys, int64_t* keys_out,
+                    int64_t* perm_out);
+/* Same with device arrays, on the context's stream. */
+int pepcg_sort_keys_device(void* ctx, int64_t n, const int64_t* d_keys, int64_t* d_keys_out,
+                           int64_t* d_perm_out);
+
+/*
+ * pepcg_sort_keys_noalloc -- sorts n 64-bit keys (ascending as unsigned
+ * 64-bit values, so a negative key sorts after every non-negative one;
  * stable: equal keys keep their input order) and returns the sorted keys and
  * the 0-based input index of each sorted key, all device pointers, enqueued
  * on `stream` (a cudaStream_t of the current device, or NULL).  It allocates
  * nothing: for callers that cannot call cudaMalloc, its scratch is a static
  * device array of the library (about 24.3 MB per device, held until exit),
  * which limits n to 1,048,576; larger n returns PEPCG_ERR_BAD_ARG.  The first
- * call on a device looks up that array's address (make it before any stream
- * capture); calls that overlap on the GPU race on the shared array.  The
- * order equals the key order of pepcg_grow_tree's key_out / perm_out.
+ * call on a device looks up that array's address and keeps it for the life of
+ * the process (make that call before any stream capture; a device reset
+ * between calls is not supported); calls that overlap on the GPU race on the
+ * shared array.  For distinct keys the order equals pepcg_grow_tree's and
+ * pepcg_sort_keys'; equal keys keep their input order here, where those two
+ * give the reference's order.
  * No counterpart in the reference.
  */
 int pepcg_sort_keys_noalloc(int64_t n, const int64_t* d_keys_in, int64_t* d_keys_out,

@@ -119,6 +119,7 @@ EXPORTS = [
     "pepcg_push_particles_device", "pepcg_apply_external_field_device",
     "pepcg_constrain_periodic_device", "pepcg_gather_device",
     "pepcg_traverse_range_device", "pepcg_restore_device",
+    "pepcg_sort_keys", "pepcg_sort_keys_device",
 ]
 
 _LIB = None
@@ -149,6 +150,8 @@ def lib():
     L.pepcg_timber_tree.argtypes = [VP]
     L.pepcg_set_stream.argtypes = [VP, VP]
     L.pepcg_sort_keys_noalloc.argtypes = [C.c_int64, VP, VP, VP, VP]
+    L.pepcg_sort_keys.argtypes = [VP, C.c_int64, I64, I64, I64]
+    L.pepcg_sort_keys_device.argtypes = [VP, C.c_int64, VP, VP, VP]
     L.pepcg_traverse_adjoint.argtypes = [VP, C.c_int64, D, D, D, D, D, D, D, D, D, D, D]
     L.pepcg_traverse_adjoint_device.argtypes = [VP, C.c_int64] + [VP] * 11
     L.pepcg_push_particles_device.argtypes = [VP, C.c_int64, C.c_double] + [VP] * 11
@@ -278,6 +281,21 @@ class TreeCode:
         self._check(lib().pepcg_traverse_tree(self._h, n, _dp(x), _dp(y), _dp(z), kp, _dp(ex),
                                               _dp(ey), _dp(ez), _dp(pt), _dp(wk)))
         return dict(ex=ex, ey=ey, ez=ez, pot=pt, work=wk)
+
+    def sort_keys(self, keys):
+        """The local key sort of domain_decompose (slsort_keys at one rank):
+        sorted keys and the 0-based input index of each, with equal keys in
+        the reference's order."""
+        keys = np.ascontiguousarray(keys, dtype=np.int64)
+        n = len(keys)
+        ko = np.zeros(n, np.int64)
+        po = np.zeros(n, np.int64)
+        self._check(lib().pepcg_sort_keys(self._h, n, _ip(keys), _ip(ko), _ip(po)))
+        return ko, po
+
+    def sort_keys_device(self, keys, keys_out, perm_out):
+        return self._check(lib().pepcg_sort_keys_device(self._h, keys.numel(), _tptr(keys),
+                                                        _tptr(keys_out), _tptr(perm_out)))
 
     def pepc_timber_tree(self):
         self._check(lib().pepcg_timber_tree(self._h))

@@ -81,6 +81,11 @@ int status_to_code(Ctx* c, uint32_t st) {
     c->err = "too many duplicate keys for the duplicate-key fix";
     return PEPCG_ERR_MAXLEVEL;
   }
+  if (st & ST_SORT_REPLAY) {
+    c->err = "internal error: the replay of the reference's key order for equal keys "
+             "found an inconsistent class list";
+    return PEPCG_ERR_CUDA;
+  }
   if (st & ST_TIMEOUT) {
     c->err = "a bounded device wait gave up";
     return PEPCG_ERR_TIMEOUT;
@@ -341,7 +346,7 @@ int pepcg_destroy(void* ctx) {
   release(c->key); release(c->perm);
   release(c->in_x); release(c->in_y); release(c->in_z); release(c->in_q);
   release(c->packed); release(c->skey); release(c->skey_alt); release(c->sval); release(c->sval_alt);
-  release(c->hist); release(c->orig_key); release(c->dup_list);
+  release(c->hist); release(c->orig_key); release(c->dup_list); release(c->tiepre); release(c->sortio);
   release(c->lev); release(c->lcpn);
   release(c->cstart); release(c->cend); release(c->sstart); release(c->send);
   release(c->scan_tmp);
@@ -863,6 +868,38 @@ int pepcg_gather_device(void* ctx, const double* d_in, double* d_out) {
   }
   cudaSetDevice(c->device);
   return gather_device(c, d_in, d_out);
+}
+
+int pepcg_sort_keys_device(void* ctx, int64_t n, const int64_t* d_keys, int64_t* d_keys_out,
+                           int64_t* d_perm_out) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || n < 0 || (n > 0 && !d_keys)) return PEPCG_ERR_BAD_ARG;
+  cudaSetDevice(c->device);
+  return sort_keys_device(c, n, d_keys, d_keys_out, d_perm_out);
+}
+
+int pepcg_sort_keys(void* ctx, int64_t n, const int64_t* keys, int64_t* keys_out,
+                    int64_t* perm_out) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || n < 0 || (n > 0 && !keys)) return PEPCG_ERR_BAD_ARG;
+  if (n == 0) return PEPCG_OK;
+  cudaSetDevice(c->device);
+  if (!ensure(c, c->sortio, 3 * (size_t)n, "sort staging")) return PEPCG_ERR_OOM;
+  cudaStream_t s = c->stream;
+  int64_t* d_in = c->sortio.p;
+  int64_t* d_k = d_in + n;
+  int64_t* d_p = d_k + n;
+  if (!cuda_ok(c, cudaMemcpyAsync(d_in, keys, n * 8, cudaMemcpyHostToDevice, s), "H2D keys"))
+    return PEPCG_ERR_CUDA;
+  int rc = sort_keys_device(c, n, d_in, keys_out ? d_k : nullptr, perm_out ? d_p : nullptr);
+  if (rc) return rc;
+  bool ok = true;
+  if (keys_out)
+    ok = cuda_ok(c, cudaMemcpyAsync(keys_out, d_k, n * 8, cudaMemcpyDeviceToHost, s), "D2H keys");
+  if (perm_out)
+    ok = ok && cuda_ok(c, cudaMemcpyAsync(perm_out, d_p, n * 8, cudaMemcpyDeviceToHost, s), "D2H perm");
+  ok = ok && cuda_ok(c, cudaStreamSynchronize(s), "sort");
+  return ok ? PEPCG_OK : PEPCG_ERR_CUDA;
 }
 
 }  // extern "C"

@@ -1060,6 +1060,50 @@ void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp
   exclusive_scan<int32_t>(in, out, n, tmp, s);
 }
 
+// The LSD radix sort of the n (key, index) pairs in skey / sval: 8 passes of 8
+// bits, ping-ponging through skey_alt / sval_alt, so the result is back in
+// skey / sval.
+static void lsd_sort(Ctx* c, int64_t n, cudaStream_t s) {
+  uint64_t* kin = c->skey.p;
+  uint64_t* kout = c->skey_alt.p;
+  int32_t* vin = c->sval.p;
+  int32_t* vout = c->sval_alt.p;
+  const int nb = (int)((n + kSortChunk - 1) / kSortChunk);
+  for (int pass = 0; pass < 8; ++pass) {
+    const int shift = 8 * pass;
+    COUNT_LAUNCH();
+    k_sort_hist<<<nb, kThreads, 0, s>>>(n, kin, shift, c->hist.p, nb);
+    exclusive_scan<uint32_t>(c->hist.p, c->hist.p, 256 * (int64_t)nb,
+                             reinterpret_cast<uint32_t*>(c->scan_tmp.p), s);
+    sort_scatter(n, kin, vin, kout, vout, shift, c->hist.p, nb, s);
+    std::swap(kin, kout);
+    std::swap(vin, vout);
+  }
+}
+
+// Scratch of the equal-key replay, borrowed from buffers that are idle between
+// the sort and the tree build: the other LSD buffers, the tree-count arrays and
+// the sort histogram.
+static TieArgs tie_args(Ctx* c, int64_t n, const unsigned long long* ndup) {
+  TieArgs a{};
+  a.n = n;
+  a.skey = c->skey.p;
+  a.sval = c->sval.p;
+  a.ndup = ndup;
+  a.kb = c->skey_alt.p;
+  a.A = c->cstart.p;
+  a.B = c->cend.p;
+  a.fp = c->sstart.p;
+  a.src = c->send.p;
+  a.dpre = c->tiepre.p;
+  a.cl = reinterpret_cast<uint16_t*>(c->sval_alt.p);
+  a.fc = a.cl + n;
+  a.seg = reinterpret_cast<int2*>(c->hist.p);
+  a.segcap = tie_segcap(n);
+  a.status = c->d_status;
+  return a;
+}
+
 int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const double* dz,
                 const double* dq) {
   cudaStream_t s = c->stream;
@@ -1074,7 +1118,8 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
   }
   const int64_t nblk_sort = (n + kSortChunk - 1) / kSortChunk;
   const int dupcap = 1 << 20;
-  if (!ensure(c, c->x, n, "x") || !ensure(c, c->y, n, "y") || !ensure(c, c->z, n, "z") ||
+  if (!ensure(c, c->tiepre, n + 1, "tiepre") ||
+      !ensure(c, c->x, n, "x") || !ensure(c, c->y, n, "y") || !ensure(c, c->z, n, "z") ||
       !ensure(c, c->q, n, "q") || !ensure(c, c->key, n, "key") || !ensure(c, c->perm, n, "perm") ||
       !ensure(c, c->skey, n, "skey") || !ensure(c, c->skey_alt, n, "skey_alt") ||
       !ensure(c, c->sval, n, "sval") || !ensure(c, c->sval_alt, n, "sval_alt") ||
@@ -1107,27 +1152,26 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
   k_keys<<<std::min(grid_for(n), 148u * 8u), kThreads, 0, s>>>(n, dx, dy, dz, dq, c->d_box, c->prm.curve, htab,
                                           c->skey.p, c->sval.p, c->packed.p);
   cudaEventRecord(c->ev[1], s);
-  // sort: 8 LSD passes of 8 bits
+  // sort: 8 LSD passes of 8 bits; the result is back in skey / sval
+  lsd_sort(c, n, s);
   uint64_t* kin = c->skey.p;
-  uint64_t* kout = c->skey_alt.p;
   int32_t* vin = c->sval.p;
-  int32_t* vout = c->sval_alt.p;
-  const int nb = (int)nblk_sort;
-  for (int pass = 0; pass < 8; ++pass) {
-    const int shift = 8 * pass;
-    COUNT_LAUNCH();
-    k_sort_hist<<<nb, kThreads, 0, s>>>(n, kin, shift, c->hist.p, nb);
-    exclusive_scan<uint32_t>(c->hist.p, c->hist.p, 256 * (int64_t)nb,
-                             reinterpret_cast<uint32_t*>(c->scan_tmp.p), s);
-    sort_scatter(n, kin, vin, kout, vout, shift, c->hist.p, nb, s);
-    std::swap(kin, kout);
-    std::swap(vin, vout);
-  }
-  // after an even number of passes the result is back in skey / sval
   COUNT_LAUNCH();
   k_permute<<<grid_for(n), kThreads, 0, s>>>(n, kin, vin, c->packed.p, c->x.p, c->y.p, c->z.p,
                                              c->q.p, c->key.p, c->orig_key.p, c->perm.p,
                                              c->d_small, c->dup_list.p, dupcap);
+  // equal keys in the reference's order (an empty launch when there are none),
+  // before the duplicate fix shifts them
+  {
+    TieArgs ta = tie_args(c, n, c->d_small);
+    ta.packed = c->packed.p;
+    ta.x = c->x.p;
+    ta.y = c->y.p;
+    ta.z = c->z.p;
+    ta.q = c->q.p;
+    ta.perm = c->perm.p;
+    if (!tie_order_launch(c, ta, s)) return PEPCG_ERR_CUDA;
+  }
   COUNT_LAUNCH();
   k_dupfix<<<1, 32, 0, s>>>(n, c->key.p, c->orig_key.p, c->x.p, c->y.p, c->z.p, c->d_small,
                             c->dup_list.p, dupcap, c->d_box, c->prm.curve, c->d_status);
@@ -1230,6 +1274,65 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
 
   c->has_tree = true;
   return PEPCG_OK;
+}
+
+// The local key sort alone (slsort_keys at one rank, sl_pepc/mpi_pepckeys.c:
+// 151-167 -> pepckeys_sort_radix, sort_radix.c:122-151): the LSD passes of the
+// grow, then the replay of the reference's order on runs of equal keys.
+namespace {
+__global__ void k_sortkeys_load(int64_t n, const int64_t* __restrict__ in,
+                                uint64_t* __restrict__ k, int32_t* __restrict__ v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    k[i] = (uint64_t)in[i];
+    v[i] = (int32_t)i;
+  }
+}
+
+__global__ void k_sortkeys_store(int64_t n, const uint64_t* __restrict__ k,
+                                 const int32_t* __restrict__ v, int64_t* __restrict__ kout,
+                                 int64_t* __restrict__ pout) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (kout) kout[i] = (int64_t)k[i];
+    if (pout) pout[i] = (int64_t)v[i];
+  }
+}
+}  // namespace
+
+int sort_keys_device(Ctx* c, int64_t n, const int64_t* d_in, int64_t* d_kout, int64_t* d_pout) {
+  cudaStream_t s = c->stream;
+  if (n < 0 || n > (int64_t)INT32_MAX / 4) {
+    c->err = "pepcg_sort_keys: n out of range";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  if (n == 0) return PEPCG_OK;
+  const int64_t nblk_sort = (n + kSortChunk - 1) / kSortChunk;
+  if (!ensure(c, c->skey, n, "skey") || !ensure(c, c->skey_alt, n, "skey_alt") ||
+      !ensure(c, c->sval, n, "sval") || !ensure(c, c->sval_alt, n, "sval_alt") ||
+      !ensure(c, c->hist, 256 * nblk_sort + 1, "hist") ||
+      !ensure(c, c->scan_tmp, 2 * ((256 * nblk_sort + n) / 2048 + 64), "scan_tmp") ||
+      !ensure(c, c->cstart, n, "cstart") || !ensure(c, c->cend, n, "cend") ||
+      !ensure(c, c->sstart, n, "sstart") || !ensure(c, c->send, n, "send") ||
+      !ensure(c, c->tiepre, n + 1, "tiepre"))
+    return PEPCG_ERR_OOM;
+  unsigned long long* npair = c->d_small + 11;
+  if (!cuda_ok(c, cudaMemsetAsync(c->d_status, 0, sizeof(uint32_t), s), "memset status") ||
+      !cuda_ok(c, cudaMemsetAsync(npair, 0, sizeof(unsigned long long), s), "memset"))
+    return PEPCG_ERR_CUDA;
+  COUNT_LAUNCH();
+  k_sortkeys_load<<<grid_for(n), kThreads, 0, s>>>(n, d_in, c->skey.p, c->sval.p);
+  lsd_sort(c, n, s);
+  count_pairs_launch(n, c->skey.p, npair, s);
+  if (!tie_order_launch(c, tie_args(c, n, npair), s)) return PEPCG_ERR_CUDA;
+  COUNT_LAUNCH();
+  k_sortkeys_store<<<grid_for(n), kThreads, 0, s>>>(n, c->skey.p, c->sval.p, d_kout, d_pout);
+  uint32_t st = 0;
+  if (!cuda_ok(c, cudaGetLastError(), "sort kernels") ||
+      !cuda_ok(c, cudaMemcpyAsync(&st, c->d_status, 4, cudaMemcpyDeviceToHost, s), "status") ||
+      !cuda_ok(c, cudaStreamSynchronize(s), "sort"))
+    return PEPCG_ERR_CUDA;
+  return st ? status_to_code(c, st) : PEPCG_OK;
 }
 
 // Tree export in the reference's insertion (forward preorder) order.
@@ -1344,7 +1447,12 @@ int export_tree(Ctx* c, int64_t* key, int32_t* level, int64_t* leaves, int64_t* 
 //    threads, or a call issued before the previous one finished) race on it;
 //  * the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (host code only holds a host-side stand-in for the
-//    symbol); make that first call before any stream capture on the device.
+//    symbol) and keeps it for the life of the process; make that first call
+//    before any stream capture on the device.  A device reset between calls
+//    would leave the kept address stale, so it is not supported;
+//  * keys are ordered as unsigned 64-bit values and equal keys keep their
+//    input order (the LSD passes are stable); pepcg_grow_tree additionally
+//    puts equal keys in the reference's order (tieorder.cu).
 // ---------------------------------------------------------------------------
 namespace pepcg {
 namespace {
@@ -1438,7 +1546,6 @@ extern "C" int pepcg_sort_keys_noalloc(int64_t n, const int64_t* d_keys_in, int6
     const int shift = 8 * pass;
     COUNT_LAUNCH();
     k_sort_hist<<<nb, kThreads, 0, s>>>(n, kin, shift, hist, nb);
-    g_launches.fetch_add(3, std::memory_order_relaxed);
     exclusive_scan<uint32_t>(hist, hist, 256 * (int64_t)nb, tmp, s);
     sort_scatter(n, kin, vin, kout, vout, shift, hist, nb, s);
     std::swap(kin, kout);

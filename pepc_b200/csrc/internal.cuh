@@ -47,6 +47,7 @@ enum : uint32_t {
   ST_NONFINITE = 1u << 3,
   ST_DUP_OVERFLOW = 1u << 4,
   ST_NOT_NEUTRAL = 1u << 5,
+  ST_SORT_REPLAY = 1u << 6,  // the replay of the reference's sort lost its way (internal)
 };
 
 template <class T>
@@ -98,6 +99,8 @@ struct Ctx {
   DBuf<uint32_t> hist;
   DBuf<int64_t> orig_key;               // sorted keys before the duplicate fix
   DBuf<int32_t> dup_list;
+  DBuf<int32_t> tiepre;                 // equal-key pairs before each sorted position (tieorder.cu)
+  DBuf<int64_t> sortio;                 // host-array staging of pepcg_sort_keys
   DBuf<int8_t> lev, lcpn;
   DBuf<int32_t> cstart, cend, sstart, send;
   DBuf<int32_t> scan_tmp;
@@ -212,10 +215,42 @@ int status_to_code(Ctx* c, uint32_t st);
 // ---- grow.cu ----
 int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const double* dz,
                 const double* dq);
+// the local key sort in the reference's order (keys as unsigned 64-bit values)
+int sort_keys_device(Ctx* c, int64_t n, const int64_t* d_in, int64_t* d_kout, int64_t* d_pout);
 int export_tree(Ctx* c, int64_t* key, int32_t* level, int64_t* leaves, int64_t* desc,
                 int64_t* parent, int64_t* first_child, int64_t* next_sibling, double* mom15);
 // device scan helper (exclusive, int32), returns the total through *total (device)
 void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp,
+                        cudaStream_t s);
+
+// ---- tieorder.cu ----
+// The replay of the reference's sort on runs of equal keys (k_tie_order).
+// Device arrays; scratch of n elements each unless stated.
+struct TieArgs {
+  int64_t n;
+  const uint64_t* skey;            // keys sorted by the LSD sort
+  int32_t* sval;                   // input index of each sorted key; rewritten on equal runs
+  const unsigned long long* ndup;  // equal neighbours in skey; 0 -> nothing to do
+  uint64_t* kb;                    // scratch: keys by input index
+  int32_t* A;                      // scratch: the arrangement being replayed
+  int32_t* B;                      // scratch
+  int32_t* fp;                     // scratch: foreign slot positions
+  int32_t* src;                    // scratch: the slot each foreign slot receives from
+  int32_t* dpre;                   // scratch, n + 1: equal pairs before each position
+  uint16_t* cl;                    // scratch: class per position
+  uint16_t* fc;                    // scratch: class per foreign slot
+  int2* seg;                       // scratch: 2 * segcap ranges
+  int64_t segcap;                  // tie_segcap(n)
+  uint32_t* status;
+  // when packed is set, the particles of the equal runs are gathered again
+  const double4* packed;
+  double *x, *y, *z, *q;
+  int32_t* perm;
+};
+int64_t tie_segcap(int64_t n);
+bool tie_order_launch(Ctx* c, const TieArgs& a, cudaStream_t s);
+// adds the number of i with skey[i] == skey[i + 1] to *npair
+void count_pairs_launch(int64_t n, const uint64_t* skey, unsigned long long* npair,
                         cudaStream_t s);
 
 // ---- walk_plain.cu / walk_mixed.cu ----

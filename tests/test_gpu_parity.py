@@ -120,9 +120,8 @@ def test_grow_duplicate_positions(gpu):
     assert np.array_equal(g.key, go["key"])
     assert len(np.unique(g.key)) == len(g.key)
     assert np.array_equal(g.x, go["x"]) and np.array_equal(g.y, go["y"]) and np.array_equal(g.z, go["z"])
-    # the order of tied particles may differ (stable sort vs the reference's
-    # in-place MSD sort): compare the particle multiset per tie group
-    assert np.array_equal(np.sort(g.perm), np.arange(4000))
+    # tied particles in the order of the reference's in-place MSD sort
+    assert np.array_equal(g.perm, go["perm"])
 
 
 @pytest.mark.parametrize("theta2", [0.0, 0.09, 0.36])
