@@ -1,10 +1,13 @@
 """GPU at the benchmark's full size and beyond, through properties that do
 not need a full-size oracle run:
-  * 4,194,304-particle Plummer sphere: keys, order and tree counts identical
-    to the oracle's grow, and the plain per-target walk bit-identical to the
-    oracle's on 2,048 sampled targets;
-  * the mixed group walk at that size meets the headline accuracy bar
-    (median relative force error <= 1e-4 against the FP64 direct sum);
+  * 4,194,304-particle Plummer sphere (scale radius 1, truncated at 20, q =
+    1/N, eps 1e-3), at every theta of the benchmark's sweep {0.2, 0.4, 0.6}:
+    keys, order and tree counts identical to the oracle's grow, and the plain
+    per-target walk bit-identical to the oracle's on 2,048 sampled targets;
+  * the mixed group walk at that size, on 8,192 sampled targets (seed 33)
+    against the FP64 direct sum: median relative force error <= 1e-4 at
+    theta 0.2 and 0.4 (the headline bar), and at every theta no larger than
+    the plain drop-in walk's;
   * 33,554,432 particles (8x the benchmark): the walk completes (every
     target's interactions cover all particles) and keeps its accuracy."""
 import numpy as np
@@ -24,9 +27,10 @@ def plummer4m():
     return plummer(N4M)
 
 
-def test_plain_4m_matches_oracle_on_sampled_targets(gpu, plummer4m):
+@pytest.mark.parametrize("theta", [0.2, 0.4, 0.6])
+def test_plain_4m_matches_oracle_on_sampled_targets(gpu, plummer4m, theta):
     x, y, z, q = plummer4m
-    kw = dict(theta2=0.16, eps2=1e-6)
+    kw = dict(theta2=theta * theta, eps2=1e-6)
     tc = P.TreeCode(walk=P.WALK_PER_TARGET, **kw)
     g = tc.pepc_grow_tree(x, y, z, q)
     orc = O.Oracle(walk=0, num_threads=16, **kw)
@@ -43,23 +47,32 @@ def test_plain_4m_matches_oracle_on_sampled_targets(gpu, plummer4m):
     orc.close()
 
 
-def test_mixed_4m_meets_the_accuracy_bar(gpu, plummer4m):
+@pytest.mark.parametrize("theta", [0.2, 0.4, 0.6])
+def test_mixed_4m_meets_the_accuracy_bar(gpu, plummer4m, theta):
     x, y, z, q = plummer4m
     dev = torch.device("cuda", 0)
-    tc = P.TreeCode(theta2=0.16, eps2=1e-6, precision=P.PRECISION_MIXED, walk=P.WALK_GROUP)
-    tc.grow_tree_device(*(torch.from_numpy(a).to(dev) for a in (x, y, z, q)))
-    out = [torch.zeros(N4M, dtype=torch.float64, device=dev) for _ in range(5)]
-    tc.traverse_self_device(*out)
-    idx = np.sort(np.random.default_rng(92).choice(N4M, 4096, replace=False))
-    d = tc.direct(idx)
-    E = torch.stack(out[:3]).cpu().numpy()[:, idx]
-    Ed = np.stack([d["ex"], d["ey"], d["ez"]])
-    rel = np.linalg.norm(E - Ed, axis=0) / np.linalg.norm(Ed, axis=0)
-    assert np.median(rel) <= 1e-4, np.median(rel)
-    assert np.percentile(rel, 99) <= 1e-3
-    st = tc.stats()
-    assert int(out[4].sum().item()) == st["leaf_interactions"] + st["twig_interactions"] + N4M
-    tc.close()
+    idx = np.sort(np.random.default_rng(33).choice(N4M, 8192, replace=False))
+    med = {}
+    for prec, walk in ((P.PRECISION_MIXED, P.WALK_GROUP), (P.PRECISION_PLAIN, P.WALK_PER_TARGET)):
+        tc = P.TreeCode(theta2=theta * theta, eps2=1e-6, precision=prec, walk=walk)
+        tc.grow_tree_device(*(torch.from_numpy(a).to(dev) for a in (x, y, z, q)))
+        out = [torch.zeros(N4M, dtype=torch.float64, device=dev) for _ in range(5)]
+        tc.traverse_self_device(*out)
+        d = tc.direct(idx)
+        E = torch.stack(out[:3]).cpu().numpy()[:, idx]
+        Ed = np.stack([d["ex"], d["ey"], d["ez"]])
+        rel = np.linalg.norm(E - Ed, axis=0) / np.linalg.norm(Ed, axis=0)
+        med[prec] = np.median(rel)
+        if prec == P.PRECISION_MIXED:
+            st = tc.stats()
+            assert int(out[4].sum().item()) == st["leaf_interactions"] + st["twig_interactions"] + N4M
+            assert np.percentile(rel, 99) <= 10 * max(med[prec], 1e-4)
+        tc.close()
+    print(f"theta {theta}: median relative force error mixed {med[P.PRECISION_MIXED]:.3e}, "
+          f"plain {med[P.PRECISION_PLAIN]:.3e}")
+    if theta <= 0.4:
+        assert med[P.PRECISION_MIXED] <= 1e-4, med
+    assert med[P.PRECISION_MIXED] <= med[P.PRECISION_PLAIN], med
 
 
 def test_32m_particles_complete_and_accurate(gpu):
