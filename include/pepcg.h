@@ -95,7 +95,13 @@ typedef struct pepcg_params {
   int32_t group_size;            /* GROUP walk: targets per bucket, 32 or 64; 0 = 64 for the
                                     mixed walk and 32 for the plain walk [0].  The adjoint
                                     supports 32. */
-  int32_t reserved[3];
+  int32_t reserved0;             /* zero */
+  double spatial_interaction_cutoff[3]; /* module_mirror_boxes.f90:52: a node whose offset
+                                    from the target has any |component| >= the cutoff is
+                                    skipped (module_tree_walk_pthreads.f90:622,639;
+                                    module_tree_walk_simple.f90:330,377); plain walks only,
+                                    >= 0 [DBL_MAX each: no cutoff] */
+  int32_t reserved[4];           /* zero */
 } pepcg_params;
 
 /* Statistics of the last grow/traverse (module_tree.f90:622-699,
@@ -268,6 +274,11 @@ int pepcg_direct(void* ctx, int64_t ntest, const int64_t* tidx, double* ex, doub
  * module_fmm_framework.f90:766-826) at nt positions; overwrites. */
 int pepcg_lattice(void* ctx, int64_t nt, const double* tx, const double* ty, const double* tz,
                   double* ex, double* ey, double* ez, double* pot);
+/* The same at one position, in the shape of fmm_sum_lattice_force(pos, e_lattice,
+ * phi_lattice) (module_fmm_framework.f90:766-826), for shims that call it per
+ * particle as calc_force_per_particle does (coulomb/module_interaction_specific.
+ * f90:393-427).  Overwrites e[3] and *phi. */
+int pepcg_lattice_force(void* ctx, const double pos[3], double e[3], double* phi);
 
 /*
  * pepcg_sort_keys -- replaces the local key sort of domain_decompose

@@ -37,6 +37,7 @@ class OrcParams(C.Structure):
         ("mac_select", C.c_int32),
         ("force_law", C.c_int32),
         ("kelbg_invsqrttemp", C.c_double),
+        ("spatial_interaction_cutoff", C.c_double * 3),
     ]
 
 
@@ -121,7 +122,8 @@ def params(**kw):
     p = OrcParams()
     lib().orc_params_default(C.byref(p))
     for k, v in kw.items():
-        if k in ("periodicity", "t_lattice_1", "t_lattice_2", "t_lattice_3", "lattice_origin"):
+        if k in ("periodicity", "t_lattice_1", "t_lattice_2", "t_lattice_3", "lattice_origin",
+                 "spatial_interaction_cutoff"):
             arr = getattr(p, k)
             for i in range(3):
                 arr[i] = v[i]

@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <thread>
 #include <vector>
 
@@ -598,6 +599,13 @@ struct Counters {
   int64_t inter = 0, mac = 0;
 };
 
+// any(abs(delta) >= spatial_interaction_cutoff): the node is skipped
+// (module_tree_walk_pthreads.f90:622,639, module_tree_walk_simple.f90:330,377)
+inline bool cut_off(const orc_ctx* c, const double d[3]) {
+  const double* sc = c->p.spatial_interaction_cutoff;
+  return std::fabs(d[0]) >= sc[0] || std::fabs(d[1]) >= sc[1] || std::fabs(d[2]) >= sc[2];
+}
+
 // walk_single_particle, treecode/lpepcsrc/module_tree_walk_pthreads.f90:558-765.
 // At one rank every child is local, so the defer list only ever holds the
 // root (:601 parses it once and pushes the root's children); the todo list is
@@ -622,6 +630,7 @@ int64_t walk_pthreads(const orc_ctx* c, const double xt[3], const double vbox[3]
     if (nd.descendants == 0) {  // leaf, :617-631
       partner += 1;
       work += 1.0;
+      if (cut_off(c, d)) continue;  // :622, after the work count
       if (dist2 > 0.0) {
         double ee[3], ph;
         law_leaf(c->p.force_law, nd.m, d, dist2, eps2, ee, ph, tq, c->p.kelbg_invsqrttemp);  // specific.f90:327-343
@@ -633,6 +642,7 @@ int64_t walk_pthreads(const orc_ctx* c, const double xt[3], const double vbox[3]
       cnt.mac += 1;
       if (mac_pass(c, nd, dist2)) {  // mac, :635 / specific.f90:256-275
         partner += nd.leaves;
+        if (cut_off(c, d)) continue;  // :639, before the work count
         double ee[3], ph;
         law_twig(c->p.force_law, nd.m, d, dist2, eps2, ee, ph);  // specific.f90:368-380
         e[0] += ee[0]; e[1] += ee[1]; e[2] += ee[2];
@@ -659,6 +669,7 @@ void walk_simple_aux(const orc_ctx* c, int64_t ni, int np, const double (*xs)[3]
     partner += 1;
     for (int ip = 0; ip < np; ++ip) {
       for (int k = 0; k < 3; ++k) d[ip][k] = (xs[ip][k] - vbox[k]) - nd.m[M_COCX + k];
+      if (cut_off(c, d[ip])) continue;  // :330, before the work count
       d2[ip] = (d[ip][0] * d[ip][0] + d[ip][1] * d[ip][1]) + d[ip][2] * d[ip][2];
       cnt.inter += 1;
       work[ip] += 1.0;
@@ -683,6 +694,7 @@ void walk_simple_aux(const orc_ctx* c, int64_t ni, int np, const double (*xs)[3]
   }
   partner += nd.leaves;  // MAC OK for the whole tile: interact
   for (int ip = 0; ip < np; ++ip) {
+    if (cut_off(c, d[ip])) continue;  // :377
     cnt.inter += 1;
     work[ip] += 1.0;
     double ee[3], ph;
@@ -906,6 +918,8 @@ void orc_params_default(orc_params* p) {
   p->t_lattice_3[2] = 1.0;
   p->num_threads = 1;
   p->force_law = 3;   // coulomb/module_interaction_specific.f90:35
+  for (int k = 0; k < 3; ++k)  // huge(0._kind_physics), module_mirror_boxes.f90:52
+    p->spatial_interaction_cutoff[k] = std::numeric_limits<double>::max();
 }
 
 void orc_box_create(int64_t n, const double* x, const double* y, const double* z,

@@ -40,6 +40,7 @@ typedef struct orc_params {
   int32_t mac_select;       /* 0 Barnes-Hut, 1 Bmax, other: no acceptance (N^2) */
   int32_t force_law;        /* 3 3D Coulomb, 2 2D Coulomb, 4 Lennard-Jones, 5 Kelbg */
   double kelbg_invsqrttemp; /* Kelbg: 1/sqrt(temperature) [0] */
+  double spatial_interaction_cutoff[3]; /* module_mirror_boxes.f90:52 [huge] */
 } orc_params;
 
 void orc_params_default(orc_params* p);

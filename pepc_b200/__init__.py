@@ -74,7 +74,9 @@ class Params(C.Structure):
         ("overwrite_results", C.c_int32),
         ("kelbg_invsqrttemp", C.c_double),
         ("group_size", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("reserved0", C.c_int32),
+        ("spatial_interaction_cutoff", C.c_double * 3),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -119,7 +121,7 @@ EXPORTS = [
     "pepcg_push_particles_device", "pepcg_apply_external_field_device",
     "pepcg_constrain_periodic_device", "pepcg_gather_device",
     "pepcg_traverse_range_device", "pepcg_restore_device",
-    "pepcg_sort_keys", "pepcg_sort_keys_device",
+    "pepcg_sort_keys", "pepcg_sort_keys_device", "pepcg_lattice_force",
 ]
 
 _LIB = None
@@ -168,6 +170,7 @@ def lib():
     L.pepcg_tree_export.argtypes = [VP, I64, I32, I64, I64, I64, I64, I64, D]
     L.pepcg_direct.argtypes = [VP, C.c_int64, I64, D, D, D, D]
     L.pepcg_lattice.argtypes = [VP, C.c_int64, D, D, D, D, D, D, D]
+    L.pepcg_lattice_force.argtypes = [VP, D, D, D]
     L.pepcg_multipole_from_particle.argtypes = [D, C.c_double, D]
     L.pepcg_shift_multipoles_up.argtypes = [D, D, C.c_int32]
     L.pepcg_force_with_leaf.argtypes = [D, D, C.c_double, C.c_double, D, D]
@@ -200,7 +203,8 @@ def make_params(**kw):
     p = Params()
     lib().pepcg_params_default(C.byref(p))
     for k, v in kw.items():
-        if k in ("periodicity", "t_lattice_1", "t_lattice_2", "t_lattice_3", "lattice_origin"):
+        if k in ("periodicity", "t_lattice_1", "t_lattice_2", "t_lattice_3", "lattice_origin",
+                 "spatial_interaction_cutoff"):
             arr = getattr(p, k)
             for i in range(3):
                 arr[i] = v[i]
@@ -251,7 +255,12 @@ class TreeCode:
 
     def set_params(self, **kw):
         for k, v in kw.items():
-            setattr(self.params, k, v)
+            if k in ("spatial_interaction_cutoff",):
+                arr = getattr(self.params, k)
+                for i in range(3):
+                    arr[i] = v[i]
+            else:
+                setattr(self.params, k, v)
         self._check(lib().pepcg_set_params(self._h, C.byref(self.params)))
 
     # -- the reference's entry points (module_pepc.f90)
@@ -399,6 +408,13 @@ class TreeCode:
         """traverse_adjoint on torch CUDA float64 tensors; dq..dz are overwritten."""
         ptrs = [_tptr(t) for t in (x, y, z, dLdE[0], dLdE[1], dLdE[2], dLdphi, dq, dx, dy, dz)]
         return self._check(lib().pepcg_traverse_adjoint_device(self._h, x.numel(), *ptrs))
+
+    def lattice_force(self, pos):
+        """fmm_sum_lattice_force at one position: (e[3], phi)."""
+        e = np.zeros(3)
+        phi = np.zeros(1)
+        self._check(lib().pepcg_lattice_force(self._h, _dp(_f64(pos)), _dp(e), _dp(phi)))
+        return e, phi[0]
 
     def lattice(self, x, y, z):
         n = len(x)

@@ -494,6 +494,10 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
     c->err = "the adjoint walk differentiates the 3D Coulomb law only (force_law = 3)";
     return PEPCG_ERR_UNSUPPORTED;
   }
+  if (has_spatial_cutoff(c->prm)) {
+    c->err = "the adjoint walk does not apply spatial_interaction_cutoff";
+    return PEPCG_ERR_UNSUPPORTED;
+  }
   if (c->prm.walk == PEPCG_WALK_GROUP && c->group_size() != 32) {
     c->err = "the adjoint of the group walk is built for buckets of 32 targets (group_size 32)";
     return PEPCG_ERR_UNSUPPORTED;

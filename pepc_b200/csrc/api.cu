@@ -6,6 +6,7 @@
 // fallback: without a usable CUDA device every entry point fails with
 // PEPCG_ERR_CUDA.
 
+#include <cfloat>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -179,6 +180,15 @@ static int check_params(Ctx* c, const pepcg_params* p) {
     c->err = "mirror_box_layers must be in 0..2";
     return PEPCG_ERR_BAD_ARG;
   }
+  for (int k = 0; k < 3; ++k)
+    if (!(p->spatial_interaction_cutoff[k] >= 0.0)) {
+      c->err = "spatial_interaction_cutoff must be >= 0 (DBL_MAX: no cutoff)";
+      return PEPCG_ERR_BAD_ARG;
+    }
+  if (has_spatial_cutoff(*p) && p->precision != PEPCG_PRECISION_PLAIN) {
+    c->err = "spatial_interaction_cutoff is applied by the plain (FP64) walks only";
+    return PEPCG_ERR_UNSUPPORTED;
+  }
   return PEPCG_OK;
 }
 
@@ -272,6 +282,8 @@ void pepcg_params_default(pepcg_params* p) {
   p->t_lattice_2[1] = 1.0;
   p->t_lattice_3[2] = 1.0;
   p->device = 0;
+  for (int k = 0; k < 3; ++k)  // huge(0._kind_physics), module_mirror_boxes.f90:52
+    p->spatial_interaction_cutoff[k] = DBL_MAX;
 }
 
 const char* pepcg_last_error(const void* ctx) {
@@ -825,6 +837,13 @@ int pepcg_lattice(void* ctx, int64_t nt, const double* tx, const double* ty, con
   return ok ? PEPCG_OK : PEPCG_ERR_CUDA;
 }
 
+int pepcg_lattice_force(void* ctx, const double pos[3], double e[3], double* phi) {
+  if (!pos || !e || !phi) {
+    if (ctx) as_ctx(ctx)->err = "pepcg_lattice_force: null argument";
+    return PEPCG_ERR_BAD_ARG;
+  }
+  return pepcg_lattice(ctx, 1, pos, pos + 1, pos + 2, e, e + 1, e + 2, phi);
+}
 
 int pepcg_push_particles_device(void* ctx, int64_t n, double dt, const double* d_q,
                                 const double* d_m, const double* d_ex, const double* d_ey,

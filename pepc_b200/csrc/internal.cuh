@@ -204,6 +204,13 @@ __device__ __forceinline__ bool pack_lane(const int32_t* __restrict__ pstart,
   return (starts & 1u) && lane < cnt && cnt <= 32;
 }
 
+// a finite spatial_interaction_cutoff in any direction (the default, huge,
+// cuts nothing)
+inline bool has_spatial_cutoff(const pepcg_params& p) {
+  return p.spatial_interaction_cutoff[0] < 1.0e308 || p.spatial_interaction_cutoff[1] < 1.0e308 ||
+         p.spatial_interaction_cutoff[2] < 1.0e308;
+}
+
 // ---- helpers implemented in api.cu ----
 bool cuda_ok(Ctx* c, cudaError_t e, const char* what);
 // error text for entry points without a context (pepcg_last_error(NULL))

@@ -59,7 +59,16 @@ struct WalkArgs {
   const int32_t* tflag;  // per target: length of the tile starting there, else 0
   const int32_t* pstart;  // packed per-tile walk: first target of each pack, then nt
   const int32_t* npacks;  // the number of packs (device)
+  // spatial_interaction_cutoff (module_mirror_boxes.f90:52), when finite
+  int has_cut;
+  double cut[3];
 };
+
+// any(abs(delta) >= spatial_interaction_cutoff) (module_tree_walk_pthreads.f90:
+// 622,639; module_tree_walk_simple.f90:330,377): the node is skipped
+__device__ __forceinline__ bool cut_off(const WalkArgs& A, double dx, double dy, double dz) {
+  return A.has_cut && (fabs(dx) >= A.cut[0] || fabs(dy) >= A.cut[1] || fabs(dz) >= A.cut[2]);
+}
 
 __device__ __forceinline__ void warp_add_counters(unsigned long long* ctr, unsigned long long a,
                                                   unsigned long long b, unsigned long long c) {
@@ -116,26 +125,30 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_target64(WalkArgs A) {
         const double dist2 = (dx * dx + dy * dy) + dz * dz;
         if (mu.y & kLeafFlag) {
           partner += 1;
-          w += 1.0;
-          ++c_leaf;
-          if (dist2 > 0.0) {
-            double fx, fy, fz, fp;
-            law_leaf64<kLaw>(a.w, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp, kel);
-            e0 += fx; e1 += fy; e2 += fz; ph += fp;
+          w += 1.0;  // counted before the cutoff test (:620-622)
+          if (!cut_off(A, dx, dy, dz)) {
+            ++c_leaf;
+            if (dist2 > 0.0) {
+              double fx, fy, fz, fp;
+              law_leaf64<kLaw>(a.w, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp, kel);
+              e0 += fx; e1 += fy; e2 += fz; ph += fp;
+            }
           }
           next = u + 1;
         } else {
           ++c_mac;
           if (A.theta2 * dist2 > (A.macb ? A.macb[u] : s_bl2[mu.y & 0xff])) {
             partner += A.nleaves[u];
-            double m[9];
+            if (!cut_off(A, dx, dy, dz)) {
+              double m[9];
 #pragma unroll
-            for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
-            double fx, fy, fz, fp;
-            law_twig64<kLaw>(a.w, m, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp);
-            e0 += fx; e1 += fy; e2 += fz; ph += fp;
-            ++c_twig;
-            w += 1.0;
+              for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
+              double fx, fy, fz, fp;
+              law_twig64<kLaw>(a.w, m, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp);
+              e0 += fx; e1 += fy; e2 += fz; ph += fp;
+              ++c_twig;
+              w += 1.0;
+            }
             next = (unsigned)mu.x;
           } else {
             next = u + 1;
@@ -217,7 +230,7 @@ __global__ void __launch_bounds__(kWalkThreads, kTPL == 1 ? 6 : 4) k_walk_tile64
           partner += 1;
 #pragma unroll
           for (int s = 0; s < kTPL; ++s)
-            if (valid[s]) {
+            if (valid[s] && !cut_off(A, dx[s], dy[s], dz[s])) {
               w[s] += 1.0;
               ++c_leaf;
               if (dist2[s] > 0.0) {
@@ -250,7 +263,7 @@ __global__ void __launch_bounds__(kWalkThreads, kTPL == 1 ? 6 : 4) k_walk_tile64
             for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
 #pragma unroll
             for (int s = 0; s < kTPL; ++s)
-              if (valid[s]) {
+              if (valid[s] && !cut_off(A, dx[s], dy[s], dz[s])) {
                 double fx, fy, fz, fp;
                 law_twig64<kLaw>(a.w, m, dx[s], dy[s], dz[s], dist2[s], A.eps2, fx, fy, fz, fp);
                 e0[s] += fx; e1[s] += fy; e2[s] += fz; ph[s] += fp;
@@ -344,12 +357,14 @@ __global__ void __launch_bounds__(kWalkThreads, 6) k_walk_tilepack64(WalkArgs A)
           const double dist2 = (dx * dx + dy * dy) + dz * dz;
           if (mu.y & kLeafFlag) {
             partner += 1;
-            w += 1.0;
-            ++c_leaf;
-            if (dist2 > 0.0) {
-              double fx, fy, fz, fp;
-              law_leaf64<kLaw>(a.w, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp, kel);
-              e0 += fx; e1 += fy; e2 += fz; ph += fp;
+            if (!cut_off(A, dx, dy, dz)) {  // before the work count (:330)
+              w += 1.0;
+              ++c_leaf;
+              if (dist2 > 0.0) {
+                double fx, fy, fz, fp;
+                law_leaf64<kLaw>(a.w, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp, kel);
+                e0 += fx; e1 += fy; e2 += fz; ph += fp;
+              }
             }
             u = (unsigned)fw.y;
             uf = (unsigned)ff.y;
@@ -361,14 +376,16 @@ __global__ void __launch_bounds__(kWalkThreads, 6) k_walk_tilepack64(WalkArgs A)
             if (lane <= first_fail) ++c_mac;
             if (tf == 0) {
               partner += A.nleaves[u];
-              double m[9];
+              if (!cut_off(A, dx, dy, dz)) {  // :377
+                double m[9];
 #pragma unroll
-              for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
-              double fx, fy, fz, fp;
-              law_twig64<kLaw>(a.w, m, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp);
-              e0 += fx; e1 += fy; e2 += fz; ph += fp;
-              w += 1.0;
-              ++c_twig;
+                for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
+                double fx, fy, fz, fp;
+                law_twig64<kLaw>(a.w, m, dx, dy, dz, dist2, A.eps2, fx, fy, fz, fp);
+                e0 += fx; e1 += fy; e2 += fz; ph += fp;
+                w += 1.0;
+                ++c_twig;
+              }
               u = (unsigned)fw.y;
               uf = (unsigned)ff.y;
             } else {
@@ -665,6 +682,8 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
   A.tflag = c->tflag.p;
   A.pstart = pstart;
   A.npacks = npacks;
+  A.has_cut = has_spatial_cutoff(c->prm) ? 1 : 0;
+  for (int k = 0; k < 3; ++k) A.cut[k] = c->prm.spatial_interaction_cutoff[k];
   const int blocks = 148 * 8;
   // chunks alternate between the context stream and walk2, so that each
   // chunk's walk starts while the previous one finishes its last buckets

@@ -30,6 +30,9 @@ module module_pepcg
       integer(c_int32_t) :: device
       integer(c_int32_t) :: overwrite_results
       real(c_double) :: kelbg_invsqrttemp
+      integer(c_int32_t) :: group_size
+      integer(c_int32_t) :: reserved0
+      real(c_double) :: spatial_interaction_cutoff(3)
       integer(c_int32_t) :: reserved(4)
    end type
 
@@ -73,10 +76,26 @@ module module_pepcg
          import :: c_int, c_ptr
          type(c_ptr), value :: ctx
       end function
+      integer(c_int) function pepcg_sort_keys(ctx, n, keys, keys_out, perm_out) &
+         bind(c, name="pepcg_sort_keys")
+         import :: c_int, c_ptr, c_int64_t
+         type(c_ptr), value :: ctx
+         integer(c_int64_t), value :: n
+         integer(c_int64_t), intent(in) :: keys(*)
+         integer(c_int64_t), intent(out) :: keys_out(*), perm_out(*)
+      end function
+      integer(c_int) function pepcg_lattice_force(ctx, pos, e, phi) &
+         bind(c, name="pepcg_lattice_force")
+         import :: c_int, c_ptr, c_double
+         type(c_ptr), value :: ctx
+         real(c_double), intent(in) :: pos(3)
+         real(c_double), intent(out) :: e(3), phi
+      end function
    end interface
 
    public :: pepcg_params_default, pepcg_create, pepcg_destroy, pepcg_last_error
    public :: pepcg_grow_tree, pepcg_traverse_tree, pepcg_timber_tree
+   public :: pepcg_sort_keys, pepcg_lattice_force
    public :: pepcg_init_from_namelists, pepcg_grow_and_sort, pepcg_traverse
 
    type(c_ptr), save, public :: pepcg_ctx = c_null_ptr
@@ -85,13 +104,17 @@ contains
 
    !> fills the parameters from the reference's namelist variables
    !> (/calc_force_coulomb/ theta2, eps2; /libpepc/ periodicity, mirror_box_layers,
-   !> force_cubic_domain) and creates the context
+   !> force_cubic_domain; the frontend's spatial_interaction_cutoff, e.g. pepc-mini's
+   !> /pepcmini/ namelist, frontends/pepc-mini/module_helper.f90:82-90) and creates the
+   !> context
    subroutine pepcg_init_from_namelists(theta2, eps2, periodicity, mirror_box_layers, &
-                                        force_cubic_domain, walk, precision)
+                                        force_cubic_domain, walk, precision, &
+                                        spatial_interaction_cutoff)
       real(c_double), intent(in) :: theta2, eps2
       logical, intent(in) :: periodicity(3), force_cubic_domain
       integer, intent(in) :: mirror_box_layers
       integer(c_int32_t), intent(in) :: walk, precision
+      real(c_double), intent(in) :: spatial_interaction_cutoff(3)
       type(pepcg_params) :: p
       integer(c_int) :: rc
       integer :: d
@@ -105,6 +128,7 @@ contains
       p%force_cubic_domain = merge(1_c_int32_t, 0_c_int32_t, force_cubic_domain)
       p%walk = walk
       p%precision = precision
+      p%spatial_interaction_cutoff = spatial_interaction_cutoff
       rc = pepcg_create(pepcg_ctx, p)
       if (rc /= PEPCG_OK) stop "pepcg_create failed"
    end subroutine

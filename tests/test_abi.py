@@ -4,6 +4,7 @@ import ctypes
 import os
 import re
 
+import numpy as np
 import pytest
 
 import pepc_b200
@@ -39,10 +40,13 @@ def test_python_binding_covers_header():
 
 
 def test_params_layout_matches_header():
-    # pepcg_params is 2 doubles + 14 int32 + 12 doubles + 8 int32 (see pepcg.h)
+    # pepcg_params: theta2, eps2; 13 int32 + 4 bytes of padding; 12 lattice
+    # doubles; device, overwrite_results; kelbg_invsqrttemp; group_size,
+    # reserved0; 3 cutoff doubles; reserved[4] (see pepcg.h)
     p = pepc_b200.make_params()
     assert p.theta2 == 0.36 and p.eps2 == 0.0 and p.force_law == 3 and p.tile_size == 16
-    assert ctypes.sizeof(pepc_b200.Params) == 2 * 8 + 14 * 4 + 12 * 8 + 8 * 4
+    assert list(p.spatial_interaction_cutoff) == [np.finfo(np.float64).max] * 3
+    assert ctypes.sizeof(pepc_b200.Params) == 2 * 8 + 14 * 4 + 12 * 8 + 2 * 4 + 8 + 2 * 4 + 3 * 8 + 4 * 4
 
 
 def test_no_device_fails_loudly():

@@ -128,3 +128,25 @@ def test_oracle_madelung_constant(gold):
     r = orc.traverse_tree(g["x"], g["y"], g["z"])
     m_est = -np.mean(g["q"] * r["pot"]) / n
     assert abs(m_est - 1.7475645946331822) < 1e-8
+
+
+def test_oracle_spatial_cutoff_zero_cuts_everything():
+    # any(abs(delta) >= 0) holds for every node: no interaction is evaluated.
+    # The pthreads walk still counts each leaf it reaches as work
+    # (module_tree_walk_pthreads.f90:620-622); the simple walk counts nothing
+    # (module_tree_walk_simple.f90:330,377)
+    rng = np.random.default_rng(74)
+    n = 500
+    x, y, z = rng.random(n), rng.random(n), rng.random(n)
+    q = rng.standard_normal(n)
+    for walk in (0, 1):
+        orc = O.Oracle(theta2=0.25, eps2=1e-4, walk=walk, spatial_interaction_cutoff=(0.0, 0.0, 0.0))
+        g = orc.grow_tree(x, y, z, q)
+        r = orc.traverse_tree(g["x"], g["y"], g["z"], keys=g["key"])
+        assert not np.any(r["pot"]) and not np.any(r["ex"])
+        assert orc.counters()["interactions"] == 0
+        if walk == 0:
+            assert np.all(r["work"] >= 1)
+        else:
+            assert not np.any(r["work"])
+        orc.close()
