@@ -138,28 +138,56 @@ def cpu_baseline(x, y, z, q, theta2, eps2, sample, threads, seed=11):
 
 
 def run_reference(args, rank):
+    """The reference arm: the oracle on all host threads.  Each step really runs
+    the grow of all N particles and the walk of a random sample of targets
+    (args.cpu_sample); the rate for all N targets is extrapolated from the
+    sample's walk time, and the line says so (extrapolated, timed_targets).
+    ms_per_step is the measured time of the step as run."""
     if rank != 0:
         return
     x, y, z, q = plummer(args.n)
     threads = os.cpu_count() or 1
-    vals = []
+    vals, step_ms = [], []
+    t_run0 = time.perf_counter()
     for i in range(args.warmup + args.steps):
         cb = cpu_baseline(x, y, z, q, args.theta ** 2, args.eps ** 2, args.cpu_sample, threads,
                           seed=100 + i)
         if i >= args.warmup:
             vals.append(cb["value"])
+            step_ms.append((cb["t_grow_s"] + cb["t_walk_sample_s"]) * 1e3)
     v = statistics.median(vals)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": args.n / v * 1e3,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": statistics.median(step_ms),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
+            "extrapolated": True, "timed_targets": min(args.cpu_sample, args.n),
+            "ms_per_step_extrapolated": args.n / v * 1e3,
+            "run_s": time.perf_counter() - t_run0,
             "config": {"workload": workload_name(args), "implementation":
                        "CPU restatement of the reference tree code (oracle, per-target walk), "
-                       "all host threads; the reference itself needs gfortran + MPI, absent here"},
+                       "all host threads; the reference itself needs gfortran + MPI, absent here",
+                       "step": f"grow of all {args.n} particles + per-target walk of "
+                               f"{min(args.cpu_sample, args.n)} random targets; value = "
+                               f"{args.n} / (grow time + sample walk time x {args.n} / sample)"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": cb["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def launch_ranks(args):
+    """--gpus N without a launcher: run this script as N ranks under
+    torch.distributed.run (one process per GPU, 127.0.0.1 rendezvous) and
+    return its exit status."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr", "127.0.0.1",
+           "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
 
 
 def hbm_peak_gbs():
@@ -359,7 +387,7 @@ def run_madelung(args, P, torch, dev, stream):
     print(json.dumps(out_line), flush=True)
 
 
-def run_sharded(args, P, torch, dev, stream, dist, rank, world, local):
+def run_sharded(args, P, torch, dev, stream, dist, rank, world, local, emit=True):
     """Target sharding (strong scaling): rank 0's particles are broadcast, every
     rank grows the same tree from them, walks its shard_range share of the
     key-ordered targets (pepcg_traverse_range_device) and all-gathers the
@@ -412,6 +440,11 @@ def run_sharded(args, P, torch, dev, stream, dist, rank, world, local):
     torch.cuda.synchronize()
     same = all(bool(torch.equal(full[0][k], ref[k])) for k in range(5))
     tc.close()
+    if not emit:
+        return {"value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "scaling": "strong",
+                "n_gpus": world, "fields_equal_single_call": same, "gpu_launches": launches,
+                "parallelism": f"target shards over {world} ranks: broadcast of the particles, "
+                               "replicated tree, all-gather of the fields"}
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": n / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
@@ -455,9 +488,13 @@ def main():
     args = ap.parse_args()
     assert args.warmup >= 3, "at least 3 warm-up steps"
 
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        sys.exit(launch_ranks(args))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        sys.exit(f"bench.py: --gpus {args.gpus} but the launcher started {world} ranks")
     if args.impl == "reference":
         run_reference(args, rank)
         return
@@ -638,6 +675,14 @@ def main():
                "api": "pepcg_grow_tree + pepcg_traverse_tree (host arrays, pinned; "
                       "overwrite_results = 1)", "fields_equal_device_path": same}
 
+    # with several ranks, the same workload sharded over them (strong scaling)
+    sharded = None
+    if world > 1:
+        sstream = torch.cuda.Stream(device=dev)
+        with torch.cuda.stream(sstream):
+            sharded = run_sharded(args, P, torch, dev, sstream, dist, rank, world, local,
+                                  emit=False)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(x, y, z, q, args.theta ** 2, args.eps ** 2, args.cpu_sample,
@@ -666,6 +711,7 @@ def main():
         "clocks": clk, "e2e": e2e, "plain": plain,
         "mixed_over_plain": (value / plain["value"]) if plain else None,
         "cpu_baseline": cpu,
+        "sharded": sharded,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

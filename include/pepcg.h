@@ -245,6 +245,19 @@ int pepcg_set_stream(void* ctx, void* stream);
 /* Total number of kernels this library has launched in the process. */
 long long pepcg_kernel_launches(void);
 
+/*
+ * pepcg_debug_fail_allocations -- allocation-failure injection for tests, in
+ * the spirit of the reference's DEBUG_ERROR checks (module_debug.f90:167),
+ * which abort the run; here the failing call returns a status instead.  After
+ * `after` more successful device allocations by the library (in this
+ * process), every further one fails as if the device had run out of memory,
+ * so the call that needed it returns PEPCG_ERR_OOM and leaves its context
+ * usable (a later call allocates again).  A negative value switches the
+ * injection off, which is the default.  Host side only: nothing reaches the
+ * device.
+ */
+void pepcg_debug_fail_allocations(int64_t after);
+
 /* replaces pepc_timber_tree (module_pepc.f90:538 -> module_libpepc_main.f90:129-148) */
 int pepcg_timber_tree(void* ctx);
 int pepcg_stats_get(void* ctx, pepcg_stats* s);

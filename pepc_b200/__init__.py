@@ -122,6 +122,7 @@ EXPORTS = [
     "pepcg_constrain_periodic_device", "pepcg_gather_device",
     "pepcg_traverse_range_device", "pepcg_restore_device",
     "pepcg_sort_keys", "pepcg_sort_keys_device", "pepcg_lattice_force",
+    "pepcg_debug_fail_allocations",
 ]
 
 _LIB = None
@@ -162,6 +163,8 @@ def lib():
     L.pepcg_gather_device.argtypes = [VP, VP, VP]
     L.pepcg_traverse_range_device.argtypes = [VP, C.c_int64, C.c_int64, VP, VP, VP, VP, VP]
     L.pepcg_restore_device.argtypes = [VP, VP, VP]
+    L.pepcg_debug_fail_allocations.argtypes = [C.c_int64]
+    L.pepcg_debug_fail_allocations.restype = None
     L.pepcg_kernel_launches.argtypes = []
     L.pepcg_kernel_launches.restype = C.c_longlong
     L.pepcg_stats_get.argtypes = [VP, C.POINTER(Stats)]

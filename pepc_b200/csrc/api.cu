@@ -29,6 +29,17 @@ bool cuda_ok(Ctx* c, cudaError_t e, const char* what) {
   return false;
 }
 
+// allocations left before the injected failures start (< 0: no injection)
+static std::atomic<int64_t> g_fail_after{-1};
+
+// true when the injection makes this allocation fail
+static bool injected_failure() {
+  int64_t left = g_fail_after.load();
+  while (left > 0 && !g_fail_after.compare_exchange_weak(left, left - 1)) {
+  }
+  return left == 0;
+}
+
 template <class T>
 bool ensure(Ctx* c, DBuf<T>& b, size_t n, const char* what) {
   if (n <= b.cap) return true;
@@ -36,6 +47,11 @@ bool ensure(Ctx* c, DBuf<T>& b, size_t n, const char* what) {
   b.p = nullptr;
   b.cap = 0;
   size_t want = n + n / 8 + 64;
+  if (injected_failure()) {
+    c->err = std::string("device allocation failed for ") + what + " (" +
+             std::to_string(want * sizeof(T)) + " bytes): injected by pepcg_debug_fail_allocations";
+    return false;
+  }
   cudaError_t e = cudaMalloc((void**)&b.p, want * sizeof(T));
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -888,6 +904,8 @@ int pepcg_gather_device(void* ctx, const double* d_in, double* d_out) {
   cudaSetDevice(c->device);
   return gather_device(c, d_in, d_out);
 }
+
+void pepcg_debug_fail_allocations(int64_t after) { g_fail_after.store(after < 0 ? -1 : after); }
 
 int pepcg_sort_keys_device(void* ctx, int64_t n, const int64_t* d_keys, int64_t* d_keys_out,
                            int64_t* d_perm_out) {

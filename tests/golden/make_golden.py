@@ -1,9 +1,10 @@
 """Generate the golden fixtures that pin the oracle to the reference.
 
-Run in a container where the reference tree is mounted (REF, default
-/root/reference) and oracle/_ref has been built (make -C oracle):
+Run where the reference tree is checked out, with its root in REF, after
+oracle/_ref has been built from it:
 
-    python tests/golden/make_golden.py
+    make -C oracle REF=<reference root>
+    REF=<reference root> python tests/golden/make_golden.py
 
 Writes tests/golden/reference_pins.npz and reference_pins.json:
   * sort_*      : the reference's own local key sort (sl_pepc sort_radix.c,
@@ -28,7 +29,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 from oracle import oracle as O  # noqa: E402
 
-REF = os.environ.get("REF", "/root/reference")
+REF = os.environ.get("REF")
 
 
 def sort_sets():
@@ -67,6 +68,8 @@ def par_rand_kat():
 
 
 def main():
+    if not REF or not os.path.isdir(REF):
+        raise SystemExit("set REF to the root of the reference checkout")
     out = {}
     prov = {"reference": "ALaDyn/pepc", "sort": "oracle/_ref/libslref.so (sl_pepc sort_radix.c)"}
     for name, keys in sort_sets().items():

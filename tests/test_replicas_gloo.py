@@ -2,7 +2,7 @@
 timing of bench.py (each rank runs its own copy of the workload, the step
 time is the slowest rank's, the job's rate counts every rank's particles),
 and the target shares of pepc_b200.shard_range (contiguous, disjoint,
-covering, 32-aligned), gathered across the ranks."""
+covering, 64-aligned), gathered across the ranks."""
 import os
 import socket
 
@@ -13,6 +13,8 @@ import torch.multiprocessing as mp
 
 import bench
 import pepc_b200
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def _free_port():
@@ -104,3 +106,14 @@ def test_gather_shards_rebuilds_the_fields(n):
                        join=True, start_method="spawn")
     want = [[10.0 * f + t for t in range(n)] for f in range(5)]
     assert out[0] == want and out[1] == want
+
+
+def test_bench_refuses_a_rank_count_that_differs_from_gpus():
+    # --gpus N must be the number of ranks the launcher started
+    import subprocess
+    import sys
+    env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2"],
+                       env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0
+    assert "--gpus 2" in r.stderr
