@@ -473,11 +473,12 @@ def main():
     ap.add_argument("--n", type=int, default=4194304)
     ap.add_argument("--theta", type=float, default=0.4)
     ap.add_argument("--eps", type=float, default=1e-3)
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "plain"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "plain", "strict"])
     ap.add_argument("--walk", default="group", choices=["group", "target", "tile"])
     ap.add_argument("--ntest", type=int, default=8192)
     ap.add_argument("--cpu-sample", type=int, default=32768)
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-strict", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--shard", action="store_true",
@@ -535,7 +536,8 @@ def main():
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
     walk = {"group": P.WALK_GROUP, "target": P.WALK_PER_TARGET, "tile": P.WALK_PER_TILE}[args.walk]
-    prec = P.PRECISION_MIXED if args.precision == "mixed" else P.PRECISION_PLAIN
+    prec = {"mixed": P.PRECISION_MIXED, "plain": P.PRECISION_PLAIN,
+            "strict": P.PRECISION_MIXED_STRICT}[args.precision]
     tc = P.TreeCode(theta2=args.theta ** 2, eps2=args.eps ** 2, precision=prec, walk=walk,
                     device=local)
     tc.set_stream(stream.cuda_stream)
@@ -588,11 +590,11 @@ def main():
 
     # roofline of the dominant kernel (the walk)
     f_mhz = clk["sm_mhz"] if clk and clk["sm_mhz"] else 1965.0
-    lanes = 128 if prec == P.PRECISION_MIXED else 64  # FP32 / FP64 lanes per SM
+    lanes = 64 if prec == P.PRECISION_PLAIN else 128  # FP64 / FP32 lanes per SM
     peak = SMS * lanes * 2 * f_mhz * 1e6 / 1e12
     flops = FLOPS_TWIG * st["twig_interactions"] + FLOPS_LEAF * st["leaf_interactions"]
     achieved = flops / (st["t_walk_ms"] * 1e-3) / 1e12
-    roof = {"bound": "fp32-core" if prec == P.PRECISION_MIXED else "fp64-core",
+    roof = {"bound": "fp64-core" if prec == P.PRECISION_PLAIN else "fp32-core",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "traffic": (WALK_DRAM_BYTES_PER_PARTICLE * n
                         if prec == P.PRECISION_MIXED and args.walk == "group" and args.theta == 0.4
@@ -625,6 +627,25 @@ def main():
                  "force_err_median": float(np.median(prel_p)),
                  "force_err_p99": float(np.percentile(prel_p, 99))}
         tp.close()
+
+    # the north star's precision form of the same group walk (FP64 offsets per
+    # interaction, compensated FP32 sums, the FP64 walk's MAC decisions)
+    strict = None
+    if not args.no_strict and prec == P.PRECISION_MIXED and args.walk == "group":
+        ts = P.TreeCode(theta2=args.theta ** 2, eps2=args.eps ** 2,
+                        precision=P.PRECISION_MIXED_STRICT, walk=P.WALK_GROUP, device=local)
+        ts.set_stream(stream.cuda_stream)
+        sms, _, _ = timed(ts, max(1, min(args.steps, 3)), 3)
+        sst = ts.stats()
+        Es = torch.stack(out[:3]).cpu().numpy()[:, tidx]
+        rel_s = np.linalg.norm(Es - Ed, axis=0) / np.linalg.norm(Ed, axis=0)
+        strict = {"value": n * world / (sms * 1e-3), "ms_per_step": sms,
+                  "walk_ms": sst["t_walk_ms"], "interactions": sst["interactions"],
+                  "force_err_median": float(np.median(rel_s)),
+                  "force_err_p99": float(np.percentile(rel_s, 99)),
+                  "form": "offsets target minus node centre in FP64 per interaction, Kahan-"
+                          "compensated FP32 sums, FP64 MAC decisions"}
+        ts.close()
 
     # end to end through the host API (pinned host buffers, copies inside the timed region)
     e2e = None
@@ -692,11 +713,11 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32 interactions + f64 offsets/sums" if prec == P.PRECISION_MIXED else "f64",
+        "dtype": "f64" if prec == P.PRECISION_PLAIN else "f32 interactions + f64 offsets/sums",
         "data": "synthetic",
         "config": {"workload": workload_name(args), "precision": args.precision,
                    "walk": args.walk,
-                   "group_size": (64 if prec == P.PRECISION_MIXED else 32) if args.walk == "group"
+                   "group_size": (32 if prec == P.PRECISION_PLAIN else 64) if args.walk == "group"
                    else None,
                    "parallelism": "replicas only" if world > 1 else "single GPU",
                    "l2": "inputs (128 MB) and tree (~0.7 GB) exceed the 126 MB L2; no flush",
@@ -710,6 +731,7 @@ def main():
         "gpu_launches": launches,
         "clocks": clk, "e2e": e2e, "plain": plain,
         "mixed_over_plain": (value / plain["value"]) if plain else None,
+        "strict": strict,
         "cpu_baseline": cpu,
         "sharded": sharded,
     }

@@ -54,6 +54,11 @@ extern "C" {
 
 #define PEPCG_PRECISION_PLAIN 0 /* FP64 throughout: the drop-in */
 #define PEPCG_PRECISION_MIXED 1 /* FP64 offsets + FP32 interactions + FP64 sums */
+#define PEPCG_PRECISION_MIXED_STRICT 2 /* the mixed form with every interaction offset the
+                                          target minus the node centre in FP64, rounded
+                                          once, Kahan-compensated FP32 sums, and the FP64
+                                          group walk's MAC decisions; GROUP walk with
+                                          64-target buckets */
 
 #define PEPCG_WALK_PER_TARGET 0 /* module_tree_walk_pthreads semantics (pepc-mini) */
 #define PEPCG_WALK_PER_TILE 1   /* module_tree_walk_simple semantics (pepc-essential) */

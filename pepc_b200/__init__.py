@@ -37,7 +37,7 @@ PEPCG_ERR_UNSUPPORTED = 9
 PEPCG_WARN_NOT_NEUTRAL = 100
 
 CURVE_HILBERT, CURVE_MORTON = 0, 1
-PRECISION_PLAIN, PRECISION_MIXED = 0, 1
+PRECISION_PLAIN, PRECISION_MIXED, PRECISION_MIXED_STRICT = 0, 1, 2
 WALK_PER_TARGET, WALK_PER_TILE, WALK_GROUP = 0, 1, 2
 
 D = C.POINTER(C.c_double)

@@ -172,9 +172,15 @@ static int check_params(Ctx* c, const pepcg_params* p) {
     c->err = "curve must be PEPCG_CURVE_HILBERT or PEPCG_CURVE_MORTON";
     return PEPCG_ERR_BAD_ARG;
   }
-  if (p->precision != PEPCG_PRECISION_PLAIN && p->precision != PEPCG_PRECISION_MIXED) {
-    c->err = "precision must be PLAIN or MIXED";
+  if (p->precision != PEPCG_PRECISION_PLAIN && p->precision != PEPCG_PRECISION_MIXED &&
+      p->precision != PEPCG_PRECISION_MIXED_STRICT) {
+    c->err = "precision must be PLAIN, MIXED or MIXED_STRICT";
     return PEPCG_ERR_BAD_ARG;
+  }
+  if (p->precision == PEPCG_PRECISION_MIXED_STRICT &&
+      (p->walk != PEPCG_WALK_GROUP || (p->group_size != 0 && p->group_size != 64))) {
+    c->err = "MIXED_STRICT is built for the GROUP walk with 64-target buckets";
+    return PEPCG_ERR_UNSUPPORTED;
   }
   if (p->walk < 0 || p->walk > 2) {
     c->err = "walk must be PER_TARGET, PER_TILE or GROUP";

@@ -180,7 +180,7 @@ struct Ctx {
   // memory, so walks of different contexts may run concurrently on one device.
   // targets per bucket of the group walk (pepcg_params.group_size, 0 resolved)
   int group_size() const {
-    return prm.group_size ? prm.group_size : (prm.precision == PEPCG_PRECISION_MIXED ? 64 : 32);
+    return prm.group_size ? prm.group_size : (prm.precision != PEPCG_PRECISION_PLAIN ? 64 : 32);
   }
   // Slot 0 serves walks on the context stream, slot 1 walks on walk2.
   unsigned int* walk_queue(int slot = 0) { return reinterpret_cast<unsigned int*>(d_small + 8 + slot); }

@@ -24,6 +24,8 @@
 // (expanding the reference's fdx.. / pre2x.. terms gives exactly these
 // polynomials), which needs 39 FP32 operations instead of ~130.
 
+#include <type_traits>
+
 #include "internal.cuh"
 
 namespace pepcg {
@@ -48,6 +50,7 @@ struct MixArgs {
   int nbox;
   float theta2;
   float eps2;
+  double theta2d;  // theta2 in FP64 (the strict form's exact MAC)
   int32_t M;
   int64_t npart;
   double* ex;
@@ -68,10 +71,22 @@ struct MixArgs {
   const int32_t* npacks;  // the number of packs (device)
 };
 
+// 1/sqrt(x) by the PTX instruction rsqrt.approx.ftz.f32 (relative error below
+// 2^-22, subnormal inputs and results flushed to zero).  The arguments here are
+// squared distances plus eps2; a zero argument gives +inf and is selected away
+// by the callers that can meet it (the leaves' self pairs).  rsqrtf would add a
+// range fix-up for subnormal arguments on every call: at 4M this form takes the
+// benchmark's walk from 38.5 to 36.0 ms with identical results.
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 __device__ __forceinline__ void leaf32(float q, float dx, float dy, float dz, float eps2,
                                        float& ax, float& ay, float& az, float& ap) {
   const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-  const float ri = rsqrtf(r2);
+  const float ri = rsqrt_ftz(r2);
   const float qr = q * ri;
   const float qr3 = qr * ri * ri;
   ap += qr;
@@ -91,7 +106,7 @@ __device__ __forceinline__ void twig32(float4 m0, float4 m1, float4 m2, float dx
                                        float dz, float eps2, float& ax, float& ay, float& az,
                                        float& ap) {
   const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-  const float ri = rsqrtf(r2);
+  const float ri = rsqrt_ftz(r2);
   const float ri2 = ri * ri;
   const float rd3 = ri * ri2;
   const float q = m2.z;
@@ -119,7 +134,7 @@ __device__ __forceinline__ void twig32x2(float4 m0, float4 m1, float4 m2, float2
                                          float2 dz, float2 eps2, float2& ax, float2& ay,
                                          float2& az, float2& ap) {
   const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
-  const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+  const float2 ri = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
   const float2 ri2 = __fmul2_rn(ri, ri);
   const float2 rd3 = __fmul2_rn(ri, ri2);
   const float2 q = f2(m2.z);
@@ -135,6 +150,39 @@ __device__ __forceinline__ void twig32x2(float4 m0, float4 m1, float4 m2, float2
   ax = __ffma2_rn(rd3, __ffma2_rn(t4, dx, __ffma2_rn(m2r, vx, f2(m0.x))), ax);
   ay = __ffma2_rn(rd3, __ffma2_rn(t4, dy, __ffma2_rn(m2r, vy, f2(m0.y))), ay);
   az = __ffma2_rn(rd3, __ffma2_rn(t4, dz, __ffma2_rn(m2r, vz, f2(m0.z))), az);
+}
+
+// twig32x2's terms of one interaction, returned instead of accumulated (the
+// strict form adds them with compensation)
+__device__ __forceinline__ void twig32x2_terms(float4 m0, float4 m1, float4 m2, float2 dx,
+                                               float2 dy, float2 dz, float2 eps2, float2& ax,
+                                               float2& ay, float2& az, float2& ap) {
+  const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
+  const float2 ri = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+  const float2 ri2 = __fmul2_rn(ri, ri);
+  const float2 rd3 = __fmul2_rn(ri, ri2);
+  const float2 q = f2(m2.z);
+  const float2 A = __ffma2_rn(dx, f2(m0.x), __ffma2_rn(dy, f2(m0.y), __ffma2_rn(dz, f2(m0.z), f2(m2.y))));
+  const float2 vx = __ffma2_rn(f2(m0.w), dx, __ffma2_rn(f2(m1.z), dy, __fmul2_rn(f2(m2.x), dz)));
+  const float2 vy = __ffma2_rn(f2(m1.z), dx, __ffma2_rn(f2(m1.x), dy, __fmul2_rn(f2(m1.w), dz)));
+  const float2 vz = __ffma2_rn(f2(m2.x), dx, __ffma2_rn(f2(m1.w), dy, __fmul2_rn(f2(m1.y), dz)));
+  const float2 B = __ffma2_rn(dx, vx, __ffma2_rn(dy, vy, __fmul2_rn(dz, vz)));
+  const float2 t1 = __ffma2_rn(ri2, B, make_float2(-A.x, -A.y));
+  ap = __fmul2_rn(ri, __ffma2_rn(ri2, t1, q));
+  const float2 t4 = __ffma2_rn(ri2, __ffma2_rn(f2(5.0f), t1, __fadd2_rn(A, A)), q);
+  const float2 m2r = __fmul2_rn(f2(-2.0f), ri2);
+  ax = __fmul2_rn(rd3, __ffma2_rn(t4, dx, __ffma2_rn(m2r, vx, f2(m0.x))));
+  ay = __fmul2_rn(rd3, __ffma2_rn(t4, dy, __ffma2_rn(m2r, vy, f2(m0.y))));
+  az = __fmul2_rn(rd3, __ffma2_rn(t4, dz, __ffma2_rn(m2r, vz, f2(m0.z))));
+}
+
+// Kahan (compensated) summation, both lanes of a pair: s += v with the
+// running compensation c (the sum is s - c)
+__device__ __forceinline__ void kahan2(float2& s, float2& c, float2 v) {
+  const float2 y = __fadd2_rn(v, make_float2(-c.x, -c.y));
+  const float2 t = __fadd2_rn(s, y);
+  c = __fadd2_rn(__fadd2_rn(t, make_float2(-s.x, -s.y)), make_float2(-y.x, -y.y));
+  s = t;
 }
 
 __device__ __forceinline__ void warp_add3(unsigned long long* ctr, unsigned long long a,
@@ -200,6 +248,12 @@ struct __align__(16) StagedTwig {
   float4 m0;  // px py pz 3qxx
   float4 m1;  // 3qyy 3qzz 1.5qxy 1.5qyz
   float4 m2;  // 1.5qzx, trace, charge, -
+};
+// the strict form's twig record: the FP64 node centre, then the moments
+struct __align__(16) StagedTwigS {
+  double cx, cy, cz;
+  float pad[2];
+  float4 m0, m1, m2;
 };
 struct __align__(16) StagedLeaf {
   float4 c;          // (x - g) rounded from FP64, charge
@@ -454,20 +508,34 @@ __global__ void __launch_bounds__(kMixThreads, 5)
 // packed add.  Against 32-target buckets the larger group is opened more
 // often (about 9 % more interactions at 4M, theta 0.4); the packed pair
 // arithmetic and the halved traversal per target more than pay for it.
-__global__ void __launch_bounds__(kMixThreads, 5)
+//
+// kStrict (PEPCG_PRECISION_MIXED_STRICT): every interaction offset is the
+// target minus the node centre formed in FP64 and then rounded, the FP32 sums
+// of a batch are Kahan-compensated, and the group's MAC decisions equal the
+// FP64 group walk's (k_walk_tile64 with two targets per lane): the bounding-
+// sphere test is made conservative by a relative margin, and every node it
+// leaves undecided gets the reference's FP64 test per target.  Twig records
+// carry the FP64 node centre; four blocks per SM (128 registers).
+template <bool kStrict>
+__global__ void __launch_bounds__(kMixThreads, kStrict ? 4 : 5)
     k_walk_group64(MixArgs A, int* __restrict__ gstack, const int4* __restrict__ child8,
                    const int* __restrict__ nchild) {
+  using TwigRec = typename std::conditional<kStrict, StagedTwigS, StagedTwig>::type;
   __shared__ float s_bl2[kMaxLevel + 1];
+  __shared__ double s_bl2d[kStrict ? kMaxLevel + 1 : 1];
   __shared__ double s_vb[3 * 125];
-  __shared__ StagedTwig s_tw[kWW][kRing];
+  __shared__ TwigRec s_tw[kWW][kRing];
   __shared__ StagedLeaf s_lf[kWW][kRing];
-  for (int i = threadIdx.x; i <= kMaxLevel; i += blockDim.x) s_bl2[i] = (float)A.bl2[i];
+  for (int i = threadIdx.x; i <= kMaxLevel; i += blockDim.x) {
+    s_bl2[i] = (float)A.bl2[i];
+    if constexpr (kStrict) s_bl2d[i] = A.bl2[i];
+  }
   for (int i = threadIdx.x; i < 3 * A.nbox; i += blockDim.x) s_vb[i] = A.vbox[i];
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
   int* stack = gstack + (int64_t)(blockIdx.x * kWW + w) * kStackCap;
-  StagedTwig* stw = s_tw[w];
+  TwigRec* stw = s_tw[w];
   StagedLeaf* stl = s_lf[w];
   const float theta2 = A.theta2;
   const int64_t nbuckets = (A.nt + 63) / 64;
@@ -516,6 +584,9 @@ __global__ void __launch_bounds__(kMixThreads, 5)
     for (int ib = 0; ib < A.nbox; ++ib) {
       const double vx = s_vb[3 * ib], vy = s_vb[3 * ib + 1], vz = s_vb[3 * ib + 2];
       const double gx = g0x - vx, gy = g0y - vy, gz = g0z - vz;
+      // the targets' shifted positions x - vbox (the strict form's offsets)
+      const double sxa = pxa - vx, sya = pya - vy, sza = pza - vz;
+      const double sxb = pxb - vx, syb = pyb - vy, szb = pzb - vz;
       int64_t partner = 0;
       int nT = 0, hT = 0, nL = 0, hL = 0;
       int top = 1;
@@ -524,13 +595,43 @@ __global__ void __launch_bounds__(kMixThreads, 5)
       auto flush_twigs = [&](int n) {
         cp_async_wait_all();
         __syncwarp();
-        if (v0) {
+        if constexpr (kStrict) {
+          if (v0) {
+            float2 PX = f2(0.f), PY = f2(0.f), PZ = f2(0.f), PP = f2(0.f);
+            float2 CX = f2(0.f), CY = f2(0.f), CZ = f2(0.f), CP = f2(0.f);
+            const float2 E2 = f2(A.eps2);
+            auto one = [&](const TwigRec& r) {
+              // target minus node centre in FP64, rounded once
+              const float2 dx = make_float2((float)(sxa - r.cx), (float)(sxb - r.cx));
+              const float2 dy = make_float2((float)(sya - r.cy), (float)(syb - r.cy));
+              const float2 dz = make_float2((float)(sza - r.cz), (float)(szb - r.cz));
+              float2 tx, ty, tz, tp;
+              twig32x2_terms(r.m0, r.m1, r.m2, dx, dy, dz, E2, tx, ty, tz, tp);
+              kahan2(PX, CX, tx);
+              kahan2(PY, CY, ty);
+              kahan2(PZ, CZ, tz);
+              kahan2(PP, CP, tp);
+            };
+            const int n1 = min(n, kRing - hT);
+            const TwigRec* r = stw + hT;
+#pragma unroll 4
+            for (int j = 0; j < n1; ++j) one(r[j]);
+#pragma unroll 2
+            for (int j = 0; j < n - n1; ++j) one(stw[j]);
+            // the compensated sum is s - c
+            Ea0 += (double)PX.x - (double)CX.x; Ea1 += (double)PY.x - (double)CY.x;
+            Ea2 += (double)PZ.x - (double)CZ.x; PHa += (double)PP.x - (double)CP.x;
+            Eb0 += (double)PX.y - (double)CX.y; Eb1 += (double)PY.y - (double)CY.y;
+            Eb2 += (double)PZ.y - (double)CZ.y; PHb += (double)PP.y - (double)CP.y;
+            c_twig += (unsigned)n * (v1 ? 2u : 1u);
+          }
+        } else if (v0) {
           float2 PX = f2(0.f), PY = f2(0.f), PZ = f2(0.f), PP = f2(0.f);
           const float2 RX = make_float2(rxa, rxb), RY = make_float2(rya, ryb),
                        RZ = make_float2(rza, rzb);
           const float2 E2 = f2(A.eps2);
           const int n1 = min(n, kRing - hT);
-          const StagedTwig* r = stw + hT;
+          const TwigRec* r = stw + hT;
 #pragma unroll 8
           for (int j = 0; j < n1; ++j) {
             // c is the negated offset: one packed add per axis
@@ -556,44 +657,29 @@ __global__ void __launch_bounds__(kMixThreads, 5)
       };
       auto flush_leaves = [&](int n) {
         __syncwarp();
-        if (v0) {
+        if (kStrict && v0) {
           float2 PX = f2(0.f), PY = f2(0.f), PZ = f2(0.f), PP = f2(0.f);
-          const float2 RX = make_float2(rxa, rxb), RY = make_float2(rya, ryb),
-                       RZ = make_float2(rza, rzb);
+          float2 CX = f2(0.f), CY = f2(0.f), CZ = f2(0.f), CP = f2(0.f);
           const float2 E2 = f2(A.eps2);
           unsigned nuse = 0;
           auto leaf = [&](const StagedLeaf& r) {
-            const float4 c = r.c;
-            float2 dx = __fadd2_rn(RX, f2(-c.x)), dy = __fadd2_rn(RY, f2(-c.y)),
-                   dz = __fadd2_rn(RZ, f2(-c.z));
-            const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-            float2 wq = f2(c.w);
-            if (d2.x == 0.f || (v1 && d2.y == 0.f)) {
-              // self (dist2 == 0 in FP64) or two points closer than the FP32
-              // resolution at the group scale: decide and evaluate in FP64
-              if (d2.x == 0.f) {
-                const double ex = (A.tx[ta] - vx) - r.x, ey = (A.ty[ta] - vy) - r.y,
-                             ez = (A.tz[ta] - vz) - r.z;
-                if (ex == 0.0 && ey == 0.0 && ez == 0.0) { wq.x = 0.f; ++nuse; }
-                dx.x = (float)ex; dy.x = (float)ey; dz.x = (float)ez;
-              }
-              if (v1 && d2.y == 0.f) {
-                const double ex = (A.tx[tb] - vx) - r.x, ey = (A.ty[tb] - vy) - r.y,
-                             ez = (A.tz[tb] - vz) - r.z;
-                if (ex == 0.0 && ey == 0.0 && ez == 0.0) { wq.y = 0.f; ++nuse; }
-                dx.y = (float)ex; dy.y = (float)ey; dz.y = (float)ez;
-              }
-            }
-            // the pair's leaf32 in packed FP32; a self pair enters with charge 0,
-            // and a zero r2 (eps2 = 0) gives no contribution instead of inf
+            const double exa = sxa - r.x, eya = sya - r.y, eza = sza - r.z;
+            const double exb = sxb - r.x, eyb = syb - r.y, ezb = szb - r.z;
+            float2 wq = f2(r.c.w);
+            // self: dist2 == 0 in FP64 (module_tree_walk_pthreads.f90:625)
+            if (exa == 0.0 && eya == 0.0 && eza == 0.0) { wq.x = 0.f; ++nuse; }
+            if (v1 && exb == 0.0 && eyb == 0.0 && ezb == 0.0) { wq.y = 0.f; ++nuse; }
+            const float2 dx = make_float2((float)exa, (float)exb);
+            const float2 dy = make_float2((float)eya, (float)eyb);
+            const float2 dz = make_float2((float)eza, (float)ezb);
             const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, E2)));
-            const float2 ri = make_float2(r2.x > 0.f ? rsqrtf(r2.x) : 0.f, r2.y > 0.f ? rsqrtf(r2.y) : 0.f);
+            const float2 ri = make_float2(r2.x > 0.f ? rsqrt_ftz(r2.x) : 0.f, r2.y > 0.f ? rsqrt_ftz(r2.y) : 0.f);
             const float2 qr = __fmul2_rn(wq, ri);
             const float2 qr3 = __fmul2_rn(__fmul2_rn(qr, ri), ri);
-            PP = __fadd2_rn(PP, qr);
-            PX = __ffma2_rn(qr3, dx, PX);
-            PY = __ffma2_rn(qr3, dy, PY);
-            PZ = __ffma2_rn(qr3, dz, PZ);
+            kahan2(PP, CP, qr);
+            kahan2(PX, CX, __fmul2_rn(qr3, dx));
+            kahan2(PY, CY, __fmul2_rn(qr3, dy));
+            kahan2(PZ, CZ, __fmul2_rn(qr3, dz));
           };
           const int n1 = min(n, kRing - hL);
           const StagedLeaf* r = stl + hL;
@@ -601,6 +687,73 @@ __global__ void __launch_bounds__(kMixThreads, 5)
           for (int j = 0; j < n1; ++j) leaf(r[j]);
 #pragma unroll 2
           for (int j = 0; j < n - n1; ++j) leaf(stl[j]);
+          Ea0 += (double)PX.x - (double)CX.x; Ea1 += (double)PY.x - (double)CY.x;
+          Ea2 += (double)PZ.x - (double)CZ.x; PHa += (double)PP.x - (double)CP.x;
+          Eb0 += (double)PX.y - (double)CX.y; Eb1 += (double)PY.y - (double)CY.y;
+          Eb2 += (double)PZ.y - (double)CZ.y; PHb += (double)PP.y - (double)CP.y;
+          c_leaf += (unsigned)n * (v1 ? 2u : 1u) - nuse;
+        } else if (v0) {
+          float2 PX = f2(0.f), PY = f2(0.f), PZ = f2(0.f), PP = f2(0.f);
+          const float2 RX = make_float2(rxa, rxb), RY = make_float2(rya, ryb),
+                       RZ = make_float2(rza, rzb);
+          const float2 E2 = f2(A.eps2);
+          unsigned nuse = 0;
+          auto leaf = [&](const StagedLeaf& r, int k, unsigned& pend) {
+            const float4 c = r.c;
+            const float2 dx = __fadd2_rn(RX, f2(-c.x)), dy = __fadd2_rn(RY, f2(-c.y)),
+                         dz = __fadd2_rn(RZ, f2(-c.z));
+            const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+            // a zero FP32 offset (the target's own leaf, or two points closer
+            // than FP32 resolves at the group scale) enters with charge 0 here,
+            // without a branch, and is decided and evaluated in FP64 after the
+            // batch (pend: one bit per record of the batch)
+            const bool za = d2.x == 0.f, zb = v1 && d2.y == 0.f;
+            pend |= (za || zb) ? (1u << k) : 0u;
+            const float2 wq = make_float2(za ? 0.f : c.w, zb ? 0.f : c.w);
+            // the pair's leaf32 in packed FP32; a zero r2 (eps2 = 0) gives no
+            // contribution instead of inf
+            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, E2)));
+            const float2 ri = make_float2(r2.x > 0.f ? rsqrt_ftz(r2.x) : 0.f, r2.y > 0.f ? rsqrt_ftz(r2.y) : 0.f);
+            const float2 qr = __fmul2_rn(wq, ri);
+            const float2 qr3 = __fmul2_rn(__fmul2_rn(qr, ri), ri);
+            PP = __fadd2_rn(PP, qr);
+            PX = __ffma2_rn(qr3, dx, PX);
+            PY = __ffma2_rn(qr3, dy, PY);
+            PZ = __ffma2_rn(qr3, dz, PZ);
+          };
+          unsigned pend = 0;
+          const int n1 = min(n, kRing - hL);
+          const StagedLeaf* r = stl + hL;
+#pragma unroll 4
+          for (int j = 0; j < n1; ++j) leaf(r[j], j, pend);
+#pragma unroll 2
+          for (int j = 0; j < n - n1; ++j) leaf(stl[j], n1 + j, pend);
+          // the zero-offset pairs: self when the FP64 offset is exactly zero
+          // (dist2 == 0, module_tree_walk_pthreads.f90:625), else evaluated on
+          // the FP64 offset rounded once
+          while (pend) {
+            const int k = __ffs(pend) - 1;
+            pend &= pend - 1;
+            const StagedLeaf& rr = stl[(hL + k) & (kRing - 1)];
+            const float4 c = rr.c;
+            for (int s2 = 0; s2 < 2; ++s2) {
+              if (s2 == 1 && !v1) break;
+              const float fx = (s2 ? rxb : rxa) - c.x, fy = (s2 ? ryb : rya) - c.y,
+                          fz = (s2 ? rzb : rza) - c.z;
+              if (fx * fx + fy * fy + fz * fz != 0.f) continue;  // evaluated in the batch
+              const int64_t tt = s2 ? tb : ta;
+              const double ex = (A.tx[tt] - vx) - rr.x, ey = (A.ty[tt] - vy) - rr.y,
+                           ez = (A.tz[tt] - vz) - rr.z;
+              if (ex == 0.0 && ey == 0.0 && ez == 0.0) {
+                ++nuse;
+                continue;
+              }
+              float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
+              leaf32(c.w, (float)ex, (float)ey, (float)ez, A.eps2, ax, ay, az, ap);
+              if (s2) { PX.y += ax; PY.y += ay; PZ.y += az; PP.y += ap; }
+              else { PX.x += ax; PY.x += ay; PZ.x += az; PP.x += ap; }
+            }
+          }
           Ea0 += (double)PX.x; Ea1 += (double)PY.x; Ea2 += (double)PZ.x; PHa += (double)PP.x;
           Eb0 += (double)PX.y; Eb1 += (double)PY.y; Eb2 += (double)PZ.y; PHb += (double)PP.y;
           c_leaf += (unsigned)n * (v1 ? 2u : 1u) - nuse;
@@ -617,6 +770,7 @@ __global__ void __launch_bounds__(kMixThreads, 5)
         __syncwarp();
         bool isleaf = false, accept = false, open = false, amb = false;
         float cx = 0.f, cy = 0.f, cz = 0.f, bl = 0.f;
+        double bld = 0.0;  // the strict form's FP64 MAC threshold
         double4 a = make_double4(0, 0, 0, 0);
         int nlv = 0, nch = 0;
         int4 c0 = make_int4(0, 0, 0, 0), c1 = c0;
@@ -633,7 +787,14 @@ __global__ void __launch_bounds__(kMixThreads, 5)
           } else {
             bl = A.macb ? (float)A.macb[node] : s_bl2[mu.y & 0xff];
             const float dc = sqrtf(cx * cx + cy * cy + cz * cz);
-            const float dmin = dc - rg, dmax = dc + rg;
+            float dmin = dc - rg, dmax = dc + rg;
+            if constexpr (kStrict) {
+              // conservative: the sphere decides only where the FP64 test of
+              // every target certainly agrees
+              bld = A.macb ? A.macb[node] : s_bl2d[mu.y & 0xff];
+              dmin = dc * (1.0f - 1e-5f) - rg;
+              dmax = dc * (1.0f + 1e-5f) + rg;
+            }
             if (dmin > 0.f && theta2 * (dmin * dmin) > bl) {
               accept = true;
               c_mac += 1;
@@ -649,14 +810,30 @@ __global__ void __launch_bounds__(kMixThreads, 5)
         while (am) {
           const int j = __ffs(am) - 1;
           am &= am - 1;
-          const float ux = __shfl_sync(0xffffffffu, cx, j);
-          const float uy = __shfl_sync(0xffffffffu, cy, j);
-          const float uz = __shfl_sync(0xffffffffu, cz, j);
-          const float ub = __shfl_sync(0xffffffffu, bl, j);
-          float dx = rxa - ux, dy = rya - uy, dz = rza - uz;
-          const bool fa = v0 && !(theta2 * fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > ub);
-          dx = rxb - ux; dy = ryb - uy; dz = rzb - uz;
-          const bool fb = v1 && !(theta2 * fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > ub);
+          bool fa, fb;
+          if constexpr (kStrict) {
+            // mac (coulomb/module_interaction_specific.f90:256-275) in FP64, in
+            // the reference's operation order: theta2 * dist2 > boxlength2
+            const double ux = __shfl_sync(0xffffffffu, a.x, j);
+            const double uy = __shfl_sync(0xffffffffu, a.y, j);
+            const double uz = __shfl_sync(0xffffffffu, a.z, j);
+            const double ub = __shfl_sync(0xffffffffu, bld, j);
+            double dx = sxa - ux, dy = sya - uy, dz = sza - uz;
+            double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+            fa = v0 && !(__dmul_rn(A.theta2d, d2) > ub);
+            dx = sxb - ux; dy = syb - uy; dz = szb - uz;
+            d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+            fb = v1 && !(__dmul_rn(A.theta2d, d2) > ub);
+          } else {
+            const float ux = __shfl_sync(0xffffffffu, cx, j);
+            const float uy = __shfl_sync(0xffffffffu, cy, j);
+            const float uz = __shfl_sync(0xffffffffu, cz, j);
+            const float ub = __shfl_sync(0xffffffffu, bl, j);
+            float dx = rxa - ux, dy = rya - uy, dz = rza - uz;
+            fa = v0 && !(theta2 * fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > ub);
+            dx = rxb - ux; dy = ryb - uy; dz = rzb - uz;
+            fb = v1 && !(theta2 * fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > ub);
+          }
           const unsigned f0 = __ballot_sync(0xffffffffu, fa);
           const unsigned f1 = __ballot_sync(0xffffffffu, fb);
           if (lane == j) {
@@ -677,8 +854,14 @@ __global__ void __launch_bounds__(kMixThreads, 5)
           partner += 1;
         }
         if (accept) {
-          StagedTwig& r = stw[(hT + nT + __popc(ab & lt)) & (kRing - 1)];
-          r.c = make_float4(-cx, -cy, -cz, (float)a.w);
+          TwigRec& r = stw[(hT + nT + __popc(ab & lt)) & (kRing - 1)];
+          if constexpr (kStrict) {
+            r.cx = a.x;
+            r.cy = a.y;
+            r.cz = a.z;
+          } else {
+            r.c = make_float4(-cx, -cy, -cz, (float)a.w);
+          }
           const float4* m = A.mom32 + kMom32Stride * (int64_t)node;
           cp_async16(&r.m0, m);
           cp_async16(&r.m1, m + 1);
@@ -939,6 +1122,7 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
   A.vbox = c->d_vbox;
   A.nbox = c->nboxes;
   A.theta2 = (float)c->prm.theta2;
+  A.theta2d = c->prm.theta2;
   A.eps2 = (float)c->prm.eps2;
   A.M = (int32_t)c->nnodes;
   A.npart = c->n;
@@ -967,9 +1151,12 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
     const int gblocks = 148 * 5;
     const size_t per = (size_t)gblocks * kWW * kStackCap;
     if (!ensure(c, c->wstack, 2 * per, "walk stacks")) return PEPCG_ERR_OOM;
-    if (tiles == nullptr && c->group_size() == 64)
-      k_walk_group64<<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p + slot * per, c->child8.p,
-                                                     c->nchild.p);
+    if (c->prm.precision == PEPCG_PRECISION_MIXED_STRICT)  // 4 blocks per SM
+      k_walk_group64<true><<<148 * 4, kMixThreads, 0, s>>>(A, c->wstack.p + slot * per,
+                                                           c->child8.p, c->nchild.p);
+    else if (tiles == nullptr && c->group_size() == 64)
+      k_walk_group64<false><<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p + slot * per,
+                                                            c->child8.p, c->nchild.p);
     else
       k_walk_group_wide<<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p + slot * per, c->child8.p,
                                                         c->nchild.p);

@@ -33,11 +33,11 @@ def test_grow_allocation_failure_then_recovery(no_injection, after):
         tc.pepc_grow_tree(x, y, z, q)
     assert e.value.code == P.PEPCG_ERR_OOM
     assert "injected" in str(e.value)
+    P.lib().pepcg_debug_fail_allocations(-1)
     # nothing was grown: a traverse is refused, not run on stale data
     with pytest.raises(P.PepcgError) as e2:
         tc.pepc_traverse_tree(x[:10], y[:10], z[:10])
     assert e2.value.code == P.PEPCG_ERR_NO_TREE
-    P.lib().pepcg_debug_fail_allocations(-1)
     g = tc.pepc_grow_tree(x, y, z, q)
     r = tc.pepc_traverse_tree(g.x, g.y, g.z, keys=g.key)
     assert np.array_equal(g.perm, g_ref.perm)

@@ -121,3 +121,42 @@ def test_mixed_group_bmax_mac_matches_plain(gpu):
     _, _, rb = run(x, y, z, q, precision=P.PRECISION_MIXED, theta2=0.36, eps2=1e-6,
                    walk=P.WALK_GROUP)
     assert rm["work"].sum() != rb["work"].sum()
+
+
+@pytest.mark.parametrize("data", ["plummer", "alternating"])
+def test_mixed_strict_equals_fp64_group_lists(gpu, data):
+    # the north star's precision form: FP64 offsets per interaction, Kahan-
+    # compensated FP32 sums, and the FP64 group walk's MAC decisions, so every
+    # target's interaction list (hence work and the counts) is the FP64 walk's
+    if data == "plummer":
+        x, y, z, q = plummer(60000, 43)
+        kw = dict(theta2=0.16, eps2=1e-6, walk=P.WALK_GROUP, group_size=64)
+    else:
+        x, y, z, q = cube(40000, 44)
+        kw = dict(theta2=0.09, eps2=1e-4, walk=P.WALK_GROUP, group_size=64)
+    n = len(x)
+    tp, gp, rp = run(x, y, z, q, precision=P.PRECISION_PLAIN, **kw)
+    ts, gs_, rs = run(x, y, z, q, precision=P.PRECISION_MIXED_STRICT, **kw)
+    tm, gm, rm = run(x, y, z, q, precision=P.PRECISION_MIXED, **kw)
+    assert np.array_equal(rs["work"], rp["work"])
+    sp, ss = tp.stats(), ts.stats()
+    assert ss["twig_interactions"] == sp["twig_interactions"]
+    # the FP64 walk counts each target's own leaf as an interaction, as the
+    # reference does (module_tree_walk_pthreads.f90:617-631); the mixed walks
+    # count only evaluated pairs
+    assert ss["leaf_interactions"] + n == sp["leaf_interactions"]
+    idx = np.arange(0, n, 13)
+    ref = {"ex": rp["ex"][idx], "ey": rp["ey"][idx], "ez": rp["ez"][idx]}
+    ds, dm = relerr(rs, ref, idx), relerr(rm, ref, idx)
+    assert np.median(ds) < 2e-6 and np.percentile(ds, 99) < 1e-4
+    # FP64 offsets and compensated sums are no less accurate than the default form
+    assert np.median(ds) <= 1.05 * np.median(dm) + 1e-9
+    d = tp.direct(idx)
+    assert np.median(relerr(rs, d, idx)) <= 1.05 * np.median(relerr(rp, d, idx)) + 1e-7
+
+
+def test_mixed_strict_only_for_the_64_target_group_walk(gpu):
+    for kw in (dict(walk=P.WALK_PER_TARGET), dict(walk=P.WALK_GROUP, group_size=32)):
+        with pytest.raises(P.PepcgError) as e:
+            P.TreeCode(precision=P.PRECISION_MIXED_STRICT, **kw)
+        assert e.value.code == P.PEPCG_ERR_UNSUPPORTED
