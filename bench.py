@@ -459,6 +459,121 @@ def run_sharded(args, P, torch, dev, stream, dist, rank, world, local, emit=True
             "fields_equal_single_call": same, "gpu_launches": launches}), flush=True)
 
 
+def direct_gradient_torch(torch, x, y, z, q, tx, ty, tz, gphi, eps2, chunk=64):
+    """FP64 direct-sum dL/dq, dL/dx for dL/dphi = gphi at the probes (torch on
+    the GPU, chunked over the probes): the error reference of the adjoint."""
+    dq = torch.zeros_like(q)
+    dx, dy, dz = torch.zeros_like(x), torch.zeros_like(x), torch.zeros_like(x)
+    for s in range(0, tx.numel(), chunk):
+        e = slice(s, s + chunk)
+        rx = tx[e, None] - x[None, :]
+        ry = ty[e, None] - y[None, :]
+        rz = tz[e, None] - z[None, :]
+        rinv = torch.rsqrt(rx * rx + ry * ry + rz * rz + eps2)
+        g = gphi[e, None]
+        dq += (g * rinv).sum(0)
+        w = g * q[None, :] * rinv ** 3
+        dx += (w * rx).sum(0)
+        dy += (w * ry).sum(0)
+        dz += (w * rz).sum(0)
+    return dq, dx, dy, dz
+
+
+def adjoint_measure(P, torch, dev, stream, prec, walk, plummer_xyzq, theta):
+    """The adjoint (pepcg_traverse_adjoint_device) against the forward of the
+    same walk and precision, both timed with CUDA events on the library's
+    stream.
+      configuration: 262,144 sources U[0,1)^3 (seed 4), q ~ N(0,1) (seed 41),
+        4,096 probes U[0.25,0.75]^3 (seed 42), L = sum (phi - phi_t)^2 with
+        phi_t from a second charge set (seed 43), theta 0.4, eps 1e-3; the
+        gradient against the FP64 direct-sum gradient (median over sources of
+        |error| / max |gradient|, dL/dq and dL/dx);
+      4M: the benchmark's particles as targets of themselves, random dL/dphi
+        and dL/dE (the full gradient) and dL/dphi alone."""
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+
+    def ev(fn, reps):
+        ms = []
+        for i in range(reps + 1):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if i >= 1:
+                ms.append(e0.elapsed_time(e1))
+        return statistics.median(ms)
+
+    n, nt = 262144, 4096
+    rng = np.random.default_rng(4)
+    x, y, z = (T(rng.random(n)) for _ in range(3))
+    q = T(np.random.default_rng(41).standard_normal(n))
+    prng = np.random.default_rng(42)
+    tx, ty, tz = (T(0.25 + 0.5 * prng.random(nt)) for _ in range(3))
+    q_t = T(np.random.default_rng(43).standard_normal(n))
+    kw = dict(theta2=0.16, eps2=1e-6, precision=prec, walk=walk)
+    zero = torch.zeros(nt, dtype=torch.float64, device=dev)
+    f = [torch.zeros(nt, dtype=torch.float64, device=dev) for _ in range(5)]
+    tt = P.TreeCode(**kw)
+    tt.set_stream(stream.cuda_stream)
+    tt.grow_tree_device(x, y, z, q_t)
+    tt.traverse_tree_device(tx, ty, tz, *f)
+    phi_t = f[3].clone()
+    tt.close()
+    tc = P.TreeCode(**kw)
+    tc.set_stream(stream.cuda_stream)
+    tc.grow_tree_device(x, y, z, q)
+
+    def fwd():
+        for o in f:
+            o.zero_()
+        tc.traverse_tree_device(tx, ty, tz, *f)
+
+    fwd_ms = ev(fwd, 3)
+    gphi = 2.0 * (f[3] - phi_t)
+    g = [torch.zeros(n, dtype=torch.float64, device=dev) for _ in range(4)]
+    adj_ms = ev(lambda: tc.traverse_adjoint_device(tx, ty, tz, [zero] * 3, gphi, *g), 3)
+    gd = direct_gradient_torch(torch, x, y, z, q, tx, ty, tz, gphi, 1e-6)
+    err = {}
+    for name, a, b in (("q", g[0], gd[0]), ("x", g[1], gd[1])):
+        err[name] = float(((a - b).abs() / b.abs().max()).median().item())
+    tc.close()
+    conf = {"forward_ms": fwd_ms, "adjoint_ms": adj_ms, "ratio": adj_ms / fwd_ms,
+            "grad_err_median": err, "against": "FP64 direct-sum gradient (torch, on the GPU)"}
+
+    # the benchmark's particles as their own targets
+    px, py, pz, pq = (T(a) for a in plummer_xyzq)
+    N = px.numel()
+    tc = P.TreeCode(theta2=theta ** 2, eps2=1e-6, precision=prec, walk=walk)
+    tc.set_stream(stream.cuda_stream)
+    tc.grow_tree_device(px, py, pz, pq)
+    key = torch.empty(N, dtype=torch.int64, device=dev)
+    perm = torch.empty_like(key)
+    kx, ky, kz, kq = (torch.empty(N, dtype=torch.float64, device=dev) for _ in range(4))
+    tc.particles_device(key, perm, kx, ky, kz, kq)
+    F = [torch.zeros(N, dtype=torch.float64, device=dev) for _ in range(5)]
+
+    def fwd4():
+        for o in F:
+            o.zero_()
+        tc.traverse_self_device(*F)
+
+    f4 = ev(fwd4, 2)
+    gen = torch.Generator(device=dev).manual_seed(7)
+    gp4 = torch.randn(N, dtype=torch.float64, device=dev, generator=gen)
+    gE4 = [torch.randn(N, dtype=torch.float64, device=dev, generator=gen) for _ in range(3)]
+    z4 = torch.zeros(N, dtype=torch.float64, device=dev)
+    G = [torch.zeros(N, dtype=torch.float64, device=dev) for _ in range(4)]
+    a_phi = ev(lambda: tc.traverse_adjoint_device(kx, ky, kz, [z4] * 3, gp4, *G), 2)
+    a_full = ev(lambda: tc.traverse_adjoint_device(kx, ky, kz, gE4, gp4, *G), 2)
+    tc.close()
+    return {"configuration": conf,
+            "self_4m": {"forward_ms": f4, "adjoint_phi_ms": a_phi, "adjoint_full_ms": a_full,
+                        "ratio_phi": a_phi / f4, "ratio_full": a_full / f4},
+            "walk": "the timed walk and precision (forward and adjoint alike)"}
+
+
 def workload_name(args):
     return (f"Plummer sphere N={args.n} (a=1, r<=20, q=1/N), theta={args.theta}, "
             f"eps={args.eps}, quadrupole, Hilbert keys, open boundaries")
@@ -479,6 +594,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=32768)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-strict", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--shard", action="store_true",
@@ -696,6 +812,11 @@ def main():
                "api": "pepcg_grow_tree + pepcg_traverse_tree (host arrays, pinned; "
                       "overwrite_results = 1)", "fields_equal_device_path": same}
 
+    # the gradient against the forward of the same walk and precision
+    adjoint = None
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        adjoint = adjoint_measure(P, torch, dev, stream, prec, walk, (x, y, z, q), args.theta)
+
     # with several ranks, the same workload sharded over them (strong scaling)
     sharded = None
     if world > 1:
@@ -732,6 +853,7 @@ def main():
         "clocks": clk, "e2e": e2e, "plain": plain,
         "mixed_over_plain": (value / plain["value"]) if plain else None,
         "strict": strict,
+        "adjoint": adjoint,
         "cpu_baseline": cpu,
         "sharded": sharded,
     }

@@ -184,8 +184,12 @@ int pepcg_traverse_self_device(void* ctx, double* d_ex, double* d_ey, double* d_
  * the grown particles in the caller's ORIGINAL order (overwrites; arrays of
  * length npart).  The interaction lists are recomputed with the context's walk
  * semantics and held fixed (MAC decisions and keys are piecewise constant).
- * FP64.  Open boundaries only: a periodic far field returns
- * PEPCG_ERR_UNSUPPORTED.
+ * The plain walks' adjoints are FP64.  With the mixed GROUP walk and 64-target
+ * buckets (the mixed default) the adjoint runs on that walk's own FP32 lists,
+ * evaluates its terms in FP32 on the group-centred offsets and sums them in
+ * FP64 across buckets, like the forward; the other mixed walks take the FP64
+ * adjoint of their semantics.  Open boundaries only: a periodic far field
+ * returns PEPCG_ERR_UNSUPPORTED.
  */
 int pepcg_traverse_adjoint(void* ctx, int64_t nt, const double* tx, const double* ty,
                            const double* tz, const double* dLdEx, const double* dLdEy,

@@ -1274,8 +1274,9 @@ int orc_lattice(orc_ctx* c, int64_t nt, const double* tx, const double* ty, cons
 }
 
 
-// Adjoint of the per-target walk (module_tree_walk_pthreads.f90 semantics):
-// dL/dq and dL/dx of the grown particles, in the caller's original order.
+// Adjoint of the per-target walk (module_tree_walk_pthreads.f90 semantics), or
+// with walk 2 of the bucket walk (the group walk's lists): dL/dq and dL/dx of
+// the grown particles, in the caller's original order.
 // Open boundaries only (returns -5 with a periodic far field).
 int orc_traverse_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double* ty,
                          const double* tz, const double* gex, const double* gey,
@@ -1286,7 +1287,54 @@ int orc_traverse_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double*
   const int64_t M = (int64_t)c->nodes.size();
   std::vector<Adj> adj(M);
   std::vector<int64_t> todo;
-  for (int64_t i = 0; i < nt; ++i) {
+  if (c->p.walk == 2) {
+    // buckets of tile_size consecutive targets, the simple walk's rule
+    // (module_tree_walk_simple.f90:343-382): a twig is accepted only if
+    // every target of the bucket passes the MAC, else its children are
+    // visited; leaves interact with every target but itself
+    const int64_t ts = std::max(1, std::min(64, c->p.tile_size));
+    for (int64_t b0 = 0; b0 < nt; b0 += ts) {
+      const int64_t np = std::min(ts, nt - b0);
+      for (auto& bx : boxes) {
+        double vb[3];
+        lattice_vect(c->p, bx, vb);
+        todo.clear();
+        todo.push_back(c->root);
+        while (!todo.empty()) {
+          const int64_t ni = todo.back();
+          todo.pop_back();
+          const Node& nd = c->nodes[ni];
+          bool all = true;
+          for (int64_t i = b0; i < b0 + np && nd.descendants != 0; ++i) {
+            const double d[3] = {(tx[i] - vb[0]) - nd.m[M_COCX], (ty[i] - vb[1]) - nd.m[M_COCY],
+                                 (tz[i] - vb[2]) - nd.m[M_COCZ]};
+            const double dist2 = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2];
+            if (!mac_pass(c, nd, dist2)) { all = false; break; }
+          }
+          if (!all) {
+            // children last to first onto the stack, so they are visited first to last
+            std::vector<int64_t> ch;
+            for (int64_t k = nd.first_child; k != kNodeInvalid; k = c->nodes[k].next_sibling)
+              ch.push_back(k);
+            for (auto it = ch.rbegin(); it != ch.rend(); ++it) todo.push_back(*it);
+            continue;
+          }
+          for (int64_t i = b0; i < b0 + np; ++i) {
+            const double gE[3] = {gex[i], gey[i], gez[i]};
+            const double d[3] = {(tx[i] - vb[0]) - nd.m[M_COCX], (ty[i] - vb[1]) - nd.m[M_COCY],
+                                 (tz[i] - vb[2]) - nd.m[M_COCZ]};
+            const double dist2 = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2];
+            if (nd.descendants == 0) {
+              if (dist2 > 0.0) leaf_adjoint(nd.m[M_Q], d, c->p.eps2, gphi[i], gE, adj[ni]);
+            } else {
+              twig_adjoint(nd.m, d, c->p.eps2, gphi[i], gE, adj[ni]);
+            }
+          }
+        }
+      }
+    }
+  }
+  for (int64_t i = 0; i < nt && c->p.walk != 2; ++i) {
     const double gE[3] = {gex[i], gey[i], gez[i]};
     for (auto& bx : boxes) {
       double vb[3];

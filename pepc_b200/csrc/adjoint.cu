@@ -298,8 +298,11 @@ __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_target(AdjArgs A) {
 }
 
 // per-tile / group semantics: the warp's targets share every node; a twig is
-// accepted if all of them pass the MAC (module_tree_walk_simple.f90:343-382)
-template <bool kWithE>
+// accepted if all of them pass the MAC (module_tree_walk_simple.f90:343-382).
+// kTPL targets per lane (2: the 64-target buckets of group_size 64, lane k
+// holding targets t0 + k and t0 + 32 + k, as the FP64 group walk does); a
+// lane's targets add into the same node record before the warp's reduction.
+template <bool kWithE, int kTPL>
 __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_group(AdjArgs A) {
   __shared__ double s_bl2[kMaxLevel + 1];
   __shared__ double s_vb[3 * 125];
@@ -317,13 +320,19 @@ __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_group(AdjArgs A) {
     b = __shfl_sync(0xffffffffu, b, 0);
     if ((int64_t)b >= nbk) break;
     const int2 tl = A.tiles[b];
-    const bool valid = lane < tl.y;
-    const int64_t t = (int64_t)tl.x + lane;
-    double px = 0, py = 0, pz = 0, gp = 0, gE[3] = {0, 0, 0};
-    if (valid) {
-      px = A.tx[t]; py = A.ty[t]; pz = A.tz[t];
-      gp = A.gphi[t];
-      gE[0] = A.gex[t]; gE[1] = A.gey[t]; gE[2] = A.gez[t];
+    bool valid[kTPL];
+    double px[kTPL], py[kTPL], pz[kTPL], gp[kTPL], gE[kTPL][3];
+#pragma unroll
+    for (int s = 0; s < kTPL; ++s) {
+      valid[s] = lane + 32 * s < tl.y;
+      const int64_t t = (int64_t)tl.x + lane + 32 * s;
+      px[s] = py[s] = pz[s] = gp[s] = 0.0;
+      gE[s][0] = gE[s][1] = gE[s][2] = 0.0;
+      if (valid[s]) {
+        px[s] = A.tx[t]; py[s] = A.ty[t]; pz[s] = A.tz[t];
+        gp[s] = A.gphi[t];
+        gE[s][0] = A.gex[t]; gE[s][1] = A.gey[t]; gE[s][2] = A.gez[t];
+      }
     }
     for (int ib = 0; ib < A.nbox; ++ib) {
       const double vx = s_vb[3 * ib], vy = s_vb[3 * ib + 1], vz = s_vb[3 * ib + 2];
@@ -335,21 +344,33 @@ __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_group(AdjArgs A) {
         const double4 nd = A.nc4[u];
         const int2 mu = A.meta[u];
         const int2 fw = A.fwd[u];
-        const double dx = (px - vx) - nd.x, dy = (py - vy) - nd.y, dz = (pz - vz) - nd.z;
-        const double dist2 = (dx * dx + dy * dy) + dz * dz;
+        double dx[kTPL], dy[kTPL], dz[kTPL], dist2[kTPL];
+#pragma unroll
+        for (int s = 0; s < kTPL; ++s) {
+          dx[s] = (px[s] - vx) - nd.x; dy[s] = (py[s] - vy) - nd.y; dz[s] = (pz[s] - vz) - nd.z;
+          dist2[s] = (dx[s] * dx[s] + dy[s] * dy[s]) + dz[s] * dz[s];
+        }
         if (mu.y & kLeafFlag) {
-          if (valid && dist2 > 0.0) leaf_adj(nd.w, dx, dy, dz, A.eps2, gp, gE, a);
+#pragma unroll
+          for (int s = 0; s < kTPL; ++s)
+            if (valid[s] && dist2[s] > 0.0)
+              leaf_adj(nd.w, dx[s], dy[s], dz[s], A.eps2, gp[s], gE[s], a);
           flush_smem(A.adj, u, a, lane, true, sred);
           u = (unsigned)fw.y;
         } else {
-          const bool ok =
-              !valid || (A.theta2 * dist2 > (A.macb ? A.macb[u] : s_bl2[mu.y & 0xff]));
+          const double thr = A.macb ? A.macb[u] : s_bl2[mu.y & 0xff];
+          bool ok = true;
+#pragma unroll
+          for (int s = 0; s < kTPL; ++s) ok = ok && (!valid[s] || (A.theta2 * dist2[s] > thr));
           if (__all_sync(0xffffffffu, ok)) {
-            if (valid) {
+            if (valid[0]) {
               double m[9];
 #pragma unroll
               for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
-              twig_adj<kWithE>(nd.w, m, dx, dy, dz, A.eps2, gp, gE, a);
+#pragma unroll
+              for (int s = 0; s < kTPL; ++s)
+                if (valid[s])
+                  twig_adj<kWithE>(nd.w, m, dx[s], dy[s], dz[s], A.eps2, gp[s], gE[s], a);
             }
             flush_smem(A.adj, u, a, lane, false, sred);
             u = (unsigned)fw.y;
@@ -471,10 +492,11 @@ __global__ void k_any_nonzero(int64_t n, const double* a, const double* b, const
     if (a[i] != 0.0 || b[i] != 0.0 || c[i] != 0.0) atomicOr(flag, 1u);
 }
 
-__global__ void k_buckets32(int64_t nt, int2* tiles) {
-  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b * 32 < nt;
+// the group walk's buckets of bs key-consecutive targets as (first, count)
+__global__ void k_buckets(int64_t nt, int bs, int2* tiles) {
+  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b * bs < nt;
        b += (int64_t)gridDim.x * blockDim.x)
-    tiles[b] = make_int2((int)(b * 32), (int)min((int64_t)32, nt - b * 32));
+    tiles[b] = make_int2((int)(b * bs), (int)min((int64_t)bs, nt - b * bs));
 }
 
 }  // namespace
@@ -496,10 +518,6 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
   }
   if (has_spatial_cutoff(c->prm)) {
     c->err = "the adjoint walk does not apply spatial_interaction_cutoff";
-    return PEPCG_ERR_UNSUPPORTED;
-  }
-  if (c->prm.walk == PEPCG_WALK_GROUP && c->group_size() != 32) {
-    c->err = "the adjoint of the group walk is built for buckets of 32 targets (group_size 32)";
     return PEPCG_ERR_UNSUPPORTED;
   }
   cudaStream_t s = c->stream;
@@ -541,6 +559,10 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
   A.sublist = nullptr;
   A.parent = c->parent.p;
   const bool per_target = (c->prm.walk == PEPCG_WALK_PER_TARGET);
+  // the mixed group walk with 64-target buckets (the benchmark's walk) has
+  // its own adjoint walk, on the forward's FP32 lists (walk_mixed.cu)
+  const bool mixed64 = c->prm.precision != PEPCG_PRECISION_PLAIN &&
+                       c->prm.walk == PEPCG_WALK_GROUP && c->group_size() == 64;
   if (per_target) {
     // split the per-target walk until about 16 warps per SM have work
     const int64_t nb = (nt + 31) / 32;
@@ -555,15 +577,16 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
       base += c->lvl_host[L];
     }
   }
-  if (!per_target) {
+  if (!per_target && !mixed64) {
     // the same tiles as the forward walk of these targets
     if (!ensure(c, c->tiles, 2 * (nt + 32), "tiles")) return PEPCG_ERR_OOM;
     int2* d_tiles = reinterpret_cast<int2*>(c->tiles.p);
     int64_t ntiles = 0;
     if (c->prm.walk == PEPCG_WALK_GROUP) {
-      ntiles = (nt + 31) / 32;
+      const int bs = c->group_size();
+      ntiles = (nt + bs - 1) / bs;
       COUNT_LAUNCH();
-      k_buckets32<<<148, 256, 0, s>>>(nt, d_tiles);
+      k_buckets<<<148, 256, 0, s>>>(nt, bs, d_tiles);
     } else {
       const int T = c->prm.tile_size;
       int rc = host_tiles(c, nt, nullptr, T, d_tiles, &ntiles);
@@ -577,14 +600,22 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
     return PEPCG_ERR_CUDA;
   COUNT_LAUNCH();
   k_reset_adj<<<1, 1, 0, s>>>(A.queue, A.item_queue);
-  COUNT_LAUNCH();
   const int blocks = 148 * 8;
-  if (per_target) {
+  if (mixed64) {
+    int rc = launch_adjoint_group64(c, nt, tx, ty, tz, gex, gey, gez, gphi, h_flag != 0, s);
+    if (rc) return rc;
+  } else if (per_target) {
+    COUNT_LAUNCH();
     if (h_flag) k_adj_target<true><<<blocks, kAdjThreads, 0, s>>>(A);
     else k_adj_target<false><<<blocks, kAdjThreads, 0, s>>>(A);
+  } else if (c->prm.walk == PEPCG_WALK_GROUP && c->group_size() == 64) {
+    COUNT_LAUNCH();
+    if (h_flag) k_adj_group<true, 2><<<blocks, kAdjThreads, 0, s>>>(A);
+    else k_adj_group<false, 2><<<blocks, kAdjThreads, 0, s>>>(A);
   } else {
-    if (h_flag) k_adj_group<true><<<blocks, kAdjThreads, 0, s>>>(A);
-    else k_adj_group<false><<<blocks, kAdjThreads, 0, s>>>(A);
+    COUNT_LAUNCH();
+    if (h_flag) k_adj_group<true, 1><<<blocks, kAdjThreads, 0, s>>>(A);
+    else k_adj_group<false, 1><<<blocks, kAdjThreads, 0, s>>>(A);
   }
   const unsigned g = (unsigned)((M + 255) / 256 > 148 * 16 ? 148 * 16 : (M + 255) / 256);
   for (int L = 0; L < c->max_level; ++L) {

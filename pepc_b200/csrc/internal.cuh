@@ -286,6 +286,11 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
                     double* pot, double* work, const double* tq = nullptr,
                     const ChunkPlan* plan = nullptr);
 
+// walk_mixed.cu: the transposed adjoint walk of the mixed 64-target group walk
+int launch_adjoint_group64(Ctx* c, int64_t nt, const double* tx, const double* ty,
+                           const double* tz, const double* gex, const double* gey,
+                           const double* gez, const double* gphi, bool with_e, cudaStream_t s);
+
 // ---- adjoint.cu ----
 int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                    const double* gex, const double* gey, const double* gez, const double* gphi,

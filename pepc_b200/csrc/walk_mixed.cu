@@ -1098,6 +1098,488 @@ __global__ void __launch_bounds__(kMixThreads) k_walk_target_mixed(MixArgs A) {
   warp_add3(A.counters, c_leaf, c_twig, c_mac);
 }
 
+// ---------------------------------------------------------------------------
+// Adjoint of the mixed group walk with 64-target buckets.  The traversal, the
+// FP32 group-centred MAC and the staging are k_walk_group64's, so each
+// bucket's interaction list is the forward list.  The staged batches are
+// evaluated transposed: lane j takes node record j of the batch and loops over
+// the bucket's 64 targets, whose group-centred FP32 offsets and gradients are
+// broadcast from shared memory two at a time (one packed FP32 operation per
+// target pair).  A lane thus sums its node's adjoint record over the bucket
+// without any cross-lane reduction, in FP32 as the forward sums its batches,
+// and adds it to the node's FP64 record with one atomic per value.  The terms
+// are the transposes of the forward's (the FP64 forms and their derivation
+// are in adjoint.cu, twig_adj / leaf_adj), rewritten with T = 3M, v = T d and
+// dTd = d.v: with s1 = gphi R1 and s3 = 3 gphi R2,
+//   qbar   += gphi R0                      (+ (g.d) R1)
+//   pbar   -= s1 d                         (+ R1 g - 3 (g.d) R2 d)
+//   Qbar_kl += s3 d_k d_l - delta_kl s1    (+ 15 (g.d) R3 d_k d_l - 3 R2 (g_k d_l + g_l d_k + delta_kl g.d))
+//   cocbar += gphi [ce d + R1 p - 2 R2 v]  (+ the Hessian terms of twig_adj)
+// with ce = q R1 - 3 R2 (p.d + tr) + 5 R3 dTd; sums over the targets of a
+// node-constant factor (the p terms, the delta terms) are taken once per batch.
+// ---------------------------------------------------------------------------
+struct AdjMixArgs {
+  int64_t nt;
+  const double *tx, *ty, *tz;
+  const double *gex, *gey, *gez, *gphi;
+  const double4* nc4;
+  const int2* meta;
+  const float4* mom32;
+  const int32_t* nleaves;
+  const double* bl2;
+  const double* macb;
+  const double* vbox;
+  int nbox;
+  float theta2, eps2;
+  int64_t npart;
+  double* adj;  // 16 doubles per node: q, p(3), Q(6: xx yy zz xy yz zx), coc(3), abs_charge, pad
+  unsigned long long* counters;
+  uint32_t* status;
+  unsigned int* queue;
+};
+
+constexpr int kNAdj = 16;
+
+struct __align__(16) StagedLeafA {
+  float4 c;        // (x - g) rounded from FP64, charge
+  double x, y, z;  // FP64 position, for the exact self test
+  int node;
+  int pad;
+};
+
+__device__ __forceinline__ void adj_add(double* __restrict__ a, float2 v) {
+  const double s = (double)v.x + (double)v.y;
+  if (s != 0.0) atomicAdd(a, s);
+}
+
+// Four resident blocks per SM (128 registers, the twig terms' pair
+// accumulators and node constants stay in registers): at 4M the full
+// gradient takes 88 ms against 111 ms at five blocks (96 registers, spills).
+template <bool kWithE>
+__global__ void __launch_bounds__(kMixThreads, 4)
+    k_adj_group64(AdjMixArgs A, int* __restrict__ gstack, const int4* __restrict__ child8,
+                  const int* __restrict__ nchild) {
+  __shared__ float s_bl2[kMaxLevel + 1];
+  __shared__ double s_vb[3 * 125];
+  __shared__ StagedTwig s_tw[kWW][kRing];
+  __shared__ StagedLeafA s_lf[kWW][kRing];
+  // per warp and target pair p (targets t0 + p, t0 + 32 + p): (rx, rx', ry, ry'),
+  // (rz, rz', gphi, gphi'), (gx, gx', gy, gy'), (gz, gz', -, -)
+  __shared__ float4 s_tg[kWW][32][kWithE ? 4 : 2];
+  for (int i = threadIdx.x; i <= kMaxLevel; i += blockDim.x) s_bl2[i] = (float)A.bl2[i];
+  for (int i = threadIdx.x; i < 3 * A.nbox; i += blockDim.x) s_vb[i] = A.vbox[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  int* stack = gstack + (int64_t)(blockIdx.x * kWW + w) * kStackCap;
+  StagedTwig* stw = s_tw[w];
+  StagedLeafA* stl = s_lf[w];
+  float4(*tg)[kWithE ? 4 : 2] = s_tg[w];
+  const float theta2 = A.theta2;
+  const float2 E2 = f2(A.eps2);
+  const int64_t nbuckets = (A.nt + 63) / 64;
+  unsigned long long c_leaf = 0, c_twig = 0, c_mac = 0;
+  for (;;) {
+    unsigned b = 0;
+    if (lane == 0) b = atomicAdd(A.queue, 1u);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    if ((int64_t)b >= nbuckets) break;
+    const int64_t t0 = (int64_t)b * 64;
+    const int cnt = (int)min((int64_t)64, A.nt - t0);
+    const bool v0 = lane < cnt, v1 = lane + 32 < cnt;
+    const unsigned vm0 = __ballot_sync(0xffffffffu, v0), vm1 = __ballot_sync(0xffffffffu, v1);
+    const int nvalid = __popc(vm0) + __popc(vm1);
+    const int64_t ta = t0 + lane, tb = t0 + 32 + lane;
+    double pxa = 0, pya = 0, pza = 0, pxb = 0, pyb = 0, pzb = 0;
+    float gpa = 0.f, gpb = 0.f, gxa = 0.f, gya = 0.f, gza = 0.f, gxb = 0.f, gyb = 0.f, gzb = 0.f;
+    if (v0) {
+      pxa = A.tx[ta]; pya = A.ty[ta]; pza = A.tz[ta];
+      gpa = (float)A.gphi[ta];
+      if (kWithE) { gxa = (float)A.gex[ta]; gya = (float)A.gey[ta]; gza = (float)A.gez[ta]; }
+    }
+    if (v1) {
+      pxb = A.tx[tb]; pyb = A.ty[tb]; pzb = A.tz[tb];
+      gpb = (float)A.gphi[tb];
+      if (kWithE) { gxb = (float)A.gex[tb]; gyb = (float)A.gey[tb]; gzb = (float)A.gez[tb]; }
+    }
+    double lo[3] = {v0 ? pxa : INFINITY, v0 ? pya : INFINITY, v0 ? pza : INFINITY};
+    double hi[3] = {v0 ? pxa : -INFINITY, v0 ? pya : -INFINITY, v0 ? pza : -INFINITY};
+    if (v1) {
+      lo[0] = fmin(lo[0], pxb); lo[1] = fmin(lo[1], pyb); lo[2] = fmin(lo[2], pzb);
+      hi[0] = fmax(hi[0], pxb); hi[1] = fmax(hi[1], pyb); hi[2] = fmax(hi[2], pzb);
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      for (int o = 16; o > 0; o >>= 1) {
+        lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+        hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+      }
+    const double g0x = 0.5 * (lo[0] + hi[0]), g0y = 0.5 * (lo[1] + hi[1]), g0z = 0.5 * (lo[2] + hi[2]);
+    const float rxa = (float)(pxa - g0x), rya = (float)(pya - g0y), rza = (float)(pza - g0z);
+    const float rxb = (float)(pxb - g0x), ryb = (float)(pyb - g0y), rzb = (float)(pzb - g0z);
+    float rg = fmaxf(v0 ? sqrtf(rxa * rxa + rya * rya + rza * rza) : 0.f,
+                     v1 ? sqrtf(rxb * rxb + ryb * ryb + rzb * rzb) : 0.f);
+    for (int o = 16; o > 0; o >>= 1) rg = fmaxf(rg, __shfl_xor_sync(0xffffffffu, rg, o));
+    rg = rg * 1.0001f + 1e-30f;  // the sphere must contain every target after rounding
+    // an absent target sits far away with zero gradients: it adds exact zeros
+    tg[lane][0] = make_float4(v0 ? rxa : 1e10f, v1 ? rxb : 1e10f, v0 ? rya : 1e10f, v1 ? ryb : 1e10f);
+    tg[lane][1] = make_float4(v0 ? rza : 1e10f, v1 ? rzb : 1e10f, gpa, gpb);
+    if constexpr (kWithE) {
+      tg[lane][2] = make_float4(gxa, gxb, gya, gyb);
+      tg[lane][3] = make_float4(gza, gzb, 0.f, 0.f);
+    }
+    __syncwarp();
+    bool complete = true;
+    for (int ib = 0; ib < A.nbox; ++ib) {
+      const double vx = s_vb[3 * ib], vy = s_vb[3 * ib + 1], vz = s_vb[3 * ib + 2];
+      const double gx = g0x - vx, gy = g0y - vy, gz = g0z - vz;
+      int64_t partner = 0;
+      int nT = 0, hT = 0, nL = 0, hL = 0;
+      int top = 1;
+      if (lane == 0) stack[0] = 0;
+      __syncwarp();
+      // twig records: lane j sums node j's record over the bucket's targets
+      auto flush_twigs = [&](int n) {
+        cp_async_wait_all();
+        __syncwarp();
+        if (lane < n) {
+          const StagedTwig& r = stw[(hT + lane) & (kRing - 1)];
+          const float4 c = r.c, m0 = r.m0, m1 = r.m1, m2 = r.m2;
+          const int node = __float_as_int(c.w);
+          const float2 CX = f2(c.x), CY = f2(c.y), CZ = f2(c.z);  // d = r_t + c
+          const float2 PX = f2(m0.x), PY = f2(m0.y), PZ = f2(m0.z);
+          const float2 Txx = f2(m0.w), Tyy = f2(m1.x), Tzz = f2(m1.y), Txy = f2(m1.z),
+                       Tyz = f2(m1.w), Tzx = f2(m2.x), TR = f2(m2.y), Q = f2(m2.z);
+          float2 aq = f2(0.f), apx = f2(0.f), apy = f2(0.f), apz = f2(0.f), aS = f2(0.f);
+          float2 axx = f2(0.f), ayy = f2(0.f), azz = f2(0.f), axy = f2(0.f), ayz = f2(0.f),
+                 azx = f2(0.f), acx = f2(0.f), acy = f2(0.f), acz = f2(0.f);
+          float2 aGx = f2(0.f), aGy = f2(0.f), aGz = f2(0.f);  // sum of 2 R2 g (with E)
+#pragma unroll 2
+          for (int p = 0; p < 32; ++p) {
+            const float4 ta4 = tg[p][0], tb4 = tg[p][1];
+            const float2 dx = __fadd2_rn(make_float2(ta4.x, ta4.y), CX);
+            const float2 dy = __fadd2_rn(make_float2(ta4.z, ta4.w), CY);
+            const float2 dz = __fadd2_rn(make_float2(tb4.x, tb4.y), CZ);
+            const float2 gp = make_float2(tb4.z, tb4.w);
+            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, E2)));
+            const float2 R0 = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+            const float2 i2 = __fmul2_rn(R0, R0);
+            const float2 R1 = __fmul2_rn(R0, i2);
+            const float2 R2 = __fmul2_rn(R1, i2);
+            const float2 R3 = __fmul2_rn(R2, i2);
+            const float2 vx = __ffma2_rn(Txx, dx, __ffma2_rn(Txy, dy, __fmul2_rn(Tzx, dz)));
+            const float2 vy = __ffma2_rn(Txy, dx, __ffma2_rn(Tyy, dy, __fmul2_rn(Tyz, dz)));
+            const float2 vz = __ffma2_rn(Tzx, dx, __ffma2_rn(Tyz, dy, __fmul2_rn(Tzz, dz)));
+            const float2 dTd = __ffma2_rn(dx, vx, __ffma2_rn(dy, vy, __fmul2_rn(dz, vz)));
+            const float2 u = __ffma2_rn(PX, dx, __ffma2_rn(PY, dy, __ffma2_rn(PZ, dz, TR)));
+            const float2 m3R2 = __fmul2_rn(f2(-3.f), R2);
+            const float2 ce = __ffma2_rn(Q, R1, __ffma2_rn(m3R2, u, __fmul2_rn(__fmul2_rn(f2(5.f), R3), dTd)));
+            const float2 s1 = __fmul2_rn(gp, R1);
+            float2 s3 = __fmul2_rn(gp, __fmul2_rn(f2(3.f), R2));
+            aq = __ffma2_rn(gp, R0, aq);
+            aS = __fadd2_rn(aS, s1);
+            float2 kd = __fmul2_rn(gp, ce);                        // coefficient of d in cocbar
+            float2 kv = __fmul2_rn(f2(-2.f / 3.f), s3);            // of v
+            float2 ex_ = f2(0.f), ey_ = f2(0.f), ez_ = f2(0.f);     // -3 R2 g
+            float2 ppx = s1, ppy = s1, ppz = s1;                    // coefficient of -d in pbar
+            if constexpr (kWithE) {
+              const float4 tc4 = tg[p][2], td4 = tg[p][3];
+              const float2 gxx = make_float2(tc4.x, tc4.y), gyy = make_float2(tc4.z, tc4.w),
+                           gzz = make_float2(td4.x, td4.y);
+              const float2 R4 = __fmul2_rn(R3, i2);
+              const float2 ga = __ffma2_rn(gxx, dx, __ffma2_rn(gyy, dy, __fmul2_rn(gzz, dz)));
+              aq = __ffma2_rn(ga, R1, aq);
+              // pbar += R1 g - 3 ga R2 d, kept as -pbar
+              const float2 h = __fmul2_rn(ga, __fmul2_rn(f2(3.f), R2));  // 3 ga R2
+              const float2 nR1 = __fmul2_rn(f2(-1.f), R1);
+              apx = __ffma2_rn(nR1, gxx, apx);
+              apy = __ffma2_rn(nR1, gyy, apy);
+              apz = __ffma2_rn(nR1, gzz, apz);
+              ppx = __fadd2_rn(s1, h); ppy = ppx; ppz = ppx;
+              // Qbar: 15 ga R3 d d - 3 R2 (g d + d g + ga I)
+              s3 = __ffma2_rn(__fmul2_rn(f2(15.f), ga), R3, s3);
+              ex_ = __fmul2_rn(m3R2, gxx);
+              ey_ = __fmul2_rn(m3R2, gyy);
+              ez_ = __fmul2_rn(m3R2, gzz);
+              aS = __fadd2_rn(aS, h);  // the delta_kl and the p terms share 3 ga R2
+              // cocbar: cd d + cg g + 3 R2 ga p - 10 R3 ga v + 2 R2 T g, cg = -ce,
+              // cd = ga (3 q R2 - 15 R3 u + 35 R4 dTd) + 3 R2 (g.p) - 10 R3 (g.v);
+              // T g is node-constant: the batch sums 2 R2 g (aG) and applies T once
+              const float2 gP = __ffma2_rn(gxx, PX, __ffma2_rn(gyy, PY, __fmul2_rn(gzz, PZ)));
+              const float2 gv = __ffma2_rn(gxx, vx, __ffma2_rn(gyy, vy, __fmul2_rn(gzz, vz)));
+              const float2 nR3x10 = __fmul2_rn(f2(-10.f), R3);
+              const float2 inner = __ffma2_rn(__fmul2_rn(f2(3.f), Q), R2,
+                                   __ffma2_rn(__fmul2_rn(f2(-15.f), R3), u, __fmul2_rn(__fmul2_rn(f2(35.f), R4), dTd)));
+              const float2 cd = __ffma2_rn(ga, inner, __ffma2_rn(__fmul2_rn(f2(3.f), R2), gP, __fmul2_rn(nR3x10, gv)));
+              kd = __fadd2_rn(kd, cd);
+              kv = __ffma2_rn(nR3x10, ga, kv);
+              const float2 R2x2 = __fmul2_rn(f2(2.f), R2);
+              aGx = __ffma2_rn(R2x2, gxx, aGx);
+              aGy = __ffma2_rn(R2x2, gyy, aGy);
+              aGz = __ffma2_rn(R2x2, gzz, aGz);
+              const float2 nce = __fmul2_rn(f2(-1.f), ce);
+              acx = __ffma2_rn(nce, gxx, acx);
+              acy = __ffma2_rn(nce, gyy, acy);
+              acz = __ffma2_rn(nce, gzz, acz);
+            }
+            apx = __ffma2_rn(ppx, dx, apx);
+            apy = __ffma2_rn(ppy, dy, apy);
+            apz = __ffma2_rn(ppz, dz, apz);
+            // Qbar's d d terms and (with E) the g d terms:
+            //   kl += (s3 d_k + e_k) d_l + e_l d_k,  e = -3 R2 g
+            const float2 wx = __ffma2_rn(s3, dx, ex_), wy = __ffma2_rn(s3, dy, ey_),
+                         wz = __ffma2_rn(s3, dz, ez_);
+            axx = __ffma2_rn(__fadd2_rn(wx, ex_), dx, axx);
+            ayy = __ffma2_rn(__fadd2_rn(wy, ey_), dy, ayy);
+            azz = __ffma2_rn(__fadd2_rn(wz, ez_), dz, azz);
+            axy = __ffma2_rn(wx, dy, __ffma2_rn(ey_, dx, axy));
+            ayz = __ffma2_rn(wy, dz, __ffma2_rn(ez_, dy, ayz));
+            azx = __ffma2_rn(wz, dx, __ffma2_rn(ex_, dz, azx));
+            acx = __ffma2_rn(kd, dx, __ffma2_rn(kv, vx, acx));
+            acy = __ffma2_rn(kd, dy, __ffma2_rn(kv, vy, acy));
+            acz = __ffma2_rn(kd, dz, __ffma2_rn(kv, vz, acz));
+          }
+          double* a = A.adj + (int64_t)kNAdj * node;
+          // the node-constant factors: the delta_kl terms and R1 p (with E also 3 R2 ga p)
+          const double S = (double)aS.x + (double)aS.y;
+          adj_add(a + 0, aq);
+          adj_add(a + 1, make_float2(-apx.x, -apx.y));
+          adj_add(a + 2, make_float2(-apy.x, -apy.y));
+          adj_add(a + 3, make_float2(-apz.x, -apz.y));
+          if (S != 0.0) {
+            atomicAdd(a + 4, (double)axx.x + (double)axx.y - S);
+            atomicAdd(a + 5, (double)ayy.x + (double)ayy.y - S);
+            atomicAdd(a + 6, (double)azz.x + (double)azz.y - S);
+          } else {
+            adj_add(a + 4, axx);
+            adj_add(a + 5, ayy);
+            adj_add(a + 6, azz);
+          }
+          adj_add(a + 7, axy);
+          adj_add(a + 8, ayz);
+          adj_add(a + 9, azx);
+          double cx = (double)acx.x + (double)acx.y + S * (double)m0.x;
+          double cy = (double)acy.x + (double)acy.y + S * (double)m0.y;
+          double cz = (double)acz.x + (double)acz.y + S * (double)m0.z;
+          if constexpr (kWithE) {
+            // + T (sum of 2 R2 g)
+            const double Gx = (double)aGx.x + (double)aGx.y, Gy = (double)aGy.x + (double)aGy.y,
+                         Gz = (double)aGz.x + (double)aGz.y;
+            cx += (double)m0.w * Gx + (double)m1.z * Gy + (double)m2.x * Gz;
+            cy += (double)m1.z * Gx + (double)m1.x * Gy + (double)m1.w * Gz;
+            cz += (double)m2.x * Gx + (double)m1.w * Gy + (double)m1.y * Gz;
+          }
+          if (cx != 0.0) atomicAdd(a + 10, cx);
+          if (cy != 0.0) atomicAdd(a + 11, cy);
+          if (cz != 0.0) atomicAdd(a + 12, cz);
+        }
+        c_twig += (unsigned)n * (unsigned)nvalid;
+        hT = (hT + n) & (kRing - 1);
+        nT -= n;
+        __syncwarp();
+      };
+      // leaf records: qbar += gphi R0 (+ g.d R1), cocbar += q [(gphi R1 (+ 3 g.d R2)) d (- R1 g)]
+      auto flush_leaves = [&](int n) {
+        __syncwarp();
+        if (lane < n) {
+          const StagedLeafA& r = stl[(hL + lane) & (kRing - 1)];
+          const float4 c = r.c;
+          const float2 NCX = f2(-c.x), NCY = f2(-c.y), NCZ = f2(-c.z);  // d = r_t - c
+          float2 aq = f2(0.f), acx = f2(0.f), acy = f2(0.f), acz = f2(0.f);
+          unsigned long long pend = 0ull;  // targets at a zero FP32 offset (bit 2p + half)
+#pragma unroll 2
+          for (int p = 0; p < 32; ++p) {
+            const float4 ta4 = tg[p][0], tb4 = tg[p][1];
+            const float2 dx = __fadd2_rn(make_float2(ta4.x, ta4.y), NCX);
+            const float2 dy = __fadd2_rn(make_float2(ta4.z, ta4.w), NCY);
+            const float2 dz = __fadd2_rn(make_float2(tb4.x, tb4.y), NCZ);
+            const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+            const bool za = d2.x == 0.f, zb = d2.y == 0.f;
+            pend |= (za ? 1ull << (2 * p) : 0ull) | (zb ? 2ull << (2 * p) : 0ull);
+            const float2 gp = make_float2(za ? 0.f : tb4.z, zb ? 0.f : tb4.w);
+            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, E2)));
+            const float2 R0 = make_float2(r2.x > 0.f ? rsqrt_ftz(r2.x) : 0.f,
+                                          r2.y > 0.f ? rsqrt_ftz(r2.y) : 0.f);
+            const float2 R1 = __fmul2_rn(R0, __fmul2_rn(R0, R0));
+            aq = __ffma2_rn(gp, R0, aq);
+            float2 k = __fmul2_rn(gp, R1);
+            if constexpr (kWithE) {
+              const float4 tc4 = tg[p][2], td4 = tg[p][3];
+              const float2 gxx = make_float2(za ? 0.f : tc4.x, zb ? 0.f : tc4.y);
+              const float2 gyy = make_float2(za ? 0.f : tc4.z, zb ? 0.f : tc4.w);
+              const float2 gzz = make_float2(za ? 0.f : td4.x, zb ? 0.f : td4.y);
+              const float2 ga = __ffma2_rn(gxx, dx, __ffma2_rn(gyy, dy, __fmul2_rn(gzz, dz)));
+              const float2 R2 = __fmul2_rn(R1, __fmul2_rn(R0, R0));
+              aq = __ffma2_rn(ga, R1, aq);
+              k = __ffma2_rn(__fmul2_rn(f2(3.f), ga), R2, k);
+              const float2 nR1 = __fmul2_rn(f2(-1.f), R1);
+              acx = __ffma2_rn(nR1, gxx, acx);
+              acy = __ffma2_rn(nR1, gyy, acy);
+              acz = __ffma2_rn(nR1, gzz, acz);
+            }
+            acx = __ffma2_rn(k, dx, acx);
+            acy = __ffma2_rn(k, dy, acy);
+            acz = __ffma2_rn(k, dz, acz);
+          }
+          // zero FP32 offsets: the target's own leaf (no interaction, FP64
+          // dist2 == 0) or a point closer than FP32 resolves at the group
+          // scale, evaluated on the FP64 offset rounded once
+          float sq = 0.f, scx = 0.f, scy = 0.f, scz = 0.f;
+          while (pend) {
+            const int bit = __ffsll((long long)pend) - 1;
+            pend &= pend - 1;
+            const int64_t t = t0 + (bit >> 1) + 32 * (bit & 1);
+            const double ex = (A.tx[t] - vx) - r.x, ey = (A.ty[t] - vy) - r.y,
+                         ez = (A.tz[t] - vz) - r.z;
+            if (ex == 0.0 && ey == 0.0 && ez == 0.0) continue;
+            const float dx = (float)ex, dy = (float)ey, dz = (float)ez;
+            const float gp = (float)A.gphi[t];
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, A.eps2)));
+            const float R0 = rsqrt_ftz(r2), R1 = R0 * R0 * R0;
+            sq = fmaf(gp, R0, sq);
+            float k = gp * R1;
+            if constexpr (kWithE) {
+              const float gx = (float)A.gex[t], gy = (float)A.gey[t], gz = (float)A.gez[t];
+              const float ga = fmaf(gx, dx, fmaf(gy, dy, gz * dz));
+              sq = fmaf(ga, R1, sq);
+              k = fmaf(3.f * ga, R1 * R0 * R0, k);
+              scx = fmaf(-R1, gx, scx);
+              scy = fmaf(-R1, gy, scy);
+              scz = fmaf(-R1, gz, scz);
+            }
+            scx = fmaf(k, dx, scx);
+            scy = fmaf(k, dy, scy);
+            scz = fmaf(k, dz, scz);
+          }
+          double* a = A.adj + (int64_t)kNAdj * r.node;
+          const double q = (double)c.w;
+          const double vq = (double)aq.x + (double)aq.y + (double)sq;
+          if (vq != 0.0) atomicAdd(a + 0, vq);
+          const double cx = q * ((double)acx.x + (double)acx.y + (double)scx);
+          const double cy = q * ((double)acy.x + (double)acy.y + (double)scy);
+          const double cz = q * ((double)acz.x + (double)acz.y + (double)scz);
+          if (cx != 0.0) atomicAdd(a + 10, cx);
+          if (cy != 0.0) atomicAdd(a + 11, cy);
+          if (cz != 0.0) atomicAdd(a + 12, cz);
+        }
+        c_leaf += (unsigned)n * (unsigned)nvalid;
+        hL = (hL + n) & (kRing - 1);
+        nL -= n;
+        __syncwarp();
+      };
+      // the traversal and MAC of k_walk_group64 (same decisions, same lists)
+      while (top > 0) {
+        const int take = top < 32 ? top : 32;
+        top -= take;
+        const int node = lane < take ? stack[top + lane] : -1;
+        __syncwarp();
+        bool isleaf = false, accept = false, open = false, amb = false;
+        float cx = 0.f, cy = 0.f, cz = 0.f, bl = 0.f;
+        double4 a = make_double4(0, 0, 0, 0);
+        int nlv = 0, nch = 0;
+        int4 c0 = make_int4(0, 0, 0, 0), c1 = c0;
+        if (node >= 0) {
+          a = A.nc4[node];
+          const int2 mu = A.meta[node];
+          nlv = A.nleaves[node];
+          nch = nchild[node];
+          c0 = child8[2 * (int64_t)node];
+          c1 = child8[2 * (int64_t)node + 1];
+          cx = (float)(a.x - gx); cy = (float)(a.y - gy); cz = (float)(a.z - gz);
+          if (mu.y & kLeafFlag) {
+            isleaf = true;
+          } else {
+            bl = A.macb ? (float)A.macb[node] : s_bl2[mu.y & 0xff];
+            const float dc = sqrtf(cx * cx + cy * cy + cz * cz);
+            const float dmin = dc - rg, dmax = dc + rg;
+            if (dmin > 0.f && theta2 * (dmin * dmin) > bl) {
+              accept = true;
+              c_mac += 1;
+            } else if (!(theta2 * (dmax * dmax) > bl)) {
+              open = true;
+              c_mac += 1;
+            } else {
+              amb = true;
+            }
+          }
+        }
+        unsigned am = __ballot_sync(0xffffffffu, amb);
+        while (am) {
+          const int j = __ffs(am) - 1;
+          am &= am - 1;
+          const float ux = __shfl_sync(0xffffffffu, cx, j);
+          const float uy = __shfl_sync(0xffffffffu, cy, j);
+          const float uz = __shfl_sync(0xffffffffu, cz, j);
+          const float ub = __shfl_sync(0xffffffffu, bl, j);
+          float dx = rxa - ux, dy = rya - uy, dz = rza - uz;
+          const bool fa = v0 && !(theta2 * fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > ub);
+          dx = rxb - ux; dy = ryb - uy; dz = rzb - uz;
+          const bool fb = v1 && !(theta2 * fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > ub);
+          const unsigned f0 = __ballot_sync(0xffffffffu, fa);
+          const unsigned f1 = __ballot_sync(0xffffffffu, fb);
+          if (lane == j) {
+            accept = (f0 | f1) == 0;
+            open = !accept;
+            c_mac += (unsigned)(f0 ? __popc(vm0 & ((2u << (__ffs(f0) - 1)) - 1u))
+                                   : __popc(vm0) + (f1 ? __popc(vm1 & ((2u << (__ffs(f1) - 1)) - 1u))
+                                                       : __popc(vm1)));
+          }
+        }
+        const unsigned lb = __ballot_sync(0xffffffffu, isleaf);
+        const unsigned ab = __ballot_sync(0xffffffffu, accept);
+        if (isleaf) {
+          StagedLeafA& r = stl[(hL + nL + __popc(lb & lt)) & (kRing - 1)];
+          r.c = make_float4(cx, cy, cz, (float)a.w);
+          r.x = a.x; r.y = a.y; r.z = a.z;
+          r.node = node;
+          partner += 1;
+        }
+        if (accept) {
+          StagedTwig& r = stw[(hT + nT + __popc(ab & lt)) & (kRing - 1)];
+          r.c = make_float4(-cx, -cy, -cz, __int_as_float(node));
+          const float4* m = A.mom32 + kMom32Stride * (int64_t)node;
+          cp_async16(&r.m0, m);
+          cp_async16(&r.m1, m + 1);
+          cp_async16(&r.m2, m + 2);
+          partner += nlv;
+        }
+        nL += __popc(lb);
+        nT += __popc(ab);
+        const int npush = open ? min(8, nch) : 0;
+        int total;
+        const int off = warp_excl_scan(npush, lane, total);
+        if (top + total > kStackCap) {
+          complete = false;
+          break;
+        }
+        if (npush > 0) {
+          int* dst = stack + top + off;
+          dst[0] = c0.x;
+          if (npush > 1) dst[1] = c0.y;
+          if (npush > 2) dst[2] = c0.z;
+          if (npush > 3) dst[3] = c0.w;
+          if (npush > 4) dst[4] = c1.x;
+          if (npush > 5) dst[5] = c1.y;
+          if (npush > 6) dst[6] = c1.z;
+          if (npush > 7) dst[7] = c1.w;
+        }
+        top += total;
+        __syncwarp();
+        if (nT >= 32) flush_twigs(32);
+        if (nL >= 32) flush_leaves(32);
+      }
+      if (nT > 0) flush_twigs(nT);
+      if (nL > 0) flush_leaves(nL);
+      for (int o = 16; o > 0; o >>= 1) partner += __shfl_xor_sync(0xffffffffu, partner, o);
+      if (partner != A.npart) complete = false;
+    }
+    __syncwarp();
+    if (__any_sync(0xffffffffu, !complete) && lane == 0) atomicOr(A.status, ST_INCOMPLETE);
+  }
+  cp_async_wait_all();
+  warp_add3(A.counters, c_leaf, c_twig, c_mac);
+}
+
 __global__ void k_reset_mixed(unsigned int* q) { *q = 0; }
 
 }  // namespace
@@ -1162,6 +1644,47 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
                                                         c->nchild.p);
   }
   return cuda_ok(c, cudaGetLastError(), "mixed walk launch") ? PEPCG_OK : PEPCG_ERR_CUDA;
+}
+
+// The adjoint walk of the mixed group walk with 64-target buckets: fills the
+// twigs' and leaves' adjoint records (adj, 16 doubles per node, zeroed by the
+// caller); the downward pass and the output are adjoint.cu's.
+int launch_adjoint_group64(Ctx* c, int64_t nt, const double* tx, const double* ty,
+                           const double* tz, const double* gex, const double* gey,
+                           const double* gez, const double* gphi, bool with_e, cudaStream_t s) {
+  AdjMixArgs A;
+  A.nt = nt;
+  A.tx = tx; A.ty = ty; A.tz = tz;
+  A.gex = gex; A.gey = gey; A.gez = gez; A.gphi = gphi;
+  A.nc4 = c->nc4.p;
+  A.meta = c->meta.p;
+  A.mom32 = reinterpret_cast<const float4*>(c->mom32.p);
+  A.nleaves = c->nleaves.p;
+  A.bl2 = c->d_box + 9;
+  {
+    int rc = prepare_mac(c, &A.macb);
+    if (rc) return rc;
+  }
+  A.vbox = c->d_vbox;
+  A.nbox = c->nboxes;
+  A.theta2 = (float)c->prm.theta2;
+  A.eps2 = (float)c->prm.eps2;
+  A.npart = c->n;
+  A.adj = c->adj.p;
+  A.counters = c->counters.p;
+  A.status = c->d_status;
+  A.queue = c->walk_queue();
+  const int gblocks = 148 * 4;
+  const size_t per = (size_t)gblocks * kWW * kStackCap;
+  if (!ensure(c, c->wstack, 2 * per, "walk stacks")) return PEPCG_ERR_OOM;
+  COUNT_LAUNCH();
+  k_reset_mixed<<<1, 1, 0, s>>>(A.queue);
+  COUNT_LAUNCH();
+  if (with_e)
+    k_adj_group64<true><<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p, c->child8.p, c->nchild.p);
+  else
+    k_adj_group64<false><<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p, c->child8.p, c->nchild.p);
+  return cuda_ok(c, cudaGetLastError(), "mixed adjoint launch") ? PEPCG_OK : PEPCG_ERR_CUDA;
 }
 
 }  // namespace pepcg

@@ -209,11 +209,76 @@ def test_adjoint_rejects_periodic_far_field(gpu):
     assert ei.value.code == P.PEPCG_ERR_UNSUPPORTED
 
 
-def test_adjoint_rejects_group_of_64(gpu):
-    rng = np.random.default_rng(6)
-    x, y, z, q = rng.random(300), rng.random(300), rng.random(300), rng.standard_normal(300)
-    tc = P.TreeCode(walk=P.WALK_GROUP, group_size=64)
+@pytest.mark.parametrize("with_e", [False, True])
+def test_adjoint_group64_matches_oracle_buckets(gpu, with_e):
+    # the FP64 adjoint of the group walk with 64-target buckets against the
+    # oracle's adjoint of the same bucket lists (walk 2, tile_size 64)
+    x, y, z, q, tx, ty, tz, gphi, gE, rng = problem(4000, 300, 72)
+    if not with_e:
+        gE = [np.zeros(len(tx))] * 3
+    kw = dict(theta2=0.16, eps2=1e-3)
+    tc = P.TreeCode(precision=P.PRECISION_PLAIN, walk=P.WALK_GROUP, group_size=64, **kw)
     tc.pepc_grow_tree(x, y, z, q)
-    with pytest.raises(P.PepcgError) as ei:
-        tc.traverse_adjoint(x[:5], y[:5], z[:5], [np.zeros(5)] * 3, np.ones(5), 300)
-    assert ei.value.code == P.PEPCG_ERR_UNSUPPORTED
+    g = tc.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
+    orc = O.Oracle(walk=2, tile_size=64, **kw)
+    orc.grow_tree(x, y, z, q)
+    go = orc.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
+    for k in ("q", "x", "y", "z"):
+        scale = np.abs(go[k]).max()
+        assert np.abs(g[k] - go[k]).max() <= 1e-9 * scale, k
+    tc.close()
+    orc.close()
+
+
+@pytest.mark.parametrize("with_e", [False, True])
+def test_mixed_adjoint_group64_against_fp64(gpu, with_e):
+    # the benchmark's walk (mixed, 64-target buckets): its adjoint on the
+    # forward's FP32 lists, in FP32 with FP64 sums across buckets, against the
+    # FP64 adjoint of the same bucket walk (the lists differ only where a MAC
+    # decision is within FP32 rounding of its threshold)
+    x, y, z, q, tx, ty, tz, gphi, gE, rng = problem(20000, 2000, 73)
+    if not with_e:
+        gE = [np.zeros(len(tx))] * 3
+    kw = dict(theta2=0.16, eps2=1e-4, walk=P.WALK_GROUP, group_size=64)
+    out = {}
+    for prec in (P.PRECISION_PLAIN, P.PRECISION_MIXED):
+        tc = P.TreeCode(precision=prec, **kw)
+        tc.pepc_grow_tree(x, y, z, q)
+        out[prec] = tc.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
+        tc.close()
+    for k in ("q", "x", "y", "z"):
+        a, b = out[P.PRECISION_MIXED][k], out[P.PRECISION_PLAIN][k]
+        rel = np.abs(a - b) / np.abs(b).max()
+        assert np.median(rel) < 1e-6, (k, np.median(rel))
+        assert np.percentile(rel, 99) < 1e-4, (k, np.percentile(rel, 99))
+
+
+def test_mixed_adjoint_configuration_against_direct(gpu):
+    # the adjoint configuration through the benchmark's walk (mixed, 64-target
+    # buckets) against the FP64 direct-sum gradient
+    n, nt = 262144, 4096
+    rng = np.random.default_rng(4)
+    x, y, z = rng.random(n), rng.random(n), rng.random(n)
+    q = np.random.default_rng(41).standard_normal(n)
+    prng = np.random.default_rng(42)
+    tx, ty, tz = (0.25 + 0.5 * prng.random(nt) for _ in range(3))
+    q_t = np.random.default_rng(43).standard_normal(n)
+    kw = dict(theta2=0.16, eps2=1e-6, walk=P.WALK_GROUP, precision=P.PRECISION_MIXED)
+    tt = P.TreeCode(**kw)
+    tt.pepc_grow_tree(x, y, z, q_t)
+    phi_t = tt.pepc_traverse_tree(tx, ty, tz)["pot"]
+    tt.close()
+    tc = P.TreeCode(**kw)
+    tc.pepc_grow_tree(x, y, z, q)
+    phi = tc.pepc_traverse_tree(tx, ty, tz)["pot"]
+    gphi = 2.0 * (phi - phi_t)
+    zero = [np.zeros(nt)] * 3
+    g = tc.traverse_adjoint(tx, ty, tz, zero, gphi, n)
+    tc.close()
+    orc = O.Oracle(theta2=0.16, eps2=1e-6, walk=0, num_threads=16)
+    orc.grow_tree(x, y, z, q)
+    gd = orc.traverse_adjoint(tx, ty, tz, zero, gphi, n, direct=True)
+    orc.close()
+    for k in ("q", "x", "y", "z"):
+        rel = np.abs(g[k] - gd[k]) / np.abs(gd[k]).max()
+        assert np.median(rel) < 1e-3, (k, np.median(rel))

@@ -42,10 +42,11 @@ def _L_direct(arrs, t, gphi, gE, eps2):
     return float(np.sum(gphi * pot + gE[0] * ex + gE[1] * ey + gE[2] * ez))
 
 
-@pytest.mark.parametrize("direct", [False, True])
-def test_oracle_adjoint_against_fd(direct):
-    x, y, z, q, tx, ty, tz, gphi, gE, rng = _problem(600, 24, 13)
-    kw = dict(theta2=0.16, eps2=1e-3, walk=0)
+@pytest.mark.parametrize("direct,walk", [(False, 0), (True, 0), (False, 2)])
+def test_oracle_adjoint_against_fd(direct, walk):
+    # walk 2: buckets of 64 consecutive targets (the group walk's lists)
+    x, y, z, q, tx, ty, tz, gphi, gE, rng = _problem(600, 24 if walk == 0 else 100, 13)
+    kw = dict(theta2=0.16, eps2=1e-3, walk=walk, tile_size=64)
     o = O.Oracle(**kw)
     o.grow_tree(x, y, z, q)
     g = o.traverse_adjoint(tx, ty, tz, gE, gphi, len(x), direct=direct)
