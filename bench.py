@@ -571,7 +571,7 @@ def adjoint_measure(P, torch, dev, stream, prec, walk, plummer_xyzq, theta):
     return {"configuration": conf,
             "self_4m": {"forward_ms": f4, "adjoint_phi_ms": a_phi, "adjoint_full_ms": a_full,
                         "ratio_phi": a_phi / f4, "ratio_full": a_full / f4},
-            "walk": "the timed walk and precision (forward and adjoint alike)"}
+            "note": "forward and adjoint of the same walk and precision"}
 
 
 def workload_name(args):
@@ -599,9 +599,12 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--shard", action="store_true",
                     help="target sharding across the ranks (strong scaling) instead of replicas")
-    ap.add_argument("--workload", default="plummer", choices=["plummer", "explosion", "madelung"],
+    ap.add_argument("--workload", default="plummer",
+                    choices=["plummer", "explosion", "madelung", "adjoint"],
                     help="plummer: the headline line; explosion / madelung: the other "
-                         "configurations, one descriptive JSON line each")
+                         "configurations, one descriptive JSON line each; adjoint: the "
+                         "adjoint measurements alone (the adjoint configuration, then the "
+                         "Plummer particles of --n as their own targets)")
     args = ap.parse_args()
     assert args.warmup >= 3, "at least 3 warm-up steps"
 
@@ -626,6 +629,17 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
+    if args.workload == "adjoint":
+        dev = torch.device("cuda", local)
+        stream = torch.cuda.Stream(device=dev)
+        torch.cuda.set_stream(stream)
+        prec = {"mixed": P.PRECISION_MIXED, "plain": P.PRECISION_PLAIN,
+                "strict": P.PRECISION_MIXED_STRICT}[args.precision]
+        walk = {"group": P.WALK_GROUP, "target": P.WALK_PER_TARGET, "tile": P.WALK_PER_TILE}[args.walk]
+        res = adjoint_measure(P, torch, dev, stream, prec, walk, plummer(args.n), args.theta)
+        print(json.dumps({"workload": "adjoint", "precision": args.precision, "walk": args.walk,
+                          "n": args.n, **res}), flush=True)
+        return
     if args.workload != "plummer":
         dev = torch.device("cuda", local)
         stream = torch.cuda.Stream(device=dev)

@@ -777,10 +777,6 @@ __global__ void __launch_bounds__(kMixThreads, kStrict ? 4 : 5)
         if (node >= 0) {
           a = A.nc4[node];
           const int2 mu = A.meta[node];
-          nlv = A.nleaves[node];
-          nch = nchild[node];
-          c0 = child8[2 * (int64_t)node];
-          c1 = child8[2 * (int64_t)node + 1];
           cx = (float)(a.x - gx); cy = (float)(a.y - gy); cz = (float)(a.z - gz);
           if (mu.y & kLeafFlag) {
             isleaf = true;
@@ -845,6 +841,14 @@ __global__ void __launch_bounds__(kMixThreads, kStrict ? 4 : 5)
                                                        : __popc(vm1)));
           }
         }
+        // the child table only for opened twigs, the leaf count only for
+        // accepted ones (most popped nodes are leaves or accepted twigs)
+        if (open) {
+          nch = nchild[node];
+          c0 = child8[2 * (int64_t)node];
+          c1 = child8[2 * (int64_t)node + 1];
+        }
+        if (accept) nlv = A.nleaves[node];
         const unsigned lb = __ballot_sync(0xffffffffu, isleaf);
         const unsigned ab = __ballot_sync(0xffffffffu, accept);
         if (isleaf) {
