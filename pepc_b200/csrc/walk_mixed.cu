@@ -1252,8 +1252,10 @@ __global__ void __launch_bounds__(kMixThreads, 4)
           const int node = __float_as_int(c.w);
           const float2 CX = f2(c.x), CY = f2(c.y), CZ = f2(c.z);  // d = r_t + c
           const float2 PX = f2(m0.x), PY = f2(m0.y), PZ = f2(m0.z);
+          // -(p.d + tr) = (-p).d + (-tr): the negated dipole and trace, once per record
+          const float2 NPX = f2(-m0.x), NPY = f2(-m0.y), NPZ = f2(-m0.z), NTR = f2(-m2.y);
           const float2 Txx = f2(m0.w), Tyy = f2(m1.x), Tzz = f2(m1.y), Txy = f2(m1.z),
-                       Tyz = f2(m1.w), Tzx = f2(m2.x), TR = f2(m2.y), Q = f2(m2.z);
+                       Tyz = f2(m1.w), Tzx = f2(m2.x), Q = f2(m2.z);
           float2 aq = f2(0.f), apx = f2(0.f), apy = f2(0.f), apz = f2(0.f), aS = f2(0.f);
           float2 axx = f2(0.f), ayy = f2(0.f), azz = f2(0.f), axy = f2(0.f), ayz = f2(0.f),
                  azx = f2(0.f), acx = f2(0.f), acy = f2(0.f), acz = f2(0.f);
@@ -1269,55 +1271,57 @@ __global__ void __launch_bounds__(kMixThreads, 4)
             const float2 R0 = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
             const float2 i2 = __fmul2_rn(R0, R0);
             const float2 R1 = __fmul2_rn(R0, i2);
-            const float2 R2 = __fmul2_rn(R1, i2);
-            const float2 R3 = __fmul2_rn(R2, i2);
+            // scaled radial factors: T3 = 3 R2, F5 = 5 R3
+            const float2 T3 = __fmul2_rn(R1, __fmul2_rn(f2(3.f), i2));
+            const float2 F5 = __fmul2_rn(T3, __fmul2_rn(f2(5.f / 3.f), i2));
             const float2 vx = __ffma2_rn(Txx, dx, __ffma2_rn(Txy, dy, __fmul2_rn(Tzx, dz)));
             const float2 vy = __ffma2_rn(Txy, dx, __ffma2_rn(Tyy, dy, __fmul2_rn(Tyz, dz)));
             const float2 vz = __ffma2_rn(Tzx, dx, __ffma2_rn(Tyz, dy, __fmul2_rn(Tzz, dz)));
             const float2 dTd = __ffma2_rn(dx, vx, __ffma2_rn(dy, vy, __fmul2_rn(dz, vz)));
-            const float2 u = __ffma2_rn(PX, dx, __ffma2_rn(PY, dy, __ffma2_rn(PZ, dz, TR)));
-            const float2 m3R2 = __fmul2_rn(f2(-3.f), R2);
-            const float2 ce = __ffma2_rn(Q, R1, __ffma2_rn(m3R2, u, __fmul2_rn(__fmul2_rn(f2(5.f), R3), dTd)));
+            const float2 nu = __ffma2_rn(NPX, dx, __ffma2_rn(NPY, dy, __ffma2_rn(NPZ, dz, NTR)));
+            // ce = q R1 - 3 R2 (p.d + tr) + 5 R3 dTd
+            const float2 ce = __ffma2_rn(Q, R1, __ffma2_rn(T3, nu, __fmul2_rn(F5, dTd)));
             const float2 s1 = __fmul2_rn(gp, R1);
-            float2 s3 = __fmul2_rn(gp, __fmul2_rn(f2(3.f), R2));
+            float2 s3 = __fmul2_rn(gp, T3);
             aq = __ffma2_rn(gp, R0, aq);
             aS = __fadd2_rn(aS, s1);
             float2 kd = __fmul2_rn(gp, ce);                        // coefficient of d in cocbar
             float2 kv = __fmul2_rn(f2(-2.f / 3.f), s3);            // of v
             float2 ex_ = f2(0.f), ey_ = f2(0.f), ez_ = f2(0.f);     // -3 R2 g
-            float2 ppx = s1, ppy = s1, ppz = s1;                    // coefficient of -d in pbar
+            float2 ppx = s1;                                        // coefficient of -d in pbar
             if constexpr (kWithE) {
               const float4 tc4 = tg[p][2], td4 = tg[p][3];
               const float2 gxx = make_float2(tc4.x, tc4.y), gyy = make_float2(tc4.z, tc4.w),
                            gzz = make_float2(td4.x, td4.y);
-              const float2 R4 = __fmul2_rn(R3, i2);
               const float2 ga = __ffma2_rn(gxx, dx, __ffma2_rn(gyy, dy, __fmul2_rn(gzz, dz)));
+              const float2 F15 = __fmul2_rn(f2(3.f), F5);
+              const float2 F10n = __fmul2_rn(f2(-2.f), F5);
+              const float2 S35 = __fmul2_rn(F5, __fmul2_rn(f2(7.f), i2));  // 35 R4
               aq = __ffma2_rn(ga, R1, aq);
               // pbar += R1 g - 3 ga R2 d, kept as -pbar
-              const float2 h = __fmul2_rn(ga, __fmul2_rn(f2(3.f), R2));  // 3 ga R2
+              const float2 h = __fmul2_rn(ga, T3);  // 3 ga R2
               const float2 nR1 = __fmul2_rn(f2(-1.f), R1);
               apx = __ffma2_rn(nR1, gxx, apx);
               apy = __ffma2_rn(nR1, gyy, apy);
               apz = __ffma2_rn(nR1, gzz, apz);
-              ppx = __fadd2_rn(s1, h); ppy = ppx; ppz = ppx;
+              ppx = __fadd2_rn(s1, h);
               // Qbar: 15 ga R3 d d - 3 R2 (g d + d g + ga I)
-              s3 = __ffma2_rn(__fmul2_rn(f2(15.f), ga), R3, s3);
-              ex_ = __fmul2_rn(m3R2, gxx);
-              ey_ = __fmul2_rn(m3R2, gyy);
-              ez_ = __fmul2_rn(m3R2, gzz);
+              s3 = __ffma2_rn(F15, ga, s3);
+              const float2 nT3 = __fmul2_rn(f2(-1.f), T3);
+              ex_ = __fmul2_rn(nT3, gxx);
+              ey_ = __fmul2_rn(nT3, gyy);
+              ez_ = __fmul2_rn(nT3, gzz);
               aS = __fadd2_rn(aS, h);  // the delta_kl and the p terms share 3 ga R2
               // cocbar: cd d + cg g + 3 R2 ga p - 10 R3 ga v + 2 R2 T g, cg = -ce,
               // cd = ga (3 q R2 - 15 R3 u + 35 R4 dTd) + 3 R2 (g.p) - 10 R3 (g.v);
               // T g is node-constant: the batch sums 2 R2 g (aG) and applies T once
               const float2 gP = __ffma2_rn(gxx, PX, __ffma2_rn(gyy, PY, __fmul2_rn(gzz, PZ)));
               const float2 gv = __ffma2_rn(gxx, vx, __ffma2_rn(gyy, vy, __fmul2_rn(gzz, vz)));
-              const float2 nR3x10 = __fmul2_rn(f2(-10.f), R3);
-              const float2 inner = __ffma2_rn(__fmul2_rn(f2(3.f), Q), R2,
-                                   __ffma2_rn(__fmul2_rn(f2(-15.f), R3), u, __fmul2_rn(__fmul2_rn(f2(35.f), R4), dTd)));
-              const float2 cd = __ffma2_rn(ga, inner, __ffma2_rn(__fmul2_rn(f2(3.f), R2), gP, __fmul2_rn(nR3x10, gv)));
+              const float2 inner = __ffma2_rn(Q, T3, __ffma2_rn(F15, nu, __fmul2_rn(S35, dTd)));
+              const float2 cd = __ffma2_rn(ga, inner, __ffma2_rn(T3, gP, __fmul2_rn(F10n, gv)));
               kd = __fadd2_rn(kd, cd);
-              kv = __ffma2_rn(nR3x10, ga, kv);
-              const float2 R2x2 = __fmul2_rn(f2(2.f), R2);
+              kv = __ffma2_rn(F10n, ga, kv);
+              const float2 R2x2 = __fmul2_rn(f2(2.f / 3.f), T3);
               aGx = __ffma2_rn(R2x2, gxx, aGx);
               aGy = __ffma2_rn(R2x2, gyy, aGy);
               aGz = __ffma2_rn(R2x2, gzz, aGz);
@@ -1327,8 +1331,8 @@ __global__ void __launch_bounds__(kMixThreads, 4)
               acz = __ffma2_rn(nce, gzz, acz);
             }
             apx = __ffma2_rn(ppx, dx, apx);
-            apy = __ffma2_rn(ppy, dy, apy);
-            apz = __ffma2_rn(ppz, dz, apz);
+            apy = __ffma2_rn(ppx, dy, apy);
+            apz = __ffma2_rn(ppx, dz, apz);
             // Qbar's d d terms and (with E) the g d terms:
             //   kl += (s3 d_k + e_k) d_l + e_l d_k,  e = -3 R2 g
             const float2 wx = __ffma2_rn(s3, dx, ex_), wy = __ffma2_rn(s3, dy, ey_),
@@ -1485,10 +1489,6 @@ __global__ void __launch_bounds__(kMixThreads, 4)
         if (node >= 0) {
           a = A.nc4[node];
           const int2 mu = A.meta[node];
-          nlv = A.nleaves[node];
-          nch = nchild[node];
-          c0 = child8[2 * (int64_t)node];
-          c1 = child8[2 * (int64_t)node + 1];
           cx = (float)(a.x - gx); cy = (float)(a.y - gy); cz = (float)(a.z - gz);
           if (mu.y & kLeafFlag) {
             isleaf = true;
@@ -1529,6 +1529,12 @@ __global__ void __launch_bounds__(kMixThreads, 4)
                                                        : __popc(vm1)));
           }
         }
+        if (open) {
+          nch = nchild[node];
+          c0 = child8[2 * (int64_t)node];
+          c1 = child8[2 * (int64_t)node + 1];
+        }
+        if (accept) nlv = A.nleaves[node];
         const unsigned lb = __ballot_sync(0xffffffffu, isleaf);
         const unsigned ab = __ballot_sync(0xffffffffu, accept);
         if (isleaf) {

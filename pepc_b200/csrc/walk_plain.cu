@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include "internal.cuh"
 
@@ -65,9 +66,12 @@ struct WalkArgs {
 };
 
 // any(abs(delta) >= spatial_interaction_cutoff) (module_tree_walk_pthreads.f90:
-// 622,639; module_tree_walk_simple.f90:330,377): the node is skipped
+// 622,639; module_tree_walk_simple.f90:330,377): the node is skipped.  The walks
+// are instantiated with and without the test (kCut), so that a walk without a
+// finite cutoff runs the code it ran before the option existed.
+template <bool kCut>
 __device__ __forceinline__ bool cut_off(const WalkArgs& A, double dx, double dy, double dz) {
-  return A.has_cut && (fabs(dx) >= A.cut[0] || fabs(dy) >= A.cut[1] || fabs(dz) >= A.cut[2]);
+  return kCut && (fabs(dx) >= A.cut[0] || fabs(dy) >= A.cut[1] || fabs(dz) >= A.cut[2]);
 }
 
 __device__ __forceinline__ void warp_add_counters(unsigned long long* ctr, unsigned long long a,
@@ -84,7 +88,7 @@ __device__ __forceinline__ void warp_add_counters(unsigned long long* ctr, unsig
   }
 }
 
-template <int kLaw>
+template <int kLaw, bool kCut>
 __global__ void __launch_bounds__(kWalkThreads) k_walk_target64(WalkArgs A) {
   __shared__ double s_bl2[kMaxLevel + 1];
   __shared__ double s_vb[3 * 125];
@@ -126,7 +130,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_target64(WalkArgs A) {
         if (mu.y & kLeafFlag) {
           partner += 1;
           w += 1.0;  // counted before the cutoff test (:620-622)
-          if (!cut_off(A, dx, dy, dz)) {
+          if (!cut_off<kCut>(A, dx, dy, dz)) {
             ++c_leaf;
             if (dist2 > 0.0) {
               double fx, fy, fz, fp;
@@ -139,7 +143,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_target64(WalkArgs A) {
           ++c_mac;
           if (A.theta2 * dist2 > (A.macb ? A.macb[u] : s_bl2[mu.y & 0xff])) {
             partner += A.nleaves[u];
-            if (!cut_off(A, dx, dy, dz)) {
+            if (!cut_off<kCut>(A, dx, dy, dz)) {
               double m[9];
 #pragma unroll
               for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
@@ -174,7 +178,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_target64(WalkArgs A) {
 // Launch bounds: six resident blocks per SM for one target per lane (the
 // plain group walk at 4M takes 223 ms against 270 ms at the unbounded 108
 // registers), four for two.
-template <int kLaw, int kTPL>
+template <int kLaw, int kTPL, bool kCut>
 __global__ void __launch_bounds__(kWalkThreads, kTPL == 1 ? 6 : 4) k_walk_tile64(WalkArgs A) {
   __shared__ double s_bl2[kMaxLevel + 1];
   __shared__ double s_vb[3 * 125];
@@ -230,7 +234,7 @@ __global__ void __launch_bounds__(kWalkThreads, kTPL == 1 ? 6 : 4) k_walk_tile64
           partner += 1;
 #pragma unroll
           for (int s = 0; s < kTPL; ++s)
-            if (valid[s] && !cut_off(A, dx[s], dy[s], dz[s])) {
+            if (valid[s] && !cut_off<kCut>(A, dx[s], dy[s], dz[s])) {
               w[s] += 1.0;
               ++c_leaf;
               if (dist2[s] > 0.0) {
@@ -263,7 +267,7 @@ __global__ void __launch_bounds__(kWalkThreads, kTPL == 1 ? 6 : 4) k_walk_tile64
             for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
 #pragma unroll
             for (int s = 0; s < kTPL; ++s)
-              if (valid[s] && !cut_off(A, dx[s], dy[s], dz[s])) {
+              if (valid[s] && !cut_off<kCut>(A, dx[s], dy[s], dz[s])) {
                 double fx, fy, fz, fp;
                 law_twig64<kLaw>(a.w, m, dx[s], dy[s], dz[s], dist2[s], A.eps2, fx, fy, fz, fp);
                 e0[s] += fx; e1[s] += fy; e2[s] += fz; ph[s] += fp;
@@ -302,7 +306,7 @@ __global__ void __launch_bounds__(kWalkThreads, kTPL == 1 ? 6 : 4) k_walk_tile64
 // decides accept / open by a ballot over its own lanes.  A lane's sequence of
 // interactions is exactly its tile's, so fields, work and MAC counts equal
 // the one-tile-per-warp walk's.
-template <int kLaw>
+template <int kLaw, bool kCut>
 // Six resident blocks per SM (80 registers, a few spilled): at 4M, T = 16,
 // 260 ms against 296 ms at the unbounded 110 registers (four blocks).
 __global__ void __launch_bounds__(kWalkThreads, 6) k_walk_tilepack64(WalkArgs A) {
@@ -357,7 +361,7 @@ __global__ void __launch_bounds__(kWalkThreads, 6) k_walk_tilepack64(WalkArgs A)
           const double dist2 = (dx * dx + dy * dy) + dz * dz;
           if (mu.y & kLeafFlag) {
             partner += 1;
-            if (!cut_off(A, dx, dy, dz)) {  // before the work count (:330)
+            if (!cut_off<kCut>(A, dx, dy, dz)) {  // before the work count (:330)
               w += 1.0;
               ++c_leaf;
               if (dist2 > 0.0) {
@@ -376,7 +380,7 @@ __global__ void __launch_bounds__(kWalkThreads, 6) k_walk_tilepack64(WalkArgs A)
             if (lane <= first_fail) ++c_mac;
             if (tf == 0) {
               partner += A.nleaves[u];
-              if (!cut_off(A, dx, dy, dz)) {  // :377
+              if (!cut_off<kCut>(A, dx, dy, dz)) {  // :377
                 double m[9];
 #pragma unroll
                 for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
@@ -497,6 +501,21 @@ __global__ void k_same_keys(int64_t n, const int64_t* __restrict__ a, const int6
 }
 
 __global__ void k_reset_counter(unsigned int* q) { *q = 0; }
+
+// calls f(law, cut) with both as compile-time constants (std::integral_constant)
+template <class F>
+void launch_law_cut(int law, bool cut, F&& f) {
+  using T = std::true_type;
+  using Fl = std::false_type;
+  auto go = [&](auto L) {
+    if (cut) f(L, T{});
+    else f(L, Fl{});
+  };
+  if (law == 2) go(std::integral_constant<int, 2>{});
+  else if (law == 4) go(std::integral_constant<int, 4>{});
+  else if (law == 5) go(std::integral_constant<int, 5>{});
+  else go(std::integral_constant<int, 3>{});
+}
 
 // mac (coulomb/module_interaction_specific.f90:256-275) for mac_select != 0,
 // as a per-twig threshold t with "accept iff theta2 dist2 > t": the Bmax MAC
@@ -710,28 +729,25 @@ int traverse_device(Ctx* c, int64_t nt, const double* tx, const double* ty, cons
       if (c->prm.precision == PEPCG_PRECISION_PLAIN) {
         COUNT_LAUNCH();
         const int law = c->prm.force_law;
+        const bool cut = A.has_cut != 0;
         if (walk == PEPCG_WALK_PER_TARGET) {
-          if (law == 2) k_walk_target64<2><<<blocks, kWalkThreads, 0, sk>>>(A);
-          else if (law == 4) k_walk_target64<4><<<blocks, kWalkThreads, 0, sk>>>(A);
-          else if (law == 5) k_walk_target64<5><<<blocks, kWalkThreads, 0, sk>>>(A);
-          else k_walk_target64<3><<<blocks, kWalkThreads, 0, sk>>>(A);
+          launch_law_cut(law, cut, [&](auto L, auto C) {
+            k_walk_target64<decltype(L)::value, decltype(C)::value><<<blocks, kWalkThreads, 0, sk>>>(A);
+          });
         } else if (packed) {
-          if (law == 2) k_walk_tilepack64<2><<<blocks, kWalkThreads, 0, sk>>>(A);
-          else if (law == 4) k_walk_tilepack64<4><<<blocks, kWalkThreads, 0, sk>>>(A);
-          else if (law == 5) k_walk_tilepack64<5><<<blocks, kWalkThreads, 0, sk>>>(A);
-          else k_walk_tilepack64<3><<<blocks, kWalkThreads, 0, sk>>>(A);
+          launch_law_cut(law, cut, [&](auto L, auto C) {
+            k_walk_tilepack64<decltype(L)::value, decltype(C)::value><<<blocks, kWalkThreads, 0, sk>>>(A);
+          });
         } else {
           if (walk == PEPCG_WALK_GROUP) A.tiles = nullptr;
           if (walk == PEPCG_WALK_GROUP && c->group_size() == 64) {
-            if (law == 2) k_walk_tile64<2, 2><<<blocks, kWalkThreads, 0, sk>>>(A);
-            else if (law == 4) k_walk_tile64<4, 2><<<blocks, kWalkThreads, 0, sk>>>(A);
-            else if (law == 5) k_walk_tile64<5, 2><<<blocks, kWalkThreads, 0, sk>>>(A);
-            else k_walk_tile64<3, 2><<<blocks, kWalkThreads, 0, sk>>>(A);
+            launch_law_cut(law, cut, [&](auto L, auto C) {
+              k_walk_tile64<decltype(L)::value, 2, decltype(C)::value><<<blocks, kWalkThreads, 0, sk>>>(A);
+            });
           } else {
-            if (law == 2) k_walk_tile64<2, 1><<<blocks, kWalkThreads, 0, sk>>>(A);
-            else if (law == 4) k_walk_tile64<4, 1><<<blocks, kWalkThreads, 0, sk>>>(A);
-            else if (law == 5) k_walk_tile64<5, 1><<<blocks, kWalkThreads, 0, sk>>>(A);
-            else k_walk_tile64<3, 1><<<blocks, kWalkThreads, 0, sk>>>(A);
+            launch_law_cut(law, cut, [&](auto L, auto C) {
+              k_walk_tile64<decltype(L)::value, 1, decltype(C)::value><<<blocks, kWalkThreads, 0, sk>>>(A);
+            });
           }
         }
       } else {
