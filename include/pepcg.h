@@ -188,8 +188,11 @@ int pepcg_traverse_self_device(void* ctx, double* d_ex, double* d_ey, double* d_
  * buckets (the mixed default) the adjoint runs on that walk's own FP32 lists,
  * evaluates its terms in FP32 on the group-centred offsets and sums them in
  * FP64 across buckets, like the forward; the other mixed walks take the FP64
- * adjoint of their semantics.  Open boundaries only: a periodic far field
- * returns PEPCG_ERR_UNSUPPORTED.
+ * adjoint of their semantics.  With periodic boundaries the mirror boxes'
+ * terms are in the walk's adjoint, and the FMM far-lattice term's adjoint
+ * (FP64, every fmm_extrinsic_correction) is added: the transpose of the
+ * lattice force and of the central box's multipole expansion, through the
+ * fictitious charges or Redlack terms to the particles.
  */
 int pepcg_traverse_adjoint(void* ctx, int64_t nt, const double* tx, const double* ty,
                            const double* tz, const double* dLdEx, const double* dLdEy,

@@ -177,6 +177,18 @@ def par_rand(iseed, n):
     return out
 
 
+GOLDEN = os.path.join(HERE, "..", "tests", "golden", "reference_pins.npz")
+
+
+def unit_cube(p):
+    """system_is_unit_cube (module_mirror_boxes.f90:248-255)."""
+    a, b, c = p.t_lattice_1, p.t_lattice_2, p.t_lattice_3
+    axes = (a[0] > 0 and a[1] == 0 and a[2] == 0 and b[0] == 0 and b[1] > 0 and b[2] == 0
+            and c[0] == 0 and c[1] == 0 and c[2] > 0)
+    nsq = lambda v: (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]  # noqa: E731
+    return axes and nsq(a) == 1.0 and nsq(b) == 1.0 and nsq(c) == 1.0
+
+
 def reference_lattice_table(gold):
     """The reference's pretabulated unit-cube MLattice (l <= 40) from the golden fixture."""
     ml = np.zeros(861, dtype=np.complex128)
@@ -198,6 +210,11 @@ class Oracle:
     def __init__(self, **kw):
         self.p = params(**kw)
         self.h = lib().orc_create(C.byref(self.p))
+        # fmm_framework_prepare (module_fmm_framework.f90:112-115): a unit-cube
+        # lattice loads the pretabulated coefficients instead of iterating
+        if (any(self.p.periodicity) and self.p.include_far_field_if_periodic
+                and unit_cube(self.p)):
+            self.set_lattice_coefficients(reference_lattice_table(np.load(GOLDEN)))
 
     def close(self):
         if self.h:

@@ -481,6 +481,11 @@ void orc_fmm_timestep(OrcFmm* f, int64_t n, const double* x, const double* y, co
                       const double* q);
 void orc_fmm_sum_lattice_force(const OrcFmm* f, const double pos[3], double e[3], double* phi);
 void orc_fmm_set_mlattice(OrcFmm* f, const double* re_im);
+void orc_fmm_adjoint(const OrcFmm* f, int64_t nt, const double* tx, const double* ty,
+                     const double* tz, const double* gex, const double* gey, const double* gez,
+                     const double* gphi, int64_t n, const double* x, const double* y,
+                     const double* z, const double* q, double* dq, double* dx, double* dy,
+                     double* dz);
 
 // ---------------------------------------------------------------------------
 // Whole-path context
@@ -1276,13 +1281,12 @@ int orc_lattice(orc_ctx* c, int64_t nt, const double* tx, const double* ty, cons
 
 // Adjoint of the per-target walk (module_tree_walk_pthreads.f90 semantics), or
 // with walk 2 of the bucket walk (the group walk's lists): dL/dq and dL/dx of
-// the grown particles, in the caller's original order.
-// Open boundaries only (returns -5 with a periodic far field).
+// the grown particles, in the caller's original order.  With a periodic far
+// field the lattice term's adjoint (orc_fmm_adjoint) is added.
 int orc_traverse_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double* ty,
                          const double* tz, const double* gex, const double* gey,
                          const double* gez, const double* gphi, double* dLdq, double* dLdx,
                          double* dLdy, double* dLdz) {
-  if (c->fmm) return -5;
   auto boxes = neighbour_boxes(c->p);
   const int64_t M = (int64_t)c->nodes.size();
   std::vector<Adj> adj(M);
@@ -1392,6 +1396,19 @@ int orc_traverse_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double*
     dLdx[io] = a.c[0];
     dLdy[io] = a.c[1];
     dLdz[io] = a.c[2];
+  }
+  if (c->fmm) {
+    const int64_t n = c->n;
+    std::vector<double> fq(n), fx(n), fy(n), fz(n);
+    orc_fmm_adjoint(c->fmm, nt, tx, ty, tz, gex, gey, gez, gphi, n, c->x.data(), c->y.data(),
+                    c->z.data(), c->q.data(), fq.data(), fx.data(), fy.data(), fz.data());
+    for (int64_t ip = 0; ip < n; ++ip) {
+      const int64_t io = c->perm[ip];
+      dLdq[io] += fq[ip];
+      dLdx[io] += fx[ip];
+      dLdy[io] += fy[ip];
+      dLdz[io] += fz[ip];
+    }
   }
   return 0;
 }

@@ -98,7 +98,7 @@ int orc_direct(orc_ctx* c, int64_t ntest, const int64_t* tidx, double* ex, doubl
                double* ez, double* pot);
 /* adjoint of the per-target walk with fixed interaction lists: dL/dq, dL/dx
  * of the grown particles (original order) for given dL/dE (gex..) and dL/dphi
- * at nt targets; open boundaries only (returns -5 otherwise) */
+ * at nt targets; with a periodic far field the lattice term's adjoint is added */
 int orc_traverse_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double* ty,
                          const double* tz, const double* gex, const double* gey,
                          const double* gez, const double* gphi, double* dLdq, double* dLdx,

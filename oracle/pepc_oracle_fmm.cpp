@@ -382,6 +382,220 @@ void orc_fmm_sum_lattice_force(const OrcFmm* f, const double pos[3], double e[3]
   *phi = ph;
 }
 
+// ---------------------------------------------------------------------------
+// Adjoint of the lattice term (no reference counterpart: the reference has no
+// differentiation).  L = sum_t gphi_t phi_lat(t) + gE_t . E_lat(t); returns
+// dL/dq and dL/dx of the n particles (x, y, z, q as given, the grown order).
+// The chain: targets -> mu (transpose of L2L to l <= 1) -> omega (transpose of
+// M2L) -> particles through O_lm(x - center), the fictitious charges (through
+// the box dipole) and the Redlack terms.  The derivative of O_lm is taken by
+// forward-mode dual numbers through omultipole's own operations, independently
+// of any ladder relation between the harmonics.
+// ---------------------------------------------------------------------------
+namespace {
+struct Dn {  // dual number v + d eps
+  double v, d;
+};
+inline Dn operator+(Dn a, Dn b) { return {a.v + b.v, a.d + b.d}; }
+inline Dn operator-(Dn a, Dn b) { return {a.v - b.v, a.d - b.d}; }
+inline Dn operator*(Dn a, Dn b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+inline Dn operator/(Dn a, Dn b) { return {a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)}; }
+inline Dn dsc(double s, Dn a) { return {s * a.v, s * a.d}; }
+inline Dn dsqrt(Dn a) {
+  double r = std::sqrt(a.v);
+  return {r, r > 0.0 ? a.d / (2.0 * r) : 0.0};
+}
+
+// legendre_p with a dual argument
+Dn legendre_p_d(int l, int m, Dn x) {
+  Dn pll = {0.0, 0.0}, pmm = {1.0, 0.0};
+  if (m > 0) {
+    Dn somx2 = dsqrt(( Dn{1.0, 0.0} - x) * (Dn{1.0, 0.0} + x));
+    double fact = 1.0;
+    for (int i = 1; i <= m; ++i) {
+      pmm = dsc(-fact, pmm) * somx2;
+      fact = fact + 2.0;
+    }
+  }
+  Dn r;
+  if (l == m) {
+    r = pmm;
+  } else {
+    Dn pmmp1 = dsc(2.0 * m + 1.0, x * pmm);
+    if (l == m + 1) {
+      r = pmmp1;
+    } else {
+      for (int ll = m + 2; ll <= l; ++ll) {
+        pll = dsc(1.0 / (double)(ll - m),
+                  dsc(2.0 * ll - 1.0, x * pmmp1) - dsc((double)(ll + m) - 1.0, pmm));
+        pmm = pmmp1;
+        pmmp1 = pll;
+      }
+      r = pll;
+    }
+  }
+  return dsc((m % 2 == 0) ? 1.0 : -1.0, r);
+}
+
+// d O_lm(c) / d c_k, by dual numbers through cart2sph and omultipole
+C omultipole_deriv(int l, int m, const double c[3], int k) {
+  Dn X[3];
+  for (int d = 0; d < 3; ++d) X[d] = {c[d], d == k ? 1.0 : 0.0};
+  Dn r = dsqrt((X[0] * X[0] + X[1] * X[1]) + X[2] * X[2]);
+  Dn ct = r.v == 0.0 ? Dn{1.0, 0.0} : X[2] / r;
+  // phi = atan2(y, x): d phi = (x dy - y dx) / (x^2 + y^2)
+  Dn ph = {0.0, 0.0};
+  if (!(c[0] == 0.0 && c[1] == 0.0)) {
+    ph.v = std::atan2(c[1], c[0]);
+    ph.d = (X[0].v * X[1].d - X[1].v * X[0].d) / (X[0].v * X[0].v + X[1].v * X[1].v);
+  }
+  Dn rl = {1.0, 0.0};
+  for (int i = 0; i < l; ++i) rl = rl * r;
+  Dn a = dsc(1.0 / factorial(l + m), rl * legendre_p_d(l, m, ct));
+  // a exp(-i m phi)
+  const double cs = std::cos(m * ph.v), sn = std::sin(m * ph.v);
+  const double dcs = -m * sn * ph.d, dsn = m * cs * ph.d;
+  return {a.d * cs + a.v * dcs, -(a.d * sn + a.v * dsn)};
+}
+}  // namespace
+
+void orc_fmm_adjoint(const OrcFmm* f, int64_t nt, const double* tx, const double* ty,
+                     const double* tz, const double* gex, const double* gey, const double* gez,
+                     const double* gphi, int64_t n, const double* x, const double* y,
+                     const double* z, const double* q, double* dq, double* dx, double* dy,
+                     double* dz) {
+  const double pi = std::acos(-1.0);
+  const double prefact = (2.0 * pi) / (3.0 * f->volume);
+  const int corr = f->p.fmm_extrinsic_correction;
+  // 1. dL/dmu (l <= Lmax_multipole), as G with L = Re sum_{l, m >= 0} G(l, m) mu(l, m),
+  //    accumulated over (l, k) with k of either sign and folded afterwards
+  const int W = 2 * kLmaxM + 1;
+  std::vector<C> A((kLmaxM + 1) * W, {0.0, 0.0});  // A(j, k), k in [-j, j]
+  auto Aat = [&](int j, int k) -> C& { return A[j * W + (k + kLmaxM)]; };
+  double dbar[3] = {0.0, 0.0, 0.0}, tbar = 0.0;
+  std::vector<double> qfbar(f->nfict, 0.0);
+  for (int64_t t = 0; t < nt; ++t) {
+    const double pos[3] = {tx[t], ty[t], tz[t]};
+    double R[3] = {pos[0] - f->center[0], pos[1] - f->center[1], pos[2] - f->center[2]};
+    auto s = cart2sph(R);
+    // L_t = Re[gphi mus(0,0) + (-gEx + i gEy) mus(1,1) - gEz mus(1,0)],
+    // mus(l, m) = sum_{j, k} O_R(j - l, k - m) mu(j, k)  (L2L, :943-976)
+    const C c00 = {gphi[t], 0.0}, c11 = {-gex[t], gey[t]}, c10 = {-gez[t], 0.0};
+    C OR[kLenM];
+    for (int l = 0; l <= kLmaxM; ++l)
+      for (int m = 0; m <= l; ++m) OR[tblinv(l, m)] = omultipole(l, m, s);
+    for (int j = 0; j <= kLmaxM; ++j)
+      for (int k = -j; k <= j; ++k) {
+        C acc = cmul(c00, tbl(OR, j, k, kLmaxM));
+        if (j >= 1) {
+          acc = cadd(acc, cmul(c11, tbl(OR, j - 1, k - 1, kLmaxM)));
+          acc = cadd(acc, cmul(c10, tbl(OR, j - 1, k, kLmaxM)));
+        }
+        Aat(j, k) = cadd(Aat(j, k), acc);
+      }
+    if (corr == 1) {
+      for (int d = 0; d < 3; ++d) dbar[d] += (2.0 * prefact) * (d == 0 ? gex[t] : d == 1 ? gey[t] : gez[t]);
+      for (int d = 0; d < 3; ++d) dbar[d] -= (2.0 * prefact) * gphi[t] * R[d];
+      tbar += prefact * gphi[t];
+    } else if (corr == 2) {
+      for (int pp = 0; pp < f->nfict; ++pp)
+        for (const auto& bx : f->boxes) {
+          double v[3], dd[3];
+          f->lvect(bx, v);
+          for (int k = 0; k < 3; ++k) dd[k] = (pos[k] - v[k]) - f->fict_pos[pp][k];
+          double r = std::sqrt((dd[0] * dd[0] + dd[1] * dd[1]) + dd[2] * dd[2]);
+          double rd = 1.0 / r, rd3 = rd * rd * rd;
+          qfbar[pp] += gphi[t] * rd + rd3 * ((gex[t] * dd[0] + gey[t] * dd[1]) + gez[t] * dd[2]);
+        }
+    }
+  }
+  // fold k < 0: mu(j, -m) = (-1)^m conj(mu(j, m))
+  std::vector<C> G(kLenM, {0.0, 0.0});
+  for (int j = 0; j <= kLmaxM; ++j)
+    for (int m = 0; m <= j; ++m) {
+      C g = Aat(j, m);
+      if (m > 0) {
+        C a = Aat(j, -m);
+        double sg = (m % 2 == 0) ? 1.0 : -1.0;
+        g = cadd(g, C{sg * a.re, -sg * a.im});
+      }
+      G[tblinv(j, m)] = g;
+    }
+  // 2. dL/domega: mu(l, m) = sum_{j, k} (-1)^j ML(j + l, k + m) omega(j, k) (M2L, :912-937)
+  std::vector<C> Ob(kLenM, {0.0, 0.0});
+  for (int j = 0; j <= kLmaxM; ++j)
+    for (int m = 0; m <= j; ++m) {
+      C b = {0.0, 0.0}, bn = {0.0, 0.0};  // B(j, m) and B(j, -m)
+      const double sj = (j % 2 == 0) ? 1.0 : -1.0;
+      for (int l = 0; l <= kLmaxM; ++l)
+        for (int mm = 0; mm <= l; ++mm) {
+          b = cadd(b, cmul(G[tblinv(l, mm)], cscale(sj, tbl(f->mlattice.data(), j + l, m + mm, kLmaxT))));
+          if (m > 0)
+            bn = cadd(bn, cmul(G[tblinv(l, mm)], cscale(sj, tbl(f->mlattice.data(), j + l, -m + mm, kLmaxT))));
+        }
+      if (m > 0) {
+        double sg = (m % 2 == 0) ? 1.0 : -1.0;
+        b = cadd(b, C{sg * bn.re, -sg * bn.im});
+      }
+      Ob[tblinv(j, m)] = b;
+    }
+  // omega(0, 0) never reaches mu: the forward removes it, or it is exactly
+  // zero and any change of a charge makes it nonzero and removed.  Its
+  // adjoint is therefore zero, which also keeps the divergent ML(0, 0) (of
+  // order 1e32 in the unit-cube table) out of every sum below
+  Ob[0] = {0.0, 0.0};
+  // 3. fictitious charges: q_f from the box dipole (:536-559)
+  if (corr == 2) {
+    for (int pp = 0; pp < f->nfict; ++pp) {
+      double rr[3] = {f->fict_pos[pp][0] - f->center[0], f->fict_pos[pp][1] - f->center[1],
+                      f->fict_pos[pp][2] - f->center[2]};
+      auto s = cart2sph(rr);
+      for (int l = 0; l <= kLmaxM; ++l)
+        for (int m = 0; m <= l; ++m) {
+          C o = omultipole(l, m, s), w = Ob[tblinv(l, m)];
+          qfbar[pp] += w.re * o.re - w.im * o.im;
+        }
+    }
+    const double qlast = qfbar[f->nfict - 1];
+    int ip = 0;
+    for (int pp = 0; pp < 3; ++pp) {
+      if (!f->p.periodicity[pp]) continue;
+      const double* L = f->lattice[pp];
+      const double len = std::sqrt((L[0] * L[0] + L[1] * L[1]) + L[2] * L[2]);
+      dbar[pp] += (qlast - qfbar[ip]) / len;
+      ++ip;
+    }
+  }
+  // 4. the particles
+  for (int64_t i = 0; i < n; ++i) {
+    const double R[3] = {x[i] - f->center[0], y[i] - f->center[1], z[i] - f->center[2]};
+    auto s = cart2sph(R);
+    double gq = 0.0, gx[3] = {0.0, 0.0, 0.0};
+    for (int l = 0; l <= kLmaxM; ++l)
+      for (int m = 0; m <= l; ++m) {
+        const C w = Ob[tblinv(l, m)];
+        const C o = omultipole(l, m, s);
+        gq += w.re * o.re - w.im * o.im;
+        for (int k = 0; k < 3; ++k) {
+          const C od = omultipole_deriv(l, m, R, k);
+          gx[k] += w.re * od.re - w.im * od.im;
+        }
+      }
+    if (corr == 1 || corr == 2) {
+      gq += (dbar[0] * R[0] + dbar[1] * R[1]) + dbar[2] * R[2];
+      for (int k = 0; k < 3; ++k) gx[k] += dbar[k];
+    }
+    if (corr == 1) {
+      gq += tbar * ((R[0] * R[0] + R[1] * R[1]) + R[2] * R[2]);
+      for (int k = 0; k < 3; ++k) gx[k] += 2.0 * tbar * R[k];
+    }
+    dq[i] = gq;
+    dx[i] = q[i] * gx[0];
+    dy[i] = q[i] * gx[1];
+    dz[i] = q[i] * gx[2];
+  }
+}
+
 void orc_fmm_set_mlattice(OrcFmm* f, const double* re_im) {
   for (int i = 0; i < kLenT; ++i) f->mlattice[i] = {re_im[2 * i], re_im[2 * i + 1]};
 }

@@ -508,10 +508,6 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
     c->err = "adjoint called without a grown tree";
     return PEPCG_ERR_NO_TREE;
   }
-  if (c->far_field) {
-    c->err = "adjoint of the periodic far-lattice term is not implemented";
-    return PEPCG_ERR_UNSUPPORTED;
-  }
   if (c->prm.force_law != 3) {
     c->err = "the adjoint walk differentiates the 3D Coulomb law only (force_law = 3)";
     return PEPCG_ERR_UNSUPPORTED;
@@ -628,7 +624,10 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
   }
   COUNT_LAUNCH();
   k_adj_out<<<g, 256, 0, s>>>(c->n, c->leafnode.p, c->perm.p, c->q.p, c->adj.p, dq, dx, dy, dz);
-  return cuda_ok(c, cudaGetLastError(), "adjoint") ? PEPCG_OK : PEPCG_ERR_CUDA;
+  if (!cuda_ok(c, cudaGetLastError(), "adjoint")) return PEPCG_ERR_CUDA;
+  // the periodic far-lattice term's adjoint (FP64, lattice.cu) adds to the walk's
+  return c->far_field ? lattice_adjoint(c, nt, tx, ty, tz, gex, gey, gez, gphi, dq, dx, dy, dz)
+                      : PEPCG_OK;
 }
 
 }  // namespace pepcg

@@ -316,6 +316,11 @@ int restore_device(Ctx* c, const double* in, double* out);
 int widen_perm_device(Ctx* c, int64_t* out, cudaStream_t st = nullptr);  // null: c->stream
 int lattice_add(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                 double* ex, double* ey, double* ez, double* pot, bool overwrite);
+// adds the lattice term's dL/dq, dL/dx of the grown particles to dq..dz (the
+// caller's original order) for dL/dE, dL/dphi at nt targets
+int lattice_adjoint(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
+                    const double* gex, const double* gey, const double* gez, const double* gphi,
+                    double* dq, double* dx, double* dy, double* dz);
 
 // ---- direct.cu ----
 int direct_device(Ctx* c, int64_t ntest, const int64_t* d_tidx, double* ex, double* ey,

@@ -5,13 +5,20 @@
 //           the iteration of calc_lattice_coefficients (:154-213).  For a
 //           unit-cube lattice the reference loads a table that was produced by
 //           that same iteration at Lmax_multipole = 50 (:253-259); running it
-//           at 50 here reproduces the table (to ~1e-14) and the first
-//           Lmax_taylor = 40 orders are kept.
+//           at 50 here reproduces the table's entries (to ~1e-14), the first
+//           Lmax_taylor = 40 orders are kept, and the entries the table does
+//           not list (odd l, m not a multiple of 4) are zero as there.
 //  timestep (fmm_framework_timestep, :132-149): box dipole and quadrupole
 //           trace, the central box's multipole expansion omega_tilde (l <= 20,
 //           fictitious charges included) and mu_cent = M2L(MLattice, omega).
 //  add      (fmm_sum_lattice_force, :766-826): per target, O(l <= 20) at the
 //           target, L2L to l <= 1, E and phi, then the extrinsic correction.
+//  adjoint  (no reference counterpart): the transpose of add and timestep for
+//           L = sum_t dL/dphi_t phi_t + dL/dE_t . E_t, giving dL/dq, dL/dx of
+//           the particles: targets -> dL/dmu -> dL/domega (M2L transposed) ->
+//           particles through O_lm(x - center) and its gradient, plus the
+//           fictitious charges' and the Redlack terms' chains through the box
+//           dipole and quadrupole trace.
 // Expansions use the flat layout tblinv(l, m) = l(l+1)/2 + m, m >= 0.
 // Compiled with --fmad=false.
 
@@ -228,10 +235,25 @@ __global__ void k_lattice_iter(int lt, int lm, const double2* __restrict__ ML,
   out[idx] = cadd(t, lstar[idx]);
 }
 
-// keep the first Lmax_taylor orders of a table of order lt
-__global__ void k_truncate(const double2* __restrict__ src, double2* __restrict__ dst) {
+// keep the first Lmax_taylor orders of a table of order lt.  For the unit
+// cube the reference starts from MLattice = 0 and loads only the entries of
+// its table (fmm_framework_prepare, :112-115; load_lattice_coefficients,
+// :260-508): l even and m a multiple of 4, as real numbers.  Every other entry
+// stays zero there -- among them (1, 0) and (1, 1), which the iteration leaves
+// at O(1) values (the conditionally convergent dipole sum) and which would
+// otherwise couple the box dipole into phi -- so the same pattern is applied.
+__global__ void k_truncate(const double2* __restrict__ src, double2* __restrict__ dst,
+                           int unit_cube_table) {
   int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx < kLenT) dst[idx] = src[idx];
+  if (idx >= kLenT) return;
+  double2 v = src[idx];
+  if (unit_cube_table) {
+    int l = 0;
+    while ((l + 1) * (l + 2) / 2 <= idx) ++l;
+    const int m = idx - l * (l + 1) / 2;
+    v = ((l & 1) == 0 && (m & 3) == 0) ? make_double2(v.x, 0.0) : make_double2(0.0, 0.0);
+  }
+  dst[idx] = v;
 }
 
 // box dipole and quadrupole trace (calc_box_dipole, :605-630): block partials
@@ -522,6 +544,350 @@ __global__ void __launch_bounds__(128) k_lattice_force(
   }
 }
 
+// ---- adjoint of the lattice term ----
+//
+// With c00 = dL/dphi, c11 = -dL/dEx + i dL/dEy and c10 = -dL/dEz, one
+// target contributes L_t = Re sum_{j, k} A(j, k) mu(j, k) over |k| <= j <= 20,
+// A(j, k) = c00 O(j, k) + c11 O(j-1, k-1) + c10 O(j-1, k) (the L2L rows
+// l <= 1).  Folding k < 0 onto k > 0 by mu(j, -m) = (-1)^m conj(mu(j, m)) and
+// O(j, -m) = (-1)^m conj(O(j, m)) gives L_t = Re sum_{m >= 0} G(j, m) mu(j, m):
+//   G(j, 0) = c00 O(j, 0) + c10 O(j-1, 0) - c11 conj(O(j-1, 1))
+//   G(j, m) = 2 c00 O(j, m) + 2 c10 O(j-1, m) + c11 O(j-1, m-1)
+//             - conj(c11) O(j-1, m+1)                          (m > 0)
+// Lane m of a warp generates O(j, m) for j = 0..20 by LegendreP's recurrence
+// (as the omega kernel) and takes O(j-1, m -+ 1) from lanes m -+ 1.  The
+// extrinsic correction's adjoints ride along in xa: the fictitious charges'
+// direct terms dL/dq_f (0..3), and for the Redlack form dL/d(dipole) (4..6)
+// and dL/d(trace) (7).
+constexpr int kLatAdjChunk = 1024;
+__global__ void __launch_bounds__(256) k_latadj_targets(
+    int64_t nt, const double* __restrict__ tx, const double* __restrict__ ty,
+    const double* __restrict__ tz, const double* __restrict__ gex, const double* __restrict__ gey,
+    const double* __restrict__ gez, const double* __restrict__ gphi, double cx, double cy,
+    double cz, double prefact, int corr, const double* __restrict__ aux,
+    const double* __restrict__ vbox, int nbox, const double* __restrict__ fact,
+    double2* __restrict__ part, double* __restrict__ xpart) {
+  __shared__ double2 s_acc[kOmWarps][kLenM];
+  __shared__ double s_x[kOmWarps][8];
+  __shared__ double s_aux[32];
+  __shared__ double s_vb[3 * 125];
+  __shared__ double s_fact[2 * kLM + 1];
+  for (int i = threadIdx.x; i < 32; i += blockDim.x) s_aux[i] = aux[i];
+  for (int i = threadIdx.x; i < 3 * nbox; i += blockDim.x) s_vb[i] = vbox[i];
+  for (int i = threadIdx.x; i <= 2 * kLM; i += blockDim.x) s_fact[i] = fact[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int m = lane;
+  const int64_t base = (int64_t)blockIdx.x * kLatAdjChunk;
+  const int cnt = (int)min((int64_t)kLatAdjChunk, nt - base);
+  const int nf = (corr == 2) ? (int)s_aux[4] : 0;
+  const int npair = nf * nbox;
+  double2 acc[kLM + 1];
+#pragma unroll
+  for (int l = 0; l <= kLM; ++l) acc[l] = make_double2(0.0, 0.0);
+  double xa[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = w; i < cnt; i += kOmWarps) {
+    const int64_t t = base + i;
+    const double px = tx[t], py = ty[t], pz = tz[t];
+    const double gp = gphi[t], g0 = gex[t], g1 = gey[t], g2 = gez[t];
+    double sph[3];
+    cart2sph(px - cx, py - cy, pz - cz, sph);
+    const double2 c11 = make_double2(-g0, g1);
+    const double c10 = -g2;
+    const double xc = sph[1];
+    double sn = 0.0, cs = 1.0;
+    double pmm = 1.0;
+    if (m <= kLM) {
+      sincos((double)m * sph[2], &sn, &cs);
+      if (m > 0) {
+        const double somx2 = sqrt((1.0 - xc) * (1.0 + xc));
+        double f = 1.0;
+        for (int k = 1; k <= m; ++k) {
+          pmm = (-pmm * f) * somx2;
+          f = f + 2.0;
+        }
+      }
+    }
+    const double sg = (m & 1) ? -1.0 : 1.0;
+    double pmmp1 = 0.0, rl = 1.0;
+    double2 prev = make_double2(0.0, 0.0);  // O(j - 1, m)
+#pragma unroll
+    for (int j = 0; j <= kLM; ++j) {
+      double2 o = make_double2(0.0, 0.0);
+      if (j >= m) {
+        double P;
+        if (j == m) {
+          P = pmm;
+        } else if (j == m + 1) {
+          pmmp1 = (xc * (2.0 * m + 1.0)) * pmm;
+          P = pmmp1;
+        } else {
+          const double pll =
+              ((xc * (2.0 * j - 1.0)) * pmmp1 - ((double)(j + m) - 1.0) * pmm) / (double)(j - m);
+          pmm = pmmp1;
+          pmmp1 = pll;
+          P = pll;
+        }
+        const double pt = (sg * P) / s_fact[j + m];
+        const double amp = (sph[0] > 0.0 || j > 0) ? rl * pt : pt;
+        o = make_double2(amp * cs, amp * -sn);
+      }
+      rl = rl * sph[0];
+      double2 lo, hi;  // O(j - 1, m - 1) and O(j - 1, m + 1)
+      lo.x = __shfl_up_sync(0xffffffffu, prev.x, 1);
+      lo.y = __shfl_up_sync(0xffffffffu, prev.y, 1);
+      hi.x = __shfl_down_sync(0xffffffffu, prev.x, 1);
+      hi.y = __shfl_down_sync(0xffffffffu, prev.y, 1);
+      if (m == 31) hi = make_double2(0.0, 0.0);
+      const double2 hic = make_double2(hi.x, -hi.y);
+      double2 g;
+      if (m == 0) {
+        const double2 a = cmul(c11, hic);
+        g = make_double2((gp * o.x + c10 * prev.x) - a.x, (gp * o.y + c10 * prev.y) - a.y);
+      } else {
+        const double2 a = cmul(c11, lo);
+        const double2 b = cmul(make_double2(c11.x, -c11.y), hi);
+        g = make_double2(((2.0 * gp) * o.x + (2.0 * c10) * prev.x) + (a.x - b.x),
+                         ((2.0 * gp) * o.y + (2.0 * c10) * prev.y) + (a.y - b.y));
+      }
+      acc[j] = cadd(acc[j], g);
+      prev = o;
+    }
+    if (corr == 1 && lane == 0) {
+      const double R[3] = {px - cx, py - cy, pz - cz};
+      const double ge[3] = {g0, g1, g2};
+      for (int d = 0; d < 3; ++d) xa[4 + d] += (2.0 * prefact) * ge[d] - ((2.0 * prefact) * gp) * R[d];
+      xa[7] += prefact * gp;
+    }
+    for (int k = lane; k < npair; k += 32) {
+      const int p = k / nbox, ib = k - p * nbox;
+      const double d0 = (px - s_vb[3 * ib]) - s_aux[8 + 4 * p];
+      const double d1 = (py - s_vb[3 * ib + 1]) - s_aux[9 + 4 * p];
+      const double d2 = (pz - s_vb[3 * ib + 2]) - s_aux[10 + 4 * p];
+      const double rd = 1.0 / sqrt((d0 * d0 + d1 * d1) + d2 * d2);
+      const double v = gp * rd + ((rd * rd) * rd) * ((g0 * d0 + g1 * d1) + g2 * d2);
+      if (p == 0) xa[0] += v;
+      else if (p == 1) xa[1] += v;
+      else if (p == 2) xa[2] += v;
+      else xa[3] += v;
+    }
+  }
+#pragma unroll
+  for (int l = 0; l <= kLM; ++l)
+    if (m <= l) s_acc[w][tblinv(l, m)] = acc[l];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    double v = xa[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) s_x[w][k] = v;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < kLenM; idx += blockDim.x) {
+    double2 t = s_acc[0][idx];
+    for (int ww = 1; ww < kOmWarps; ++ww) t = cadd(t, s_acc[ww][idx]);
+    part[(int64_t)blockIdx.x * kLenM + idx] = t;
+  }
+  if (threadIdx.x < 8) {
+    double v = s_x[0][threadIdx.x];
+    for (int ww = 1; ww < kOmWarps; ++ww) v += s_x[ww][threadIdx.x];
+    xpart[(int64_t)blockIdx.x * 8 + threadIdx.x] = v;
+  }
+}
+
+struct LatAdjGeom {
+  int per[3];
+  double len[3];  // |t_lattice_p|
+  double cx, cy, cz;
+  int corr;
+};
+
+// One block: G = sum of the partials (block order); dL/domega = the M2L
+// transpose of G, B(j, k) = (-1)^j sum_{l, m >= 0} G(l, m) ML(j + l, k + m),
+// folded onto k >= 0, and zero at (0, 0).  Then
+// the fictitious charges: dL/dq_f = the direct terms + Re sum dL/domega O(x_f
+// - c), and q_p = -d_p / |L_p|, q_last = -sum q_p give dL/d(dipole).  The
+// output coef holds dL/domega and the gradient tables Dx, Dy, Dz with
+// Re sum_{a, b >= 0} D(a, b) O(a, b) = d/dx Re sum dL/domega(l, m) O(l, m),
+// from the ladder relations d/dz O(l, m) = O(l-1, m) and (d/dx +- i d/dy)
+// O(l, m) = +-O(l-1, m-+1):
+//   Dx(a, b) = (W(a+1, b+1) - W(a+1, b-1) - [b = 1] conj(W(a+1, 0))) / 2
+//   Dy(a, b) = -i (W(a+1, b+1) + W(a+1, b-1) + [b = 1] conj(W(a+1, 0))) / 2
+//   Dz(a, b) = W(a+1, b)        (W(a+1, -1) read as 0), then dL/d(dipole)
+// and dL/d(trace) in coef[4 kLenM ..].
+__global__ void __launch_bounds__(256) k_latadj_final(int nparts, const double2* __restrict__ part,
+                                                      const double* __restrict__ xpart,
+                                                      const double2* __restrict__ ML,
+                                                      const double* __restrict__ aux,
+                                                      LatAdjGeom geo, const double* fact,
+                                                      double2* __restrict__ coef) {
+  __shared__ double2 s_G[kLenM], s_W[kLenM];
+  __shared__ double s_X[8], s_qf[4];
+  const int idx = threadIdx.x;
+  if (idx < kLenM) {
+    double2 t = make_double2(0.0, 0.0);
+    for (int b = 0; b < nparts; ++b) t = cadd(t, part[(int64_t)b * kLenM + idx]);
+    s_G[idx] = t;
+  }
+  if (idx < 8) {
+    double v = 0.0;
+    for (int b = 0; b < nparts; ++b) v += xpart[(int64_t)b * 8 + idx];
+    s_X[idx] = v;
+  }
+  __syncthreads();
+  int j = 0, m = 0;
+  if (idx < kLenM) {
+    while ((j + 1) * (j + 2) / 2 <= idx) ++j;
+    m = idx - j * (j + 1) / 2;
+    const double sj = (j & 1) ? -1.0 : 1.0;
+    double2 b = make_double2(0.0, 0.0), bn = make_double2(0.0, 0.0);
+    for (int l = 0; l <= kLM; ++l)
+      for (int mm = 0; mm <= l; ++mm) {
+        const double2 g = s_G[tblinv(l, mm)];
+        const double2 a = tbl(ML, j + l, m + mm, kLT);
+        b = cadd(b, cmul(g, make_double2(sj * a.x, sj * a.y)));
+        if (m > 0) {
+          const double2 an = tbl(ML, j + l, mm - m, kLT);
+          bn = cadd(bn, cmul(g, make_double2(sj * an.x, sj * an.y)));
+        }
+      }
+    if (m > 0) {
+      const double s = (m & 1) ? -1.0 : 1.0;
+      b = cadd(b, make_double2(s * bn.x, -s * bn.y));
+    }
+    // omega(0, 0) never reaches mu (removed, or exactly zero with every
+    // change of a charge making it removed): its adjoint is zero, which also
+    // keeps the divergent ML(0, 0) (~1e32 in the unit-cube table) out of the
+    // fictitious charges' difference below
+    if (idx == 0) b = make_double2(0.0, 0.0);
+    s_W[idx] = b;
+    coef[idx] = b;
+  }
+  __syncthreads();
+  const int nf = (geo.corr == 2) ? (int)aux[4] : 0;
+  if (idx < nf) {
+    double s[3];
+    cart2sph(aux[8 + 4 * idx] - geo.cx, aux[9 + 4 * idx] - geo.cy, aux[10 + 4 * idx] - geo.cz, s);
+    double v = s_X[idx];
+    for (int l = 0; l <= kLM; ++l)
+      for (int mm = 0; mm <= l; ++mm) {
+        const double2 o = omultipole(l, mm, s, fact), wv = s_W[tblinv(l, mm)];
+        v += wv.x * o.x - wv.y * o.y;
+      }
+    s_qf[idx] = v;
+  }
+  __syncthreads();
+  if (idx == 0) {
+    double db[3] = {0.0, 0.0, 0.0}, tb = 0.0;
+    if (geo.corr == 1) {
+      for (int d = 0; d < 3; ++d) db[d] = s_X[4 + d];
+      tb = s_X[7];
+    } else if (geo.corr == 2) {
+      const double qlast = s_qf[nf - 1];
+      int ip = 0;
+      for (int p = 0; p < 3; ++p) {
+        if (!geo.per[p]) continue;
+        db[p] = (qlast - s_qf[ip]) / geo.len[p];
+        ++ip;
+      }
+    }
+    coef[4 * kLenM] = make_double2(db[0], db[1]);
+    coef[4 * kLenM + 1] = make_double2(db[2], tb);
+  }
+  if (idx < kLenM) {
+    const int a = j, bb = m;
+    double2 dxv = make_double2(0.0, 0.0), dyv = dxv, dzv = dxv;
+    if (a < kLM) {
+      const double2 up = s_W[tblinv(a + 1, bb + 1)];
+      const double2 dn = (bb >= 1) ? s_W[tblinv(a + 1, bb - 1)] : make_double2(0.0, 0.0);
+      double2 ex = make_double2(0.0, 0.0);
+      if (bb == 1) ex = make_double2(s_W[tblinv(a + 1, 0)].x, -s_W[tblinv(a + 1, 0)].y);
+      const double2 sx = make_double2((up.x - dn.x) - ex.x, (up.y - dn.y) - ex.y);
+      const double2 sy = make_double2((up.x + dn.x) + ex.x, (up.y + dn.y) + ex.y);
+      dxv = make_double2(0.5 * sx.x, 0.5 * sx.y);
+      dyv = make_double2(0.5 * sy.y, -0.5 * sy.x);  // -i sy / 2
+      dzv = s_W[tblinv(a + 1, bb)];
+    }
+    coef[kLenM + idx] = dxv;
+    coef[2 * kLenM + idx] = dyv;
+    coef[3 * kLenM + idx] = dzv;
+  }
+}
+
+// per particle (key order): dL/dq = Re sum W O(x - c) + dipole-bar . R +
+// trace-bar |R|^2, dL/dx = q (Re sum D O + dipole-bar + 2 trace-bar R), added
+// at the caller's original index perm[i]
+__global__ void __launch_bounds__(128) k_latadj_particles(
+    int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+    const double* __restrict__ z, const double* __restrict__ q, const int32_t* __restrict__ perm,
+    const double2* __restrict__ coef, double cx, double cy, double cz,
+    const double* __restrict__ fact, double* dq, double* dx, double* dy, double* dz) {
+  __shared__ double2 s_c[4 * kLenM + 2];
+  __shared__ double s_fact[2 * kLM + 1];
+  for (int i = threadIdx.x; i < 4 * kLenM + 2; i += blockDim.x) s_c[i] = coef[i];
+  for (int i = threadIdx.x; i <= 2 * kLM; i += blockDim.x) s_fact[i] = fact[i];
+  __syncthreads();
+  const double db0 = s_c[4 * kLenM].x, db1 = s_c[4 * kLenM].y, db2 = s_c[4 * kLenM + 1].x;
+  const double tb = s_c[4 * kLenM + 1].y;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double R0 = x[i] - cx, R1 = y[i] - cy, R2 = z[i] - cz;
+    double s[3];
+    cart2sph(R0, R1, R2, s);
+    double gq = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0;
+    for (int m = 0; m <= kLM; ++m) {
+      double sn, cs;
+      sincos((double)m * s[2], &sn, &cs);
+      const double sg = (m & 1) ? -1.0 : 1.0;
+      const double xc = s[1];
+      double pmm = 1.0;
+      if (m > 0) {
+        const double somx2 = sqrt((1.0 - xc) * (1.0 + xc));
+        double f = 1.0;
+        for (int k = 1; k <= m; ++k) {
+          pmm = (-pmm * f) * somx2;
+          f = f + 2.0;
+        }
+      }
+      double rl = 1.0;
+      for (int k = 0; k < m; ++k) rl = rl * s[0];
+      double pmmp1 = 0.0;
+      for (int a = m; a <= kLM; ++a) {
+        double P;
+        if (a == m) {
+          P = pmm;
+        } else if (a == m + 1) {
+          pmmp1 = (xc * (2.0 * m + 1.0)) * pmm;
+          P = pmmp1;
+        } else {
+          const double pll =
+              ((xc * (2.0 * a - 1.0)) * pmmp1 - ((double)(a + m) - 1.0) * pmm) / (double)(a - m);
+          pmm = pmmp1;
+          pmmp1 = pll;
+          P = pll;
+        }
+        const double pt = (sg * P) / s_fact[a + m];
+        const double amp = (s[0] > 0.0 || a > 0) ? rl * pt : pt;
+        rl = rl * s[0];
+        const double ox = amp * cs, oy = amp * -sn;
+        const int t = tblinv(a, m);
+        const double2 wv = s_c[t], ax = s_c[kLenM + t], ay = s_c[2 * kLenM + t],
+                      az = s_c[3 * kLenM + t];
+        gq += wv.x * ox - wv.y * oy;
+        g0 += ax.x * ox - ax.y * oy;
+        g1 += ay.x * ox - ay.y * oy;
+        g2 += az.x * ox - az.y * oy;
+      }
+    }
+    gq += ((db0 * R0 + db1 * R1) + db2 * R2) + tb * ((R0 * R0 + R1 * R1) + R2 * R2);
+    const double qi = q[i];
+    const int64_t o = perm[i];
+    dq[o] += gq;
+    dx[o] += qi * ((g0 + db0) + (2.0 * tb) * R0);
+    dy[o] += qi * ((g1 + db1) + (2.0 * tb) * R1);
+    dz[o] += qi * ((g2 + db2) + (2.0 * tb) * R2);
+  }
+}
+
 double host_factorial(int n) {  // factorial, :1247-1314 (the exact values to 24!, gamma above)
   static const double f[25] = {1.0, 1.0, 2.0, 6.0, 24.0, 120.0, 720.0, 5040.0, 40320.0,
                                362880.0, 3628800.0, 39916800.0, 479001600.0, 6227020800.0,
@@ -585,7 +951,7 @@ int lattice_prepare(Ctx* c) {
       std::swap(ml0, ml1);
     }
     COUNT_LAUNCH();
-    k_truncate<<<(kLenT + 127) / 128, 128, 0, s>>>(ml0, c->d_mlattice);
+    k_truncate<<<(kLenT + 127) / 128, 128, 0, s>>>(ml0, c->d_mlattice, lm == kLMTable ? 1 : 0);
     ok = cuda_ok(c, cudaGetLastError(), "lattice coefficients") &&
          cuda_ok(c, cudaStreamSynchronize(s), "lattice coefficients");
   }
@@ -662,6 +1028,67 @@ int lattice_add(Ctx* c, int64_t nt, const double* tx, const double* ty, const do
                                          cx, cy, cz, volume, p.fmm_extrinsic_correction,
                                          c->d_factorial, ex, ey, ez, pot, overwrite ? 1 : 0);
   return cuda_ok(c, cudaGetLastError(), "lattice force") ? PEPCG_OK : PEPCG_ERR_CUDA;
+}
+
+int lattice_adjoint(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
+                    const double* gex, const double* gey, const double* gez, const double* gphi,
+                    double* dq, double* dx, double* dy, double* dz) {
+  const pepcg_params& p = c->prm;
+  cudaStream_t s = c->stream;
+  LatAdjGeom geo;
+  geo.cx = 0.5 * ((p.t_lattice_1[0] + p.t_lattice_2[0]) + p.t_lattice_3[0]) + p.lattice_origin[0];
+  geo.cy = 0.5 * ((p.t_lattice_1[1] + p.t_lattice_2[1]) + p.t_lattice_3[1]) + p.lattice_origin[1];
+  geo.cz = 0.5 * ((p.t_lattice_1[2] + p.t_lattice_2[2]) + p.t_lattice_3[2]) + p.lattice_origin[2];
+  const double* lv[3] = {p.t_lattice_1, p.t_lattice_2, p.t_lattice_3};
+  for (int d = 0; d < 3; ++d) {
+    geo.per[d] = p.periodicity[d];
+    geo.len[d] = std::sqrt((lv[d][0] * lv[d][0] + lv[d][1] * lv[d][1]) + lv[d][2] * lv[d][2]);
+  }
+  geo.corr = p.fmm_extrinsic_correction;
+  const double* a = p.t_lattice_1;
+  const double* b = p.t_lattice_2;
+  const double* cc = p.t_lattice_3;
+  double cr[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+  const double volume = std::fabs((cr[0] * cc[0] + cr[1] * cc[1]) + cr[2] * cc[2]);
+  const double prefact = (2.0 * std::acos(-1.0)) / (3.0 * volume);
+  const int64_t nparts = nt > 0 ? (nt + kLatAdjChunk - 1) / kLatAdjChunk : 1;
+  double2* part = nullptr;
+  double* xpart = nullptr;
+  double2* coef = nullptr;
+  bool ok = cuda_ok(c, cudaMallocAsync((void**)&part, nparts * kLenM * 16, s), "lattice adjoint") &&
+            cuda_ok(c, cudaMallocAsync((void**)&xpart, nparts * 8 * 8, s), "lattice adjoint") &&
+            cuda_ok(c, cudaMallocAsync((void**)&coef, (4 * kLenM + 2) * 16, s), "lattice adjoint");
+  if (!ok) {
+    for (void* v : {(void*)part, (void*)xpart, (void*)coef})
+      if (v) cudaFreeAsync(v, s);
+    return PEPCG_ERR_OOM;
+  }
+  if (nt > 0) {
+    COUNT_LAUNCH();
+    k_latadj_targets<<<(unsigned)nparts, 256, 0, s>>>(nt, tx, ty, tz, gex, gey, gez, gphi, geo.cx,
+                                                      geo.cy, geo.cz, prefact, geo.corr,
+                                                      c->d_fmm_aux, c->d_vbox, c->nboxes,
+                                                      c->d_factorial, part, xpart);
+  } else {
+    cudaMemsetAsync(part, 0, kLenM * 16, s);
+    cudaMemsetAsync(xpart, 0, 8 * 8, s);
+  }
+  COUNT_LAUNCH();
+  k_latadj_final<<<1, 256, 0, s>>>((int)nparts, part, xpart, c->d_mlattice, c->d_fmm_aux, geo,
+                                   c->d_factorial, coef);
+  const int64_t n = c->n;
+  unsigned blocks = (unsigned)((n + 127) / 128);
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  if (blocks == 0) blocks = 1;
+  COUNT_LAUNCH();
+  k_latadj_particles<<<blocks, 128, 0, s>>>(n, c->x.p, c->y.p, c->z.p, c->q.p, c->perm.p, coef,
+                                            geo.cx, geo.cy, geo.cz, c->d_factorial, dq, dx, dy,
+                                            dz);
+  ok = cuda_ok(c, cudaGetLastError(), "lattice adjoint");
+  cudaFreeAsync(part, s);
+  cudaFreeAsync(xpart, s);
+  cudaFreeAsync(coef, s);
+  return ok ? PEPCG_OK : PEPCG_ERR_CUDA;
 }
 
 }  // namespace pepcg

@@ -7,11 +7,16 @@ Checks, all in FP64:
   * against central finite differences of the GPU forward pass (h = 1e-6,
     the whole grow + traverse re-run per point): relative 1e-5, allowing a
     coordinate whose perturbation flips a MAC decision or a key;
+  * periodic boundaries with the FMM lattice term (each extrinsic
+    correction): against the oracle, whose lattice adjoint differentiates the
+    harmonics independently, and FD;
   * the adjoint configuration -- 262,144 sources U[0,1)^3 with q ~ N(0,1),
     4,096 probes U[0.25,0.75]^3, L = sum (phi - phi_target)^2 with
     phi_target from a second charge set, theta = 0.4, eps = 1e-3 -- against
     the FP64 direct-sum gradient (tree-code accuracy) and FD on 64 random
     coordinates."""
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -20,6 +25,7 @@ import pepc_b200 as P
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_pins.npz"))
 
 
 def forward_L(x, y, z, q, tx, ty, tz, gphi, gE, **kw):
@@ -198,15 +204,101 @@ def test_autograd_harness_against_torch_direct_gradient(gpu):
     tc.close()
 
 
-def test_adjoint_rejects_periodic_far_field(gpu):
-    rng = np.random.default_rng(5)
-    x, y, z = rng.random(200), rng.random(200), rng.random(200)
-    q = np.where(np.arange(200) % 2 == 0, 1.0, -1.0)
-    tc = P.TreeCode(periodicity=(1, 1, 1))
-    tc.pepc_grow_tree(x, y, z, q)
-    with pytest.raises(P.PepcgError) as ei:
-        tc.traverse_adjoint(x[:5], y[:5], z[:5], [np.zeros(5)] * 3, np.ones(5), 200)
-    assert ei.value.code == P.PEPCG_ERR_UNSUPPORTED
+def periodic_problem(n, nt, seed, neutral):
+    rng = np.random.default_rng(seed)
+    x, y, z = rng.random(n), rng.random(n), rng.random(n)
+    q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0) if neutral else rng.standard_normal(n)
+    tx, ty, tz = rng.random(nt), rng.random(nt), rng.random(nt)
+    gphi = rng.standard_normal(nt)
+    gE = [rng.standard_normal(nt) for _ in range(3)]
+    return x, y, z, q, tx, ty, tz, gphi, gE, rng
+
+
+@pytest.mark.parametrize("corr,neutral", [(0, False), (1, False), (2, False), (2, True)])
+def test_periodic_far_field_adjoint_matches_oracle_and_fd(gpu, corr, neutral):
+    """27 mirror boxes plus the FMM lattice term, for each extrinsic correction
+    (0 none, 1 Redlack, 2 fictitious charges), with the monopole removed
+    (random charges) or exactly zero (a neutral box): the GPU adjoint -- walk plus the
+    lattice term's transpose -- against the oracle's (whose lattice part
+    differentiates the harmonics by dual numbers, not by the ladder relations
+    the GPU uses) to 1e-9 of the gradient's scale, and against central FD of
+    the GPU forward pass (relative 1e-5, one MAC flip allowed)."""
+    x, y, z, q, tx, ty, tz, gphi, gE, rng = periodic_problem(2000, 60, 90 + corr, neutral)
+    kw = dict(theta2=0.16, eps2=1e-3, periodicity=(1, 1, 1), fmm_extrinsic_correction=corr)
+    grads = {}
+    for ff in (0, 1):
+        tc = P.TreeCode(precision=P.PRECISION_PLAIN, walk=P.WALK_PER_TARGET,
+                        include_far_field_if_periodic=ff, **kw)
+        tc.pepc_grow_tree(x, y, z, q)
+        if ff:
+            assert (tc.last_status == P.PEPCG_WARN_NOT_NEUTRAL) == (not neutral)
+        g = tc.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
+        orc = O.Oracle(walk=0, num_threads=8, include_far_field_if_periodic=ff, **kw)
+        if ff:
+            orc.set_lattice_coefficients(O.reference_lattice_table(GOLD))
+        orc.grow_tree(x, y, z, q)
+        go = orc.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
+        orc.close()
+        grads[ff] = (g, go)
+        if not ff:
+            tc.close()
+    g, go = grads[1]
+    for k in ("q", "x", "y", "z"):
+        scale = np.abs(go[k]).max()
+        assert np.abs(g[k] - go[k]).max() <= 1e-9 * scale, k
+        # the lattice term's own part (far minus near field), to its own scale
+        lat, olat = g[k] - grads[0][0][k], go[k] - grads[0][1][k]
+        assert np.abs(olat).max() > 0.0, k
+        assert np.abs(lat - olat).max() <= 1e-9 * np.abs(olat).max(), k
+
+    def L(a):
+        tc.pepc_grow_tree(a["x"], a["y"], a["z"], a["q"])
+        r = tc.pepc_traverse_tree(tx, ty, tz)
+        return float(np.sum(gphi * r["pot"] + gE[0] * r["ex"] + gE[1] * r["ey"] + gE[2] * r["ez"]))
+
+    h = 1e-6
+    bad = 0
+    # a charge perturbed in a neutral box makes it non-neutral and the forward
+    # removes the monopole: dL/dq is that (one-sided and FD) derivative
+    for trial in range(12):
+        j = int(rng.integers(len(x)))
+        key = "xyzq"[trial % 4]
+        arrs = {"x": x, "y": y, "z": z, "q": q}
+        plus = {k: (v.copy() if k == key else v) for k, v in arrs.items()}
+        minus = {k: (v.copy() if k == key else v) for k, v in arrs.items()}
+        plus[key][j] += h
+        minus[key][j] -= h
+        fd = (L(plus) - L(minus)) / (2 * h)
+        an = g[key][j]
+        if abs(fd - an) > 1e-5 * max(abs(fd), abs(an), 1e-8):
+            bad += 1
+    assert bad <= 1, bad
+    tc.close()
+
+
+def test_periodic_far_field_adjoint_mixed_walk(gpu):
+    # the benchmark's walk (mixed, 64-target buckets) with the lattice term:
+    # its adjoint against the FP64 adjoint of the same bucket walk
+    x, y, z, q, tx, ty, tz, gphi, gE, rng = periodic_problem(20000, 2000, 95, True)
+    kw = dict(theta2=0.16, eps2=1e-4, walk=P.WALK_GROUP, group_size=64, periodicity=(1, 1, 1))
+    out = {}
+    for prec in (P.PRECISION_PLAIN, P.PRECISION_MIXED):
+        tc = P.TreeCode(precision=prec, **kw)
+        tc.pepc_grow_tree(x, y, z, q)
+        out[prec] = tc.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
+        tc.close()
+    # without the lattice term the gradient is measurably different
+    tn = P.TreeCode(precision=P.PRECISION_PLAIN, include_far_field_if_periodic=0, **kw)
+    tn.pepc_grow_tree(x, y, z, q)
+    near = tn.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
+    tn.close()
+    for k in ("q", "x", "y", "z"):
+        a, b = out[P.PRECISION_MIXED][k], out[P.PRECISION_PLAIN][k]
+        rel = np.abs(a - b) / np.abs(b).max()
+        assert np.median(rel) < 1e-6, (k, np.median(rel))
+        assert np.percentile(rel, 99) < 1e-4, (k, np.percentile(rel, 99))
+        # the lattice term is present: the near-field-only gradient differs
+        assert np.abs(b - near[k]).max() > 1e-6 * np.abs(b).max(), k
 
 
 @pytest.mark.parametrize("with_e", [False, True])

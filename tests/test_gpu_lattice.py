@@ -43,6 +43,32 @@ def test_lattice_term_matches_oracle(gpu):
         assert np.abs(a[k] - b[k]).max() <= 1e-11 * scale, k
 
 
+@pytest.mark.parametrize("corr", [0, 1, 2])
+def test_lattice_term_each_correction_dipolar_box(gpu, corr):
+    # random charges: a non-neutral box (monopole removed) with a dipole.
+    # With the fictitious charges (2) the dipole is cancelled; without (0) or
+    # with the Redlack terms (1) it couples to MLattice(1, m), which the
+    # reference's unit-cube table holds at zero
+    rng = np.random.default_rng(53 + corr)
+    n = 3000
+    x, y, z = rng.random(n), rng.random(n), rng.random(n)
+    q = rng.standard_normal(n)
+    tc = P.TreeCode(theta2=0.16, eps2=0.0, periodicity=(1, 1, 1), fmm_extrinsic_correction=corr)
+    orc = O.Oracle(theta2=0.16, eps2=0.0, periodicity=(1, 1, 1), fmm_extrinsic_correction=corr,
+                   num_threads=8)
+    orc.set_lattice_coefficients(O.reference_lattice_table(GOLD))
+    tc.pepc_grow_tree(x, y, z, q)
+    assert tc.last_status == P.PEPCG_WARN_NOT_NEUTRAL
+    orc.grow_tree(x, y, z, q)
+    px, py, pz = rng.random(500), rng.random(500), rng.random(500)
+    a, b = tc.lattice(px, py, pz), orc.lattice(px, py, pz)
+    for k in ("ex", "ey", "ez", "pot"):
+        scale = np.abs(b[k]).max()
+        assert np.abs(a[k] - b[k]).max() <= 1e-11 * scale, k
+    tc.close()
+    orc.close()
+
+
 def test_periodic_traverse_matches_oracle(gpu):
     rng = np.random.default_rng(52)
     x, y, z, q = rocksalt(10)

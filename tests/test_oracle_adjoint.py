@@ -4,7 +4,10 @@ gradient (orc_direct_adjoint) against central finite differences.
 The tree adjoint is the exact derivative of the tree-code fields with the
 interaction lists held fixed, so FD of the oracle's forward walk agrees with
 it to FD accuracy wherever a perturbation flips no MAC decision; the direct
-gradient is checked against FD of a numpy direct sum."""
+gradient is checked against FD of a numpy direct sum.  With periodic
+boundaries and the FMM lattice term (each extrinsic correction) the adjoint
+adds the lattice term's transpose, whose harmonic gradients come from dual
+numbers; checked against FD of the oracle's full periodic forward pass."""
 import numpy as np
 import pytest
 
@@ -82,3 +85,45 @@ def test_oracle_adjoint_close_to_direct_gradient():
     for k in ("q", "x", "y", "z"):
         rel = np.abs(gt[k] - gd[k]) / np.abs(gd[k]).max()
         assert np.median(rel) < 1e-3, (k, np.median(rel))
+
+
+@pytest.mark.parametrize("corr,neutral", [(0, False), (1, False), (2, False), (2, True)])
+def test_oracle_periodic_far_field_adjoint_against_fd(corr, neutral):
+    # a neutral box keeps omega(0, 0) = 0; perturbing a charge there removes
+    # the monopole, and the adjoint gives that (FD) derivative
+    rng = np.random.default_rng(3)
+    n, nt = 300, 20
+    x, y, z = rng.random(n), rng.random(n), rng.random(n)
+    q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0) if neutral else rng.standard_normal(n)
+    tx, ty, tz = (rng.random(nt) for _ in range(3))
+    gphi = rng.standard_normal(nt)
+    gE = [rng.standard_normal(nt) for _ in range(3)]
+    kw = dict(theta2=0.16, eps2=1e-3, periodicity=(1, 1, 1), fmm_extrinsic_correction=corr,
+              num_threads=8)
+    o = O.Oracle(**kw)
+    o.grow_tree(x, y, z, q)
+    g = o.traverse_adjoint(tx, ty, tz, gE, gphi, n)
+    near = O.Oracle(include_far_field_if_periodic=0, **kw)
+    near.grow_tree(x, y, z, q)
+    gn = near.traverse_adjoint(tx, ty, tz, gE, gphi, n)
+    near.close()
+
+    def L(a):
+        o.grow_tree(a["x"], a["y"], a["z"], a["q"])
+        r = o.traverse_tree(tx, ty, tz)
+        return float(np.sum(gphi * r["pot"] + gE[0] * r["ex"] + gE[1] * r["ey"] + gE[2] * r["ez"]))
+
+    h = 1e-6
+    for trial in range(12):
+        j = int(rng.integers(n))
+        key = "xyzq"[trial % 4]
+        arrs = {"x": x, "y": y, "z": z, "q": q}
+        plus = {k: (v.copy() if k == key else v) for k, v in arrs.items()}
+        minus = {k: (v.copy() if k == key else v) for k, v in arrs.items()}
+        plus[key][j] += h
+        minus[key][j] -= h
+        fd = (L(plus) - L(minus)) / (2 * h)
+        assert abs(fd - g[key][j]) <= 1e-6 * max(abs(fd), 1e-6), (key, j, fd, g[key][j])
+        # the lattice term contributes to this coordinate
+        assert g[key][j] != gn[key][j]
+    o.close()
