@@ -874,7 +874,7 @@ __global__ void __launch_bounds__(256) k_level_scatter(int64_t M, const int2* __
     LevelRecord r;
     r.pos = a;
     r.ab = make_double2(fabs(a.w), 0.0);
-    r.pad[0] = r.pad[1] = 0;
+    r.link = make_int4(0, L | kLeafFlag, 1, (int)u);
     drec[p] = r;
   }
 }
@@ -902,9 +902,9 @@ constexpr int kUpThreads = 128;
 __global__ void __launch_bounds__(kUpThreads) k_upward_level(
     int level, const int32_t* __restrict__ lvl, const int32_t* __restrict__ twiglist,
     const int2* __restrict__ tinfo, const int32_t* __restrict__ cfirst,
-    const int32_t* __restrict__ tfirst, LevelRecord* __restrict__ drec,
-    double* __restrict__ dmom, double4* __restrict__ nc4, double* __restrict__ mom,
-    float4* __restrict__ mom32) {
+    const int32_t* __restrict__ tfirst, const int32_t* __restrict__ nleaves,
+    LevelRecord* __restrict__ drec, double* __restrict__ dmom, double4* __restrict__ nc4,
+    double* __restrict__ mom, float4* __restrict__ mom32) {
   const int cnt = lvl[level];
   const int base = level_base(lvl, level);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
@@ -984,7 +984,7 @@ __global__ void __launch_bounds__(kUpThreads) k_upward_level(
     LevelRecord r;
     r.pos = c4;
     r.ab = make_double2(absq, bmax);
-    r.pad[0] = r.pad[1] = 0;
+    r.link = make_int4(cs, level | (nc << 16), nleaves[u], (int)u);
     drec[pu] = r;
     double2* o = reinterpret_cast<double2*>(mom + kMomStride * u);
     o[0] = make_double2(d0, d1);
@@ -1262,7 +1262,7 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
       if (cnt <= 0) continue;
       COUNT_LAUNCH();
       k_upward_level<<<grid_for(cnt, kUpThreads), kUpThreads, 0, s>>>(
-          L, c->lvlcnt.p, c->twiglist.p, c->tinfo.p, cc, tcn, c->drec.p, c->dmom.p, c->nc4.p,
+          L, c->lvlcnt.p, c->twiglist.p, c->tinfo.p, cc, tcn, c->nleaves.p, c->drec.p, c->dmom.p, c->nc4.p,
           c->mom.p, m32);
     }
   }

@@ -67,12 +67,18 @@ constexpr int kMomAbs = 9;
 constexpr int kMomBmax = 10;
 constexpr int kMom32Stride = 4;
 
-// The upward pass's level-ordered copy of a node: centre and charge and
-// (abs_charge, bmax), padded to 64 bytes.
+// The upward pass's level-ordered copy of a node: centre and charge,
+// (abs_charge, bmax), and the links by which the 64-target group walk
+// traverses the tree in this order (a twig's children are consecutive here):
+//   link.x  level-order position of child slot 0 (twigs; 0 for leaves)
+//   link.y  level | leaf flag << 8 | number of children << 16
+//   link.z  leaves below the node (1 for a leaf)
+//   link.w  the node's RPO index (moments, MAC thresholds)
+// 64 bytes, two whole sectors.
 struct __align__(16) LevelRecord {
   double4 pos;
   double2 ab;
-  double pad[2];
+  int4 link;
 };
 
 struct Ctx {

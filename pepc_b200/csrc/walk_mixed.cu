@@ -44,6 +44,7 @@ struct MixArgs {
   const int2* meta;
   const float4* mom32;  // kMom32Stride float4 per node, the first 3 used
   const int32_t* nleaves;
+  const LevelRecord* drec;  // level-ordered node records with walk links (grow.cu)
   const double* bl2;
   const double* macb;  // per-twig MAC threshold, or nullptr: bl2 of the level (Barnes-Hut)
   const double* vbox;
@@ -518,8 +519,7 @@ __global__ void __launch_bounds__(kMixThreads, 5)
 // carry the FP64 node centre; four blocks per SM (128 registers).
 template <bool kStrict>
 __global__ void __launch_bounds__(kMixThreads, kStrict ? 4 : 5)
-    k_walk_group64(MixArgs A, int* __restrict__ gstack, const int4* __restrict__ child8,
-                   const int* __restrict__ nchild) {
+    k_walk_group64(MixArgs A, int* __restrict__ gstack) {
   using TwigRec = typename std::conditional<kStrict, StagedTwigS, StagedTwig>::type;
   __shared__ float s_bl2[kMaxLevel + 1];
   __shared__ double s_bl2d[kStrict ? kMaxLevel + 1 : 1];
@@ -772,22 +772,25 @@ __global__ void __launch_bounds__(kMixThreads, kStrict ? 4 : 5)
         float cx = 0.f, cy = 0.f, cz = 0.f, bl = 0.f;
         double bld = 0.0;  // the strict form's FP64 MAC threshold
         double4 a = make_double4(0, 0, 0, 0);
-        int nlv = 0, nch = 0;
-        int4 c0 = make_int4(0, 0, 0, 0), c1 = c0;
+        // the node's level-ordered record: centre and charge, then its links
+        // (first child, level | leaf flag | child count, leaves, RPO index);
+        // siblings are consecutive, so one round's loads are mostly runs
+        int4 lk = make_int4(0, 0, 0, 0);
         if (node >= 0) {
-          a = A.nc4[node];
-          const int2 mu = A.meta[node];
+          const LevelRecord* rec = A.drec + node;
+          a = rec->pos;
+          lk = rec->link;
           cx = (float)(a.x - gx); cy = (float)(a.y - gy); cz = (float)(a.z - gz);
-          if (mu.y & kLeafFlag) {
+          if (lk.y & kLeafFlag) {
             isleaf = true;
           } else {
-            bl = A.macb ? (float)A.macb[node] : s_bl2[mu.y & 0xff];
+            bl = A.macb ? (float)A.macb[lk.w] : s_bl2[lk.y & 0xff];
             const float dc = sqrtf(cx * cx + cy * cy + cz * cz);
             float dmin = dc - rg, dmax = dc + rg;
             if constexpr (kStrict) {
               // conservative: the sphere decides only where the FP64 test of
               // every target certainly agrees
-              bld = A.macb ? A.macb[node] : s_bl2d[mu.y & 0xff];
+              bld = A.macb ? A.macb[lk.w] : s_bl2d[lk.y & 0xff];
               dmin = dc * (1.0f - 1e-5f) - rg;
               dmax = dc * (1.0f + 1e-5f) + rg;
             }
@@ -841,14 +844,6 @@ __global__ void __launch_bounds__(kMixThreads, kStrict ? 4 : 5)
                                                        : __popc(vm1)));
           }
         }
-        // the child table only for opened twigs, the leaf count only for
-        // accepted ones (most popped nodes are leaves or accepted twigs)
-        if (open) {
-          nch = nchild[node];
-          c0 = child8[2 * (int64_t)node];
-          c1 = child8[2 * (int64_t)node + 1];
-        }
-        if (accept) nlv = A.nleaves[node];
         const unsigned lb = __ballot_sync(0xffffffffu, isleaf);
         const unsigned ab = __ballot_sync(0xffffffffu, accept);
         if (isleaf) {
@@ -866,15 +861,16 @@ __global__ void __launch_bounds__(kMixThreads, kStrict ? 4 : 5)
           } else {
             r.c = make_float4(-cx, -cy, -cz, (float)a.w);
           }
-          const float4* m = A.mom32 + kMom32Stride * (int64_t)node;
+          const float4* m = A.mom32 + kMom32Stride * (int64_t)lk.w;
           cp_async16(&r.m0, m);
           cp_async16(&r.m1, m + 1);
           cp_async16(&r.m2, m + 2);
-          partner += nlv;
+          partner += lk.z;
         }
         nL += __popc(lb);
         nT += __popc(ab);
-        const int npush = open ? min(8, nch) : 0;
+        // an opened twig's children: level-order positions first .. first + nch - 1
+        const int npush = open ? min(8, lk.y >> 16) : 0;
         int total;
         const int off = warp_excl_scan(npush, lane, total);
         if (top + total > kStackCap) {
@@ -883,14 +879,9 @@ __global__ void __launch_bounds__(kMixThreads, kStrict ? 4 : 5)
         }
         if (npush > 0) {
           int* dst = stack + top + off;
-          dst[0] = c0.x;
-          if (npush > 1) dst[1] = c0.y;
-          if (npush > 2) dst[2] = c0.z;
-          if (npush > 3) dst[3] = c0.w;
-          if (npush > 4) dst[4] = c1.x;
-          if (npush > 5) dst[5] = c1.y;
-          if (npush > 6) dst[6] = c1.z;
-          if (npush > 7) dst[7] = c1.w;
+#pragma unroll
+          for (int k = 0; k < 8; ++k)
+            if (k < npush) dst[k] = lk.x + k;
         }
         top += total;
         __syncwarp();
@@ -1606,6 +1597,7 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
   A.meta = c->meta.p;
   A.mom32 = reinterpret_cast<const float4*>(c->mom32.p);
   A.nleaves = c->nleaves.p;
+  A.drec = c->drec.p;
   A.bl2 = c->d_box + 9;
   {
     int rc = prepare_mac(c, &A.macb);
@@ -1644,11 +1636,9 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
     const size_t per = (size_t)gblocks * kWW * kStackCap;
     if (!ensure(c, c->wstack, 2 * per, "walk stacks")) return PEPCG_ERR_OOM;
     if (c->prm.precision == PEPCG_PRECISION_MIXED_STRICT)  // 4 blocks per SM
-      k_walk_group64<true><<<148 * 4, kMixThreads, 0, s>>>(A, c->wstack.p + slot * per,
-                                                           c->child8.p, c->nchild.p);
+      k_walk_group64<true><<<148 * 4, kMixThreads, 0, s>>>(A, c->wstack.p + slot * per);
     else if (tiles == nullptr && c->group_size() == 64)
-      k_walk_group64<false><<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p + slot * per,
-                                                            c->child8.p, c->nchild.p);
+      k_walk_group64<false><<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p + slot * per);
     else
       k_walk_group_wide<<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p + slot * per, c->child8.p,
                                                         c->nchild.p);
