@@ -229,6 +229,18 @@ int pepcg_apply_external_field_device(void* ctx, int64_t n, double ez_ext, const
                                       double* d_ez, double* d_pot);
 int pepcg_constrain_periodic_device(void* ctx, int64_t n, double* d_x, double* d_y, double* d_z);
 int pepcg_gather_device(void* ctx, const double* d_in, double* d_out);
+/*
+ * pepcg_potential_energy_device -- the potential energy of pepc-b's
+ * diagnostics (potenergy, frontends/pepc-b/module_diagnostics.f90:227-263):
+ * *epot = sum over the n particles of 0.5 q phi, accumulated in FP64 on the
+ * device (block partials added in a fixed order, so the result does not vary
+ * from run to run; the reference's sequential sum differs from it only by
+ * rounding), so the potentials need not come back to the host.  d_q and d_pot
+ * are device arrays in the same order; epot is a host pointer (the call waits
+ * for the result).
+ */
+int pepcg_potential_energy_device(void* ctx, int64_t n, const double* d_q, const double* d_pot,
+                                  double* epot);
 
 /*
  * Sharding the targets of the grown particles over ranks (one GPU each, the

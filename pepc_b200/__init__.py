@@ -119,6 +119,7 @@ EXPORTS = [
     "pepcg_set_stream", "pepcg_kernel_launches", "pepcg_sort_keys_noalloc",
     "pepcg_traverse_adjoint", "pepcg_traverse_adjoint_device",
     "pepcg_push_particles_device", "pepcg_apply_external_field_device",
+    "pepcg_potential_energy_device",
     "pepcg_constrain_periodic_device", "pepcg_gather_device",
     "pepcg_traverse_range_device", "pepcg_restore_device",
     "pepcg_sort_keys", "pepcg_sort_keys_device", "pepcg_lattice_force",
@@ -159,6 +160,7 @@ def lib():
     L.pepcg_traverse_adjoint_device.argtypes = [VP, C.c_int64] + [VP] * 11
     L.pepcg_push_particles_device.argtypes = [VP, C.c_int64, C.c_double] + [VP] * 11
     L.pepcg_apply_external_field_device.argtypes = [VP, C.c_int64, C.c_double, VP, VP, VP]
+    L.pepcg_potential_energy_device.argtypes = [VP, C.c_int64, VP, VP, C.POINTER(C.c_double)]
     L.pepcg_constrain_periodic_device.argtypes = [VP, C.c_int64, VP, VP, VP]
     L.pepcg_gather_device.argtypes = [VP, VP, VP]
     L.pepcg_traverse_range_device.argtypes = [VP, C.c_int64, C.c_int64, VP, VP, VP, VP, VP]
@@ -341,6 +343,14 @@ class TreeCode:
     def apply_external_field_device(self, ez_ext, z, ez, pot):
         return self._check(lib().pepcg_apply_external_field_device(
             self._h, z.numel(), float(ez_ext), _tptr(z), _tptr(ez), _tptr(pot)))
+
+    def potential_energy_device(self, q, pot):
+        """sum of 0.5 q phi over device arrays, in FP64 on the device (pepc-b's
+        potenergy, module_diagnostics.f90:227-263)."""
+        e = C.c_double(0.0)
+        self._check(lib().pepcg_potential_energy_device(self._h, q.numel(), _tptr(q), _tptr(pot),
+                                                        C.byref(e)))
+        return e.value
 
     def constrain_periodic_device(self, x, y, z):
         return self._check(lib().pepcg_constrain_periodic_device(self._h, x.numel(), _tptr(x),

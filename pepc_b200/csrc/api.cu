@@ -889,6 +889,16 @@ int pepcg_apply_external_field_device(void* ctx, int64_t n, double ez_ext, const
   return external_field_device(c, n, ez_ext, d_z, d_ez, d_pot);
 }
 
+int pepcg_potential_energy_device(void* ctx, int64_t n, const double* d_q, const double* d_pot,
+                                  double* epot) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || n < 0 || !epot || (n > 0 && (!d_q || !d_pot))) return PEPCG_ERR_BAD_ARG;
+  *epot = 0.0;
+  if (n == 0) return PEPCG_OK;
+  cudaSetDevice(c->device);
+  return potential_energy_device(c, n, d_q, d_pot, epot);
+}
+
 int pepcg_constrain_periodic_device(void* ctx, int64_t n, double* d_x, double* d_y, double* d_z) {
   Ctx* c = as_ctx(ctx);
   if (!c || n < 0 || (n > 0 && (!d_x || !d_y || !d_z))) return PEPCG_ERR_BAD_ARG;

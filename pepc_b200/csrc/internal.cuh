@@ -318,6 +318,8 @@ int external_field_device(Ctx* c, int64_t n, double ez_ext, const double* z, dou
                           double* pot);
 int wrap_device(Ctx* c, int64_t n, double* x, double* y, double* z);
 int gather_device(Ctx* c, const double* in, double* out);
+int potential_energy_device(Ctx* c, int64_t n, const double* q, const double* pot,
+                            double* epot);
 int restore_device(Ctx* c, const double* in, double* out);
 int widen_perm_device(Ctx* c, int64_t* out, cudaStream_t st = nullptr);  // null: c->stream
 int lattice_add(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,

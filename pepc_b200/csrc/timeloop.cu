@@ -12,7 +12,10 @@
 //               mass, ...) into the key order of the last grow, as the
 //               reference's domain_decompose moves whole particle records;
 //   restore     out[perm[i]] = in[i]: the way back to the input order
-//               (domain_restore, module_domains.f90:372-408).
+//               (domain_restore, module_domains.f90:372-408);
+//   energy      the potential energy of pepc-b's diagnostics (potenergy,
+//               frontends/pepc-b/module_diagnostics.f90:227-263): the sum of
+//               0.5 q phi in FP64, block partials added in block order.
 // Compiled with --fmad=false, so every result is the reference expression in
 // its order, rounded once per operation.
 
@@ -113,7 +116,51 @@ __global__ void k_widen(int64_t n, const int32_t* __restrict__ in, int64_t* __re
     out[i] = in[i];
 }
 
+// partial sums of (0.5 q) phi (the reference's 0.5 * q(p) * pot(p), left to
+// right) over a grid-stride range, one per block
+constexpr int kEpotBlocks = 296;
+__global__ void __launch_bounds__(kTL) k_epot_partial(int64_t n, const double* __restrict__ q,
+                                                      const double* __restrict__ pot,
+                                                      double* __restrict__ part) {
+  __shared__ double sw[kTL / 32];
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    s = s + (0.5 * q[i]) * pot[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kTL / 32; ++w) t = t + sw[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_epot_final(int nb, const double* __restrict__ part, double* __restrict__ out) {
+  if (threadIdx.x != 0) return;
+  double t = 0.0;
+  for (int b = 0; b < nb; ++b) t = t + part[b];
+  *out = t;
+}
+
 }  // namespace
+
+int potential_energy_device(Ctx* c, int64_t n, const double* q, const double* pot,
+                            double* epot) {
+  cudaStream_t s = c->stream;
+  double* part = c->d_part;  // 6 * 512 doubles: kEpotBlocks partials and the total
+  COUNT_LAUNCH();
+  k_epot_partial<<<kEpotBlocks, kTL, 0, s>>>(n, q, pot, part);
+  COUNT_LAUNCH();
+  k_epot_final<<<1, 32, 0, s>>>(kEpotBlocks, part, part + kEpotBlocks);
+  if (!cuda_ok(c, cudaGetLastError(), "potential energy") ||
+      !cuda_ok(c, cudaMemcpyAsync(epot, part + kEpotBlocks, sizeof(double),
+                                  cudaMemcpyDeviceToHost, s), "potential energy") ||
+      !cuda_ok(c, cudaStreamSynchronize(s), "potential energy"))
+    return PEPCG_ERR_CUDA;
+  return PEPCG_OK;
+}
 
 int push_device(Ctx* c, int64_t n, double dt, const double* q, const double* m, const double* ex,
                 const double* ey, const double* ez, double* vx, double* vy, double* vz, double* x,

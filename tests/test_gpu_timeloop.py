@@ -179,3 +179,32 @@ def test_restore_undoes_gather(gpu):
     tc.restore_device(a, b)
     assert torch.equal(b, v)
     tc.close()
+
+
+def test_potential_energy_reduction(gpu):
+    # pepc-b's potenergy (module_diagnostics.f90:227-263): sum of 0.5 q phi in
+    # FP64, here on the device.  Against the exactly rounded sum (math.fsum) to
+    # a few ulps of the magnitudes summed, the same value on repeated calls,
+    # exact where every partial sum is exact, and 0 for no particles.
+    import math
+    rng = np.random.default_rng(77)
+    x, y, z = rng.random(200000), rng.random(200000), rng.random(200000)
+    q = rng.standard_normal(200000)
+    tc = P.TreeCode(theta2=0.16, eps2=1e-4)
+    g = tc.pepc_grow_tree(x, y, z, q)
+    qd = T(q[g.perm])
+    out = [torch.zeros(len(q), dtype=torch.float64, device=DEV) for _ in range(5)]
+    tc.traverse_self_device(*out)
+    pot = out[3]
+    e1 = tc.potential_energy_device(qd, pot)
+    e2 = tc.potential_energy_device(qd, pot)
+    assert e1 == e2
+    terms = (0.5 * H(qd)) * H(pot)
+    exact = math.fsum(terms)
+    assert abs(e1 - exact) <= 1e-15 * len(terms) * np.abs(terms).max()
+    # small integers: every partial sum is exact, so the result is too
+    qi = T(rng.integers(-8, 8, 100001).astype(np.float64))
+    pi = T(rng.integers(-64, 64, 100001).astype(np.float64))
+    assert tc.potential_energy_device(qi, pi) == math.fsum(0.5 * H(qi) * H(pi))
+    assert tc.potential_energy_device(qi[:0], pi[:0]) == 0.0
+    tc.close()
