@@ -188,7 +188,13 @@ int pepcg_traverse_self_device(void* ctx, double* d_ex, double* d_ey, double* d_
  * buckets (the mixed default) the adjoint runs on that walk's own FP32 lists,
  * evaluates its terms in FP32 on the group-centred offsets and sums them in
  * FP64 across buckets, like the forward; the other mixed walks take the FP64
- * adjoint of their semantics.  With periodic boundaries the mirror boxes'
+ * adjoint of their semantics.  Force laws 3 (3D Coulomb, closed forms), 2 (2D
+ * Coulomb) and 4 (Lennard-Jones): the last two differentiate the forward
+ * kernels themselves (forward-mode dual numbers for the offset, unit moments
+ * for the charge and moments), FP64 walks only, as the forward.  Law 5
+ * (Kelbg) returns PEPCG_ERR_UNSUPPORTED: its leaf kernel needs each target's
+ * own charge, which the adjoint's targets do not carry.  With periodic
+ * boundaries the mirror boxes'
  * terms are in the walk's adjoint, and the FMM far-lattice term's adjoint
  * (FP64, every fmm_extrinsic_correction) is added: the transpose of the
  * lattice force and of the central box's multipole expansion, through the

@@ -14,6 +14,7 @@
 #include <array>
 #include <atomic>
 #include <cmath>
+#include <complex>
 #include <cstdint>
 #include <cstring>
 #include <limits>
@@ -331,26 +332,35 @@ inline void force_twig(const double* t, const double d[3], double dist2, double 
                     + ((dx * pre2z) * t[M_ZX])) + ((dy * pre2z) * t[M_YZ])) + (pre1 * t[M_XY]));
 }
 
+// The 2D Coulomb and Lennard-Jones kernels are templates on the scalar type:
+// double for the walk, std::complex<double> for the complex-step derivative of
+// the adjoint (orc_traverse_adjoint with force_law 2 or 4).  rv() is the real
+// part, for the one comparison (calc_force_LJ's cutoff).
+inline double rv(double x) { return x; }
+inline double rv(const std::complex<double>& x) { return x.real(); }
+
 // calc_force_coulomb_2D_direct, coulomb/module_coulomb_kernels.f90:267-279
 // (d2 = dx^2 + dy^2 + eps2)
-inline void force_leaf_2d(const double* t, const double d[3], double d2, double e[3],
-                          double& phi) {
-  phi = -((0.5 * t[M_Q]) * std::log(d2));
-  const double rd2charge = t[M_Q] / d2;
+template <class T>
+inline void force_leaf_2d(const double* t, const T d[3], T d2, T e[3], T& phi) {
+  using std::log;
+  phi = -((0.5 * t[M_Q]) * log(d2));
+  const T rd2charge = t[M_Q] / d2;
   e[0] = rd2charge * d[0];
   e[1] = rd2charge * d[1];
   e[2] = 0.0;
 }
 
 // calc_force_coulomb_2D, coulomb/module_coulomb_kernels.f90:155-195
-inline void force_twig_2d(const double* t, const double d[3], double d2, double e[3],
-                          double& phi) {
-  const double dx = d[0], dy = d[1];
-  const double rd2 = 1.0 / d2, rd4 = rd2 * rd2, rd6 = rd4 * rd2;
-  const double dx2 = dx * dx, dy2 = dy * dy, dx3 = dx2 * dx, dy3 = dy2 * dy;
+template <class T>
+inline void force_twig_2d(const double* t, const T d[3], T d2, T e[3], T& phi) {
+  using std::log;
+  const T dx = d[0], dy = d[1];
+  const T rd2 = 1.0 / d2, rd4 = rd2 * rd2, rd6 = rd4 * rd2;
+  const T dx2 = dx * dx, dy2 = dy * dy, dx3 = dx2 * dx, dy3 = dy2 * dy;
   const double q = t[M_Q], p1 = t[M_DX], p2 = t[M_DY];
   const double q1 = t[M_QXX], q2 = t[M_QYY], qxy = t[M_XY];
-  phi = ((((-((0.5 * q) * std::log(d2))) - ((dx * p1) + (dy * p2)) * rd2) +
+  phi = ((((-((0.5 * q) * log(d2))) - ((dx * p1) + (dy * p2)) * rd2) +
           q1 * (((2.0 * dx2) * rd4) - rd2)) +
          q2 * (((2.0 * dy2) * rd4) - rd2)) +
         (((2.0 * qxy) * dx) * dy) * rd4;
@@ -367,14 +377,16 @@ inline void force_twig_2d(const double* t, const double d[3], double d2, double 
 
 // calc_force_LJ, coulomb/module_coulomb_kernels.f90:204-235 (r2 unsoftened,
 // aii2 = eps2; the same for leaves and twigs)
-inline void force_lj(const double d[3], double r2, double aii2, double e[3], double& phi) {
+template <class T>
+inline void force_lj(const T d[3], T r2, double aii2, T e[3], T& phi) {
+  using std::sqrt;
   const double epsc2 = 0.8 * aii2;
-  const double aii2_r2 = (r2 > epsc2) ? aii2 / r2 : aii2 / epsc2;
-  const double aii4_r4 = aii2_r2 * aii2_r2;
-  const double flj = 2.0 * (aii4_r4 * aii4_r4) - aii4_r4;
+  const T aii2_r2 = (rv(r2) > epsc2) ? T(aii2 / r2) : T(aii2 / epsc2);
+  const T aii4_r4 = aii2_r2 * aii2_r2;
+  const T flj = 2.0 * (aii4_r4 * aii4_r4) - aii4_r4;
   phi = 0.0;
-  const double r = std::sqrt(r2);
-  const double fljrd = flj / r;
+  const T r = sqrt(r2);
+  const T fljrd = flj / r;
   e[0] = d[0] * fljrd;
   e[1] = d[1] * fljrd;
   e[2] = d[2] * fljrd;
@@ -852,6 +864,72 @@ void leaf_adjoint(double q, const double d[3], double eps2, double gphi, const d
   }
 }
 
+// Adjoint of one interaction for force_law 2 (2D Coulomb) and 4 (Lennard-
+// Jones), where no closed form is written out.  The 2D fields are linear in
+// the node's charge and moments, so dL/dq and dL/dm are L of the unit moments;
+// the Lennard-Jones fields depend on neither.  The offset derivative is the
+// complex step, dL/dd_j = Im L(d + i h e_j) / h with h = 1e-40, exact to
+// rounding for these analytic expressions (law_leaf / law_twig's arguments,
+// evaluated by the same kernels on complex offsets).
+void law_adjoint(int law, bool leaf, const double* m, const double d[3], double eps2, double gphi,
+                 const double gE[3], Adj& a) {
+  using Cx = std::complex<double>;
+  auto Lreal = [&](const double* t) {
+    double e[3], ph;
+    const double dist2 = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2];
+    if (leaf) law_leaf(law, t, d, dist2, eps2, e, ph);
+    else law_twig(law, t, d, dist2, eps2, e, ph);
+    return gphi * ph + ((gE[0] * e[0] + gE[1] * e[1]) + gE[2] * e[2]);
+  };
+  if (law == 2) {
+    double t[M_N];
+    for (int k = 0; k < M_N; ++k) t[k] = 0.0;
+    t[M_Q] = 1.0;
+    a.q += Lreal(t);
+    if (!leaf) {
+      t[M_Q] = 0.0;
+      for (int k = 0; k < 3; ++k) {
+        t[M_DX + k] = 1.0;
+        a.p[k] += Lreal(t);
+        t[M_DX + k] = 0.0;
+      }
+      const int qs[6] = {M_QXX, M_QYY, M_QZZ, M_XY, M_YZ, M_ZX};
+      for (int k = 0; k < 6; ++k) {
+        t[qs[k]] = 1.0;
+        a.Q[k] += Lreal(t);
+        t[qs[k]] = 0.0;
+      }
+    }
+  }
+  const double h = 1e-40;
+  for (int j = 0; j < 3; ++j) {
+    Cx dc[3] = {Cx(d[0], 0.0), Cx(d[1], 0.0), Cx(d[2], 0.0)};
+    dc[j] = Cx(d[j], h);
+    Cx e[3], ph;
+    if (law == 2) {
+      const Cx d2 = (dc[0] * dc[0] + dc[1] * dc[1]) + eps2;
+      if (leaf) force_leaf_2d(m, dc, d2, e, ph);
+      else force_twig_2d(m, dc, d2, e, ph);
+    } else {
+      force_lj(dc, (dc[0] * dc[0] + dc[1] * dc[1]) + dc[2] * dc[2], eps2, e, ph);
+    }
+    const Cx L = gphi * ph + ((gE[0] * e[0] + gE[1] * e[1]) + gE[2] * e[2]);
+    a.c[j] -= L.imag() / h;  // d = target - node centre
+  }
+}
+
+// the interaction adjoint of the context's force law (3: closed forms above)
+void any_leaf_adjoint(int law, const double* m, const double d[3], double eps2, double gphi,
+                      const double gE[3], Adj& a) {
+  if (law == 3) leaf_adjoint(m[M_Q], d, eps2, gphi, gE, a);
+  else law_adjoint(law, true, m, d, eps2, gphi, gE, a);
+}
+void any_twig_adjoint(int law, const double* m, const double d[3], double eps2, double gphi,
+                      const double gE[3], Adj& a) {
+  if (law == 3) twig_adjoint(m, d, eps2, gphi, gE, a);
+  else law_adjoint(law, false, m, d, eps2, gphi, gE, a);
+}
+
 inline double sgn(double v) { return (double)((v > 0.0) - (v < 0.0)); }
 
 // transpose of shift_multipoles_up (coulomb/module_interaction_specific.f90:84-140)
@@ -1287,6 +1365,7 @@ int orc_traverse_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double*
                          const double* tz, const double* gex, const double* gey,
                          const double* gez, const double* gphi, double* dLdq, double* dLdx,
                          double* dLdy, double* dLdz) {
+  if (c->p.force_law == 5) return -7;  // Kelbg: needs each target's own charge
   auto boxes = neighbour_boxes(c->p);
   const int64_t M = (int64_t)c->nodes.size();
   std::vector<Adj> adj(M);
@@ -1329,9 +1408,9 @@ int orc_traverse_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double*
                                  (tz[i] - vb[2]) - nd.m[M_COCZ]};
             const double dist2 = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2];
             if (nd.descendants == 0) {
-              if (dist2 > 0.0) leaf_adjoint(nd.m[M_Q], d, c->p.eps2, gphi[i], gE, adj[ni]);
+              if (dist2 > 0.0) any_leaf_adjoint(c->p.force_law, nd.m, d, c->p.eps2, gphi[i], gE, adj[ni]);
             } else {
-              twig_adjoint(nd.m, d, c->p.eps2, gphi[i], gE, adj[ni]);
+              any_twig_adjoint(c->p.force_law, nd.m, d, c->p.eps2, gphi[i], gE, adj[ni]);
             }
           }
         }
@@ -1354,9 +1433,9 @@ int orc_traverse_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double*
         const double d[3] = {sh[0] - nd.m[M_COCX], sh[1] - nd.m[M_COCY], sh[2] - nd.m[M_COCZ]};
         const double dist2 = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2];
         if (nd.descendants == 0) {
-          if (dist2 > 0.0) leaf_adjoint(nd.m[M_Q], d, c->p.eps2, gphi[i], gE, adj[ni]);
+          if (dist2 > 0.0) any_leaf_adjoint(c->p.force_law, nd.m, d, c->p.eps2, gphi[i], gE, adj[ni]);
         } else if (mac_pass(c, nd, dist2)) {
-          twig_adjoint(nd.m, d, c->p.eps2, gphi[i], gE, adj[ni]);
+          any_twig_adjoint(c->p.force_law, nd.m, d, c->p.eps2, gphi[i], gE, adj[ni]);
         } else {
           for (int64_t ch = nd.first_child; ch != kNodeInvalid; ch = c->nodes[ch].next_sibling)
             todo.push_back(ch);
@@ -1418,6 +1497,7 @@ int orc_traverse_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double*
 int orc_direct_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double* ty,
                        const double* tz, const double* gex, const double* gey, const double* gez,
                        const double* gphi, double* dLdq, double* dLdx, double* dLdy, double* dLdz) {
+  if (c->p.force_law == 5) return -7;  // Kelbg: needs each target's own charge
   auto boxes = neighbour_boxes(c->p);
   const int64_t n = c->n;
   int nth = std::max(1, c->p.num_threads);
@@ -1431,7 +1511,9 @@ int orc_direct_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double* t
         const double d[3] = {(tx[i] - vb[0]) - c->x[j], (ty[i] - vb[1]) - c->y[j],
                              (tz[i] - vb[2]) - c->z[j]};
         if (d[0] == 0.0 && d[1] == 0.0 && d[2] == 0.0) continue;
-        leaf_adjoint(c->q[j], d, c->p.eps2, gphi[i], gE, a);
+        double t[M_N] = {};
+        t[M_Q] = c->q[j];
+        any_leaf_adjoint(c->p.force_law, t, d, c->p.eps2, gphi[i], gE, a);
       }
     }
     const int64_t io = c->perm[j];

@@ -123,6 +123,70 @@ __host__ __device__ __forceinline__ void leaf_adj(double q, double dx, double dy
   a[12] += cd * dz - q * R1 * gE[2];
 }
 
+// The adjoint of one interaction for force_law 2 (2D Coulomb) and 4
+// (Lennard-Jones), from the forward kernels themselves (law_leaf64 /
+// law_twig64's calls): the 2D fields are linear in the node's charge and
+// moments, so dL/dq and dL/dm are L of the unit moments (the Lennard-Jones
+// fields depend on neither); dL/d(offset) comes from one evaluation on D3
+// offsets (forward-mode derivatives along x, y, z) with the node's own
+// charge and moments.  The offset is target minus node centre, so the centre's
+// adjoint takes the negative.  FP64 throughout.
+template <int kLaw>
+__device__ __forceinline__ void law_adj(bool leaf, double q, const double* m, double dx, double dy,
+                                        double dz, double eps2, double gphi, const double gE[3],
+                                        double a[14]) {
+  auto L = [&](double qq, const double* mm) {
+    double ex, ey, ez, ph;
+    if (leaf) {
+      force_leaf_2d64(qq, dx, dy, (dx * dx + dy * dy) + eps2, ex, ey, ez, ph);
+    } else {
+      force_twig_2d64(qq, mm, dx, dy, (dx * dx + dy * dy) + eps2, ex, ey, ez, ph);
+    }
+    return gphi * ph + ((gE[0] * ex + gE[1] * ey) + gE[2] * ez);
+  };
+  if (kLaw == 2) {
+    double u[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    a[0] += L(1.0, u);
+    if (!leaf) {
+      // only the moments the 2D kernel reads: p_x, p_y, q_xx, q_yy, q_xy
+      const int used[5] = {0, 1, 3, 4, 6};
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        u[used[k]] = 1.0;
+        a[1 + used[k]] += L(0.0, u);
+        u[used[k]] = 0.0;
+      }
+    }
+  }
+  const D3 X(dx, 1.0, 0.0, 0.0), Y(dy, 0.0, 1.0, 0.0), Z(dz, 0.0, 0.0, 1.0);
+  D3 ex, ey, ez, ph;
+  if (kLaw == 2) {
+    if (leaf) force_leaf_2d64(q, X, Y, (X * X + Y * Y) + eps2, ex, ey, ez, ph);
+    else force_twig_2d64(q, m, X, Y, (X * X + Y * Y) + eps2, ex, ey, ez, ph);
+  } else {
+    force_lj64(X, Y, Z, (X * X + Y * Y) + Z * Z, eps2, ex, ey, ez, ph);
+  }
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+    a[10 + j] -= gphi * ph.g[j] + ((gE[0] * ex.g[j] + gE[1] * ey.g[j]) + gE[2] * ez.g[j]);
+}
+
+// the interaction adjoints of force law kLaw (3: the closed forms above)
+template <bool kWithE, int kLaw>
+__device__ __forceinline__ void twig_adj_law(double q, const double* m, double dx, double dy,
+                                             double dz, double eps2, double gphi,
+                                             const double gE[3], double a[14]) {
+  if constexpr (kLaw == 3) twig_adj<kWithE>(q, m, dx, dy, dz, eps2, gphi, gE, a);
+  else law_adj<kLaw>(false, q, m, dx, dy, dz, eps2, gphi, gE, a);
+}
+template <int kLaw>
+__device__ __forceinline__ void leaf_adj_law(double q, double dx, double dy, double dz,
+                                             double eps2, double gphi, const double gE[3],
+                                             double a[14]) {
+  if constexpr (kLaw == 3) leaf_adj(q, dx, dy, dz, eps2, gphi, gE, a);
+  else law_adj<kLaw>(true, q, nullptr, dx, dy, dz, eps2, gphi, gE, a);
+}
+
 // The warp's records for one node summed through shared memory (a leaf's
 // record has charge and position terms only, a[0] and a[10..12]; a twig's
 // everything but the abs_charge slot, which only the downward pass fills):
@@ -199,7 +263,7 @@ struct AdjArgs {
 // (atomic) adjoint sums changes.
 // Five resident blocks per SM (at most 102 registers; 126 unbounded): the
 // 262,144-target self adjoint takes 10.0 / 13.2 ms against 11.2 / 13.6 ms.
-template <bool kWithE>
+template <bool kWithE, int kLaw>
 __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_target(AdjArgs A) {
   __shared__ double s_bl2[kMaxLevel + 1];
   __shared__ double s_vb[3 * 125];
@@ -262,7 +326,7 @@ __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_target(AdjArgs A) {
           const double dist2 = (dx * dx + dy * dy) + dz * dz;
           if (leaf) {
             if (dist2 > 0.0) {
-              leaf_adj(nd.w, dx, dy, dz, A.eps2, gp, gE, a);
+              leaf_adj_law<kLaw>(nd.w, dx, dy, dz, A.eps2, gp, gE, a);
               contrib = true;
             }
             next = u + 1;
@@ -270,7 +334,7 @@ __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_target(AdjArgs A) {
             double m[9];
 #pragma unroll
             for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
-            twig_adj<kWithE>(nd.w, m, dx, dy, dz, A.eps2, gp, gE, a);
+            twig_adj_law<kWithE, kLaw>(nd.w, m, dx, dy, dz, A.eps2, gp, gE, a);
             contrib = true;
             next = (unsigned)mu.x;
           } else {
@@ -302,7 +366,7 @@ __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_target(AdjArgs A) {
 // kTPL targets per lane (2: the 64-target buckets of group_size 64, lane k
 // holding targets t0 + k and t0 + 32 + k, as the FP64 group walk does); a
 // lane's targets add into the same node record before the warp's reduction.
-template <bool kWithE, int kTPL>
+template <bool kWithE, int kTPL, int kLaw>
 __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_group(AdjArgs A) {
   __shared__ double s_bl2[kMaxLevel + 1];
   __shared__ double s_vb[3 * 125];
@@ -354,7 +418,7 @@ __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_group(AdjArgs A) {
 #pragma unroll
           for (int s = 0; s < kTPL; ++s)
             if (valid[s] && dist2[s] > 0.0)
-              leaf_adj(nd.w, dx[s], dy[s], dz[s], A.eps2, gp[s], gE[s], a);
+              leaf_adj_law<kLaw>(nd.w, dx[s], dy[s], dz[s], A.eps2, gp[s], gE[s], a);
           flush_smem(A.adj, u, a, lane, true, sred);
           u = (unsigned)fw.y;
         } else {
@@ -370,7 +434,8 @@ __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_group(AdjArgs A) {
 #pragma unroll
               for (int s = 0; s < kTPL; ++s)
                 if (valid[s])
-                  twig_adj<kWithE>(nd.w, m, dx[s], dy[s], dz[s], A.eps2, gp[s], gE[s], a);
+                  twig_adj_law<kWithE, kLaw>(nd.w, m, dx[s], dy[s], dz[s], A.eps2, gp[s],
+                                             gE[s], a);
             }
             flush_smem(A.adj, u, a, lane, false, sred);
             u = (unsigned)fw.y;
@@ -499,6 +564,28 @@ __global__ void k_buckets(int64_t nt, int bs, int2* tiles) {
     tiles[b] = make_int2((int)(b * bs), (int)min((int64_t)bs, nt - b * bs));
 }
 
+// the FP64 adjoint walk of the context's semantics and force law
+template <int kLaw>
+void launch_adj(bool per_target, int tpl, bool with_e, int blocks, cudaStream_t s,
+                const AdjArgs& A) {
+  if (per_target) {
+    if (with_e) k_adj_target<true, kLaw><<<blocks, kAdjThreads, 0, s>>>(A);
+    else k_adj_target<false, kLaw><<<blocks, kAdjThreads, 0, s>>>(A);
+  } else if (tpl == 2) {
+    if (with_e) k_adj_group<true, 2, kLaw><<<blocks, kAdjThreads, 0, s>>>(A);
+    else k_adj_group<false, 2, kLaw><<<blocks, kAdjThreads, 0, s>>>(A);
+  } else {
+    if (with_e) k_adj_group<true, 1, kLaw><<<blocks, kAdjThreads, 0, s>>>(A);
+    else k_adj_group<false, 1, kLaw><<<blocks, kAdjThreads, 0, s>>>(A);
+  }
+}
+void launch_adj_law(int law, bool per_target, int tpl, bool with_e, int blocks, cudaStream_t s,
+                    const AdjArgs& A) {
+  if (law == 2) launch_adj<2>(per_target, tpl, with_e, blocks, s, A);
+  else if (law == 4) launch_adj<4>(per_target, tpl, with_e, blocks, s, A);
+  else launch_adj<3>(per_target, tpl, with_e, blocks, s, A);
+}
+
 }  // namespace
 
 int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
@@ -508,8 +595,9 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
     c->err = "adjoint called without a grown tree";
     return PEPCG_ERR_NO_TREE;
   }
-  if (c->prm.force_law != 3) {
-    c->err = "the adjoint walk differentiates the 3D Coulomb law only (force_law = 3)";
+  if (c->prm.force_law == 5) {
+    c->err = "the adjoint of the Kelbg law (force_law = 5) is not built: its leaf kernel needs "
+             "each target's own charge, which the adjoint's targets do not carry";
     return PEPCG_ERR_UNSUPPORTED;
   }
   if (has_spatial_cutoff(c->prm)) {
@@ -600,18 +688,10 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
   if (mixed64) {
     int rc = launch_adjoint_group64(c, nt, tx, ty, tz, gex, gey, gez, gphi, h_flag != 0, s);
     if (rc) return rc;
-  } else if (per_target) {
-    COUNT_LAUNCH();
-    if (h_flag) k_adj_target<true><<<blocks, kAdjThreads, 0, s>>>(A);
-    else k_adj_target<false><<<blocks, kAdjThreads, 0, s>>>(A);
-  } else if (c->prm.walk == PEPCG_WALK_GROUP && c->group_size() == 64) {
-    COUNT_LAUNCH();
-    if (h_flag) k_adj_group<true, 2><<<blocks, kAdjThreads, 0, s>>>(A);
-    else k_adj_group<false, 2><<<blocks, kAdjThreads, 0, s>>>(A);
   } else {
+    const int tpl = (!per_target && c->prm.walk == PEPCG_WALK_GROUP && c->group_size() == 64) ? 2 : 1;
     COUNT_LAUNCH();
-    if (h_flag) k_adj_group<true, 1><<<blocks, kAdjThreads, 0, s>>>(A);
-    else k_adj_group<false, 1><<<blocks, kAdjThreads, 0, s>>>(A);
+    launch_adj_law(c->prm.force_law, per_target, tpl, h_flag != 0, blocks, s, A);
   }
   const unsigned g = (unsigned)((M + 255) / 256 > 148 * 16 ? 148 * 16 : (M + 255) / 256);
   for (int L = 0; L < c->max_level; ++L) {

@@ -454,24 +454,75 @@ __host__ __device__ __forceinline__ void shift_up64(const Moments* ch, int nc, M
   p.bmax = bmax;
 }
 
+// A number with its derivatives along three directions (forward-mode
+// differentiation): the adjoint walk evaluates the 2D Coulomb and
+// Lennard-Jones kernels below on D3 offsets to get the fields' derivatives
+// with respect to the offset.  Those kernels are templates on the scalar
+// type; their double instantiation is the walk's arithmetic, unchanged.
+// (the namespace's sqrt / log overloads for D3 must not hide the global ones)
+using ::log;
+using ::sqrt;
+struct D3 {
+  double v, g[3];
+  __host__ __device__ D3() : v(0.0), g{0.0, 0.0, 0.0} {}
+  __host__ __device__ D3(double a) : v(a), g{0.0, 0.0, 0.0} {}
+  __host__ __device__ D3(double a, double g0, double g1, double g2) : v(a), g{g0, g1, g2} {}
+};
+__host__ __device__ __forceinline__ D3 operator+(const D3& a, const D3& b) {
+  return D3(a.v + b.v, a.g[0] + b.g[0], a.g[1] + b.g[1], a.g[2] + b.g[2]);
+}
+__host__ __device__ __forceinline__ D3 operator-(const D3& a, const D3& b) {
+  return D3(a.v - b.v, a.g[0] - b.g[0], a.g[1] - b.g[1], a.g[2] - b.g[2]);
+}
+__host__ __device__ __forceinline__ D3 operator-(const D3& a) {
+  return D3(-a.v, -a.g[0], -a.g[1], -a.g[2]);
+}
+__host__ __device__ __forceinline__ D3 operator*(const D3& a, const D3& b) {
+  return D3(a.v * b.v, a.g[0] * b.v + a.v * b.g[0], a.g[1] * b.v + a.v * b.g[1],
+            a.g[2] * b.v + a.v * b.g[2]);
+}
+__host__ __device__ __forceinline__ D3 operator/(const D3& a, const D3& b) {
+  const double r = 1.0 / b.v, v = a.v * r;
+  return D3(v, (a.g[0] - v * b.g[0]) * r, (a.g[1] - v * b.g[1]) * r, (a.g[2] - v * b.g[2]) * r);
+}
+__host__ __device__ __forceinline__ D3 operator+(const D3& a, double b) { return a + D3(b); }
+__host__ __device__ __forceinline__ D3 operator+(double a, const D3& b) { return D3(a) + b; }
+__host__ __device__ __forceinline__ D3 operator-(const D3& a, double b) { return a - D3(b); }
+__host__ __device__ __forceinline__ D3 operator-(double a, const D3& b) { return D3(a) - b; }
+__host__ __device__ __forceinline__ D3 operator*(const D3& a, double b) {
+  return D3(a.v * b, a.g[0] * b, a.g[1] * b, a.g[2] * b);
+}
+__host__ __device__ __forceinline__ D3 operator*(double a, const D3& b) { return b * a; }
+__host__ __device__ __forceinline__ D3 operator/(const D3& a, double b) { return a / D3(b); }
+__host__ __device__ __forceinline__ D3 operator/(double a, const D3& b) { return D3(a) / b; }
+__host__ __device__ __forceinline__ bool operator>(const D3& a, double b) { return a.v > b; }
+__host__ __device__ __forceinline__ D3 sqrt(const D3& a) {
+  const double r = ::sqrt(a.v), h = 0.5 / r;
+  return D3(r, a.g[0] * h, a.g[1] * h, a.g[2] * h);
+}
+__host__ __device__ __forceinline__ D3 log(const D3& a) {
+  const double r = 1.0 / a.v;
+  return D3(::log(a.v), a.g[0] * r, a.g[1] * r, a.g[2] * r);
+}
+
 // calc_force_coulomb_2D_direct, coulomb/module_coulomb_kernels.f90:267-279
 // (d2 = dx^2 + dy^2 + eps2; E_z = 0)
-__host__ __device__ __forceinline__ void force_leaf_2d64(double q, double dx, double dy, double d2,
-                                                         double& ex, double& ey, double& ez,
-                                                         double& phi) {
+template <class T>
+__host__ __device__ __forceinline__ void force_leaf_2d64(double q, T dx, T dy, T d2, T& ex, T& ey,
+                                                         T& ez, T& phi) {
   phi = -((0.5 * q) * log(d2));
-  const double rd2charge = q / d2;
+  const T rd2charge = q / d2;
   ex = rd2charge * dx;
   ey = rd2charge * dy;
   ez = 0.0;
 }
 
 // calc_force_coulomb_2D, coulomb/module_coulomb_kernels.f90:155-195
-__host__ __device__ __forceinline__ void force_twig_2d64(double q, const double* m, double dx,
-                                                         double dy, double d2, double& ex,
-                                                         double& ey, double& ez, double& phi) {
-  const double rd2 = 1.0 / d2, rd4 = rd2 * rd2, rd6 = rd4 * rd2;
-  const double dx2 = dx * dx, dy2 = dy * dy, dx3 = dx2 * dx, dy3 = dy2 * dy;
+template <class T>
+__host__ __device__ __forceinline__ void force_twig_2d64(double q, const double* m, T dx, T dy,
+                                                         T d2, T& ex, T& ey, T& ez, T& phi) {
+  const T rd2 = 1.0 / d2, rd4 = rd2 * rd2, rd6 = rd4 * rd2;
+  const T dx2 = dx * dx, dy2 = dy * dy, dx3 = dx2 * dx, dy3 = dy2 * dy;
   const double p1 = m[0], p2 = m[1], q1 = m[3], q2 = m[4], qxy = m[6];
   phi = ((((-((0.5 * q) * log(d2))) - ((dx * p1) + (dy * p2)) * rd2) +
           q1 * (((2.0 * dx2) * rd4) - rd2)) +
@@ -490,15 +541,15 @@ __host__ __device__ __forceinline__ void force_twig_2d64(double q, const double*
 
 // calc_force_LJ, coulomb/module_coulomb_kernels.f90:204-235 (r2 unsoftened,
 // aii2 = eps2; leaves and twigs alike, phi = 0)
-__host__ __device__ __forceinline__ void force_lj64(double dx, double dy, double dz, double r2,
-                                                    double aii2, double& ex, double& ey,
-                                                    double& ez, double& phi) {
+template <class T>
+__host__ __device__ __forceinline__ void force_lj64(T dx, T dy, T dz, T r2, double aii2, T& ex,
+                                                    T& ey, T& ez, T& phi) {
   const double epsc2 = 0.8 * aii2;
-  const double aii2_r2 = (r2 > epsc2) ? aii2 / r2 : aii2 / epsc2;
-  const double aii4_r4 = aii2_r2 * aii2_r2;
-  const double flj = 2.0 * (aii4_r4 * aii4_r4) - aii4_r4;
+  const T aii2_r2 = (r2 > epsc2) ? T(aii2 / r2) : T(aii2 / epsc2);
+  const T aii4_r4 = aii2_r2 * aii2_r2;
+  const T flj = 2.0 * (aii4_r4 * aii4_r4) - aii4_r4;
   phi = 0.0;
-  const double fljrd = flj / sqrt(r2);
+  const T fljrd = flj / sqrt(r2);
   ex = dx * fljrd;
   ey = dy * fljrd;
   ez = dz * fljrd;

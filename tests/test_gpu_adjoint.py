@@ -7,6 +7,7 @@ Checks, all in FP64:
   * against central finite differences of the GPU forward pass (h = 1e-6,
     the whole grow + traverse re-run per point): relative 1e-5, allowing a
     coordinate whose perturbation flips a MAC decision or a key;
+  * force_law 2 (2D Coulomb) and 4 (Lennard-Jones) against the oracle and FD;
   * periodic boundaries with the FMM lattice term (each extrinsic
     correction): against the oracle, whose lattice adjoint differentiates the
     harmonics independently, and FD;
@@ -201,6 +202,61 @@ def test_autograd_harness_against_torch_direct_gradient(gpu):
                        ("y", leaves[1].grad, dy), ("z", leaves[2].grad, dz)):
         rel = ((a - b).abs() / b.abs().max()).cpu().numpy()
         assert np.median(rel) < 1e-3, (name, np.median(rel))
+    tc.close()
+
+
+@pytest.mark.parametrize("law", [2, 4])
+@pytest.mark.parametrize("walk,owalk", [(P.WALK_PER_TARGET, 0), (P.WALK_GROUP, 2)])
+def test_adjoint_other_force_laws(gpu, law, walk, owalk):
+    """force_law 2 (2D Coulomb) and 4 (Lennard-Jones): the GPU adjoint differentiates
+    the forward kernels by forward-mode dual numbers (D3), the oracle by the complex
+    step.  GPU against oracle to 1e-9 of each component's scale (per-target and
+    32-target bucket lists), then FD of the GPU forward to 1e-6 of that scale."""
+    x, y, z, q, tx, ty, tz, gphi, gE, rng = problem(3000, 70, 90 + law)
+    kw = dict(theta2=0.16, eps2=1e-3, force_law=law)
+    tc = P.TreeCode(precision=P.PRECISION_PLAIN, walk=walk, group_size=32, **kw)
+    tc.pepc_grow_tree(x, y, z, q)
+    g = tc.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
+    orc = O.Oracle(walk=owalk, tile_size=32, num_threads=8, **kw)
+    orc.grow_tree(x, y, z, q)
+    go = orc.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
+    orc.close()
+    for k in ("q", "x", "y", "z"):
+        scale = np.abs(go[k]).max()
+        if law == 2 and k == "z":  # the 2D law reads no z offsets
+            assert np.abs(g[k]).max() <= 1e-12 * np.abs(go["x"]).max()
+            continue
+        assert np.abs(g[k] - go[k]).max() <= 1e-9 * scale, (k, scale)
+    if walk != P.WALK_PER_TARGET:
+        tc.close()
+        return
+
+    def L(a):
+        tc.pepc_grow_tree(a["x"], a["y"], a["z"], a["q"])
+        r = tc.pepc_traverse_tree(tx, ty, tz)
+        return float(np.sum(gphi * r["pot"] + gE[0] * r["ex"] + gE[1] * r["ey"] + gE[2] * r["ez"]))
+
+    h = 1e-5
+    for trial in range(12):
+        j = int(rng.integers(len(x)))
+        key = "xyq"[trial % 3]
+        arrs = {"x": x, "y": y, "z": z, "q": q}
+        plus = {k: (v.copy() if k == key else v) for k, v in arrs.items()}
+        minus = {k: (v.copy() if k == key else v) for k, v in arrs.items()}
+        plus[key][j] += h
+        minus[key][j] -= h
+        fd = (L(plus) - L(minus)) / (2 * h)
+        assert abs(fd - g[key][j]) <= 1e-6 * np.abs(g[key]).max(), (key, j, fd, g[key][j])
+    tc.close()
+
+
+def test_adjoint_refuses_kelbg(gpu):
+    x, y, z, q, tx, ty, tz, gphi, gE, rng = problem(500, 8, 94)
+    tc = P.TreeCode(precision=P.PRECISION_PLAIN, force_law=5, kelbg_invsqrttemp=1.0, eps2=0.0)
+    tc.pepc_grow_tree(x, y, z, np.where(np.arange(500) % 2 == 0, 1.0, -1.0))
+    with pytest.raises(P.PepcgError) as e:
+        tc.traverse_adjoint(tx, ty, tz, gE, gphi, 500)
+    assert e.value.code == P.PEPCG_ERR_UNSUPPORTED
     tc.close()
 
 

@@ -127,3 +127,41 @@ def test_oracle_periodic_far_field_adjoint_against_fd(corr, neutral):
         # the lattice term contributes to this coordinate
         assert g[key][j] != gn[key][j]
     o.close()
+
+
+@pytest.mark.parametrize("law", [2, 4])
+def test_oracle_adjoint_other_force_laws_against_fd(law):
+    # force_law 2 (2D Coulomb) and 4 (Lennard-Jones): the oracle's adjoint
+    # takes the offset derivative by the complex step through the forward
+    # kernels and the 2D charge / moment derivatives as fields of unit moments.
+    # The Lennard-Jones fields do not depend on the charges, so their dL/dq
+    # comes only through the centres of charge and is small next to L: the
+    # tolerance is relative to each gradient component's largest entry.
+    x, y, z, q, tx, ty, tz, gphi, gE, rng = _problem(400, 16, 5)
+    kw = dict(theta2=0.16, eps2=1e-3, force_law=law, walk=0)
+    o = O.Oracle(**kw)
+    o.grow_tree(x, y, z, q)
+    g = o.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
+    o.close()
+    t = (tx, ty, tz)
+    h = 1e-5
+    for trial in range(16):
+        j = int(rng.integers(len(x)))
+        key = "xyzq"[trial % 4]
+        arrs = {"x": x, "y": y, "z": z, "q": q}
+        plus = {k: (v.copy() if k == key else v) for k, v in arrs.items()}
+        minus = {k: (v.copy() if k == key else v) for k, v in arrs.items()}
+        plus[key][j] += h
+        minus[key][j] -= h
+        fd = (_L_tree(plus, t, gphi, gE, **kw) - _L_tree(minus, t, gphi, gE, **kw)) / (2 * h)
+        scale = np.abs(g[key]).max()
+        assert abs(fd - g[key][j]) <= 1e-6 * scale, (law, key, j, fd, g[key][j], scale)
+
+
+def test_oracle_adjoint_refuses_kelbg():
+    x, y, z, q, tx, ty, tz, gphi, gE, _ = _problem(100, 4, 6)
+    o = O.Oracle(theta2=0.16, eps2=1e-3, force_law=5, kelbg_invsqrttemp=1.0)
+    o.grow_tree(x, y, z, np.where(np.arange(100) % 2 == 0, 1.0, -1.0))
+    with pytest.raises(RuntimeError):
+        o.traverse_adjoint(tx, ty, tz, gE, gphi, 100)
+    o.close()
