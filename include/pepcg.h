@@ -99,13 +99,13 @@ typedef struct pepcg_params {
   double kelbg_invsqrttemp;      /* force_law 5: 1/sqrt(temperature) (specific.f90:40) [0] */
   int32_t group_size;            /* GROUP walk: targets per bucket, 32 or 64; 0 = 64 for the
                                     mixed walk and 32 for the plain walk [0].  The adjoint
-                                    supports 32. */
+                                    supports both. */
   int32_t reserved0;             /* zero */
   double spatial_interaction_cutoff[3]; /* module_mirror_boxes.f90:52: a node whose offset
                                     from the target has any |component| >= the cutoff is
                                     skipped (module_tree_walk_pthreads.f90:622,639;
-                                    module_tree_walk_simple.f90:330,377); plain walks only,
-                                    >= 0 [DBL_MAX each: no cutoff] */
+                                    module_tree_walk_simple.f90:330,377); plain walks and
+                                    their adjoint only, >= 0 [DBL_MAX each: no cutoff] */
   int32_t reserved[4];           /* zero */
 } pepcg_params;
 

@@ -1407,6 +1407,7 @@ int orc_traverse_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double*
             const double d[3] = {(tx[i] - vb[0]) - nd.m[M_COCX], (ty[i] - vb[1]) - nd.m[M_COCY],
                                  (tz[i] - vb[2]) - nd.m[M_COCZ]};
             const double dist2 = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2];
+            if (cut_off(c, d)) continue;  // the forward's skip (:330, :377)
             if (nd.descendants == 0) {
               if (dist2 > 0.0) any_leaf_adjoint(c->p.force_law, nd.m, d, c->p.eps2, gphi[i], gE, adj[ni]);
             } else {
@@ -1433,9 +1434,11 @@ int orc_traverse_adjoint(orc_ctx* c, int64_t nt, const double* tx, const double*
         const double d[3] = {sh[0] - nd.m[M_COCX], sh[1] - nd.m[M_COCY], sh[2] - nd.m[M_COCZ]};
         const double dist2 = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2];
         if (nd.descendants == 0) {
-          if (dist2 > 0.0) any_leaf_adjoint(c->p.force_law, nd.m, d, c->p.eps2, gphi[i], gE, adj[ni]);
+          if (dist2 > 0.0 && !cut_off(c, d))  // :622
+            any_leaf_adjoint(c->p.force_law, nd.m, d, c->p.eps2, gphi[i], gE, adj[ni]);
         } else if (mac_pass(c, nd, dist2)) {
-          any_twig_adjoint(c->p.force_law, nd.m, d, c->p.eps2, gphi[i], gE, adj[ni]);
+          if (!cut_off(c, d))  // :639
+            any_twig_adjoint(c->p.force_law, nd.m, d, c->p.eps2, gphi[i], gE, adj[ni]);
         } else {
           for (int64_t ch = nd.first_child; ch != kNodeInvalid; ch = c->nodes[ch].next_sibling)
             todo.push_back(ch);

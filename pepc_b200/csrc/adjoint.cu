@@ -251,7 +251,15 @@ struct AdjArgs {
   const int32_t* parent;
   unsigned int* queue;             // bucket counter (k_adj_group), zeroed before the launch
   unsigned long long* item_queue;  // item counter (k_adj_target), zeroed before the launch
+  // spatial_interaction_cutoff: an interaction whose offset has any |component|
+  // >= cut is skipped, as in the forward walks (after the leaf / MAC decision)
+  int has_cut;
+  double cut[3];
 };
+
+__device__ __forceinline__ bool adj_cut(const AdjArgs& A, double dx, double dy, double dz) {
+  return A.has_cut && (fabs(dx) >= A.cut[0] || fabs(dy) >= A.cut[1] || fabs(dz) >= A.cut[2]);
+}
 
 // per-target semantics: the min-next-index schedule of k_walk_target64.
 // With few targets the walk of a 32-target bucket is cut into work items so
@@ -325,17 +333,19 @@ __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_target(AdjArgs A) {
           const double dx = sx - nd.x, dy = sy - nd.y, dz = sz - nd.z;
           const double dist2 = (dx * dx + dy * dy) + dz * dz;
           if (leaf) {
-            if (dist2 > 0.0) {
+            if (dist2 > 0.0 && !adj_cut(A, dx, dy, dz)) {
               leaf_adj_law<kLaw>(nd.w, dx, dy, dz, A.eps2, gp, gE, a);
               contrib = true;
             }
             next = u + 1;
           } else if (A.theta2 * dist2 > (A.macb ? A.macb[u] : s_bl2[mu.y & 0xff])) {
-            double m[9];
+            if (!adj_cut(A, dx, dy, dz)) {
+              double m[9];
 #pragma unroll
-            for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
-            twig_adj_law<kWithE, kLaw>(nd.w, m, dx, dy, dz, A.eps2, gp, gE, a);
-            contrib = true;
+              for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
+              twig_adj_law<kWithE, kLaw>(nd.w, m, dx, dy, dz, A.eps2, gp, gE, a);
+              contrib = true;
+            }
             next = (unsigned)mu.x;
           } else {
             next = u + 1;
@@ -417,7 +427,7 @@ __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_group(AdjArgs A) {
         if (mu.y & kLeafFlag) {
 #pragma unroll
           for (int s = 0; s < kTPL; ++s)
-            if (valid[s] && dist2[s] > 0.0)
+            if (valid[s] && dist2[s] > 0.0 && !adj_cut(A, dx[s], dy[s], dz[s]))
               leaf_adj_law<kLaw>(nd.w, dx[s], dy[s], dz[s], A.eps2, gp[s], gE[s], a);
           flush_smem(A.adj, u, a, lane, true, sred);
           u = (unsigned)fw.y;
@@ -433,7 +443,7 @@ __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_group(AdjArgs A) {
               for (int k = 0; k < 9; ++k) m[k] = A.mom[kMomStride * (int64_t)u + k];
 #pragma unroll
               for (int s = 0; s < kTPL; ++s)
-                if (valid[s])
+                if (valid[s] && !adj_cut(A, dx[s], dy[s], dz[s]))
                   twig_adj_law<kWithE, kLaw>(nd.w, m, dx[s], dy[s], dz[s], A.eps2, gp[s],
                                              gE[s], a);
             }
@@ -600,10 +610,8 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
              "each target's own charge, which the adjoint's targets do not carry";
     return PEPCG_ERR_UNSUPPORTED;
   }
-  if (has_spatial_cutoff(c->prm)) {
-    c->err = "the adjoint walk does not apply spatial_interaction_cutoff";
-    return PEPCG_ERR_UNSUPPORTED;
-  }
+  // the mixed walks refuse a finite cutoff already (check_params); the FP64
+  // adjoint walks skip the interactions the forward skips
   cudaStream_t s = c->stream;
   const int64_t M = c->nnodes;
   if (!ensure(c, c->adj, (size_t)kNA * M, "adjoint")) return PEPCG_ERR_OOM;
@@ -642,6 +650,8 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
   A.nsub = 0;
   A.sublist = nullptr;
   A.parent = c->parent.p;
+  A.has_cut = has_spatial_cutoff(c->prm) ? 1 : 0;
+  for (int k = 0; k < 3; ++k) A.cut[k] = c->prm.spatial_interaction_cutoff[k];
   const bool per_target = (c->prm.walk == PEPCG_WALK_PER_TARGET);
   // the mixed group walk with 64-target buckets (the benchmark's walk) has
   // its own adjoint walk, on the forward's FP32 lists (walk_mixed.cu)

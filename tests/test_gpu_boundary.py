@@ -8,6 +8,8 @@ namelists, against the oracle.
     pthreads walk counts a skipped leaf, module_tree_walk_pthreads.f90:620-622;
     the simple walk counts nothing, module_tree_walk_simple.f90:330,377), and
     both are reproduced bit for bit;
+  * the adjoint with the cutoff skips the same interactions (against the
+    oracle's adjoint and FD);
   * the scalar lattice entry point pepcg_lattice_force equals the array form."""
 import numpy as np
 import pytest
@@ -55,12 +57,50 @@ def test_spatial_cutoff_refused_where_not_applied(gpu):
     with pytest.raises(P.PepcgError) as e:
         P.TreeCode(spatial_interaction_cutoff=(-1.0, 1.0, 1.0))
     assert e.value.code == P.PEPCG_ERR_BAD_ARG
-    x, y, z, q = cube(2000, 72, charges="normal")
-    tc = P.TreeCode(spatial_interaction_cutoff=cut)
+
+
+@pytest.mark.parametrize("walk,owalk", [(P.WALK_PER_TARGET, 0), (P.WALK_GROUP, 2)])
+@pytest.mark.parametrize("periodic", [False, True])
+def test_spatial_cutoff_adjoint(gpu, walk, owalk, periodic):
+    # the adjoint skips exactly the interactions the forward skips: against the
+    # oracle's adjoint (1e-9 of each component's scale) and FD of the GPU forward
+    x, y, z, q = cube(3000, 73, charges="normal")
+    rng = np.random.default_rng(74)
+    nt = 60
+    tx, ty, tz = rng.random(nt), rng.random(nt), rng.random(nt)
+    gphi = rng.standard_normal(nt)
+    gE = [rng.standard_normal(nt) for _ in range(3)]
+    kw = dict(theta2=0.25, eps2=1e-4, spatial_interaction_cutoff=(0.3, 0.45, 0.2))
+    if periodic:
+        kw.update(periodicity=(1, 1, 1), include_far_field_if_periodic=0)
+    tc = P.TreeCode(walk=walk, group_size=32, **kw)
     tc.pepc_grow_tree(x, y, z, q)
-    with pytest.raises(P.PepcgError) as e:
-        tc.traverse_adjoint(x[:10], y[:10], z[:10], (np.zeros(10),) * 3, np.ones(10), 2000)
-    assert e.value.code == P.PEPCG_ERR_UNSUPPORTED
+    g = tc.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
+    orc = O.Oracle(walk=owalk, tile_size=32, num_threads=8, **kw)
+    orc.grow_tree(x, y, z, q)
+    go = orc.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
+    orc.close()
+    for k in ("q", "x", "y", "z"):
+        assert np.abs(g[k] - go[k]).max() <= 1e-9 * np.abs(go[k]).max(), k
+
+    def L(a):
+        tc.pepc_grow_tree(a["x"], a["y"], a["z"], a["q"])
+        r = tc.pepc_traverse_tree(tx, ty, tz)
+        return float(np.sum(gphi * r["pot"] + gE[0] * r["ex"] + gE[1] * r["ey"] + gE[2] * r["ez"]))
+
+    h, bad = 1e-6, 0
+    for trial in range(8):
+        j = int(rng.integers(len(x)))
+        key = "xyzq"[trial % 4]
+        arrs = {"x": x, "y": y, "z": z, "q": q}
+        plus = {k: (v.copy() if k == key else v) for k, v in arrs.items()}
+        minus = {k: (v.copy() if k == key else v) for k, v in arrs.items()}
+        plus[key][j] += h
+        minus[key][j] -= h
+        fd = (L(plus) - L(minus)) / (2 * h)
+        if abs(fd - g[key][j]) > 1e-5 * np.abs(g[key]).max():
+            bad += 1  # a perturbation may flip a MAC or cutoff decision
+    assert bad <= 1
     tc.close()
 
 

@@ -165,3 +165,35 @@ def test_oracle_adjoint_refuses_kelbg():
     with pytest.raises(RuntimeError):
         o.traverse_adjoint(tx, ty, tz, gE, gphi, 100)
     o.close()
+
+
+@pytest.mark.parametrize("walk", [0, 2])
+def test_oracle_adjoint_spatial_cutoff_against_fd(walk):
+    # spatial_interaction_cutoff: the adjoint skips the interactions the walk
+    # skips (module_tree_walk_pthreads.f90:622,639; module_tree_walk_simple.f90:330,377)
+    x, y, z, q, tx, ty, tz, gphi, gE, rng = _problem(500, 24, 19)
+    kw = dict(theta2=0.16, eps2=1e-3, walk=walk, tile_size=32,
+              spatial_interaction_cutoff=(0.25, 0.3, 0.2))
+    o = O.Oracle(**kw)
+    o.grow_tree(x, y, z, q)
+    g = o.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
+    o.close()
+    full = O.Oracle(**{k: v for k, v in kw.items() if k != "spatial_interaction_cutoff"})
+    full.grow_tree(x, y, z, q)
+    gf = full.traverse_adjoint(tx, ty, tz, gE, gphi, len(x))
+    full.close()
+    assert not np.array_equal(g["q"], gf["q"])  # the cutoff removed interactions
+    t = (tx, ty, tz)
+    h, bad = 1e-6, 0
+    for trial in range(16):
+        j = int(rng.integers(len(x)))
+        key = "xyzq"[trial % 4]
+        arrs = {"x": x, "y": y, "z": z, "q": q}
+        plus = {k: (v.copy() if k == key else v) for k, v in arrs.items()}
+        minus = {k: (v.copy() if k == key else v) for k, v in arrs.items()}
+        plus[key][j] += h
+        minus[key][j] -= h
+        fd = (_L_tree(plus, t, gphi, gE, **kw) - _L_tree(minus, t, gphi, gE, **kw)) / (2 * h)
+        if abs(fd - g[key][j]) > 1e-6 * np.abs(g[key]).max():
+            bad += 1  # a perturbation may flip a MAC or cutoff decision
+    assert bad <= 1, bad
