@@ -625,12 +625,17 @@ int pepcg_traverse_tree(void* ctx, int64_t nt, const double* tx, const double* t
   const bool chunked = nt >= kChunkedTargets && !keys_used && c->prm.walk != PEPCG_WALK_PER_TILE &&
                        !c->far_field && c->has_tree;
   if (chunked) {
-    // three chunks, small ones first and last: the walk starts after 1/16 of
-    // the upload and only 1/16 of the download trails it
+    // five chunks of 1/32, 2/32, 25/32, 3/32 and 1/32 of the targets: the walk
+    // starts after 1/32 of the upload, each later chunk's upload finishes
+    // while the earlier chunks walk (an upload moves 24 bytes per target, the
+    // walk takes ~8 ns per target, PCIe ~50 GB/s), each chunk's download (40
+    // bytes per target) runs while the later chunks walk, and only the last
+    // 1/32 of the download trails the walk
     if (!copy_streams(c)) return PEPCG_ERR_CUDA;
-    const int nch = 3;
+    const int nch = 5;
     auto al = [](int64_t v) { return v & ~(int64_t)63; };  // whole group-walk buckets
-    const int64_t bounds[nch + 1] = {0, al(nt / 16), al(nt - nt / 16), nt};
+    const int64_t bounds[nch + 1] = {0, al(nt / 32), al(3 * (nt / 32)), al(nt - 4 * (nt / 32)),
+                                     al(nt - nt / 32), nt};
     bool ok = true;
     for (int k = 0; k < nch; ++k) {
       const int64_t t0 = bounds[k], len = bounds[k + 1] - bounds[k];
