@@ -32,10 +32,10 @@ sys.path.insert(0, ROOT)
 METRIC = "particle force evals/s at 4M, mixed vs FP64 GPU walk, at ≤1e-4 median force err"
 UNIT = "force evals/s"
 # DRAM bytes per particle of one mixed group-walk launch (k_walk_group64), from one
-# ncu capture of the kernel (Plummer N = 1,048,576, theta = 0.4: 357.4 MB read +
-# 67.5 MB written), scaled by the particle count: the tree the walk re-reads grows
+# ncu capture of the kernel (Plummer N = 1,048,576, theta = 0.4: 283.7 MB read +
+# 57.1 MB written), scaled by the particle count: the tree the walk re-reads grows
 # with N
-WALK_DRAM_BYTES_PER_PARTICLE = (357.4e6 + 67.5e6) / 1048576
+WALK_DRAM_BYTES_PER_PARTICLE = (283.7e6 + 57.1e6) / 1048576
 FLOPS_TWIG = 144  # counted from coulomb/module_coulomb_kernels.f90:60-145 + delta, dist2, MAC, sums
 FLOPS_LEAF = 22   # counted from module_coulomb_kernels.f90:242-257 + delta, dist2, sums
 SMS = 148
