@@ -17,6 +17,7 @@ of the reference algorithm (the oracle) on the host cores instead.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -257,6 +258,112 @@ def event_ms(torch, stream, fn):
     e1.record(stream)
     torch.cuda.synchronize()
     return e0.elapsed_time(e1)
+
+
+def kaplan_sphere(n, seed=1234):
+    """pepc-benchmark's 'test' setup (frontends/pepc-benchmark/module_helper.f90:194-227):
+    particle k of n at radius s = (1/(1 - k/n) - 1)^(1/3) (Kaplan's Eq. 9, mu = 1) in a
+    random direction (phi uniform, cos theta uniform).  The reference draws the angles
+    from its own generator; numpy's PCG64 (seed) stands in for it."""
+    rng = np.random.default_rng(seed)
+    k = np.arange(n, dtype=np.float64)
+    s = (1.0 / (1.0 - k / n) - 1.0) ** (1.0 / 3.0)
+    phi = rng.random(n) * 2.0 * math.pi
+    th = np.arccos(rng.random(n) * 2.0 - 1.0)
+    return s * np.cos(phi) * np.sin(th), s * np.sin(phi) * np.sin(th), s * np.cos(th)
+
+
+def benchmark_check(P, torch, dev, n, prec, walk, stream=None, seed=1234):
+    """pepc-benchmark's correctness run (benchmark/benchmark.xml, tag check; the loop of
+    frontends/pepc-benchmark/pepc.f90:49-93) on the device time loop: n electrons
+    (q = -2/n, m = 1e-3, at rest) from kaplan_sphere, theta2 = 0.25, eps2 = 1e-4, dt =
+    0.02.  Every step: results cleared, grow, traverse (the particles' own fields), push.
+    Every diag_interval = 100 steps: the direct test on 1000 random particles
+    (test_particles, module_helper.f90:455-524: L2 = sqrt(sum |E - E_direct|^2) / 1000)
+    and the energies after the push (check_energies_local, :272-310: kinetic from v half
+    a step back, relativistic; potential sum 0.5 q phi, here pepcg_potential_energy_device).
+    The check step is the first diagnostic step at or after sqrt(n / 1000) * 210
+    (pepc.f90:60): there the velocity histogram of the particles at 7 <= r <= 8.5
+    (histogram_local, :342-376: 50 bins of v_max / 50) has its runs of occupied bins
+    counted (test_histogram, :378-428), and the check passes with exactly 2.  egy_drop
+    is the JUBE pattern's (max - min) / max of the total energy, in percent."""
+    q = torch.full((n,), -2.0 / n, dtype=torch.float64, device=dev)
+    m = torch.full((n,), 1e-3, dtype=torch.float64, device=dev)
+    zeros = lambda: torch.zeros(n, dtype=torch.float64, device=dev)  # noqa: E731
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    x0, y0, z0 = kaplan_sphere(n, seed)
+    st = {"x": T(x0), "y": T(y0), "z": T(z0), "q": q, "m": m,
+          "vx": zeros(), "vy": zeros(), "vz": zeros()}
+    tc = P.TreeCode(theta2=0.25, eps2=1e-4, precision=prec, walk=walk)
+    if stream is not None:
+        tc.set_stream(stream.cuda_stream)
+    key = torch.empty(n, dtype=torch.int64, device=dev)
+    perm = torch.empty(n, dtype=torch.int64, device=dev)
+    out = [zeros() for _ in range(5)]
+    dt, diag, ndirect = 0.02, 100, 1000
+    check_at = math.sqrt(n / 1000.0) * 210
+    rng = np.random.default_rng(seed + 1)
+    energies, l2 = [], []
+    step = 0
+    t0 = time.time()
+    while True:
+        do_diag = step % diag == 0
+        do_check = step >= check_at and step > 0 and step < check_at + diag
+        tc.grow_tree_device(st["x"], st["y"], st["z"], st["q"])
+        nx, ny, nz, nq, nm, nvx, nvy, nvz = (torch.empty_like(q) for _ in range(8))
+        tc.particles_device(key, perm, nx, ny, nz, nq)
+        for src, dst in ((st["m"], nm), (st["vx"], nvx), (st["vy"], nvy), (st["vz"], nvz)):
+            tc.gather_device(src, dst)
+        for o in out:
+            o.zero_()
+        tc.traverse_self_device(*out)
+        if do_diag:
+            idx = np.sort((rng.random(ndirect) * (n - 1)).astype(np.int64))
+            d = tc.direct(idx)
+            E = torch.stack(out[:3]).cpu().numpy()[:, idx]
+            dE = (E[0] - d["ex"]) ** 2 + (E[1] - d["ey"]) ** 2 + (E[2] - d["ez"]) ** 2
+            Ed2 = d["ex"] ** 2 + d["ey"] ** 2 + d["ez"] ** 2
+            l2.append((math.sqrt(dE.sum()) / ndirect, math.sqrt(dE.sum() / Ed2.sum())))
+        tc.push_particles_device(dt, nq, nm, out[:3], (nvx, nvy, nvz), (nx, ny, nz))
+        st.update(x=nx, y=ny, z=nz, q=nq, m=nm, vx=nvx, vy=nvy, vz=nvz)
+        if do_diag:
+            f = (dt * 0.5) * (nq / nm)
+            vx_, vy_, vz_ = nvx - f * out[0], nvy - f * out[1], nvz - f * out[2]
+            gam = torch.sqrt(1.0 + (vx_ * vx_ + vy_ * vy_ + vz_ * vz_))
+            e_kin = float(((gam - 1.0) * nm).sum())
+            e_pot = tc.potential_energy_device(nq, out[3])
+            energies.append(e_kin + e_pot)
+            if do_check:
+                v = torch.sqrt(nvx * nvx + nvy * nvy + nvz * nvz)
+                r = torch.sqrt(nx * nx + ny * ny + nz * nz)
+                sel = (r >= 7.0) & (r <= 8.5)
+                pos = (v[sel] / (float(v.max()) / 50)).long()
+                hist = torch.bincount(pos, minlength=51).cpu().numpy()[:51]
+                runs = int(sum(1 for b in range(51) if hist[b] > 0 and (b == 0 or hist[b - 1] == 0)))
+                break
+        step += 1
+    seconds = time.time() - t0
+    tc.close()
+    e = np.array(energies)
+    return {"n": n, "check_step": step, "steps": step + 1, "seconds": seconds,
+            "histogram_peaks": runs, "check": "passed" if runs == 2 else "failed",
+            "histogram": hist.tolist(),
+            "egy_drop_pct": float((e.max() - e.min()) / abs(e.max()) * 100),
+            "energy_first": float(e[0]), "energy_last": float(e[-1]),
+            "l2_last": l2[-1][0], "l2_rel_max": max(v[1] for v in l2)}
+
+
+def run_benchmark_check(args, P, torch, dev, stream):
+    """the benchmark-check workload: benchmark_check at the reference's size (n = --n,
+    1,048,576 unless given), one descriptive JSON line"""
+    n = args.n if args.n != 4194304 else 1048576
+    prec = {"mixed": P.PRECISION_MIXED, "plain": P.PRECISION_PLAIN,
+            "strict": P.PRECISION_MIXED_STRICT}[args.precision]
+    walk = {"group": P.WALK_GROUP, "target": P.WALK_PER_TARGET, "tile": P.WALK_PER_TILE}[args.walk]
+    res = benchmark_check(P, torch, dev, n, prec, walk, stream)
+    res["ms_per_step"] = res["seconds"] / res["steps"] * 1e3
+    print(json.dumps({"workload": "pepc-benchmark correctness check (Kaplan Coulomb explosion)",
+                      "precision": args.precision, "walk": args.walk, **res}), flush=True)
 
 
 def run_explosion(args, P, torch, dev, stream):
@@ -600,11 +707,13 @@ def main():
     ap.add_argument("--shard", action="store_true",
                     help="target sharding across the ranks (strong scaling) instead of replicas")
     ap.add_argument("--workload", default="plummer",
-                    choices=["plummer", "explosion", "madelung", "adjoint"],
+                    choices=["plummer", "explosion", "madelung", "adjoint", "benchmark-check"],
                     help="plummer: the headline line; explosion / madelung: the other "
                          "configurations, one descriptive JSON line each; adjoint: the "
                          "adjoint measurements alone (the adjoint configuration, then the "
-                         "Plummer particles of --n as their own targets)")
+                         "Plummer particles of --n as their own targets); benchmark-check: "
+                         "pepc-benchmark's correctness run (Kaplan Coulomb explosion, "
+                         "histogram and energy checks) at n = 1,048,576 unless --n is given")
     args = ap.parse_args()
     assert args.warmup >= 3, "at least 3 warm-up steps"
 
@@ -644,7 +753,8 @@ def main():
         dev = torch.device("cuda", local)
         stream = torch.cuda.Stream(device=dev)
         torch.cuda.set_stream(stream)
-        (run_explosion if args.workload == "explosion" else run_madelung)(args, P, torch, dev, stream)
+        {"explosion": run_explosion, "madelung": run_madelung,
+         "benchmark-check": run_benchmark_check}[args.workload](args, P, torch, dev, stream)
         return
 
     if args.shard:
