@@ -526,6 +526,9 @@ __global__ void __launch_bounds__(kMixThreads, kStrict ? 4 : 5)
   __shared__ double s_vb[3 * 125];
   __shared__ TwigRec s_tw[kWW][kRing];
   __shared__ StagedLeaf s_lf[kWW][kRing];
+  // the two targets' FP64 sums (E, phi) live here rather than in registers: they
+  // change once per batch of 32 records, and the registers go to the batches
+  __shared__ double s_acc[8][kMixThreads];
   for (int i = threadIdx.x; i <= kMaxLevel; i += blockDim.x) {
     s_bl2[i] = (float)A.bl2[i];
     if constexpr (kStrict) s_bl2d[i] = A.bl2[i];
@@ -551,7 +554,10 @@ __global__ void __launch_bounds__(kMixThreads, kStrict ? 4 : 5)
     const unsigned vm0 = __ballot_sync(0xffffffffu, v0), vm1 = __ballot_sync(0xffffffffu, v1);
     const int64_t ta = t0 + lane, tb = t0 + 32 + lane;
     double pxa = 0, pya = 0, pza = 0, pxb = 0, pyb = 0, pzb = 0;
-    double Ea0 = 0, Ea1 = 0, Ea2 = 0, PHa = 0, Eb0 = 0, Eb1 = 0, Eb2 = 0, PHb = 0;
+    double &Ea0 = s_acc[0][threadIdx.x], &Ea1 = s_acc[1][threadIdx.x], &Ea2 = s_acc[2][threadIdx.x],
+           &PHa = s_acc[3][threadIdx.x], &Eb0 = s_acc[4][threadIdx.x], &Eb1 = s_acc[5][threadIdx.x],
+           &Eb2 = s_acc[6][threadIdx.x], &PHb = s_acc[7][threadIdx.x];
+    Ea0 = Ea1 = Ea2 = PHa = Eb0 = Eb1 = Eb2 = PHb = 0.0;
     double W = 0;  // interactions of this call (the same list for all targets)
     if (v0) {
       pxa = A.tx[ta]; pya = A.ty[ta]; pza = A.tz[ta];
@@ -1629,9 +1635,9 @@ int launch_walk_mixed(Ctx* c, int64_t nt, const double* tx, const double* ty, co
   } else if (tflag) {
     k_walk_tilepack_mixed<<<148 * 8, kMixThreads, 0, s>>>(A);
   } else {
-    // 5 resident blocks per SM (launch bounds: 96 registers, 31.8 KB shared
-    // memory each); the grid is exactly one wave.  One set of stacks per walk
-    // stream.
+    // 5 resident blocks per SM (launch bounds: at most 96 registers; the
+    // 64-target walk holds 39 KB of shared memory per block); the grid is
+    // exactly one wave.  One set of stacks per walk stream.
     const int gblocks = 148 * 5;
     const size_t per = (size_t)gblocks * kWW * kStackCap;
     if (!ensure(c, c->wstack, 2 * per, "walk stacks")) return PEPCG_ERR_OOM;
