@@ -638,7 +638,7 @@ __global__ void __launch_bounds__(kMixThreads, kStrict ? 4 : 5)
           const float2 E2 = f2(A.eps2);
           const int n1 = min(n, kRing - hT);
           const TwigRec* r = stw + hT;
-#pragma unroll 8
+#pragma unroll 16
           for (int j = 0; j < n1; ++j) {
             // c is the negated offset: one packed add per axis
             const float4 c = r[j].c, m0 = r[j].m0, m1 = r[j].m1, m2 = r[j].m2;
