@@ -460,79 +460,87 @@ __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_group(AdjArgs A) {
 }
 
 // transpose of shift_multipoles_up for the twigs of one level (top-down);
-// the twigs of a level come from the per-level lists built by the grow
+// the twigs of a level come from the per-level lists built by the grow, and
+// each twig's children are read as one run of the grow's level-ordered
+// records (drec: centre and charge, abs_charge; link.w the RPO index of the
+// child's adjoint record) and its twig children's dipoles from dmom at their
+// twig-list positions -- the values of nc4 and mom, without chasing the
+// children through meta.  Children in key order, as shift_multipoles_up.
 __global__ void k_adj_down_level(int level, const int32_t* __restrict__ lvl,
                                  const int32_t* __restrict__ twiglist,
-                                 const int2* __restrict__ meta,
-                                 const double4* __restrict__ nc4, const double* __restrict__ mom,
-                                 double* __restrict__ adj) {
+                                 const int2* __restrict__ tinfo,
+                                 const int32_t* __restrict__ cfirst,
+                                 const int32_t* __restrict__ tfirst,
+                                 const LevelRecord* __restrict__ drec,
+                                 const double* __restrict__ dmom, double* __restrict__ adj) {
   int base = 0;
   for (int l = 0; l < level; ++l) base += lvl[l];
   const int cnt = lvl[level];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
-    const int64_t u = twiglist[base + i];
-    const int2 mu = meta[u];
-    const double4 pc = nc4[u];
-    const double A = mom[kMomStride * u + kMomAbs];
+    const int P = base + i;
+    const int64_t u = twiglist[P];
+    const int2 ti = tinfo[P];
+    const int nc = ti.x & 0xff;
+    const unsigned lm = (unsigned)ti.x >> 8;  // leaf children, by slot
+    const LevelRecord* rc = drec + cfirst[P] + 1;  // child slot 0
+    const int ts = tfirst[P] + 1;                  // twig-list position of the first twig child
+    const double4 pc = drec[ti.y].pos;
+    const double A = drec[ti.y].ab.x;
     const double* pa = adj + kNA * u;
     const double Pq = pa[0];
     const double Pp[3] = {pa[1], pa[2], pa[3]};
     const double PQ[6] = {pa[4], pa[5], pa[6], pa[7], pa[8], pa[9]};
     double cocbar[3] = {pa[10], pa[11], pa[12]};
     const double PA = pa[13];
-    int64_t ch[8];
-    int nc = 0;
-    for (int64_t c = u + 1; c < mu.x && nc < 8; c = meta[c].x) ch[nc++] = c;
     // first pass: everything except the centre-of-charge chain rule
     for (int k = 0; k < nc; ++k) {
-      const int64_t c = ch[k];
-      const double4 cc = nc4[c];
-      const bool leafc = (meta[c].y & kLeafFlag) != 0;
+      const double4 cc = rc[k].pos;
+      const bool leafc = (lm >> k) & 1u;
       double pcv[3] = {0, 0, 0};
-      if (!leafc)
-        for (int i = 0; i < 3; ++i) pcv[i] = mom[kMomStride * c + i];
+      if (!leafc) {
+        const double* dm = dmom + 9 * (int64_t)(ts + __popc(~lm & ((1u << k) - 1u)));
+        for (int j = 0; j < 3; ++j) pcv[j] = dm[j];
+      }
       const double qc = cc.w;
       const double sc[3] = {pc.x - cc.x, pc.y - cc.y, pc.z - cc.z};
       double sbar[3] = {0, 0, 0};
-      for (int i = 0; i < 3; ++i) sbar[i] += Pp[i] * qc;
-      for (int i = 0; i < 3; ++i) sbar[i] += PQ[i] * (pcv[i] + qc * sc[i]);
+      for (int j = 0; j < 3; ++j) sbar[j] += Pp[j] * qc;
+      for (int j = 0; j < 3; ++j) sbar[j] += PQ[j] * (pcv[j] + qc * sc[j]);
       sbar[0] += PQ[3] * (pcv[1] + qc * sc[1]); sbar[1] += PQ[3] * (pcv[0] + qc * sc[0]);
       sbar[1] += PQ[4] * (pcv[2] + qc * sc[2]); sbar[2] += PQ[4] * (pcv[1] + qc * sc[1]);
       sbar[2] += PQ[5] * (pcv[0] + qc * sc[0]); sbar[0] += PQ[5] * (pcv[2] + qc * sc[2]);
-      double* a = adj + kNA * c;
+      double* a = adj + kNA * (int64_t)rc[k].link.w;
       double aq = Pq;
-      for (int i = 0; i < 3; ++i) aq += Pp[i] * sc[i] + PQ[i] * 0.5 * sc[i] * sc[i];
+      for (int j = 0; j < 3; ++j) aq += Pp[j] * sc[j] + PQ[j] * 0.5 * sc[j] * sc[j];
       aq += PQ[3] * sc[0] * sc[1] + PQ[4] * sc[1] * sc[2] + PQ[5] * sc[2] * sc[0];
       a[0] += aq;
       a[1] += Pp[0] + PQ[0] * sc[0] + PQ[3] * sc[1] + PQ[5] * sc[2];
       a[2] += Pp[1] + PQ[1] * sc[1] + PQ[3] * sc[0] + PQ[4] * sc[2];
       a[3] += Pp[2] + PQ[2] * sc[2] + PQ[4] * sc[1] + PQ[5] * sc[0];
-      for (int s = 0; s < 6; ++s) a[4 + s] += PQ[s];
-      for (int i = 0; i < 3; ++i) {
-        a[10 + i] -= sbar[i];
-        cocbar[i] += sbar[i];
+      for (int s2 = 0; s2 < 6; ++s2) a[4 + s2] += PQ[s2];
+      for (int j = 0; j < 3; ++j) {
+        a[10 + j] -= sbar[j];
+        cocbar[j] += sbar[j];
       }
       a[13] += PA;
     }
     // second pass: coc = sum coc_c A_c / A (or the plain mean when A = 0)
     for (int k = 0; k < nc; ++k) {
-      const int64_t c = ch[k];
-      const double4 cc = nc4[c];
-      const bool leafc = (meta[c].y & kLeafFlag) != 0;
-      double* a = adj + kNA * c;
+      const double4 cc = rc[k].pos;
+      double* a = adj + kNA * (int64_t)rc[k].link.w;
       if (A != 0.0) {
-        const double Ac = leafc ? fabs(cc.w) : mom[kMomStride * c + kMomAbs];
+        const double Ac = rc[k].ab.x;  // abs_charge (a leaf's |q|)
         const double w = Ac / A;
         const double cv[3] = {cc.x, cc.y, cc.z};
         const double pv[3] = {pc.x, pc.y, pc.z};
         double g = 0.0;
-        for (int i = 0; i < 3; ++i) {
-          a[10 + i] += cocbar[i] * w;
-          g += cocbar[i] * (cv[i] - pv[i]);
+        for (int j = 0; j < 3; ++j) {
+          a[10 + j] += cocbar[j] * w;
+          g += cocbar[j] * (cv[j] - pv[j]);
         }
         a[13] += g / A;
       } else {
-        for (int i = 0; i < 3; ++i) a[10 + i] += cocbar[i] / (double)nc;
+        for (int j = 0; j < 3; ++j) a[10 + j] += cocbar[j] / (double)nc;
       }
     }
   }
@@ -709,8 +717,9 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
     if (cnt <= 0) continue;
     const unsigned gl = (unsigned)std::min<int64_t>((cnt + 255) / 256, 148 * 16);
     COUNT_LAUNCH();
-    k_adj_down_level<<<gl, 256, 0, s>>>(L, c->lvlcnt.p, c->twiglist.p, c->meta.p, c->nc4.p,
-                                        c->mom.p, c->adj.p);
+    k_adj_down_level<<<gl, 256, 0, s>>>(L, c->lvlcnt.p, c->twiglist.p, c->tinfo.p,
+                                        c->tcounts.p, c->tcounts.p + c->ntwig, c->drec.p,
+                                        c->dmom.p, c->adj.p);
   }
   COUNT_LAUNCH();
   k_adj_out<<<g, 256, 0, s>>>(c->n, c->leafnode.p, c->perm.p, c->q.p, c->adj.p, dq, dx, dy, dz);

@@ -1127,6 +1127,7 @@ struct AdjMixArgs {
   const int2* meta;
   const float4* mom32;
   const int32_t* nleaves;
+  const LevelRecord* drec;  // level-ordered node records with walk links (grow.cu)
   const double* bl2;
   const double* macb;
   const double* vbox;
@@ -1158,8 +1159,7 @@ __device__ __forceinline__ void adj_add(double* __restrict__ a, float2 v) {
 // gradient takes 88 ms against 111 ms at five blocks (96 registers, spills).
 template <bool kWithE>
 __global__ void __launch_bounds__(kMixThreads, 4)
-    k_adj_group64(AdjMixArgs A, int* __restrict__ gstack, const int4* __restrict__ child8,
-                  const int* __restrict__ nchild) {
+    k_adj_group64(AdjMixArgs A, int* __restrict__ gstack) {
   __shared__ float s_bl2[kMaxLevel + 1];
   __shared__ double s_vb[3 * 125];
   __shared__ StagedTwig s_tw[kWW][kRing];
@@ -1257,7 +1257,7 @@ __global__ void __launch_bounds__(kMixThreads, 4)
           float2 axx = f2(0.f), ayy = f2(0.f), azz = f2(0.f), axy = f2(0.f), ayz = f2(0.f),
                  azx = f2(0.f), acx = f2(0.f), acy = f2(0.f), acz = f2(0.f);
           float2 aGx = f2(0.f), aGy = f2(0.f), aGz = f2(0.f);  // sum of 2 R2 g (with E)
-#pragma unroll 2
+#pragma unroll 4
           for (int p = 0; p < 32; ++p) {
             const float4 ta4 = tg[p][0], tb4 = tg[p][1];
             const float2 dx = __fadd2_rn(make_float2(ta4.x, ta4.y), CX);
@@ -1481,16 +1481,18 @@ __global__ void __launch_bounds__(kMixThreads, 4)
         bool isleaf = false, accept = false, open = false, amb = false;
         float cx = 0.f, cy = 0.f, cz = 0.f, bl = 0.f;
         double4 a = make_double4(0, 0, 0, 0);
-        int nlv = 0, nch = 0;
-        int4 c0 = make_int4(0, 0, 0, 0), c1 = c0;
+        // the node's level-ordered record and links (k_walk_group64's traversal);
+        // the adjoint records are indexed by the RPO index, lk.w
+        int4 lk = make_int4(0, 0, 0, 0);
         if (node >= 0) {
-          a = A.nc4[node];
-          const int2 mu = A.meta[node];
+          const LevelRecord* rec = A.drec + node;
+          a = rec->pos;
+          lk = rec->link;
           cx = (float)(a.x - gx); cy = (float)(a.y - gy); cz = (float)(a.z - gz);
-          if (mu.y & kLeafFlag) {
+          if (lk.y & kLeafFlag) {
             isleaf = true;
           } else {
-            bl = A.macb ? (float)A.macb[node] : s_bl2[mu.y & 0xff];
+            bl = A.macb ? (float)A.macb[lk.w] : s_bl2[lk.y & 0xff];
             const float dc = sqrtf(cx * cx + cy * cy + cz * cz);
             const float dmin = dc - rg, dmax = dc + rg;
             if (dmin > 0.f && theta2 * (dmin * dmin) > bl) {
@@ -1526,33 +1528,27 @@ __global__ void __launch_bounds__(kMixThreads, 4)
                                                        : __popc(vm1)));
           }
         }
-        if (open) {
-          nch = nchild[node];
-          c0 = child8[2 * (int64_t)node];
-          c1 = child8[2 * (int64_t)node + 1];
-        }
-        if (accept) nlv = A.nleaves[node];
         const unsigned lb = __ballot_sync(0xffffffffu, isleaf);
         const unsigned ab = __ballot_sync(0xffffffffu, accept);
         if (isleaf) {
           StagedLeafA& r = stl[(hL + nL + __popc(lb & lt)) & (kRing - 1)];
           r.c = make_float4(cx, cy, cz, (float)a.w);
           r.x = a.x; r.y = a.y; r.z = a.z;
-          r.node = node;
+          r.node = lk.w;
           partner += 1;
         }
         if (accept) {
           StagedTwig& r = stw[(hT + nT + __popc(ab & lt)) & (kRing - 1)];
-          r.c = make_float4(-cx, -cy, -cz, __int_as_float(node));
-          const float4* m = A.mom32 + kMom32Stride * (int64_t)node;
+          r.c = make_float4(-cx, -cy, -cz, __int_as_float(lk.w));
+          const float4* m = A.mom32 + kMom32Stride * (int64_t)lk.w;
           cp_async16(&r.m0, m);
           cp_async16(&r.m1, m + 1);
           cp_async16(&r.m2, m + 2);
-          partner += nlv;
+          partner += lk.z;
         }
         nL += __popc(lb);
         nT += __popc(ab);
-        const int npush = open ? min(8, nch) : 0;
+        const int npush = open ? min(8, lk.y >> 16) : 0;
         int total;
         const int off = warp_excl_scan(npush, lane, total);
         if (top + total > kStackCap) {
@@ -1561,14 +1557,9 @@ __global__ void __launch_bounds__(kMixThreads, 4)
         }
         if (npush > 0) {
           int* dst = stack + top + off;
-          dst[0] = c0.x;
-          if (npush > 1) dst[1] = c0.y;
-          if (npush > 2) dst[2] = c0.z;
-          if (npush > 3) dst[3] = c0.w;
-          if (npush > 4) dst[4] = c1.x;
-          if (npush > 5) dst[5] = c1.y;
-          if (npush > 6) dst[6] = c1.z;
-          if (npush > 7) dst[7] = c1.w;
+#pragma unroll
+          for (int k = 0; k < 8; ++k)
+            if (k < npush) dst[k] = lk.x + k;
         }
         top += total;
         __syncwarp();
@@ -1666,6 +1657,7 @@ int launch_adjoint_group64(Ctx* c, int64_t nt, const double* tx, const double* t
   A.meta = c->meta.p;
   A.mom32 = reinterpret_cast<const float4*>(c->mom32.p);
   A.nleaves = c->nleaves.p;
+  A.drec = c->drec.p;
   A.bl2 = c->d_box + 9;
   {
     int rc = prepare_mac(c, &A.macb);
@@ -1687,9 +1679,9 @@ int launch_adjoint_group64(Ctx* c, int64_t nt, const double* tx, const double* t
   k_reset_mixed<<<1, 1, 0, s>>>(A.queue);
   COUNT_LAUNCH();
   if (with_e)
-    k_adj_group64<true><<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p, c->child8.p, c->nchild.p);
+    k_adj_group64<true><<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p);
   else
-    k_adj_group64<false><<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p, c->child8.p, c->nchild.p);
+    k_adj_group64<false><<<gblocks, kMixThreads, 0, s>>>(A, c->wstack.p);
   return cuda_ok(c, cudaGetLastError(), "mixed adjoint launch") ? PEPCG_OK : PEPCG_ERR_CUDA;
 }
 
