@@ -249,6 +249,7 @@ struct AdjArgs {
   int nsub;
   const int32_t* sublist;
   const int32_t* parent;
+  const int32_t* lvlpos;  // RPO index -> the adjoint record's position (level order)
   unsigned int* queue;             // bucket counter (k_adj_group), zeroed before the launch
   unsigned long long* item_queue;  // item counter (k_adj_target), zeroed before the launch
   // spatial_interaction_cutoff: an interaction whose offset has any |component|
@@ -355,7 +356,7 @@ __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_target(AdjArgs A) {
         if (cm != 0u && __popc(cm) <= kDirectLanes) {
           // few contributors: each adds its own record, no warp reduction
           if (contrib) {
-            double* d = A.adj + (int64_t)kNA * u;
+            double* d = A.adj + (int64_t)kNA * A.lvlpos[u];
 #pragma unroll
             for (int k = 0; k < 13; ++k) {
               if ((leaf && k >= 1 && k < 10) || a[k] == 0.0) continue;
@@ -364,7 +365,7 @@ __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_target(AdjArgs A) {
             }
           }
         } else if (cm != 0u) {
-          flush_smem(A.adj, u, a, lane, leaf, sred);
+          flush_smem(A.adj, (unsigned)A.lvlpos[u], a, lane, leaf, sred);
         }
       }
     }
@@ -429,7 +430,7 @@ __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_group(AdjArgs A) {
           for (int s = 0; s < kTPL; ++s)
             if (valid[s] && dist2[s] > 0.0 && !adj_cut(A, dx[s], dy[s], dz[s]))
               leaf_adj_law<kLaw>(nd.w, dx[s], dy[s], dz[s], A.eps2, gp[s], gE[s], a);
-          flush_smem(A.adj, u, a, lane, true, sred);
+          flush_smem(A.adj, (unsigned)A.lvlpos[u], a, lane, true, sred);
           u = (unsigned)fw.y;
         } else {
           const double thr = A.macb ? A.macb[u] : s_bl2[mu.y & 0xff];
@@ -447,7 +448,7 @@ __global__ void __launch_bounds__(kAdjThreads, 5) k_adj_group(AdjArgs A) {
                   twig_adj_law<kWithE, kLaw>(nd.w, m, dx[s], dy[s], dz[s], A.eps2, gp[s],
                                              gE[s], a);
             }
-            flush_smem(A.adj, u, a, lane, false, sred);
+            flush_smem(A.adj, (unsigned)A.lvlpos[u], a, lane, false, sred);
             u = (unsigned)fw.y;
           } else {
             u = (unsigned)fw.x;
@@ -486,7 +487,7 @@ __global__ void k_adj_down_level(int level, const int32_t* __restrict__ lvl,
     const int ts = tfirst[P] + 1;                  // twig-list position of the first twig child
     const double4 pc = drec[ti.y].pos;
     const double A = drec[ti.y].ab.x;
-    const double* pa = adj + kNA * u;
+    const double* pa = adj + kNA * (int64_t)ti.y;
     const double Pq = pa[0];
     const double Pp[3] = {pa[1], pa[2], pa[3]};
     const double PQ[6] = {pa[4], pa[5], pa[6], pa[7], pa[8], pa[9]};
@@ -509,7 +510,7 @@ __global__ void k_adj_down_level(int level, const int32_t* __restrict__ lvl,
       sbar[0] += PQ[3] * (pcv[1] + qc * sc[1]); sbar[1] += PQ[3] * (pcv[0] + qc * sc[0]);
       sbar[1] += PQ[4] * (pcv[2] + qc * sc[2]); sbar[2] += PQ[4] * (pcv[1] + qc * sc[1]);
       sbar[2] += PQ[5] * (pcv[0] + qc * sc[0]); sbar[0] += PQ[5] * (pcv[2] + qc * sc[2]);
-      double* a = adj + kNA * (int64_t)rc[k].link.w;
+      double* a = adj + kNA * (int64_t)(cfirst[P] + 1 + k);
       double aq = Pq;
       for (int j = 0; j < 3; ++j) aq += Pp[j] * sc[j] + PQ[j] * 0.5 * sc[j] * sc[j];
       aq += PQ[3] * sc[0] * sc[1] + PQ[4] * sc[1] * sc[2] + PQ[5] * sc[2] * sc[0];
@@ -527,7 +528,7 @@ __global__ void k_adj_down_level(int level, const int32_t* __restrict__ lvl,
     // second pass: coc = sum coc_c A_c / A (or the plain mean when A = 0)
     for (int k = 0; k < nc; ++k) {
       const double4 cc = rc[k].pos;
-      double* a = adj + kNA * (int64_t)rc[k].link.w;
+      double* a = adj + kNA * (int64_t)(cfirst[P] + 1 + k);
       if (A != 0.0) {
         const double Ac = rc[k].ab.x;  // abs_charge (a leaf's |q|)
         const double w = Ac / A;
@@ -548,12 +549,13 @@ __global__ void k_adj_down_level(int level, const int32_t* __restrict__ lvl,
 
 // leaves -> particles in the caller's original order
 __global__ void k_adj_out(int64_t n, const int32_t* __restrict__ leafnode,
+                          const int32_t* __restrict__ lvlpos,
                           const int32_t* __restrict__ perm, const double* __restrict__ q,
                           const double* __restrict__ adj, double* dq, double* dx, double* dy,
                           double* dz) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const double* a = adj + (int64_t)kNA * leafnode[i];
+    const double* a = adj + (int64_t)kNA * lvlpos[leafnode[i]];
     const int64_t o = perm[i];
     const double sg = (double)((q[i] > 0.0) - (q[i] < 0.0));
     dq[o] = a[0] + a[13] * sg;
@@ -658,6 +660,7 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
   A.nsub = 0;
   A.sublist = nullptr;
   A.parent = c->parent.p;
+  A.lvlpos = c->lvlpos.p;
   A.has_cut = has_spatial_cutoff(c->prm) ? 1 : 0;
   for (int k = 0; k < 3; ++k) A.cut[k] = c->prm.spatial_interaction_cutoff[k];
   const bool per_target = (c->prm.walk == PEPCG_WALK_PER_TARGET);
@@ -722,7 +725,8 @@ int adjoint_device(Ctx* c, int64_t nt, const double* tx, const double* ty, const
                                         c->dmom.p, c->adj.p);
   }
   COUNT_LAUNCH();
-  k_adj_out<<<g, 256, 0, s>>>(c->n, c->leafnode.p, c->perm.p, c->q.p, c->adj.p, dq, dx, dy, dz);
+  k_adj_out<<<g, 256, 0, s>>>(c->n, c->leafnode.p, c->lvlpos.p, c->perm.p, c->q.p, c->adj.p, dq,
+                              dx, dy, dz);
   if (!cuda_ok(c, cudaGetLastError(), "adjoint")) return PEPCG_ERR_CUDA;
   // the periodic far-lattice term's adjoint (FP64, lattice.cu) adds to the walk's
   return c->far_field ? lattice_adjoint(c, nt, tx, ty, tz, gex, gey, gez, gphi, dq, dx, dy, dz)

@@ -387,7 +387,7 @@ int pepcg_destroy(void* ctx) {
   release(c->nc4); release(c->meta); release(c->fwd); release(c->fwdf); release(c->tflag); release(c->tpack); release(c->mom);
   release(c->mom32);
   release(c->parent); release(c->nchild); release(c->twiglist); release(c->lvlcnt); release(c->lvlblk);
-  release(c->drec); release(c->dmom);
+  release(c->drec); release(c->lvlpos); release(c->dmom);
   release(c->tinfo); release(c->tcounts); release(c->macb); release(c->first_part);
   release(c->nleaves); release(c->child8); release(c->wstack); release(c->leafnode);
   release(c->adj); release(c->fpo2rpo); release(c->rpo2fpo); release(c->nkey);

@@ -825,6 +825,7 @@ __global__ void __launch_bounds__(256) k_level_scatter(int64_t M, const int2* __
                                                        int nblk, int32_t* __restrict__ twiglist,
                                                        const double4* __restrict__ nc4,
                                                        LevelRecord* __restrict__ drec,
+                                                       int32_t* __restrict__ lvlpos,
                                                        const int4* __restrict__ child8,
                                                        const int32_t* __restrict__ nchild,
                                                        int2* __restrict__ tinfo,
@@ -854,6 +855,7 @@ __global__ void __launch_bounds__(256) k_level_scatter(int64_t M, const int2* __
   __syncthreads();
   if (L < 0) return;
   const int p = bofs_all[(int64_t)L * nblk + blockIdx.x] + wa[warp][L] + ra;
+  lvlpos[u] = p;
   if (!leaf) {
     const int P = bofs_twig[(int64_t)L * nblk + blockIdx.x] + wt[warp][L] + rt;
     twiglist[P] = (int32_t)u;
@@ -1239,7 +1241,8 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
     const size_t nlb = (size_t)(kMaxLevel + 1) * gM;
     const int64_t ntw = M - n;
     if (!ensure(c, c->lvlblk, 2 * nlb, "level blocks") ||
-        !ensure(c, c->drec, M, "level records") || !ensure(c, c->dmom, 9 * ntw, "dmom") ||
+        !ensure(c, c->drec, M, "level records") || !ensure(c, c->lvlpos, M, "level positions") ||
+        !ensure(c, c->dmom, 9 * ntw, "dmom") ||
         !ensure(c, c->tinfo, ntw, "twig info") || !ensure(c, c->tcounts, 2 * ntw, "twig counts"))
       return PEPCG_ERR_OOM;
     int32_t* bt = c->lvlblk.p;
@@ -1252,7 +1255,7 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
     int32_t* cc = c->tcounts.p;
     int32_t* tcn = c->tcounts.p + ntw;
     k_level_scatter<<<gM, kThreads, 0, s>>>(M, c->meta.p, bt, ba, (int)gM, c->twiglist.p,
-                                            c->nc4.p, c->drec.p, c->child8.p,
+                                            c->nc4.p, c->drec.p, c->lvlpos.p, c->child8.p,
                                             c->nchild.p, c->tinfo.p, cc, tcn);
     exclusive_scan<int32_t>(cc, cc, ntw, c->scan_tmp.p, s);
     exclusive_scan<int32_t>(tcn, tcn, ntw, c->scan_tmp.p, s);

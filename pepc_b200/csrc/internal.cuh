@@ -128,6 +128,7 @@ struct Ctx {
   // level-ordered copy of the node records for the upward pass: centre /
   // charge and (abs_charge, bmax); the twigs' moments by twig-list position
   DBuf<LevelRecord> drec;
+  DBuf<int32_t> lvlpos;    // RPO index -> position in drec (the adjoint records' order)
   DBuf<double> dmom;
   DBuf<int2> tinfo;        // per twig-list position: child count | leaf mask << 8, own position
   DBuf<int32_t> tcounts;   // per twig-list position: children, then twig children (scanned)

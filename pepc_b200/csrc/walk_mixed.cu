@@ -1134,7 +1134,7 @@ struct AdjMixArgs {
   int nbox;
   float theta2, eps2;
   int64_t npart;
-  double* adj;  // 16 doubles per node: q, p(3), Q(6: xx yy zz xy yz zx), coc(3), abs_charge, pad
+  double* adj;  // 16 doubles per node, level order: q, p(3), Q(6: xx yy zz xy yz zx), coc(3), abs_charge, pad
   unsigned long long* counters;
   uint32_t* status;
   unsigned int* queue;
@@ -1482,7 +1482,7 @@ __global__ void __launch_bounds__(kMixThreads, 4)
         float cx = 0.f, cy = 0.f, cz = 0.f, bl = 0.f;
         double4 a = make_double4(0, 0, 0, 0);
         // the node's level-ordered record and links (k_walk_group64's traversal);
-        // the adjoint records are indexed by the RPO index, lk.w
+        // the adjoint records are in the same level order
         int4 lk = make_int4(0, 0, 0, 0);
         if (node >= 0) {
           const LevelRecord* rec = A.drec + node;
@@ -1534,12 +1534,12 @@ __global__ void __launch_bounds__(kMixThreads, 4)
           StagedLeafA& r = stl[(hL + nL + __popc(lb & lt)) & (kRing - 1)];
           r.c = make_float4(cx, cy, cz, (float)a.w);
           r.x = a.x; r.y = a.y; r.z = a.z;
-          r.node = lk.w;
+          r.node = node;
           partner += 1;
         }
         if (accept) {
           StagedTwig& r = stw[(hT + nT + __popc(ab & lt)) & (kRing - 1)];
-          r.c = make_float4(-cx, -cy, -cz, __int_as_float(lk.w));
+          r.c = make_float4(-cx, -cy, -cz, __int_as_float(node));
           const float4* m = A.mom32 + kMom32Stride * (int64_t)lk.w;
           cp_async16(&r.m0, m);
           cp_async16(&r.m1, m + 1);
