@@ -372,7 +372,8 @@ void sort_scatter(int64_t n, const uint64_t* kin, const int32_t* vin, uint64_t* 
 }
 
 // ---------------------------------------------------------------------------
-// Exclusive scans (uint32 / int32): reduce per block, scan block sums, apply.
+// Exclusive scans (uint32 / int32): reduce per block, then apply (each block
+// adding the sums of the blocks before it).
 // ---------------------------------------------------------------------------
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kThreads * kScanItems;  // 2048
@@ -418,26 +419,20 @@ __global__ void k_scan_reduce(const T* __restrict__ in, int64_t n, T* __restrict
   if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
 }
 
-template <class T>
-__global__ void k_scan_blocks(T* __restrict__ bsum, int64_t nb) {
-  // single block: sequential over tiles of kThreads
-  __shared__ T sm[32];
-  T carry = 0;
-  for (int64_t b0 = 0; b0 < nb; b0 += kThreads) {
-    int64_t i = b0 + threadIdx.x;
-    T v = i < nb ? bsum[i] : T(0);
-    T tot;
-    T ex = block_exclusive_scan<T>(v, sm, tot);
-    if (i < nb) bsum[i] = carry + ex;
-    carry += tot;
-  }
-  if (threadIdx.x == 0) bsum[nb] = carry;
-}
-
+// Each block adds the sums of the blocks before it itself (at most a few
+// thousand integers, read from L2) instead of a separate single-block scan of
+// the block sums: one launch fewer per scan.
 template <class T>
 __global__ void k_scan_apply(const T* __restrict__ in, int64_t n, const T* __restrict__ bsum,
                              T* __restrict__ out) {
   __shared__ T sm[32];
+  T pre = 0;
+  for (int64_t b = threadIdx.x; b < (int64_t)blockIdx.x; b += blockDim.x) pre += bsum[b];
+  {
+    T t;
+    block_exclusive_scan<T>(pre, sm, t);
+    pre = t;
+  }
   int64_t base = (int64_t)blockIdx.x * kScanTile;
   T v[kScanItems];
   T s = 0;
@@ -447,7 +442,7 @@ __global__ void k_scan_apply(const T* __restrict__ in, int64_t n, const T* __res
     s += v[k];
   }
   T tot;
-  T ex = block_exclusive_scan<T>(s, sm, tot) + bsum[blockIdx.x];
+  T ex = block_exclusive_scan<T>(s, sm, tot) + pre;
   for (int k = 0; k < kScanItems; ++k) {
     int64_t i = base + (int64_t)threadIdx.x * kScanItems + k;
     if (i < n) out[i] = ex;
@@ -460,8 +455,6 @@ void exclusive_scan(const T* in, T* out, int64_t n, T* tmp, cudaStream_t s) {
   int64_t nb = (n + kScanTile - 1) / kScanTile;
   COUNT_LAUNCH();
   k_scan_reduce<T><<<(unsigned)nb, kThreads, 0, s>>>(in, n, tmp);
-  COUNT_LAUNCH();
-  k_scan_blocks<T><<<1, kThreads, 0, s>>>(tmp, nb);
   COUNT_LAUNCH();
   k_scan_apply<T><<<(unsigned)nb, kThreads, 0, s>>>(in, n, tmp, out);
 }
