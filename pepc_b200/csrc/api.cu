@@ -342,12 +342,16 @@ int pepcg_create(void** out, const pepcg_params* p) {
     return PEPCG_ERR_CUDA;
   }
   c->own_stream = true;
-  for (int i = 0; i < 8; ++i) cudaEventCreate(&c->ev[i]);
+  for (int i = 0; i < Ctx::kEvents; ++i) cudaEventCreate(&c->ev[i]);
   bool ok = cuda_ok(nullptr, cudaMalloc((void**)&c->d_box, 64 * sizeof(double)), "box") &&
             cuda_ok(nullptr, cudaMalloc((void**)&c->d_status, 16), "status") &&
             cuda_ok(nullptr, cudaMalloc((void**)&c->d_small, 16 * sizeof(unsigned long long)), "small") &&
             cuda_ok(nullptr, cudaMalloc((void**)&c->d_vbox, 3 * 125 * sizeof(double)), "vbox") &&
-            cuda_ok(nullptr, cudaMalloc((void**)&c->d_part, 6 * 512 * sizeof(double)), "part");
+            cuda_ok(nullptr, cudaMalloc((void**)&c->d_part, 6 * 512 * sizeof(double)), "part") &&
+            cuda_ok(nullptr, cudaHostAlloc((void**)&c->h_sum, sizeof(Ctx::GrowSummary),
+                                           cudaHostAllocMapped), "grow summary") &&
+            cuda_ok(nullptr, cudaHostGetDevicePointer((void**)&c->d_sum, c->h_sum, 0), "grow summary") &&
+            cuda_ok(nullptr, cudaEventCreateWithFlags(&c->sum_ev, cudaEventDisableTiming), "grow summary");
   if (!ok) {
     pepcg_destroy(c);
     return PEPCG_ERR_CUDA;
@@ -396,8 +400,10 @@ int pepcg_destroy(void* ctx) {
                   (void*)c->d_part, (void*)c->d_mlattice, (void*)c->d_omega, (void*)c->d_mu,
                   (void*)c->d_fmm_aux, (void*)c->d_factorial})
     if (p) cudaFree(p);
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < Ctx::kEvents; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  if (c->h_sum) cudaFreeHost(c->h_sum);
+  if (c->sum_ev) cudaEventDestroy(c->sum_ev);
   for (int i = 0; i < Ctx::kMaxChunks; ++i) {
     if (c->ready[i]) cudaEventDestroy(c->ready[i]);
     if (c->done[i]) cudaEventDestroy(c->done[i]);
@@ -486,19 +492,30 @@ int pepcg_grow_tree(void* ctx, int64_t n, const double* x, const double* y, cons
       !ensure(c, c->in_z, n, "in_z") || !ensure(c, c->in_q, n, "in_q"))
     return PEPCG_ERR_OOM;
   cudaStream_t s = c->stream;
+  if (!copy_streams(c)) return PEPCG_ERR_CUDA;
+  // x y z on the context stream; the charges follow on the upload stream and
+  // cross PCIe while the keys are formed and sorted (the gather into key order
+  // is the first step that reads them)
   if (!cuda_ok(c, cudaMemcpyAsync(c->in_x.p, x, n * 8, cudaMemcpyHostToDevice, s), "H2D x") ||
       !cuda_ok(c, cudaMemcpyAsync(c->in_y.p, y, n * 8, cudaMemcpyHostToDevice, s), "H2D y") ||
       !cuda_ok(c, cudaMemcpyAsync(c->in_z.p, z, n * 8, cudaMemcpyHostToDevice, s), "H2D z") ||
-      !cuda_ok(c, cudaMemcpyAsync(c->in_q.p, q, n * 8, cudaMemcpyHostToDevice, s), "H2D q"))
-    return PEPCG_ERR_CUDA;
-  int rc = pepcg_grow_tree_device(c, n, c->in_x.p, c->in_y.p, c->in_z.p, c->in_q.p);
-  if (rc && rc != PEPCG_WARN_NOT_NEUTRAL) return rc;
-  // The outputs are final once the duplicate fix has run (event 2, before the
-  // tree build): copy them back on the device-to-host stream while the tree
-  // build and the upward pass run on the context stream.  The call returns
-  // when the copies are done; the rest of the grow stays stream-ordered
-  // before the next call's work.
-  if (!copy_streams(c)) return PEPCG_ERR_CUDA;
+      !cuda_ok(c, cudaEventRecord(c->fork, s), "H2D q") ||
+      !cuda_ok(c, cudaStreamWaitEvent(c->h2d, c->fork, 0), "H2D q") ||
+      !cuda_ok(c, cudaMemcpyAsync(c->in_q.p, q, n * 8, cudaMemcpyHostToDevice, c->h2d), "H2D q") ||
+      !cuda_ok(c, cudaEventRecord(c->join, c->h2d), "H2D q"))
+    return drain_copies(c, false), PEPCG_ERR_CUDA;
+  int rc = grow_device(c, n, c->in_x.p, c->in_y.p, c->in_z.p, c->in_q.p, c->join);
+  if (rc) return drain_copies(c, false), rc;
+  if (c->far_field) {
+    rc = lattice_timestep(c);
+    if (rc && rc != PEPCG_WARN_NOT_NEUTRAL) return drain_copies(c, false), rc;
+  }
+  c->grow_times_pending = true;
+  // The outputs are final once the particles stand in key order and the
+  // duplicate fix has run (event 2, before the tree build): copy them back on
+  // the device-to-host stream while the tree build and the upward pass run on
+  // the context stream.  The call returns when the copies are done; the rest
+  // of the grow stays stream-ordered before the next call's work.
   cudaStream_t t = c->d2h;
   bool ok = cuda_ok(c, cudaStreamWaitEvent(t, c->ev[2], 0), "grow outputs");
   if (key_out)
@@ -767,8 +784,15 @@ int pepcg_stats_get(void* ctx, pepcg_stats* s) {
   if (c->grow_times_pending && cudaEventSynchronize(c->ev[4]) == cudaSuccess) {
     float ms = 0;
     if (cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]) == cudaSuccess) c->st.t_keys_ms = ms;
-    if (cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]) == cudaSuccess) c->st.t_sort_ms = ms;
-    if (cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]) == cudaSuccess) c->st.t_tree_ms = ms;
+    // the particle gather (a sort-phase step) runs after the node counts (a
+    // tree-phase step), while the host reads the grow summary
+    float a = 0, b = 0;
+    if (cudaEventElapsedTime(&a, c->ev[1], c->ev[8]) == cudaSuccess &&
+        cudaEventElapsedTime(&b, c->ev[9], c->ev[2]) == cudaSuccess)
+      c->st.t_sort_ms = a + b;
+    if (cudaEventElapsedTime(&a, c->ev[8], c->ev[9]) == cudaSuccess &&
+        cudaEventElapsedTime(&b, c->ev[2], c->ev[3]) == cudaSuccess)
+      c->st.t_tree_ms = a + b;
     if (cudaEventElapsedTime(&ms, c->ev[3], c->ev[4]) == cudaSuccess) c->st.t_upward_ms = ms;
     c->grow_times_pending = false;
   }

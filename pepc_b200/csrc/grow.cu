@@ -186,7 +186,7 @@ __global__ void k_keys(int64_t n, const double* __restrict__ x, const double* __
        i += (int64_t)gridDim.x * blockDim.x) {
     const double xi = x[i], yi = y[i], zi = z[i];
     // the particle, packed in input order for the permutation's gather
-    packed[i] = make_double4(xi, yi, zi, q[i]);
+    packed[i] = make_double4(xi, yi, zi, q ? q[i] : 0.0);
     const int64_t i0 = quantise(xi, sb[0], sb[3], sb[6]);
     const int64_t i1 = quantise(yi, sb[1], sb[4], sb[7]);
     const int64_t i2 = quantise(zi, sb[2], sb[5], sb[8]);
@@ -216,17 +216,20 @@ __global__ void k_keys(int64_t n, const double* __restrict__ x, const double* __
 }
 
 // ---------------------------------------------------------------------------
-// LSD radix sort of (uint64 key, int32 index), 8 passes of 8 bits, stable.
+// LSD radix sort of (uint64 key, int32 index), stable, digits of 8 or 9 bits.
 // Pass = per-block digit histogram -> exclusive scan over (digit, block) ->
-// stable scatter (warp match + block prefix per 256-key row).
+// stable scatter (per-bit ballots + block prefix per 256-key row).
 // ---------------------------------------------------------------------------
 constexpr int kSortRows = 16;                       // rows of 256 keys per block
 constexpr int kSortChunk = kSortRows * kThreads;    // 4096 keys per block
+constexpr int kMaxDigits = 512;                     // 9-bit digits at most
 
+template <int kBits>
 __global__ void k_sort_hist(int64_t n, const uint64_t* __restrict__ keys, int shift,
                             uint32_t* __restrict__ hist, int nblocks) {
-  __shared__ uint32_t h[256];
-  h[threadIdx.x] = 0;
+  constexpr int D = 1 << kBits;
+  __shared__ uint32_t h[D];
+  for (int d = threadIdx.x; d < D; d += kThreads) h[d] = 0;
   __syncthreads();
   const int64_t base = (int64_t)blockIdx.x * kSortChunk;
   uint64_t kr[kSortRows];  // every row's key requested before the first count
@@ -237,9 +240,9 @@ __global__ void k_sort_hist(int64_t n, const uint64_t* __restrict__ keys, int sh
   }
 #pragma unroll
   for (int r = 0; r < kSortRows; ++r)
-    if (base + r * kThreads + threadIdx.x < n) atomicAdd(&h[(kr[r] >> shift) & 255u], 1u);
+    if (base + r * kThreads + threadIdx.x < n) atomicAdd(&h[(kr[r] >> shift) & (D - 1)], 1u);
   __syncthreads();
-  hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+  for (int d = threadIdx.x; d < D; d += kThreads) hist[(int64_t)d * nblocks + blockIdx.x] = h[d];
 }
 
 // barrier for the first 256 threads of the block only (the digit lanes)
@@ -255,43 +258,50 @@ __device__ __forceinline__ void named_barrier_256() {
 // per-digit counts are then prefixed over the warps, which keeps the ranks
 // stable, and over the digits, which gives each digit's run in the tile.
 // The tile is sorted by digit in shared memory (the keys and indices re-read
-// from global memory, which keeps the kernel at 40 registers and three blocks
+// from global memory, which keeps the kernel small enough for three blocks
 // per SM) and written out in that order, so that consecutive threads store
 // consecutive addresses of a digit's run in the output (the run of digit d of
-// tile b starts at offs[d * nblocks + b]).
+// tile b starts at offs[d * nblocks + b]).  A warp's count of one digit is at
+// most 256, so the per-warp counts are 16-bit.
 constexpr int kScatterThreads = 512;
 constexpr int kWarpsSort = kScatterThreads / 32;
 constexpr int kPerWarp = kSortChunk / kWarpsSort;  // 256 keys
-constexpr int kScatterSmem = kSortChunk * 8 + kSortChunk * 4 + 2 * 256 * 4 + kWarpsSort * 256 * 4;
+template <int kBits>
+constexpr int scatter_smem() {
+  return kSortChunk * 8 + kSortChunk * 4 + 2 * (1 << kBits) * 4 + kWarpsSort * (1 << kBits) * 2;
+}
 
+template <int kBits>
 __global__ void __launch_bounds__(kScatterThreads, 3) k_sort_scatter(int64_t n, const uint64_t* __restrict__ kin,
                                                            const int32_t* __restrict__ vin,
                                                            uint64_t* __restrict__ kout,
                                                            int32_t* __restrict__ vout, int shift,
                                                            const uint32_t* __restrict__ offs,
                                                            int nblocks) {
+  constexpr int D = 1 << kBits;
+  static_assert(D == 256 || D == kScatterThreads, "one digit per prefix thread");
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ uint32_t wtot[8];
+  __shared__ uint32_t wtot[D / 32];
   uint64_t* sk = reinterpret_cast<uint64_t*>(smem);
   int32_t* sv = reinterpret_cast<int32_t*>(sk + kSortChunk);
   uint32_t* lstart = reinterpret_cast<uint32_t*>(sv + kSortChunk);  // tile-local run starts
-  uint32_t* gbase = lstart + 256;                                   // output run starts
-  uint32_t(*wcnt)[256] = reinterpret_cast<uint32_t(*)[256]>(gbase + 256);
+  uint32_t* gbase = lstart + D;                                     // output run starts
+  uint16_t(*wcnt)[D] = reinterpret_cast<uint16_t(*)[D]>(gbase + D);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   const int64_t base = (int64_t)blockIdx.x * kSortChunk;
   const int cnt = (int)min((int64_t)kSortChunk, n - base);
-  if (threadIdx.x < 256) gbase[threadIdx.x] = offs[(int64_t)threadIdx.x * nblocks + blockIdx.x];
-  for (int i = threadIdx.x; i < kWarpsSort * 256; i += kScatterThreads) (&wcnt[0][0])[i] = 0;
-  uint8_t dg[kPerWarp / 32];
+  if (threadIdx.x < D) gbase[threadIdx.x] = offs[(int64_t)threadIdx.x * nblocks + blockIdx.x];
+  for (int i = threadIdx.x; i < kWarpsSort * D; i += kScatterThreads) (&wcnt[0][0])[i] = 0;
+  uint16_t dg[kPerWarp / 32];
 #pragma unroll
   for (int j = 0; j < kPerWarp / 32; ++j) {
     const int i = warp * kPerWarp + j * 32 + lane;
-    dg[j] = i < cnt ? (uint8_t)((kin[base + i] >> shift) & 255u) : 0;
+    dg[j] = i < cnt ? (uint16_t)((kin[base + i] >> shift) & (D - 1)) : 0;
   }
   __syncthreads();
   int rk[kPerWarp / 32];
-  uint32_t* my = wcnt[warp];
+  uint16_t* my = wcnt[warp];
 #pragma unroll
   for (int j = 0; j < kPerWarp / 32; ++j) {
     const bool valid = warp * kPerWarp + j * 32 + lane < cnt;
@@ -300,7 +310,7 @@ __global__ void __launch_bounds__(kScatterThreads, 3) k_sort_scatter(int64_t n, 
     unsigned peers = __ballot_sync(0xffffffffu, valid);
     if (!valid) peers = ~peers;
 #pragma unroll
-    for (int bit = 0; bit < 8; ++bit) {
+    for (int bit = 0; bit < kBits; ++bit) {
       const bool on = (d >> bit) & 1;
       const unsigned m = __ballot_sync(0xffffffffu, on);
       peers &= on ? m : ~m;
@@ -310,17 +320,17 @@ __global__ void __launch_bounds__(kScatterThreads, 3) k_sort_scatter(int64_t n, 
     if (valid && lane == leader) c0 = my[d];
     c0 = __shfl_sync(0xffffffffu, c0, leader);
     rk[j] = (int)c0 + __popc(peers & lt);
-    if (valid && lane == leader) my[d] = c0 + __popc(peers);
+    if (valid && lane == leader) my[d] = (uint16_t)(c0 + __popc(peers));
     __syncwarp();
   }
   __syncthreads();
-  if (threadIdx.x < 256) {  // digit threadIdx.x: prefix over the warps, then the tile's run starts
+  if (threadIdx.x < D) {  // digit threadIdx.x: prefix over the warps, then the tile's run starts
     const int b = threadIdx.x;
     uint32_t run = 0;
 #pragma unroll
     for (int w = 0; w < kWarpsSort; ++w) {
       const uint32_t t = wcnt[w][b];
-      wcnt[w][b] = run;
+      wcnt[w][b] = (uint16_t)run;  // at most 4096 - 256: fits
       run += t;
     }
     uint32_t x = run;
@@ -330,7 +340,8 @@ __global__ void __launch_bounds__(kScatterThreads, 3) k_sort_scatter(int64_t n, 
       if (lane >= o) x += y;
     }
     if (lane == 31) wtot[warp] = x;
-    named_barrier_256();
+    if constexpr (D == kScatterThreads) __syncthreads();
+    else named_barrier_256();
     uint32_t pre = 0;
     for (int w = 0; w < warp; ++w) pre += wtot[w];
     lstart[b] = pre + x - run;
@@ -349,26 +360,11 @@ __global__ void __launch_bounds__(kScatterThreads, 3) k_sort_scatter(int64_t n, 
   __syncthreads();
   for (int i = threadIdx.x; i < cnt; i += kScatterThreads) {
     const uint64_t k = sk[i];
-    const int d = (int)((k >> shift) & 255u);
+    const int d = (int)((k >> shift) & (D - 1));
     const uint32_t dst = gbase[d] + (uint32_t)(i - (int)lstart[d]);
     kout[dst] = k;
     vout[dst] = sv[i];
   }
-}
-
-// k_sort_scatter needs more than the default 48 KB of dynamic shared memory
-void sort_scatter(int64_t n, const uint64_t* kin, const int32_t* vin, uint64_t* kout,
-                  int32_t* vout, int shift, const uint32_t* offs, int nblocks, cudaStream_t s) {
-  static thread_local int configured_device = -1;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (configured_device != dev) {
-    cudaFuncSetAttribute(k_sort_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, kScatterSmem);
-    configured_device = dev;
-  }
-  COUNT_LAUNCH();
-  k_sort_scatter<<<nblocks, kScatterThreads, kScatterSmem, s>>>(n, kin, vin, kout, vout, shift,
-                                                                 offs, nblocks);
 }
 
 // ---------------------------------------------------------------------------
@@ -459,34 +455,68 @@ void exclusive_scan(const T* in, T* out, int64_t n, T* tmp, cudaStream_t s) {
   k_scan_apply<T><<<(unsigned)nb, kThreads, 0, s>>>(in, n, tmp, out);
 }
 
+// One LSD pass over digit bits [shift, shift + kBits): histogram, scan of the
+// (digit, block) counts, scatter.  hist holds (1 << kBits) * nblocks + 1
+// counts; k_sort_scatter needs more than the default 48 KB of dynamic shared
+// memory.
+template <int kBits>
+void sort_pass(int64_t n, const uint64_t* kin, const int32_t* vin, uint64_t* kout, int32_t* vout,
+               int shift, uint32_t* hist, uint32_t* scan_tmp, cudaStream_t s) {
+  static thread_local int configured_device = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (configured_device != dev) {
+    cudaFuncSetAttribute(k_sort_scatter<kBits>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         scatter_smem<kBits>());
+    configured_device = dev;
+  }
+  const int nb = (int)((n + kSortChunk - 1) / kSortChunk);
+  COUNT_LAUNCH();
+  k_sort_hist<kBits><<<nb, kThreads, 0, s>>>(n, kin, shift, hist, nb);
+  exclusive_scan<uint32_t>(hist, hist, (int64_t)(1 << kBits) * nb, scan_tmp, s);
+  COUNT_LAUNCH();
+  k_sort_scatter<kBits><<<nb, kScatterThreads, scatter_smem<kBits>(), s>>>(n, kin, vin, kout, vout,
+                                                                          shift, hist, nb);
+}
+
 // ---------------------------------------------------------------------------
 // Permute the payload into key order, flag duplicates (module_domains.f90:199-234)
 // ---------------------------------------------------------------------------
-// Particles into key order: one 32-byte gather per particle from the packed
-// copy that k_keys wrote.
-__global__ void k_permute(int64_t n, const uint64_t* __restrict__ skey,
-                          const int32_t* __restrict__ sval, const double4* __restrict__ packed,
-                          double* __restrict__ xo, double* __restrict__ yo,
-                          double* __restrict__ zo, double* __restrict__ qo,
-                          int64_t* __restrict__ ko, int64_t* __restrict__ korig,
-                          int32_t* __restrict__ perm, unsigned long long* dupcount,
-                          int32_t* duplist, int dupcap) {
+// The sorted keys (also kept as the keys before the duplicate fix), and the
+// positions i with key(i + 1) == key(i).
+__global__ void k_sorted_keys(int64_t n, const uint64_t* __restrict__ skey,
+                              int64_t* __restrict__ ko, int64_t* __restrict__ korig,
+                              unsigned long long* dupcount, int32_t* duplist, int dupcap) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    int32_t j = sval[i];
-    uint64_t k = skey[i];
-    const double4 p = packed[j];
-    xo[i] = p.x;
-    yo[i] = p.y;
-    zo[i] = p.z;
-    qo[i] = p.w;
+    const uint64_t k = skey[i];
     ko[i] = (int64_t)k;
     korig[i] = (int64_t)k;
-    perm[i] = j;
     if (i + 1 < n && skey[i + 1] == k) {
       unsigned long long slot = atomicAdd(dupcount, 1ull);
       if (slot < (unsigned long long)dupcap) duplist[slot] = (int32_t)i;
     }
+  }
+}
+
+// Particles into key order: one 32-byte gather per particle from the packed
+// copy that k_keys wrote, with the charge from qsrc instead when the charges
+// arrived after the keys were formed (the host-array grow uploads them while
+// the keys are sorted).
+__global__ void k_gather(int64_t n, const int32_t* __restrict__ sval,
+                         const double4* __restrict__ packed, const double* __restrict__ qsrc,
+                         double* __restrict__ xo, double* __restrict__ yo,
+                         double* __restrict__ zo, double* __restrict__ qo,
+                         int32_t* __restrict__ perm) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t j = sval[i];
+    const double4 p = packed[j];
+    xo[i] = p.x;
+    yo[i] = p.y;
+    zo[i] = p.z;
+    qo[i] = qsrc ? qsrc[j] : p.w;
+    perm[i] = j;
   }
 }
 
@@ -523,13 +553,13 @@ __device__ void key_to_intcoord_morton(int64_t key, int64_t ic[3]) {
 }
 
 // Duplicate-key fix, module_domains.f90:268-307, executed in the reference's
-// sequential order by one thread over the (rare) duplicate positions.  Keys
-// that changed get new coordinates from key_to_coord (module_spacefilling.f90:445-471).
-__global__ void k_dupfix(int64_t n, int64_t* __restrict__ key, const int64_t* __restrict__ korig,
-                         double* __restrict__ x, double* __restrict__ y, double* __restrict__ z,
-                         const unsigned long long* __restrict__ dupcount,
-                         int32_t* __restrict__ duplist, int dupcap, const double* __restrict__ box,
-                         int curve, uint32_t* status) {
+// sequential order by one thread over the (rare) duplicate positions.  The
+// range of positions whose key may have changed goes to range[0..1] for
+// k_dupfix_coords.
+__global__ void k_dupfix_keys(int64_t n, int64_t* __restrict__ key,
+                              const unsigned long long* __restrict__ dupcount,
+                              int32_t* __restrict__ duplist, int dupcap,
+                              int64_t* __restrict__ range, uint32_t* status) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   unsigned long long nd = *dupcount;
   if (nd == 0) return;
@@ -571,7 +601,23 @@ __global__ void k_dupfix(int64_t n, int64_t* __restrict__ key, const int64_t* __
       }
     }
   }
-  for (int64_t i = lo_changed; i <= hi_changed; ++i) {
+  range[0] = lo_changed;
+  range[1] = hi_changed;
+}
+
+// The particles whose key the fix changed get the coordinates of their new
+// key (key_to_coord, module_spacefilling.f90:445-471); runs after the gather.
+__global__ void k_dupfix_coords(int64_t n, const int64_t* __restrict__ key,
+                                const int64_t* __restrict__ korig, double* __restrict__ x,
+                                double* __restrict__ y, double* __restrict__ z,
+                                const unsigned long long* __restrict__ dupcount, int dupcap,
+                                const int64_t* __restrict__ range, const double* __restrict__ box,
+                                int curve) {
+  const unsigned long long nd = *dupcount;
+  if (nd == 0 || nd > (unsigned long long)dupcap) return;
+  const int64_t lo = range[0], hi = range[1];
+  for (int64_t i = lo + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= hi;
+       i += (int64_t)gridDim.x * blockDim.x) {
     if (key[i] == korig[i]) continue;
     int64_t ic[3];
     if (curve == PEPCG_CURVE_MORTON) key_to_intcoord_morton(key[i], ic);
@@ -643,6 +689,27 @@ __global__ void k_node_counts(int64_t n, const int64_t* __restrict__ key,
   __syncthreads();
   if (threadIdx.x == 0 && bmax > 0) atomicMax(maxlev, bmax);
   if (threadIdx.x <= kMaxLevel && h[threadIdx.x]) atomicAdd(&lvl[threadIdx.x], h[threadIdx.x]);
+}
+
+// The values the host needs before the rest of the tree can be launched,
+// into mapped host memory: the node starts of the last particle (scanned and
+// its own, their sum is the node count), box and boxlength2, the duplicate
+// count, the deepest leaf level, twigs per level and the status word.
+__global__ void k_grow_summary(int64_t n, const int32_t* __restrict__ sstart,
+                               const int32_t* __restrict__ cstart, const double* __restrict__ box,
+                               const unsigned long long* __restrict__ small,
+                               const uint32_t* __restrict__ status,
+                               const int32_t* __restrict__ lvl, Ctx::GrowSummary* out) {
+  const int t = threadIdx.x;
+  if (t < 9 + kMaxLevel + 1) out->box[t] = box[t];
+  if (t <= kMaxLevel) out->lvl[t] = lvl[t];
+  if (t == 0) {
+    out->dup_count = small[0];
+    out->starts_before_last = sstart[n - 1];
+    out->starts_last = cstart[n - 1];
+    out->status = *status;
+    out->max_level = *reinterpret_cast<const int*>(small + 2);
+  }
 }
 
 __device__ __forceinline__ int64_t group_end(const int64_t* __restrict__ key, int64_t n,
@@ -1058,21 +1125,30 @@ void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp
 // The LSD radix sort of the n (key, index) pairs in skey / sval: 8 passes of 8
 // bits, ping-ponging through skey_alt / sval_alt, so the result is back in
 // skey / sval.
-static void lsd_sort(Ctx* c, int64_t n, cudaStream_t s) {
+static void lsd_sort(Ctx* c, int64_t n, bool grow_keys, cudaStream_t s) {
   uint64_t* kin = c->skey.p;
   uint64_t* kout = c->skey_alt.p;
   int32_t* vin = c->sval.p;
   int32_t* vout = c->sval_alt.p;
-  const int nb = (int)((n + kSortChunk - 1) / kSortChunk);
-  for (int pass = 0; pass < 8; ++pass) {
-    const int shift = 8 * pass;
-    COUNT_LAUNCH();
-    k_sort_hist<<<nb, kThreads, 0, s>>>(n, kin, shift, c->hist.p, nb);
-    exclusive_scan<uint32_t>(c->hist.p, c->hist.p, 256 * (int64_t)nb,
-                             reinterpret_cast<uint32_t*>(c->scan_tmp.p), s);
-    sort_scatter(n, kin, vin, kout, vout, shift, c->hist.p, nb, s);
+  uint32_t* tmp = reinterpret_cast<uint32_t*>(c->scan_tmp.p);
+  auto swap = [&]() {
     std::swap(kin, kout);
     std::swap(vin, vout);
+  };
+  if (grow_keys) {
+    // bits 0 .. 59 in four passes of 9 bits and three of 8
+    for (int shift = 0; shift < 36; shift += 9, swap())
+      sort_pass<9>(n, kin, vin, kout, vout, shift, c->hist.p, tmp, s);
+    for (int shift = 36; shift < 60; shift += 8, swap())
+      sort_pass<8>(n, kin, vin, kout, vout, shift, c->hist.p, tmp, s);
+  } else {
+    for (int shift = 0; shift < 64; shift += 8, swap())
+      sort_pass<8>(n, kin, vin, kout, vout, shift, c->hist.p, tmp, s);
+  }
+  // an odd pass count leaves the result in the other buffers
+  if (kin != c->skey.p) {
+    std::swap(c->skey, c->skey_alt);
+    std::swap(c->sval, c->sval_alt);
   }
 }
 
@@ -1100,7 +1176,7 @@ static TieArgs tie_args(Ctx* c, int64_t n, const unsigned long long* ndup) {
 }
 
 int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const double* dz,
-                const double* dq) {
+                const double* dq, cudaEvent_t q_ready) {
   cudaStream_t s = c->stream;
   c->has_tree = false;
   if (n < 2) {
@@ -1118,8 +1194,8 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
       !ensure(c, c->q, n, "q") || !ensure(c, c->key, n, "key") || !ensure(c, c->perm, n, "perm") ||
       !ensure(c, c->skey, n, "skey") || !ensure(c, c->skey_alt, n, "skey_alt") ||
       !ensure(c, c->sval, n, "sval") || !ensure(c, c->sval_alt, n, "sval_alt") ||
-      !ensure(c, c->hist, 256 * nblk_sort + 1, "hist") ||
-      !ensure(c, c->scan_tmp, 2 * ((256 * nblk_sort + n) / 2048 + 64), "scan_tmp") ||
+      !ensure(c, c->hist, kMaxDigits * nblk_sort + 1, "hist") ||
+      !ensure(c, c->scan_tmp, 2 * ((kMaxDigits * nblk_sort + n) / 2048 + 64), "scan_tmp") ||
       !ensure(c, c->orig_key, n, "orig_key") || !ensure(c, c->dup_list, dupcap, "dup_list") ||
       !ensure(c, c->lev, n, "lev") || !ensure(c, c->lcpn, n, "lcpn") ||
       !ensure(c, c->cstart, n, "cstart") || !ensure(c, c->cend, n, "cend") ||
@@ -1144,34 +1220,31 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
   // keys
   COUNT_LAUNCH();
   static const HilbertTable htab = hilbert_table();
-  k_keys<<<std::min(grid_for(n), 148u * 8u), kThreads, 0, s>>>(n, dx, dy, dz, dq, c->d_box, c->prm.curve, htab,
-                                          c->skey.p, c->sval.p, c->packed.p);
+  k_keys<<<std::min(grid_for(n), 148u * 8u), kThreads, 0, s>>>(n, dx, dy, dz, q_ready ? nullptr : dq,
+                                                              c->d_box, c->prm.curve, htab,
+                                                              c->skey.p, c->sval.p, c->packed.p);
   cudaEventRecord(c->ev[1], s);
-  // sort: 8 LSD passes of 8 bits; the result is back in skey / sval
-  lsd_sort(c, n, s);
+  // sort: 7 LSD passes over the 60 key bits below the placeholder; the result
+  // is in skey / sval
+  lsd_sort(c, n, true, s);
   uint64_t* kin = c->skey.p;
   int32_t* vin = c->sval.p;
   COUNT_LAUNCH();
-  k_permute<<<grid_for(n), kThreads, 0, s>>>(n, kin, vin, c->packed.p, c->x.p, c->y.p, c->z.p,
-                                             c->q.p, c->key.p, c->orig_key.p, c->perm.p,
-                                             c->d_small, c->dup_list.p, dupcap);
+  k_sorted_keys<<<grid_for(n), kThreads, 0, s>>>(n, kin, c->key.p, c->orig_key.p, c->d_small,
+                                                 c->dup_list.p, dupcap);
   // equal keys in the reference's order (an empty launch when there are none),
-  // before the duplicate fix shifts them
+  // before the duplicate fix shifts them: the replay rewrites the sorted
+  // indices, which the gather below then follows
   {
     TieArgs ta = tie_args(c, n, c->d_small);
-    ta.packed = c->packed.p;
-    ta.x = c->x.p;
-    ta.y = c->y.p;
-    ta.z = c->z.p;
-    ta.q = c->q.p;
-    ta.perm = c->perm.p;
     if (!tie_order_launch(c, ta, s)) return PEPCG_ERR_CUDA;
   }
+  int64_t* dup_range = reinterpret_cast<int64_t*>(c->d_small + 12);
   COUNT_LAUNCH();
-  k_dupfix<<<1, 32, 0, s>>>(n, c->key.p, c->orig_key.p, c->x.p, c->y.p, c->z.p, c->d_small,
-                            c->dup_list.p, dupcap, c->d_box, c->prm.curve, c->d_status);
-  cudaEventRecord(c->ev[2], s);
-  // tree
+  k_dupfix_keys<<<1, 32, 0, s>>>(n, c->key.p, c->d_small, c->dup_list.p, dupcap, dup_range,
+                                 c->d_status);
+  cudaEventRecord(c->ev[8], s);
+  // tree: per-particle node counts and their scans
   COUNT_LAUNCH();
   k_node_counts<<<grid_for(n), kThreads, 0, s>>>(n, c->key.p, c->lev.p, c->lcpn.p, c->cstart.p,
                                                   c->cend.p, c->d_status,
@@ -1179,28 +1252,37 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
                                                   c->lvlcnt.p);
   exclusive_scan<int32_t>(c->cstart.p, c->sstart.p, n, c->scan_tmp.p, s);
   exclusive_scan<int32_t>(c->cend.p, c->send.p, n, c->scan_tmp.p + (n / 2048 + 32), s);
-  // total number of nodes M and the box go to the host (the grid sizes below need M)
-  int32_t last[2];
-  int32_t lastc;
-  if (!cuda_ok(c, cudaMemcpyAsync(&last[0], c->sstart.p + (n - 1), 4, cudaMemcpyDeviceToHost, s),
-               "M") ||
-      !cuda_ok(c, cudaMemcpyAsync(&lastc, c->cstart.p + (n - 1), 4, cudaMemcpyDeviceToHost, s),
-               "M") ||
-      !cuda_ok(c, cudaMemcpyAsync(c->box, c->d_box, 9 * sizeof(double), cudaMemcpyDeviceToHost, s),
-               "box") ||
-      !cuda_ok(c, cudaMemcpyAsync(c->boxlength2, c->d_box + 9, 21 * sizeof(double),
-                                  cudaMemcpyDeviceToHost, s), "box") ||
-      !cuda_ok(c, cudaMemcpyAsync(&c->dup_count, c->d_small, 8, cudaMemcpyDeviceToHost, s), "dup") ||
-      !cuda_ok(c, cudaMemcpyAsync(&c->max_level, c->d_small + 2, 4, cudaMemcpyDeviceToHost, s), "maxlev") ||
-      !cuda_ok(c, cudaMemcpyAsync(c->lvl_host, c->lvlcnt.p, sizeof(c->lvl_host),
-                                  cudaMemcpyDeviceToHost, s), "levels"))
-    return PEPCG_ERR_CUDA;
-  uint32_t st = 0;
-  if (!cuda_ok(c, cudaMemcpyAsync(&st, c->d_status, 4, cudaMemcpyDeviceToHost, s), "status") ||
-      !cuda_ok(c, cudaStreamSynchronize(s), "grow (keys/sort)"))
-    return PEPCG_ERR_CUDA;
-  if (st) return status_to_code(c, st);
-  const int64_t M = (int64_t)last[0] + lastc;
+  // the host needs the node count M (grid sizes, allocations), the box, the
+  // level counts and the status: one kernel writes them to mapped host memory
+  COUNT_LAUNCH();
+  k_grow_summary<<<1, 64, 0, s>>>(n, c->sstart.p, c->cstart.p, c->d_box, c->d_small, c->d_status,
+                                  c->lvlcnt.p, c->d_sum);
+  if (!cuda_ok(c, cudaEventRecord(c->sum_ev, s), "grow summary")) return PEPCG_ERR_CUDA;
+  cudaEventRecord(c->ev[9], s);
+  // the particles into key order run while the host waits for the summary
+  if (q_ready && !cuda_ok(c, cudaStreamWaitEvent(s, q_ready, 0), "charges")) return PEPCG_ERR_CUDA;
+  COUNT_LAUNCH();
+  k_gather<<<grid_for(n), kThreads, 0, s>>>(n, vin, c->packed.p, q_ready ? dq : nullptr, c->x.p,
+                                            c->y.p, c->z.p, c->q.p, c->perm.p);
+  COUNT_LAUNCH();
+  k_dupfix_coords<<<148 * 2, kThreads, 0, s>>>(n, c->key.p, c->orig_key.p, c->x.p, c->y.p, c->z.p,
+                                               c->d_small, dupcap, dup_range, c->d_box,
+                                               c->prm.curve);
+  cudaEventRecord(c->ev[2], s);
+  if (!cuda_ok(c, cudaEventSynchronize(c->sum_ev), "grow (keys/sort)")) return PEPCG_ERR_CUDA;
+  const Ctx::GrowSummary& gs = *c->h_sum;
+  for (int k = 0; k < 9; ++k) c->box[k] = gs.box[k];
+  for (int k = 0; k <= kMaxLevel; ++k) c->boxlength2[k] = gs.box[9 + k];
+  for (int k = 0; k <= kMaxLevel; ++k) c->lvl_host[k] = gs.lvl[k];
+  c->dup_count = (int64_t)gs.dup_count;
+  c->max_level = gs.max_level;
+  if (gs.status) {
+    // the gather and the fix were queued behind the summary: let them finish
+    // before the caller reuses the buffers
+    cudaStreamSynchronize(s);
+    return status_to_code(c, gs.status);
+  }
+  const int64_t M = (int64_t)gs.starts_before_last + gs.starts_last;
   // every particle starts at most kMaxLevel + 1 nodes
   if (M < 2 || M > (int64_t)(kMaxLevel + 1) * n || M >= (int64_t)INT32_MAX) {
     c->err = "node count out of range";
@@ -1306,8 +1388,8 @@ int sort_keys_device(Ctx* c, int64_t n, const int64_t* d_in, int64_t* d_kout, in
   const int64_t nblk_sort = (n + kSortChunk - 1) / kSortChunk;
   if (!ensure(c, c->skey, n, "skey") || !ensure(c, c->skey_alt, n, "skey_alt") ||
       !ensure(c, c->sval, n, "sval") || !ensure(c, c->sval_alt, n, "sval_alt") ||
-      !ensure(c, c->hist, 256 * nblk_sort + 1, "hist") ||
-      !ensure(c, c->scan_tmp, 2 * ((256 * nblk_sort + n) / 2048 + 64), "scan_tmp") ||
+      !ensure(c, c->hist, kMaxDigits * nblk_sort + 1, "hist") ||
+      !ensure(c, c->scan_tmp, 2 * ((kMaxDigits * nblk_sort + n) / 2048 + 64), "scan_tmp") ||
       !ensure(c, c->cstart, n, "cstart") || !ensure(c, c->cend, n, "cend") ||
       !ensure(c, c->sstart, n, "sstart") || !ensure(c, c->send, n, "send") ||
       !ensure(c, c->tiepre, n + 1, "tiepre"))
@@ -1318,7 +1400,7 @@ int sort_keys_device(Ctx* c, int64_t n, const int64_t* d_in, int64_t* d_kout, in
     return PEPCG_ERR_CUDA;
   COUNT_LAUNCH();
   k_sortkeys_load<<<grid_for(n), kThreads, 0, s>>>(n, d_in, c->skey.p, c->sval.p);
-  lsd_sort(c, n, s);
+  lsd_sort(c, n, false, s);
   count_pairs_launch(n, c->skey.p, npair, s);
   if (!tie_order_launch(c, tie_args(c, n, npair), s)) return PEPCG_ERR_CUDA;
   COUNT_LAUNCH();
@@ -1538,12 +1620,8 @@ extern "C" int pepcg_sort_keys_noalloc(int64_t n, const int64_t* d_keys_in, int6
   const int nb = (int)((n + kSortChunk - 1) / kSortChunk);
   COUNT_LAUNCH();
   k_noalloc_load<<<grid_for(n), kThreads, 0, s>>>(n, d_keys_in, kin, vin);
-  for (int pass = 0; pass < 8; ++pass) {
-    const int shift = 8 * pass;
-    COUNT_LAUNCH();
-    k_sort_hist<<<nb, kThreads, 0, s>>>(n, kin, shift, hist, nb);
-    exclusive_scan<uint32_t>(hist, hist, 256 * (int64_t)nb, tmp, s);
-    sort_scatter(n, kin, vin, kout, vout, shift, hist, nb, s);
+  for (int shift = 0; shift < 64; shift += 8) {
+    sort_pass<8>(n, kin, vin, kout, vout, shift, hist, tmp, s);
     std::swap(kin, kout);
     std::swap(vin, vout);
   }

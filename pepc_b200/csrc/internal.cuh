@@ -155,6 +155,21 @@ struct Ctx {
   double boxlength2[kMaxLevel + 1];
   int max_level = 0;
   int64_t dup_count = 0;
+  // What the host needs from the first half of a grow (node count, box,
+  // levels, status), written by one kernel into mapped pinned host memory:
+  // the host waits on sum_ev while the particle gather runs on the device.
+  struct GrowSummary {
+    double box[9 + kMaxLevel + 1];  // box, then boxlength2
+    unsigned long long dup_count;
+    int32_t starts_before_last;     // nodes started by particles 0 .. n-2
+    int32_t starts_last;            // nodes started by particle n-1
+    uint32_t status;
+    int32_t max_level;
+    int32_t lvl[kMaxLevel + 1];
+  };
+  GrowSummary* h_sum = nullptr;  // host address
+  GrowSummary* d_sum = nullptr;  // its device address
+  cudaEvent_t sum_ev = nullptr;
 
   // periodic lattice state
   bool periodic = false, far_field = false;
@@ -170,7 +185,10 @@ struct Ctx {
 
   // statistics
   pepcg_stats st{};
-  cudaEvent_t ev[8];
+  // phase events: [0] grow start, [1] keys done, [8] sort done, [9] node
+  // counts done, [2] particles in key order, [3] tree, [4] upward; [5..7] walk
+  static constexpr int kEvents = 10;
+  cudaEvent_t ev[kEvents];
   bool grow_times_pending = false;
 
   // host-transfer overlap (the host-array entry points): one stream per copy
@@ -227,8 +245,10 @@ bool ensure(Ctx* c, DBuf<T>& b, size_t n, const char* what);
 int status_to_code(Ctx* c, uint32_t st);
 
 // ---- grow.cu ----
+// q_ready: the charges dq arrive after the keys are formed; the gather into
+// key order waits for this event and reads them from dq (null: dq is ready)
 int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const double* dz,
-                const double* dq);
+                const double* dq, cudaEvent_t q_ready = nullptr);
 // the local key sort in the reference's order (keys as unsigned 64-bit values)
 int sort_keys_device(Ctx* c, int64_t n, const int64_t* d_in, int64_t* d_kout, int64_t* d_pout);
 int export_tree(Ctx* c, int64_t* key, int32_t* level, int64_t* leaves, int64_t* desc,
@@ -256,10 +276,6 @@ struct TieArgs {
   int2* seg;                       // scratch: 2 * segcap ranges
   int64_t segcap;                  // tie_segcap(n)
   uint32_t* status;
-  // when packed is set, the particles of the equal runs are gathered again
-  const double4* packed;
-  double *x, *y, *z, *q;
-  int32_t* perm;
 };
 int64_t tie_segcap(int64_t n);
 bool tie_order_launch(Ctx* c, const TieArgs& a, cudaStream_t s);

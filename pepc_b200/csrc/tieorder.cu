@@ -16,7 +16,7 @@
 // k_tie_order replays the reference's class passes, only where they decide the
 // order of equal keys, and rewrites the permutation on the runs of equal keys.
 // It is one block: it returns at once when the sorted keys have no equal
-// neighbours (the count comes from k_permute or k_count_pairs), so the grow
+// neighbours (the count comes from k_sorted_keys or k_count_pairs), so the grow
 // pays one empty launch.  With ties, the replay covers:
 //  * the first class pass over all n elements (every tie lies in it);
 //  * then, level by level, only the class ranges that hold two equal keys:
@@ -294,16 +294,7 @@ __global__ void __launch_bounds__(kTieThreads, 1) k_tie_order(TieArgs a) {
   for (int i = tid; i < n; i += kTieThreads) {
     const bool tie = (a.dpre[i + 1] - a.dpre[i]) > 0 || (i > 0 && a.dpre[i] - a.dpre[i - 1] > 0);
     if (!tie) continue;
-    const int32_t j = a.A[i];
-    a.sval[i] = j;
-    if (a.packed) {
-      const double4 p = a.packed[j];
-      a.x[i] = p.x;
-      a.y[i] = p.y;
-      a.z[i] = p.z;
-      a.q[i] = p.w;
-      a.perm[i] = j;
-    }
+    a.sval[i] = a.A[i];
   }
 }
 

@@ -82,6 +82,9 @@ def test_c2_explosion_ten_steps(gpu):
         zeros = lambda: torch.zeros(n, dtype=torch.float64, device=dev)  # noqa: E731
         st = dict(x=T(x0), y=T(y0), z=T(z0), q=q, m=q.clone(), vx=zeros(), vy=zeros(), vz=zeros())
         tc = P.TreeCode(precision=prec, walk=walk, **kw)
+        # the library's device calls are ordered on its stream: put it on
+        # torch's, so the torch reads and fills here are ordered with them
+        tc.set_stream(torch.cuda.current_stream().cuda_stream)
         key = torch.empty(n, dtype=torch.int64, device=dev)
         perm = torch.empty(n, dtype=torch.int64, device=dev)
         out = [zeros() for _ in range(5)]

@@ -55,6 +55,7 @@ def test_mixed_4m_meets_the_accuracy_bar(gpu, plummer4m, theta):
     med = {}
     for prec, walk in ((P.PRECISION_MIXED, P.WALK_GROUP), (P.PRECISION_PLAIN, P.WALK_PER_TARGET)):
         tc = P.TreeCode(theta2=theta * theta, eps2=1e-6, precision=prec, walk=walk)
+        tc.set_stream(torch.cuda.current_stream().cuda_stream)  # ordered with the torch fills
         tc.grow_tree_device(*(torch.from_numpy(a).to(dev) for a in (x, y, z, q)))
         out = [torch.zeros(N4M, dtype=torch.float64, device=dev) for _ in range(5)]
         tc.traverse_self_device(*out)
@@ -82,6 +83,7 @@ def test_32m_particles_complete_and_accurate(gpu):
     x, y, z = (torch.from_numpy(rng.random(n)).to(dev) for _ in range(3))
     q = torch.full((n,), 1.0 / n, dtype=torch.float64, device=dev)
     tc = P.TreeCode(theta2=0.16, eps2=1e-8, precision=P.PRECISION_MIXED, walk=P.WALK_GROUP)
+    tc.set_stream(torch.cuda.current_stream().cuda_stream)  # ordered with the torch fills
     tc.grow_tree_device(x, y, z, q)  # raises on a node-pool or level overflow
     out = [torch.zeros(n, dtype=torch.float64, device=dev) for _ in range(5)]
     tc.traverse_self_device(*out)  # raises PEPCG_ERR_INCOMPLETE_WALK if a walk lost leaves

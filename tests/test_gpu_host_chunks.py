@@ -17,6 +17,7 @@ N = 300000  # above the chunking threshold (262,144 targets)
 
 def device_fields(tc, x, y, z, q, init=0.0):
     dev = torch.device("cuda", 0)
+    tc.set_stream(torch.cuda.current_stream().cuda_stream)  # ordered with the torch fills
     tc.grow_tree_device(*(torch.from_numpy(a).to(dev) for a in (x, y, z, q)))
     out = [torch.full((len(x),), init, dtype=torch.float64, device=dev) for _ in range(5)]
     tc.traverse_self_device(*out)
