@@ -499,7 +499,7 @@ __global__ void k_adj_down_level(int level, const int32_t* __restrict__ lvl,
       const bool leafc = (lm >> k) & 1u;
       double pcv[3] = {0, 0, 0};
       if (!leafc) {
-        const double* dm = dmom + 9 * (int64_t)(ts + __popc(~lm & ((1u << k) - 1u)));
+        const double* dm = dmom + kDmomStride * (int64_t)(ts + __popc(~lm & ((1u << k) - 1u)));
         for (int j = 0; j < 3; ++j) pcv[j] = dm[j];
       }
       const double qc = cc.w;

@@ -953,12 +953,15 @@ __global__ void __launch_bounds__(256) k_level_scatter(int64_t M, const int2* __
 // Memory: a twig's own data (twig list, tinfo, scanned counts) is read at
 // its list position; its children's records from the level-ordered copy
 // (drec: consecutive threads read consecutive runs), and its twig children's
-// nine moments from dmom at their twig-list positions, likewise consecutive
-// for consecutive parents.  The children's records are re-read by each sum
-// (L1 hits) rather than held in registers, which keeps the kernel at 68
-// registers and lets more twigs be in flight per SM.  The twig writes its
-// record both to the RPO arrays the walks read (nc4, mom, mom32, all whole
-// sectors) and to the level-ordered copy its parent will read.
+// nine moments from dmom at their twig-list positions (kDmomStride doubles
+// each), likewise consecutive for consecutive parents.  The kernel is bound by
+// its count of scattered memory instructions (each warp load touches ~10
+// sectors), so the children are read in two passes (the sums that give the
+// centre, then the shifted moments; the second pass re-reads from L1 rather
+// than holding eight records in registers), centres as single 256-bit loads.
+// The twig writes its record both to the RPO arrays the walks read (nc4, mom,
+// mom32: whole sectors, 256-bit stores) and to the level-ordered copy its
+// parent will read.
 constexpr int kUpThreads = 128;
 
 __global__ void __launch_bounds__(kUpThreads) k_upward_level(
@@ -979,41 +982,35 @@ __global__ void __launch_bounds__(kUpThreads) k_upward_level(
     const int cs = cfirst[P] + 1;  // level-order position of child slot 0
     const int ts = tfirst[P] + 1;  // twig-list position of the first twig child
     const LevelRecord* rc = drec + cs;
+    // one pass over the children for the charge, the |charge| and both
+    // centre-of-charge candidates (abs_charge-weighted, and the plain mean
+    // used when the |charge| sum is 0): each sum keeps its own order
     double charge = 0.0, absq = 0.0;
+    double wx = 0.0, wy = 0.0, wz = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
 #pragma unroll
-    for (int k = 7; k >= 0; --k)
-      if (k < nc) charge = charge + rc[k].pos.w;
-#pragma unroll
-    for (int k = 7; k >= 0; --k)
-      if (k < nc) absq = absq + rc[k].ab.x;
-    double cx = 0.0, cy = 0.0, cz = 0.0;
+    for (int k = 7; k >= 0; --k) {
+      if (k < nc) {
+        const double4 a = ld256(&rc[k].pos);
+        const double b = rc[k].ab.x;
+        charge = charge + a.w;
+        absq = absq + b;
+        wx = wx + a.x * b;
+        wy = wy + a.y * b;
+        wz = wz + a.z * b;
+        gx = gx + a.x;
+        gy = gy + a.y;
+        gz = gz + a.z;
+      }
+    }
+    double cx, cy, cz;
     if (absq != 0.0) {
-#pragma unroll
-      for (int k = 7; k >= 0; --k) {
-        if (k < nc) {
-          const double4 a = rc[k].pos;
-          const double b = rc[k].ab.x;
-          cx = cx + a.x * b;
-          cy = cy + a.y * b;
-          cz = cz + a.z * b;
-        }
-      }
-      cx = cx / absq;
-      cy = cy / absq;
-      cz = cz / absq;
+      cx = wx / absq;
+      cy = wy / absq;
+      cz = wz / absq;
     } else {
-#pragma unroll
-      for (int k = 7; k >= 0; --k) {
-        if (k < nc) {
-          const double4 a = rc[k].pos;
-          cx = cx + a.x;
-          cy = cy + a.y;
-          cz = cz + a.z;
-        }
-      }
-      cx = cx / (double)nc;
-      cy = cy / (double)nc;
-      cz = cz / (double)nc;
+      cx = gx / (double)nc;
+      cy = gy / (double)nc;
+      cz = gz / (double)nc;
     }
     double d0 = 0, d1 = 0, d2 = 0, q0 = 0, q1 = 0, q2 = 0, xy = 0, yz = 0, zx = 0;
     double bmax = 0.0;
@@ -1021,11 +1018,16 @@ __global__ void __launch_bounds__(kUpThreads) k_upward_level(
     for (int k = 7; k >= 0; --k) {
       if (k < nc) {
         const bool lf = (lm >> k) & 1u;
-        const double* src = dmom + 9 * (int64_t)(ts + __popc(~lm & ((1u << k) - 1u)));
-        double m[9];
+        const double2* src = reinterpret_cast<const double2*>(
+            dmom + kDmomStride * (int64_t)(ts + __popc(~lm & ((1u << k) - 1u))));
+        double m[10];
 #pragma unroll
-        for (int j = 0; j < 9; ++j) m[j] = lf ? 0.0 : src[j];
-        const double4 a = rc[k].pos;
+        for (int j = 0; j < 5; ++j) {
+          const double2 v = lf ? make_double2(0.0, 0.0) : src[j];
+          m[2 * j] = v.x;
+          m[2 * j + 1] = v.y;
+        }
+        const double4 a = ld256(&rc[k].pos);
         const double s0 = cx - a.x, s1 = cy - a.y, s2 = cz - a.z;
         const double q = a.w;
         d0 = (d0 + m[0]) + q * s0;
@@ -1042,30 +1044,29 @@ __global__ void __launch_bounds__(kUpThreads) k_upward_level(
       }
     }
     const double4 c4 = make_double4(cx, cy, cz, charge);
-    nc4[u] = c4;
-    LevelRecord r;
-    r.pos = c4;
-    r.ab = make_double2(absq, bmax);
-    r.link = make_int4(cs, level | (nc << 16), nleaves[u], (int)u);
-    drec[pu] = r;
-    double2* o = reinterpret_cast<double2*>(mom + kMomStride * u);
-    o[0] = make_double2(d0, d1);
-    o[1] = make_double2(d2, q0);
-    o[2] = make_double2(q1, q2);
-    o[3] = make_double2(xy, yz);
-    o[4] = make_double2(zx, absq);
-    o[5] = make_double2(bmax, 0.0);
-    double* od = dmom + 9 * (int64_t)P;
-    od[0] = d0; od[1] = d1; od[2] = d2; od[3] = q0; od[4] = q1; od[5] = q2;
-    od[6] = xy; od[7] = yz; od[8] = zx;
+    st256(nc4 + u, c4);
+    LevelRecord* rp = drec + pu;
+    st256(&rp->pos, c4);
+    rp->ab = make_double2(absq, bmax);
+    rp->link = make_int4(cs, level | (nc << 16), nleaves[u], (int)u);
+    double* o = mom + kMomStride * u;
+    st256(o, make_double4(d0, d1, d2, q0));
+    st256(o + 4, make_double4(q1, q2, xy, yz));
+    st256(o + 8, make_double4(zx, absq, bmax, 0.0));
+    double2* od = reinterpret_cast<double2*>(dmom + kDmomStride * (int64_t)P);
+    od[0] = make_double2(d0, d1);
+    od[1] = make_double2(d2, q0);
+    od[2] = make_double2(q1, q2);
+    od[3] = make_double2(xy, yz);
+    od[4] = make_double2(zx, 0.0);
     // FP32 copy for the mixed walk, the quadrupole matrix M (off-diagonals
     // halved) scaled by 3: (px, py, pz, 3qxx), (3qyy, 3qzz, 1.5qxy, 1.5qyz),
     // (1.5qzx, qxx+qyy+qzz, charge, 0), padded to a whole 64-byte record
     float4* m4 = mom32 + kMom32Stride * u;
-    m4[0] = make_float4((float)d0, (float)d1, (float)d2, (float)(3.0 * q0));
-    m4[1] = make_float4((float)(3.0 * q1), (float)(3.0 * q2), (float)(1.5 * xy), (float)(1.5 * yz));
-    m4[2] = make_float4((float)(1.5 * zx), (float)((q0 + q1) + q2), (float)charge, 0.f);
-    m4[3] = make_float4(0.f, 0.f, 0.f, 0.f);
+    st256f(m4, make_float4((float)d0, (float)d1, (float)d2, (float)(3.0 * q0)),
+           make_float4((float)(3.0 * q1), (float)(3.0 * q2), (float)(1.5 * xy), (float)(1.5 * yz)));
+    st256f(m4 + 2, make_float4((float)(1.5 * zx), (float)((q0 + q1) + q2), (float)charge, 0.f),
+           make_float4(0.f, 0.f, 0.f, 0.f));
   }
 }
 
@@ -1317,7 +1318,7 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
     const int64_t ntw = M - n;
     if (!ensure(c, c->lvlblk, 2 * nlb, "level blocks") ||
         !ensure(c, c->drec, M, "level records") || !ensure(c, c->lvlpos, M, "level positions") ||
-        !ensure(c, c->dmom, 9 * ntw, "dmom") ||
+        !ensure(c, c->dmom, kDmomStride * ntw, "dmom") ||
         !ensure(c, c->tinfo, ntw, "twig info") || !ensure(c, c->tcounts, 2 * ntw, "twig counts"))
       return PEPCG_ERR_OOM;
     int32_t* bt = c->lvlblk.p;

@@ -66,6 +66,27 @@ constexpr int kMomStride = 12;
 constexpr int kMomAbs = 9;
 constexpr int kMomBmax = 10;
 constexpr int kMom32Stride = 4;
+// The upward pass's level-ordered twig moments (dmom): the nine moments padded
+// to ten doubles, so that each entry is five aligned 16-byte pairs
+constexpr int kDmomStride = 10;
+
+// 256-bit global loads and stores (sm_100): one instruction for 32 bytes at a
+// 32-byte aligned address.  ld256 is free to be scheduled like a plain load:
+// only for data that the running kernel does not write.
+__device__ __forceinline__ double4 ld256(const void* p) {
+  double4 v;
+  asm("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];"
+               : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ void st256(void* p, double4 v) {
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(v.x), "d"(v.y), "d"(v.z),
+               "d"(v.w) : "memory");
+}
+__device__ __forceinline__ void st256f(void* p, float4 a, float4 b) {
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(a.x),
+               "f"(a.y), "f"(a.z), "f"(a.w), "f"(b.x), "f"(b.y), "f"(b.z), "f"(b.w) : "memory");
+}
 
 // The upward pass's level-ordered copy of a node: centre and charge,
 // (abs_charge, bmax), and the links by which the 64-target group walk
