@@ -186,7 +186,7 @@ __global__ void k_keys(int64_t n, const double* __restrict__ x, const double* __
        i += (int64_t)gridDim.x * blockDim.x) {
     const double xi = x[i], yi = y[i], zi = z[i];
     // the particle, packed in input order for the permutation's gather
-    packed[i] = make_double4(xi, yi, zi, q ? q[i] : 0.0);
+    st256(packed + i, make_double4(xi, yi, zi, q ? q[i] : 0.0));
     const int64_t i0 = quantise(xi, sb[0], sb[3], sb[6]);
     const int64_t i1 = quantise(yi, sb[1], sb[4], sb[7]);
     const int64_t i2 = quantise(zi, sb[2], sb[5], sb[8]);
@@ -401,58 +401,103 @@ __device__ __forceinline__ T block_exclusive_scan(T v, T* smem, T& total) {
   return wpre + x - v;
 }
 
+// One or two arrays of the same length per launch (blockIdx.y picks the
+// array); block sums at bsum[blockIdx.y * gridDim.x + blockIdx.x].
 template <class T>
-__global__ void k_scan_reduce(const T* __restrict__ in, int64_t n, T* __restrict__ bsum) {
-  __shared__ T sm[32];
-  int64_t base = (int64_t)blockIdx.x * kScanTile;
-  T s = 0;
-  for (int k = 0; k < kScanItems; ++k) {
-    int64_t i = base + (int64_t)threadIdx.x * kScanItems + k;
-    if (i < n) s += in[i];
+struct ScanPair {
+  const T* in[2];
+  T* out[2];
+};
+
+// a thread's kScanItems consecutive values: two 16-byte loads for a full tile
+// of an aligned array, else element by element
+template <class T>
+__device__ __forceinline__ void scan_load(const T* __restrict__ in, int64_t base, int64_t n,
+                                          T (&v)[kScanItems]) {
+  static_assert(sizeof(T) == 4 && kScanItems == 8, "two 16-byte loads per thread");
+  const int64_t i0 = base + (int64_t)threadIdx.x * kScanItems;
+  if (base + kScanTile <= n && ((reinterpret_cast<uintptr_t>(in) & 15) == 0)) {
+    const int4 a = reinterpret_cast<const int4*>(in + i0)[0];
+    const int4 b = reinterpret_cast<const int4*>(in + i0)[1];
+    v[0] = (T)a.x; v[1] = (T)a.y; v[2] = (T)a.z; v[3] = (T)a.w;
+    v[4] = (T)b.x; v[5] = (T)b.y; v[6] = (T)b.z; v[7] = (T)b.w;
+  } else {
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) v[k] = i0 + k < n ? in[i0 + k] : T(0);
   }
+}
+
+template <class T>
+__global__ void k_scan_reduce(ScanPair<T> a, int64_t n, T* __restrict__ bsum) {
+  __shared__ T sm[32];
+  const int64_t base = (int64_t)blockIdx.x * kScanTile;
+  T v[kScanItems];
+  scan_load<T>(blockIdx.y ? a.in[1] : a.in[0], base, n, v);
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) s += v[k];
   T tot;
   block_exclusive_scan<T>(s, sm, tot);
-  if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+  if (threadIdx.x == 0) bsum[(int64_t)blockIdx.y * gridDim.x + blockIdx.x] = tot;
 }
 
 // Each block adds the sums of the blocks before it itself (at most a few
 // thousand integers, read from L2) instead of a separate single-block scan of
 // the block sums: one launch fewer per scan.
 template <class T>
-__global__ void k_scan_apply(const T* __restrict__ in, int64_t n, const T* __restrict__ bsum,
-                             T* __restrict__ out) {
+__global__ void k_scan_apply(ScanPair<T> a, int64_t n, const T* __restrict__ bsum) {
   __shared__ T sm[32];
+  const T* bs = bsum + (int64_t)blockIdx.y * gridDim.x;
   T pre = 0;
-  for (int64_t b = threadIdx.x; b < (int64_t)blockIdx.x; b += blockDim.x) pre += bsum[b];
+  for (int64_t b = threadIdx.x; b < (int64_t)blockIdx.x; b += blockDim.x) pre += bs[b];
   {
     T t;
     block_exclusive_scan<T>(pre, sm, t);
     pre = t;
   }
-  int64_t base = (int64_t)blockIdx.x * kScanTile;
+  const int64_t base = (int64_t)blockIdx.x * kScanTile;
   T v[kScanItems];
+  scan_load<T>(blockIdx.y ? a.in[1] : a.in[0], base, n, v);
   T s = 0;
-  for (int k = 0; k < kScanItems; ++k) {
-    int64_t i = base + (int64_t)threadIdx.x * kScanItems + k;
-    v[k] = i < n ? in[i] : T(0);
-    s += v[k];
-  }
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) s += v[k];
   T tot;
   T ex = block_exclusive_scan<T>(s, sm, tot) + pre;
+  T* out = blockIdx.y ? a.out[1] : a.out[0];
+  const int64_t i0 = base + (int64_t)threadIdx.x * kScanItems;
+  T o[kScanItems];
+#pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
-    int64_t i = base + (int64_t)threadIdx.x * kScanItems + k;
-    if (i < n) out[i] = ex;
+    o[k] = ex;
     ex += v[k];
   }
+  if (base + kScanTile <= n && ((reinterpret_cast<uintptr_t>(out) & 15) == 0)) {
+    reinterpret_cast<int4*>(out + i0)[0] = make_int4((int)o[0], (int)o[1], (int)o[2], (int)o[3]);
+    reinterpret_cast<int4*>(out + i0)[1] = make_int4((int)o[4], (int)o[5], (int)o[6], (int)o[7]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+      if (i0 + k < n) out[i0 + k] = o[k];
+  }
+}
+
+// exclusive scans of one array, or of two arrays of the same length in the
+// same launches (tmp: one block sum per 2048 elements and array)
+template <class T>
+void exclusive_scan2(const T* in0, T* out0, const T* in1, T* out1, int64_t n, T* tmp,
+                     cudaStream_t s) {
+  const int64_t nb = (n + kScanTile - 1) / kScanTile;
+  ScanPair<T> a{{in0, in1}, {out0, out1}};
+  const dim3 grid((unsigned)nb, in1 ? 2u : 1u);
+  COUNT_LAUNCH();
+  k_scan_reduce<T><<<grid, kThreads, 0, s>>>(a, n, tmp);
+  COUNT_LAUNCH();
+  k_scan_apply<T><<<grid, kThreads, 0, s>>>(a, n, tmp);
 }
 
 template <class T>
 void exclusive_scan(const T* in, T* out, int64_t n, T* tmp, cudaStream_t s) {
-  int64_t nb = (n + kScanTile - 1) / kScanTile;
-  COUNT_LAUNCH();
-  k_scan_reduce<T><<<(unsigned)nb, kThreads, 0, s>>>(in, n, tmp);
-  COUNT_LAUNCH();
-  k_scan_apply<T><<<(unsigned)nb, kThreads, 0, s>>>(in, n, tmp, out);
+  exclusive_scan2<T>(in, out, nullptr, nullptr, n, tmp, s);
 }
 
 // One LSD pass over digit bits [shift, shift + kBits): histogram, scan of the
@@ -511,7 +556,7 @@ __global__ void k_gather(int64_t n, const int32_t* __restrict__ sval,
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const int32_t j = sval[i];
-    const double4 p = packed[j];
+    const double4 p = ld256(packed + j);
     xo[i] = p.x;
     yo[i] = p.y;
     zo[i] = p.z;
@@ -762,7 +807,7 @@ __global__ void k_build_nodes(int64_t n, int64_t M, const int64_t* __restrict__ 
       nleaves[rpo] = (int32_t)(e - s + 1);
       nkey[rpo] = (int64_t)prefix;
       if (leaf) {
-        nc4[rpo] = make_double4(x[s], y[s], z[s], q[s]);
+        st256(nc4 + rpo, make_double4(x[s], y[s], z[s], q[s]));
         leafnode[s] = (int32_t)rpo;
       }
     }
@@ -932,12 +977,13 @@ __global__ void __launch_bounds__(256) k_level_scatter(int64_t M, const int2* __
     ccnt[P] = nc;
     tcnt[P] = nc - __popc(lm);
   } else {
-    const double4 a = nc4[u];
-    LevelRecord r;
-    r.pos = a;
-    r.ab = make_double2(fabs(a.w), 0.0);
-    r.link = make_int4(0, L | kLeafFlag, 1, (int)u);
-    drec[p] = r;
+    // the record as two 256-bit stores: (centre, charge), then (|charge|,
+    // bmax = 0) and the links (first child 0, level | leaf flag, 1 leaf, u)
+    const double4 a = ld256(nc4 + u);
+    st256(drec + p, a);
+    st256(reinterpret_cast<double*>(drec + p) + 4,
+          make_double4(fabs(a.w), 0.0, __hiloint2double(L | kLeafFlag, 0),
+                       __hiloint2double((int)u, 1)));
   }
 }
 
@@ -1251,8 +1297,7 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
                                                   c->cend.p, c->d_status,
                                                   reinterpret_cast<int*>(c->d_small + 2),
                                                   c->lvlcnt.p);
-  exclusive_scan<int32_t>(c->cstart.p, c->sstart.p, n, c->scan_tmp.p, s);
-  exclusive_scan<int32_t>(c->cend.p, c->send.p, n, c->scan_tmp.p + (n / 2048 + 32), s);
+  exclusive_scan2<int32_t>(c->cstart.p, c->sstart.p, c->cend.p, c->send.p, n, c->scan_tmp.p, s);
   // the host needs the node count M (grid sizes, allocations), the box, the
   // level counts and the status: one kernel writes them to mapped host memory
   COUNT_LAUNCH();
@@ -1319,22 +1364,22 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
     if (!ensure(c, c->lvlblk, 2 * nlb, "level blocks") ||
         !ensure(c, c->drec, M, "level records") || !ensure(c, c->lvlpos, M, "level positions") ||
         !ensure(c, c->dmom, kDmomStride * ntw, "dmom") ||
-        !ensure(c, c->tinfo, ntw, "twig info") || !ensure(c, c->tcounts, 2 * ntw, "twig counts"))
+        !ensure(c, c->tinfo, ntw, "twig info") || !ensure(c, c->tcounts, 2 * ntw, "twig counts") ||
+        // block sums of the paired scans below
+        !ensure(c, c->scan_tmp, 2 * (std::max<int64_t>((int64_t)nlb, ntw) / kScanTile + 2), "scan_tmp"))
       return PEPCG_ERR_OOM;
     int32_t* bt = c->lvlblk.p;
     int32_t* ba = c->lvlblk.p + nlb;
     COUNT_LAUNCH();
     k_level_count<<<gM, kThreads, 0, s>>>(M, c->meta.p, bt, ba, (int)gM);
-    exclusive_scan<int32_t>(bt, bt, (int64_t)nlb, c->scan_tmp.p, s);
-    exclusive_scan<int32_t>(ba, ba, (int64_t)nlb, c->scan_tmp.p, s);
+    exclusive_scan2<int32_t>(bt, bt, ba, ba, (int64_t)nlb, c->scan_tmp.p, s);
     COUNT_LAUNCH();
     int32_t* cc = c->tcounts.p;
     int32_t* tcn = c->tcounts.p + ntw;
     k_level_scatter<<<gM, kThreads, 0, s>>>(M, c->meta.p, bt, ba, (int)gM, c->twiglist.p,
                                             c->nc4.p, c->drec.p, c->lvlpos.p, c->child8.p,
                                             c->nchild.p, c->tinfo.p, cc, tcn);
-    exclusive_scan<int32_t>(cc, cc, ntw, c->scan_tmp.p, s);
-    exclusive_scan<int32_t>(tcn, tcn, ntw, c->scan_tmp.p, s);
+    exclusive_scan2<int32_t>(cc, cc, tcn, tcn, ntw, c->scan_tmp.p, s);
     float4* m32 = reinterpret_cast<float4*>(c->mom32.p);
     for (int L = c->max_level - 1; L >= 0; --L) {
       const int64_t cnt = c->lvl_host[L];

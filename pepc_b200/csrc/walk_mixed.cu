@@ -784,7 +784,7 @@ __global__ void __launch_bounds__(kMixThreads, kStrict ? 4 : 5)
         int4 lk = make_int4(0, 0, 0, 0);
         if (node >= 0) {
           const LevelRecord* rec = A.drec + node;
-          a = rec->pos;
+          a = ld256(&rec->pos);
           lk = rec->link;
           cx = (float)(a.x - gx); cy = (float)(a.y - gy); cz = (float)(a.z - gz);
           if (lk.y & kLeafFlag) {
@@ -1486,7 +1486,7 @@ __global__ void __launch_bounds__(kMixThreads, 4)
         int4 lk = make_int4(0, 0, 0, 0);
         if (node >= 0) {
           const LevelRecord* rec = A.drec + node;
-          a = rec->pos;
+          a = ld256(&rec->pos);
           lk = rec->link;
           cx = (float)(a.x - gx); cy = (float)(a.y - gy); cz = (float)(a.z - gz);
           if (lk.y & kLeafFlag) {
