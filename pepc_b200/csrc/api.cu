@@ -351,7 +351,8 @@ int pepcg_create(void** out, const pepcg_params* p) {
             cuda_ok(nullptr, cudaHostAlloc((void**)&c->h_sum, sizeof(Ctx::GrowSummary),
                                            cudaHostAllocMapped), "grow summary") &&
             cuda_ok(nullptr, cudaHostGetDevicePointer((void**)&c->d_sum, c->h_sum, 0), "grow summary") &&
-            cuda_ok(nullptr, cudaEventCreateWithFlags(&c->sum_ev, cudaEventDisableTiming), "grow summary");
+            cuda_ok(nullptr, cudaEventCreateWithFlags(&c->sum_ev, cudaEventDisableTiming), "grow summary") &&
+            cuda_ok(nullptr, cudaEventCreateWithFlags(&c->keys_ev, cudaEventDisableTiming), "grow keys");
   if (!ok) {
     pepcg_destroy(c);
     return PEPCG_ERR_CUDA;
@@ -404,6 +405,7 @@ int pepcg_destroy(void* ctx) {
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->h_sum) cudaFreeHost(c->h_sum);
   if (c->sum_ev) cudaEventDestroy(c->sum_ev);
+  if (c->keys_ev) cudaEventDestroy(c->keys_ev);
   for (int i = 0; i < Ctx::kMaxChunks; ++i) {
     if (c->ready[i]) cudaEventDestroy(c->ready[i]);
     if (c->done[i]) cudaEventDestroy(c->done[i]);
@@ -511,22 +513,24 @@ int pepcg_grow_tree(void* ctx, int64_t n, const double* x, const double* y, cons
     if (rc && rc != PEPCG_WARN_NOT_NEUTRAL) return drain_copies(c, false), rc;
   }
   c->grow_times_pending = true;
-  // The outputs are final once the particles stand in key order and the
-  // duplicate fix has run (event 2, before the tree build): copy them back on
-  // the device-to-host stream while the tree build and the upward pass run on
-  // the context stream.  The call returns when the copies are done; the rest
-  // of the grow stays stream-ordered before the next call's work.
+  // Copy the outputs back on the device-to-host stream while the rest of the
+  // grow runs on the context stream: the keys and the permutation (the sorted
+  // indices) once the duplicate fix has shifted the keys (keys_ev), the
+  // coordinates once the particles stand in key order (event 2, before the
+  // tree build).  The call returns when the copies are done; the rest of the
+  // grow stays stream-ordered before the next call's work.
   cudaStream_t t = c->d2h;
-  bool ok = cuda_ok(c, cudaStreamWaitEvent(t, c->ev[2], 0), "grow outputs");
+  bool ok = cuda_ok(c, cudaStreamWaitEvent(t, c->keys_ev, 0), "grow outputs");
   if (key_out)
     ok = ok && cuda_ok(c, cudaMemcpyAsync(key_out, c->key.p, n * 8, cudaMemcpyDeviceToHost, t), "D2H key");
   if (perm_out) {
     // widened to 64 bits on the device (scratch: the target-key buffer)
     if (!ensure(c, c->tkeys, n, "perm")) return drain_copies(c, false), PEPCG_ERR_OOM;
-    ok = ok && widen_perm_device(c, c->tkeys.p, t) == PEPCG_OK &&
+    ok = ok && widen_perm_device(c, c->tkeys.p, t, c->sval.p) == PEPCG_OK &&
          cuda_ok(c, cudaMemcpyAsync(perm_out, c->tkeys.p, n * 8, cudaMemcpyDeviceToHost, t),
                  "D2H perm");
   }
+  ok = ok && cuda_ok(c, cudaStreamWaitEvent(t, c->ev[2], 0), "grow outputs");
   if (x_out) ok = ok && cuda_ok(c, cudaMemcpyAsync(x_out, c->x.p, n * 8, cudaMemcpyDeviceToHost, t), "D2H x");
   if (y_out) ok = ok && cuda_ok(c, cudaMemcpyAsync(y_out, c->y.p, n * 8, cudaMemcpyDeviceToHost, t), "D2H y");
   if (z_out) ok = ok && cuda_ok(c, cudaMemcpyAsync(z_out, c->z.p, n * 8, cudaMemcpyDeviceToHost, t), "D2H z");

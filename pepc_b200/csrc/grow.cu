@@ -1290,6 +1290,7 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
   COUNT_LAUNCH();
   k_dupfix_keys<<<1, 32, 0, s>>>(n, c->key.p, c->d_small, c->dup_list.p, dupcap, dup_range,
                                  c->d_status);
+  cudaEventRecord(c->keys_ev, s);  // keys and sorted indices final: the host grow copies them back
   cudaEventRecord(c->ev[8], s);
   // tree: per-particle node counts and their scans
   COUNT_LAUNCH();

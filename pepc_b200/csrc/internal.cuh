@@ -191,6 +191,7 @@ struct Ctx {
   GrowSummary* h_sum = nullptr;  // host address
   GrowSummary* d_sum = nullptr;  // its device address
   cudaEvent_t sum_ev = nullptr;
+  cudaEvent_t keys_ev = nullptr;  // the keys and the sorted indices are final (before the gather)
 
   // periodic lattice state
   bool periodic = false, far_field = false;
@@ -359,7 +360,9 @@ int gather_device(Ctx* c, const double* in, double* out);
 int potential_energy_device(Ctx* c, int64_t n, const double* q, const double* pot,
                             double* epot);
 int restore_device(Ctx* c, const double* in, double* out);
-int widen_perm_device(Ctx* c, int64_t* out, cudaStream_t st = nullptr);  // null: c->stream
+// out = the last grow's permutation as int64 (from src, default c->perm);
+// st null: c->stream
+int widen_perm_device(Ctx* c, int64_t* out, cudaStream_t st = nullptr, const int32_t* src = nullptr);
 int lattice_add(Ctx* c, int64_t nt, const double* tx, const double* ty, const double* tz,
                 double* ex, double* ey, double* ez, double* pot, bool overwrite);
 // adds the lattice term's dL/dq, dL/dx of the grown particles to dq..dz (the

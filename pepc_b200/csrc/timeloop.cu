@@ -230,9 +230,9 @@ int restore_device(Ctx* c, const double* in, double* out) {
   return cuda_ok(c, cudaGetLastError(), "restore") ? PEPCG_OK : PEPCG_ERR_CUDA;
 }
 
-int widen_perm_device(Ctx* c, int64_t* out, cudaStream_t st) {
+int widen_perm_device(Ctx* c, int64_t* out, cudaStream_t st, const int32_t* src) {
   COUNT_LAUNCH();
-  k_widen<<<grid_of(c->n), kTL, 0, st ? st : c->stream>>>(c->n, c->perm.p, out);
+  k_widen<<<grid_of(c->n), kTL, 0, st ? st : c->stream>>>(c->n, src ? src : c->perm.p, out);
   return cuda_ok(c, cudaGetLastError(), "perm") ? PEPCG_OK : PEPCG_ERR_CUDA;
 }
 

@@ -341,6 +341,13 @@ def test_errors_are_reported(gpu):
     with pytest.raises(P.PepcgError) as ei:
         tc.pepc_grow_tree(x, y, z, q)
     assert ei.value.code == P.PEPCG_ERR_BAD_ARG
+    # the failed grow's queued work (gather into key order) ends before the call
+    # returns: the same context grows the corrected set like a fresh one
+    x[7] = 0.25
+    g = tc.pepc_grow_tree(x, y, z, q)
+    go = O.Oracle().grow_tree(x, y, z, q)
+    assert np.array_equal(g.key, go["key"]) and np.array_equal(g.perm, go["perm"])
+    assert np.array_equal(g.x, go["x"])
     tc2 = P.TreeCode()
     with pytest.raises(P.PepcgError) as ei:
         tc2.pepc_traverse_tree([0.1], [0.1], [0.1])
