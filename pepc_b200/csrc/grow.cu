@@ -1169,9 +1169,10 @@ void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp
   exclusive_scan<int32_t>(in, out, n, tmp, s);
 }
 
-// The LSD radix sort of the n (key, index) pairs in skey / sval: 8 passes of 8
-// bits, ping-ponging through skey_alt / sval_alt, so the result is back in
-// skey / sval.
+// The LSD radix sort of the n (key, index) pairs in skey / sval, ping-ponging
+// through skey_alt / sval_alt.  Grow keys (placeholder bit 60, key bits 0..59)
+// take 7 passes over bits 0..59, any other 64-bit keys 8 passes of 8 bits; the
+// result is in skey / sval (after an odd pass count the buffers are swapped).
 static void lsd_sort(Ctx* c, int64_t n, bool grow_keys, cudaStream_t s) {
   uint64_t* kin = c->skey.p;
   uint64_t* kout = c->skey_alt.p;
