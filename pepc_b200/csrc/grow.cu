@@ -814,15 +814,23 @@ __global__ void k_build_nodes(int64_t n, int64_t M, const int64_t* __restrict__ 
   }
 }
 
-// links: parent / number of children (twigs) and key-order traversal pointers
-__global__ void k_link(int64_t M, const int2* __restrict__ meta,
+// links: parent / number of children (twigs) and key-order traversal pointers;
+// one node per thread, blocks of 256 nodes, each block also counting its
+// twigs and nodes per level for the level lists (bcnt_*[level * nblk + block])
+__global__ void __launch_bounds__(256) k_link(int64_t M, const int2* __restrict__ meta,
                        const int32_t* __restrict__ rpo2fpo, const int32_t* __restrict__ fpo2rpo,
                        int2* __restrict__ fwd, int2* __restrict__ fwdf,
                        int32_t* __restrict__ parent,
-                       int32_t* __restrict__ nchild, int4* __restrict__ child8) {
-  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < M;
-       u += (int64_t)gridDim.x * blockDim.x) {
+                       int32_t* __restrict__ nchild, int4* __restrict__ child8,
+                       int32_t* __restrict__ bcnt_twig, int32_t* __restrict__ bcnt_all, int nblk) {
+  __shared__ int ht[kMaxLevel + 1], ha[kMaxLevel + 1];
+  if (threadIdx.x <= kMaxLevel) ht[threadIdx.x] = ha[threadIdx.x] = 0;
+  __syncthreads();
+  const int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (u < M) {
     int2 mu = meta[u];
+    atomicAdd(&ha[mu.y & 0xff], 1);
+    if (!(mu.y & kLeafFlag)) atomicAdd(&ht[mu.y & 0xff], 1);
     const bool leaf = (mu.y & kLeafFlag) != 0;
     const int64_t size = (int64_t)mu.x - u;
     const int64_t f = rpo2fpo[u];
@@ -847,6 +855,11 @@ __global__ void k_link(int64_t M, const int2* __restrict__ meta,
       nchild[u] = 0;
     }
   }
+  __syncthreads();
+  if (threadIdx.x <= kMaxLevel) {
+    bcnt_twig[(int64_t)threadIdx.x * nblk + blockIdx.x] = ht[threadIdx.x];
+    bcnt_all[(int64_t)threadIdx.x * nblk + blockIdx.x] = ha[threadIdx.x];
+  }
 }
 
 // Twigs grouped by level for the upward pass and the adjoint's downward pass.
@@ -867,25 +880,6 @@ __device__ __forceinline__ int level_base(const int32_t* lvl, int level) {
   int b = 0;
   for (int l = 0; l < level; ++l) b += lvl[l];
   return b;
-}
-
-__global__ void __launch_bounds__(256) k_level_count(int64_t M, const int2* __restrict__ meta,
-                                                     int32_t* __restrict__ bcnt_twig,
-                                                     int32_t* __restrict__ bcnt_all, int nblk) {
-  __shared__ int ht[kMaxLevel + 1], ha[kMaxLevel + 1];
-  if (threadIdx.x <= kMaxLevel) ht[threadIdx.x] = ha[threadIdx.x] = 0;
-  __syncthreads();
-  const int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (u < M) {
-    const int2 mu = meta[u];
-    atomicAdd(&ha[mu.y & 0xff], 1);
-    if (!(mu.y & kLeafFlag)) atomicAdd(&ht[mu.y & 0xff], 1);
-  }
-  __syncthreads();
-  if (threadIdx.x <= kMaxLevel) {
-    bcnt_twig[(int64_t)threadIdx.x * nblk + blockIdx.x] = ht[threadIdx.x];
-    bcnt_all[(int64_t)threadIdx.x * nblk + blockIdx.x] = ha[threadIdx.x];
-  }
 }
 
 // rank of this lane among the block's lanes with the same key (-1: none),
@@ -1027,6 +1021,16 @@ __global__ void __launch_bounds__(kUpThreads) k_upward_level(
     const int pu = ti.y;
     const int cs = cfirst[P] + 1;  // level-order position of child slot 0
     const int ts = tfirst[P] + 1;  // twig-list position of the first twig child
+    // the twig children's moments are one run of dmom: into L1 now, so the
+    // second pass does not wait for them after the first
+    {
+      const int ntc = nc - __popc(lm);
+      const uintptr_t b0 = reinterpret_cast<uintptr_t>(dmom + kDmomStride * (int64_t)ts);
+      const uintptr_t b1 = reinterpret_cast<uintptr_t>(dmom + kDmomStride * (int64_t)(ts + ntc));
+      for (uintptr_t a = b0 & ~(uintptr_t)127; ntc > 0 && a < b1; a += 128)
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(a));
+    }
+    const int32_t nlv = nleaves[u];
     const LevelRecord* rc = drec + cs;
     // one pass over the children for the charge, the |charge| and both
     // centre-of-charge candidates (abs_charge-weighted, and the plain mean
@@ -1094,7 +1098,7 @@ __global__ void __launch_bounds__(kUpThreads) k_upward_level(
     LevelRecord* rp = drec + pu;
     st256(&rp->pos, c4);
     rp->ab = make_double2(absq, bmax);
-    rp->link = make_int4(cs, level | (nc << 16), nleaves[u], (int)u);
+    rp->link = make_int4(cs, level | (nc << 16), nlv, (int)u);
     double* o = mom + kMomStride * u;
     st256(o, make_double4(d0, d1, d2, q0));
     st256(o + 4, make_double4(q1, q2, xy, yz));
@@ -1352,28 +1356,27 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
                                                   c->nc4.p, c->meta.p, c->fpo2rpo.p, c->rpo2fpo.p,
                                                   c->first_part.p, c->nleaves.p, c->nkey.p,
                                                   c->leafnode.p);
+  // the level lists' per-block counts come from k_link: its blocks are the
+  // level lists' blocks of 256 nodes
+  const unsigned gM = (unsigned)((M + kThreads - 1) / kThreads);
+  const size_t nlb = (size_t)(kMaxLevel + 1) * gM;
+  const int64_t ntw = M - n;
+  if (!ensure(c, c->lvlblk, 2 * nlb, "level blocks") ||
+      !ensure(c, c->drec, M, "level records") || !ensure(c, c->lvlpos, M, "level positions") ||
+      !ensure(c, c->dmom, kDmomStride * ntw, "dmom") ||
+      !ensure(c, c->tinfo, ntw, "twig info") || !ensure(c, c->tcounts, 2 * ntw, "twig counts") ||
+      // block sums of the paired scans below
+      !ensure(c, c->scan_tmp, 2 * (std::max<int64_t>((int64_t)nlb, ntw) / kScanTile + 2), "scan_tmp"))
+    return PEPCG_ERR_OOM;
+  int32_t* bt = c->lvlblk.p;
+  int32_t* ba = c->lvlblk.p + nlb;
   COUNT_LAUNCH();
-  k_link<<<grid_for(M), kThreads, 0, s>>>(M, c->meta.p, c->rpo2fpo.p, c->fpo2rpo.p, c->fwd.p,
-                                          c->fwdf.p,
-                                          c->parent.p, c->nchild.p, c->child8.p);
+  k_link<<<gM, kThreads, 0, s>>>(M, c->meta.p, c->rpo2fpo.p, c->fpo2rpo.p, c->fwd.p, c->fwdf.p,
+                                 c->parent.p, c->nchild.p, c->child8.p, bt, ba, (int)gM);
   cudaEventRecord(c->ev[3], s);
   // twigs by level, then one launch per level, sized by the level's twig
   // count; the deepest twig level is one above the deepest leaf level
   {
-    const unsigned gM = (unsigned)((M + kThreads - 1) / kThreads);
-    const size_t nlb = (size_t)(kMaxLevel + 1) * gM;
-    const int64_t ntw = M - n;
-    if (!ensure(c, c->lvlblk, 2 * nlb, "level blocks") ||
-        !ensure(c, c->drec, M, "level records") || !ensure(c, c->lvlpos, M, "level positions") ||
-        !ensure(c, c->dmom, kDmomStride * ntw, "dmom") ||
-        !ensure(c, c->tinfo, ntw, "twig info") || !ensure(c, c->tcounts, 2 * ntw, "twig counts") ||
-        // block sums of the paired scans below
-        !ensure(c, c->scan_tmp, 2 * (std::max<int64_t>((int64_t)nlb, ntw) / kScanTile + 2), "scan_tmp"))
-      return PEPCG_ERR_OOM;
-    int32_t* bt = c->lvlblk.p;
-    int32_t* ba = c->lvlblk.p + nlb;
-    COUNT_LAUNCH();
-    k_level_count<<<gM, kThreads, 0, s>>>(M, c->meta.p, bt, ba, (int)gM);
     exclusive_scan2<int32_t>(bt, bt, ba, ba, (int64_t)nlb, c->scan_tmp.p, s);
     COUNT_LAUNCH();
     int32_t* cc = c->tcounts.p;
