@@ -1010,11 +1010,6 @@ __global__ void __launch_bounds__(kUpThreads) k_upward_level(
     const int32_t* __restrict__ tfirst, const int32_t* __restrict__ nleaves,
     LevelRecord* __restrict__ drec, double* __restrict__ dmom, double4* __restrict__ nc4,
     double* __restrict__ mom, float4* __restrict__ mom32) {
-  // Programmatic dependent launch: the next level's launch may begin once
-  // every block of this one has started; it reads its own list entries (all
-  // written before the first level ran) while this level finishes, and waits
-  // for this level's completion before it touches the records written here.
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int cnt = lvl[level];
   const int base = level_base(lvl, level);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
@@ -1026,10 +1021,6 @@ __global__ void __launch_bounds__(kUpThreads) k_upward_level(
     const int pu = ti.y;
     const int cs = cfirst[P] + 1;  // level-order position of child slot 0
     const int ts = tfirst[P] + 1;  // twig-list position of the first twig child
-    const int32_t nlv = nleaves[u];
-    // the previous level (the children) complete and visible; a no-op when
-    // this launch does not depend programmatically on the previous one
-    asm volatile("griddepcontrol.wait;" ::: "memory");
     // the twig children's moments are one run of dmom: into L1 now, so the
     // second pass does not wait for them after the first
     {
@@ -1039,6 +1030,7 @@ __global__ void __launch_bounds__(kUpThreads) k_upward_level(
       for (uintptr_t a = b0 & ~(uintptr_t)127; ntc > 0 && a < b1; a += 128)
         asm volatile("prefetch.global.L1 [%0];" ::"l"(a));
     }
+    const int32_t nlv = nleaves[u];
     const LevelRecord* rc = drec + cs;
     // one pass over the children for the charge, the |charge| and both
     // centre-of-charge candidates (abs_charge-weighted, and the plain mean
@@ -1394,34 +1386,13 @@ int grow_device(Ctx* c, int64_t n, const double* dx, const double* dy, const dou
                                             c->nchild.p, c->tinfo.p, cc, tcn);
     exclusive_scan2<int32_t>(cc, cc, tcn, tcn, ntw, c->scan_tmp.p, s);
     float4* m32 = reinterpret_cast<float4*>(c->mom32.p);
-    // each level after the first is a programmatic dependent launch of the
-    // one before (k_upward_level waits for it before reading its records)
-    bool first = true;
     for (int L = c->max_level - 1; L >= 0; --L) {
       const int64_t cnt = c->lvl_host[L];
       if (cnt <= 0) continue;
-      cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3(grid_for(cnt, kUpThreads));
-      cfg.blockDim = dim3(kUpThreads);
-      cfg.dynamicSmemBytes = 0;
-      cfg.stream = s;
-      cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-      attr[0].val.programmaticStreamSerializationAllowed = 1;
-      cfg.attrs = attr;
-      cfg.numAttrs = first ? 0 : 1;
-      first = false;
       COUNT_LAUNCH();
-      const int32_t* lvc = c->lvlcnt.p;
-      const int32_t* twl = c->twiglist.p;
-      const int2* tin = c->tinfo.p;
-      const int32_t* cf = cc;
-      const int32_t* tf = tcn;
-      const int32_t* nlp = c->nleaves.p;
-      if (!cuda_ok(c, cudaLaunchKernelEx(&cfg, k_upward_level, L, lvc, twl, tin, cf, tf, nlp,
-                                         c->drec.p, c->dmom.p, c->nc4.p, c->mom.p, m32),
-                   "upward level"))
-        return PEPCG_ERR_CUDA;
+      k_upward_level<<<grid_for(cnt, kUpThreads), kUpThreads, 0, s>>>(
+          L, c->lvlcnt.p, c->twiglist.p, c->tinfo.p, cc, tcn, c->nleaves.p, c->drec.p, c->dmom.p, c->nc4.p,
+          c->mom.p, m32);
     }
   }
   cudaEventRecord(c->ev[4], s);
